@@ -1,0 +1,141 @@
+// Shared device/host helpers for the cuopt_b200 PDLP library (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <utility>
+
+namespace cuopt_b200 {
+
+// Error carried from the device side back to the C interface.
+struct cuda_error : std::runtime_error {
+  explicit cuda_error(const std::string& s) : std::runtime_error(s) {}
+};
+
+#define B200_CUDA_CHECK(expr)                                                                 \
+  do {                                                                                       \
+    cudaError_t _e = (expr);                                                                 \
+    if (_e != cudaSuccess) {                                                                 \
+      throw ::cuopt_b200::cuda_error(std::string("CUDA error ") + cudaGetErrorString(_e) +   \
+                                     " at " + __FILE__ + ":" + std::to_string(__LINE__));    \
+    }                                                                                        \
+  } while (0)
+
+#define B200_LAUNCH_CHECK() B200_CUDA_CHECK(cudaGetLastError())
+
+constexpr int kWarp = 32;
+
+// Device buffer owning `n` elements of T.
+template <typename T>
+class dbuf {
+ public:
+  dbuf() = default;
+  explicit dbuf(size_t n) { resize(n); }
+  ~dbuf() { release(); }
+  dbuf(const dbuf&)            = delete;
+  dbuf& operator=(const dbuf&) = delete;
+  dbuf(dbuf&& o) noexcept : p_(o.p_), n_(o.n_)
+  {
+    o.p_ = nullptr;
+    o.n_ = 0;
+  }
+  dbuf& operator=(dbuf&& o) noexcept
+  {
+    if (this != &o) {
+      release();
+      p_   = o.p_;
+      n_   = o.n_;
+      o.p_ = nullptr;
+      o.n_ = 0;
+    }
+    return *this;
+  }
+  void resize(size_t n)
+  {
+    release();
+    if (n) B200_CUDA_CHECK(cudaMalloc(&p_, n * sizeof(T)));
+    n_ = n;
+  }
+  void release()
+  {
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    n_ = 0;
+  }
+  void zero(cudaStream_t s)
+  {
+    if (n_) B200_CUDA_CHECK(cudaMemsetAsync(p_, 0, n_ * sizeof(T), s));
+  }
+  void upload(const T* h, size_t n, cudaStream_t s)
+  {
+    if (n) B200_CUDA_CHECK(cudaMemcpyAsync(p_, h, n * sizeof(T), cudaMemcpyDefault, s));
+  }
+  void download(T* h, size_t n, cudaStream_t s) const
+  {
+    if (n) B200_CUDA_CHECK(cudaMemcpyAsync(h, p_, n * sizeof(T), cudaMemcpyDefault, s));
+  }
+  T* data() { return p_; }
+  const T* data() const { return p_; }
+  size_t size() const { return n_; }
+
+ private:
+  T* p_     = nullptr;
+  size_t n_ = 0;
+};
+
+#ifdef __CUDACC__
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_sum(float v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Neumaier-compensated running sum (FP64 norms and objectives of the termination test).
+struct ksum {
+  double s = 0.0, c = 0.0;
+  __device__ __forceinline__ void add(double v)
+  {
+    double t = s + v;
+    if (fabs(s) >= fabs(v))
+      c += (s - t) + v;
+    else
+      c += (v - t) + s;
+    s = t;
+  }
+  __device__ __forceinline__ double value() const { return s + c; }
+};
+
+// Streaming (evict-first) loads for matrix data that is read once per sweep, so the L2 keeps the
+// iterate vectors that the gathers reuse.
+__device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p); }
+__device__ __forceinline__ float ld_stream(const float* p) { return __ldcs(p); }
+__device__ __forceinline__ int ld_stream(const int* p) { return __ldcs(p); }
+
+#endif  // __CUDACC__
+
+#ifdef __CUDACC__
+#define B200_HD __host__ __device__
+#else
+#define B200_HD
+#endif
+
+B200_HD inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace cuopt_b200

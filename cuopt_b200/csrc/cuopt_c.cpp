@@ -1,0 +1,574 @@
+// The cuOpt LP C interface (see include/cuopt/linear_programming/cuopt_c.h).
+//
+// Behaviour mirrors the reference's cpp/src/pdlp/cuopt_c.cpp: the same null-argument checks, the
+// same return codes, input arrays copied at creation, getters copying into caller buffers.
+#include <cuopt/linear_programming/cuopt_c.h>
+#include <cuopt_b200.h>
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "lp_model.hpp"
+
+using cuopt_b200::lp_problem;
+using cuopt_b200::lp_settings;
+using cuopt_b200::lp_solution;
+
+namespace {
+
+constexpr int kVersionMajor = 26, kVersionMinor = 4, kVersionPatch = 0;
+
+// Copies n elements from a host or device pointer (the reference accepts both).
+template <typename T>
+void copy_in(std::vector<T>& dst, const T* src, size_t n)
+{
+  dst.resize(n);
+  if (n == 0) return;
+  cudaPointerAttributes attr{};
+  if (cudaPointerGetAttributes(&attr, src) == cudaSuccess &&
+      (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged)) {
+    if (cudaMemcpy(dst.data(), src, n * sizeof(T), cudaMemcpyDefault) != cudaSuccess)
+      throw std::invalid_argument("cannot read device array");
+    return;
+  }
+  cudaGetLastError();  // clear a "no device" / "invalid value" answer for plain host memory
+  std::memcpy(dst.data(), src, n * sizeof(T));
+}
+
+template <typename T>
+void copy_out(T* dst, const std::vector<T>& src)
+{
+  if (src.empty()) return;
+  cudaPointerAttributes attr{};
+  if (cudaPointerGetAttributes(&attr, dst) == cudaSuccess &&
+      (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged)) {
+    cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyDefault);
+    return;
+  }
+  cudaGetLastError();
+  std::memcpy(dst, src.data(), src.size() * sizeof(T));
+}
+
+lp_problem* P(cuOptOptimizationProblem p) { return static_cast<lp_problem*>(p); }
+lp_settings* S(cuOptSolverSettings s) { return static_cast<lp_settings*>(s); }
+lp_solution* R(cuOptSolution s) { return static_cast<lp_solution*>(s); }
+
+cuopt_int_t create_common(cuopt_int_t m, cuopt_int_t n, cuopt_int_t sense, cuopt_float_t offset,
+                          const cuopt_float_t* c, const cuopt_int_t* off, const cuopt_int_t* idx,
+                          const cuopt_float_t* val, const cuopt_float_t* vlo,
+                          const cuopt_float_t* vup, const char* vtypes, lp_problem* p)
+{
+  if (m < 0 || n < 0) return CUOPT_INVALID_ARGUMENT;
+  p->m          = m;
+  p->n          = n;
+  p->maximize   = sense == CUOPT_MAXIMIZE;
+  p->obj_offset = offset;
+  copy_in(p->c, c, n);
+  copy_in(p->row_off, off, (size_t)m + 1);
+  const int64_t nnz = p->row_off[m];
+  if (nnz < 0) return CUOPT_INVALID_ARGUMENT;
+  copy_in(p->col_idx, idx, (size_t)nnz);
+  copy_in(p->val, val, (size_t)nnz);
+  copy_in(p->var_lo, vlo, n);
+  copy_in(p->var_up, vup, n);
+  if (vtypes) {
+    std::vector<char> t;
+    copy_in(t, vtypes, n);
+    p->var_types.resize(n);
+    for (int j = 0; j < n; ++j) p->var_types[j] = t[j] == CUOPT_CONTINUOUS ? 'C' : 'I';
+  } else {
+    p->var_types.assign(n, 'C');
+  }
+  return CUOPT_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+int8_t cuOptGetFloatSize() { return sizeof(cuopt_float_t); }
+int8_t cuOptGetIntSize() { return sizeof(cuopt_int_t); }
+
+cuopt_int_t cuOptGetVersion(cuopt_int_t* major, cuopt_int_t* minor, cuopt_int_t* patch)
+{
+  if (!major || !minor || !patch) return CUOPT_INVALID_ARGUMENT;
+  *major = kVersionMajor;
+  *minor = kVersionMinor;
+  *patch = kVersionPatch;
+  return CUOPT_SUCCESS;
+}
+
+cuopt_int_t cuOptReadProblem(const char* filename, cuOptOptimizationProblem* problem_ptr)
+{
+  if (!filename || !problem_ptr) return CUOPT_INVALID_ARGUMENT;
+  auto* p = new (std::nothrow) lp_problem();
+  if (!p) return CUOPT_OUT_OF_MEMORY;
+  std::string err;
+  int rc = cuopt_b200::read_mps(filename, *p, err);
+  if (rc != CUOPT_SUCCESS) {
+    delete p;
+    *problem_ptr = nullptr;
+    return rc;
+  }
+  *problem_ptr = p;
+  return CUOPT_SUCCESS;
+}
+
+cuopt_int_t cuOptWriteProblem(cuOptOptimizationProblem problem, const char* filename,
+                              cuopt_int_t format)
+{
+  if (!problem || !filename || std::strlen(filename) == 0) return CUOPT_INVALID_ARGUMENT;
+  if (format != CUOPT_FILE_FORMAT_MPS) return CUOPT_INVALID_ARGUMENT;
+  return cuopt_b200::write_mps(*P(problem), filename);
+}
+
+cuopt_int_t cuOptCreateProblem(cuopt_int_t num_constraints, cuopt_int_t num_variables,
+                               cuopt_int_t objective_sense, cuopt_float_t objective_offset,
+                               const cuopt_float_t* objective_coefficients,
+                               const cuopt_int_t* constraint_matrix_row_offsets,
+                               const cuopt_int_t* constraint_matrix_column_indices,
+                               const cuopt_float_t* constraint_matrix_coefficent_values,
+                               const char* constraint_sense, const cuopt_float_t* rhs,
+                               const cuopt_float_t* lower_bounds,
+                               const cuopt_float_t* upper_bounds, const char* variable_types,
+                               cuOptOptimizationProblem* problem_ptr)
+{
+  if (!problem_ptr || !objective_coefficients || !constraint_matrix_row_offsets ||
+      !constraint_matrix_column_indices || !constraint_matrix_coefficent_values ||
+      !constraint_sense || !rhs || !lower_bounds || !upper_bounds || !variable_types)
+    return CUOPT_INVALID_ARGUMENT;
+  auto* p = new (std::nothrow) lp_problem();
+  if (!p) return CUOPT_OUT_OF_MEMORY;
+  try {
+    cuopt_int_t rc = create_common(num_constraints, num_variables, objective_sense,
+                                   objective_offset, objective_coefficients,
+                                   constraint_matrix_row_offsets, constraint_matrix_column_indices,
+                                   constraint_matrix_coefficent_values, lower_bounds, upper_bounds,
+                                   variable_types, p);
+    if (rc != CUOPT_SUCCESS) {
+      delete p;
+      return rc;
+    }
+    p->ranged = false;
+    copy_in(p->row_types, constraint_sense, num_constraints);
+    copy_in(p->rhs, rhs, num_constraints);
+  } catch (const std::exception&) {
+    delete p;
+    return CUOPT_INVALID_ARGUMENT;
+  }
+  *problem_ptr = p;
+  return CUOPT_SUCCESS;
+}
+
+cuopt_int_t cuOptCreateRangedProblem(cuopt_int_t num_constraints, cuopt_int_t num_variables,
+                                     cuopt_int_t objective_sense, cuopt_float_t objective_offset,
+                                     const cuopt_float_t* objective_coefficients,
+                                     const cuopt_int_t* constraint_matrix_row_offsets,
+                                     const cuopt_int_t* constraint_matrix_column_indices,
+                                     const cuopt_float_t* constraint_matrix_coefficients,
+                                     const cuopt_float_t* constraint_lower_bounds,
+                                     const cuopt_float_t* constraint_upper_bounds,
+                                     const cuopt_float_t* variable_lower_bounds,
+                                     const cuopt_float_t* variable_upper_bounds,
+                                     const char* variable_types,
+                                     cuOptOptimizationProblem* problem_ptr)
+{
+  if (!problem_ptr || !objective_coefficients || !constraint_matrix_row_offsets ||
+      !constraint_matrix_column_indices || !constraint_matrix_coefficients ||
+      !constraint_lower_bounds || !constraint_upper_bounds || !variable_lower_bounds ||
+      !variable_upper_bounds || !variable_types)
+    return CUOPT_INVALID_ARGUMENT;
+  auto* p = new (std::nothrow) lp_problem();
+  if (!p) return CUOPT_OUT_OF_MEMORY;
+  try {
+    cuopt_int_t rc =
+      create_common(num_constraints, num_variables, objective_sense, objective_offset,
+                    objective_coefficients, constraint_matrix_row_offsets,
+                    constraint_matrix_column_indices, constraint_matrix_coefficients,
+                    variable_lower_bounds, variable_upper_bounds, variable_types, p);
+    if (rc != CUOPT_SUCCESS) {
+      delete p;
+      return rc;
+    }
+    p->ranged = true;
+    copy_in(p->con_lo, constraint_lower_bounds, num_constraints);
+    copy_in(p->con_up, constraint_upper_bounds, num_constraints);
+  } catch (const std::exception&) {
+    delete p;
+    return CUOPT_INVALID_ARGUMENT;
+  }
+  *problem_ptr = p;
+  return CUOPT_SUCCESS;
+}
+
+cuopt_int_t cuOptCreateQuadraticProblem(cuopt_int_t, cuopt_int_t, cuopt_int_t, cuopt_float_t,
+                                        const cuopt_float_t*, const cuopt_int_t*,
+                                        const cuopt_int_t*, const cuopt_float_t*,
+                                        const cuopt_int_t*, const cuopt_int_t*,
+                                        const cuopt_float_t*, const char*, const cuopt_float_t*,
+                                        const cuopt_float_t*, const cuopt_float_t*,
+                                        cuOptOptimizationProblem* problem_ptr)
+{
+  if (problem_ptr) *problem_ptr = nullptr;
+  return CUOPT_INVALID_ARGUMENT;
+}
+
+cuopt_int_t cuOptCreateQuadraticRangedProblem(
+  cuopt_int_t, cuopt_int_t, cuopt_int_t, cuopt_float_t, const cuopt_float_t*, const cuopt_int_t*,
+  const cuopt_int_t*, const cuopt_float_t*, const cuopt_int_t*, const cuopt_int_t*,
+  const cuopt_float_t*, const cuopt_float_t*, const cuopt_float_t*, const cuopt_float_t*,
+  const cuopt_float_t*, cuOptOptimizationProblem* problem_ptr)
+{
+  if (problem_ptr) *problem_ptr = nullptr;
+  return CUOPT_INVALID_ARGUMENT;
+}
+
+void cuOptDestroyProblem(cuOptOptimizationProblem* problem_ptr)
+{
+  if (!problem_ptr || !*problem_ptr) return;
+  delete P(*problem_ptr);
+  *problem_ptr = nullptr;
+}
+
+#define CHECK2(a, b) \
+  if (!(a) || !(b)) return CUOPT_INVALID_ARGUMENT
+
+cuopt_int_t cuOptGetNumConstraints(cuOptOptimizationProblem problem, cuopt_int_t* v)
+{
+  CHECK2(problem, v);
+  *v = P(problem)->m;
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetNumVariables(cuOptOptimizationProblem problem, cuopt_int_t* v)
+{
+  CHECK2(problem, v);
+  *v = P(problem)->n;
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetObjectiveSense(cuOptOptimizationProblem problem, cuopt_int_t* v)
+{
+  CHECK2(problem, v);
+  *v = P(problem)->maximize ? CUOPT_MAXIMIZE : CUOPT_MINIMIZE;
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetObjectiveOffset(cuOptOptimizationProblem problem, cuopt_float_t* v)
+{
+  CHECK2(problem, v);
+  *v = P(problem)->obj_offset;
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetObjectiveCoefficients(cuOptOptimizationProblem problem, cuopt_float_t* v)
+{
+  CHECK2(problem, v);
+  copy_out(v, P(problem)->c);
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetNumNonZeros(cuOptOptimizationProblem problem, cuopt_int_t* v)
+{
+  CHECK2(problem, v);
+  *v = (cuopt_int_t)P(problem)->val.size();
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetConstraintMatrix(cuOptOptimizationProblem problem, cuopt_int_t* off,
+                                     cuopt_int_t* idx, cuopt_float_t* val)
+{
+  if (!problem || !off || !idx || !val) return CUOPT_INVALID_ARGUMENT;
+  copy_out(val, P(problem)->val);
+  copy_out(idx, P(problem)->col_idx);
+  copy_out(off, P(problem)->row_off);
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetConstraintSense(cuOptOptimizationProblem problem, char* v)
+{
+  CHECK2(problem, v);
+  copy_out(v, P(problem)->row_types);
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetConstraintRightHandSide(cuOptOptimizationProblem problem, cuopt_float_t* v)
+{
+  CHECK2(problem, v);
+  copy_out(v, P(problem)->rhs);
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetConstraintLowerBounds(cuOptOptimizationProblem problem, cuopt_float_t* v)
+{
+  CHECK2(problem, v);
+  copy_out(v, P(problem)->con_lo);
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetConstraintUpperBounds(cuOptOptimizationProblem problem, cuopt_float_t* v)
+{
+  CHECK2(problem, v);
+  copy_out(v, P(problem)->con_up);
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetVariableLowerBounds(cuOptOptimizationProblem problem, cuopt_float_t* v)
+{
+  CHECK2(problem, v);
+  copy_out(v, P(problem)->var_lo);
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetVariableUpperBounds(cuOptOptimizationProblem problem, cuopt_float_t* v)
+{
+  CHECK2(problem, v);
+  copy_out(v, P(problem)->var_up);
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetVariableTypes(cuOptOptimizationProblem problem, char* v)
+{
+  CHECK2(problem, v);
+  copy_out(v, P(problem)->var_types);
+  return CUOPT_SUCCESS;
+}
+
+cuopt_int_t cuOptCreateSolverSettings(cuOptSolverSettings* settings_ptr)
+{
+  if (!settings_ptr) return CUOPT_INVALID_ARGUMENT;
+  auto* s = new (std::nothrow) lp_settings();
+  if (!s) return CUOPT_OUT_OF_MEMORY;
+  *settings_ptr = s;
+  return CUOPT_SUCCESS;
+}
+void cuOptDestroySolverSettings(cuOptSolverSettings* settings_ptr)
+{
+  if (!settings_ptr) return;
+  delete S(*settings_ptr);
+  *settings_ptr = nullptr;
+}
+cuopt_int_t cuOptSetParameter(cuOptSolverSettings settings, const char* name, const char* value)
+{
+  if (!settings || !name || !value) return CUOPT_INVALID_ARGUMENT;
+  return S(settings)->set_from_string(name, value);
+}
+cuopt_int_t cuOptGetParameter(cuOptSolverSettings settings, const char* name, cuopt_int_t size,
+                              char* value)
+{
+  if (!settings || !name || !value || size <= 0) return CUOPT_INVALID_ARGUMENT;
+  std::string v;
+  if (S(settings)->get_as_string(name, v) != CUOPT_SUCCESS) return CUOPT_INVALID_ARGUMENT;
+  std::snprintf(value, size, "%s", v.c_str());
+  return CUOPT_SUCCESS;
+}
+// Integer setter falls back to the boolean registry (reference cuopt_c.cpp:642-660).
+cuopt_int_t cuOptSetIntegerParameter(cuOptSolverSettings settings, const char* name,
+                                     cuopt_int_t value)
+{
+  if (!settings || !name) return CUOPT_INVALID_ARGUMENT;
+  if (S(settings)->set_int(name, value) == CUOPT_SUCCESS) return CUOPT_SUCCESS;
+  return S(settings)->set_bool(name, value != 0);
+}
+cuopt_int_t cuOptGetIntegerParameter(cuOptSolverSettings settings, const char* name,
+                                     cuopt_int_t* value)
+{
+  if (!settings || !name || !value) return CUOPT_INVALID_ARGUMENT;
+  int32_t v;
+  if (S(settings)->get_int(name, v) == CUOPT_SUCCESS) {
+    *value = v;
+    return CUOPT_SUCCESS;
+  }
+  bool bv;
+  if (S(settings)->get_bool(name, bv) == CUOPT_SUCCESS) {
+    *value = bv ? 1 : 0;
+    return CUOPT_SUCCESS;
+  }
+  return CUOPT_INVALID_ARGUMENT;
+}
+cuopt_int_t cuOptSetFloatParameter(cuOptSolverSettings settings, const char* name,
+                                   cuopt_float_t value)
+{
+  if (!settings || !name) return CUOPT_INVALID_ARGUMENT;
+  return S(settings)->set_float(name, value);
+}
+cuopt_int_t cuOptGetFloatParameter(cuOptSolverSettings settings, const char* name,
+                                   cuopt_float_t* value)
+{
+  if (!settings || !name || !value) return CUOPT_INVALID_ARGUMENT;
+  return S(settings)->get_float(name, *value);
+}
+
+cuopt_int_t cuOptSetMIPGetSolutionCallback(cuOptSolverSettings, cuOptMIPGetSolutionCallback,
+                                           void*)
+{
+  return CUOPT_INVALID_ARGUMENT;
+}
+cuopt_int_t cuOptSetMIPSetSolutionCallback(cuOptSolverSettings, cuOptMIPSetSolutionCallback,
+                                           void*)
+{
+  return CUOPT_INVALID_ARGUMENT;
+}
+
+cuopt_int_t cuOptSetInitialPrimalSolution(cuOptSolverSettings settings,
+                                          const cuopt_float_t* primal, cuopt_int_t n)
+{
+  if (!settings || !primal || n <= 0) return CUOPT_INVALID_ARGUMENT;
+  try {
+    copy_in(S(settings)->initial_primal, primal, n);
+  } catch (const std::exception&) {
+    return CUOPT_INVALID_ARGUMENT;
+  }
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptSetInitialDualSolution(cuOptSolverSettings settings, const cuopt_float_t* dual,
+                                        cuopt_int_t m)
+{
+  if (!settings || !dual || m <= 0) return CUOPT_INVALID_ARGUMENT;
+  try {
+    copy_in(S(settings)->initial_dual, dual, m);
+  } catch (const std::exception&) {
+    return CUOPT_INVALID_ARGUMENT;
+  }
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptAddMIPStart(cuOptSolverSettings, const cuopt_float_t*, cuopt_int_t)
+{
+  return CUOPT_INVALID_ARGUMENT;
+}
+
+cuopt_int_t cuOptIsMIP(cuOptOptimizationProblem problem, cuopt_int_t* is_mip)
+{
+  CHECK2(problem, is_mip);
+  *is_mip = P(problem)->is_mip() ? 1 : 0;
+  return CUOPT_SUCCESS;
+}
+
+cuopt_int_t cuOptSolve(cuOptOptimizationProblem problem, cuOptSolverSettings settings,
+                       cuOptSolution* solution_ptr)
+{
+  if (!problem || !settings || !solution_ptr) return CUOPT_INVALID_ARGUMENT;
+  auto* sol = new (std::nothrow) lp_solution();
+  if (!sol) return CUOPT_OUT_OF_MEMORY;
+  *sol          = cuopt_b200::solve_problem(*P(problem), *S(settings));
+  *solution_ptr = sol;
+  return sol->error_code;
+}
+
+void cuOptDestroySolution(cuOptSolution* solution_ptr)
+{
+  if (!solution_ptr || !*solution_ptr) return;
+  delete R(*solution_ptr);
+  *solution_ptr = nullptr;
+}
+
+cuopt_int_t cuOptGetTerminationStatus(cuOptSolution solution, cuopt_int_t* v)
+{
+  CHECK2(solution, v);
+  *v = R(solution)->r.status;
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetErrorStatus(cuOptSolution solution, cuopt_int_t* v)
+{
+  CHECK2(solution, v);
+  *v = R(solution)->error_code;
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetErrorString(cuOptSolution solution, char* buf, cuopt_int_t size)
+{
+  CHECK2(solution, buf);
+  std::snprintf(buf, size, "%s", R(solution)->error_message.c_str());
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetPrimalSolution(cuOptSolution solution, cuopt_float_t* v)
+{
+  CHECK2(solution, v);
+  copy_out(v, R(solution)->r.x);
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetObjectiveValue(cuOptSolution solution, cuopt_float_t* v)
+{
+  CHECK2(solution, v);
+  *v = R(solution)->r.primal_obj;
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetSolveTime(cuOptSolution solution, cuopt_float_t* v)
+{
+  CHECK2(solution, v);
+  *v = R(solution)->r.solve_time;
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetMIPGap(cuOptSolution solution, cuopt_float_t* v)
+{
+  CHECK2(solution, v);
+  return CUOPT_INVALID_ARGUMENT;  // LP solution (reference cuopt_c.cpp:1030-1045)
+}
+cuopt_int_t cuOptGetSolutionBound(cuOptSolution solution, cuopt_float_t* v)
+{
+  CHECK2(solution, v);
+  return CUOPT_INVALID_ARGUMENT;
+}
+cuopt_int_t cuOptGetDualSolution(cuOptSolution solution, cuopt_float_t* v)
+{
+  CHECK2(solution, v);
+  copy_out(v, R(solution)->r.y);
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetDualObjectiveValue(cuOptSolution solution, cuopt_float_t* v)
+{
+  CHECK2(solution, v);
+  *v = R(solution)->r.dual_obj;
+  return CUOPT_SUCCESS;
+}
+cuopt_int_t cuOptGetReducedCosts(cuOptSolution solution, cuopt_float_t* v)
+{
+  CHECK2(solution, v);
+  copy_out(v, R(solution)->r.rc);
+  return CUOPT_SUCCESS;
+}
+
+cuopt_int_t cuOptGetPDLPStatistics(cuOptSolution solution, cuOptPDLPStatistics* st)
+{
+  CHECK2(solution, st);
+  const auto& r                       = R(solution)->r;
+  st->number_of_steps_taken           = (cuopt_int_t)r.iterations;
+  st->total_number_of_attempted_steps = (cuopt_int_t)r.iterations;
+  st->l2_primal_residual              = r.l2_primal;
+  st->l2_relative_primal_residual     = r.rel_primal;
+  st->l2_dual_residual                = r.l2_dual;
+  st->l2_relative_dual_residual       = r.rel_dual;
+  st->primal_objective                = r.primal_obj;
+  st->dual_objective                  = r.dual_obj;
+  st->gap                             = r.gap;
+  st->relative_gap                    = r.rel_gap;
+  st->solve_time                      = r.solve_time;
+  st->solved_by_pdlp                  = R(solution)->solved_by_pdlp ? 1 : 0;
+  st->restarts                        = r.restarts;
+  st->power_iterations                = r.power_iterations;
+  st->refinement_passes               = r.refinement_passes;
+  st->step_size                       = r.step_size;
+  st->primal_weight                   = r.primal_weight;
+  st->setup_time                      = r.setup_time;
+  st->loop_time                       = r.loop_time;
+  return CUOPT_SUCCESS;
+}
+
+cuopt_int_t cuOptBatchSolve(const cuOptOptimizationProblem* problems, cuopt_int_t count,
+                            cuOptSolverSettings settings, cuOptSolution* solutions)
+{
+  if (!problems || !settings || !solutions || count < 0) return CUOPT_INVALID_ARGUMENT;
+  cuopt_int_t first_error = CUOPT_SUCCESS;
+  for (cuopt_int_t i = 0; i < count; ++i) {
+    solutions[i] = nullptr;
+    if (!problems[i]) return CUOPT_INVALID_ARGUMENT;
+  }
+  for (cuopt_int_t i = 0; i < count; ++i) {
+    cuopt_int_t rc = cuOptSolve(problems[i], settings, &solutions[i]);
+    if (rc != CUOPT_SUCCESS && first_error == CUOPT_SUCCESS) first_error = rc;
+  }
+  return first_error;
+}
+
+cuopt_int_t cuOptSolutionAdjoint(cuOptOptimizationProblem problem, cuOptSolution solution,
+                                 const cuopt_float_t* dl_dx, const cuopt_float_t*,
+                                 cuopt_float_t*, cuopt_float_t*, cuopt_float_t*, cuopt_float_t*)
+{
+  if (!problem || !solution || !dl_dx) return CUOPT_INVALID_ARGUMENT;
+  return CUOPT_INVALID_ARGUMENT;
+}
+
+}  // extern "C"

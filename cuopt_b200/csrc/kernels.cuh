@@ -1,0 +1,599 @@
+// sm_100a kernels of the PDLP path.
+//
+// Every matrix sweep is one launch of `sell_map_kernel`: warps either walk one long row (CSR,
+// lanes stride along the row) or one 32-row slice of the sliced-ELL part (lane t owns row t and
+// reads element k at base + 32k + t, so each warp load is one contiguous segment).  The row's dot
+// product is handed to an epilogue functor that performs the PDHG projection / reflection /
+// Halpern step (or a termination / fixed-point-error term) for that row, so x, y and the reflected
+// iterate cross HBM once per sweep.  Epilogues may also contribute to up to four block-level sums
+// that are reduced deterministically (fixed tree, then one ordered pass over blocks).
+#pragma once
+
+#include "common.cuh"
+
+namespace cuopt_b200 {
+
+constexpr int kBlock         = 256;
+constexpr int kWarpsPerBlock = kBlock / kWarp;
+
+template <typename T>
+struct dev_sell {
+  int rows;
+  int n_long;
+  int n_slices;
+  const int64_t* long_off;
+  const int64_t* slice_off;
+  const int* idx;
+  const T* val;
+};
+
+B200_HD inline int long_blocks(int n_long) { return ceil_div(n_long, kWarpsPerBlock); }
+template <typename T>
+inline int sell_grid(const dev_sell<T>& a)
+{
+  return long_blocks(a.n_long) + ceil_div(a.n_slices, kWarpsPerBlock);
+}
+
+// Scalars that change between iterations live on the device so captured graphs stay valid.
+struct pdlp_scalars {
+  double tau;      // primal step  = eta / omega
+  double sigma;    // dual step    = eta * omega
+  double eta;      // step size
+  double omega;    // primal weight
+  long long t0;    // iterations since the last restart, at the start of the next step
+};
+
+__device__ __forceinline__ double halpern_weight(const pdlp_scalars* st, int it_off)
+{
+  const double t = (double)(st->t0 + it_off);
+  return (t + 1.0) / (t + 2.0);
+}
+
+template <int K>
+struct red_t {
+  double v[K > 0 ? K : 1];
+};
+
+// Block reduction of K doubles; thread 0 writes partials[blockIdx.x * K + r].
+template <int K>
+__device__ __forceinline__ void block_reduce_store(red_t<K>& r, double* partials)
+{
+  if constexpr (K > 0) {
+    __shared__ double sm[kWarpsPerBlock][K];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+      double v = warp_sum(r.v[q]);
+      if (lane == 0) sm[warp][q] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+      double s = 0.0;
+#pragma unroll
+      for (int w = 0; w < kWarpsPerBlock; ++w) s += sm[w][threadIdx.x];
+      partials[(size_t)blockIdx.x * K + threadIdx.x] = s;
+    }
+  }
+}
+
+// out[q] = sum over blocks of partials[b*K+q] (single block, ordered, compensated).
+template <int K>
+__global__ void __launch_bounds__(kBlock) finalize_sum_kernel(const double* partials, int nblocks,
+                                                              double* out)
+{
+  __shared__ double sm[kBlock];
+  for (int q = 0; q < K; ++q) {
+    ksum acc;
+    for (int b = threadIdx.x; b < nblocks; b += kBlock) acc.add(partials[(size_t)b * K + q]);
+    sm[threadIdx.x] = acc.value();
+    __syncthreads();
+    for (int s = kBlock / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) sm[threadIdx.x] += sm[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[q] = sm[0];
+    __syncthreads();
+  }
+}
+
+// Generic fused sweep: acc_r = sum_k A[r,k] * g[idx[r,k]], then epi(r, acc_r, red).
+template <typename TM, typename TG, class Epi>
+__global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
+                                                          const TG* __restrict__ g, Epi epi,
+                                                          double* partials)
+{
+  constexpr int K = Epi::kRed;
+  red_t<K> red;
+#pragma unroll
+  for (int q = 0; q < (K > 0 ? K : 1); ++q) red.v[q] = 0.0;
+  if (epi.skip()) {
+    // Uniform early exit (e.g. converged power iteration): every block still stores zeros.
+    block_reduce_store<K>(red, partials);
+    return;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lb   = long_blocks(A.n_long);
+  if ((int)blockIdx.x < lb) {
+    const int row = blockIdx.x * kWarpsPerBlock + warp;
+    if (row < A.n_long) {
+      const int64_t b = A.long_off[row], e = A.long_off[row + 1];
+      double acc      = 0.0;
+      for (int64_t k = b + lane; k < e; k += kWarp)
+        acc += (double)ld_stream(A.val + k) * (double)g[ld_stream(A.idx + k)];
+      acc = warp_sum(acc);
+      if (lane == 0) epi(row, acc, red);
+    }
+  } else {
+    const int s = (blockIdx.x - lb) * kWarpsPerBlock + warp;
+    if (s < A.n_slices) {
+      const int64_t base = A.slice_off[s];
+      const int len      = (int)((A.slice_off[s + 1] - base) >> 5);
+      const TM* v        = A.val + base + lane;
+      const int* ix      = A.idx + base + lane;
+      double acc         = 0.0;
+      int k              = 0;
+      for (; k + 4 <= len; k += 4) {
+        const int i0 = ld_stream(ix), i1 = ld_stream(ix + 32), i2 = ld_stream(ix + 64),
+                  i3 = ld_stream(ix + 96);
+        const TM v0 = ld_stream(v), v1 = ld_stream(v + 32), v2 = ld_stream(v + 64),
+                 v3 = ld_stream(v + 96);
+        const TG g0 = g[i0], g1 = g[i1], g2 = g[i2], g3 = g[i3];
+        acc += (double)v0 * (double)g0;
+        acc += (double)v1 * (double)g1;
+        acc += (double)v2 * (double)g2;
+        acc += (double)v3 * (double)g3;
+        v += 128;
+        ix += 128;
+      }
+      for (; k < len; ++k) {
+        acc += (double)ld_stream(v) * (double)g[ld_stream(ix)];
+        v += 32;
+        ix += 32;
+      }
+      const int row = A.n_long + s * kWarp + lane;
+      if (row < A.rows) epi(row, acc, red);
+    }
+  }
+  block_reduce_store<K>(red, partials);
+}
+
+// ---------------------------------------------------------------------------------------------
+// PDHG epilogues (reflected variant, reference pdhg.cu:431-530 and pdlp.cu:2506-2563).
+
+// Row j of A^T:  x_next = x - tau (c - A^T y);  x_hat = clamp(x_next, l, u);
+//                slack = (x_hat - x_next) / tau;  x_bar = 2 x_hat - x;
+//                (fused Halpern)  x <- w x_bar + (1 - w) x_anchor.
+template <typename TX, bool MAJOR, bool HALPERN, bool SAVE_ATY>
+struct primal_epi {
+  static constexpr int kRed = 0;
+  const TX* x;
+  const TX* c;
+  const TX* lo;
+  const TX* up;
+  const TX* xa;
+  TX* xbar;
+  TX* xout;
+  TX* xhat;
+  TX* slack;
+  TX* aty;
+  const pdlp_scalars* st;
+  int it_off;
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ void operator()(int j, double acc, red_t<0>&) const
+  {
+    const double tau  = st->tau;
+    const double xj   = (double)x[j];
+    const double next = xj - tau * ((double)c[j] - acc);
+    const double cl   = fmax(fmin(next, (double)up[j]), (double)lo[j]);
+    if constexpr (MAJOR) {
+      xhat[j]  = (TX)cl;
+      slack[j] = (TX)((cl - next) / tau);
+    }
+    const double xb = 2.0 * cl - xj;
+    if constexpr (SAVE_ATY) aty[j] = (TX)acc;
+    if constexpr (HALPERN) {
+      const double w = halpern_weight(st, it_off);
+      xbar[j]        = (TX)xb;
+      xout[j]        = (TX)(w * xb + (1.0 - w) * (double)xa[j]);
+    } else {
+      xbar[j] = (TX)xb;
+    }
+  }
+};
+
+// Row i of A:  t = y / sigma - A x_bar;  y_hat = (t - clamp(t, -u, -l)) sigma;  y_bar = 2 y_hat - y;
+//              (fused Halpern) y <- w y_bar + (1 - w) y_anchor;  (FPE) red += (y_bar - y)^2.
+template <typename TX, bool MAJOR, bool HALPERN, bool FPE>
+struct dual_epi {
+  static constexpr int kRed = FPE ? 1 : 0;
+  const TX* y;
+  const TX* lo;
+  const TX* up;
+  const TX* ya;
+  TX* ybar;
+  TX* yout;
+  TX* yhat;
+  const pdlp_scalars* st;
+  int it_off;
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ void operator()(int i, double acc, red_t<kRed>& r) const
+  {
+    const double sigma = st->sigma;
+    const double yi    = (double)y[i];
+    const double t     = yi / sigma - acc;
+    const double tp    = fmax(-(double)up[i], fmin(t, -(double)lo[i]));
+    const double ny    = (t - tp) * sigma;
+    if constexpr (MAJOR) yhat[i] = (TX)ny;
+    const double yb = 2.0 * ny - yi;
+    if constexpr (FPE) {
+      const double d = yb - yi;
+      r.v[0] += d * d;
+    }
+    if constexpr (HALPERN) {
+      const double w = halpern_weight(st, it_off);
+      yout[i]        = (TX)(w * yb + (1.0 - w) * (double)ya[i]);
+    } else {
+      ybar[i] = (TX)yb;
+    }
+  }
+};
+
+// Row j of A^T applied to y_bar: interaction (A^T y_bar - A^T y) . (x_bar - x) and |x_bar - x|^2
+// (reference adaptive_step_size_strategy.cu:352-518).
+template <typename TX>
+struct fpe_epi {
+  static constexpr int kRed = 2;
+  const TX* aty;
+  const TX* xbar;
+  const TX* x;
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ void operator()(int j, double acc, red_t<2>& r) const
+  {
+    const double d  = acc - (double)aty[j];
+    const double dx = (double)xbar[j] - (double)x[j];
+    r.v[0] += d * dx;
+    r.v[1] += dx * dx;
+  }
+};
+
+// Halpern update for iterations whose step kept x / y (fixed-point-error iterations).
+template <typename TX>
+__global__ void halpern_kernel(TX* x, const TX* xbar, const TX* xa, int n, TX* y, const TX* ybar,
+                               const TX* ya, int m, const pdlp_scalars* st)
+{
+  const double w = halpern_weight(st, 0);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x) {
+    if (i < n)
+      x[i] = (TX)(w * (double)xbar[i] + (1.0 - w) * (double)xa[i]);
+    else {
+      const int r = i - n;
+      y[r]        = (TX)(w * (double)ybar[r] + (1.0 - w) * (double)ya[r]);
+    }
+  }
+}
+
+__global__ void advance_kernel(pdlp_scalars* st, int steps) { st->t0 += steps; }
+__global__ void set_scalars_kernel(pdlp_scalars* st, double tau, double sigma, double eta,
+                                   double omega, long long t0)
+{
+  st->tau   = tau;
+  st->sigma = sigma;
+  st->eta   = eta;
+  st->omega = omega;
+  st->t0    = t0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Termination (reference convergence_information.cu:492-811) on the unscaled FP64 problem.
+
+// x_u = (x_hat dc) / beta ; y_u = (y_hat dr) / gamma ; s_u = (slack / dc) / gamma
+// (unscale_solutions, initial_scaling.cu:684-790).
+template <typename TX>
+__global__ void unscale_kernel(const TX* xhat, const TX* yhat, const TX* slack, const double* dc,
+                               const double* dr, double inv_beta, double inv_gamma, int n, int m,
+                               double* xu, double* yu, double* su)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x) {
+    if (i < n) {
+      const double d = dc[i];
+      xu[i]          = ((double)xhat[i] * d) * inv_beta;
+      const double s = (double)slack[i];
+      su[i]          = (d != 0.0 ? s / d : s) * inv_gamma;
+    } else {
+      const int r = i - n;
+      yu[r]       = ((double)yhat[r] * dr[r]) * inv_gamma;
+    }
+  }
+}
+
+__device__ __forceinline__ double finite_or_zero(double v) { return isfinite(v) ? v : 0.0; }
+
+// Row i of A (unscaled): r_p = Ax - clamp(Ax, lc, uc); primal slack for the dual objective.
+struct term_primal_epi {
+  static constexpr int kRed = 2;
+  const double* lc;
+  const double* uc;
+  const double* y;
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ void operator()(int i, double ax, red_t<2>& r) const
+  {
+    const double l = lc[i], u = uc[i];
+    const double cl = fmax(l, fmin(ax, u));
+    const double rp = ax - cl;
+    const double yi = y[i];
+    r.v[0] += rp * rp;
+    r.v[1] += fmax(yi, 0.0) * finite_or_zero(l) + fmin(yi, 0.0) * finite_or_zero(u);
+  }
+};
+
+// Row j of A^T (unscaled): r_d = (c - A^T y) - slack; c.x; slack.x.
+struct term_dual_epi {
+  static constexpr int kRed = 3;
+  const double* c;
+  const double* x;
+  const double* s;
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ void operator()(int j, double aty, red_t<3>& r) const
+  {
+    const double cj = c[j], xj = x[j], sj = s[j];
+    const double rd = (cj - aty) - sj;
+    r.v[0] += rd * rd;
+    r.v[1] += cj * xj;
+    r.v[2] += sj * xj;
+  }
+};
+
+// Plain sweep epilogues.
+template <typename TX>
+struct store_epi {  // out[r] = acc
+  static constexpr int kRed = 0;
+  TX* out;
+  const int* done;  // optional early-exit flag
+  __device__ bool skip() const { return done && *done; }
+  __device__ __forceinline__ void operator()(int r, double acc, red_t<0>&) const { out[r] = (TX)acc; }
+};
+
+// Power iteration z = A (A^T q) with q . z accumulated (reference pdlp.cu:2664-2711).
+struct power_z_epi {
+  static constexpr int kRed = 1;
+  double* z;
+  const double* q;
+  const int* done;
+  __device__ bool skip() const { return *done != 0; }
+  __device__ __forceinline__ void operator()(int i, double acc, red_t<1>& r) const
+  {
+    z[i] = acc;
+    r.v[0] += q[i] * acc;
+  }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Reductions over plain vectors (block partials; finalize with finalize_sum_kernel).
+
+// mode 0: sum x^2 ; mode 1: sum (a-b)^2 ; mode 2: bound norm terms of (lo, up)
+template <int MODE, typename TA>
+__global__ void __launch_bounds__(kBlock) vec_reduce_kernel(const TA* a, const TA* b, int n,
+                                                            double* partials, const int* done)
+{
+  red_t<1> r;
+  r.v[0] = 0.0;
+  if (!(done && *done)) {
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+      if constexpr (MODE == 0) {
+        const double v = (double)a[i];
+        r.v[0] += v * v;
+      } else if constexpr (MODE == 1) {
+        const double d = (double)a[i] - (double)b[i];
+        r.v[0] += d * d;
+      } else {
+        const double l = (double)a[i], u = (double)b[i];
+        double s       = 0.0;
+        if (isfinite(l) && l != u) s += l * l;
+        if (isfinite(u)) s += u * u;
+        r.v[0] += s;
+      }
+    }
+  }
+  block_reduce_store<1>(r, partials);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Power iteration helpers (reference pdlp.cu:2620-2731).  State on device:
+//   pi[0] = |z|, pi[1] = sigma_max^2, pi[2] = |residual|, done flag, iteration counter.
+struct power_state {
+  double norm_z;
+  double s2;
+  double resid;
+  int done;
+  int iters;
+};
+
+__global__ void power_normalize_kernel(const double* z, double* q, int m, const double* sumsq,
+                                       power_state* ps)
+{
+  if (ps->done) return;
+  const double nq = sqrt(*sumsq);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    q[i] = z[i] / nq;
+  if (blockIdx.x == 0 && threadIdx.x == 0) ps->norm_z = nq;
+}
+
+// q <- q * (-s2) + z ; partial sum of squares of the result.
+__global__ void __launch_bounds__(kBlock) power_residual_kernel(double* q, const double* z, int m,
+                                                                const double* s2,
+                                                                const power_state* ps,
+                                                                double* partials)
+{
+  red_t<1> r;
+  r.v[0] = 0.0;
+  if (!ps->done) {
+    const double s = *s2;
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < m; i += gridDim.x * kBlock) {
+      const double v = q[i] * -s + z[i];
+      q[i]           = v;
+      r.v[0] += v * v;
+    }
+  }
+  block_reduce_store<1>(r, partials);
+}
+
+__global__ void power_check_kernel(power_state* ps, const double* s2, const double* rsq, double tol)
+{
+  if (ps->done) return;
+  ps->s2    = *s2;
+  ps->resid = sqrt(*rsq);
+  ps->iters += 1;
+  if (ps->resid < tol) ps->done = 1;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Scaling (reference initial_scaling.cu:152-569).
+
+// For every row r of layout A: out[r] = max_k |v (s_first) (s_second)| (MODE 0) or
+// sum_k |v s_first s_second|^alpha (MODE 1), where for A (TRANSPOSED=false) the product is
+// (a_ij dr_i) dc_j and for A^T (TRANSPOSED=true) it is (a_ij dr_i) dc_j with i = idx, j = row.
+template <int MODE, bool TRANSPOSED>
+__global__ void __launch_bounds__(kBlock) row_scaled_abs_kernel(const dev_sell<double> A,
+                                                                const double* dr,
+                                                                const double* dc, double alpha,
+                                                                double* out)
+{
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lb   = long_blocks(A.n_long);
+  auto term      = [&](double v, int row, int col) {
+    const double p = TRANSPOSED ? (v * dr[col]) * dc[row] : (v * dr[row]) * dc[col];
+    const double a = fabs(p);
+    return MODE == 0 ? a : pow(a, alpha);
+  };
+  if ((int)blockIdx.x < lb) {
+    const int row = blockIdx.x * kWarpsPerBlock + warp;
+    if (row < A.n_long) {
+      double acc = 0.0;
+      for (int64_t k = A.long_off[row] + lane; k < A.long_off[row + 1]; k += kWarp) {
+        const double t = term(A.val[k], row, A.idx[k]);
+        acc            = MODE == 0 ? fmax(acc, t) : acc + t;
+      }
+      acc = MODE == 0 ? warp_max(acc) : warp_sum(acc);
+      if (lane == 0) out[row] = acc;
+    }
+  } else {
+    const int s = (blockIdx.x - lb) * kWarpsPerBlock + warp;
+    if (s < A.n_slices) {
+      const int64_t base = A.slice_off[s];
+      const int len      = (int)((A.slice_off[s + 1] - base) >> 5);
+      const int row      = A.n_long + s * kWarp + lane;
+      if (row < A.rows) {
+        double acc = 0.0;
+        for (int k = 0; k < len; ++k) {
+          const int64_t p = base + (int64_t)k * 32 + lane;
+          const double v  = A.val[p];
+          if (v == 0.0) continue;  // padding (and explicit zeros, which contribute nothing)
+          const double t = term(v, row, A.idx[p]);
+          acc            = MODE == 0 ? fmax(acc, t) : acc + t;
+        }
+        out[row] = acc;
+      }
+    }
+  }
+}
+
+// d[i] <- d[i] / sqrt(v[i]) where v[i] > 0 (a_divides_sqrt_b_bounded, utils.cuh:156-163)
+__global__ void apply_root_scaling_kernel(double* d, const double* v, int n)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double b = v[i];
+    if (b > 0.0) d[i] = d[i] / sqrt(b);
+  }
+}
+
+// Scaled copy of the matrix values: A_s = (a dr_i) dc_j, A^T_s = (a dc_j) dr_i.
+template <typename TM, bool TRANSPOSED>
+__global__ void __launch_bounds__(kBlock) scale_values_kernel(const dev_sell<double> A,
+                                                              const double* dr, const double* dc,
+                                                              TM* out)
+{
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lb   = long_blocks(A.n_long);
+  auto scaled    = [&](double v, int row, int col) {
+    return TRANSPOSED ? (v * dc[row]) * dr[col] : (v * dr[row]) * dc[col];
+  };
+  if ((int)blockIdx.x < lb) {
+    const int row = blockIdx.x * kWarpsPerBlock + warp;
+    if (row < A.n_long)
+      for (int64_t k = A.long_off[row] + lane; k < A.long_off[row + 1]; k += kWarp)
+        out[k] = (TM)scaled(A.val[k], row, A.idx[k]);
+  } else {
+    const int s = (blockIdx.x - lb) * kWarpsPerBlock + warp;
+    if (s < A.n_slices) {
+      const int64_t base = A.slice_off[s];
+      const int len      = (int)((A.slice_off[s + 1] - base) >> 5);
+      const int row      = A.n_long + s * kWarp + lane;
+      for (int k = 0; k < len; ++k) {
+        const int64_t p = base + (int64_t)k * 32 + lane;
+        out[p]          = row < A.rows ? (TM)scaled(A.val[p], row, A.idx[p]) : (TM)0;
+      }
+    }
+  }
+}
+
+// First pass of the vector scaling: c*dc, bounds/dc (divide_check_zero), constraint bounds*dr.
+__global__ void scale_vectors_kernel(const double* c, const double* l, const double* u,
+                                     const double* lc, const double* uc, const double* dc,
+                                     const double* dr, int n, int m, double* cs, double* ls,
+                                     double* us, double* lcs, double* ucs)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x) {
+    if (i < n) {
+      const double d = dc[i];
+      cs[i]          = c[i] * d;
+      if (d == 0.0) {
+        ls[i] = 0.0;
+        us[i] = 0.0;
+      } else {
+        ls[i] = l[i] / d;
+        us[i] = u[i] / d;
+      }
+    } else {
+      const int r = i - n;
+      lcs[r]      = lc[r] * dr[r];
+      ucs[r]      = uc[r] * dr[r];
+    }
+  }
+}
+
+// Second pass: bound rescaling beta and objective rescaling gamma; converts to the iterate type.
+template <typename TX>
+__global__ void rescale_vectors_kernel(const double* cs, const double* ls, const double* us,
+                                       const double* lcs, const double* ucs, double beta,
+                                       double gamma, int n, int m, TX* c_out, TX* l_out, TX* u_out,
+                                       TX* lc_out, TX* uc_out)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x) {
+    if (i < n) {
+      c_out[i] = (TX)(cs[i] * gamma);
+      l_out[i] = (TX)(ls[i] * beta);
+      u_out[i] = (TX)(us[i] * beta);
+    } else {
+      const int r = i - n;
+      lc_out[r]   = (TX)(lcs[r] * beta);
+      uc_out[r]   = (TX)(ucs[r] * beta);
+    }
+  }
+}
+
+// Elementwise helpers
+template <typename TX>
+__global__ void clamp_kernel(TX* x, const TX* l, const TX* u, int n)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = (TX)fmin(fmax((double)x[i], (double)l[i]), (double)u[i]);
+}
+
+template <typename TA, typename TB>
+__global__ void copy_convert_kernel(TB* dst, const TA* src, int n)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    dst[i] = (TB)src[i];
+}
+
+}  // namespace cuopt_b200

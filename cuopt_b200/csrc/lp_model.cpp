@@ -1,0 +1,450 @@
+// Problem / settings / solution objects behind the C interface, validation and solve dispatch.
+#include "lp_model.hpp"
+
+#include <cuopt/linear_programming/constants.h>
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <limits>
+#include <new>
+#include <stdexcept>
+
+#include "common.cuh"
+
+namespace cuopt_b200 {
+
+namespace {
+constexpr double kInf = std::numeric_limits<double>::infinity();
+}
+
+void lp_problem::constraint_bounds(std::vector<double>& lo, std::vector<double>& up) const
+{
+  if (ranged) {
+    lo = con_lo;
+    up = con_up;
+    return;
+  }
+  lo.resize(m);
+  up.resize(m);
+  for (int i = 0; i < m; ++i) {  // transform_bounds_functor (problem_helpers.cuh:26-51)
+    const char t = row_types[i];
+    if (t == 'E') {
+      lo[i] = rhs[i];
+      up[i] = rhs[i];
+    } else if (t == 'G') {
+      lo[i] = rhs[i];
+      up[i] = kInf;
+    } else if (t == 'L') {
+      lo[i] = -kInf;
+      up[i] = rhs[i];
+    } else {
+      lo[i] = -kInf;
+      up[i] = -kInf;
+    }
+  }
+}
+
+bool lp_problem::is_mip() const
+{
+  return std::any_of(var_types.begin(), var_types.end(), [](char t) { return t == 'I'; });
+}
+
+// ------------------------------------------------------------------------------------------
+// Settings registry: same names, ranges and defaults as the reference
+// (cpp/src/math_optimization/solver_settings.cu:55-135), plus this library's pdlp_* additions.
+
+lp_settings::lp_settings()
+{
+  const double inf = kInf;
+  fparams          = {
+    {CUOPT_TIME_LIMIT, 0.0, inf, inf},
+    {CUOPT_WORK_LIMIT, 0.0, inf, inf},
+    {CUOPT_ABSOLUTE_DUAL_TOLERANCE, 0.0, 1e-1, 1e-4},
+    {CUOPT_RELATIVE_DUAL_TOLERANCE, 0.0, 1e-1, 1e-4},
+    {CUOPT_ABSOLUTE_PRIMAL_TOLERANCE, 0.0, 1e-1, 1e-4},
+    {CUOPT_RELATIVE_PRIMAL_TOLERANCE, 0.0, 1e-1, 1e-4},
+    {CUOPT_ABSOLUTE_GAP_TOLERANCE, 0.0, 1e-1, 1e-4},
+    {CUOPT_RELATIVE_GAP_TOLERANCE, 0.0, 1e-1, 1e-4},
+    {CUOPT_MIP_ABSOLUTE_TOLERANCE, 0.0, 1e-1, 1e-4},
+    {CUOPT_MIP_RELATIVE_TOLERANCE, 0.0, 1e-1, 1e-4},
+    {CUOPT_MIP_INTEGRALITY_TOLERANCE, 0.0, 1e-1, 1e-5},
+    {CUOPT_MIP_ABSOLUTE_GAP, 0.0, inf, 1e-10},
+    {CUOPT_MIP_RELATIVE_GAP, 0.0, 1e-1, 1e-4},
+    {CUOPT_PRIMAL_INFEASIBLE_TOLERANCE, 0.0, 1e-1, 1e-10},
+    {CUOPT_DUAL_INFEASIBLE_TOLERANCE, 0.0, 1e-1, 1e-10},
+    {CUOPT_MIP_CUT_CHANGE_THRESHOLD, 0.0, inf, 1e-3},
+    {CUOPT_MIP_CUT_MIN_ORTHOGONALITY, 0.0, 1.0, 0.5},
+    {CUOPT_PDLP_REFINEMENT_TOLERANCE, 0.0, 1e-1, 1e-8},
+  };
+  iparams = {
+    {CUOPT_ITERATION_LIMIT, 0, INT_MAX, INT_MAX},
+    {CUOPT_PDLP_SOLVER_MODE, CUOPT_PDLP_SOLVER_MODE_STABLE1, CUOPT_PDLP_SOLVER_MODE_STABLE3,
+     CUOPT_PDLP_SOLVER_MODE_STABLE3},
+    {CUOPT_METHOD, CUOPT_METHOD_CONCURRENT, CUOPT_METHOD_BARRIER, CUOPT_METHOD_CONCURRENT},
+    {CUOPT_NUM_CPU_THREADS, -1, INT_MAX, -1},
+    {CUOPT_AUGMENTED, -1, 1, -1},
+    {CUOPT_FOLDING, -1, 1, -1},
+    {CUOPT_DUALIZE, -1, 1, -1},
+    {CUOPT_ORDERING, -1, 1, -1},
+    {CUOPT_BARRIER_DUAL_INITIAL_POINT, -1, 1, -1},
+    {CUOPT_MIP_CUT_PASSES, -1, INT_MAX, 10},
+    {CUOPT_MIP_MIXED_INTEGER_ROUNDING_CUTS, -1, 1, -1},
+    {CUOPT_MIP_MIXED_INTEGER_GOMORY_CUTS, -1, 1, -1},
+    {CUOPT_MIP_KNAPSACK_CUTS, -1, 1, -1},
+    {CUOPT_MIP_STRONG_CHVATAL_GOMORY_CUTS, -1, 1, -1},
+    {CUOPT_MIP_REDUCED_COST_STRENGTHENING, -1, INT_MAX, -1},
+    {CUOPT_NUM_GPUS, 1, 2, 1},
+    {CUOPT_MIP_BATCH_PDLP_STRONG_BRANCHING, 0, 1, 0},
+    {CUOPT_PRESOLVE, CUOPT_PRESOLVE_DEFAULT, CUOPT_PRESOLVE_PSLP, CUOPT_PRESOLVE_DEFAULT},
+    {CUOPT_MIP_DETERMINISM_MODE, CUOPT_MODE_OPPORTUNISTIC, CUOPT_MODE_DETERMINISTIC,
+     CUOPT_MODE_OPPORTUNISTIC},
+    {CUOPT_RANDOM_SEED, -1, INT_MAX, -1},
+    {CUOPT_MIP_RELIABILITY_BRANCHING, -1, INT_MAX, -1},
+    {CUOPT_PDLP_PRECISION, CUOPT_PDLP_PRECISION_FP64, CUOPT_PDLP_PRECISION_MIXED,
+     CUOPT_PDLP_PRECISION_FP64},
+    {CUOPT_PDLP_REFINEMENT_PASSES, 0, 64, 4},
+  };
+  bparams = {
+    {CUOPT_INFEASIBILITY_DETECTION, false}, {CUOPT_STRICT_INFEASIBILITY, false},
+    {CUOPT_PER_CONSTRAINT_RESIDUAL, false}, {CUOPT_SAVE_BEST_PRIMAL_SO_FAR, false},
+    {CUOPT_FIRST_PRIMAL_FEASIBLE, false},   {CUOPT_MIP_SCALING, true},
+    {CUOPT_MIP_HEURISTICS_ONLY, false},     {CUOPT_LOG_TO_CONSOLE, true},
+    {CUOPT_CROSSOVER, false},               {CUOPT_ELIMINATE_DENSE_COLUMNS, true},
+    {CUOPT_CUDSS_DETERMINISTIC, false},     {CUOPT_DUAL_POSTSOLVE, true},
+  };
+  sparams = {{CUOPT_LOG_FILE, ""}, {CUOPT_SOLUTION_FILE, ""}, {CUOPT_USER_PROBLEM_FILE, ""}};
+}
+
+namespace {
+bool parse_int(const std::string& v, int32_t& out)
+{
+  try {
+    out = std::stoi(v);
+    return true;
+  } catch (const std::exception&) {
+    return false;
+  }
+}
+bool parse_float(const std::string& v, double& out)
+{
+  try {
+    out = std::stod(v);
+    return true;
+  } catch (const std::exception&) {
+    return false;
+  }
+}
+bool parse_bool(const std::string& v, bool& out)
+{
+  if (v == "true" || v == "True" || v == "TRUE" || v == "1" || v == "t" || v == "T") {
+    out = true;
+    return true;
+  }
+  if (v == "false" || v == "False" || v == "FALSE" || v == "0" || v == "f" || v == "F") {
+    out = false;
+    return true;
+  }
+  return false;
+}
+}  // namespace
+
+// set_parameter_from_string (reference solver_settings.cu:137-204)
+int lp_settings::set_from_string(const std::string& name, const std::string& value)
+{
+  for (auto& p : iparams)
+    if (name == p.name) {
+      int32_t v;
+      if (!parse_int(value, v) || v < p.min || v > p.max) return CUOPT_INVALID_ARGUMENT;
+      p.value = v;
+      return CUOPT_SUCCESS;
+    }
+  for (auto& p : fparams)
+    if (name == p.name) {
+      double v;
+      if (!parse_float(value, v) || v < p.min || v > p.max) return CUOPT_INVALID_ARGUMENT;
+      p.value = v;
+      return CUOPT_SUCCESS;
+    }
+  for (auto& p : bparams)
+    if (name == p.name) {
+      bool v;
+      if (!parse_bool(value, v)) return CUOPT_INVALID_ARGUMENT;
+      p.value = v;
+      return CUOPT_SUCCESS;
+    }
+  for (auto& p : sparams)
+    if (name == p.name) {
+      p.value = value;
+      return CUOPT_SUCCESS;
+    }
+  return CUOPT_INVALID_ARGUMENT;
+}
+
+int lp_settings::set_int(const std::string& name, int32_t v)
+{
+  for (auto& p : iparams)
+    if (name == p.name) {
+      if (v < p.min || v > p.max) return CUOPT_INVALID_ARGUMENT;
+      p.value = v;
+      return CUOPT_SUCCESS;
+    }
+  return CUOPT_INVALID_ARGUMENT;
+}
+int lp_settings::set_float(const std::string& name, double v)
+{
+  for (auto& p : fparams)
+    if (name == p.name) {
+      if (!(v >= p.min && v <= p.max)) return CUOPT_INVALID_ARGUMENT;
+      p.value = v;
+      return CUOPT_SUCCESS;
+    }
+  return CUOPT_INVALID_ARGUMENT;
+}
+int lp_settings::set_bool(const std::string& name, bool v)
+{
+  for (auto& p : bparams)
+    if (name == p.name) {
+      p.value = v;
+      return CUOPT_SUCCESS;
+    }
+  return CUOPT_INVALID_ARGUMENT;
+}
+int lp_settings::get_int(const std::string& name, int32_t& v) const
+{
+  for (auto& p : iparams)
+    if (name == p.name) {
+      v = p.value;
+      return CUOPT_SUCCESS;
+    }
+  return CUOPT_INVALID_ARGUMENT;
+}
+int lp_settings::get_float(const std::string& name, double& v) const
+{
+  for (auto& p : fparams)
+    if (name == p.name) {
+      v = p.value;
+      return CUOPT_SUCCESS;
+    }
+  return CUOPT_INVALID_ARGUMENT;
+}
+int lp_settings::get_bool(const std::string& name, bool& v) const
+{
+  for (auto& p : bparams)
+    if (name == p.name) {
+      v = p.value;
+      return CUOPT_SUCCESS;
+    }
+  return CUOPT_INVALID_ARGUMENT;
+}
+int lp_settings::get_as_string(const std::string& name, std::string& v) const
+{
+  for (auto& p : iparams)
+    if (name == p.name) {
+      v = std::to_string(p.value);
+      return CUOPT_SUCCESS;
+    }
+  for (auto& p : fparams)
+    if (name == p.name) {
+      v = std::to_string(p.value);
+      return CUOPT_SUCCESS;
+    }
+  for (auto& p : bparams)
+    if (name == p.name) {
+      v = p.value ? "true" : "false";
+      return CUOPT_SUCCESS;
+    }
+  for (auto& p : sparams)
+    if (name == p.name) {
+      v = p.value;
+      return CUOPT_SUCCESS;
+    }
+  return CUOPT_INVALID_ARGUMENT;
+}
+double lp_settings::f(const char* name) const
+{
+  double v = 0;
+  get_float(name, v);
+  return v;
+}
+int32_t lp_settings::i(const char* name) const
+{
+  int32_t v = 0;
+  get_int(name, v);
+  return v;
+}
+bool lp_settings::b(const char* name) const
+{
+  bool v = false;
+  get_bool(name, v);
+  return v;
+}
+
+// ------------------------------------------------------------------------------------------
+
+std::string validate_problem(const lp_problem& p)
+{
+  if (p.m < 0 || p.n < 0) return "Negative problem dimensions.";
+  if ((int)p.row_off.size() != p.m + 1) return "A_offsets must have num_constraints + 1 entries.";
+  if (p.row_off[0] != 0) return "A_offsets first value should be 0.";
+  for (int i = 0; i < p.m; ++i)
+    if (p.row_off[i + 1] < p.row_off[i]) return "A_offsets values must in an increasing order.";
+  const int64_t nnz = p.row_off[p.m];
+  if ((int64_t)p.col_idx.size() != nnz || (int64_t)p.val.size() != nnz)
+    return "A_index and A_values must have same sizes.";
+  for (int64_t k = 0; k < nnz; ++k)
+    if (p.col_idx[k] < 0 || p.col_idx[k] >= p.n)
+      return "A_indices values must positive lower than the number of variables (c size).";
+  if ((int)p.c.size() != p.n) return "c must be set before calling the solver.";
+  if ((int)p.var_lo.size() != p.n || (int)p.var_up.size() != p.n)
+    return "Sizes for vectors related to the variables are not the same.";
+  if (p.ranged) {
+    if ((int)p.con_lo.size() != p.m || (int)p.con_up.size() != p.m)
+      return "Sizes for vectors related to the constraints are not the same.";
+  } else {
+    if ((int)p.row_types.size() != p.m || (int)p.rhs.size() != p.m)
+      return "Sizes for vectors related to the constraints are not the same.";
+    for (char t : p.row_types)
+      if (t != 'E' && t != 'G' && t != 'L') return "row_types values must equal to 'E', 'G' or 'L'.";
+  }
+  return "";
+}
+
+namespace {
+
+// Variables with no constraints: each coordinate minimises c_j x_j over [l_j, u_j] on its own.
+// (The reference hands such problems to dual simplex under Concurrent, and returns
+// NumericalError from PDLP, solve.cu:562-567.)
+lp_solution solve_without_constraints(const lp_problem& p)
+{
+  lp_solution s;
+  auto& r      = s.r;
+  const double sg = p.maximize ? -1.0 : 1.0;
+  r.x.assign(p.n, 0.0);
+  r.rc.assign(p.n, 0.0);
+  double obj   = 0.0;
+  bool bounded = true;
+  for (int j = 0; j < p.n; ++j) {
+    const double cj = sg * p.c[j];
+    double v;
+    if (cj > 0)
+      v = p.var_lo[j];
+    else if (cj < 0)
+      v = p.var_up[j];
+    else
+      v = std::min(std::max(0.0, p.var_lo[j]), p.var_up[j]);
+    if (!std::isfinite(v)) bounded = false;
+    r.x[j]  = v;
+    r.rc[j] = p.c[j];
+    obj += p.c[j] * (std::isfinite(v) ? v : 0.0);
+  }
+  r.status     = bounded ? CUOPT_TERIMINATION_STATUS_OPTIMAL : CUOPT_TERIMINATION_STATUS_UNBOUNDED;
+  r.primal_obj = obj + p.obj_offset;
+  r.dual_obj   = r.primal_obj;
+  s.solved_by_pdlp = false;
+  return s;
+}
+
+}  // namespace
+
+lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
+{
+  lp_solution out;
+  const auto t0 = std::chrono::steady_clock::now();
+  try {
+    if (p.quadratic) {
+      out.error_code    = CUOPT_VALIDATION_ERROR;
+      out.error_message = "Quadratic objectives are not supported by this library.";
+      return out;
+    }
+    if (p.is_mip()) {
+      out.error_code    = CUOPT_VALIDATION_ERROR;
+      out.error_message = "Integer variables are not supported by this library (LP only).";
+      return out;
+    }
+    std::string err = validate_problem(p);
+    if (!err.empty()) {
+      out.error_code    = CUOPT_VALIDATION_ERROR;
+      out.error_message = err;
+      return out;
+    }
+    std::vector<double> lo, up;
+    p.constraint_bounds(lo, up);
+    // has_crossing_bounds (reference problem_checking.cu:316-339)
+    for (int j = 0; j < p.n; ++j)
+      if (!(p.var_up[j] >= p.var_lo[j])) {
+        out.r.status = CUOPT_TERIMINATION_STATUS_INFEASIBLE;
+        return out;
+      }
+    if (p.ranged)
+      for (int i = 0; i < p.m; ++i)
+        if (!(up[i] >= lo[i])) {
+          out.r.status = CUOPT_TERIMINATION_STATUS_INFEASIBLE;
+          return out;
+        }
+    const int method = st.i(CUOPT_METHOD);
+    if (p.m == 0) {
+      if (method == CUOPT_METHOD_PDLP) {
+        out.r.status = CUOPT_TERIMINATION_STATUS_NUMERICAL_ERROR;
+        return out;
+      }
+      out = solve_without_constraints(p);
+      out.r.solve_time =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      return out;
+    }
+    if (p.n == 0) {
+      out.r.status = CUOPT_TERIMINATION_STATUS_NUMERICAL_ERROR;
+      return out;
+    }
+    pdlp_params prm;
+    prm.abs_primal      = st.f(CUOPT_ABSOLUTE_PRIMAL_TOLERANCE);
+    prm.rel_primal      = st.f(CUOPT_RELATIVE_PRIMAL_TOLERANCE);
+    prm.abs_dual        = st.f(CUOPT_ABSOLUTE_DUAL_TOLERANCE);
+    prm.rel_dual        = st.f(CUOPT_RELATIVE_DUAL_TOLERANCE);
+    prm.abs_gap         = st.f(CUOPT_ABSOLUTE_GAP_TOLERANCE);
+    prm.rel_gap         = st.f(CUOPT_RELATIVE_GAP_TOLERANCE);
+    prm.iteration_limit = st.i(CUOPT_ITERATION_LIMIT);
+    prm.time_limit      = st.f(CUOPT_TIME_LIMIT);
+    prm.precision       = st.i(CUOPT_PDLP_PRECISION);
+    prm.refinement_passes = st.i(CUOPT_PDLP_REFINEMENT_PASSES);
+    prm.refinement_tol    = st.f(CUOPT_PDLP_REFINEMENT_TOLERANCE);
+    prm.log_to_console    = st.b(CUOPT_LOG_TO_CONSOLE);
+    if ((int)st.initial_primal.size() == p.n) prm.initial_primal = st.initial_primal;
+    if ((int)st.initial_dual.size() == p.m) prm.initial_dual = st.initial_dual;
+    lp_input in;
+    in.m          = p.m;
+    in.n          = p.n;
+    in.row_off    = p.row_off.data();
+    in.col_idx    = p.col_idx.data();
+    in.val        = p.val.data();
+    in.c          = p.c.data();
+    in.con_lo     = lo.data();
+    in.con_up     = up.data();
+    in.var_lo     = p.var_lo.data();
+    in.var_up     = p.var_up.data();
+    in.obj_offset = p.obj_offset;
+    in.maximize   = p.maximize;
+    out.r         = pdlp_solve(in, prm);
+    if (prm.log_to_console)
+      std::printf("PDLP status %d  objective %+.10e  iterations %lld  time %.3fs\n", out.r.status,
+                  out.r.primal_obj, (long long)out.r.iterations, out.r.solve_time);
+  } catch (const std::bad_alloc& e) {
+    out.error_code    = CUOPT_OUT_OF_MEMORY;
+    out.error_message = "Memory allocation failed";
+  } catch (const cuda_error& e) {
+    out.error_code    = CUOPT_RUNTIME_ERROR;
+    out.error_message = e.what();
+  } catch (const std::invalid_argument& e) {
+    out.error_code    = CUOPT_VALIDATION_ERROR;
+    out.error_message = e.what();
+  } catch (const std::exception& e) {
+    out.error_code    = CUOPT_RUNTIME_ERROR;
+    out.error_message = e.what();
+  }
+  return out;
+}
+
+}  // namespace cuopt_b200

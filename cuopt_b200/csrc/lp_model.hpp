@@ -1,0 +1,85 @@
+// Host-side objects behind the opaque C handles.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "pdlp_engine.hpp"
+
+namespace cuopt_b200 {
+
+// cuOptOptimizationProblem: the user's LP, copied at creation (reference optimization_problem_t,
+// cpp/include/cuopt/linear_programming/optimization_problem.hpp:160-319).
+struct lp_problem {
+  int m = 0, n = 0;
+  bool maximize     = false;
+  double obj_offset = 0.0;
+  std::vector<double> c;
+  std::vector<int> row_off, col_idx;
+  std::vector<double> val;
+  bool ranged = false;           // true: con_lo / con_up given; false: row_types + rhs
+  std::vector<char> row_types;   // 'E' 'L' 'G'
+  std::vector<double> rhs;
+  std::vector<double> con_lo, con_up;
+  std::vector<double> var_lo, var_up;
+  std::vector<char> var_types;   // 'C' 'I'
+  bool quadratic = false;
+  std::vector<std::string> row_names, col_names;
+  std::string name, objective_name;
+
+  // Constraint bounds as PDLP sees them (reference problem_helpers.cuh:26-51).
+  void constraint_bounds(std::vector<double>& lo, std::vector<double>& up) const;
+  bool is_mip() const;
+};
+
+// Parameter registry mirroring the reference's solver_settings_t
+// (cpp/src/math_optimization/solver_settings.cu:55-135): names, ranges and defaults.
+struct lp_settings {
+  lp_settings();
+  // Each returns 0 on success, CUOPT_INVALID_ARGUMENT otherwise.
+  int set_from_string(const std::string& name, const std::string& value);
+  int set_int(const std::string& name, int32_t v);
+  int set_float(const std::string& name, double v);
+  int set_bool(const std::string& name, bool v);
+  int get_int(const std::string& name, int32_t& v) const;
+  int get_float(const std::string& name, double& v) const;
+  int get_bool(const std::string& name, bool& v) const;
+  int get_as_string(const std::string& name, std::string& v) const;
+
+  struct fparam { const char* name; double min, max, value; };
+  struct iparam { const char* name; int32_t min, max, value; };
+  struct bparam { const char* name; bool value; };
+  struct sparam { const char* name; std::string value; };
+  std::vector<fparam> fparams;
+  std::vector<iparam> iparams;
+  std::vector<bparam> bparams;
+  std::vector<sparam> sparams;
+
+  double f(const char* name) const;
+  int32_t i(const char* name) const;
+  bool b(const char* name) const;
+
+  std::vector<double> initial_primal, initial_dual;
+};
+
+// cuOptSolution
+struct lp_solution {
+  int error_code = 0;  // CUOPT_SUCCESS / CUOPT_VALIDATION_ERROR / ...
+  std::string error_message;
+  pdlp_result r;
+  bool solved_by_pdlp = true;
+};
+
+// Validation of a problem before solving (reference pdlp/utilities/problem_checking.cu:20-300).
+// Returns an empty string when valid, otherwise the reason.
+std::string validate_problem(const lp_problem& p);
+
+// Full solve as done by cuOptSolve: validation, trivial cases, PDLP.
+lp_solution solve_problem(const lp_problem& p, const lp_settings& s);
+
+// MPS input / output (reference cpp/libmps_parser).  read_mps returns 0 or CUOPT_MPS_* codes.
+int read_mps(const std::string& path, lp_problem& out, std::string& err);
+int write_mps(const lp_problem& p, const std::string& path);
+
+}  // namespace cuopt_b200

@@ -1,0 +1,671 @@
+// PDLP (Stable3: restarted reflected Halpern PDHG with cuPDLPx restarts) on sm_100a.
+//
+// Host driver counterpart of the reference's pdlp_solver_t::run_solver
+// (cpp/src/pdlp/pdlp.cu:2013-2457).  The host keeps the scalar state that the reference keeps on
+// the host (restart decision, PID primal weight, fixed-point errors); all vector and matrix work
+// is in the kernels of kernels.cuh.  Iterations that need neither a termination test, a "major"
+// step nor a fixed-point error are replayed from cached CUDA graphs of 2^k iterations.
+#include "kernels.cuh"
+#include "layout.hpp"
+#include "pdlp_engine.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <limits>
+#include <map>
+#include <memory>
+#include <random>
+
+namespace cuopt_b200 {
+
+namespace {
+
+constexpr int kOptimal = 1, kIterationLimit = 4, kTimeLimit = 5, kNumericalError = 6,
+              kPrimalFeasible = 7, kNoTermination = 0;
+
+// Stable3 constants (reference solve.cu:167-209, pdlp_hyper_params.cuh:12-56,
+// pdlp_restart_strategy.cu:689-836, pdlp.cu:2620-2731).
+constexpr long kMajor                 = 200;
+constexpr double kArtificialRestart   = 0.36;
+constexpr double kSufficientReduction = 0.2;
+constexpr double kNecessaryReduction  = 0.8;
+constexpr double kKp = 0.99, kKi = 0.01, kKd = 0.0, kISmooth = 0.3;
+constexpr int kPowerMaxIters          = 5000;
+constexpr double kPowerTol            = 1e-4;
+constexpr double kStepScaling         = 0.998;
+constexpr int kRuizIterations         = 10;
+constexpr double kPcAlpha             = 1.0;
+
+long conditional_major(long k)  // reference utils.cuh:63-81
+{
+  long step = 10, threshold = 1000;
+  while (k >= threshold) {
+    step *= 10;
+    threshold *= 10;
+  }
+  return step;
+}
+
+bool is_check(long k) { return (k % kMajor == 0 && k > 0) || k <= 0 || k % conditional_major(k) == 0; }
+bool is_major_step(long k) { return ((k + 1) % kMajor == 0) || ((k + 2) % conditional_major(k + 2)) == 0; }
+
+double now_s()
+{
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct dev_matrix {
+  int rows = 0, cols = 0, n_long = 0, n_slices = 0;
+  dbuf<int64_t> long_off, slice_off;
+  dbuf<int> idx;
+  dbuf<double> val;  // unscaled FP64
+  void upload(const sell_host& h, cudaStream_t s)
+  {
+    rows     = h.rows;
+    cols     = h.cols;
+    n_long   = h.n_long;
+    n_slices = h.n_slices;
+    long_off.resize(h.long_off.size());
+    long_off.upload(h.long_off.data(), h.long_off.size(), s);
+    slice_off.resize(h.slice_off.size());
+    slice_off.upload(h.slice_off.data(), h.slice_off.size(), s);
+    idx.resize(h.idx.size());
+    idx.upload(h.idx.data(), h.idx.size(), s);
+    val.resize(h.val.size());
+    val.upload(h.val.data(), h.val.size(), s);
+  }
+  template <typename T>
+  dev_sell<T> view(const T* v) const
+  {
+    return dev_sell<T>{rows, n_long, n_slices, long_off.data(), slice_off.data(), idx.data(), v};
+  }
+  dev_sell<double> view64() const { return view<double>(val.data()); }
+  int64_t stored() const { return (int64_t)idx.size(); }
+};
+
+struct conv_info {
+  double l2_primal, l2_dual, primal_obj, dual_obj, gap, abs_obj;
+};
+
+template <typename TX>
+class engine {
+ public:
+  engine(const lp_input& in, const pdlp_params& p) : in_(in), p_(p)
+  {
+    B200_CUDA_CHECK(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+    int dev = 0;
+    B200_CUDA_CHECK(cudaGetDevice(&dev));
+    B200_CUDA_CHECK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
+    B200_CUDA_CHECK(cudaMallocHost(&hres_, 64 * sizeof(double)));
+  }
+  ~engine()
+  {
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    if (hres_) cudaFreeHost(hres_);
+    if (s_) cudaStreamDestroy(s_);
+  }
+
+  pdlp_result run()
+  {
+    t_start_ = now_s();
+    pdlp_result r;
+    setup();
+    r.power_iterations = power_iters_;
+    if (!(std::isfinite(eta_) && eta_ > 0)) {
+      r.status    = kNumericalError;
+      r.step_size = eta_;
+      finish_times(r);
+      return r;
+    }
+    t_loop_ = now_s();
+    loop(r);
+    return r;
+  }
+
+ private:
+  // ------------------------------------------------------------------ setup
+  void setup()
+  {
+    const int m = in_.m, n = in_.n;
+    L_ = build_layout(m, n, in_.row_off, in_.col_idx, in_.val);
+    A_.upload(L_.a, s_);
+    AT_.upload(L_.at, s_);
+    vgrid_ = sms_ * 4;
+    const int g = std::max({sell_grid(A_.view64()), sell_grid(AT_.view64()), vgrid_});
+    partials_.resize((size_t)g * 4);
+    dres_.resize(64);
+
+    // Unscaled vectors in internal order; objective negated for maximisation
+    // (reference problem_helpers.cuh:132-151).
+    std::vector<double> c(n), l(n), u(n), lc(m), uc(m);
+    const double sgn = in_.maximize ? -1.0 : 1.0;
+    for (int j = 0; j < n; ++j) {
+      const int o = L_.col_new2old[j];
+      c[j]        = sgn * in_.c[o];
+      l[j]        = in_.var_lo[o];
+      u[j]        = in_.var_up[o];
+    }
+    for (int i = 0; i < m; ++i) {
+      const int o = L_.row_new2old[i];
+      lc[i]       = in_.con_lo[o];
+      uc[i]       = in_.con_up[o];
+    }
+    obj_scale_  = in_.maximize ? -1.0 : 1.0;
+    obj_offset_ = in_.maximize ? -in_.obj_offset : in_.obj_offset;
+    c64_.resize(n);
+    c64_.upload(c.data(), n, s_);
+    l64_.resize(n);
+    l64_.upload(l.data(), n, s_);
+    u64_.resize(n);
+    u64_.upload(u.data(), n, s_);
+    lc64_.resize(m);
+    lc64_.upload(lc.data(), m, s_);
+    uc64_.resize(m);
+    uc64_.upload(uc.data(), m, s_);
+
+    // Constant norms of the unscaled problem (reference convergence_information.cu:92-106).
+    c_norm_ = std::sqrt(reduce<0>(c64_.data(), (const double*)nullptr, n));
+    b_norm_ = std::sqrt(reduce<2>(lc64_.data(), uc64_.data(), m));
+
+    // Ruiz (10 passes) then Pock-Chambolle (alpha = 1) (reference initial_scaling.cu:152-365).
+    dr_.resize(m);
+    dc_.resize(n);
+    fill(dr_.data(), m, 1.0);
+    fill(dc_.data(), n, 1.0);
+    dbuf<double> rtmp(m), ctmp(n);
+    for (int it = 0; it < kRuizIterations; ++it) {
+      row_scaled_abs_kernel<0, false><<<sell_grid(A_.view64()), kBlock, 0, s_>>>(
+        A_.view64(), dr_.data(), dc_.data(), 0.0, rtmp.data());
+      row_scaled_abs_kernel<0, true><<<sell_grid(AT_.view64()), kBlock, 0, s_>>>(
+        AT_.view64(), dr_.data(), dc_.data(), 0.0, ctmp.data());
+      apply_root_scaling_kernel<<<vgrid_, kBlock, 0, s_>>>(dr_.data(), rtmp.data(), m);
+      apply_root_scaling_kernel<<<vgrid_, kBlock, 0, s_>>>(dc_.data(), ctmp.data(), n);
+    }
+    row_scaled_abs_kernel<1, false><<<sell_grid(A_.view64()), kBlock, 0, s_>>>(
+      A_.view64(), dr_.data(), dc_.data(), kPcAlpha, rtmp.data());
+    row_scaled_abs_kernel<1, true><<<sell_grid(AT_.view64()), kBlock, 0, s_>>>(
+      AT_.view64(), dr_.data(), dc_.data(), 2.0 - kPcAlpha, ctmp.data());
+    apply_root_scaling_kernel<<<vgrid_, kBlock, 0, s_>>>(dr_.data(), rtmp.data(), m);
+    apply_root_scaling_kernel<<<vgrid_, kBlock, 0, s_>>>(dc_.data(), ctmp.data(), n);
+    B200_LAUNCH_CHECK();
+
+    // Scaled matrix values in the iterate precision.
+    As_.resize(A_.stored());
+    ATs_.resize(AT_.stored());
+    scale_values_kernel<TX, false><<<sell_grid(A_.view64()), kBlock, 0, s_>>>(
+      A_.view64(), dr_.data(), dc_.data(), As_.data());
+    scale_values_kernel<TX, true><<<sell_grid(AT_.view64()), kBlock, 0, s_>>>(
+      AT_.view64(), dr_.data(), dc_.data(), ATs_.data());
+
+    // Scaled vectors, then bound / objective rescaling (reference initial_scaling.cu:95-149, 417-569).
+    dbuf<double> cs(n), ls(n), us(n), lcs(m), ucs(m);
+    scale_vectors_kernel<<<vgrid_, kBlock, 0, s_>>>(c64_.data(), l64_.data(), u64_.data(),
+                                                    lc64_.data(), uc64_.data(), dc_.data(),
+                                                    dr_.data(), n, m, cs.data(), ls.data(),
+                                                    us.data(), lcs.data(), ucs.data());
+    beta_  = 1.0 / (std::sqrt(reduce<2>(lcs.data(), ucs.data(), m)) + 1.0);
+    gamma_ = 1.0 / (std::sqrt(reduce<0>(cs.data(), (const double*)nullptr, n)) + 1.0);
+    cs_.resize(n);
+    ls_.resize(n);
+    us_.resize(n);
+    lcs_.resize(m);
+    ucs_.resize(m);
+    rescale_vectors_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(
+      cs.data(), ls.data(), us.data(), lcs.data(), ucs.data(), beta_, gamma_, n, m, cs_.data(),
+      ls_.data(), us_.data(), lcs_.data(), ucs_.data());
+    B200_LAUNCH_CHECK();
+
+    // Step size from the largest singular value of the scaled A (reference pdlp.cu:2620-2731).
+    power_iteration();
+    omega_      = 1.0;  // bound_objective_rescaling => primal weight 1 (pdlp.cu:2799-2810)
+    best_omega_ = 1.0;
+
+    // Iterates (internal order, scaled).
+    for (auto* b : {&x_, &xhat_, &slack_, &xbar_, &xa_, &aty_}) {
+      b->resize(n);
+      b->zero(s_);
+    }
+    for (auto* b : {&y_, &yhat_, &ybar_, &ya_}) {
+      b->resize(m);
+      b->zero(s_);
+    }
+    xu_.resize(n);
+    su_.resize(n);
+    yu_.resize(m);
+    if (!p_.initial_primal.empty() || !p_.initial_dual.empty()) load_initial_solution();
+    // project_initial_primal (reference pdlp.cu:2237-2262): only the current primal iterate.
+    clamp_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(x_.data(), ls_.data(), us_.data(), n);
+    scalars_.resize(1);
+    B200_LAUNCH_CHECK();
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+  }
+
+  // Initial iterates: copied to x, x_hat and the anchor, then scaled
+  // (reference pdlp.cu:1109-1245, compute_initial_primal_weight_before_scaling branch).
+  void load_initial_solution()
+  {
+    const int m = in_.m, n = in_.n;
+    std::vector<double> dr(m), dc(n);
+    dr_.download(dr.data(), m, s_);
+    dc_.download(dc.data(), n, s_);
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    if (!p_.initial_primal.empty()) {
+      std::vector<TX> x(n);
+      for (int j = 0; j < n; ++j) {
+        double v = p_.initial_primal[L_.col_new2old[j]];
+        v        = dc[j] != 0.0 ? v / dc[j] : v;
+        x[j]     = (TX)(v * beta_);
+      }
+      for (auto* b : {&x_, &xhat_, &xa_}) b->upload(x.data(), n, s_);
+    }
+    if (!p_.initial_dual.empty()) {
+      std::vector<TX> y(m);
+      for (int i = 0; i < m; ++i) {
+        double v = p_.initial_dual[L_.row_new2old[i]];
+        if (in_.maximize) v = -v;
+        v    = dr[i] != 0.0 ? v / dr[i] : v;
+        y[i] = (TX)(v * gamma_);
+      }
+      for (auto* b : {&y_, &yhat_, &ya_}) b->upload(y.data(), m, s_);
+    }
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+  }
+
+  void fill(double* p, int n, double v)
+  {
+    std::vector<double> h(n, v);
+    B200_CUDA_CHECK(cudaMemcpyAsync(p, h.data(), n * sizeof(double), cudaMemcpyHostToDevice, s_));
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+  }
+
+  // Sum reduction of a vector expression (see vec_reduce_kernel) returned to the host.
+  template <int MODE, typename TA>
+  double reduce(const TA* a, const TA* b, int n)
+  {
+    vec_reduce_kernel<MODE, TA><<<vgrid_, kBlock, 0, s_>>>(a, b, n, partials_.data(), nullptr);
+    finalize_sum_kernel<1><<<1, kBlock, 0, s_>>>(partials_.data(), vgrid_, dres_.data());
+    B200_LAUNCH_CHECK();
+    B200_CUDA_CHECK(cudaMemcpyAsync(hres_, dres_.data(), sizeof(double), cudaMemcpyDeviceToHost, s_));
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    return hres_[0];
+  }
+
+  void power_iteration()
+  {
+    const int m = in_.m, n = in_.n;
+    // Start vector: std::mt19937(1) normals in the user's constraint order (pdlp.cu:2632-2638).
+    std::vector<double> z0(m), z(m);
+    std::mt19937 gen(1);
+    std::normal_distribution<double> dist(0.0, 1.0);
+    for (int i = 0; i < m; ++i) z0[i] = dist(gen);
+    for (int i = 0; i < m; ++i) z[i] = z0[L_.row_new2old[i]];
+    dbuf<double> dz(m), dq(m), datq(n);
+    dbuf<power_state> ps(1);
+    ps.zero(s_);
+    dz.upload(z.data(), m, s_);
+    dbuf<TX> q_tx, atq_tx;
+    const auto As  = A_.view<TX>(As_.data());
+    const auto ATs = AT_.view<TX>(ATs_.data());
+    const int ga = sell_grid(As), gt = sell_grid(ATs);
+    double* res = dres_.data();
+    auto one_iteration = [&]() {
+      vec_reduce_kernel<0, double><<<vgrid_, kBlock, 0, s_>>>(dz.data(), nullptr, m,
+                                                              partials_.data(), &ps.data()->done);
+      finalize_sum_kernel<1><<<1, kBlock, 0, s_>>>(partials_.data(), vgrid_, res + 0);
+      power_normalize_kernel<<<vgrid_, kBlock, 0, s_>>>(dz.data(), dq.data(), m, res + 0, ps.data());
+      sell_map_kernel<TX, double, store_epi<double>><<<gt, kBlock, 0, s_>>>(
+        ATs, dq.data(), store_epi<double>{datq.data(), &ps.data()->done}, partials_.data());
+      sell_map_kernel<TX, double, power_z_epi><<<ga, kBlock, 0, s_>>>(
+        As, datq.data(), power_z_epi{dz.data(), dq.data(), &ps.data()->done}, partials_.data());
+      finalize_sum_kernel<1><<<1, kBlock, 0, s_>>>(partials_.data(), ga, res + 1);
+      power_residual_kernel<<<vgrid_, kBlock, 0, s_>>>(dq.data(), dz.data(), m, res + 1,
+                                                       ps.data(), partials_.data());
+      finalize_sum_kernel<1><<<1, kBlock, 0, s_>>>(partials_.data(), vgrid_, res + 2);
+      power_check_kernel<<<1, 1, 0, s_>>>(ps.data(), res + 1, res + 2, kPowerTol);
+    };
+    // Chunks of 32 iterations are captured once into a graph and replayed until convergence.
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    B200_CUDA_CHECK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < 32; ++i) one_iteration();
+    B200_CUDA_CHECK(cudaStreamEndCapture(s_, &graph));
+    B200_CUDA_CHECK(cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphDestroy(graph);
+    power_state h{};
+    for (int done_iters = 0; done_iters < kPowerMaxIters; done_iters += 32) {
+      if (kPowerMaxIters - done_iters < 32) {
+        for (int i = 0; i < kPowerMaxIters - done_iters; ++i) one_iteration();
+      } else {
+        B200_CUDA_CHECK(cudaGraphLaunch(exec, s_));
+      }
+      B200_CUDA_CHECK(cudaMemcpyAsync(&h, ps.data(), sizeof(h), cudaMemcpyDeviceToHost, s_));
+      B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+      if (h.done) break;
+    }
+    cudaGraphExecDestroy(exec);
+    power_iters_ = h.iters;
+    eta_         = kStepScaling / std::sqrt(h.s2);
+  }
+
+  // ------------------------------------------------------------------ iteration kernels
+  dev_sell<TX> As_view() const { return A_.view<TX>(As_.data()); }
+  dev_sell<TX> ATs_view() const { return AT_.view<TX>(ATs_.data()); }
+
+  template <bool MAJOR, bool HALPERN, bool SAVE_ATY>
+  void launch_primal(int it_off)
+  {
+    const auto A = ATs_view();
+    primal_epi<TX, MAJOR, HALPERN, SAVE_ATY> e{x_.data(),    cs_.data(),    ls_.data(),
+                                               us_.data(),   xa_.data(),    xbar_.data(),
+                                               x_.data(),    xhat_.data(),  slack_.data(),
+                                               aty_.data(),  scalars_.data(), it_off};
+    sell_map_kernel<TX, TX, decltype(e)><<<sell_grid(A), kBlock, 0, s_>>>(A, y_.data(), e,
+                                                                         partials_.data());
+  }
+  template <bool MAJOR, bool HALPERN, bool FPE>
+  void launch_dual(int it_off)
+  {
+    const auto A = As_view();
+    dual_epi<TX, MAJOR, HALPERN, FPE> e{y_.data(),    lcs_.data(), ucs_.data(),     ya_.data(),
+                                        ybar_.data(), y_.data(),   yhat_.data(),    scalars_.data(),
+                                        it_off};
+    sell_map_kernel<TX, TX, decltype(e)><<<sell_grid(A), kBlock, 0, s_>>>(A, xbar_.data(), e,
+                                                                         partials_.data());
+  }
+
+  void plain_iterations(int L)  // L fused iterations, then t0 += L
+  {
+    for (int i = 0; i < L; ++i) {
+      launch_primal<false, true, false>(i);
+      launch_dual<false, true, false>(i);
+    }
+    advance_kernel<<<1, 1, 0, s_>>>(scalars_.data(), L);
+  }
+
+  void run_plain(long R)
+  {
+    for (int L = 128; L >= 1; L >>= 1) {
+      while (R >= L) {
+        auto it = graphs_.find(L);
+        if (it == graphs_.end()) {
+          cudaGraph_t g;
+          cudaGraphExec_t e;
+          B200_CUDA_CHECK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+          plain_iterations(L);
+          B200_CUDA_CHECK(cudaStreamEndCapture(s_, &g));
+          B200_CUDA_CHECK(cudaGraphInstantiate(&e, g, 0));
+          cudaGraphDestroy(g);
+          it = graphs_.emplace(L, e).first;
+        }
+        B200_CUDA_CHECK(cudaGraphLaunch(it->second, s_));
+        R -= L;
+      }
+    }
+  }
+
+  void set_scalars(long long t0)
+  {
+    set_scalars_kernel<<<1, 1, 0, s_>>>(scalars_.data(), eta_ / omega_, eta_ * omega_, eta_,
+                                        omega_, t0);
+    B200_LAUNCH_CHECK();
+  }
+
+  // ------------------------------------------------------------------ termination
+  conv_info evaluate()
+  {
+    const int m = in_.m, n = in_.n;
+    unscale_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(xhat_.data(), yhat_.data(), slack_.data(),
+                                                  dc_.data(), dr_.data(), 1.0 / beta_,
+                                                  1.0 / gamma_, n, m, xu_.data(), yu_.data(),
+                                                  su_.data());
+    const auto A = A_.view64(), AT = AT_.view64();
+    sell_map_kernel<double, double, term_primal_epi><<<sell_grid(A), kBlock, 0, s_>>>(
+      A, xu_.data(), term_primal_epi{lc64_.data(), uc64_.data(), yu_.data()}, partials_.data());
+    finalize_sum_kernel<2><<<1, kBlock, 0, s_>>>(partials_.data(), sell_grid(A), dres_.data());
+    sell_map_kernel<double, double, term_dual_epi><<<sell_grid(AT), kBlock, 0, s_>>>(
+      AT, yu_.data(), term_dual_epi{c64_.data(), xu_.data(), su_.data()}, partials_.data());
+    finalize_sum_kernel<3><<<1, kBlock, 0, s_>>>(partials_.data(), sell_grid(AT),
+                                                 dres_.data() + 2);
+    B200_LAUNCH_CHECK();
+    B200_CUDA_CHECK(
+      cudaMemcpyAsync(hres_, dres_.data(), 5 * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    conv_info cv;
+    cv.l2_primal  = std::sqrt(hres_[0]);
+    cv.l2_dual    = std::sqrt(hres_[2]);
+    cv.primal_obj = hres_[3];
+    cv.dual_obj   = hres_[4] + hres_[1];
+    if (obj_scale_ != 1.0 || obj_offset_ != 0.0) {
+      cv.primal_obj = obj_scale_ * (cv.primal_obj + obj_offset_);
+      cv.dual_obj   = obj_scale_ * (cv.dual_obj + obj_offset_);
+    }
+    cv.gap     = std::fabs(cv.primal_obj - cv.dual_obj);
+    cv.abs_obj = std::fabs(cv.primal_obj) + std::fabs(cv.dual_obj);
+    return cv;
+  }
+
+  void finish(pdlp_result& r, int status, const conv_info& cv, long k)
+  {
+    const int m = in_.m, n = in_.n;
+    r.status     = status;
+    r.iterations = k;
+    r.primal_obj = cv.primal_obj;
+    r.dual_obj   = cv.dual_obj;
+    r.l2_primal  = cv.l2_primal;
+    r.l2_dual    = cv.l2_dual;
+    r.rel_primal = cv.l2_primal / (1.0 + b_norm_);
+    r.rel_dual   = cv.l2_dual / (1.0 + c_norm_);
+    r.gap        = cv.gap;
+    r.rel_gap    = cv.gap / (1.0 + cv.abs_obj);
+    r.step_size  = eta_;
+    r.primal_weight = omega_;
+    r.restarts   = restarts_;
+    std::vector<double> x(n), y(m), s(n);
+    xu_.download(x.data(), n, s_);
+    yu_.download(y.data(), m, s_);
+    su_.download(s.data(), n, s_);
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    r.x.resize(n);
+    r.rc.resize(n);
+    r.y.resize(m);
+    const double sgn = in_.maximize ? -1.0 : 1.0;  // reference solve.cu:584-588
+    for (int j = 0; j < n; ++j) {
+      r.x[L_.col_new2old[j]]  = x[j];
+      r.rc[L_.col_new2old[j]] = sgn * s[j];
+    }
+    for (int i = 0; i < m; ++i) r.y[L_.row_new2old[i]] = sgn * y[i];
+    finish_times(r);
+  }
+
+  void finish_times(pdlp_result& r)
+  {
+    const double t = now_s();
+    r.solve_time   = t - t_start_;
+    r.setup_time   = (t_loop_ > 0 ? t_loop_ : t) - t_start_;
+    r.loop_time    = t_loop_ > 0 ? t - t_loop_ : 0.0;
+  }
+
+  // ------------------------------------------------------------------ main loop
+  void loop(pdlp_result& r)
+  {
+    const int m = in_.m, n = in_.n;
+    const double qnan = std::numeric_limits<double>::quiet_NaN();
+    const double inf  = std::numeric_limits<double>::infinity();
+    double fpe = qnan, fpe0 = qnan, last_trial = inf;
+    double pid_sum = 0.0, pid_last = 0.0, best_gap = inf;
+    long since = 0;
+    set_scalars(0);
+    const auto A = As_view(), AT = ATs_view();
+
+    for (long k = 0;;) {
+      const bool major = (k % kMajor == 0 && k > 0) || k <= 0;
+      const bool cond  = (k % conditional_major(k)) == 0;
+      bool restarted   = false;
+      if (major || cond) {
+        const conv_info cv = evaluate();
+        const bool primal_ok = cv.l2_primal <= p_.abs_primal + p_.rel_primal * b_norm_;
+        int status           = kNoTermination;
+        if (cv.l2_dual <= p_.abs_dual + p_.rel_dual * c_norm_ && primal_ok &&
+            cv.gap <= p_.abs_gap + p_.rel_gap * cv.abs_obj)
+          status = kOptimal;
+        else if (primal_ok)
+          status = kPrimalFeasible;
+        if (p_.log_to_console && (k % 1000 == 0))
+          std::printf("%7ld %+.8e %+.8e  %8.2e   %8.2e     %8.2e   %.3fs\n", k, cv.primal_obj,
+                      cv.dual_obj, cv.gap, cv.l2_primal, cv.l2_dual, now_s() - t_start_);
+        if (k > 1 && status == kOptimal) return finish(r, kOptimal, cv, k);
+        if (now_s() - t_start_ >= p_.time_limit) return finish(r, kTimeLimit, cv, k);
+        if (k >= p_.iteration_limit) return finish(r, kIterationLimit, cv, k);
+        if (!std::isfinite(cv.l2_primal) || !std::isfinite(cv.l2_dual))
+          return finish(r, kNumericalError, cv, k);
+
+        if (major) {
+          // should_cupdlpx_restart (reference pdlp_restart_strategy.cu:689-754)
+          bool restart = false;
+          if (k == kMajor)
+            restart = true;
+          else if (k > kMajor) {
+            if (fpe <= kSufficientReduction * fpe0)
+              restart = true;
+            else if (fpe <= kNecessaryReduction * fpe0 && fpe > last_trial)
+              restart = true;
+            else if ((double)since >= kArtificialRestart * (double)k)
+              restart = true;
+          }
+          last_trial = fpe;
+          if (restart) {
+            // cupdlpx_restart + PID primal weight (reference pdlp_restart_strategy.cu:758-986)
+            const double pd = reduce<1>(xa_.data(), xhat_.data(), n);
+            const double dd = reduce<1>(ya_.data(), yhat_.data(), m);
+            const double rel_dual   = cv.l2_dual / (1.0 + c_norm_);
+            const double rel_primal = cv.l2_primal / (1.0 + b_norm_);
+            const double lp = std::sqrt(pd), ld = std::sqrt(dd);
+            const double ratio = rel_primal == 0.0 ? inf : rel_dual / rel_primal;
+            if (lp > 1e-16 && ld > 1e-16 && lp < 1e12 && ld < 1e12 && ratio > 1e-8 &&
+                ratio < 1e8) {
+              const double err  = std::log(ld) - std::log(lp) - std::log(omega_);
+              pid_sum           = pid_sum * kISmooth + err;
+              const double derr = err - pid_last;
+              omega_   = std::exp(kKp * err + kKi * pid_sum + kKd * derr) * omega_;
+              pid_last = err;
+            } else {
+              omega_   = best_omega_;
+              pid_sum  = 0.0;
+              pid_last = 0.0;
+            }
+            const double rgap = std::fabs(std::log10(ratio));
+            if (rgap < best_gap) {
+              best_gap    = rgap;
+              best_omega_ = omega_;
+            }
+            B200_CUDA_CHECK(cudaMemcpyAsync(x_.data(), xhat_.data(), n * sizeof(TX),
+                                            cudaMemcpyDeviceToDevice, s_));
+            B200_CUDA_CHECK(cudaMemcpyAsync(xa_.data(), xhat_.data(), n * sizeof(TX),
+                                            cudaMemcpyDeviceToDevice, s_));
+            B200_CUDA_CHECK(cudaMemcpyAsync(y_.data(), yhat_.data(), m * sizeof(TX),
+                                            cudaMemcpyDeviceToDevice, s_));
+            B200_CUDA_CHECK(cudaMemcpyAsync(ya_.data(), yhat_.data(), m * sizeof(TX),
+                                            cudaMemcpyDeviceToDevice, s_));
+            since      = 0;
+            last_trial = inf;
+            restarted  = true;
+            ++restarts_;
+            set_scalars(0);
+          }
+        }
+      }
+
+      const bool mstep = is_major_step(k);
+      const bool fpe_it = ((k + 1) % kMajor == 0) || restarted;
+      if (!mstep && !fpe_it) {
+        long R = 1;
+        while (R < 255) {
+          const long kk = k + R;
+          if (is_check(kk) || is_major_step(kk) || ((kk + 1) % kMajor == 0)) break;
+          ++R;
+        }
+        run_plain(R);
+        k += R;
+        since += R;
+        continue;
+      }
+
+      // A step that keeps x_hat / y_hat / slack (major) and/or measures the fixed-point error.
+      if (fpe_it) {
+        if (mstep) {
+          launch_primal<true, false, true>(0);
+          launch_dual<true, false, true>(0);
+        } else {
+          launch_primal<false, false, true>(0);
+          launch_dual<false, false, true>(0);
+        }
+        finalize_sum_kernel<1><<<1, kBlock, 0, s_>>>(partials_.data(), sell_grid(A),
+                                                     dres_.data() + 8);
+        // compute_fixed_error (reference pdlp.cu:1749-1857)
+        sell_map_kernel<TX, TX, fpe_epi<TX>><<<sell_grid(AT), kBlock, 0, s_>>>(
+          AT, ybar_.data(), fpe_epi<TX>{aty_.data(), xbar_.data(), x_.data()}, partials_.data());
+        finalize_sum_kernel<2><<<1, kBlock, 0, s_>>>(partials_.data(), sell_grid(AT),
+                                                     dres_.data() + 9);
+        halpern_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(x_.data(), xbar_.data(), xa_.data(), n,
+                                                      y_.data(), ybar_.data(), ya_.data(), m,
+                                                      scalars_.data());
+        advance_kernel<<<1, 1, 0, s_>>>(scalars_.data(), 1);
+        B200_LAUNCH_CHECK();
+        B200_CUDA_CHECK(cudaMemcpyAsync(hres_ + 8, dres_.data() + 8, 3 * sizeof(double),
+                                        cudaMemcpyDeviceToHost, s_));
+        B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+        const double ndy = hres_[8], inter = hres_[9], ndx = hres_[10];
+        const double movement = ndx * omega_ + ndy / omega_;
+        fpe = std::sqrt(movement + 2.0 * inter * eta_);
+        if (restarted) fpe0 = fpe;
+      } else {
+        launch_primal<true, true, false>(0);
+        launch_dual<true, true, false>(0);
+        advance_kernel<<<1, 1, 0, s_>>>(scalars_.data(), 1);
+        B200_LAUNCH_CHECK();
+      }
+      ++k;
+      ++since;
+    }
+  }
+
+  // ------------------------------------------------------------------ state
+  const lp_input& in_;
+  const pdlp_params& p_;
+  cudaStream_t s_ = nullptr;
+  int sms_ = 148, vgrid_ = 592;
+  double* hres_ = nullptr;
+  double t_start_ = 0, t_loop_ = 0;
+
+  lp_layout L_;
+  dev_matrix A_, AT_;
+  dbuf<TX> As_, ATs_;
+  dbuf<double> c64_, l64_, u64_, lc64_, uc64_, dr_, dc_;
+  dbuf<TX> cs_, ls_, us_, lcs_, ucs_;
+  dbuf<TX> x_, xhat_, slack_, xbar_, xa_, aty_, y_, yhat_, ybar_, ya_;
+  dbuf<double> xu_, yu_, su_;
+  dbuf<double> partials_, dres_;
+  dbuf<pdlp_scalars> scalars_;
+  std::map<int, cudaGraphExec_t> graphs_;
+
+  double obj_scale_ = 1.0, obj_offset_ = 0.0;
+  double c_norm_ = 0, b_norm_ = 0, beta_ = 1, gamma_ = 1;
+  double eta_ = 0, omega_ = 1, best_omega_ = 1;
+  int power_iters_ = 0, restarts_ = 0;
+};
+
+}  // namespace
+
+pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p)
+{
+  if (p.precision == 1) {
+    engine<float> e(in, p);
+    return e.run();
+  }
+  engine<double> e(in, p);
+  return e.run();
+}
+
+}  // namespace cuopt_b200

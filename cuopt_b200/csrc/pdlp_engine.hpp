@@ -1,0 +1,57 @@
+// PDLP engine interface used by the C API layer.
+//
+// Counterpart of the reference's solve_lp -> run_pdlp -> pdlp_solver_t::run_solver chain
+// (cpp/src/pdlp/solve.cu:556-590, 1124-1342; cpp/src/pdlp/pdlp.cu:2013-2457).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace cuopt_b200 {
+
+// The LP as handed over by the C interface: user order, minimise or maximise,
+// con_lo <= A x <= con_up, var_lo <= x <= var_up.
+struct lp_input {
+  int m = 0, n = 0;
+  const int* row_off    = nullptr;  // m + 1
+  const int* col_idx    = nullptr;  // nnz
+  const double* val     = nullptr;  // nnz
+  const double* c       = nullptr;  // n
+  const double* con_lo  = nullptr;  // m
+  const double* con_up  = nullptr;  // m
+  const double* var_lo  = nullptr;  // n
+  const double* var_up  = nullptr;  // n
+  double obj_offset     = 0.0;
+  bool maximize         = false;
+};
+
+struct pdlp_params {
+  double abs_primal = 1e-4, rel_primal = 1e-4;
+  double abs_dual = 1e-4, rel_dual = 1e-4;
+  double abs_gap = 1e-4, rel_gap = 1e-4;
+  int64_t iteration_limit = 2147483647;
+  double time_limit       = 1e300;
+  int precision           = 0;  // 0 FP64, 1 mixed FP32/FP64
+  int refinement_passes   = 4;
+  double refinement_tol   = 1e-8;
+  bool log_to_console     = false;
+  std::vector<double> initial_primal;  // user order, optional
+  std::vector<double> initial_dual;    // user order, optional
+};
+
+struct pdlp_result {
+  int status = 0;  // CUOPT_TERIMINATION_STATUS_*
+  std::vector<double> x, y, rc;
+  int64_t iterations = 0;
+  double primal_obj = 0, dual_obj = 0;
+  double l2_primal = 0, l2_dual = 0, rel_primal = 0, rel_dual = 0, gap = 0, rel_gap = 0;
+  double solve_time = 0, setup_time = 0, loop_time = 0;
+  double step_size = 0, primal_weight = 0;
+  int restarts = 0, power_iterations = 0, refinement_passes = 0;
+};
+
+// Runs PDLP (Stable3) on the GPU.  Throws std::exception subclasses on CUDA or input errors.
+pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p);
+
+}  // namespace cuopt_b200

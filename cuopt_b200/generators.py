@@ -1,0 +1,185 @@
+"""Seeded synthetic LPs with an optimum known by construction (the benchmark workloads).
+
+Every generator returns an ``LP`` with CSR constraint matrix, bounds, and the constructed primal /
+dual optimum (x_star, y_star) and reduced costs (s_star) that satisfy the KKT conditions exactly:
+    A x* within [con_lo, con_up],   var_lo <= x* <= var_up,
+    c = A^T y* + s*,   s*_j >= 0 where x*_j = var_lo_j,  s*_j <= 0 where x*_j = var_up_j, else 0,
+    y*_i >= 0 only on active lower row bounds, y*_i <= 0 only on active upper row bounds.
+So c.x* is the optimal objective.  Random numbers come from numpy's PCG64 seeded with
+``config_id * 1000 + instance``.
+
+Workloads (sizes are parameters so the tests can run them small):
+  constructed_lp   config 0 / 1 / 4: equality rows, [0, 10] bounds, k non-zeros per column at
+                   uniform rows, N(0,1) values; 30% of x* at 0, the rest U(0.5, 5).
+  skewed_lp        config 2: Zipf(1.3) row lengths capped at 5000, uniform columns, log-uniform
+                   magnitudes in [1e-3, 1e3] with random signs, 50% 'E' / 50% 'L' rows
+                   (the slack of an 'L' row is implicit), bounds [0, U(1,100)], 10% free columns.
+  batch_lps        config 3: many config-0 LPs with m log-uniform in [200, 20000], n = 2.5 m,
+                   non-zeros per column uniform in 6..12.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class LP:
+    m: int
+    n: int
+    row_off: np.ndarray  # int32 [m+1]
+    col_idx: np.ndarray  # int32 [nnz]
+    val: np.ndarray      # float64 [nnz]
+    c: np.ndarray
+    con_lo: np.ndarray
+    con_up: np.ndarray
+    var_lo: np.ndarray
+    var_up: np.ndarray
+    x_star: np.ndarray
+    y_star: np.ndarray
+    s_star: np.ndarray
+    name: str = "lp"
+
+    @property
+    def nnz(self) -> int:
+        return int(self.row_off[-1])
+
+    @property
+    def optimal_objective(self) -> float:
+        return float(np.dot(self.c, self.x_star))
+
+    def matvec(self, x: np.ndarray) -> np.ndarray:
+        """A @ x with numpy (row sums)."""
+        rows = np.repeat(np.arange(self.m), np.diff(self.row_off))
+        return np.bincount(rows, weights=self.val * x[self.col_idx], minlength=self.m)
+
+    def rmatvec(self, y: np.ndarray) -> np.ndarray:
+        """A^T @ y with numpy."""
+        rows = np.repeat(np.arange(self.m), np.diff(self.row_off))
+        return np.bincount(self.col_idx, weights=self.val * y[rows], minlength=self.n)
+
+
+def _csr_from_columns(m: int, n: int, rows: np.ndarray, cols: np.ndarray, vals: np.ndarray):
+    """CSR (rows sorted, columns ascending inside a row) from coordinate lists."""
+    order = np.lexsort((cols, rows))
+    rows, cols, vals = rows[order], cols[order], vals[order]
+    counts = np.bincount(rows, minlength=m)
+    row_off = np.zeros(m + 1, dtype=np.int64)
+    np.cumsum(counts, out=row_off[1:])
+    return row_off.astype(np.int32), cols.astype(np.int32), vals.astype(np.float64)
+
+
+def _distinct_rows_per_column(rng: np.random.Generator, m: int, n: int, k: int) -> np.ndarray:
+    """[n, k] row indices, distinct inside each column, uniform over [0, m)."""
+    if k > m:
+        raise ValueError("more non-zeros per column than rows")
+    r = rng.integers(0, m, size=(n, k), dtype=np.int64)
+    while True:
+        s = np.sort(r, axis=1)
+        bad = np.any(s[:, 1:] == s[:, :-1], axis=1)
+        if not bad.any():
+            return r
+        r[bad] = rng.integers(0, m, size=(int(bad.sum()), k), dtype=np.int64)
+
+
+def constructed_lp(m: int, n: int, nnz_per_col: int = 8, seed: int = 0, upper: float = 10.0,
+                   name: str = "constructed") -> LP:
+    """Config-0 generator: min c.x s.t. A x = b, 0 <= x <= upper, optimum known."""
+    rng = np.random.default_rng(seed)
+    rows = _distinct_rows_per_column(rng, m, n, nnz_per_col)
+    vals = rng.standard_normal((n, nnz_per_col))
+    cols = np.repeat(np.arange(n, dtype=np.int64), nnz_per_col)
+    row_off, col_idx, val = _csr_from_columns(m, n, rows.ravel(), cols, vals.ravel())
+    x = rng.uniform(0.5, 5.0, size=n)
+    zero = rng.random(n) < 0.3
+    x[zero] = 0.0
+    y = rng.standard_normal(m)
+    s = np.where(zero, rng.uniform(0.1, 1.0, size=n), 0.0)
+    lp = LP(m, n, row_off, col_idx, val, np.zeros(n), np.zeros(m), np.zeros(m),
+            np.zeros(n), np.full(n, float(upper)), x, y, s, name)
+    b = lp.matvec(x)
+    lp.con_lo = b.copy()
+    lp.con_up = b.copy()
+    lp.c = lp.rmatvec(y) + s
+    return lp
+
+
+def skewed_lp(m: int, n: int, seed: int = 2000, zipf_a: float = 1.3, cap: int = 5000,
+              name: str = "skewed") -> LP:
+    """Config-2 generator (row lengths Zipf(a) capped, mixed senses, free columns)."""
+    rng = np.random.default_rng(seed)
+    lens = np.minimum(rng.zipf(zipf_a, size=m), min(cap, n)).astype(np.int64)
+    rows = np.repeat(np.arange(m, dtype=np.int64), lens)
+    cols = rng.integers(0, n, size=int(lens.sum()), dtype=np.int64)
+    # drop duplicate (row, col) pairs
+    key = rows * n + cols
+    key, first = np.unique(key, return_index=True)
+    rows, cols = rows[first], cols[first]
+    mag = 10.0 ** rng.uniform(-3.0, 3.0, size=rows.size)
+    sign = np.where(rng.random(rows.size) < 0.5, -1.0, 1.0)
+    row_off, col_idx, val = _csr_from_columns(m, n, rows, cols, mag * sign)
+    ub = rng.uniform(1.0, 100.0, size=n)
+    lb = np.zeros(n)
+    free = rng.random(n) < 0.1
+    lb[free], ub[free] = -np.inf, np.inf
+    # x*: bounded columns 30% at lower, 10% at upper, rest interior; free columns N(0, 1).
+    u = rng.random(n)
+    at_lo = (~free) & (u < 0.3)
+    at_up = (~free) & (u >= 0.3) & (u < 0.4)
+    x = np.where(free, rng.standard_normal(n), rng.uniform(0.1, 0.9, size=n) * np.where(free, 1.0, ub))
+    x[at_lo] = 0.0
+    x[at_up] = ub[at_up]
+    s = np.zeros(n)
+    s[at_lo] = rng.uniform(0.1, 1.0, size=int(at_lo.sum()))
+    s[at_up] = -rng.uniform(0.1, 1.0, size=int(at_up.sum()))
+    lp = LP(m, n, row_off, col_idx, val, np.zeros(n), np.zeros(m), np.zeros(m), lb, ub, x,
+            np.zeros(m), s, name)
+    ax = lp.matvec(x)
+    eq = rng.random(m) < 0.5
+    active = rng.random(m) < 0.5
+    y = np.where(eq, rng.standard_normal(m), 0.0)
+    le_active = (~eq) & active
+    y[le_active] = -rng.uniform(0.1, 1.0, size=int(le_active.sum()))
+    slack = np.where((~eq) & (~active), rng.uniform(0.1, 1.0, size=m) * (1.0 + np.abs(ax)), 0.0)
+    lp.con_lo = np.where(eq, ax, -np.inf)
+    lp.con_up = ax + slack
+    lp.y_star = y
+    lp.c = lp.rmatvec(y) + s
+    return lp
+
+
+def batch_lps(count: int = 512, seed: int = 3000, m_lo: int = 200, m_hi: int = 20000):
+    """Config-3 generator: `count` config-0 LPs of uneven sizes."""
+    rng = np.random.default_rng(seed)
+    ms = np.exp(rng.uniform(np.log(m_lo), np.log(m_hi), size=count)).astype(int)
+    ks = rng.integers(6, 13, size=count)
+    return [constructed_lp(int(m), int(2.5 * m), int(k), seed=seed + 1 + i, name=f"batch{i}")
+            for i, (m, k) in enumerate(zip(ms, ks))]
+
+
+def kkt_relative_error(lp: LP, x: np.ndarray, y: np.ndarray) -> dict:
+    """Relative KKT errors of (x, y) with the reference's definitions
+    (convergence_information.cu:492-811): primal residual against the row bounds, dual residual
+    with the reduced cost taken as the projection of c - A^T y onto the normal cone of the
+    variable bounds at x, and the primal/dual objective gap."""
+    ax = lp.matvec(x)
+    rp = ax - np.clip(ax, lp.con_lo, lp.con_up)
+    g = lp.c - lp.rmatvec(y)
+    # reduced cost allowed only where the bound is active
+    rc = np.where(np.isfinite(lp.var_lo) & (x <= lp.var_lo) & (g > 0), g, 0.0) + \
+        np.where(np.isfinite(lp.var_up) & (x >= lp.var_up) & (g < 0), g, 0.0)
+    rd = g - rc
+    fin = lambda v: np.where(np.isfinite(v), v, 0.0)
+    pobj = float(lp.c @ x)
+    dobj = float(np.sum(np.maximum(y, 0) * fin(lp.con_lo) + np.minimum(y, 0) * fin(lp.con_up))
+                 + np.sum(np.maximum(rc, 0) * fin(lp.var_lo) + np.minimum(rc, 0) * fin(lp.var_up)))
+    bnorm = np.sqrt(np.sum(np.where(np.isfinite(lp.con_lo) & (lp.con_lo != lp.con_up),
+                                    fin(lp.con_lo) ** 2, 0.0) + fin(lp.con_up) ** 2))
+    return {
+        "rel_primal": float(np.linalg.norm(rp) / (1.0 + bnorm)),
+        "rel_dual": float(np.linalg.norm(rd) / (1.0 + np.linalg.norm(lp.c))),
+        "rel_gap": abs(pobj - dobj) / (1.0 + abs(pobj) + abs(dobj)),
+        "primal_objective": pobj,
+        "dual_objective": dobj,
+    }

@@ -1,0 +1,76 @@
+/*
+ * cuopt_b200 extensions to the cuOpt LP C interface.
+ *
+ * These entry points sit beside the drop-in cuopt_c.h interface.  Each one names the reference
+ * interface it replaces, or says that it has no counterpart in the reference.
+ */
+#ifndef CUOPT_B200_H
+#define CUOPT_B200_H
+
+#include <cuopt/linear_programming/cuopt_c.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Per-solve statistics, the counterpart of optimization_problem_solution_t::
+ * additional_termination_information_t (cpp/include/cuopt/linear_programming/pdlp/
+ * solver_solution.hpp:53-93) plus the fields this library adds (power iterations, restarts,
+ * refinement passes, device time of the iteration loop). */
+typedef struct {
+  cuopt_int_t number_of_steps_taken;
+  cuopt_int_t total_number_of_attempted_steps;
+  cuopt_float_t l2_primal_residual;
+  cuopt_float_t l2_relative_primal_residual;
+  cuopt_float_t l2_dual_residual;
+  cuopt_float_t l2_relative_dual_residual;
+  cuopt_float_t primal_objective;
+  cuopt_float_t dual_objective;
+  cuopt_float_t gap;
+  cuopt_float_t relative_gap;
+  cuopt_float_t solve_time;
+  cuopt_int_t solved_by_pdlp;
+  /* additions */
+  cuopt_int_t restarts;
+  cuopt_int_t power_iterations;
+  cuopt_int_t refinement_passes;
+  cuopt_float_t step_size;
+  cuopt_float_t primal_weight;
+  cuopt_float_t setup_time;     /* seconds spent before the first PDHG iteration */
+  cuopt_float_t loop_time;      /* seconds spent in the iteration loop */
+} cuOptPDLPStatistics;
+
+cuopt_int_t cuOptGetPDLPStatistics(cuOptSolution solution, cuOptPDLPStatistics* stats);
+
+/* Solve `count` independent LPs in one call.  The counterpart of the reference's
+ * cuopt::cython::call_batch_solve (cpp/src/pdlp/utilities/cython_solve.cu:317-352, used by the
+ * Python BatchSolve, python/cuopt/cuopt/linear_programming/solver/solver.py:109), which runs the
+ * problems on up to four host threads.  Here all instances advance in one persistent device
+ * launch with per-instance restart and termination.  solutions[i] receives the solution of
+ * problems[i]; each must be released with cuOptDestroySolution.  Returns CUOPT_SUCCESS when every
+ * instance ran (inspect each termination status), or the first error code. */
+cuopt_int_t cuOptBatchSolve(const cuOptOptimizationProblem* problems,
+                            cuopt_int_t count,
+                            cuOptSolverSettings settings,
+                            cuOptSolution* solutions);
+
+/* Reverse-mode sensitivity of an optimal LP solution (no counterpart in the reference).
+ * Given dL/dx (size n) and optionally dL/dy (size m, may be NULL) at the solution returned by
+ * cuOptSolve, computes dL/dc (n), dL/dlower and dL/dupper of the constraint bounds (m each) and
+ * dL/dA for every stored non-zero of the constraint matrix (nnz, CSR order of the problem), by
+ * implicit differentiation of the KKT conditions on the solution's active set.  Any output
+ * pointer may be NULL.  Returns CUOPT_INVALID_ARGUMENT if the solution is not Optimal. */
+cuopt_int_t cuOptSolutionAdjoint(cuOptOptimizationProblem problem,
+                                 cuOptSolution solution,
+                                 const cuopt_float_t* dl_dx,
+                                 const cuopt_float_t* dl_dy,
+                                 cuopt_float_t* dl_dc,
+                                 cuopt_float_t* dl_dlower,
+                                 cuopt_float_t* dl_dupper,
+                                 cuopt_float_t* dl_dvalues);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUOPT_B200_H */

@@ -1,0 +1,64 @@
+"""Regenerates the golden fixtures in this folder from the reference project (run where the
+reference tree is available; the fixtures are committed so tests never read the reference).
+
+Fixtures:
+  *.mps           copies of the reference's small LP datasets (datasets/linear_programming/)
+  golden.json     expected values taken from the reference's own tests, with their source lines.
+"""
+from __future__ import annotations
+
+import json
+import shutil
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+DATASETS = ["afiro_original.mps", "good-max.mps", "max_offset.mps", "lp-model-no-constraints.mps",
+            "empty_matrix.mps", "lp_model_with_var_bounds.mps", "good-mps-fixed-ranges.mps"]
+
+GOLDEN = {
+    "afiro_objective": {
+        "value": -464.7531, "rel_tol": 0.01,
+        "source": "python/cuopt/cuopt/tests/linear_programming/test_lp_solver.py:109; "
+                  "cpp/tests/linear_programming/pdlp_test.cu:48-74 (1% tolerance)"},
+    "afiro_methodical1_initial_step_size": {
+        "value": 1.4893, "abs_tol": 1e-4,
+        "source": "cpp/tests/linear_programming/pdlp_test.cu:243-286"},
+    "afiro_methodical1_initial_primal_weight": {
+        "value": 0.0141652, "abs_tol": 1e-4,
+        "source": "cpp/tests/linear_programming/pdlp_test.cu:243-286"},
+    "good_max_objective": {
+        "value": 17.0, "abs_tol": 1e-4,
+        "source": "cpp/tests/linear_programming/pdlp_test.cu:993-1011"},
+    "max_offset_objective": {
+        "value": 0.0, "abs_tol": 1e-4,
+        "source": "cpp/tests/linear_programming/pdlp_test.cu:1013-1031"},
+    "no_constraints_objective": {
+        "value": 1.0, "abs_tol": 1e-4,
+        "source": "cpp/tests/linear_programming/pdlp_test.cu:1033-1053 (method Concurrent)"},
+    "empty_matrix_pdlp_status": {
+        "value": 6, "source": "cpp/tests/linear_programming/pdlp_test.cu:952-968 (NumericalError)"},
+    "ranged_problem_objective": {
+        "value": 32.0, "abs_tol": 1e-3,
+        "source": "cpp/tests/linear_programming/c_api_tests/c_api_tests.cpp:105-112, "
+                  "c_api_test.c:927-1041"},
+    "maximize_dual_objective_match": {
+        "abs_tol": 1e-2,
+        "source": "cpp/tests/linear_programming/c_api_tests/c_api_tests.cpp:149-165, "
+                  "c_api_test.c:1461-1614"},
+    "chess_set_dual_simplex": {
+        "objective": 1333.333333, "x": [0.0, 66.666667], "tol": 1e-5,
+        "source": "cpp/tests/dual_simplex/unit_tests/solve.cpp:23-94"},
+}
+
+
+def main(ref_root: str = "/root/reference") -> None:
+    src = Path(ref_root) / "datasets" / "linear_programming"
+    for name in DATASETS:
+        shutil.copyfile(src / name, HERE / name)
+    (HERE / "golden.json").write_text(json.dumps(GOLDEN, indent=2) + "\n")
+    print("wrote", len(DATASETS), "datasets and golden.json to", HERE)
+
+
+if __name__ == "__main__":
+    main(*sys.argv[1:])
