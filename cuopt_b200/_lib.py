@@ -41,6 +41,7 @@ class PDLPStatistics(C.Structure):
         ("primal_weight", cuopt_float_t),
         ("setup_time", cuopt_float_t),
         ("loop_time", cuopt_float_t),
+        ("kernel_launches", cuopt_float_t),
     ]
 
 
@@ -109,6 +110,12 @@ SIGNATURES = {
     "cuOptGetDualObjectiveValue": (cuopt_int_t, [handle_t, _P_float]),
     "cuOptGetReducedCosts": (cuopt_int_t, [handle_t, C.c_void_p]),
     "cuOptGetPDLPStatistics": (cuopt_int_t, [handle_t, C.POINTER(PDLPStatistics)]),
+    "cuOptSolveDevice": (cuopt_int_t, [cuopt_int_t, cuopt_int_t, cuopt_int_t, cuopt_float_t] +
+                         [C.c_void_p] * 8 + [handle_t, C.c_void_p] + [C.c_void_p] * 3 +
+                         [C.POINTER(PDLPStatistics), C.POINTER(cuopt_int_t)]),
+    "cuOptProfilePDHGSweeps": (cuopt_int_t, [cuopt_int_t, cuopt_int_t] + [C.c_void_p] * 8 +
+                               [handle_t, C.c_void_p, cuopt_int_t] +
+                               [C.POINTER(C.c_double)] * 4),
     "cuOptBatchSolve": (cuopt_int_t, [C.POINTER(handle_t), cuopt_int_t, handle_t,
                                       C.POINTER(handle_t)]),
     "cuOptSolutionAdjoint": (cuopt_int_t, [handle_t, handle_t] + [C.c_void_p] * 6),

@@ -544,6 +544,89 @@ cuopt_int_t cuOptGetPDLPStatistics(cuOptSolution solution, cuOptPDLPStatistics* 
   st->primal_weight                   = r.primal_weight;
   st->setup_time                      = r.setup_time;
   st->loop_time                       = r.loop_time;
+  st->kernel_launches                 = r.kernel_launches;
+  return CUOPT_SUCCESS;
+}
+
+cuopt_int_t cuOptSolveDevice(cuopt_int_t m, cuopt_int_t n, cuopt_int_t sense, cuopt_float_t offset,
+                             const cuopt_float_t* d_c, const cuopt_int_t* d_off,
+                             const cuopt_int_t* d_idx, const cuopt_float_t* d_val,
+                             const cuopt_float_t* d_lo, const cuopt_float_t* d_up,
+                             const cuopt_float_t* d_vlo, const cuopt_float_t* d_vup,
+                             cuOptSolverSettings settings, void* stream, cuopt_float_t* d_x,
+                             cuopt_float_t* d_y, cuopt_float_t* d_rc, cuOptPDLPStatistics* stats,
+                             cuopt_int_t* termination_status)
+{
+  if (!settings || !d_c || !d_off || !d_lo || !d_up || !d_vlo || !d_vup || !d_x || !d_y || !d_rc)
+    return CUOPT_INVALID_ARGUMENT;
+  if (m <= 0 || n <= 0) return CUOPT_INVALID_ARGUMENT;
+  lp_solution sol;
+  try {
+    cuopt_b200::lp_device_input in;
+    in.m          = m;
+    in.n          = n;
+    in.row_off    = d_off;
+    in.col_idx    = d_idx;
+    in.val        = d_val;
+    in.c          = d_c;
+    in.con_lo     = d_lo;
+    in.con_up     = d_up;
+    in.var_lo     = d_vlo;
+    in.var_up     = d_vup;
+    in.obj_offset = offset;
+    in.maximize   = sense == CUOPT_MAXIMIZE;
+    cuopt_b200::pdlp_params prm = cuopt_b200::params_from_settings(*S(settings));
+    prm.log_to_console          = false;
+    sol.r = cuopt_b200::pdlp_solve_device(in, prm, static_cast<cudaStream_t>(stream), d_x, d_y, d_rc);
+  } catch (const std::bad_alloc&) {
+    return CUOPT_OUT_OF_MEMORY;
+  } catch (const std::invalid_argument&) {
+    return CUOPT_VALIDATION_ERROR;
+  } catch (const std::exception&) {
+    return CUOPT_RUNTIME_ERROR;
+  }
+  if (termination_status) *termination_status = sol.r.status;
+  if (stats) cuOptGetPDLPStatistics(&sol, stats);
+  return CUOPT_SUCCESS;
+}
+
+cuopt_int_t cuOptProfilePDHGSweeps(cuopt_int_t m, cuopt_int_t n, const cuopt_float_t* d_c,
+                                   const cuopt_int_t* d_off, const cuopt_int_t* d_idx,
+                                   const cuopt_float_t* d_val, const cuopt_float_t* d_lo,
+                                   const cuopt_float_t* d_up, const cuopt_float_t* d_vlo,
+                                   const cuopt_float_t* d_vup, cuOptSolverSettings settings,
+                                   void* stream, cuopt_int_t iterations, double* ms_primal,
+                                   double* ms_dual, double* bytes_primal, double* bytes_dual)
+{
+  if (!settings || !d_c || !d_off || !d_lo || !d_up || !d_vlo || !d_vup || m <= 0 || n <= 0 ||
+      iterations <= 0 || !ms_primal || !ms_dual || !bytes_primal || !bytes_dual)
+    return CUOPT_INVALID_ARGUMENT;
+  try {
+    cuopt_b200::lp_device_input in;
+    in.m       = m;
+    in.n       = n;
+    in.row_off = d_off;
+    in.col_idx = d_idx;
+    in.val     = d_val;
+    in.c       = d_c;
+    in.con_lo  = d_lo;
+    in.con_up  = d_up;
+    in.var_lo  = d_vlo;
+    in.var_up  = d_vup;
+    auto prm   = cuopt_b200::params_from_settings(*S(settings));
+    auto prof  = cuopt_b200::pdlp_profile_sweeps(in, prm, static_cast<cudaStream_t>(stream),
+                                                 iterations);
+    *ms_primal    = prof.ms_primal;
+    *ms_dual      = prof.ms_dual;
+    *bytes_primal = prof.bytes_primal;
+    *bytes_dual   = prof.bytes_dual;
+  } catch (const std::bad_alloc&) {
+    return CUOPT_OUT_OF_MEMORY;
+  } catch (const std::invalid_argument&) {
+    return CUOPT_VALIDATION_ERROR;
+  } catch (const std::exception&) {
+    return CUOPT_RUNTIME_ERROR;
+  }
   return CUOPT_SUCCESS;
 }
 

@@ -581,6 +581,21 @@ __global__ void rescale_vectors_kernel(const double* cs, const double* ls, const
   }
 }
 
+// Initial iterate in scaled space: v / d (d != 0) times factor, written to three buffers
+// (scale_solutions, initial_scaling.cu:571-640).
+template <typename TX>
+__global__ void scale_initial_kernel(const double* v, const double* d, double factor, int n, TX* a,
+                                     TX* b, TX* c)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double s = d[i] != 0.0 ? v[i] / d[i] : v[i];
+    const TX w     = (TX)(s * factor);
+    a[i]           = w;
+    b[i]           = w;
+    c[i]           = w;
+  }
+}
+
 // Elementwise helpers
 template <typename TX>
 __global__ void clamp_kernel(TX* x, const TX* l, const TX* u, int n)

@@ -349,6 +349,24 @@ lp_solution solve_without_constraints(const lp_problem& p)
 
 }  // namespace
 
+pdlp_params params_from_settings(const lp_settings& st)
+{
+  pdlp_params prm;
+  prm.abs_primal        = st.f(CUOPT_ABSOLUTE_PRIMAL_TOLERANCE);
+  prm.rel_primal        = st.f(CUOPT_RELATIVE_PRIMAL_TOLERANCE);
+  prm.abs_dual          = st.f(CUOPT_ABSOLUTE_DUAL_TOLERANCE);
+  prm.rel_dual          = st.f(CUOPT_RELATIVE_DUAL_TOLERANCE);
+  prm.abs_gap           = st.f(CUOPT_ABSOLUTE_GAP_TOLERANCE);
+  prm.rel_gap           = st.f(CUOPT_RELATIVE_GAP_TOLERANCE);
+  prm.iteration_limit   = st.i(CUOPT_ITERATION_LIMIT);
+  prm.time_limit        = st.f(CUOPT_TIME_LIMIT);
+  prm.precision         = st.i(CUOPT_PDLP_PRECISION);
+  prm.refinement_passes = st.i(CUOPT_PDLP_REFINEMENT_PASSES);
+  prm.refinement_tol    = st.f(CUOPT_PDLP_REFINEMENT_TOLERANCE);
+  prm.log_to_console    = st.b(CUOPT_LOG_TO_CONSOLE);
+  return prm;
+}
+
 lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
 {
   lp_solution out;
@@ -399,19 +417,7 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
       out.r.status = CUOPT_TERIMINATION_STATUS_NUMERICAL_ERROR;
       return out;
     }
-    pdlp_params prm;
-    prm.abs_primal      = st.f(CUOPT_ABSOLUTE_PRIMAL_TOLERANCE);
-    prm.rel_primal      = st.f(CUOPT_RELATIVE_PRIMAL_TOLERANCE);
-    prm.abs_dual        = st.f(CUOPT_ABSOLUTE_DUAL_TOLERANCE);
-    prm.rel_dual        = st.f(CUOPT_RELATIVE_DUAL_TOLERANCE);
-    prm.abs_gap         = st.f(CUOPT_ABSOLUTE_GAP_TOLERANCE);
-    prm.rel_gap         = st.f(CUOPT_RELATIVE_GAP_TOLERANCE);
-    prm.iteration_limit = st.i(CUOPT_ITERATION_LIMIT);
-    prm.time_limit      = st.f(CUOPT_TIME_LIMIT);
-    prm.precision       = st.i(CUOPT_PDLP_PRECISION);
-    prm.refinement_passes = st.i(CUOPT_PDLP_REFINEMENT_PASSES);
-    prm.refinement_tol    = st.f(CUOPT_PDLP_REFINEMENT_TOLERANCE);
-    prm.log_to_console    = st.b(CUOPT_LOG_TO_CONSOLE);
+    pdlp_params prm = params_from_settings(st);
     if ((int)st.initial_primal.size() == p.n) prm.initial_primal = st.initial_primal;
     if ((int)st.initial_dual.size() == p.m) prm.initial_dual = st.initial_dual;
     lp_input in;

@@ -75,6 +75,9 @@ struct lp_solution {
 // Returns an empty string when valid, otherwise the reason.
 std::string validate_problem(const lp_problem& p);
 
+// Solver parameters from the settings registry.
+pdlp_params params_from_settings(const lp_settings& s);
+
 // Full solve as done by cuOptSolve: validation, trivial cases, PDLP.
 lp_solution solve_problem(const lp_problem& p, const lp_settings& s);
 

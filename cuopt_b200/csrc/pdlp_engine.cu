@@ -5,8 +5,8 @@
 // the host (restart decision, PID primal weight, fixed-point errors); all vector and matrix work
 // is in the kernels of kernels.cuh.  Iterations that need neither a termination test, a "major"
 // step nor a fixed-point error are replayed from cached CUDA graphs of 2^k iterations.
+#include "device_layout.cuh"
 #include "kernels.cuh"
-#include "layout.hpp"
 #include "pdlp_engine.hpp"
 
 #include <algorithm>
@@ -56,34 +56,13 @@ double now_s()
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-struct dev_matrix {
-  int rows = 0, cols = 0, n_long = 0, n_slices = 0;
-  dbuf<int64_t> long_off, slice_off;
-  dbuf<int> idx;
-  dbuf<double> val;  // unscaled FP64
-  void upload(const sell_host& h, cudaStream_t s)
-  {
-    rows     = h.rows;
-    cols     = h.cols;
-    n_long   = h.n_long;
-    n_slices = h.n_slices;
-    long_off.resize(h.long_off.size());
-    long_off.upload(h.long_off.data(), h.long_off.size(), s);
-    slice_off.resize(h.slice_off.size());
-    slice_off.upload(h.slice_off.data(), h.slice_off.size(), s);
-    idx.resize(h.idx.size());
-    idx.upload(h.idx.data(), h.idx.size(), s);
-    val.resize(h.val.size());
-    val.upload(h.val.data(), h.val.size(), s);
-  }
-  template <typename T>
-  dev_sell<T> view(const T* v) const
-  {
-    return dev_sell<T>{rows, n_long, n_slices, long_off.data(), slice_off.data(), idx.data(), v};
-  }
-  dev_sell<double> view64() const { return view<double>(val.data()); }
-  int64_t stored() const { return (int64_t)idx.size(); }
-};
+template <typename T>
+dev_sell<T> view_of(const dev_matrix& M, const T* v)
+{
+  return dev_sell<T>{M.rows, M.n_long, M.n_slices, M.long_off.data(), M.slice_off.data(),
+                     M.idx.data(), v};
+}
+inline dev_sell<double> view64(const dev_matrix& M) { return view_of<double>(M, M.val.data()); }
 
 struct conv_info {
   double l2_primal, l2_dual, primal_obj, dual_obj, gap, abs_obj;
@@ -92,9 +71,8 @@ struct conv_info {
 template <typename TX>
 class engine {
  public:
-  engine(const lp_input& in, const pdlp_params& p) : in_(in), p_(p)
+  engine(const lp_device_input& in, const pdlp_params& p, cudaStream_t s) : in_(in), p_(p), s_(s)
   {
-    B200_CUDA_CHECK(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
     int dev = 0;
     B200_CUDA_CHECK(cudaGetDevice(&dev));
     B200_CUDA_CHECK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
@@ -104,11 +82,13 @@ class engine {
   {
     for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
     if (hres_) cudaFreeHost(hres_);
-    if (s_) cudaStreamDestroy(s_);
   }
 
-  pdlp_result run()
+  pdlp_result run(double* x_out, double* y_out, double* rc_out)
   {
+    x_out_   = x_out;
+    y_out_   = y_out;
+    rc_out_  = rc_out;
     t_start_ = now_s();
     pdlp_result r;
     setup();
@@ -129,41 +109,27 @@ class engine {
   void setup()
   {
     const int m = in_.m, n = in_.n;
-    L_ = build_layout(m, n, in_.row_off, in_.col_idx, in_.val);
-    A_.upload(L_.a, s_);
-    AT_.upload(L_.at, s_);
+    build_device_layout(m, n, in_.row_off, in_.col_idx, in_.val, s_, L_);
     vgrid_ = sms_ * 4;
-    const int g = std::max({sell_grid(A_.view64()), sell_grid(AT_.view64()), vgrid_});
+    const int g = std::max({sell_grid(view64(L_.A)), sell_grid(view64(L_.AT)), vgrid_});
     partials_.resize((size_t)g * 4);
     dres_.resize(64);
 
     // Unscaled vectors in internal order; objective negated for maximisation
     // (reference problem_helpers.cuh:132-151).
-    std::vector<double> c(n), l(n), u(n), lc(m), uc(m);
     const double sgn = in_.maximize ? -1.0 : 1.0;
-    for (int j = 0; j < n; ++j) {
-      const int o = L_.col_new2old[j];
-      c[j]        = sgn * in_.c[o];
-      l[j]        = in_.var_lo[o];
-      u[j]        = in_.var_up[o];
-    }
-    for (int i = 0; i < m; ++i) {
-      const int o = L_.row_new2old[i];
-      lc[i]       = in_.con_lo[o];
-      uc[i]       = in_.con_up[o];
-    }
-    obj_scale_  = in_.maximize ? -1.0 : 1.0;
-    obj_offset_ = in_.maximize ? -in_.obj_offset : in_.obj_offset;
+    obj_scale_       = in_.maximize ? -1.0 : 1.0;
+    obj_offset_      = in_.maximize ? -in_.obj_offset : in_.obj_offset;
     c64_.resize(n);
-    c64_.upload(c.data(), n, s_);
     l64_.resize(n);
-    l64_.upload(l.data(), n, s_);
     u64_.resize(n);
-    u64_.upload(u.data(), n, s_);
     lc64_.resize(m);
-    lc64_.upload(lc.data(), m, s_);
     uc64_.resize(m);
-    uc64_.upload(uc.data(), m, s_);
+    permute_gather(in_.c, L_.col_new2old.data(), n, sgn, c64_.data(), s_);
+    permute_gather(in_.var_lo, L_.col_new2old.data(), n, 1.0, l64_.data(), s_);
+    permute_gather(in_.var_up, L_.col_new2old.data(), n, 1.0, u64_.data(), s_);
+    permute_gather(in_.con_lo, L_.row_new2old.data(), m, 1.0, lc64_.data(), s_);
+    permute_gather(in_.con_up, L_.row_new2old.data(), m, 1.0, uc64_.data(), s_);
 
     // Constant norms of the unscaled problem (reference convergence_information.cu:92-106).
     c_norm_ = std::sqrt(reduce<0>(c64_.data(), (const double*)nullptr, n));
@@ -176,28 +142,28 @@ class engine {
     fill(dc_.data(), n, 1.0);
     dbuf<double> rtmp(m), ctmp(n);
     for (int it = 0; it < kRuizIterations; ++it) {
-      row_scaled_abs_kernel<0, false><<<sell_grid(A_.view64()), kBlock, 0, s_>>>(
-        A_.view64(), dr_.data(), dc_.data(), 0.0, rtmp.data());
-      row_scaled_abs_kernel<0, true><<<sell_grid(AT_.view64()), kBlock, 0, s_>>>(
-        AT_.view64(), dr_.data(), dc_.data(), 0.0, ctmp.data());
+      row_scaled_abs_kernel<0, false><<<sell_grid(view64(L_.A)), kBlock, 0, s_>>>(
+        view64(L_.A), dr_.data(), dc_.data(), 0.0, rtmp.data());
+      row_scaled_abs_kernel<0, true><<<sell_grid(view64(L_.AT)), kBlock, 0, s_>>>(
+        view64(L_.AT), dr_.data(), dc_.data(), 0.0, ctmp.data());
       apply_root_scaling_kernel<<<vgrid_, kBlock, 0, s_>>>(dr_.data(), rtmp.data(), m);
       apply_root_scaling_kernel<<<vgrid_, kBlock, 0, s_>>>(dc_.data(), ctmp.data(), n);
     }
-    row_scaled_abs_kernel<1, false><<<sell_grid(A_.view64()), kBlock, 0, s_>>>(
-      A_.view64(), dr_.data(), dc_.data(), kPcAlpha, rtmp.data());
-    row_scaled_abs_kernel<1, true><<<sell_grid(AT_.view64()), kBlock, 0, s_>>>(
-      AT_.view64(), dr_.data(), dc_.data(), 2.0 - kPcAlpha, ctmp.data());
+    row_scaled_abs_kernel<1, false><<<sell_grid(view64(L_.A)), kBlock, 0, s_>>>(
+      view64(L_.A), dr_.data(), dc_.data(), kPcAlpha, rtmp.data());
+    row_scaled_abs_kernel<1, true><<<sell_grid(view64(L_.AT)), kBlock, 0, s_>>>(
+      view64(L_.AT), dr_.data(), dc_.data(), 2.0 - kPcAlpha, ctmp.data());
     apply_root_scaling_kernel<<<vgrid_, kBlock, 0, s_>>>(dr_.data(), rtmp.data(), m);
     apply_root_scaling_kernel<<<vgrid_, kBlock, 0, s_>>>(dc_.data(), ctmp.data(), n);
     B200_LAUNCH_CHECK();
 
     // Scaled matrix values in the iterate precision.
-    As_.resize(A_.stored());
-    ATs_.resize(AT_.stored());
-    scale_values_kernel<TX, false><<<sell_grid(A_.view64()), kBlock, 0, s_>>>(
-      A_.view64(), dr_.data(), dc_.data(), As_.data());
-    scale_values_kernel<TX, true><<<sell_grid(AT_.view64()), kBlock, 0, s_>>>(
-      AT_.view64(), dr_.data(), dc_.data(), ATs_.data());
+    As_.resize(L_.A.stored());
+    ATs_.resize(L_.AT.stored());
+    scale_values_kernel<TX, false><<<sell_grid(view64(L_.A)), kBlock, 0, s_>>>(
+      view64(L_.A), dr_.data(), dc_.data(), As_.data());
+    scale_values_kernel<TX, true><<<sell_grid(view64(L_.AT)), kBlock, 0, s_>>>(
+      view64(L_.AT), dr_.data(), dc_.data(), ATs_.data());
 
     // Scaled vectors, then bound / objective rescaling (reference initial_scaling.cu:95-149, 417-569).
     dbuf<double> cs(n), ls(n), us(n), lcs(m), ucs(m);
@@ -234,7 +200,7 @@ class engine {
     xu_.resize(n);
     su_.resize(n);
     yu_.resize(m);
-    if (!p_.initial_primal.empty() || !p_.initial_dual.empty()) load_initial_solution();
+    if (in_.initial_primal || in_.initial_dual) load_initial_solution();
     // project_initial_primal (reference pdlp.cu:2237-2262): only the current primal iterate.
     clamp_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(x_.data(), ls_.data(), us_.data(), n);
     scalars_.resize(1);
@@ -247,30 +213,21 @@ class engine {
   void load_initial_solution()
   {
     const int m = in_.m, n = in_.n;
-    std::vector<double> dr(m), dc(n);
-    dr_.download(dr.data(), m, s_);
-    dc_.download(dc.data(), n, s_);
-    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
-    if (!p_.initial_primal.empty()) {
-      std::vector<TX> x(n);
-      for (int j = 0; j < n; ++j) {
-        double v = p_.initial_primal[L_.col_new2old[j]];
-        v        = dc[j] != 0.0 ? v / dc[j] : v;
-        x[j]     = (TX)(v * beta_);
-      }
-      for (auto* b : {&x_, &xhat_, &xa_}) b->upload(x.data(), n, s_);
+    if (in_.initial_primal) {
+      dbuf<double> v(n);
+      permute_gather(in_.initial_primal, L_.col_new2old.data(), n, 1.0, v.data(), s_);
+      scale_initial_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(v.data(), dc_.data(), beta_, n,
+                                                          x_.data(), xhat_.data(), xa_.data());
+      B200_CUDA_CHECK(cudaStreamSynchronize(s_));
     }
-    if (!p_.initial_dual.empty()) {
-      std::vector<TX> y(m);
-      for (int i = 0; i < m; ++i) {
-        double v = p_.initial_dual[L_.row_new2old[i]];
-        if (in_.maximize) v = -v;
-        v    = dr[i] != 0.0 ? v / dr[i] : v;
-        y[i] = (TX)(v * gamma_);
-      }
-      for (auto* b : {&y_, &yhat_, &ya_}) b->upload(y.data(), m, s_);
+    if (in_.initial_dual) {
+      dbuf<double> v(m);
+      permute_gather(in_.initial_dual, L_.row_new2old.data(), m, 1.0, v.data(), s_);
+      scale_initial_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(v.data(), dr_.data(), gamma_, m,
+                                                          y_.data(), yhat_.data(), ya_.data());
+      B200_CUDA_CHECK(cudaStreamSynchronize(s_));
     }
-    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    B200_LAUNCH_CHECK();
   }
 
   void fill(double* p, int n, double v)
@@ -286,6 +243,7 @@ class engine {
   {
     vec_reduce_kernel<MODE, TA><<<vgrid_, kBlock, 0, s_>>>(a, b, n, partials_.data(), nullptr);
     finalize_sum_kernel<1><<<1, kBlock, 0, s_>>>(partials_.data(), vgrid_, dres_.data());
+    launches_ += 2;
     B200_LAUNCH_CHECK();
     B200_CUDA_CHECK(cudaMemcpyAsync(hres_, dres_.data(), sizeof(double), cudaMemcpyDeviceToHost, s_));
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
@@ -296,18 +254,19 @@ class engine {
   {
     const int m = in_.m, n = in_.n;
     // Start vector: std::mt19937(1) normals in the user's constraint order (pdlp.cu:2632-2638).
-    std::vector<double> z0(m), z(m);
+    std::vector<double> z0(m);
     std::mt19937 gen(1);
     std::normal_distribution<double> dist(0.0, 1.0);
     for (int i = 0; i < m; ++i) z0[i] = dist(gen);
-    for (int i = 0; i < m; ++i) z[i] = z0[L_.row_new2old[i]];
     dbuf<double> dz(m), dq(m), datq(n);
     dbuf<power_state> ps(1);
     ps.zero(s_);
-    dz.upload(z.data(), m, s_);
+    dq.upload(z0.data(), m, s_);
+    permute_gather(dq.data(), L_.row_new2old.data(), m, 1.0, dz.data(), s_);
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
     dbuf<TX> q_tx, atq_tx;
-    const auto As  = A_.view<TX>(As_.data());
-    const auto ATs = AT_.view<TX>(ATs_.data());
+    const auto As  = view_of<TX>(L_.A, As_.data());
+    const auto ATs = view_of<TX>(L_.AT, ATs_.data());
     const int ga = sell_grid(As), gt = sell_grid(ATs);
     double* res = dres_.data();
     auto one_iteration = [&]() {
@@ -340,6 +299,7 @@ class engine {
       } else {
         B200_CUDA_CHECK(cudaGraphLaunch(exec, s_));
       }
+      launches_ += 9.0 * std::min(32, kPowerMaxIters - done_iters);
       B200_CUDA_CHECK(cudaMemcpyAsync(&h, ps.data(), sizeof(h), cudaMemcpyDeviceToHost, s_));
       B200_CUDA_CHECK(cudaStreamSynchronize(s_));
       if (h.done) break;
@@ -350,8 +310,8 @@ class engine {
   }
 
   // ------------------------------------------------------------------ iteration kernels
-  dev_sell<TX> As_view() const { return A_.view<TX>(As_.data()); }
-  dev_sell<TX> ATs_view() const { return AT_.view<TX>(ATs_.data()); }
+  dev_sell<TX> As_view() const { return view_of<TX>(L_.A, As_.data()); }
+  dev_sell<TX> ATs_view() const { return view_of<TX>(L_.AT, ATs_.data()); }
 
   template <bool MAJOR, bool HALPERN, bool SAVE_ATY>
   void launch_primal(int it_off)
@@ -363,6 +323,7 @@ class engine {
                                                aty_.data(),  scalars_.data(), it_off};
     sell_map_kernel<TX, TX, decltype(e)><<<sell_grid(A), kBlock, 0, s_>>>(A, y_.data(), e,
                                                                          partials_.data());
+    ++launches_;
   }
   template <bool MAJOR, bool HALPERN, bool FPE>
   void launch_dual(int it_off)
@@ -373,6 +334,7 @@ class engine {
                                         it_off};
     sell_map_kernel<TX, TX, decltype(e)><<<sell_grid(A), kBlock, 0, s_>>>(A, xbar_.data(), e,
                                                                          partials_.data());
+    ++launches_;
   }
 
   void plain_iterations(int L)  // L fused iterations, then t0 += L
@@ -382,6 +344,7 @@ class engine {
       launch_dual<false, true, false>(i);
     }
     advance_kernel<<<1, 1, 0, s_>>>(scalars_.data(), L);
+    ++launches_;
   }
 
   void run_plain(long R)
@@ -393,13 +356,16 @@ class engine {
           cudaGraph_t g;
           cudaGraphExec_t e;
           B200_CUDA_CHECK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+          const double before = launches_;
           plain_iterations(L);
+          launches_ = before;  // captured, not launched
           B200_CUDA_CHECK(cudaStreamEndCapture(s_, &g));
           B200_CUDA_CHECK(cudaGraphInstantiate(&e, g, 0));
           cudaGraphDestroy(g);
           it = graphs_.emplace(L, e).first;
         }
         B200_CUDA_CHECK(cudaGraphLaunch(it->second, s_));
+        launches_ += 2.0 * L + 1.0;
         R -= L;
       }
     }
@@ -409,6 +375,7 @@ class engine {
   {
     set_scalars_kernel<<<1, 1, 0, s_>>>(scalars_.data(), eta_ / omega_, eta_ * omega_, eta_,
                                         omega_, t0);
+    ++launches_;
     B200_LAUNCH_CHECK();
   }
 
@@ -420,7 +387,7 @@ class engine {
                                                   dc_.data(), dr_.data(), 1.0 / beta_,
                                                   1.0 / gamma_, n, m, xu_.data(), yu_.data(),
                                                   su_.data());
-    const auto A = A_.view64(), AT = AT_.view64();
+    const auto A = view64(L_.A), AT = view64(L_.AT);
     sell_map_kernel<double, double, term_primal_epi><<<sell_grid(A), kBlock, 0, s_>>>(
       A, xu_.data(), term_primal_epi{lc64_.data(), uc64_.data(), yu_.data()}, partials_.data());
     finalize_sum_kernel<2><<<1, kBlock, 0, s_>>>(partials_.data(), sell_grid(A), dres_.data());
@@ -428,6 +395,7 @@ class engine {
       AT, yu_.data(), term_dual_epi{c64_.data(), xu_.data(), su_.data()}, partials_.data());
     finalize_sum_kernel<3><<<1, kBlock, 0, s_>>>(partials_.data(), sell_grid(AT),
                                                  dres_.data() + 2);
+    launches_ += 5;
     B200_LAUNCH_CHECK();
     B200_CUDA_CHECK(
       cudaMemcpyAsync(hres_, dres_.data(), 5 * sizeof(double), cudaMemcpyDeviceToHost, s_));
@@ -462,20 +430,12 @@ class engine {
     r.step_size  = eta_;
     r.primal_weight = omega_;
     r.restarts   = restarts_;
-    std::vector<double> x(n), y(m), s(n);
-    xu_.download(x.data(), n, s_);
-    yu_.download(y.data(), m, s_);
-    su_.download(s.data(), n, s_);
-    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
-    r.x.resize(n);
-    r.rc.resize(n);
-    r.y.resize(m);
+    r.kernel_launches = launches_;
     const double sgn = in_.maximize ? -1.0 : 1.0;  // reference solve.cu:584-588
-    for (int j = 0; j < n; ++j) {
-      r.x[L_.col_new2old[j]]  = x[j];
-      r.rc[L_.col_new2old[j]] = sgn * s[j];
-    }
-    for (int i = 0; i < m; ++i) r.y[L_.row_new2old[i]] = sgn * y[i];
+    if (x_out_) permute_scatter(xu_.data(), L_.col_new2old.data(), n, 1.0, x_out_, s_);
+    if (rc_out_) permute_scatter(su_.data(), L_.col_new2old.data(), n, sgn, rc_out_, s_);
+    if (y_out_) permute_scatter(yu_.data(), L_.row_new2old.data(), m, sgn, y_out_, s_);
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
     finish_times(r);
   }
 
@@ -612,6 +572,7 @@ class engine {
                                                       y_.data(), ybar_.data(), ya_.data(), m,
                                                       scalars_.data());
         advance_kernel<<<1, 1, 0, s_>>>(scalars_.data(), 1);
+        launches_ += 5;
         B200_LAUNCH_CHECK();
         B200_CUDA_CHECK(cudaMemcpyAsync(hres_ + 8, dres_.data() + 8, 3 * sizeof(double),
                                         cudaMemcpyDeviceToHost, s_));
@@ -624,6 +585,7 @@ class engine {
         launch_primal<true, true, false>(0);
         launch_dual<true, true, false>(0);
         advance_kernel<<<1, 1, 0, s_>>>(scalars_.data(), 1);
+        ++launches_;
         B200_LAUNCH_CHECK();
       }
       ++k;
@@ -632,15 +594,15 @@ class engine {
   }
 
   // ------------------------------------------------------------------ state
-  const lp_input& in_;
+  const lp_device_input& in_;
   const pdlp_params& p_;
   cudaStream_t s_ = nullptr;
+  double *x_out_ = nullptr, *y_out_ = nullptr, *rc_out_ = nullptr;
   int sms_ = 148, vgrid_ = 592;
   double* hres_ = nullptr;
   double t_start_ = 0, t_loop_ = 0;
 
-  lp_layout L_;
-  dev_matrix A_, AT_;
+  device_layout L_;
   dbuf<TX> As_, ATs_;
   dbuf<double> c64_, l64_, u64_, lc64_, uc64_, dr_, dc_;
   dbuf<TX> cs_, ls_, us_, lcs_, ucs_;
@@ -654,18 +616,131 @@ class engine {
   double c_norm_ = 0, b_norm_ = 0, beta_ = 1, gamma_ = 1;
   double eta_ = 0, omega_ = 1, best_omega_ = 1;
   int power_iters_ = 0, restarts_ = 0;
+  double launches_ = 0;
+
+ public:
+  // Times plain iterations sweep by sweep (measurement hook).
+  sweep_profile profile(int iterations)
+  {
+    t_start_ = now_s();
+    setup();
+    set_scalars(0);
+    const int m = in_.m, n = in_.n;
+    const auto A = As_view(), AT = ATs_view();
+    std::vector<cudaEvent_t> ev(3 * iterations);
+    for (auto& e : ev) B200_CUDA_CHECK(cudaEventCreate(&e));
+    for (int i = 0; i < 3; ++i) plain_iterations(1);  // warm-up
+    for (int i = 0; i < iterations; ++i) {
+      B200_CUDA_CHECK(cudaEventRecord(ev[3 * i], s_));
+      launch_primal<false, true, false>(0);
+      B200_CUDA_CHECK(cudaEventRecord(ev[3 * i + 1], s_));
+      launch_dual<false, true, false>(0);
+      B200_CUDA_CHECK(cudaEventRecord(ev[3 * i + 2], s_));
+      advance_kernel<<<1, 1, 0, s_>>>(scalars_.data(), 1);
+    }
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    sweep_profile p;
+    for (int i = 0; i < iterations; ++i) {
+      float a = 0, b = 0;
+      B200_CUDA_CHECK(cudaEventElapsedTime(&a, ev[3 * i], ev[3 * i + 1]));
+      B200_CUDA_CHECK(cudaEventElapsedTime(&b, ev[3 * i + 1], ev[3 * i + 2]));
+      p.ms_primal += a;
+      p.ms_dual += b;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    p.ms_primal /= iterations;
+    p.ms_dual /= iterations;
+    // Algorithmic bytes (CSR accounting): matrix values + indices, row offsets, one gather pass,
+    // epilogue vectors (primal: read x c l u x_anchor, write x_bar x; dual: read y lc uc y_anchor,
+    // write y).
+    const double nnz = (double)L_.nnz, sv = sizeof(TX), sf = sizeof(TX);
+    p.bytes_primal = nnz * (sv + 4) + (n + 1) * 4.0 + m * sf + 7.0 * n * sf;
+    p.bytes_dual   = nnz * (sv + 4) + (m + 1) * 4.0 + n * sf + 5.0 * m * sf;
+    (void)A;
+    (void)AT;
+    return p;
+  }
 };
 
 }  // namespace
 
-pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p)
+pdlp_result pdlp_solve_device(const lp_device_input& in, const pdlp_params& p, cudaStream_t stream,
+                              double* x_out, double* y_out, double* rc_out)
 {
   if (p.precision == 1) {
-    engine<float> e(in, p);
-    return e.run();
+    engine<float> e(in, p, stream);
+    return e.run(x_out, y_out, rc_out);
   }
-  engine<double> e(in, p);
-  return e.run();
+  engine<double> e(in, p, stream);
+  return e.run(x_out, y_out, rc_out);
+}
+
+sweep_profile pdlp_profile_sweeps(const lp_device_input& in, const pdlp_params& p,
+                                  cudaStream_t stream, int iterations)
+{
+  if (p.precision == 1) {
+    engine<float> e(in, p, stream);
+    return e.profile(iterations);
+  }
+  engine<double> e(in, p, stream);
+  return e.profile(iterations);
+}
+
+pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p)
+{
+  cudaStream_t s;
+  B200_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct stream_guard {
+    cudaStream_t s;
+    ~stream_guard() { cudaStreamDestroy(s); }
+  } guard{s};
+  const int m = in.m, n = in.n;
+  const int64_t nnz = in.row_off[m];
+  dbuf<int> off(m + 1), idx(std::max<int64_t>(nnz, 1));
+  dbuf<double> val(std::max<int64_t>(nnz, 1)), c(n), lo(m), up(m), vl(n), vu(n), x(n), y(m), rc(n),
+    ip, id;
+  off.upload(in.row_off, m + 1, s);
+  idx.upload(in.col_idx, nnz, s);
+  val.upload(in.val, nnz, s);
+  c.upload(in.c, n, s);
+  lo.upload(in.con_lo, m, s);
+  up.upload(in.con_up, m, s);
+  vl.upload(in.var_lo, n, s);
+  vu.upload(in.var_up, n, s);
+  lp_device_input d;
+  d.m = m;
+  d.n = n;
+  d.row_off = off.data();
+  d.col_idx = idx.data();
+  d.val     = val.data();
+  d.c       = c.data();
+  d.con_lo  = lo.data();
+  d.con_up  = up.data();
+  d.var_lo  = vl.data();
+  d.var_up  = vu.data();
+  d.obj_offset = in.obj_offset;
+  d.maximize   = in.maximize;
+  if ((int)p.initial_primal.size() == n) {
+    ip.resize(n);
+    ip.upload(p.initial_primal.data(), n, s);
+    d.initial_primal = ip.data();
+  }
+  if ((int)p.initial_dual.size() == m) {
+    id.resize(m);
+    id.upload(p.initial_dual.data(), m, s);
+    d.initial_dual = id.data();
+  }
+  pdlp_result r = pdlp_solve_device(d, p, s, x.data(), y.data(), rc.data());
+  if (r.status != kNumericalError || r.iterations > 0) {
+    r.x.resize(n);
+    r.y.resize(m);
+    r.rc.resize(n);
+    x.download(r.x.data(), n, s);
+    y.download(r.y.data(), m, s);
+    rc.download(r.rc.data(), n, s);
+    B200_CUDA_CHECK(cudaStreamSynchronize(s));
+  }
+  return r;
 }
 
 }  // namespace cuopt_b200

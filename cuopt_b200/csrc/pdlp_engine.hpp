@@ -4,6 +4,8 @@
 // (cpp/src/pdlp/solve.cu:556-590, 1124-1342; cpp/src/pdlp/pdlp.cu:2013-2457).
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -49,9 +51,41 @@ struct pdlp_result {
   double solve_time = 0, setup_time = 0, loop_time = 0;
   double step_size = 0, primal_weight = 0;
   int restarts = 0, power_iterations = 0, refinement_passes = 0;
+  double kernel_launches = 0;
 };
 
-// Runs PDLP (Stable3) on the GPU.  Throws std::exception subclasses on CUDA or input errors.
+struct sweep_profile {
+  double ms_primal = 0, ms_dual = 0, bytes_primal = 0, bytes_dual = 0;
+};
+
+// The same LP with every array in device memory (user order).
+struct lp_device_input {
+  int m = 0, n = 0;
+  const int* row_off   = nullptr;
+  const int* col_idx   = nullptr;
+  const double* val    = nullptr;
+  const double* c      = nullptr;
+  const double* con_lo = nullptr;
+  const double* con_up = nullptr;
+  const double* var_lo = nullptr;
+  const double* var_up = nullptr;
+  double obj_offset    = 0.0;
+  bool maximize        = false;
+  const double* initial_primal = nullptr;  // optional, n (user order)
+  const double* initial_dual   = nullptr;  // optional, m
+};
+
+// Runs PDLP (Stable3) on the GPU from host arrays (uploads them, returns x / y / rc on the host).
+// Throws std::exception subclasses on CUDA or input errors.
 pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p);
+
+// Runs PDLP on device-resident arrays.  x_out (n), y_out (m), rc_out (n) are device arrays in the
+// user's order; the returned result carries statistics only (its x / y / rc stay empty).
+pdlp_result pdlp_solve_device(const lp_device_input& in, const pdlp_params& p, cudaStream_t stream,
+                              double* x_out, double* y_out, double* rc_out);
+
+// Times `iterations` plain iterations sweep by sweep (see cuOptProfilePDHGSweeps).
+sweep_profile pdlp_profile_sweeps(const lp_device_input& in, const pdlp_params& p,
+                                  cudaStream_t stream, int iterations);
 
 }  // namespace cuopt_b200

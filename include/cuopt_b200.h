@@ -38,9 +38,63 @@ typedef struct {
   cuopt_float_t primal_weight;
   cuopt_float_t setup_time;     /* seconds spent before the first PDHG iteration */
   cuopt_float_t loop_time;      /* seconds spent in the iteration loop */
+  cuopt_float_t kernel_launches; /* kernels this library launched for the solve */
 } cuOptPDLPStatistics;
 
 cuopt_int_t cuOptGetPDLPStatistics(cuOptSolution solution, cuOptPDLPStatistics* stats);
+
+/* Solve an LP whose arrays all live in device memory, writing the solution to device memory.
+ * Counterpart of the reference's C++ entry solve_lp(optimization_problem_t&, settings)
+ * (cpp/include/cuopt/linear_programming/solve.hpp:42-47), whose problem setters accept device
+ * pointers; the reference C API has no device-resident variant.  Inputs are in the user's order
+ * (CSR rows = constraints); `stream` is a cudaStream_t (NULL: the legacy default stream).  The
+ * arrays are read, never modified or kept.  d_primal (n), d_dual (m), d_reduced_cost (n) receive the
+ * solution; `stats` and `termination_status` may be NULL.  Returns CUOPT_SUCCESS or an error code
+ * (CUOPT_VALIDATION_ERROR for inconsistent sizes or column indices out of range). */
+cuopt_int_t cuOptSolveDevice(cuopt_int_t num_constraints,
+                             cuopt_int_t num_variables,
+                             cuopt_int_t objective_sense,
+                             cuopt_float_t objective_offset,
+                             const cuopt_float_t* d_objective_coefficients,
+                             const cuopt_int_t* d_row_offsets,
+                             const cuopt_int_t* d_column_indices,
+                             const cuopt_float_t* d_values,
+                             const cuopt_float_t* d_constraint_lower_bounds,
+                             const cuopt_float_t* d_constraint_upper_bounds,
+                             const cuopt_float_t* d_variable_lower_bounds,
+                             const cuopt_float_t* d_variable_upper_bounds,
+                             cuOptSolverSettings settings,
+                             void* stream,
+                             cuopt_float_t* d_primal,
+                             cuopt_float_t* d_dual,
+                             cuopt_float_t* d_reduced_cost,
+                             cuOptPDLPStatistics* stats,
+                             cuopt_int_t* termination_status);
+
+/* Measurement hook (no counterpart in the reference): prepares the device-resident LP exactly as
+ * cuOptSolveDevice does, then runs `iterations` plain PDHG iterations launching the two fused
+ * sweeps separately between CUDA events on `stream`.  Returns the mean device time of one primal
+ * sweep (A^T y fused with the primal projection / reflection / Halpern step) and of one dual sweep
+ * (A x_bar fused with the dual step), in milliseconds, and the algorithmic bytes each sweep must
+ * move (matrix values and indices, row offsets, one gather pass, the epilogue's vector reads and
+ * writes). */
+cuopt_int_t cuOptProfilePDHGSweeps(cuopt_int_t num_constraints,
+                                   cuopt_int_t num_variables,
+                                   const cuopt_float_t* d_objective_coefficients,
+                                   const cuopt_int_t* d_row_offsets,
+                                   const cuopt_int_t* d_column_indices,
+                                   const cuopt_float_t* d_values,
+                                   const cuopt_float_t* d_constraint_lower_bounds,
+                                   const cuopt_float_t* d_constraint_upper_bounds,
+                                   const cuopt_float_t* d_variable_lower_bounds,
+                                   const cuopt_float_t* d_variable_upper_bounds,
+                                   cuOptSolverSettings settings,
+                                   void* stream,
+                                   cuopt_int_t iterations,
+                                   double* ms_primal_sweep,
+                                   double* ms_dual_sweep,
+                                   double* bytes_primal_sweep,
+                                   double* bytes_dual_sweep);
 
 /* Solve `count` independent LPs in one call.  The counterpart of the reference's
  * cuopt::cython::call_batch_solve (cpp/src/pdlp/utilities/cython_solve.cu:317-352, used by the

@@ -1,0 +1,58 @@
+"""Shared helpers for the tests: LP <-> DataModel conversion and the oracle adapter."""
+from __future__ import annotations
+
+from types import SimpleNamespace
+
+import numpy as np
+
+from cuopt_b200 import linear_programming as lpm
+
+
+def datamodel_from_lp(lp, maximize=False, offset=0.0) -> lpm.DataModel:
+    dm = lpm.DataModel()
+    dm.set_maximize(maximize)
+    dm.set_objective_offset(offset)
+    dm.set_csr_constraint_matrix(lp.val, lp.col_idx, lp.row_off)
+    dm.set_objective_coefficients(lp.c)
+    dm.set_constraint_lower_bounds(lp.con_lo)
+    dm.set_constraint_upper_bounds(lp.con_up)
+    dm.set_variable_lower_bounds(lp.var_lo)
+    dm.set_variable_upper_bounds(lp.var_up)
+    return dm
+
+
+def oracle_view(dm: lpm.DataModel):
+    """The arrays of a DataModel in the layout the oracle takes."""
+    m, n = dm.n_constraints, dm.n_variables
+    lo = dm.constraint_lower_bounds
+    up = dm.constraint_upper_bounds
+    if lo is None:
+        rt = dm.row_types.astype(str)
+        b = dm.b
+        lo = np.where(rt == "L", -np.inf, b)
+        up = np.where(rt == "G", np.inf, b)
+    return SimpleNamespace(
+        row_off=dm.A_offsets, col_idx=dm.A_indices, val=dm.A_values, c=dm.c, con_lo=lo, con_up=up,
+        var_lo=dm.variable_lower_bounds if dm.variable_lower_bounds is not None else np.zeros(n),
+        var_up=dm.variable_upper_bounds if dm.variable_upper_bounds is not None else np.full(n, np.inf),
+        obj_offset=dm.objective_offset, maximize=dm.maximize, m=m, n=n)
+
+
+def settings(tol=1e-4, iteration_limit=None, time_limit=None, precision=None, method=None,
+             quiet=True) -> lpm.SolverSettings:
+    s = lpm.SolverSettings()
+    s.set_optimality_tolerance(tol)
+    if iteration_limit is not None:
+        s.set_parameter(lpm.CUOPT_ITERATION_LIMIT, int(iteration_limit))
+    if time_limit is not None:
+        s.set_parameter(lpm.CUOPT_TIME_LIMIT, float(time_limit))
+    if precision is not None:
+        s.set_parameter(lpm.CUOPT_PDLP_PRECISION, int(precision))
+    s.set_parameter(lpm.CUOPT_METHOD, int(method if method is not None else lpm.SolverMethod.PDLP))
+    if quiet:
+        s.set_parameter(lpm.CUOPT_LOG_TO_CONSOLE, False)
+    return s
+
+
+def rel(a, b):
+    return abs(a - b) / max(1.0, abs(b))

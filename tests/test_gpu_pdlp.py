@@ -1,0 +1,141 @@
+"""GPU parity tests of the PDLP path through the C-ABI (libcuopt_b200.so).
+
+Reference for every expectation: the CPU oracle (oracle/pdlp_oracle.cpp, an FP64 restatement of the
+reference's Stable3 PDLP), the optimum known by construction of the synthetic LPs, and the golden
+values of the reference's own tests (tests/golden/golden.json).
+
+Floating-point tolerances (FP64 path): iterates after the same number of iterations agree with the
+oracle to 1e-9 relative (summation order differs), objectives to 1e-9 relative, and solved
+problems reach the relative KKT targets asked for.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from cuopt_b200 import generators as gen
+from cuopt_b200 import linear_programming as lpm
+from oracle import oracle as O
+from tests.helpers import datamodel_from_lp, oracle_view, rel, settings
+
+pytestmark = pytest.mark.gpu
+
+ITERATE_RTOL = 1e-9
+
+
+@pytest.fixture(scope="module")
+def small_lp():
+    return gen.constructed_lp(200, 500, 8, seed=11)
+
+
+@pytest.mark.parametrize("k", [0, 10, 50, 200, 400, 1000])
+def test_iterates_match_oracle(small_lp, k):
+    """Same returned iterate as the oracle after k iterations (iteration limit)."""
+    dm = datamodel_from_lp(small_lp)
+    sol = lpm.Solve(dm, settings(tol=1e-12, iteration_limit=k))
+    res, x, y, rc = O.solve(small_lp, tol=1e-12, iteration_limit=k)
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.IterationLimit
+    assert res["status"] == 4
+    assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+    sx, sy = sol.get_primal_solution(), sol.get_dual_solution()
+    scale_x = 1.0 + np.max(np.abs(x))
+    scale_y = 1.0 + np.max(np.abs(y))
+    assert np.max(np.abs(sx - x)) <= ITERATE_RTOL * scale_x
+    assert np.max(np.abs(sy - y)) <= ITERATE_RTOL * scale_y
+    assert np.max(np.abs(sol.get_reduced_cost() - rc)) <= ITERATE_RTOL * (1 + np.max(np.abs(rc)))
+    assert rel(sol.get_primal_objective(), res["primal_obj"]) <= 1e-9
+    assert rel(sol.get_dual_objective(), res["dual_obj"]) <= 1e-9
+
+
+def test_solve_matches_oracle_and_optimum(small_lp):
+    dm = datamodel_from_lp(small_lp)
+    sol = lpm.Solve(dm, settings(tol=1e-6))
+    res, x, y, _ = O.solve(small_lp, tol=1e-6)
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert res["status"] == 1
+    assert abs(sol.get_lp_stats()["nb_iterations"] - res["iterations"]) <= 0.05 * res["iterations"]
+    opt = small_lp.optimal_objective
+    assert rel(sol.get_primal_objective(), opt) <= 1e-5
+    kkt = gen.kkt_relative_error(small_lp, sol.get_primal_solution(), sol.get_dual_solution())
+    assert kkt["rel_primal"] <= 1e-6 and kkt["rel_gap"] <= 1e-6
+
+
+def test_config0_full_size():
+    """Config 0 (2000 x 5000, 8 nnz / column): Optimal at 1e-6, objective within 1e-6 of the
+    constructed optimum relative to its magnitude, same status and iteration count as the oracle."""
+    lp = gen.constructed_lp(2000, 5000, 8, seed=0)
+    sol = lpm.Solve(datamodel_from_lp(lp), settings(tol=1e-6))
+    res, _, _, _ = O.solve(lp, tol=1e-6)
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal == res["status"]
+    assert abs(sol.get_lp_stats()["nb_iterations"] - res["iterations"]) <= 0.05 * res["iterations"]
+    assert rel(sol.get_primal_objective(), lp.optimal_objective) <= 1e-5
+    kkt = gen.kkt_relative_error(lp, sol.get_primal_solution(), sol.get_dual_solution())
+    assert max(kkt["rel_primal"], kkt["rel_gap"]) <= 1e-6
+
+
+def test_afiro_objective(golden, golden_dir):
+    g = golden["afiro_objective"]
+    dm = lpm.ReadMps(golden_dir / "afiro_original.mps")
+    sol = lpm.Solve(dm, settings(tol=1e-4))
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert rel(sol.get_primal_objective(), g["value"]) <= g["rel_tol"]
+    res, _, _, _ = O.solve(oracle_view(dm), tol=1e-4)
+    assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+    assert rel(sol.get_primal_objective(), res["primal_obj"]) <= 1e-9
+    tight = lpm.Solve(dm, settings(tol=1e-8))
+    assert abs(tight.get_primal_objective() - g["value"]) <= 1e-4
+
+
+@pytest.mark.parametrize("name,key", [("max_offset.mps", "max_offset_objective"),
+                                      ("good-max.mps", "good_max_objective")])
+def test_maximize_fixtures(golden, golden_dir, name, key):
+    g = golden[key]
+    dm = lpm.ReadMps(golden_dir / name)
+    sol = lpm.Solve(dm, settings(tol=1e-8))
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert abs(sol.get_primal_objective() - g["value"]) <= g["abs_tol"]
+
+
+def test_no_constraints(golden, golden_dir):
+    dm = lpm.ReadMps(golden_dir / "lp-model-no-constraints.mps")
+    sol = lpm.Solve(dm, settings(method=lpm.SolverMethod.Concurrent))
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert abs(sol.get_primal_objective() - golden["no_constraints_objective"]["value"]) <= 1e-4
+    assert not sol.get_solved_by_pdlp()
+    pd = lpm.Solve(lpm.ReadMps(golden_dir / "empty_matrix.mps"), settings())
+    assert int(pd.get_termination_status()) == golden["empty_matrix_pdlp_status"]["value"]
+
+
+def test_time_limit_zero(small_lp):
+    sol = lpm.Solve(datamodel_from_lp(small_lp), settings(tol=1e-8, time_limit=0.0))
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.TimeLimit
+
+
+def test_inequality_and_free_rows_match_oracle():
+    lp = gen.skewed_lp(300, 900, seed=5, cap=200)
+    dm = datamodel_from_lp(lp)
+    for k in (10, 200):
+        sol = lpm.Solve(dm, settings(tol=1e-12, iteration_limit=k))
+        res, x, y, _ = O.solve(lp, tol=1e-12, iteration_limit=k)
+        assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+        np.testing.assert_allclose(sol.get_primal_solution(), x, rtol=1e-8,
+                                   atol=1e-8 * (1 + np.max(np.abs(x))))
+        np.testing.assert_allclose(sol.get_dual_solution(), y, rtol=1e-8,
+                                   atol=1e-8 * (1 + np.max(np.abs(y))))
+
+
+def test_maximize_offset_matches_oracle(small_lp):
+    dm = datamodel_from_lp(small_lp, maximize=True, offset=3.5)
+    dm.set_objective_coefficients(-small_lp.c)
+    sol = lpm.Solve(dm, settings(tol=1e-6))
+    res, x, y, _ = O.solve(oracle_view(dm), tol=1e-6)
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert rel(sol.get_primal_objective(), res["primal_obj"]) <= 1e-8
+    assert rel(sol.get_primal_objective(), -small_lp.optimal_objective + 3.5) <= 1e-5
+    np.testing.assert_allclose(sol.get_dual_solution(), y, atol=1e-7 * (1 + np.abs(y).max()))
+
+
+def test_mixed_precision_reaches_tolerance(small_lp):
+    sol = lpm.Solve(datamodel_from_lp(small_lp), settings(tol=1e-4, precision=1))
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert rel(sol.get_primal_objective(), small_lp.optimal_objective) <= 1e-3

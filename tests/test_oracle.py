@@ -1,0 +1,111 @@
+"""The CPU oracle pinned against the reference's golden values and against constructed optima.
+
+The oracle (oracle/pdlp_oracle.cpp) is the FP64 restatement of the reference's Stable3 PDLP path.
+These tests run on the CPU only.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from cuopt_b200 import generators as gen
+from cuopt_b200 import linear_programming as lpm
+from oracle import oracle as O
+from tests.helpers import oracle_view, rel
+
+
+def test_methodical1_initial_step_and_weight_match_reference_golden(golden, golden_dir):
+    """pdlp_test.cu:243-286: Methodical1 initial step size 1.4893 and primal weight 0.0141652 on
+    afiro.  Pins Ruiz (5 passes), Pock-Chambolle (alpha 1), max-|A| step size and the
+    combined-bounds primal weight."""
+    dm = lpm.ReadMps(golden_dir / "afiro_original.mps")
+    step, weight = O.initial_step_and_weight(oracle_view(dm), mode=2)
+    g1 = golden["afiro_methodical1_initial_step_size"]
+    g2 = golden["afiro_methodical1_initial_primal_weight"]
+    assert abs(step - g1["value"]) <= g1["abs_tol"]
+    assert abs(weight - g2["value"]) <= g2["abs_tol"]
+
+
+def test_stable3_initial_weight_is_one(golden_dir):
+    """Stable3 with bound/objective rescaling uses primal weight 1 (pdlp.cu:2799-2810)."""
+    dm = lpm.ReadMps(golden_dir / "afiro_original.mps")
+    step, weight = O.initial_step_and_weight(oracle_view(dm), mode=4)
+    assert weight == 1.0
+    assert 0.0 < step < 10.0
+
+
+def test_afiro_objective(golden, golden_dir):
+    g = golden["afiro_objective"]
+    dm = lpm.ReadMps(golden_dir / "afiro_original.mps")
+    res, x, y, _ = O.solve(oracle_view(dm), tol=1e-4)
+    assert res["status"] == 1
+    assert rel(res["primal_obj"], g["value"]) <= g["rel_tol"]
+    res8, _, _, _ = O.solve(oracle_view(dm), tol=1e-8)
+    assert abs(res8["primal_obj"] - g["value"]) <= 1e-4
+
+
+@pytest.mark.parametrize("name,key", [("max_offset.mps", "max_offset_objective"),
+                                      ("good-max.mps", "good_max_objective")])
+def test_maximize_fixtures(golden, golden_dir, name, key):
+    dm = lpm.ReadMps(golden_dir / name)
+    res, _, _, _ = O.solve(oracle_view(dm), tol=1e-8)
+    assert res["status"] == 1
+    assert abs(res["primal_obj"] - golden[key]["value"]) <= golden[key]["abs_tol"]
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_constructed_optimum_small(seed):
+    lp = gen.constructed_lp(200, 500, 8, seed=seed)
+    res, x, y, _ = O.solve(lp, tol=1e-7)
+    assert res["status"] == 1
+    assert rel(res["primal_obj"], lp.optimal_objective) <= 1e-6
+    kkt = gen.kkt_relative_error(lp, x, y)
+    assert kkt["rel_primal"] <= 1e-7 and kkt["rel_gap"] <= 1e-7
+
+
+def test_constructed_optimum_config0():
+    """Config 0 (2000 x 5000) to 1e-6: objective within 1e-6 relative of the constructed optimum."""
+    lp = gen.constructed_lp(2000, 5000, 8, seed=0)
+    res, x, y, _ = O.solve(lp, tol=1e-6)
+    assert res["status"] == 1
+    assert rel(res["primal_obj"], lp.optimal_objective) <= 1e-5
+    assert gen.kkt_relative_error(lp, x, y)["rel_primal"] <= 1e-6
+
+
+def test_skewed_generator_is_consistent():
+    lp = gen.skewed_lp(400, 1200, seed=3, cap=300)
+    kkt = gen.kkt_relative_error(lp, lp.x_star, lp.y_star)
+    assert kkt["rel_primal"] < 1e-12 and kkt["rel_dual"] < 1e-12 and kkt["rel_gap"] < 1e-9
+    res, x, y, _ = O.solve(lp, tol=1e-6)
+    assert res["status"] == 1
+    assert rel(res["primal_obj"], lp.optimal_objective) <= 1e-4
+
+
+def test_constructed_generator_kkt_exact():
+    lp = gen.constructed_lp(300, 800, 8, seed=4)
+    kkt = gen.kkt_relative_error(lp, lp.x_star, lp.y_star)
+    assert max(kkt["rel_primal"], kkt["rel_dual"], kkt["rel_gap"]) < 1e-12
+
+
+def test_iteration_limit_and_no_constraints():
+    lp = gen.constructed_lp(100, 250, 8, seed=9)
+    res, _, _, _ = O.solve(lp, tol=1e-12, iteration_limit=1)
+    assert res["status"] == 4 and res["iterations"] == 10  # limit checked at conditional majors
+    res0, _, _, _ = O.solve(lp, tol=1e-12, iteration_limit=0)
+    assert res0["status"] == 4 and res0["iterations"] == 0
+
+
+def test_highs_cross_check():
+    """Third-party cross-check (SciPy HiGHS, not the reference) on a small constructed LP."""
+    scipy = pytest.importorskip("scipy")
+    from scipy.optimize import linprog
+    from scipy.sparse import csr_matrix
+
+    lp = gen.constructed_lp(150, 400, 8, seed=21)
+    A = csr_matrix((lp.val, lp.col_idx, lp.row_off), shape=(lp.m, lp.n))
+    r = linprog(lp.c, A_eq=A, b_eq=lp.con_lo, bounds=list(zip(lp.var_lo, lp.var_up)),
+                method="highs")
+    assert r.status == 0
+    assert rel(r.fun, lp.optimal_objective) <= 1e-9
+    res, _, _, _ = O.solve(lp, tol=1e-8)
+    assert rel(res["primal_obj"], r.fun) <= 1e-7
