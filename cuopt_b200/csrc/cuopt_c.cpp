@@ -579,10 +579,13 @@ cuopt_int_t cuOptSolveDevice(cuopt_int_t m, cuopt_int_t n, cuopt_int_t sense, cu
     prm.log_to_console          = false;
     sol.r = cuopt_b200::pdlp_solve_device(in, prm, static_cast<cudaStream_t>(stream), d_x, d_y, d_rc);
   } catch (const std::bad_alloc&) {
+    std::fprintf(stderr, "cuOptSolveDevice: out of memory\n");
     return CUOPT_OUT_OF_MEMORY;
-  } catch (const std::invalid_argument&) {
+  } catch (const std::invalid_argument& e) {
+    std::fprintf(stderr, "cuOptSolveDevice: %s\n", e.what());
     return CUOPT_VALIDATION_ERROR;
-  } catch (const std::exception&) {
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "cuOptSolveDevice: %s\n", e.what());
     return CUOPT_RUNTIME_ERROR;
   }
   if (termination_status) *termination_status = sol.r.status;
@@ -622,9 +625,11 @@ cuopt_int_t cuOptProfilePDHGSweeps(cuopt_int_t m, cuopt_int_t n, const cuopt_flo
     *bytes_dual   = prof.bytes_dual;
   } catch (const std::bad_alloc&) {
     return CUOPT_OUT_OF_MEMORY;
-  } catch (const std::invalid_argument&) {
+  } catch (const std::invalid_argument& e) {
+    std::fprintf(stderr, "cuOptProfilePDHGSweeps: %s\n", e.what());
     return CUOPT_VALIDATION_ERROR;
-  } catch (const std::exception&) {
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "cuOptProfilePDHGSweeps: %s\n", e.what());
     return CUOPT_RUNTIME_ERROR;
   }
   return CUOPT_SUCCESS;

@@ -664,25 +664,51 @@ class engine {
 
 }  // namespace
 
+namespace {
+
+// The engine captures CUDA graphs, which the legacy default stream does not allow, so it always
+// works on its own non-blocking stream ordered after / before the caller's stream with events.
+struct joined_stream {
+  cudaStream_t caller, own = nullptr;
+  cudaEvent_t ev = nullptr;
+  explicit joined_stream(cudaStream_t c) : caller(c)
+  {
+    B200_CUDA_CHECK(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+    B200_CUDA_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    B200_CUDA_CHECK(cudaEventRecord(ev, caller));
+    B200_CUDA_CHECK(cudaStreamWaitEvent(own, ev, 0));
+  }
+  ~joined_stream()
+  {
+    if (cudaEventRecord(ev, own) == cudaSuccess) cudaStreamWaitEvent(caller, ev, 0);
+    cudaEventDestroy(ev);
+    cudaStreamDestroy(own);
+  }
+};
+
+}  // namespace
+
 pdlp_result pdlp_solve_device(const lp_device_input& in, const pdlp_params& p, cudaStream_t stream,
                               double* x_out, double* y_out, double* rc_out)
 {
+  joined_stream js(stream);
   if (p.precision == 1) {
-    engine<float> e(in, p, stream);
+    engine<float> e(in, p, js.own);
     return e.run(x_out, y_out, rc_out);
   }
-  engine<double> e(in, p, stream);
+  engine<double> e(in, p, js.own);
   return e.run(x_out, y_out, rc_out);
 }
 
 sweep_profile pdlp_profile_sweeps(const lp_device_input& in, const pdlp_params& p,
                                   cudaStream_t stream, int iterations)
 {
+  joined_stream js(stream);
   if (p.precision == 1) {
-    engine<float> e(in, p, stream);
+    engine<float> e(in, p, js.own);
     return e.profile(iterations);
   }
-  engine<double> e(in, p, stream);
+  engine<double> e(in, p, js.own);
   return e.profile(iterations);
 }
 

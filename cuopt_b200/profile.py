@@ -1,0 +1,95 @@
+"""Profiling driver for the PDLP kernels (used under ncu; also a quick standalone timing tool).
+
+    python -m cuopt_b200.profile --config c1 --mode solve  --precision mixed
+    python -m cuopt_b200.profile --config c1_small --mode sweeps --precision mixed --iterations 3
+
+`solve`  runs one full solve to 1e-6 relative KKT from device-resident inputs (cuOptSolveDevice);
+`sweeps` prepares the LP and launches the two fused PDHG sweeps separately between CUDA events
+         (cuOptProfilePDHGSweeps).  Prints one JSON line with the timings.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+CONFIGS = {
+    "c0": (2_000, 5_000, 8, 0),
+    "c1": (1_000_000, 2_000_000, 8, 1000),
+    "c1_small": (750_000, 1_500_000, 8, 1000),
+    "c4": (5_000, 10_000, 8, 4000),
+}
+
+
+def main() -> None:
+    import numpy as np
+    import torch
+
+    from cuopt_b200 import generators as gen
+    from cuopt_b200._lib import PDLPStatistics, lib
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="c1_small")
+    ap.add_argument("--mode", choices=["solve", "sweeps"], default="sweeps")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--iterations", type=int, default=3)
+    ap.add_argument("--tol", type=float, default=1e-6)
+    a = ap.parse_args()
+
+    m, n, k, seed = CONFIGS[a.config]
+    lp = gen.constructed_lp(m, n, k, seed=seed)
+    dev = torch.device("cuda", 0)
+    t = lambda x, dt: torch.as_tensor(np.ascontiguousarray(x), device=dev, dtype=dt)
+    arrs = [t(lp.c, torch.float64), t(lp.row_off, torch.int32), t(lp.col_idx, torch.int32),
+            t(lp.val, torch.float64), t(lp.con_lo, torch.float64), t(lp.con_up, torch.float64),
+            t(lp.var_lo, torch.float64), t(lp.var_up, torch.float64)]
+    ptr = [C.c_void_p(x.data_ptr()) for x in arrs]
+    L = lib()
+    s = C.c_void_p()
+    L.cuOptCreateSolverSettings(C.byref(s))
+    for name in ("absolute_primal_tolerance", "relative_primal_tolerance", "absolute_dual_tolerance",
+                 "relative_dual_tolerance", "absolute_gap_tolerance", "relative_gap_tolerance"):
+        L.cuOptSetFloatParameter(s, name.encode(), a.tol)
+    L.cuOptSetIntegerParameter(s, b"pdlp_precision", 1 if a.precision == "mixed" else 0)
+    L.cuOptSetParameter(s, b"log_to_console", b"false")
+    stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    out = {"config": a.config, "m": m, "n": n, "nnz": lp.nnz, "precision": a.precision, "mode": a.mode}
+    if a.mode == "solve":
+        x = torch.empty(n, device=dev, dtype=torch.float64)
+        y = torch.empty(m, device=dev, dtype=torch.float64)
+        rc = torch.empty(n, device=dev, dtype=torch.float64)
+        st, status = PDLPStatistics(), C.c_int32()
+        t0 = time.perf_counter()
+        code = L.cuOptSolveDevice(m, n, 1, 0.0, *ptr, s, stream, C.c_void_p(x.data_ptr()),
+                                  C.c_void_p(y.data_ptr()), C.c_void_p(rc.data_ptr()), C.byref(st),
+                                  C.byref(status))
+        torch.cuda.synchronize()
+        out.update({"rc": code, "status": status.value, "wall_s": time.perf_counter() - t0})
+        out.update({f: getattr(st, f) for f, _ in PDLPStatistics._fields_})
+        if code != 0:
+            print(json.dumps(out))
+            sys.exit(1)
+    else:
+        vals = [C.c_double() for _ in range(4)]
+        code = L.cuOptProfilePDHGSweeps(m, n, *ptr, s, stream, a.iterations, *[C.byref(v) for v in vals])
+        out.update({"rc": code, "ms_primal": vals[0].value, "ms_dual": vals[1].value,
+                    "bytes_primal": vals[2].value, "bytes_dual": vals[3].value})
+        if code == 0:
+            out["gbs_primal"] = vals[2].value / vals[0].value / 1e6
+            out["gbs_dual"] = vals[3].value / vals[1].value / 1e6
+        else:
+            print(json.dumps(out))
+            sys.exit(1)
+    L.cuOptDestroySolverSettings(C.byref(s))
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()
