@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <climits>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -29,7 +30,43 @@ struct cuda_error : std::runtime_error {
 
 constexpr int kWarp = 32;
 
-// Device buffer owning `n` elements of T.
+// Stream on which device buffers are allocated and released (stream-ordered allocator).  Solver
+// entry points set it for their duration with alloc_scope; buffers remember their stream and free
+// themselves asynchronously on it, so a release is ordered after the kernels that used the memory.
+inline cudaStream_t& alloc_stream_ref()
+{
+  static thread_local cudaStream_t s = nullptr;
+  return s;
+}
+struct alloc_scope {
+  cudaStream_t prev;
+  explicit alloc_scope(cudaStream_t s) : prev(alloc_stream_ref()) { alloc_stream_ref() = s; }
+  ~alloc_scope() { alloc_stream_ref() = prev; }
+};
+
+// Keeps freed device memory in the default pool between solves (configured once per device).
+inline void configure_pool_once()
+{
+  static thread_local int configured_device = -1;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev == configured_device) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t threshold = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+  }
+  configured_device = dev;
+}
+
+// Small pinned host scratch for scalar read-backs (per thread, allocated once).
+inline double* pinned_scratch()
+{
+  static thread_local double* p = nullptr;
+  if (!p) B200_CUDA_CHECK(cudaMallocHost(&p, 64 * sizeof(double)));
+  return p;
+}
+
+// Device buffer owning `n` elements of T (stream-ordered allocation on alloc_stream_ref()).
 template <typename T>
 class dbuf {
  public:
@@ -38,7 +75,7 @@ class dbuf {
   ~dbuf() { release(); }
   dbuf(const dbuf&)            = delete;
   dbuf& operator=(const dbuf&) = delete;
-  dbuf(dbuf&& o) noexcept : p_(o.p_), n_(o.n_)
+  dbuf(dbuf&& o) noexcept : p_(o.p_), n_(o.n_), s_(o.s_)
   {
     o.p_ = nullptr;
     o.n_ = 0;
@@ -49,6 +86,7 @@ class dbuf {
       release();
       p_   = o.p_;
       n_   = o.n_;
+      s_   = o.s_;
       o.p_ = nullptr;
       o.n_ = 0;
     }
@@ -57,12 +95,13 @@ class dbuf {
   void resize(size_t n)
   {
     release();
-    if (n) B200_CUDA_CHECK(cudaMalloc(&p_, n * sizeof(T)));
+    s_ = alloc_stream_ref();
+    if (n) B200_CUDA_CHECK(cudaMallocAsync(&p_, n * sizeof(T), s_));
     n_ = n;
   }
   void release()
   {
-    if (p_) cudaFree(p_);
+    if (p_) cudaFreeAsync(p_, s_);
     p_ = nullptr;
     n_ = 0;
   }
@@ -83,8 +122,9 @@ class dbuf {
   size_t size() const { return n_; }
 
  private:
-  T* p_     = nullptr;
-  size_t n_ = 0;
+  T* p_          = nullptr;
+  size_t n_      = 0;
+  cudaStream_t s_ = nullptr;
 };
 
 #ifdef __CUDACC__
@@ -137,5 +177,16 @@ __device__ __forceinline__ int ld_stream(const int* p) { return __ldcs(p); }
 #endif
 
 B200_HD inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
+
+// Sliced-ELL element address.  A slice holds 32 rows; row t of the slice owns lane t.  Elements are
+// grouped in chunks of 4 consecutive row elements per lane, and the 32 lanes' chunks are adjacent:
+// element k of lane t lives at base + ((k / 4) * 32 + t) * 4 + k % 4.  A warp therefore reads one
+// chunk of every row with a single 128-bit load per lane (512 contiguous bytes for 32-bit data).
+// Slice lengths are multiples of 4 and slice bases multiples of 4 elements (16-byte aligned).
+constexpr int kChunk = 4;
+B200_HD inline int64_t sell_pos(int64_t base, int k, int lane)
+{
+  return base + ((int64_t)(k >> 2) * 32 + lane) * kChunk + (k & 3);
+}
 
 }  // namespace cuopt_b200

@@ -112,7 +112,7 @@ __global__ void slice_words_kernel(const int* off, int rows, int n_long, int n_s
       const int r = n_long + s * 32 + t;
       if (r < rows) mx = max(mx, off[r + 1] - off[r]);
     }
-    words[s] = 32 * (int64_t)mx;
+    words[s] = 32 * (int64_t)((mx + kChunk - 1) / kChunk * kChunk);
   }
 }
 
@@ -146,7 +146,7 @@ __global__ void sell_fill_kernel(const int* off, const int* idx, const double* v
     }
     int last = (e > b) ? idx[b] : 0;
     for (int k = 0; k < len; ++k) {
-      const int64_t p = base + (int64_t)k * 32 + lane;
+      const int64_t p = sell_pos(base, k, lane);
       if (b + k < e) {
         last    = idx[b + k];
         oidx[p] = last;
@@ -236,8 +236,10 @@ void to_sell(int rows, int cols, int n_long, const int* off, const int* idx, con
   B200_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(tmp.get(bytes), bytes, words.data(),
                                                 M.slice_off.data(), M.n_slices + 1, s));
   B200_CUDA_CHECK(cudaStreamSynchronize(s));
+  // The sliced part starts on a 4-element boundary so its 128-bit loads are aligned.
+  const int64_t sell_base = (long_nnz + kChunk - 1) / kChunk * kChunk;
   add_base_kernel<<<grid_for(M.n_slices + 1), kT, 0, s>>>(M.slice_off.data(), M.n_slices + 1,
-                                                          long_nnz);
+                                                          sell_base);
   int64_t total = 0;
   B200_CUDA_CHECK(cudaMemcpyAsync(&total, M.slice_off.data() + M.n_slices, sizeof(int64_t),
                                   cudaMemcpyDeviceToHost, s));
@@ -246,6 +248,11 @@ void to_sell(int rows, int cols, int n_long, const int* off, const int* idx, con
   M.idx.resize(std::max<int64_t>(total, 1));
   M.val.resize(std::max<int64_t>(total, 1));
   M.src.resize(std::max<int64_t>(total, 1));
+  if (sell_base > long_nnz) {  // alignment gap: padding elements
+    B200_CUDA_CHECK(cudaMemsetAsync(M.idx.data() + long_nnz, 0, (sell_base - long_nnz) * sizeof(int), s));
+    B200_CUDA_CHECK(cudaMemsetAsync(M.val.data() + long_nnz, 0, (sell_base - long_nnz) * sizeof(double), s));
+    B200_CUDA_CHECK(cudaMemsetAsync(M.src.data() + long_nnz, 0xFF, (sell_base - long_nnz) * sizeof(int), s));
+  }
   if (long_nnz > 0) {
     B200_CUDA_CHECK(cudaMemcpyAsync(M.idx.data(), idx, long_nnz * sizeof(int), cudaMemcpyDeviceToDevice, s));
     B200_CUDA_CHECK(cudaMemcpyAsync(M.val.data(), val, long_nnz * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -273,12 +280,7 @@ void build_device_layout(int m, int n, const int* d_off, const int* d_idx, const
   out.nnz           = nnz;
   temp_store tmp;
   dbuf<int> counters(2);
-  int* hcount = nullptr;
-  B200_CUDA_CHECK(cudaMallocHost(&hcount, 2 * sizeof(int)));
-  struct pin_guard {
-    int* p;
-    ~pin_guard() { cudaFreeHost(p); }
-  } guard{hcount};
+  int* hcount = reinterpret_cast<int*>(pinned_scratch() + 32);
 
   dbuf<int> rlen(std::max(m, 1)), clen(std::max(n, 1));
   row_len_kernel<<<grid_for(m), kT, 0, s>>>(d_off, m, rlen.data());

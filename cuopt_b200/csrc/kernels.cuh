@@ -96,7 +96,32 @@ __global__ void __launch_bounds__(kBlock) finalize_sum_kernel(const double* part
   }
 }
 
-// Generic fused sweep: acc_r = sum_k A[r,k] * g[idx[r,k]], then epi(r, acc_r, red).
+// 4 consecutive values of one lane chunk (16-byte aligned), streamed with evict-first loads.
+__device__ __forceinline__ void load_chunk(const float* p, double (&v)[4])
+{
+  const float4 t = __ldcs(reinterpret_cast<const float4*>(p));
+  v[0]           = t.x;
+  v[1]           = t.y;
+  v[2]           = t.z;
+  v[3]           = t.w;
+}
+__device__ __forceinline__ void load_chunk(const double* p, double (&v)[4])
+{
+  const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+  const double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+  v[0]            = a.x;
+  v[1]            = a.y;
+  v[2]            = b.x;
+  v[3]            = b.y;
+}
+__device__ __forceinline__ int4 load_idx_chunk(const int* p)
+{
+  return __ldcs(reinterpret_cast<const int4*>(p));
+}
+
+// Generic fused sweep: acc_r = sum_k A[r,k] * g[idx[r,k]], then epi(r, acc_r, pre, red).
+// The epilogue's per-row operands (`pre`) are loaded before the matrix loop so their memory latency
+// overlaps the gathers.  Sliced rows are read in 4-element lane chunks, two chunks in flight.
 template <typename TM, typename TG, class Epi>
 __global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
                                                           const TG* __restrict__ g, Epi epi,
@@ -116,42 +141,55 @@ __global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
   if ((int)blockIdx.x < lb) {
     const int row = blockIdx.x * kWarpsPerBlock + warp;
     if (row < A.n_long) {
+      const auto pre  = epi.load(row);
       const int64_t b = A.long_off[row], e = A.long_off[row + 1];
       double acc      = 0.0;
       for (int64_t k = b + lane; k < e; k += kWarp)
         acc += (double)ld_stream(A.val + k) * (double)g[ld_stream(A.idx + k)];
       acc = warp_sum(acc);
-      if (lane == 0) epi(row, acc, red);
+      if (lane == 0) epi(row, acc, pre, red);
     }
   } else {
     const int s = (blockIdx.x - lb) * kWarpsPerBlock + warp;
     if (s < A.n_slices) {
+      const int row      = A.n_long + s * kWarp + lane;
+      const bool valid   = row < A.rows;
+      const auto pre     = epi.load(valid ? row : A.rows - 1);
       const int64_t base = A.slice_off[s];
-      const int len      = (int)((A.slice_off[s + 1] - base) >> 5);
-      const TM* v        = A.val + base + lane;
-      const int* ix      = A.idx + base + lane;
+      const int nchunk   = (int)((A.slice_off[s + 1] - base) >> 7);  // 32 lanes x 4 elements
+      const TM* v        = A.val + base + lane * kChunk;
+      const int* ix      = A.idx + base + lane * kChunk;
       double acc         = 0.0;
-      int k              = 0;
-      for (; k + 4 <= len; k += 4) {
-        const int i0 = ld_stream(ix), i1 = ld_stream(ix + 32), i2 = ld_stream(ix + 64),
-                  i3 = ld_stream(ix + 96);
-        const TM v0 = ld_stream(v), v1 = ld_stream(v + 32), v2 = ld_stream(v + 64),
-                 v3 = ld_stream(v + 96);
-        const TG g0 = g[i0], g1 = g[i1], g2 = g[i2], g3 = g[i3];
-        acc += (double)v0 * (double)g0;
-        acc += (double)v1 * (double)g1;
-        acc += (double)v2 * (double)g2;
-        acc += (double)v3 * (double)g3;
-        v += 128;
-        ix += 128;
+      int q              = 0;
+      for (; q + 2 <= nchunk; q += 2) {
+        const int4 i0 = load_idx_chunk(ix), i1 = load_idx_chunk(ix + 32 * kChunk);
+        double v0[4], v1[4];
+        load_chunk(v, v0);
+        load_chunk(v + 32 * kChunk, v1);
+        const TG g0 = g[i0.x], g1 = g[i0.y], g2 = g[i0.z], g3 = g[i0.w];
+        const TG g4 = g[i1.x], g5 = g[i1.y], g6 = g[i1.z], g7 = g[i1.w];
+        acc += v0[0] * (double)g0;
+        acc += v0[1] * (double)g1;
+        acc += v0[2] * (double)g2;
+        acc += v0[3] * (double)g3;
+        acc += v1[0] * (double)g4;
+        acc += v1[1] * (double)g5;
+        acc += v1[2] * (double)g6;
+        acc += v1[3] * (double)g7;
+        v += 64 * kChunk;
+        ix += 64 * kChunk;
       }
-      for (; k < len; ++k) {
-        acc += (double)ld_stream(v) * (double)g[ld_stream(ix)];
-        v += 32;
-        ix += 32;
+      if (q < nchunk) {
+        const int4 i0 = load_idx_chunk(ix);
+        double v0[4];
+        load_chunk(v, v0);
+        const TG g0 = g[i0.x], g1 = g[i0.y], g2 = g[i0.z], g3 = g[i0.w];
+        acc += v0[0] * (double)g0;
+        acc += v0[1] * (double)g1;
+        acc += v0[2] * (double)g2;
+        acc += v0[3] * (double)g3;
       }
-      const int row = A.n_long + s * kWarp + lane;
-      if (row < A.rows) epi(row, acc, red);
+      if (valid) epi(row, acc, pre, red);
     }
   }
   block_reduce_store<K>(red, partials);
@@ -178,13 +216,20 @@ struct primal_epi {
   TX* aty;
   const pdlp_scalars* st;
   int it_off;
+  struct pre_t {
+    TX x, c, lo, up, xa;
+  };
   __device__ bool skip() const { return false; }
-  __device__ __forceinline__ void operator()(int j, double acc, red_t<0>&) const
+  __device__ __forceinline__ pre_t load(int j) const
+  {
+    return pre_t{x[j], c[j], lo[j], up[j], HALPERN ? xa[j] : TX(0)};
+  }
+  __device__ __forceinline__ void operator()(int j, double acc, const pre_t& p, red_t<0>&) const
   {
     const double tau  = st->tau;
-    const double xj   = (double)x[j];
-    const double next = xj - tau * ((double)c[j] - acc);
-    const double cl   = fmax(fmin(next, (double)up[j]), (double)lo[j]);
+    const double xj   = (double)p.x;
+    const double next = xj - tau * ((double)p.c - acc);
+    const double cl   = fmax(fmin(next, (double)p.up), (double)p.lo);
     if constexpr (MAJOR) {
       xhat[j]  = (TX)cl;
       slack[j] = (TX)((cl - next) / tau);
@@ -194,7 +239,7 @@ struct primal_epi {
     if constexpr (HALPERN) {
       const double w = halpern_weight(st, it_off);
       xbar[j]        = (TX)xb;
-      xout[j]        = (TX)(w * xb + (1.0 - w) * (double)xa[j]);
+      xout[j]        = (TX)(w * xb + (1.0 - w) * (double)p.xa);
     } else {
       xbar[j] = (TX)xb;
     }
@@ -215,13 +260,21 @@ struct dual_epi {
   TX* yhat;
   const pdlp_scalars* st;
   int it_off;
+  struct pre_t {
+    TX y, lo, up, ya;
+  };
   __device__ bool skip() const { return false; }
-  __device__ __forceinline__ void operator()(int i, double acc, red_t<kRed>& r) const
+  __device__ __forceinline__ pre_t load(int i) const
+  {
+    return pre_t{y[i], lo[i], up[i], HALPERN ? ya[i] : TX(0)};
+  }
+  __device__ __forceinline__ void operator()(int i, double acc, const pre_t& p,
+                                             red_t<kRed>& r) const
   {
     const double sigma = st->sigma;
-    const double yi    = (double)y[i];
+    const double yi    = (double)p.y;
     const double t     = yi / sigma - acc;
-    const double tp    = fmax(-(double)up[i], fmin(t, -(double)lo[i]));
+    const double tp    = fmax(-(double)p.up, fmin(t, -(double)p.lo));
     const double ny    = (t - tp) * sigma;
     if constexpr (MAJOR) yhat[i] = (TX)ny;
     const double yb = 2.0 * ny - yi;
@@ -231,7 +284,7 @@ struct dual_epi {
     }
     if constexpr (HALPERN) {
       const double w = halpern_weight(st, it_off);
-      yout[i]        = (TX)(w * yb + (1.0 - w) * (double)ya[i]);
+      yout[i]        = (TX)(w * yb + (1.0 - w) * (double)p.ya);
     } else {
       ybar[i] = (TX)yb;
     }
@@ -246,11 +299,15 @@ struct fpe_epi {
   const TX* aty;
   const TX* xbar;
   const TX* x;
+  struct pre_t {
+    TX aty, xbar, x;
+  };
   __device__ bool skip() const { return false; }
-  __device__ __forceinline__ void operator()(int j, double acc, red_t<2>& r) const
+  __device__ __forceinline__ pre_t load(int j) const { return pre_t{aty[j], xbar[j], x[j]}; }
+  __device__ __forceinline__ void operator()(int j, double acc, const pre_t& p, red_t<2>& r) const
   {
-    const double d  = acc - (double)aty[j];
-    const double dx = (double)xbar[j] - (double)x[j];
+    const double d  = acc - (double)p.aty;
+    const double dx = (double)p.xbar - (double)p.x;
     r.v[0] += d * dx;
     r.v[1] += dx * dx;
   }
@@ -314,13 +371,17 @@ struct term_primal_epi {
   const double* lc;
   const double* uc;
   const double* y;
+  struct pre_t {
+    double l, u, y;
+  };
   __device__ bool skip() const { return false; }
-  __device__ __forceinline__ void operator()(int i, double ax, red_t<2>& r) const
+  __device__ __forceinline__ pre_t load(int i) const { return pre_t{lc[i], uc[i], y[i]}; }
+  __device__ __forceinline__ void operator()(int i, double ax, const pre_t& p, red_t<2>& r) const
   {
-    const double l = lc[i], u = uc[i];
+    const double l = p.l, u = p.u;
     const double cl = fmax(l, fmin(ax, u));
     const double rp = ax - cl;
-    const double yi = y[i];
+    const double yi = p.y;
     r.v[0] += rp * rp;
     r.v[1] += fmax(yi, 0.0) * finite_or_zero(l) + fmin(yi, 0.0) * finite_or_zero(u);
   }
@@ -332,10 +393,14 @@ struct term_dual_epi {
   const double* c;
   const double* x;
   const double* s;
+  struct pre_t {
+    double c, x, s;
+  };
   __device__ bool skip() const { return false; }
-  __device__ __forceinline__ void operator()(int j, double aty, red_t<3>& r) const
+  __device__ __forceinline__ pre_t load(int j) const { return pre_t{c[j], x[j], s[j]}; }
+  __device__ __forceinline__ void operator()(int j, double aty, const pre_t& p, red_t<3>& r) const
   {
-    const double cj = c[j], xj = x[j], sj = s[j];
+    const double cj = p.c, xj = p.x, sj = p.s;
     const double rd = (cj - aty) - sj;
     r.v[0] += rd * rd;
     r.v[1] += cj * xj;
@@ -349,8 +414,13 @@ struct store_epi {  // out[r] = acc
   static constexpr int kRed = 0;
   TX* out;
   const int* done;  // optional early-exit flag
+  struct pre_t {};
   __device__ bool skip() const { return done && *done; }
-  __device__ __forceinline__ void operator()(int r, double acc, red_t<0>&) const { out[r] = (TX)acc; }
+  __device__ __forceinline__ pre_t load(int) const { return pre_t{}; }
+  __device__ __forceinline__ void operator()(int r, double acc, const pre_t&, red_t<0>&) const
+  {
+    out[r] = (TX)acc;
+  }
 };
 
 // Power iteration z = A (A^T q) with q . z accumulated (reference pdlp.cu:2664-2711).
@@ -359,11 +429,15 @@ struct power_z_epi {
   double* z;
   const double* q;
   const int* done;
+  struct pre_t {
+    double q;
+  };
   __device__ bool skip() const { return *done != 0; }
-  __device__ __forceinline__ void operator()(int i, double acc, red_t<1>& r) const
+  __device__ __forceinline__ pre_t load(int i) const { return pre_t{q[i]}; }
+  __device__ __forceinline__ void operator()(int i, double acc, const pre_t& p, red_t<1>& r) const
   {
     z[i] = acc;
-    r.v[0] += q[i] * acc;
+    r.v[0] += p.q * acc;
   }
 };
 
@@ -484,8 +558,8 @@ __global__ void __launch_bounds__(kBlock) row_scaled_abs_kernel(const dev_sell<d
       const int row      = A.n_long + s * kWarp + lane;
       if (row < A.rows) {
         double acc = 0.0;
-        for (int k = 0; k < len; ++k) {
-          const int64_t p = base + (int64_t)k * 32 + lane;
+          for (int k = 0; k < len; ++k) {
+          const int64_t p = sell_pos(base, k, lane);
           const double v  = A.val[p];
           if (v == 0.0) continue;  // padding (and explicit zeros, which contribute nothing)
           const double t = term(v, row, A.idx[p]);
@@ -529,7 +603,7 @@ __global__ void __launch_bounds__(kBlock) scale_values_kernel(const dev_sell<dou
       const int len      = (int)((A.slice_off[s + 1] - base) >> 5);
       const int row      = A.n_long + s * kWarp + lane;
       for (int k = 0; k < len; ++k) {
-        const int64_t p = base + (int64_t)k * 32 + lane;
+        const int64_t p = sell_pos(base, k, lane);
         out[p]          = row < A.rows ? (TM)scaled(A.val[p], row, A.idx[p]) : (TM)0;
       }
     }

@@ -76,16 +76,17 @@ class engine {
     int dev = 0;
     B200_CUDA_CHECK(cudaGetDevice(&dev));
     B200_CUDA_CHECK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
-    B200_CUDA_CHECK(cudaMallocHost(&hres_, 64 * sizeof(double)));
+    configure_pool_once();
+    hres_ = pinned_scratch();
   }
   ~engine()
   {
     for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
-    if (hres_) cudaFreeHost(hres_);
   }
 
   pdlp_result run(double* x_out, double* y_out, double* rc_out)
   {
+    alloc_scope scope(s_);
     x_out_   = x_out;
     y_out_   = y_out;
     rc_out_  = rc_out;
@@ -622,6 +623,7 @@ class engine {
   // Times plain iterations sweep by sweep (measurement hook).
   sweep_profile profile(int iterations)
   {
+    alloc_scope scope(s_);
     t_start_ = now_s();
     setup();
     set_scalars(0);
@@ -720,6 +722,8 @@ pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p)
     cudaStream_t s;
     ~stream_guard() { cudaStreamDestroy(s); }
   } guard{s};
+  alloc_scope scope(s);
+  configure_pool_once();
   const int m = in.m, n = in.n;
   const int64_t nnz = in.row_off[m];
   dbuf<int> off(m + 1), idx(std::max<int64_t>(nnz, 1));
