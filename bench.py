@@ -45,7 +45,7 @@ CONFIGS = {
 # FP64 Stable3 iterations to 1e-6 on config 1 (the oracle and the GPU FP64 path follow the same
 # iterates; measured by the FP64 leg of this benchmark on a B200).  Used only to scale the CPU
 # per-iteration time of the reference arm into the LPs/s unit.
-FP64_ITERATIONS_C1 = None
+FP64_ITERATIONS_C1 = 1700
 
 
 def _peaks():

@@ -3,9 +3,11 @@
 
 #include <cuda_runtime.h>
 
+#include <chrono>
+#include <climits>
 #include <cstdint>
 #include <cstdio>
-#include <climits>
+#include <cstdlib>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -64,6 +66,17 @@ inline double* pinned_scratch()
   static thread_local double* p = nullptr;
   if (!p) B200_CUDA_CHECK(cudaMallocHost(&p, 64 * sizeof(double)));
   return p;
+}
+
+// Phase timing printed to stderr when the environment variable CUOPT_B200_TRACE is set.
+inline void trace(const char* what)
+{
+  static const bool on = std::getenv("CUOPT_B200_TRACE") != nullptr;
+  if (!on) return;
+  static thread_local double last = 0;
+  const double t = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  if (last > 0) std::fprintf(stderr, "[cuopt_b200] %-40s %8.3f ms\n", what, (t - last) * 1e3);
+  last = t;
 }
 
 // Device buffer owning `n` elements of T (stream-ordered allocation on alloc_stream_ref()).

@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "common.cuh"
 #include "lp_model.hpp"
 
 using cuopt_b200::lp_problem;
@@ -444,7 +445,9 @@ cuopt_int_t cuOptSolve(cuOptOptimizationProblem problem, cuOptSolverSettings set
   if (!problem || !settings || !solution_ptr) return CUOPT_INVALID_ARGUMENT;
   auto* sol = new (std::nothrow) lp_solution();
   if (!sol) return CUOPT_OUT_OF_MEMORY;
+  cuopt_b200::trace("cuOptSolve: enter");
   *sol          = cuopt_b200::solve_problem(*P(problem), *S(settings));
+  cuopt_b200::trace("cuOptSolve: solve_problem");
   *solution_ptr = sol;
   return sol->error_code;
 }

@@ -371,6 +371,7 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
 {
   lp_solution out;
   const auto t0 = std::chrono::steady_clock::now();
+  trace("solve_problem: start");
   try {
     if (p.quadratic) {
       out.error_code    = CUOPT_VALIDATION_ERROR;
@@ -388,6 +389,7 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
       out.error_message = err;
       return out;
     }
+    trace("validate_problem");
     std::vector<double> lo, up;
     p.constraint_bounds(lo, up);
     // has_crossing_bounds (reference problem_checking.cu:316-339)
@@ -433,7 +435,9 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
     in.var_up     = p.var_up.data();
     in.obj_offset = p.obj_offset;
     in.maximize   = p.maximize;
+    trace("constraint bounds + checks");
     out.r         = pdlp_solve(in, prm);
+    trace("pdlp_solve");
     if (prm.log_to_console)
       std::printf("PDLP status %d  objective %+.10e  iterations %lld  time %.3fs\n", out.r.status,
                   out.r.primal_obj, (long long)out.r.iterations, out.r.solve_time);

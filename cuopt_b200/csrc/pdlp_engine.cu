@@ -110,7 +110,10 @@ class engine {
   void setup()
   {
     const int m = in_.m, n = in_.n;
+    trace("engine: start");
     build_device_layout(m, n, in_.row_off, in_.col_idx, in_.val, s_, L_);
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    trace("engine: layout");
     vgrid_ = sms_ * 4;
     const int g = std::max({sell_grid(view64(L_.A)), sell_grid(view64(L_.AT)), vgrid_});
     partials_.resize((size_t)g * 4);
@@ -184,8 +187,11 @@ class engine {
       ls_.data(), us_.data(), lcs_.data(), ucs_.data());
     B200_LAUNCH_CHECK();
 
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    trace("engine: scaling");
     // Step size from the largest singular value of the scaled A (reference pdlp.cu:2620-2731).
     power_iteration();
+    trace("engine: power iteration");
     omega_      = 1.0;  // bound_objective_rescaling => primal weight 1 (pdlp.cu:2799-2810)
     best_omega_ = 1.0;
 
@@ -760,7 +766,9 @@ pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p)
     id.upload(p.initial_dual.data(), m, s);
     d.initial_dual = id.data();
   }
+  trace("host path: upload");
   pdlp_result r = pdlp_solve_device(d, p, s, x.data(), y.data(), rc.data());
+  trace("host path: device solve");
   if (r.status != kNumericalError || r.iterations > 0) {
     r.x.resize(n);
     r.y.resize(m);
