@@ -11,8 +11,10 @@
 #include <cstring>
 #include <limits>
 #include <new>
+#include <algorithm>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -26,21 +28,44 @@ namespace {
 
 constexpr int kVersionMajor = 26, kVersionMinor = 4, kVersionPatch = 0;
 
+// Parallel host copy for large arrays (problem creation copies the user's arrays).
+void parallel_memcpy(void* dst, const void* src, size_t bytes)
+{
+  constexpr size_t kChunk = size_t(16) << 20;
+  const unsigned hw       = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  if (bytes < 2 * kChunk || hw == 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < hw; ++t) {
+    const size_t lo = bytes * t / hw, hi = bytes * (t + 1) / hw;
+    pool.emplace_back([=] {
+      std::memcpy(static_cast<char*>(dst) + lo, static_cast<const char*>(src) + lo, hi - lo);
+    });
+  }
+  for (auto& th : pool) th.join();
+}
+
 // Copies n elements from a host or device pointer (the reference accepts both).
 template <typename T>
 void copy_in(std::vector<T>& dst, const T* src, size_t n)
 {
-  dst.resize(n);
-  if (n == 0) return;
+  if (n == 0) {
+    dst.clear();
+    return;
+  }
   cudaPointerAttributes attr{};
   if (cudaPointerGetAttributes(&attr, src) == cudaSuccess &&
       (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged)) {
+    dst.resize(n);
     if (cudaMemcpy(dst.data(), src, n * sizeof(T), cudaMemcpyDefault) != cudaSuccess)
       throw std::invalid_argument("cannot read device array");
     return;
   }
   cudaGetLastError();  // clear a "no device" / "invalid value" answer for plain host memory
-  std::memcpy(dst.data(), src, n * sizeof(T));
+  dst.resize(n);
+  parallel_memcpy(dst.data(), src, n * sizeof(T));
 }
 
 template <typename T>

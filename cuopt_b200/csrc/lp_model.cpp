@@ -294,9 +294,8 @@ std::string validate_problem(const lp_problem& p)
   const int64_t nnz = p.row_off[p.m];
   if ((int64_t)p.col_idx.size() != nnz || (int64_t)p.val.size() != nnz)
     return "A_index and A_values must have same sizes.";
-  for (int64_t k = 0; k < nnz; ++k)
-    if (p.col_idx[k] < 0 || p.col_idx[k] >= p.n)
-      return "A_indices values must positive lower than the number of variables (c size).";
+  // Column indices are range-checked on the device while the matrix layout is built
+  // (a violation is reported as CUOPT_VALIDATION_ERROR by cuOptSolve).
   if ((int)p.c.size() != p.n) return "c must be set before calling the solver.";
   if ((int)p.var_lo.size() != p.n || (int)p.var_up.size() != p.n)
     return "Sizes for vectors related to the variables are not the same.";
