@@ -127,7 +127,7 @@ def make_lp(cfg: str):
     return gen.constructed_lp(m, n, k, seed=seed, name=cfg)
 
 
-def settings_handle(L, tol, precision, iteration_limit=None):
+def settings_handle(L, tol, precision, iteration_limit=None, refine_passes=0, refine_tol=1e-8):
     h = C.c_void_p()
     assert L.cuOptCreateSolverSettings(C.byref(h)) == 0
     for name in ("absolute_primal_tolerance", "relative_primal_tolerance", "absolute_dual_tolerance",
@@ -138,6 +138,9 @@ def settings_handle(L, tol, precision, iteration_limit=None):
     assert L.cuOptSetParameter(h, b"log_to_console", b"false") == 0
     if iteration_limit is not None:
         assert L.cuOptSetIntegerParameter(h, b"iteration_limit", int(iteration_limit)) == 0
+    if refine_passes:
+        assert L.cuOptSetIntegerParameter(h, b"pdlp_refinement_passes", int(refine_passes)) == 0
+        assert L.cuOptSetFloatParameter(h, b"pdlp_refinement_tolerance", float(refine_tol)) == 0
     return h
 
 
@@ -310,6 +313,23 @@ def run_b200(args):
             "speedup_mixed_vs_fp64": ms_fp64 / ms_mixed,
         }
 
+    # Mixed precision followed by FP64 iterative refinement to 1e-8 relative KKT
+    refine = None
+    if not args.no_refine:
+        s_ref = settings_handle(L, tol, 1, refine_passes=8, refine_tol=1e-8)
+        ms_ref, st_ref, _ = timed(s_ref, 1, 1)
+        L.cuOptDestroySolverSettings(C.byref(s_ref))
+        status_ref, last_ref = st_ref[-1]
+        kkt_ref = gen.kkt_relative_error(lp, dlp.x.cpu().numpy(), dlp.y.cpu().numpy())
+        refine = {"ms_per_solve": ms_ref, "status": status_ref,
+                  "iterations": last_ref["number_of_steps_taken"],
+                  "refinement_passes": last_ref["refinement_passes"],
+                  "rel_primal": last_ref["l2_relative_primal_residual"],
+                  "rel_dual": last_ref["l2_relative_dual_residual"],
+                  "rel_gap": last_ref["relative_gap"], "kkt_check": kkt_ref,
+                  "objective_rel_error": abs(last_ref["primal_objective"] - lp.optimal_objective)
+                  / abs(lp.optimal_objective)}
+
     # Roofline of the dominant fused sweep (mixed precision = the headline path)
     prof = {}
     for prec, name in ((1, "mixed"), (0, "fp64")):
@@ -381,6 +401,7 @@ def run_b200(args):
         "pdhg_iter_per_s": last_mixed["number_of_steps_taken"] / (last_mixed["loop_time"] or 1e-9),
         "setup_s": last_mixed["setup_time"], "loop_s": last_mixed["loop_time"],
         "objective_rel_error": obj_err_mixed, "kkt": kkt_mixed, "fp64": fp64,
+        "mixed_refined_to_1e-8": refine,
         "roofline": roofline, "cpu_baseline": cpu,
         "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "LPs/s to 1e-6 rel. KKT",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
@@ -410,6 +431,7 @@ def main():
     ap.add_argument("--cpu-iterations", type=int, default=0)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-refine", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -105,7 +105,7 @@ lp_settings::lp_settings()
     {CUOPT_MIP_RELIABILITY_BRANCHING, -1, INT_MAX, -1},
     {CUOPT_PDLP_PRECISION, CUOPT_PDLP_PRECISION_FP64, CUOPT_PDLP_PRECISION_MIXED,
      CUOPT_PDLP_PRECISION_FP64},
-    {CUOPT_PDLP_REFINEMENT_PASSES, 0, 64, 4},
+    {CUOPT_PDLP_REFINEMENT_PASSES, 0, 64, 0},
   };
   bparams = {
     {CUOPT_INFEASIBILITY_DETECTION, false}, {CUOPT_STRICT_INFEASIBILITY, false},

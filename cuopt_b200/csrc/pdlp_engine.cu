@@ -102,6 +102,9 @@ class engine {
     }
     t_loop_ = now_s();
     loop(r);
+    if (p_.precision == 1 && p_.refinement_passes > 0 && r.status == kOptimal) refine(r);
+    write_outputs();
+    finish_times(r);
     return r;
   }
 
@@ -135,10 +138,6 @@ class engine {
     permute_gather(in_.con_lo, L_.row_new2old.data(), m, 1.0, lc64_.data(), s_);
     permute_gather(in_.con_up, L_.row_new2old.data(), m, 1.0, uc64_.data(), s_);
 
-    // Constant norms of the unscaled problem (reference convergence_information.cu:92-106).
-    c_norm_ = std::sqrt(reduce<0>(c64_.data(), (const double*)nullptr, n));
-    b_norm_ = std::sqrt(reduce<2>(lc64_.data(), uc64_.data(), m));
-
     // Ruiz (10 passes) then Pock-Chambolle (alpha = 1) (reference initial_scaling.cu:152-365).
     dr_.resize(m);
     dc_.resize(n);
@@ -169,7 +168,29 @@ class engine {
     scale_values_kernel<TX, true><<<sell_grid(view64(L_.AT)), kBlock, 0, s_>>>(
       view64(L_.AT), dr_.data(), dc_.data(), ATs_.data());
 
-    // Scaled vectors, then bound / objective rescaling (reference initial_scaling.cu:95-149, 417-569).
+    prepare_vectors();
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    trace("engine: scaling");
+    // Step size from the largest singular value of the scaled A (reference pdlp.cu:2620-2731).
+    power_iteration();
+    trace("engine: power iteration");
+
+    xu_.resize(n);
+    su_.resize(n);
+    yu_.resize(m);
+    scalars_.resize(1);
+    reset_iterates(true);
+  }
+
+  // Norms of the unscaled vectors and their scaled copies in the iterate precision (bound /
+  // objective rescaling recomputed, reference initial_scaling.cu:95-149, 417-569).  Called once
+  // for the LP and once per refinement pass for the correction LP; the matrix scaling is shared.
+  void prepare_vectors()
+  {
+    const int m = in_.m, n = in_.n;
+    // Constant norms of the unscaled problem (reference convergence_information.cu:92-106).
+    c_norm_ = std::sqrt(reduce<0>(c64_.data(), (const double*)nullptr, n));
+    b_norm_ = std::sqrt(reduce<2>(lc64_.data(), uc64_.data(), m));
     dbuf<double> cs(n), ls(n), us(n), lcs(m), ucs(m);
     scale_vectors_kernel<<<vgrid_, kBlock, 0, s_>>>(c64_.data(), l64_.data(), u64_.data(),
                                                     lc64_.data(), uc64_.data(), dc_.data(),
@@ -185,17 +206,18 @@ class engine {
     rescale_vectors_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(
       cs.data(), ls.data(), us.data(), lcs.data(), ucs.data(), beta_, gamma_, n, m, cs_.data(),
       ls_.data(), us_.data(), lcs_.data(), ucs_.data());
+    launches_ += 2;
     B200_LAUNCH_CHECK();
-
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
-    trace("engine: scaling");
-    // Step size from the largest singular value of the scaled A (reference pdlp.cu:2620-2731).
-    power_iteration();
-    trace("engine: power iteration");
+  }
+
+  // Zeroed iterates (plus the caller's initial solution on the first solve), projected primal.
+  void reset_iterates(bool with_initial)
+  {
+    const int m = in_.m, n = in_.n;
     omega_      = 1.0;  // bound_objective_rescaling => primal weight 1 (pdlp.cu:2799-2810)
     best_omega_ = 1.0;
-
-    // Iterates (internal order, scaled).
+    restarts_   = 0;
     for (auto* b : {&x_, &xhat_, &slack_, &xbar_, &xa_, &aty_}) {
       b->resize(n);
       b->zero(s_);
@@ -204,13 +226,10 @@ class engine {
       b->resize(m);
       b->zero(s_);
     }
-    xu_.resize(n);
-    su_.resize(n);
-    yu_.resize(m);
-    if (in_.initial_primal || in_.initial_dual) load_initial_solution();
+    if (with_initial && (in_.initial_primal || in_.initial_dual)) load_initial_solution();
     // project_initial_primal (reference pdlp.cu:2237-2262): only the current primal iterate.
     clamp_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(x_.data(), ls_.data(), us_.data(), n);
-    scalars_.resize(1);
+    ++launches_;
     B200_LAUNCH_CHECK();
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
   }
@@ -394,6 +413,13 @@ class engine {
                                                   dc_.data(), dr_.data(), 1.0 / beta_,
                                                   1.0 / gamma_, n, m, xu_.data(), yu_.data(),
                                                   su_.data());
+    ++launches_;
+    return evaluate_unscaled();
+  }
+
+  // Residuals and objectives of (xu_, yu_, su_) on the unscaled problem (c64_, lc64_, uc64_).
+  conv_info evaluate_unscaled()
+  {
     const auto A = view64(L_.A), AT = view64(L_.AT);
     sell_map_kernel<double, double, term_primal_epi><<<sell_grid(A), kBlock, 0, s_>>>(
       A, xu_.data(), term_primal_epi{lc64_.data(), uc64_.data(), yu_.data()}, partials_.data());
@@ -402,7 +428,7 @@ class engine {
       AT, yu_.data(), term_dual_epi{c64_.data(), xu_.data(), su_.data()}, partials_.data());
     finalize_sum_kernel<3><<<1, kBlock, 0, s_>>>(partials_.data(), sell_grid(AT),
                                                  dres_.data() + 2);
-    launches_ += 5;
+    launches_ += 4;
     B200_LAUNCH_CHECK();
     B200_CUDA_CHECK(
       cudaMemcpyAsync(hres_, dres_.data(), 5 * sizeof(double), cudaMemcpyDeviceToHost, s_));
@@ -423,7 +449,6 @@ class engine {
 
   void finish(pdlp_result& r, int status, const conv_info& cv, long k)
   {
-    const int m = in_.m, n = in_.n;
     r.status     = status;
     r.iterations = k;
     r.primal_obj = cv.primal_obj;
@@ -438,12 +463,121 @@ class engine {
     r.primal_weight = omega_;
     r.restarts   = restarts_;
     r.kernel_launches = launches_;
-    const double sgn = in_.maximize ? -1.0 : 1.0;  // reference solve.cu:584-588
+  }
+
+  bool meets(const conv_info& cv, double tol) const
+  {
+    return cv.l2_primal <= tol + tol * b_norm_ && cv.l2_dual <= tol + tol * c_norm_ &&
+           cv.gap <= tol + tol * cv.abs_obj;
+  }
+  static double rel_kkt(const conv_info& cv, double bn, double cn)
+  {
+    return std::max({cv.l2_primal / (1.0 + bn), cv.l2_dual / (1.0 + cn), cv.gap / (1.0 + cv.abs_obj)});
+  }
+
+  void copy_d(double* dst, const double* src, int n)
+  {
+    B200_CUDA_CHECK(cudaMemcpyAsync(dst, src, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+  }
+
+  // FP64 iterative refinement of a mixed-precision solution (x, y, s).  The correction LP
+  //   min (dd (c - A^T y))^T z   s.t.  dp (lc - A x) <= A z <= dp (uc - A x),  dp (l - x) <= z <= dp (u - x)
+  // has the same matrix, so the layout, the Ruiz / Pock-Chambolle scaling and the step size are
+  // reused; only the vectors are rebuilt.  Its solution (z, w, s_w) gives x += z / dp,
+  // y += w / dd, s = s_w / dd, with dp, dd the inverse primal / dual residual norms of the current
+  // point.  Passes stop once the original LP meets `refinement_tol`; a pass that does not improve
+  // the relative KKT error is discarded.
+  void refine(pdlp_result& r)
+  {
+    const int m = in_.m, n = in_.n;
+    dbuf<double> c0(n), l0(n), u0(n), lc0(m), uc0(m), X(n), Y(m), S(n), AX(m), ATY(n);
+    dbuf<double> Xb(n), Yb(m), Sb(n);
+    copy_d(c0.data(), c64_.data(), n);
+    copy_d(l0.data(), l64_.data(), n);
+    copy_d(u0.data(), u64_.data(), n);
+    copy_d(lc0.data(), lc64_.data(), m);
+    copy_d(uc0.data(), uc64_.data(), m);
+    copy_d(X.data(), xu_.data(), n);
+    copy_d(Y.data(), yu_.data(), m);
+    copy_d(S.data(), su_.data(), n);
+    const double scale0 = obj_scale_, offset0 = obj_offset_, cn0 = c_norm_, bn0 = b_norm_;
+    const double tol = p_.refinement_tol;
+    const auto A = view64(L_.A), AT = view64(L_.AT);
+    long total = r.iterations;
+    int passes = 0;
+    conv_info cv = evaluate_unscaled();
+    double best  = rel_kkt(cv, bn0, cn0);
+    while (passes < p_.refinement_passes && !meets(cv, tol) && now_s() - t_start_ < p_.time_limit) {
+      const double dp = std::min(std::max(1.0 / std::max(cv.l2_primal, 1e-300), 1.0), 1e12);
+      const double dd = std::min(std::max(1.0 / std::max(cv.l2_dual, 1e-300), 1.0), 1e12);
+      sell_map_kernel<double, double, store_epi<double>><<<sell_grid(A), kBlock, 0, s_>>>(
+        A, X.data(), store_epi<double>{AX.data(), nullptr}, partials_.data());
+      sell_map_kernel<double, double, store_epi<double>><<<sell_grid(AT), kBlock, 0, s_>>>(
+        AT, Y.data(), store_epi<double>{ATY.data(), nullptr}, partials_.data());
+      refine_vectors_kernel<<<vgrid_, kBlock, 0, s_>>>(
+        c0.data(), l0.data(), u0.data(), lc0.data(), uc0.data(), X.data(), AX.data(), ATY.data(),
+        dp, dd, n, m, c64_.data(), l64_.data(), u64_.data(), lc64_.data(), uc64_.data());
+      launches_ += 3;
+      B200_LAUNCH_CHECK();
+      obj_scale_  = 1.0;
+      obj_offset_ = 0.0;
+      prepare_vectors();
+      reset_iterates(false);
+      pdlp_result rr;
+      loop(rr);
+      total += rr.iterations;
+      ++passes;
+      // candidate = current + correction
+      copy_d(Xb.data(), X.data(), n);
+      copy_d(Yb.data(), Y.data(), m);
+      copy_d(Sb.data(), S.data(), n);
+      refine_update_kernel<<<vgrid_, kBlock, 0, s_>>>(Xb.data(), Yb.data(), Sb.data(), xu_.data(),
+                                                      yu_.data(), su_.data(), dp, dd, n, m);
+      ++launches_;
+      // evaluate the candidate on the original LP
+      copy_d(c64_.data(), c0.data(), n);
+      copy_d(l64_.data(), l0.data(), n);
+      copy_d(u64_.data(), u0.data(), n);
+      copy_d(lc64_.data(), lc0.data(), m);
+      copy_d(uc64_.data(), uc0.data(), m);
+      obj_scale_  = scale0;
+      obj_offset_ = offset0;
+      c_norm_     = cn0;
+      b_norm_     = bn0;
+      copy_d(xu_.data(), Xb.data(), n);
+      copy_d(yu_.data(), Yb.data(), m);
+      copy_d(su_.data(), Sb.data(), n);
+      const conv_info cand = evaluate_unscaled();
+      const double err     = rel_kkt(cand, bn0, cn0);
+      if (!(err < best)) break;  // no improvement: keep the previous point
+      best = err;
+      cv   = cand;
+      copy_d(X.data(), Xb.data(), n);
+      copy_d(Y.data(), Yb.data(), m);
+      copy_d(S.data(), Sb.data(), n);
+    }
+    // final point on the original LP
+    copy_d(xu_.data(), X.data(), n);
+    copy_d(yu_.data(), Y.data(), m);
+    copy_d(su_.data(), S.data(), n);
+    c_norm_ = cn0;
+    b_norm_ = bn0;
+    const long keep_iters = total;
+    finish(r, kOptimal, cv, keep_iters);
+    r.refinement_passes = passes;
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+  }
+
+  // Solution in the user's order; duals and reduced costs negated for maximisation
+  // (reference solve.cu:584-588).
+  void write_outputs()
+  {
+    const int m = in_.m, n = in_.n;
+    const double sgn = in_.maximize ? -1.0 : 1.0;
     if (x_out_) permute_scatter(xu_.data(), L_.col_new2old.data(), n, 1.0, x_out_, s_);
     if (rc_out_) permute_scatter(su_.data(), L_.col_new2old.data(), n, sgn, rc_out_, s_);
     if (y_out_) permute_scatter(yu_.data(), L_.row_new2old.data(), m, sgn, y_out_, s_);
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
-    finish_times(r);
   }
 
   void finish_times(pdlp_result& r)

@@ -35,7 +35,7 @@ struct pdlp_params {
   int64_t iteration_limit = 2147483647;
   double time_limit       = 1e300;
   int precision           = 0;  // 0 FP64, 1 mixed FP32/FP64
-  int refinement_passes   = 4;
+  int refinement_passes   = 0;
   double refinement_tol   = 1e-8;
   bool log_to_console     = false;
   std::vector<double> initial_primal;  // user order, optional

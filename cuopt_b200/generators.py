@@ -11,7 +11,7 @@ So c.x* is the optimal objective.  Random numbers come from numpy's PCG64 seeded
 Workloads (sizes are parameters so the tests can run them small):
   constructed_lp   config 0 / 1 / 4: equality rows, [0, 10] bounds, k non-zeros per column at
                    uniform rows, N(0,1) values; 30% of x* at 0, the rest U(0.5, 5).
-  skewed_lp        config 2: Zipf(1.3) row lengths capped at 5000, uniform columns, log-uniform
+  skewed_lp        config 2: Zipf(1.3) row lengths on [1, 5000], uniform columns, log-uniform
                    magnitudes in [1e-3, 1e3] with random signs, 50% 'E' / 50% 'L' rows
                    (the slack of an 'L' row is implicit), bounds [0, U(1,100)], 10% free columns.
   batch_lps        config 3: many config-0 LPs with m log-uniform in [200, 20000], n = 2.5 m,
@@ -105,20 +105,35 @@ def constructed_lp(m: int, n: int, nnz_per_col: int = 8, seed: int = 0, upper: f
     return lp
 
 
+def _truncated_zipf(rng: np.random.Generator, a: float, cap: int, size: int) -> np.ndarray:
+    """Samples of P(k) proportional to k^-a on k = 1..cap (mean 150.8 for a = 1.3, cap = 5000)."""
+    k = np.arange(1, cap + 1, dtype=np.float64)
+    cdf = np.cumsum(k ** -a)
+    cdf /= cdf[-1]
+    return np.searchsorted(cdf, rng.random(size), side="right").astype(np.int64) + 1
+
+
 def skewed_lp(m: int, n: int, seed: int = 2000, zipf_a: float = 1.3, cap: int = 5000,
               name: str = "skewed") -> LP:
-    """Config-2 generator (row lengths Zipf(a) capped, mixed senses, free columns)."""
+    """Config-2 generator (row lengths Zipf(a) on [1, cap], mixed senses, free columns)."""
     rng = np.random.default_rng(seed)
-    lens = np.minimum(rng.zipf(zipf_a, size=m), min(cap, n)).astype(np.int64)
+    lens = np.minimum(_truncated_zipf(rng, zipf_a, cap, m), n)
     rows = np.repeat(np.arange(m, dtype=np.int64), lens)
-    cols = rng.integers(0, n, size=int(lens.sum()), dtype=np.int64)
-    # drop duplicate (row, col) pairs
-    key = rows * n + cols
-    key, first = np.unique(key, return_index=True)
-    rows, cols = rows[first], cols[first]
+    key = rows * n + rng.integers(0, n, size=int(lens.sum()), dtype=np.int64)
+    del rows
+    key.sort()
+    keep = np.ones(key.size, dtype=bool)
+    keep[1:] = key[1:] != key[:-1]  # drop duplicate (row, column) pairs
+    key = key[keep]
+    rows, cols = key // n, key % n
+    del key
     mag = 10.0 ** rng.uniform(-3.0, 3.0, size=rows.size)
     sign = np.where(rng.random(rows.size) < 0.5, -1.0, 1.0)
-    row_off, col_idx, val = _csr_from_columns(m, n, rows, cols, mag * sign)
+    counts = np.bincount(rows, minlength=m)
+    row_off = np.zeros(m + 1, dtype=np.int64)
+    np.cumsum(counts, out=row_off[1:])
+    row_off, col_idx, val = row_off.astype(np.int32), cols.astype(np.int32), mag * sign
+    del rows, cols
     ub = rng.uniform(1.0, 100.0, size=n)
     lb = np.zeros(n)
     free = rng.random(n) < 0.1

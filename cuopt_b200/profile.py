@@ -21,9 +21,12 @@ if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
 CONFIGS = {
+    # name: (m, n, non-zeros per column (0: skewed generator), seed)
     "c0": (2_000, 5_000, 8, 0),
     "c1": (1_000_000, 2_000_000, 8, 1000),
     "c1_small": (750_000, 1_500_000, 8, 1000),
+    "c2": (500_000, 1_500_000, 0, 2000),
+    "c2_small": (50_000, 150_000, 0, 2000),
     "c4": (5_000, 10_000, 8, 4000),
 }
 
@@ -41,10 +44,12 @@ def main() -> None:
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--iterations", type=int, default=3)
     ap.add_argument("--tol", type=float, default=1e-6)
+    ap.add_argument("--time-limit", type=float, default=0.0)
+    ap.add_argument("--refine", type=int, default=0, help="FP64 refinement passes (mixed precision)")
     a = ap.parse_args()
 
     m, n, k, seed = CONFIGS[a.config]
-    lp = gen.constructed_lp(m, n, k, seed=seed)
+    lp = gen.constructed_lp(m, n, k, seed=seed) if k else gen.skewed_lp(m, n, seed=seed)
     dev = torch.device("cuda", 0)
     t = lambda x, dt: torch.as_tensor(np.ascontiguousarray(x), device=dev, dtype=dt)
     arrs = [t(lp.c, torch.float64), t(lp.row_off, torch.int32), t(lp.col_idx, torch.int32),
@@ -59,6 +64,10 @@ def main() -> None:
         L.cuOptSetFloatParameter(s, name.encode(), a.tol)
     L.cuOptSetIntegerParameter(s, b"pdlp_precision", 1 if a.precision == "mixed" else 0)
     L.cuOptSetParameter(s, b"log_to_console", b"false")
+    if a.time_limit > 0:
+        L.cuOptSetFloatParameter(s, b"time_limit", a.time_limit)
+    if a.refine:
+        L.cuOptSetIntegerParameter(s, b"pdlp_refinement_passes", a.refine)
     stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
     out = {"config": a.config, "m": m, "n": n, "nnz": lp.nnz, "precision": a.precision, "mode": a.mode}
     if a.mode == "solve":
@@ -73,6 +82,8 @@ def main() -> None:
         torch.cuda.synchronize()
         out.update({"rc": code, "status": status.value, "wall_s": time.perf_counter() - t0})
         out.update({f: getattr(st, f) for f, _ in PDLPStatistics._fields_})
+        out["objective_rel_error"] = abs(st.primal_objective - lp.optimal_objective) / max(
+            1.0, abs(lp.optimal_objective))
         if code != 0:
             print(json.dumps(out))
             sys.exit(1)

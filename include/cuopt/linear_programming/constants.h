@@ -81,8 +81,9 @@
 /* Parameters added by this library (no counterpart in the reference).  "pdlp_precision" picks the
  * arithmetic of the PDHG iterations: 0 = FP64 throughout (the reference's behaviour, default),
  * 1 = mixed (FP32 matrix and iterates, FP64 termination/restart/step ratio, FP64 refinement).
- * "pdlp_refinement_passes" bounds the number of FP64 iterative-refinement passes of the mixed mode.
- * "pdlp_refinement_tolerance" is the relative KKT target of the refinement passes. */
+ * "pdlp_refinement_passes" (default 0 = off) bounds the number of FP64 iterative-refinement passes
+ * applied after a mixed-precision solve reached its tolerances; "pdlp_refinement_tolerance"
+ * (default 1e-8) is the tolerance the refinement passes aim for on the original LP. */
 #define CUOPT_PDLP_PRECISION            "pdlp_precision"
 #define CUOPT_PDLP_REFINEMENT_PASSES    "pdlp_refinement_passes"
 #define CUOPT_PDLP_REFINEMENT_TOLERANCE "pdlp_refinement_tolerance"

@@ -139,3 +139,20 @@ def test_mixed_precision_reaches_tolerance(small_lp):
     sol = lpm.Solve(datamodel_from_lp(small_lp), settings(tol=1e-4, precision=1))
     assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
     assert rel(sol.get_primal_objective(), small_lp.optimal_objective) <= 1e-3
+
+
+def test_mixed_precision_refinement_reaches_1e8():
+    """Mixed precision to 1e-6, then FP64 iterative refinement to 1e-8 on the original LP."""
+    lp = gen.constructed_lp(2000, 5000, 8, seed=0)
+    s = settings(tol=1e-6, precision=1)
+    s.set_parameter(lpm.CUOPT_PDLP_REFINEMENT_PASSES, 8)
+    s.set_parameter(lpm.CUOPT_PDLP_REFINEMENT_TOLERANCE, 1e-8)
+    sol = lpm.Solve(datamodel_from_lp(lp), s)
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    st = sol.stats
+    assert st["refinement_passes"] >= 1
+    assert max(st["l2_relative_primal_residual"], st["l2_relative_dual_residual"],
+               st["relative_gap"]) <= 1e-8
+    kkt = gen.kkt_relative_error(lp, sol.get_primal_solution(), sol.get_dual_solution())
+    assert kkt["rel_primal"] <= 1e-8 and kkt["rel_gap"] <= 1e-8
+    assert rel(sol.get_primal_objective(), lp.optimal_objective) <= 1e-8
