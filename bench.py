@@ -127,7 +127,8 @@ def make_lp(cfg: str):
     return gen.constructed_lp(m, n, k, seed=seed, name=cfg)
 
 
-def settings_handle(L, tol, precision, iteration_limit=None, refine_passes=0, refine_tol=1e-8):
+def settings_handle(L, tol, precision, iteration_limit=None, refine_passes=0, refine_tol=1e-8,
+                    time_limit=None):
     h = C.c_void_p()
     assert L.cuOptCreateSolverSettings(C.byref(h)) == 0
     for name in ("absolute_primal_tolerance", "relative_primal_tolerance", "absolute_dual_tolerance",
@@ -138,6 +139,8 @@ def settings_handle(L, tol, precision, iteration_limit=None, refine_passes=0, re
     assert L.cuOptSetParameter(h, b"log_to_console", b"false") == 0
     if iteration_limit is not None:
         assert L.cuOptSetIntegerParameter(h, b"iteration_limit", int(iteration_limit)) == 0
+    if time_limit is not None:
+        assert L.cuOptSetFloatParameter(h, b"time_limit", float(time_limit)) == 0
     if refine_passes:
         assert L.cuOptSetIntegerParameter(h, b"pdlp_refinement_passes", int(refine_passes)) == 0
         assert L.cuOptSetFloatParameter(h, b"pdlp_refinement_tolerance", float(refine_tol)) == 0
@@ -316,7 +319,7 @@ def run_b200(args):
     # Mixed precision followed by FP64 iterative refinement to 1e-8 relative KKT
     refine = None
     if not args.no_refine:
-        s_ref = settings_handle(L, tol, 1, refine_passes=8, refine_tol=1e-8)
+        s_ref = settings_handle(L, tol, 1, refine_passes=8, refine_tol=1e-8, time_limit=20.0)
         ms_ref, st_ref, _ = timed(s_ref, 1, 1)
         L.cuOptDestroySolverSettings(C.byref(s_ref))
         status_ref, last_ref = st_ref[-1]

@@ -71,7 +71,8 @@ struct conv_info {
 template <typename TX>
 class engine {
  public:
-  engine(const lp_device_input& in, const pdlp_params& p, cudaStream_t s) : in_(in), p_(p), s_(s)
+  engine(const lp_device_input& in, const pdlp_params& p, cudaStream_t s)
+    : in_(in), p_(p), s_(s), iteration_limit_(p.iteration_limit)
   {
     int dev = 0;
     B200_CUDA_CHECK(cudaGetDevice(&dev));
@@ -507,7 +508,14 @@ class engine {
     int passes = 0;
     conv_info cv = evaluate_unscaled();
     double best  = rel_kkt(cv, bn0, cn0);
-    while (passes < p_.refinement_passes && !meets(cv, tol) && now_s() - t_start_ < p_.time_limit) {
+    // Each correction solve gets at most 4x the first solve's iterations (plus 1000), within what
+    // is left of the caller's iteration and time limits; a correction solve that stops on that
+    // budget still yields a candidate, but ends the refinement.
+    const long user_limit = p_.iteration_limit;
+    const long pass_cap   = 4 * (long)r.iterations + 1000;
+    bool more             = true;
+    while (more && passes < p_.refinement_passes && !meets(cv, tol) &&
+           now_s() - t_start_ < p_.time_limit && total < user_limit) {
       const double dp = std::min(std::max(1.0 / std::max(cv.l2_primal, 1e-300), 1.0), 1e12);
       const double dd = std::min(std::max(1.0 / std::max(cv.l2_dual, 1e-300), 1.0), 1e12);
       sell_map_kernel<double, double, store_epi<double>><<<sell_grid(A), kBlock, 0, s_>>>(
@@ -524,7 +532,10 @@ class engine {
       prepare_vectors();
       reset_iterates(false);
       pdlp_result rr;
+      iteration_limit_ = std::min(pass_cap, user_limit - total);
       loop(rr);
+      iteration_limit_ = user_limit;
+      more             = rr.status == kOptimal;
       total += rr.iterations;
       ++passes;
       // candidate = current + correction
@@ -618,7 +629,7 @@ class engine {
                       cv.dual_obj, cv.gap, cv.l2_primal, cv.l2_dual, now_s() - t_start_);
         if (k > 1 && status == kOptimal) return finish(r, kOptimal, cv, k);
         if (now_s() - t_start_ >= p_.time_limit) return finish(r, kTimeLimit, cv, k);
-        if (k >= p_.iteration_limit) return finish(r, kIterationLimit, cv, k);
+        if (k >= iteration_limit_) return finish(r, kIterationLimit, cv, k);
         if (!std::isfinite(cv.l2_primal) || !std::isfinite(cv.l2_dual))
           return finish(r, kNumericalError, cv, k);
 
@@ -738,6 +749,7 @@ class engine {
   const lp_device_input& in_;
   const pdlp_params& p_;
   cudaStream_t s_ = nullptr;
+  long iteration_limit_;  // limit of the running loop (lowered for correction solves)
   double *x_out_ = nullptr, *y_out_ = nullptr, *rc_out_ = nullptr;
   int sms_ = 148, vgrid_ = 592;
   double* hres_ = nullptr;

@@ -156,3 +156,52 @@ def test_mixed_precision_refinement_reaches_1e8():
     kkt = gen.kkt_relative_error(lp, sol.get_primal_solution(), sol.get_dual_solution())
     assert kkt["rel_primal"] <= 1e-8 and kkt["rel_gap"] <= 1e-8
     assert rel(sol.get_primal_objective(), lp.optimal_objective) <= 1e-8
+
+
+def _transposed_lp(lp, seed):
+    """An LP whose matrix is lp's transpose, so that long rows become long columns (A^T sweeps)."""
+    import scipy.sparse as sp
+    rng = np.random.default_rng(seed)
+    a = sp.csr_matrix((lp.val, lp.col_idx, lp.row_off), shape=(lp.m, lp.n)).T.tocsr()
+    a.sort_indices()
+    m, n = a.shape
+    x0 = rng.uniform(-1.0, 1.0, n)
+    ax = a @ x0
+    eq = rng.random(m) < 0.4
+    lo = np.where(eq, ax, ax - rng.uniform(0.0, 1.0, m))
+    up = np.where(eq, ax, np.where(rng.random(m) < 0.5, np.inf, ax + rng.uniform(0.0, 1.0, m)))
+    vlo = np.where(rng.random(n) < 0.1, -np.inf, -2.0)
+    vup = np.where(np.isinf(vlo), np.inf, 2.0)
+    return gen.LP(m, n, a.indptr.astype(np.int32), a.indices.astype(np.int32), a.data.copy(),
+                  rng.standard_normal(n), lo, up, vlo, vup, x0, np.zeros(m), np.zeros(n), "transposed")
+
+
+@pytest.mark.parametrize("transpose", [False, True])
+def test_long_rows_and_columns_match_oracle(transpose):
+    """Rows (or, transposed, columns) of up to ~1800 elements take the long-row path of the sweeps
+    (one warp per row); the iterates still match the oracle after 10, 200 and 400 iterations."""
+    lp = gen.skewed_lp(400, 3000, seed=7, cap=3000)
+    if transpose:
+        lp = _transposed_lp(lp, seed=8)
+    lens = np.diff(lp.row_off) if not transpose else np.bincount(lp.col_idx, minlength=lp.n)
+    assert lens.max() > 4 * 256
+    dm = datamodel_from_lp(lp)
+    for k in (10, 200, 400):
+        sol = lpm.Solve(dm, settings(tol=1e-12, iteration_limit=k))
+        res, x, y, _ = O.solve(lp, tol=1e-12, iteration_limit=k)
+        assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+        np.testing.assert_allclose(sol.get_primal_solution(), x, rtol=1e-8,
+                                   atol=1e-8 * (1 + np.max(np.abs(x))))
+        np.testing.assert_allclose(sol.get_dual_solution(), y, rtol=1e-8,
+                                   atol=1e-8 * (1 + np.max(np.abs(y))))
+
+
+def test_repeat_solves_bitwise_identical():
+    """Two solves of the same LP give bit-identical iterates (every row sum and every reduction is
+    combined in a fixed order)."""
+    lp = gen.skewed_lp(400, 3000, seed=7, cap=3000)
+    dm = datamodel_from_lp(lp)
+    a = lpm.Solve(dm, settings(tol=1e-12, iteration_limit=300))
+    b = lpm.Solve(dm, settings(tol=1e-12, iteration_limit=300))
+    assert np.array_equal(a.get_primal_solution(), b.get_primal_solution())
+    assert np.array_equal(a.get_dual_solution(), b.get_dual_solution())
