@@ -119,6 +119,8 @@ SIGNATURES = {
     "cuOptBatchSolve": (cuopt_int_t, [C.POINTER(handle_t), cuopt_int_t, handle_t,
                                       C.POINTER(handle_t)]),
     "cuOptSolutionAdjoint": (cuopt_int_t, [handle_t, handle_t] + [C.c_void_p] * 6),
+    "cuOptComputeKKTErrorsNoAlloc": (cuopt_int_t, [cuopt_int_t, cuopt_int_t, cuopt_int_t,
+                                                   cuopt_float_t] + [C.c_void_p] * 11),
 }
 
 _lib = None

@@ -123,6 +123,35 @@ cuopt_int_t cuOptSolutionAdjoint(cuOptOptimizationProblem problem,
                                  cuopt_float_t* dl_dupper,
                                  cuopt_float_t* dl_dvalues);
 
+/* KKT errors of a given point, computed without allocating device memory (no counterpart in the
+ * reference).  For an LP in device memory (user's CSR order, as for cuOptSolveDevice) and a point
+ * (d_primal n, d_dual m, d_reduced_cost n, signs as cuOptSolveDevice returns them), writes to the
+ * device array d_out (9 doubles), in stream order: l2 primal residual, l2 dual residual, primal
+ * objective, dual objective, gap, relative primal residual, relative dual residual, relative gap
+ * (the quantities of cuOptPDLPStatistics), and the count of column indices outside [0, n) (when it
+ * is non-zero the eight values are NaN).  For callers that cannot allocate: a memory pool that is
+ * already fully reserved, or a loop that must not pay cudaMalloc's implicit synchronisation.
+ * Scratch is a fixed static device array: num_variables may be at most 524288 (larger sizes
+ * return CUOPT_INVALID_ARGUMENT with a message on stderr); constraints and non-zeros are not
+ * bounded.  The first call on a device looks up the scratch addresses (setup), so make it before
+ * any stream capture.  Calls that overlap in time on one device share the scratch and race; order
+ * them. */
+cuopt_int_t cuOptComputeKKTErrorsNoAlloc(cuopt_int_t num_constraints,
+                                         cuopt_int_t num_variables,
+                                         cuopt_int_t objective_sense,
+                                         cuopt_float_t objective_offset,
+                                         const cuopt_float_t* d_objective_coefficients,
+                                         const cuopt_int_t* d_row_offsets,
+                                         const cuopt_int_t* d_column_indices,
+                                         const cuopt_float_t* d_values,
+                                         const cuopt_float_t* d_constraint_lower_bounds,
+                                         const cuopt_float_t* d_constraint_upper_bounds,
+                                         const cuopt_float_t* d_primal,
+                                         const cuopt_float_t* d_dual,
+                                         const cuopt_float_t* d_reduced_cost,
+                                         void* stream,
+                                         cuopt_float_t* d_out);
+
 #ifdef __cplusplus
 }
 #endif
