@@ -1,0 +1,1159 @@
+// Batched PDLP: many independent LPs solved together as one block-diagonal LP.
+//
+// Counterpart of the reference's batch solve (the Python BatchSolve through
+// cuopt::cython::call_batch_solve, cpp/src/pdlp/utilities/cython_solve.cu:317-352, which runs one
+// PDLP per problem on host threads) and of its batch climbers (cpp/src/pdlp/pdlp.cu:1447-1746).
+// Here the instances are concatenated into one block-diagonal matrix and every PDHG sweep is one
+// launch over all of them; each row reads the step sizes of its own instance.  Every instance
+// keeps its own Stable3 state — scaling factors, step size (its own power iteration), primal
+// weight, restart / PID state and termination — and follows the schedule of a single solve: that
+// schedule depends only on the iteration count, which all instances share.  An instance that
+// terminates is frozen: the sweeps skip its rows and no kernel writes its vectors again.
+//
+// Per-instance sums (norms, residuals, fixed-point errors) are formed deterministically: the
+// epilogues write one value per row into a row buffer, and one block per instance adds its rows in
+// a fixed order (the layout keeps every instance's rows contiguous inside the long-row and the
+// sliced parts, see make_keys_kernel).
+#include "device_layout.cuh"
+#include "kernels.cuh"
+#include "pdlp_engine.hpp"
+#include "pdlp_schedule.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <limits>
+#include <map>
+#include <random>
+#include <stdexcept>
+
+namespace cuopt_b200 {
+
+namespace {
+
+double now_s()
+{
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+template <typename T>
+dev_sell<T> bview(const dev_matrix& M, const T* v)
+{
+  return dev_sell<T>{M.rows, M.n_long, M.n_slices, M.long_off.data(), M.slice_off.data(),
+                     M.idx.data(), v};
+}
+
+// ------------------------------------------------------------------------------------------------
+// Device side
+
+// Instance lookup shared by the batch epilogues.
+struct inst_ctx {
+  const int* inst;         // instance of every internal row of the swept matrix
+  const int* active;       // per instance: still iterating
+  const pdlp_scalars* sc;  // per instance step scalars
+  // Rows r0..r1 lie in one class (long or sliced), where instances are sorted, so the instances
+  // present are inst[r0]..inst[r1].
+  __device__ __forceinline__ bool all_frozen(int r0, int r1) const
+  {
+    for (int b = inst[r0]; b <= inst[r1]; ++b)
+      if (active[b]) return false;
+    return true;
+  }
+};
+
+template <typename TX, bool MAJOR, bool HALPERN, bool SAVE_ATY>
+struct b_primal_epi {
+  static constexpr int kRed = 0;
+  const TX *x, *c, *lo, *up, *xa;
+  TX *xbar, *xout, *xhat, *slack, *aty;
+  inst_ctx ctx;
+  int it_off;
+  struct pre_t {
+    TX x, c, lo, up, xa;
+    int b;
+  };
+  __device__ bool skip() const { return false; }
+  __device__ bool skip_range(int r0, int r1) const { return ctx.all_frozen(r0, r1); }
+  __device__ __forceinline__ pre_t load(int j) const
+  {
+    return pre_t{x[j], c[j], lo[j], up[j], HALPERN ? xa[j] : TX(0), ctx.inst[j]};
+  }
+  __device__ __forceinline__ void operator()(int j, double acc, const pre_t& p, red_t<0>&) const
+  {
+    if (!ctx.active[p.b]) return;
+    primal_row_step<TX, MAJOR, HALPERN, SAVE_ATY>(j, acc, p, ctx.sc + p.b, it_off, xbar, xout,
+                                                  xhat, slack, aty);
+  }
+};
+
+// FPE: rowbuf[i] = (y_bar_i - y_i)^2.
+template <typename TX, bool MAJOR, bool HALPERN, bool FPE>
+struct b_dual_epi {
+  static constexpr int kRed = 0;
+  const TX *y, *lo, *up, *ya;
+  TX *ybar, *yout, *yhat;
+  double* rowbuf;
+  inst_ctx ctx;
+  int it_off;
+  struct pre_t {
+    TX y, lo, up, ya;
+    int b;
+  };
+  __device__ bool skip() const { return false; }
+  __device__ bool skip_range(int r0, int r1) const { return ctx.all_frozen(r0, r1); }
+  __device__ __forceinline__ pre_t load(int i) const
+  {
+    return pre_t{y[i], lo[i], up[i], HALPERN ? ya[i] : TX(0), ctx.inst[i]};
+  }
+  __device__ __forceinline__ void operator()(int i, double acc, const pre_t& p, red_t<0>&) const
+  {
+    if (!ctx.active[p.b]) return;
+    const double d2 =
+      dual_row_step<TX, MAJOR, HALPERN>(i, acc, p, ctx.sc + p.b, it_off, ybar, yout, yhat);
+    if constexpr (FPE) rowbuf[i] = d2;
+  }
+};
+
+// rowbuf[j] = (A^T y_bar - A^T y)_j (x_bar - x)_j ; rowbuf[stride + j] = (x_bar - x)_j^2.
+template <typename TX>
+struct b_fpe_epi {
+  static constexpr int kRed = 0;
+  const TX *aty, *xbar, *x;
+  double* rowbuf;
+  size_t stride;
+  inst_ctx ctx;
+  struct pre_t {
+    TX aty, xbar, x;
+    int b;
+  };
+  __device__ bool skip() const { return false; }
+  __device__ bool skip_range(int r0, int r1) const { return ctx.all_frozen(r0, r1); }
+  __device__ __forceinline__ pre_t load(int j) const
+  {
+    return pre_t{aty[j], xbar[j], x[j], ctx.inst[j]};
+  }
+  __device__ __forceinline__ void operator()(int j, double acc, const pre_t& p, red_t<0>&) const
+  {
+    if (!ctx.active[p.b]) return;
+    const double d  = acc - (double)p.aty;
+    const double dx = (double)p.xbar - (double)p.x;
+    rowbuf[j]          = d * dx;
+    rowbuf[stride + j] = dx * dx;
+  }
+};
+
+// Unscaled termination terms of row i of A: rp^2 and the dual-objective bound term.
+struct b_term_primal_epi {
+  static constexpr int kRed = 0;
+  const double *lc, *uc, *y;
+  double* rowbuf;
+  size_t stride;
+  inst_ctx ctx;
+  struct pre_t {
+    double l, u, y;
+    int b;
+  };
+  __device__ bool skip() const { return false; }
+  __device__ bool skip_range(int r0, int r1) const { return ctx.all_frozen(r0, r1); }
+  __device__ __forceinline__ pre_t load(int i) const
+  {
+    return pre_t{lc[i], uc[i], y[i], ctx.inst[i]};
+  }
+  __device__ __forceinline__ void operator()(int i, double ax, const pre_t& p, red_t<0>&) const
+  {
+    if (!ctx.active[p.b]) return;
+    const double cl = fmax(p.l, fmin(ax, p.u));
+    const double rp = ax - cl;
+    rowbuf[i]          = rp * rp;
+    rowbuf[stride + i] = fmax(p.y, 0.0) * finite_or_zero(p.l) + fmin(p.y, 0.0) * finite_or_zero(p.u);
+  }
+};
+
+// Unscaled termination terms of row j of A^T: rd^2, c.x, s.x.
+struct b_term_dual_epi {
+  static constexpr int kRed = 0;
+  const double *c, *x, *s;
+  double* rowbuf;
+  size_t stride;
+  inst_ctx ctx;
+  struct pre_t {
+    double c, x, s;
+    int b;
+  };
+  __device__ bool skip() const { return false; }
+  __device__ bool skip_range(int r0, int r1) const { return ctx.all_frozen(r0, r1); }
+  __device__ __forceinline__ pre_t load(int j) const
+  {
+    return pre_t{c[j], x[j], s[j], ctx.inst[j]};
+  }
+  __device__ __forceinline__ void operator()(int j, double aty, const pre_t& p, red_t<0>&) const
+  {
+    if (!ctx.active[p.b]) return;
+    const double rd        = (p.c - aty) - p.s;
+    rowbuf[j]              = rd * rd;
+    rowbuf[stride + j]     = p.c * p.x;
+    rowbuf[2 * stride + j] = p.s * p.x;
+  }
+};
+
+// Power iteration sweeps: out = A^T q (store) and z = A (A^T q) with rowbuf = q z.
+template <typename TX>
+struct b_store_epi {
+  static constexpr int kRed = 0;
+  TX* out;
+  inst_ctx ctx;
+  struct pre_t {};
+  __device__ bool skip() const { return false; }
+  __device__ bool skip_range(int r0, int r1) const { return ctx.all_frozen(r0, r1); }
+  __device__ __forceinline__ pre_t load(int) const { return pre_t{}; }
+  __device__ __forceinline__ void operator()(int r, double acc, const pre_t&, red_t<0>&) const
+  {
+    out[r] = (TX)acc;
+  }
+};
+struct b_power_z_epi {
+  static constexpr int kRed = 0;
+  double* z;
+  const double* q;
+  double* rowbuf;
+  inst_ctx ctx;
+  struct pre_t {
+    double q;
+    int b;
+  };
+  __device__ bool skip() const { return false; }
+  __device__ bool skip_range(int r0, int r1) const { return ctx.all_frozen(r0, r1); }
+  __device__ __forceinline__ pre_t load(int i) const { return pre_t{q[i], ctx.inst[i]}; }
+  __device__ __forceinline__ void operator()(int i, double acc, const pre_t& p, red_t<0>&) const
+  {
+    if (!ctx.active[p.b]) return;
+    z[i]      = acc;
+    rowbuf[i] = p.q * acc;
+  }
+};
+
+// One block per instance: out[b K + q] = sum of plane q of rowbuf over the instance's two ranges
+// (long rows, sliced rows), in a fixed order (compensated per thread, then a fixed tree).
+template <int K>
+__global__ void __launch_bounds__(kBlock) seg_reduce_kernel(const double* rowbuf, size_t stride,
+                                                            const int4* ranges, const int* want,
+                                                            double* out)
+{
+  const int b = blockIdx.x;
+  if (want && !want[b]) return;
+  const int4 r = ranges[b];
+  __shared__ double sm[kBlock];
+  for (int q = 0; q < K; ++q) {
+    const double* v = rowbuf + (size_t)q * stride;
+    ksum acc;
+    for (int i = r.x + threadIdx.x; i < r.y; i += kBlock) acc.add(v[i]);
+    for (int i = r.z + threadIdx.x; i < r.w; i += kBlock) acc.add(v[i]);
+    sm[threadIdx.x] = acc.value();
+    __syncthreads();
+    for (int h = kBlock / 2; h > 0; h >>= 1) {
+      if (threadIdx.x < h) sm[threadIdx.x] += sm[threadIdx.x + h];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[(size_t)b * K + q] = sm[0];
+    __syncthreads();
+  }
+}
+
+// Elementwise fills of the row buffer.
+template <typename TA>
+__global__ void sq_diff_kernel(const TA* a, const TA* b, int n, double* out)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double d = b ? (double)a[i] - (double)b[i] : (double)a[i];
+    out[i]         = d * d;
+  }
+}
+__global__ void bound_terms_kernel(const double* lo, const double* up, int n, double* out)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double l = lo[i], u = up[i];
+    double s       = 0.0;
+    if (isfinite(l) && l != u) s += l * l;
+    if (isfinite(u)) s += u * u;
+    out[i] = s;
+  }
+}
+
+__global__ void gather_int_kernel(const int* src, const int* perm, int count, int* dst)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    dst[i] = src[perm[i]];
+}
+__global__ void scale_by_inst_kernel(double* v, const int* inst, const double* f, int count)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    v[i] *= f[inst[i]];
+}
+// dst[perm[i]] = f[inst[i]] * src[i]
+__global__ void scatter_by_inst_kernel(const double* src, const int* perm, const int* inst,
+                                       const double* f, int count, double* dst)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    dst[perm[i]] = (f ? f[inst[i]] : 1.0) * src[i];
+}
+
+// Bound / objective rescaling with each instance's beta and gamma.
+template <typename TX>
+__global__ void b_rescale_vectors_kernel(const double* cs, const double* ls, const double* us,
+                                         const double* lcs, const double* ucs, const double* beta,
+                                         const double* gamma, const int* cinst, const int* rinst,
+                                         int n, int m, TX* c_out, TX* l_out, TX* u_out, TX* lc_out,
+                                         TX* uc_out)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x) {
+    if (i < n) {
+      const int b = cinst[i];
+      c_out[i]    = (TX)(cs[i] * gamma[b]);
+      l_out[i]    = (TX)(ls[i] * beta[b]);
+      u_out[i]    = (TX)(us[i] * beta[b]);
+    } else {
+      const int r = i - n, b = rinst[r];
+      lc_out[r]   = (TX)(lcs[r] * beta[b]);
+      uc_out[r]   = (TX)(ucs[r] * beta[b]);
+    }
+  }
+}
+
+template <typename TX>
+__global__ void b_unscale_kernel(const TX* xhat, const TX* yhat, const TX* slack, const double* dc,
+                                 const double* dr, const double* beta, const double* gamma,
+                                 const int* cinst, const int* rinst, const int* active, int n,
+                                 int m, double* xu, double* yu, double* su)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x) {
+    if (i < n) {
+      const int b = cinst[i];
+      if (!active[b]) continue;
+      const double ib = 1.0 / beta[b], ig = 1.0 / gamma[b];
+      const double d  = dc[i];
+      xu[i]           = ((double)xhat[i] * d) * ib;
+      const double s  = (double)slack[i];
+      su[i]           = (d != 0.0 ? s / d : s) * ig;
+    } else {
+      const int r = i - n, b = rinst[r];
+      if (!active[b]) continue;
+      yu[r] = ((double)yhat[r] * dr[r]) * (1.0 / gamma[b]);
+    }
+  }
+}
+
+template <typename TX>
+__global__ void b_halpern_kernel(TX* x, const TX* xbar, const TX* xa, int n, TX* y, const TX* ybar,
+                                 const TX* ya, int m, const int* cinst, const int* rinst,
+                                 const int* active, const pdlp_scalars* sc)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x) {
+    if (i < n) {
+      const int b = cinst[i];
+      if (!active[b]) continue;
+      const double w = halpern_weight(sc + b, 0);
+      x[i]           = (TX)(w * (double)xbar[i] + (1.0 - w) * (double)xa[i]);
+    } else {
+      const int r = i - n, b = rinst[r];
+      if (!active[b]) continue;
+      const double w = halpern_weight(sc + b, 0);
+      y[r]           = (TX)(w * (double)ybar[r] + (1.0 - w) * (double)ya[r]);
+    }
+  }
+}
+
+// Restart to the current average: x, x_anchor <- x_hat (and y) for flagged instances.
+template <typename TX>
+__global__ void b_restart_kernel(TX* x, TX* xa, const TX* xhat, int n, TX* y, TX* ya,
+                                 const TX* yhat, int m, const int* cinst, const int* rinst,
+                                 const int* flag)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x) {
+    if (i < n) {
+      if (!flag[cinst[i]]) continue;
+      x[i]  = xhat[i];
+      xa[i] = xhat[i];
+    } else {
+      const int r = i - n;
+      if (!flag[rinst[r]]) continue;
+      y[r]  = yhat[r];
+      ya[r] = yhat[r];
+    }
+  }
+}
+
+__global__ void b_advance_kernel(pdlp_scalars* sc, const int* active, int count, int steps)
+{
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < count; b += gridDim.x * blockDim.x)
+    if (active[b]) sc[b].t0 += steps;
+}
+
+// Power iteration per instance (reference pdlp.cu:2620-2731).
+struct b_power_state {
+  double s2;
+  double resid;
+  int iters;
+  int pad;
+};
+__global__ void b_power_normalize_kernel(const double* z, double* q, int m, const int* rinst,
+                                         const int* pactive, const double* sumsq)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const int b = rinst[i];
+    if (!pactive[b]) continue;
+    q[i] = z[i] / sqrt(sumsq[b]);
+  }
+}
+__global__ void b_power_residual_kernel(double* q, const double* z, int m, const int* rinst,
+                                        const int* pactive, const double* s2, double* rowbuf)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const int b = rinst[i];
+    if (!pactive[b]) continue;
+    const double v = q[i] * -s2[b] + z[i];
+    q[i]           = v;
+    rowbuf[i]      = v * v;
+  }
+}
+__global__ void b_power_check_kernel(b_power_state* ps, int* pactive, const double* s2,
+                                     const double* rsq, int count, double tol, int* remaining)
+{
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < count; b += gridDim.x * blockDim.x) {
+    if (!pactive[b]) continue;
+    ps[b].s2    = s2[b];
+    ps[b].resid = sqrt(rsq[b]);
+    ps[b].iters += 1;
+    if (ps[b].resid < tol) {
+      pactive[b] = 0;
+      atomicSub(remaining, 1);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Host side
+
+struct inst_conv {
+  double l2_primal = 0, l2_dual = 0, primal_obj = 0, dual_obj = 0, gap = 0, abs_obj = 0;
+};
+
+template <typename TX>
+class batch_engine {
+ public:
+  batch_engine(const batch_device_input& in, const pdlp_params& p, cudaStream_t s)
+    : in_(in), p_(p), s_(s), B_(in.count)
+  {
+    int dev = 0;
+    B200_CUDA_CHECK(cudaGetDevice(&dev));
+    B200_CUDA_CHECK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
+    B200_CUDA_CHECK(cudaMallocHost(&hbuf_, sizeof(double) * 8 * (size_t)std::max(B_, 1)));
+  }
+  ~batch_engine()
+  {
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    cudaFreeHost(hbuf_);
+  }
+
+  std::vector<pdlp_result> run(double* x_out, double* y_out, double* rc_out)
+  {
+    alloc_scope scope(s_);
+    t_start_ = now_s();
+    results_.assign(B_, pdlp_result{});
+    setup();
+    t_loop_ = now_s();
+    loop();
+    trace("batch: loop");
+    write_outputs(x_out, y_out, rc_out);
+    const double t = now_s();
+    for (int b = 0; b < B_; ++b) {
+      results_[b].setup_time      = t_loop_ - t_start_;
+      results_[b].loop_time       = results_[b].solve_time - (t_loop_ - t_start_);
+      results_[b].kernel_launches = launches_;
+      results_[b].power_iterations = power_iters_[b];
+    }
+    (void)t;
+    return results_;
+  }
+
+ private:
+  // ---------------------------------------------------------------- setup
+  void setup()
+  {
+    const int m = in_.m, n = in_.n;
+    layout_params lp;
+    lp.row_inst = in_.row_inst;
+    lp.col_inst = in_.col_inst;
+    trace("batch: start");
+    build_device_layout(m, n, in_.row_off, in_.col_idx, in_.val, s_, L_, lp);
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    trace("batch: layout");
+    vgrid_ = sms_ * 4;
+    const int g = std::max({sell_grid(bview(L_.A, L_.A.val.data())),
+                            sell_grid(bview(L_.AT, L_.AT.val.data())), vgrid_});
+    partials_.resize((size_t)g * 4);
+    stride_ = (size_t)std::max(m, n);
+    rowbuf_.resize(3 * stride_);
+    segout_.resize((size_t)B_ * 8);
+
+    // Instance of every internal row / column, and each instance's ranges.
+    rinst_.resize(m);
+    cinst_.resize(n);
+    gather_int_kernel<<<vgrid_, kBlock, 0, s_>>>(in_.row_inst, L_.row_new2old.data(), m,
+                                                 rinst_.data());
+    gather_int_kernel<<<vgrid_, kBlock, 0, s_>>>(in_.col_inst, L_.col_new2old.data(), n,
+                                                 cinst_.data());
+    B200_LAUNCH_CHECK();
+    rranges_ = ranges_of(rinst_, m, L_.A.n_long);
+    cranges_ = ranges_of(cinst_, n, L_.AT.n_long);
+    rr_d_.resize(B_);
+    cr_d_.resize(B_);
+    rr_d_.upload(rranges_.data(), B_, s_);
+    cr_d_.upload(cranges_.data(), B_, s_);
+
+    // Per-instance sign (maximisation) and objective scale / offset.
+    std::vector<double> sgn(B_);
+    obj_scale_.resize(B_);
+    obj_offset_.resize(B_);
+    for (int b = 0; b < B_; ++b) {
+      const bool mx  = in_.maximize[b] != 0;
+      sgn[b]         = mx ? -1.0 : 1.0;
+      obj_scale_[b]  = mx ? -1.0 : 1.0;
+      obj_offset_[b] = mx ? -in_.obj_offset[b] : in_.obj_offset[b];
+    }
+    sgn_d_.resize(B_);
+    sgn_d_.upload(sgn.data(), B_, s_);
+
+    c64_.resize(n);
+    l64_.resize(n);
+    u64_.resize(n);
+    lc64_.resize(m);
+    uc64_.resize(m);
+    permute_gather(in_.c, L_.col_new2old.data(), n, 1.0, c64_.data(), s_);
+    scale_by_inst_kernel<<<vgrid_, kBlock, 0, s_>>>(c64_.data(), cinst_.data(), sgn_d_.data(), n);
+    permute_gather(in_.var_lo, L_.col_new2old.data(), n, 1.0, l64_.data(), s_);
+    permute_gather(in_.var_up, L_.col_new2old.data(), n, 1.0, u64_.data(), s_);
+    permute_gather(in_.con_lo, L_.row_new2old.data(), m, 1.0, lc64_.data(), s_);
+    permute_gather(in_.con_up, L_.row_new2old.data(), m, 1.0, uc64_.data(), s_);
+
+    // Ruiz (10 passes) then Pock-Chambolle (alpha = 1); row / column operations, so the batch
+    // scales every instance exactly as a single solve would (reference initial_scaling.cu:152-365).
+    const auto A64 = bview(L_.A, L_.A.val.data()), AT64 = bview(L_.AT, L_.AT.val.data());
+    dr_.resize(m);
+    dc_.resize(n);
+    fill(dr_.data(), m, 1.0);
+    fill(dc_.data(), n, 1.0);
+    dbuf<double> rtmp(m), ctmp(n);
+    for (int it = 0; it < kRuizIterations; ++it) {
+      row_scaled_abs_kernel<0, false><<<sell_grid(A64), kBlock, 0, s_>>>(A64, dr_.data(),
+                                                                        dc_.data(), 0.0,
+                                                                        rtmp.data());
+      row_scaled_abs_kernel<0, true><<<sell_grid(AT64), kBlock, 0, s_>>>(AT64, dr_.data(),
+                                                                        dc_.data(), 0.0,
+                                                                        ctmp.data());
+      apply_root_scaling_kernel<<<vgrid_, kBlock, 0, s_>>>(dr_.data(), rtmp.data(), m);
+      apply_root_scaling_kernel<<<vgrid_, kBlock, 0, s_>>>(dc_.data(), ctmp.data(), n);
+    }
+    row_scaled_abs_kernel<1, false><<<sell_grid(A64), kBlock, 0, s_>>>(A64, dr_.data(), dc_.data(),
+                                                                      kPcAlpha, rtmp.data());
+    row_scaled_abs_kernel<1, true><<<sell_grid(AT64), kBlock, 0, s_>>>(
+      AT64, dr_.data(), dc_.data(), 2.0 - kPcAlpha, ctmp.data());
+    apply_root_scaling_kernel<<<vgrid_, kBlock, 0, s_>>>(dr_.data(), rtmp.data(), m);
+    apply_root_scaling_kernel<<<vgrid_, kBlock, 0, s_>>>(dc_.data(), ctmp.data(), n);
+    B200_LAUNCH_CHECK();
+    As_.resize(L_.A.stored());
+    ATs_.resize(L_.AT.stored());
+    scale_values_kernel<TX, false><<<sell_grid(A64), kBlock, 0, s_>>>(A64, dr_.data(), dc_.data(),
+                                                                     As_.data());
+    scale_values_kernel<TX, true><<<sell_grid(AT64), kBlock, 0, s_>>>(AT64, dr_.data(),
+                                                                     dc_.data(), ATs_.data());
+    B200_LAUNCH_CHECK();
+
+    // All instances active from here on (the power iteration has its own flags).
+    active_h_.assign(B_, 1);
+    active_d_.resize(B_);
+    active_d_.upload(active_h_.data(), B_, s_);
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    trace("batch: ranges + scaling");
+    prepare_vectors();
+    trace("batch: vectors");
+    power_iteration();
+    trace("batch: power iteration");
+
+    xu_.resize(n);
+    su_.resize(n);
+    yu_.resize(m);
+    xu_.zero(s_);
+    su_.zero(s_);
+    yu_.zero(s_);
+    sc_d_.resize(B_);
+    omega_.assign(B_, 1.0);
+    best_omega_.assign(B_, 1.0);
+    restarts_.assign(B_, 0);
+    for (auto* b : {&x_, &xhat_, &slack_, &xbar_, &xa_, &aty_}) {
+      b->resize(n);
+      b->zero(s_);
+    }
+    for (auto* b : {&y_, &yhat_, &ybar_, &ya_}) {
+      b->resize(m);
+      b->zero(s_);
+    }
+    clamp_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(x_.data(), ls_.data(), us_.data(), n);
+    launches_ += 1;
+    B200_LAUNCH_CHECK();
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+  }
+
+  // Ranges {long_lo, long_hi, short_lo, short_hi} of every instance in an internal order whose
+  // instance ids are sorted inside [0, n_long) and inside [n_long, count).
+  std::vector<int4> ranges_of(const dbuf<int>& inst, int count, int n_long)
+  {
+    std::vector<int> h(count);
+    inst.download(h.data(), count, s_);
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    std::vector<int4> r(B_, int4{0, 0, 0, 0});
+    std::vector<char> seen_long(B_, 0), seen_short(B_, 0);
+    for (int i = 0; i < count; ++i) {
+      const int b      = h[i];
+      const bool is_lo = i < n_long;
+      if (b < 0 || b >= B_) throw std::runtime_error("batch layout: instance id out of range");
+      if (i > 0 && i != n_long && h[i - 1] > b)
+        throw std::runtime_error("batch layout: instances not contiguous");
+      auto& seen = is_lo ? seen_long : seen_short;
+      if (!seen[b]) {
+        seen[b] = 1;
+        if (is_lo)
+          r[b].x = i;
+        else
+          r[b].z = i;
+      }
+      if (is_lo)
+        r[b].y = i + 1;
+      else
+        r[b].w = i + 1;
+    }
+    return r;
+  }
+
+  void fill(double* p, int n, double v)
+  {
+    std::vector<double> h(n, v);
+    B200_CUDA_CHECK(cudaMemcpyAsync(p, h.data(), n * sizeof(double), cudaMemcpyHostToDevice, s_));
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+  }
+
+  // Per-instance sums of K planes of the row buffer over rows (ROWS) or columns; result in
+  // segout_ + offset, optionally only for active instances.
+  template <int K>
+  void seg_reduce(bool rows, size_t offset, bool only_active)
+  {
+    seg_reduce_kernel<K><<<B_, kBlock, 0, s_>>>(rowbuf_.data(), stride_,
+                                               rows ? rr_d_.data() : cr_d_.data(),
+                                               only_active ? active_d_.data() : nullptr,
+                                               segout_.data() + offset);
+    ++launches_;
+  }
+  void fetch(size_t offset, size_t count, double* dst)
+  {
+    B200_CUDA_CHECK(cudaMemcpyAsync(dst, segout_.data() + offset, count * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s_));
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+  }
+
+  void prepare_vectors()
+  {
+    const int m = in_.m, n = in_.n;
+    std::vector<double> h(4 * (size_t)B_);
+    sq_diff_kernel<double><<<vgrid_, kBlock, 0, s_>>>(c64_.data(), nullptr, n, rowbuf_.data());
+    seg_reduce<1>(false, 0, false);
+    bound_terms_kernel<<<vgrid_, kBlock, 0, s_>>>(lc64_.data(), uc64_.data(), m, rowbuf_.data());
+    seg_reduce<1>(true, B_, false);
+    dbuf<double> cs(n), ls(n), us(n), lcs(m), ucs(m);
+    scale_vectors_kernel<<<vgrid_, kBlock, 0, s_>>>(c64_.data(), l64_.data(), u64_.data(),
+                                                    lc64_.data(), uc64_.data(), dc_.data(),
+                                                    dr_.data(), n, m, cs.data(), ls.data(),
+                                                    us.data(), lcs.data(), ucs.data());
+    sq_diff_kernel<double><<<vgrid_, kBlock, 0, s_>>>(cs.data(), nullptr, n, rowbuf_.data());
+    seg_reduce<1>(false, 2 * (size_t)B_, false);
+    bound_terms_kernel<<<vgrid_, kBlock, 0, s_>>>(lcs.data(), ucs.data(), m, rowbuf_.data());
+    seg_reduce<1>(true, 3 * (size_t)B_, false);
+    launches_ += 5;
+    B200_LAUNCH_CHECK();
+    fetch(0, 4 * (size_t)B_, h.data());
+    c_norm_.resize(B_);
+    b_norm_.resize(B_);
+    std::vector<double> beta(B_), gamma(B_);
+    for (int b = 0; b < B_; ++b) {
+      c_norm_[b] = std::sqrt(h[b]);
+      b_norm_[b] = std::sqrt(h[B_ + b]);
+      gamma[b]   = 1.0 / (std::sqrt(h[2 * B_ + b]) + 1.0);
+      beta[b]    = 1.0 / (std::sqrt(h[3 * B_ + b]) + 1.0);
+    }
+    beta_d_.resize(B_);
+    gamma_d_.resize(B_);
+    beta_d_.upload(beta.data(), B_, s_);
+    gamma_d_.upload(gamma.data(), B_, s_);
+    beta_  = beta;
+    gamma_ = gamma;
+    cs_.resize(n);
+    ls_.resize(n);
+    us_.resize(n);
+    lcs_.resize(m);
+    ucs_.resize(m);
+    b_rescale_vectors_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(
+      cs.data(), ls.data(), us.data(), lcs.data(), ucs.data(), beta_d_.data(), gamma_d_.data(),
+      cinst_.data(), rinst_.data(), n, m, cs_.data(), ls_.data(), us_.data(), lcs_.data(),
+      ucs_.data());
+    ++launches_;
+    B200_LAUNCH_CHECK();
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+  }
+
+  // Power iteration of every instance (graph chunks of 32 iterations; converged instances freeze).
+  void power_iteration()
+  {
+    const int m = in_.m, n = in_.n;
+    std::vector<double> z0(m);
+    for (int b = 0; b < B_; ++b) {
+      std::mt19937 gen(1);
+      std::normal_distribution<double> dist(0.0, 1.0);
+      for (int i = in_.row_start[b]; i < in_.row_start[b + 1]; ++i) z0[i] = dist(gen);
+    }
+    dbuf<double> dz(m), dq(m), datq(n);
+    dq.upload(z0.data(), m, s_);
+    permute_gather(dq.data(), L_.row_new2old.data(), m, 1.0, dz.data(), s_);
+    dbuf<b_power_state> ps(B_);
+    ps.zero(s_);
+    dbuf<int> pact(B_), remaining(1);
+    std::vector<int> ones(B_, 1);
+    pact.upload(ones.data(), B_, s_);
+    remaining.upload(&B_, 1, s_);
+    const auto As  = bview<TX>(L_.A, As_.data());
+    const auto ATs = bview<TX>(L_.AT, ATs_.data());
+    const inst_ctx rctx{rinst_.data(), pact.data(), nullptr};
+    const inst_ctx cctx{cinst_.data(), pact.data(), nullptr};
+    double* sumsq = segout_.data();
+    double* s2    = segout_.data() + B_;
+    double* rsq   = segout_.data() + 2 * (size_t)B_;
+    auto one_iteration = [&]() {
+      sq_diff_kernel<double><<<vgrid_, kBlock, 0, s_>>>(dz.data(), nullptr, m, rowbuf_.data());
+      seg_reduce_kernel<1><<<B_, kBlock, 0, s_>>>(rowbuf_.data(), stride_, rr_d_.data(),
+                                                 pact.data(), sumsq);
+      b_power_normalize_kernel<<<vgrid_, kBlock, 0, s_>>>(dz.data(), dq.data(), m, rinst_.data(),
+                                                          pact.data(), sumsq);
+      sell_map_kernel<TX, double, b_store_epi<double>><<<sell_grid(ATs), kBlock, 0, s_>>>(
+        ATs, dq.data(), b_store_epi<double>{datq.data(), cctx}, partials_.data());
+      sell_map_kernel<TX, double, b_power_z_epi><<<sell_grid(As), kBlock, 0, s_>>>(
+        As, datq.data(), b_power_z_epi{dz.data(), dq.data(), rowbuf_.data(), rctx},
+        partials_.data());
+      seg_reduce_kernel<1><<<B_, kBlock, 0, s_>>>(rowbuf_.data(), stride_, rr_d_.data(),
+                                                 pact.data(), s2);
+      b_power_residual_kernel<<<vgrid_, kBlock, 0, s_>>>(dq.data(), dz.data(), m, rinst_.data(),
+                                                         pact.data(), s2, rowbuf_.data());
+      seg_reduce_kernel<1><<<B_, kBlock, 0, s_>>>(rowbuf_.data(), stride_, rr_d_.data(),
+                                                 pact.data(), rsq);
+      b_power_check_kernel<<<ceil_div(B_, kBlock), kBlock, 0, s_>>>(
+        ps.data(), pact.data(), s2, rsq, B_, kPowerTol, remaining.data());
+    };
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    B200_CUDA_CHECK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < 32; ++i) one_iteration();
+    B200_CUDA_CHECK(cudaStreamEndCapture(s_, &graph));
+    B200_CUDA_CHECK(cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphDestroy(graph);
+    int left = B_;
+    for (int done_iters = 0; done_iters < kPowerMaxIters; done_iters += 32) {
+      if (kPowerMaxIters - done_iters < 32) {
+        for (int i = 0; i < kPowerMaxIters - done_iters; ++i) one_iteration();
+      } else {
+        B200_CUDA_CHECK(cudaGraphLaunch(exec, s_));
+      }
+      launches_ += 9.0 * std::min(32, kPowerMaxIters - done_iters);
+      remaining.download(&left, 1, s_);
+      B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+      if (left == 0) break;
+    }
+    cudaGraphExecDestroy(exec);
+    std::vector<b_power_state> h(B_);
+    ps.download(h.data(), B_, s_);
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    eta_.resize(B_);
+    power_iters_.resize(B_);
+    for (int b = 0; b < B_; ++b) {
+      eta_[b]         = kStepScaling / std::sqrt(h[b].s2);
+      power_iters_[b] = h[b].iters;
+    }
+  }
+
+  // ---------------------------------------------------------------- iterations
+  inst_ctx ctx_rows() const { return inst_ctx{rinst_.data(), active_d_.data(), sc_d_.data()}; }
+  inst_ctx ctx_cols() const { return inst_ctx{cinst_.data(), active_d_.data(), sc_d_.data()}; }
+
+  template <bool MAJOR, bool HALPERN, bool SAVE_ATY>
+  void launch_primal(int it_off)
+  {
+    const auto A = bview<TX>(L_.AT, ATs_.data());
+    b_primal_epi<TX, MAJOR, HALPERN, SAVE_ATY> e{x_.data(),    cs_.data(),   ls_.data(),
+                                                 us_.data(),   xa_.data(),   xbar_.data(),
+                                                 x_.data(),    xhat_.data(), slack_.data(),
+                                                 aty_.data(),  ctx_cols(),   it_off};
+    sell_map_kernel<TX, TX, decltype(e)><<<sell_grid(A), kBlock, 0, s_>>>(A, y_.data(), e,
+                                                                         partials_.data());
+    ++launches_;
+  }
+  template <bool MAJOR, bool HALPERN, bool FPE>
+  void launch_dual(int it_off)
+  {
+    const auto A = bview<TX>(L_.A, As_.data());
+    b_dual_epi<TX, MAJOR, HALPERN, FPE> e{y_.data(),     lcs_.data(),  ucs_.data(),
+                                          ya_.data(),    ybar_.data(), y_.data(),
+                                          yhat_.data(),  rowbuf_.data(), ctx_rows(), it_off};
+    sell_map_kernel<TX, TX, decltype(e)><<<sell_grid(A), kBlock, 0, s_>>>(A, xbar_.data(), e,
+                                                                         partials_.data());
+    ++launches_;
+  }
+  void advance(int steps)
+  {
+    b_advance_kernel<<<ceil_div(B_, kBlock), kBlock, 0, s_>>>(sc_d_.data(), active_d_.data(), B_,
+                                                             steps);
+    ++launches_;
+  }
+  void plain_iterations(int L)
+  {
+    for (int i = 0; i < L; ++i) {
+      launch_primal<false, true, false>(i);
+      launch_dual<false, true, false>(i);
+    }
+    advance(L);
+  }
+  void run_plain(long R)
+  {
+    for (int L = 128; L >= 1; L >>= 1) {
+      while (R >= L) {
+        auto it = graphs_.find(L);
+        if (it == graphs_.end()) {
+          cudaGraph_t g;
+          cudaGraphExec_t e;
+          B200_CUDA_CHECK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+          const double before = launches_;
+          plain_iterations(L);
+          launches_ = before;
+          B200_CUDA_CHECK(cudaStreamEndCapture(s_, &g));
+          B200_CUDA_CHECK(cudaGraphInstantiate(&e, g, 0));
+          cudaGraphDestroy(g);
+          it = graphs_.emplace(L, e).first;
+        }
+        B200_CUDA_CHECK(cudaGraphLaunch(it->second, s_));
+        launches_ += 2.0 * L + 1.0;
+        R -= L;
+      }
+    }
+  }
+
+  void upload_scalars(const std::vector<long>& since)
+  {
+    std::vector<pdlp_scalars> h(B_);
+    for (int b = 0; b < B_; ++b)
+      h[b] = pdlp_scalars{eta_[b] / omega_[b], eta_[b] * omega_[b], eta_[b], omega_[b],
+                          (long long)since[b]};
+    sc_d_.upload(h.data(), B_, s_);
+    active_d_.upload(active_h_.data(), B_, s_);
+  }
+
+  // Unscaled residuals / objectives of every active instance (x_hat, y_hat, slack of the last
+  // major step), like the single-LP evaluation.
+  std::vector<inst_conv> evaluate()
+  {
+    const int m = in_.m, n = in_.n;
+    b_unscale_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(
+      xhat_.data(), yhat_.data(), slack_.data(), dc_.data(), dr_.data(), beta_d_.data(),
+      gamma_d_.data(), cinst_.data(), rinst_.data(), active_d_.data(), n, m, xu_.data(), yu_.data(),
+      su_.data());
+    const auto A = bview(L_.A, L_.A.val.data()), AT = bview(L_.AT, L_.AT.val.data());
+    sell_map_kernel<double, double, b_term_primal_epi><<<sell_grid(A), kBlock, 0, s_>>>(
+      A, xu_.data(),
+      b_term_primal_epi{lc64_.data(), uc64_.data(), yu_.data(), rowbuf_.data(), stride_,
+                        ctx_rows()},
+      partials_.data());
+    seg_reduce<2>(true, 0, true);
+    sell_map_kernel<double, double, b_term_dual_epi><<<sell_grid(AT), kBlock, 0, s_>>>(
+      AT, yu_.data(),
+      b_term_dual_epi{c64_.data(), xu_.data(), su_.data(), rowbuf_.data(), stride_, ctx_cols()},
+      partials_.data());
+    seg_reduce<3>(false, 2 * (size_t)B_, true);
+    launches_ += 3;
+    B200_LAUNCH_CHECK();
+    fetch(0, 5 * (size_t)B_, hbuf_);
+    std::vector<inst_conv> cv(B_);
+    for (int b = 0; b < B_; ++b) {
+      if (!active_h_[b]) continue;
+      const double* pr = hbuf_ + 2 * b;
+      const double* du = hbuf_ + 2 * B_ + 3 * b;
+      inst_conv& c     = cv[b];
+      c.l2_primal      = std::sqrt(pr[0]);
+      c.l2_dual        = std::sqrt(du[0]);
+      c.primal_obj     = du[1];
+      c.dual_obj       = du[2] + pr[1];
+      if (obj_scale_[b] != 1.0 || obj_offset_[b] != 0.0) {
+        c.primal_obj = obj_scale_[b] * (c.primal_obj + obj_offset_[b]);
+        c.dual_obj   = obj_scale_[b] * (c.dual_obj + obj_offset_[b]);
+      }
+      c.gap     = std::fabs(c.primal_obj - c.dual_obj);
+      c.abs_obj = std::fabs(c.primal_obj) + std::fabs(c.dual_obj);
+    }
+    return cv;
+  }
+
+  void finish(int b, int status, const inst_conv& c, long k)
+  {
+    pdlp_result& r   = results_[b];
+    r.status         = status;
+    r.iterations     = k;
+    r.primal_obj     = c.primal_obj;
+    r.dual_obj       = c.dual_obj;
+    r.l2_primal      = c.l2_primal;
+    r.l2_dual        = c.l2_dual;
+    r.rel_primal     = c.l2_primal / (1.0 + b_norm_[b]);
+    r.rel_dual       = c.l2_dual / (1.0 + c_norm_[b]);
+    r.gap            = c.gap;
+    r.rel_gap        = c.gap / (1.0 + c.abs_obj);
+    r.step_size      = eta_[b];
+    r.primal_weight  = omega_[b];
+    r.restarts       = restarts_[b];
+    r.solve_time     = now_s() - t_start_;
+    active_h_[b]     = 0;
+  }
+
+  // Same schedule and per-instance decisions as engine::loop of the single-LP solver.
+  void loop()
+  {
+    const int m = in_.m, n = in_.n;
+    const double qnan = std::numeric_limits<double>::quiet_NaN();
+    const double inf  = std::numeric_limits<double>::infinity();
+    std::vector<double> fpe(B_, qnan), fpe0(B_, qnan), last_trial(B_, inf);
+    std::vector<double> pid_sum(B_, 0.0), pid_last(B_, 0.0), best_gap(B_, inf);
+    std::vector<long> since(B_, 0);
+    std::vector<int> restarted(B_, 0);
+    int n_active = B_;
+    upload_scalars(since);
+
+    for (long k = 0;;) {
+      const bool major = (k % kMajor == 0 && k > 0) || k <= 0;
+      const bool cond  = (k % conditional_major(k)) == 0;
+      std::fill(restarted.begin(), restarted.end(), 0);
+      bool any_restart = false;
+      if (major || cond) {
+        const std::vector<inst_conv> cv = evaluate();
+        const bool out_of_time = now_s() - t_start_ >= p_.time_limit;
+        for (int b = 0; b < B_; ++b) {
+          if (!active_h_[b]) continue;
+          const inst_conv& c   = cv[b];
+          const bool primal_ok = c.l2_primal <= p_.abs_primal + p_.rel_primal * b_norm_[b];
+          const bool optimal   = c.l2_dual <= p_.abs_dual + p_.rel_dual * c_norm_[b] &&
+                               primal_ok && c.gap <= p_.abs_gap + p_.rel_gap * c.abs_obj;
+          if (k > 1 && optimal)
+            finish(b, kOptimal, c, k);
+          else if (out_of_time)
+            finish(b, kTimeLimit, c, k);
+          else if (k >= p_.iteration_limit)
+            finish(b, kIterationLimit, c, k);
+          else if (!std::isfinite(c.l2_primal) || !std::isfinite(c.l2_dual))
+            finish(b, kNumericalError, c, k);
+        }
+        n_active = (int)std::count(active_h_.begin(), active_h_.end(), 1);
+        if (n_active == 0) break;
+
+        if (major) {
+          // Restart distances of every active instance.
+          sq_diff_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(xa_.data(), xhat_.data(), n,
+                                                        rowbuf_.data());
+          active_d_.upload(active_h_.data(), B_, s_);
+          seg_reduce<1>(false, 0, true);
+          sq_diff_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(ya_.data(), yhat_.data(), m,
+                                                        rowbuf_.data());
+          seg_reduce<1>(true, B_, true);
+          launches_ += 2;
+          fetch(0, 2 * (size_t)B_, hbuf_);
+          for (int b = 0; b < B_; ++b) {
+            if (!active_h_[b]) continue;
+            // should_cupdlpx_restart (reference pdlp_restart_strategy.cu:689-754)
+            bool restart = false;
+            if (k == kMajor)
+              restart = true;
+            else if (k > kMajor) {
+              if (fpe[b] <= kSufficientReduction * fpe0[b])
+                restart = true;
+              else if (fpe[b] <= kNecessaryReduction * fpe0[b] && fpe[b] > last_trial[b])
+                restart = true;
+              else if ((double)since[b] >= kArtificialRestart * (double)k)
+                restart = true;
+            }
+            last_trial[b] = fpe[b];
+            if (!restart) continue;
+            // cupdlpx_restart + PID primal weight (reference pdlp_restart_strategy.cu:758-986)
+            const inst_conv& c      = cv[b];
+            const double rel_dual   = c.l2_dual / (1.0 + c_norm_[b]);
+            const double rel_primal = c.l2_primal / (1.0 + b_norm_[b]);
+            const double lp = std::sqrt(hbuf_[b]), ld = std::sqrt(hbuf_[B_ + b]);
+            const double ratio = rel_primal == 0.0 ? inf : rel_dual / rel_primal;
+            if (lp > 1e-16 && ld > 1e-16 && lp < 1e12 && ld < 1e12 && ratio > 1e-8 &&
+                ratio < 1e8) {
+              const double err  = std::log(ld) - std::log(lp) - std::log(omega_[b]);
+              pid_sum[b]        = pid_sum[b] * kISmooth + err;
+              const double derr = err - pid_last[b];
+              omega_[b]   = std::exp(kKp * err + kKi * pid_sum[b] + kKd * derr) * omega_[b];
+              pid_last[b] = err;
+            } else {
+              omega_[b]    = best_omega_[b];
+              pid_sum[b]   = 0.0;
+              pid_last[b]  = 0.0;
+            }
+            const double rgap = std::fabs(std::log10(ratio));
+            if (rgap < best_gap[b]) {
+              best_gap[b]    = rgap;
+              best_omega_[b] = omega_[b];
+            }
+            since[b]      = 0;
+            last_trial[b] = inf;
+            restarted[b]  = 1;
+            any_restart   = true;
+            ++restarts_[b];
+          }
+          if (any_restart) {
+            restart_flags_.resize(B_);
+            restart_flags_.upload(restarted.data(), B_, s_);
+            b_restart_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(
+              x_.data(), xa_.data(), xhat_.data(), n, y_.data(), ya_.data(), yhat_.data(), m,
+              cinst_.data(), rinst_.data(), restart_flags_.data());
+            ++launches_;
+          }
+        }
+        upload_scalars(since);
+        B200_LAUNCH_CHECK();
+      }
+
+      const bool mstep   = is_major_step(k);
+      const bool fpe_all = ((k + 1) % kMajor == 0);
+      if (!mstep && !fpe_all && !any_restart) {
+        long R = 1;
+        while (R < 255) {
+          const long kk = k + R;
+          if (is_check(kk) || is_major_step(kk) || ((kk + 1) % kMajor == 0)) break;
+          ++R;
+        }
+        run_plain(R);
+        k += R;
+        for (int b = 0; b < B_; ++b)
+          if (active_h_[b]) since[b] += R;
+        continue;
+      }
+
+      if (fpe_all || any_restart) {
+        // Every active instance takes the fixed-point-error form of the step (the same update
+        // with the Halpern step applied separately); only instances that need the error use it.
+        if (mstep) {
+          launch_primal<true, false, true>(0);
+          launch_dual<true, false, true>(0);
+        } else {
+          launch_primal<false, false, true>(0);
+          launch_dual<false, false, true>(0);
+        }
+        seg_reduce<1>(true, 0, true);
+        const auto AT = bview<TX>(L_.AT, ATs_.data());
+        sell_map_kernel<TX, TX, b_fpe_epi<TX>><<<sell_grid(AT), kBlock, 0, s_>>>(
+          AT, ybar_.data(),
+          b_fpe_epi<TX>{aty_.data(), xbar_.data(), x_.data(), rowbuf_.data(), stride_, ctx_cols()},
+          partials_.data());
+        seg_reduce<2>(false, B_, true);
+        b_halpern_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(x_.data(), xbar_.data(), xa_.data(), n,
+                                                        y_.data(), ybar_.data(), ya_.data(), m,
+                                                        cinst_.data(), rinst_.data(),
+                                                        active_d_.data(), sc_d_.data());
+        advance(1);
+        launches_ += 2;
+        B200_LAUNCH_CHECK();
+        fetch(0, 3 * (size_t)B_, hbuf_);
+        for (int b = 0; b < B_; ++b) {
+          if (!active_h_[b] || !(fpe_all || restarted[b])) continue;
+          const double ndy = hbuf_[b], inter = hbuf_[B_ + 2 * b], ndx = hbuf_[B_ + 2 * b + 1];
+          const double movement = ndx * omega_[b] + ndy / omega_[b];
+          fpe[b]                = std::sqrt(movement + 2.0 * inter * eta_[b]);
+          if (restarted[b]) fpe0[b] = fpe[b];
+        }
+      } else {
+        launch_primal<true, true, false>(0);
+        launch_dual<true, true, false>(0);
+        advance(1);
+        B200_LAUNCH_CHECK();
+      }
+      ++k;
+      for (int b = 0; b < B_; ++b)
+        if (active_h_[b]) ++since[b];
+    }
+  }
+
+  void write_outputs(double* x_out, double* y_out, double* rc_out)
+  {
+    const int m = in_.m, n = in_.n;
+    if (x_out)
+      scatter_by_inst_kernel<<<vgrid_, kBlock, 0, s_>>>(xu_.data(), L_.col_new2old.data(),
+                                                        cinst_.data(), nullptr, n, x_out);
+    if (rc_out)
+      scatter_by_inst_kernel<<<vgrid_, kBlock, 0, s_>>>(su_.data(), L_.col_new2old.data(),
+                                                        cinst_.data(), sgn_d_.data(), n, rc_out);
+    if (y_out)
+      scatter_by_inst_kernel<<<vgrid_, kBlock, 0, s_>>>(yu_.data(), L_.row_new2old.data(),
+                                                        rinst_.data(), sgn_d_.data(), m, y_out);
+    B200_LAUNCH_CHECK();
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+  }
+
+  // ---------------------------------------------------------------- state
+  const batch_device_input& in_;
+  const pdlp_params& p_;
+  cudaStream_t s_;
+  int B_;
+  int sms_ = 148, vgrid_ = 592;
+  double* hbuf_ = nullptr;
+  double t_start_ = 0, t_loop_ = 0;
+  double launches_ = 0;
+  size_t stride_ = 0;
+
+  device_layout L_;
+  dbuf<TX> As_, ATs_;
+  dbuf<int> rinst_, cinst_, active_d_, restart_flags_;
+  dbuf<int4> rr_d_, cr_d_;
+  std::vector<int4> rranges_, cranges_;
+  dbuf<double> c64_, l64_, u64_, lc64_, uc64_, dr_, dc_, sgn_d_, beta_d_, gamma_d_;
+  dbuf<TX> cs_, ls_, us_, lcs_, ucs_;
+  dbuf<TX> x_, xhat_, slack_, xbar_, xa_, aty_, y_, yhat_, ybar_, ya_;
+  dbuf<double> xu_, yu_, su_, rowbuf_, segout_, partials_;
+  dbuf<pdlp_scalars> sc_d_;
+
+  std::vector<double> obj_scale_, obj_offset_, c_norm_, b_norm_, beta_, gamma_, eta_, omega_,
+    best_omega_;
+  std::vector<int> restarts_, power_iters_, active_h_;
+  std::vector<pdlp_result> results_;
+  std::map<int, cudaGraphExec_t> graphs_;
+};
+
+
+}  // namespace
+
+std::vector<pdlp_result> pdlp_batch_solve_device(const batch_device_input& in,
+                                                 const pdlp_params& p, cudaStream_t stream,
+                                                 double* x_out, double* y_out, double* rc_out)
+{
+  if (in.count <= 0 || in.count > 65535)
+    throw std::invalid_argument("batch size must be in [1, 65535]");
+  configure_pool_once();
+  joined_stream js(stream);
+  if (p.precision == 1) {
+    batch_engine<float> e(in, p, js.own);
+    return e.run(x_out, y_out, rc_out);
+  }
+  batch_engine<double> e(in, p, js.own);
+  return e.run(x_out, y_out, rc_out);
+}
+
+}  // namespace cuopt_b200

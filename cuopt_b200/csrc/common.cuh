@@ -68,6 +68,26 @@ inline double* pinned_scratch()
   return p;
 }
 
+// The engines capture CUDA graphs, which the legacy default stream does not allow, so they
+// always work on its own non-blocking stream ordered after / before the caller's stream with events.
+struct joined_stream {
+  cudaStream_t caller, own = nullptr;
+  cudaEvent_t ev = nullptr;
+  explicit joined_stream(cudaStream_t c) : caller(c)
+  {
+    B200_CUDA_CHECK(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+    B200_CUDA_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    B200_CUDA_CHECK(cudaEventRecord(ev, caller));
+    B200_CUDA_CHECK(cudaStreamWaitEvent(own, ev, 0));
+  }
+  ~joined_stream()
+  {
+    if (cudaEventRecord(ev, own) == cudaSuccess) cudaStreamWaitEvent(caller, ev, 0);
+    cudaEventDestroy(ev);
+    cudaStreamDestroy(own);
+  }
+};
+
 // Phase timing printed to stderr when the environment variable CUOPT_B200_TRACE is set.
 inline void trace(const char* what)
 {

@@ -667,14 +667,27 @@ cuopt_int_t cuOptBatchSolve(const cuOptOptimizationProblem* problems, cuopt_int_
                             cuOptSolverSettings settings, cuOptSolution* solutions)
 {
   if (!problems || !settings || !solutions || count < 0) return CUOPT_INVALID_ARGUMENT;
-  cuopt_int_t first_error = CUOPT_SUCCESS;
+  std::vector<const cuopt_b200::lp_problem*> ps(count);
   for (cuopt_int_t i = 0; i < count; ++i) {
     solutions[i] = nullptr;
     if (!problems[i]) return CUOPT_INVALID_ARGUMENT;
+    ps[i] = P(problems[i]);
   }
+  std::vector<lp_solution> rs;
+  try {
+    rs = cuopt_b200::solve_batch(ps, *S(settings));
+  } catch (const std::bad_alloc&) {
+    return CUOPT_OUT_OF_MEMORY;
+  }
+  cuopt_int_t first_error = CUOPT_SUCCESS;
   for (cuopt_int_t i = 0; i < count; ++i) {
-    cuopt_int_t rc = cuOptSolve(problems[i], settings, &solutions[i]);
-    if (rc != CUOPT_SUCCESS && first_error == CUOPT_SUCCESS) first_error = rc;
+    auto* sol = new (std::nothrow) lp_solution(std::move(rs[i]));
+    if (!sol) {
+      for (cuopt_int_t j = 0; j < i; ++j) cuOptDestroySolution(&solutions[j]);
+      return CUOPT_OUT_OF_MEMORY;
+    }
+    solutions[i] = sol;
+    if (sol->error_code != CUOPT_SUCCESS && first_error == CUOPT_SUCCESS) first_error = sol->error_code;
   }
   return first_error;
 }

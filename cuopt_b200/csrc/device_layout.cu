@@ -33,20 +33,23 @@ __global__ void col_count_kernel(const int* idx, int64_t nnz, int n, int* cnt, i
   }
 }
 
-// Sort keys: long rows (len > thr) first by length descending; the rest by (window, length
-// descending).  A stable radix sort on these keys with values 0..count-1 keeps original order on
-// ties, which makes the permutation deterministic.
-__global__ void make_keys_kernel(const int* len, int count, int thr, int window, uint64_t* keys,
-                                 int* ids, int* nlong)
+// Sort keys: long rows (len > thr) first by (instance, length descending); the rest by
+// (instance, window, length descending).  `inst` (optional) gives each item's instance in a
+// block-diagonal batch, so every instance's items stay contiguous inside each class; without it
+// all items are instance 0.  A stable radix sort on these keys with values 0..count-1 keeps
+// original order on ties, which makes the permutation deterministic.
+__global__ void make_keys_kernel(const int* len, const int* inst, int count, int thr, int window,
+                                 uint64_t* keys, int* ids, int* nlong)
 {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    const int l = len[i];
+    const int l      = len[i];
+    const uint64_t b = inst ? (uint64_t)inst[i] : 0ull;  // < 2^16
     uint64_t k;
     if (l > thr) {
-      k = (uint64_t)(INT_MAX - l);
+      k = (b << 31) | (uint64_t)(INT_MAX - l);
       atomicAdd(nlong, 1);
     } else {
-      k = (1ull << 63) | ((uint64_t)(i / window) << 32) | (uint32_t)(thr - l);
+      k = (1ull << 63) | (b << 47) | ((uint64_t)(i / window) << 31) | (uint64_t)(thr - l);
     }
     keys[i] = k;
     ids[i]  = i;
@@ -191,15 +194,16 @@ struct temp_store {
 };
 
 // Relabelling of `count` items with lengths `len` (device).  Returns the number of long items.
-int order_items(const int* len, int count, const layout_params& p, cudaStream_t s, temp_store& tmp,
-                dbuf<int>& new2old, dbuf<int>& old2new, int* d_counter, int* h_counter)
+int order_items(const int* len, const int* inst, int count, const layout_params& p,
+                cudaStream_t s, temp_store& tmp, dbuf<int>& new2old, dbuf<int>& old2new,
+                int* d_counter, int* h_counter)
 {
   dbuf<uint64_t> keys(count), keys_out(count);
   dbuf<int> ids(count);
   new2old.resize(count);
   old2new.resize(count);
   B200_CUDA_CHECK(cudaMemsetAsync(d_counter, 0, sizeof(int), s));
-  make_keys_kernel<<<grid_for(count), kT, 0, s>>>(len, count, p.long_threshold, p.window,
+  make_keys_kernel<<<grid_for(count), kT, 0, s>>>(len, inst, count, p.long_threshold, p.window,
                                                   keys.data(), ids.data(), d_counter);
   B200_LAUNCH_CHECK();
   size_t bytes = 0;
@@ -294,10 +298,10 @@ void build_device_layout(int m, int n, const int* d_off, const int* d_idx, const
   B200_CUDA_CHECK(cudaStreamSynchronize(s));
   if (hcount[1]) throw std::invalid_argument("constraint matrix column index out of range");
 
-  const int a_long = order_items(rlen.data(), m, p, s, tmp, out.row_new2old, out.row_old2new,
-                                 counters.data(), hcount);
-  const int t_long = order_items(clen.data(), n, p, s, tmp, out.col_new2old, out.col_old2new,
-                                 counters.data(), hcount);
+  const int a_long = order_items(rlen.data(), p.row_inst, m, p, s, tmp, out.row_new2old,
+                                 out.row_old2new, counters.data(), hcount);
+  const int t_long = order_items(clen.data(), p.col_inst, n, p, s, tmp, out.col_new2old,
+                                 out.col_old2new, counters.data(), hcount);
 
   // Internal A (CSR) ----------------------------------------------------------------------
   dbuf<int> alen(m + 1), aoff(m + 1);

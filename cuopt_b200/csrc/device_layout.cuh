@@ -43,6 +43,9 @@ struct device_layout {
 struct layout_params {
   int long_threshold = 96;
   int window         = 1 << 15;
+  // Block-diagonal batches: instance of every user row / column (device, < 65536), or null.
+  const int* row_inst = nullptr;
+  const int* col_inst = nullptr;
 };
 
 // d_off (m+1), d_idx (nnz), d_val (nnz): the user's CSR on the device.  Throws on CUDA errors or

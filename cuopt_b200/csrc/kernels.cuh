@@ -9,6 +9,8 @@
 // that are reduced deterministically (fixed tree, then one ordered pass over blocks).
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace cuopt_b200 {
@@ -119,6 +121,22 @@ __device__ __forceinline__ int4 load_idx_chunk(const int* p)
   return __ldcs(reinterpret_cast<const int4*>(p));
 }
 
+// Epilogues of block-diagonal batches may declare `bool skip_range(int r0, int r1)`: true when
+// rows r0..r1 belong only to finished instances, so a warp can skip their dot products.
+template <class E, class = void>
+struct has_skip_range : std::false_type {};
+template <class E>
+struct has_skip_range<E, std::void_t<decltype(&E::skip_range)>> : std::true_type {};
+
+template <class Epi>
+__device__ __forceinline__ bool skip_rows(const Epi& epi, int r0, int r1)
+{
+  if constexpr (has_skip_range<Epi>::value)
+    return epi.skip_range(r0, r1);
+  else
+    return false;
+}
+
 // Generic fused sweep: acc_r = sum_k A[r,k] * g[idx[r,k]], then epi(r, acc_r, pre, red).
 // The epilogue's per-row operands (`pre`) are loaded before the matrix loop so their memory latency
 // overlaps the gathers.  Sliced rows are read in 4-element lane chunks, two chunks in flight.
@@ -140,7 +158,7 @@ __global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
   const int lb   = long_blocks(A.n_long);
   if ((int)blockIdx.x < lb) {
     const int row = blockIdx.x * kWarpsPerBlock + warp;
-    if (row < A.n_long) {
+    if (row < A.n_long && !skip_rows(epi, row, row)) {
       const auto pre  = epi.load(row);
       const int64_t b = A.long_off[row], e = A.long_off[row + 1];
       double acc      = 0.0;
@@ -151,7 +169,8 @@ __global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
     }
   } else {
     const int s = (blockIdx.x - lb) * kWarpsPerBlock + warp;
-    if (s < A.n_slices) {
+    if (s < A.n_slices &&
+        !skip_rows(epi, A.n_long + s * kWarp, min(A.n_long + s * kWarp + kWarp, A.rows) - 1)) {
       const int row      = A.n_long + s * kWarp + lane;
       const bool valid   = row < A.rows;
       const auto pre     = epi.load(valid ? row : A.rows - 1);
@@ -198,6 +217,55 @@ __global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
 // ---------------------------------------------------------------------------------------------
 // PDHG epilogues (reflected variant, reference pdhg.cu:431-530 and pdlp.cu:2506-2563).
 
+// The primal update of one variable j (shared by the single-LP and batch epilogues); `p` holds
+// x_j, c_j, l_j, u_j and the anchor x_a,j, `st` the step scalars of j's LP.
+template <typename TX, bool MAJOR, bool HALPERN, bool SAVE_ATY, class P>
+__device__ __forceinline__ void primal_row_step(int j, double acc, const P& p,
+                                                const pdlp_scalars* st, int it_off, TX* xbar,
+                                                TX* xout, TX* xhat, TX* slack, TX* aty)
+{
+  const double tau  = st->tau;
+  const double xj   = (double)p.x;
+  const double next = xj - tau * ((double)p.c - acc);
+  const double cl   = fmax(fmin(next, (double)p.up), (double)p.lo);
+  if constexpr (MAJOR) {
+    xhat[j]  = (TX)cl;
+    slack[j] = (TX)((cl - next) / tau);
+  }
+  const double xb = 2.0 * cl - xj;
+  if constexpr (SAVE_ATY) aty[j] = (TX)acc;
+  if constexpr (HALPERN) {
+    const double w = halpern_weight(st, it_off);
+    xbar[j]        = (TX)xb;
+    xout[j]        = (TX)(w * xb + (1.0 - w) * (double)p.xa);
+  } else {
+    xbar[j] = (TX)xb;
+  }
+}
+
+// The dual update of one constraint i; returns (y_bar_i - y_i)^2 for the fixed-point error.
+template <typename TX, bool MAJOR, bool HALPERN, class P>
+__device__ __forceinline__ double dual_row_step(int i, double acc, const P& p,
+                                                const pdlp_scalars* st, int it_off, TX* ybar,
+                                                TX* yout, TX* yhat)
+{
+  const double sigma = st->sigma;
+  const double yi    = (double)p.y;
+  const double t     = yi / sigma - acc;
+  const double tp    = fmax(-(double)p.up, fmin(t, -(double)p.lo));
+  const double ny    = (t - tp) * sigma;
+  if constexpr (MAJOR) yhat[i] = (TX)ny;
+  const double yb = 2.0 * ny - yi;
+  if constexpr (HALPERN) {
+    const double w = halpern_weight(st, it_off);
+    yout[i]        = (TX)(w * yb + (1.0 - w) * (double)p.ya);
+  } else {
+    ybar[i] = (TX)yb;
+  }
+  const double d = yb - yi;
+  return d * d;
+}
+
 // Row j of A^T:  x_next = x - tau (c - A^T y);  x_hat = clamp(x_next, l, u);
 //                slack = (x_hat - x_next) / tau;  x_bar = 2 x_hat - x;
 //                (fused Halpern)  x <- w x_bar + (1 - w) x_anchor.
@@ -226,23 +294,8 @@ struct primal_epi {
   }
   __device__ __forceinline__ void operator()(int j, double acc, const pre_t& p, red_t<0>&) const
   {
-    const double tau  = st->tau;
-    const double xj   = (double)p.x;
-    const double next = xj - tau * ((double)p.c - acc);
-    const double cl   = fmax(fmin(next, (double)p.up), (double)p.lo);
-    if constexpr (MAJOR) {
-      xhat[j]  = (TX)cl;
-      slack[j] = (TX)((cl - next) / tau);
-    }
-    const double xb = 2.0 * cl - xj;
-    if constexpr (SAVE_ATY) aty[j] = (TX)acc;
-    if constexpr (HALPERN) {
-      const double w = halpern_weight(st, it_off);
-      xbar[j]        = (TX)xb;
-      xout[j]        = (TX)(w * xb + (1.0 - w) * (double)p.xa);
-    } else {
-      xbar[j] = (TX)xb;
-    }
+    primal_row_step<TX, MAJOR, HALPERN, SAVE_ATY>(j, acc, p, st, it_off, xbar, xout, xhat, slack,
+                                                  aty);
   }
 };
 
@@ -271,23 +324,8 @@ struct dual_epi {
   __device__ __forceinline__ void operator()(int i, double acc, const pre_t& p,
                                              red_t<kRed>& r) const
   {
-    const double sigma = st->sigma;
-    const double yi    = (double)p.y;
-    const double t     = yi / sigma - acc;
-    const double tp    = fmax(-(double)p.up, fmin(t, -(double)p.lo));
-    const double ny    = (t - tp) * sigma;
-    if constexpr (MAJOR) yhat[i] = (TX)ny;
-    const double yb = 2.0 * ny - yi;
-    if constexpr (FPE) {
-      const double d = yb - yi;
-      r.v[0] += d * d;
-    }
-    if constexpr (HALPERN) {
-      const double w = halpern_weight(st, it_off);
-      yout[i]        = (TX)(w * yb + (1.0 - w) * (double)p.ya);
-    } else {
-      ybar[i] = (TX)yb;
-    }
+    const double d2 = dual_row_step<TX, MAJOR, HALPERN>(i, acc, p, st, it_off, ybar, yout, yhat);
+    if constexpr (FPE) r.v[0] += d2;
   }
 };
 
@@ -329,8 +367,8 @@ __global__ void halpern_kernel(TX* x, const TX* xbar, const TX* xa, int n, TX* y
   }
 }
 
-__global__ void advance_kernel(pdlp_scalars* st, int steps) { st->t0 += steps; }
-__global__ void set_scalars_kernel(pdlp_scalars* st, double tau, double sigma, double eta,
+static __global__ void advance_kernel(pdlp_scalars* st, int steps) { st->t0 += steps; }
+static __global__ void set_scalars_kernel(pdlp_scalars* st, double tau, double sigma, double eta,
                                    double omega, long long t0)
 {
   st->tau   = tau;
@@ -482,7 +520,7 @@ struct power_state {
   int iters;
 };
 
-__global__ void power_normalize_kernel(const double* z, double* q, int m, const double* sumsq,
+static __global__ void power_normalize_kernel(const double* z, double* q, int m, const double* sumsq,
                                        power_state* ps)
 {
   if (ps->done) return;
@@ -493,7 +531,7 @@ __global__ void power_normalize_kernel(const double* z, double* q, int m, const 
 }
 
 // q <- q * (-s2) + z ; partial sum of squares of the result.
-__global__ void __launch_bounds__(kBlock) power_residual_kernel(double* q, const double* z, int m,
+static __global__ void __launch_bounds__(kBlock) power_residual_kernel(double* q, const double* z, int m,
                                                                 const double* s2,
                                                                 const power_state* ps,
                                                                 double* partials)
@@ -511,7 +549,7 @@ __global__ void __launch_bounds__(kBlock) power_residual_kernel(double* q, const
   block_reduce_store<1>(r, partials);
 }
 
-__global__ void power_check_kernel(power_state* ps, const double* s2, const double* rsq, double tol)
+static __global__ void power_check_kernel(power_state* ps, const double* s2, const double* rsq, double tol)
 {
   if (ps->done) return;
   ps->s2    = *s2;
@@ -572,7 +610,7 @@ __global__ void __launch_bounds__(kBlock) row_scaled_abs_kernel(const dev_sell<d
 }
 
 // d[i] <- d[i] / sqrt(v[i]) where v[i] > 0 (a_divides_sqrt_b_bounded, utils.cuh:156-163)
-__global__ void apply_root_scaling_kernel(double* d, const double* v, int n)
+static __global__ void apply_root_scaling_kernel(double* d, const double* v, int n)
 {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double b = v[i];
@@ -611,7 +649,7 @@ __global__ void __launch_bounds__(kBlock) scale_values_kernel(const dev_sell<dou
 }
 
 // First pass of the vector scaling: c*dc, bounds/dc (divide_check_zero), constraint bounds*dr.
-__global__ void scale_vectors_kernel(const double* c, const double* l, const double* u,
+static __global__ void scale_vectors_kernel(const double* c, const double* l, const double* u,
                                      const double* lc, const double* uc, const double* dc,
                                      const double* dr, int n, int m, double* cs, double* ls,
                                      double* us, double* lcs, double* ucs)
@@ -672,7 +710,7 @@ __global__ void scale_initial_kernel(const double* v, const double* d, double fa
 
 // Correction LP of an iterative-refinement pass (FP64, unscaled, internal order):
 //   c' = dd (c - A^T y),  [l', u'] = dp ([l, u] - x),  [lc', uc'] = dp ([lc, uc] - A x).
-__global__ void refine_vectors_kernel(const double* c0, const double* l0, const double* u0,
+static __global__ void refine_vectors_kernel(const double* c0, const double* l0, const double* u0,
                                       const double* lc0, const double* uc0, const double* x,
                                       const double* ax, const double* aty, double dp, double dd,
                                       int n, int m, double* c, double* l, double* u, double* lc,
@@ -692,7 +730,7 @@ __global__ void refine_vectors_kernel(const double* c0, const double* l0, const 
 }
 
 // x += z / dp, y += w / dd, s = s_w / dd (refinement update).
-__global__ void refine_update_kernel(double* x, double* y, double* s, const double* z,
+static __global__ void refine_update_kernel(double* x, double* y, double* s, const double* z,
                                      const double* w, const double* sw, double dp, double dd,
                                      int n, int m)
 {

@@ -366,58 +366,73 @@ pdlp_params params_from_settings(const lp_settings& st)
   return prm;
 }
 
+// The checks and special cases that come before PDLP (reference solve.cu:1124-1342 and
+// problem_checking.cu).  Returns true when the problem goes to PDLP with constraint bounds lo / up;
+// otherwise `out` already holds the answer.
+static bool prepare_for_pdlp(const lp_problem& p, const lp_settings& st, std::vector<double>& lo,
+                             std::vector<double>& up, lp_solution& out)
+{
+  const auto t0 = std::chrono::steady_clock::now();
+  if (p.quadratic) {
+    out.error_code    = CUOPT_VALIDATION_ERROR;
+    out.error_message = "Quadratic objectives are not supported by this library.";
+    return false;
+  }
+  if (p.is_mip()) {
+    out.error_code    = CUOPT_VALIDATION_ERROR;
+    out.error_message = "Integer variables are not supported by this library (LP only).";
+    return false;
+  }
+  std::string err = validate_problem(p);
+  if (!err.empty()) {
+    out.error_code    = CUOPT_VALIDATION_ERROR;
+    out.error_message = err;
+    return false;
+  }
+  trace("validate_problem");
+  p.constraint_bounds(lo, up);
+  // has_crossing_bounds (reference problem_checking.cu:316-339)
+  for (int j = 0; j < p.n; ++j)
+    if (!(p.var_up[j] >= p.var_lo[j])) {
+      out.r.status = CUOPT_TERIMINATION_STATUS_INFEASIBLE;
+      return false;
+    }
+  if (p.ranged)
+    for (int i = 0; i < p.m; ++i)
+      if (!(up[i] >= lo[i])) {
+        out.r.status = CUOPT_TERIMINATION_STATUS_INFEASIBLE;
+        return false;
+      }
+  const int method = st.i(CUOPT_METHOD);
+  if (p.m == 0) {
+    if (method == CUOPT_METHOD_PDLP) {
+      out.r.status = CUOPT_TERIMINATION_STATUS_NUMERICAL_ERROR;
+      return false;
+    }
+    out = solve_without_constraints(p);
+    out.r.solve_time = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return false;
+  }
+  if (p.n == 0) {
+    out.r.status = CUOPT_TERIMINATION_STATUS_NUMERICAL_ERROR;
+    return false;
+  }
+  return true;
+}
+
+static void set_error(lp_solution& out, int code, const char* what)
+{
+  out.error_code    = code;
+  out.error_message = what;
+}
+
 lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
 {
   lp_solution out;
-  const auto t0 = std::chrono::steady_clock::now();
   trace("solve_problem: start");
   try {
-    if (p.quadratic) {
-      out.error_code    = CUOPT_VALIDATION_ERROR;
-      out.error_message = "Quadratic objectives are not supported by this library.";
-      return out;
-    }
-    if (p.is_mip()) {
-      out.error_code    = CUOPT_VALIDATION_ERROR;
-      out.error_message = "Integer variables are not supported by this library (LP only).";
-      return out;
-    }
-    std::string err = validate_problem(p);
-    if (!err.empty()) {
-      out.error_code    = CUOPT_VALIDATION_ERROR;
-      out.error_message = err;
-      return out;
-    }
-    trace("validate_problem");
     std::vector<double> lo, up;
-    p.constraint_bounds(lo, up);
-    // has_crossing_bounds (reference problem_checking.cu:316-339)
-    for (int j = 0; j < p.n; ++j)
-      if (!(p.var_up[j] >= p.var_lo[j])) {
-        out.r.status = CUOPT_TERIMINATION_STATUS_INFEASIBLE;
-        return out;
-      }
-    if (p.ranged)
-      for (int i = 0; i < p.m; ++i)
-        if (!(up[i] >= lo[i])) {
-          out.r.status = CUOPT_TERIMINATION_STATUS_INFEASIBLE;
-          return out;
-        }
-    const int method = st.i(CUOPT_METHOD);
-    if (p.m == 0) {
-      if (method == CUOPT_METHOD_PDLP) {
-        out.r.status = CUOPT_TERIMINATION_STATUS_NUMERICAL_ERROR;
-        return out;
-      }
-      out = solve_without_constraints(p);
-      out.r.solve_time =
-        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-      return out;
-    }
-    if (p.n == 0) {
-      out.r.status = CUOPT_TERIMINATION_STATUS_NUMERICAL_ERROR;
-      return out;
-    }
+    if (!prepare_for_pdlp(p, st, lo, up, out)) return out;
     pdlp_params prm = params_from_settings(st);
     if ((int)st.initial_primal.size() == p.n) prm.initial_primal = st.initial_primal;
     if ((int)st.initial_dual.size() == p.m) prm.initial_dual = st.initial_dual;
@@ -452,6 +467,139 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
   } catch (const std::exception& e) {
     out.error_code    = CUOPT_RUNTIME_ERROR;
     out.error_message = e.what();
+  }
+  return out;
+}
+
+// One block-diagonal batch on the device (see pdlp_batch_solve_device).
+static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
+                              const std::vector<size_t>& ids,
+                              const std::vector<std::vector<double>>& lo,
+                              const std::vector<std::vector<double>>& up, const pdlp_params& prm,
+                              std::vector<lp_solution>& out)
+{
+  batch_device_input bi;
+  bi.count = (int)ids.size();
+  bi.row_start.assign(1, 0);
+  bi.col_start.assign(1, 0);
+  int64_t nnz = 0;
+  for (size_t id : ids) {
+    const lp_problem& p = *ps[id];
+    bi.row_start.push_back(bi.row_start.back() + p.m);
+    bi.col_start.push_back(bi.col_start.back() + p.n);
+    nnz += p.row_off[p.m];
+    bi.obj_offset.push_back(p.obj_offset);
+    bi.maximize.push_back(p.maximize ? 1 : 0);
+  }
+  const int m = bi.row_start.back(), n = bi.col_start.back();
+  std::vector<int> off(m + 1), idx(std::max<int64_t>(nnz, 1)), rinst(m), cinst(n);
+  std::vector<double> val(std::max<int64_t>(nnz, 1)), c(n), clo(m), cup(m), vlo(n), vup(n);
+  for (int b = 0; b < bi.count; ++b) {
+    const lp_problem& p = *ps[ids[b]];
+    const int r0 = bi.row_start[b], c0 = bi.col_start[b], e0 = off[r0];
+    for (int i = 0; i < p.m; ++i) {
+      off[r0 + i + 1] = e0 + p.row_off[i + 1];
+      clo[r0 + i]     = lo[ids[b]][i];
+      cup[r0 + i]     = up[ids[b]][i];
+      rinst[r0 + i]   = b;
+    }
+    for (int k = 0; k < p.row_off[p.m]; ++k) {
+      idx[e0 + k] = p.col_idx[k] + c0;
+      val[e0 + k] = p.val[k];
+    }
+    for (int j = 0; j < p.n; ++j) {
+      c[c0 + j]     = p.c[j];
+      vlo[c0 + j]   = p.var_lo[j];
+      vup[c0 + j]   = p.var_up[j];
+      cinst[c0 + j] = b;
+    }
+  }
+  trace("batch: concatenate");
+  cudaStream_t s;
+  B200_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct stream_guard {
+    cudaStream_t s;
+    ~stream_guard() { cudaStreamDestroy(s); }
+  } guard{s};
+  alloc_scope scope(s);
+  configure_pool_once();
+  dbuf<int> doff(m + 1), didx(idx.size()), dri(m), dci(n);
+  dbuf<double> dval(val.size()), dc(n), dlo(m), dup(m), dvl(n), dvu(n), x(n), y(m), rc(n);
+  doff.upload(off.data(), m + 1, s);
+  didx.upload(idx.data(), idx.size(), s);
+  dval.upload(val.data(), val.size(), s);
+  dri.upload(rinst.data(), m, s);
+  dci.upload(cinst.data(), n, s);
+  dc.upload(c.data(), n, s);
+  dlo.upload(clo.data(), m, s);
+  dup.upload(cup.data(), m, s);
+  dvl.upload(vlo.data(), n, s);
+  dvu.upload(vup.data(), n, s);
+  bi.m        = m;
+  bi.n        = n;
+  bi.row_off  = doff.data();
+  bi.col_idx  = didx.data();
+  bi.val      = dval.data();
+  bi.c        = dc.data();
+  bi.con_lo   = dlo.data();
+  bi.con_up   = dup.data();
+  bi.var_lo   = dvl.data();
+  bi.var_up   = dvu.data();
+  bi.row_inst = dri.data();
+  bi.col_inst = dci.data();
+  trace("batch: upload");
+  std::vector<pdlp_result> rs = pdlp_batch_solve_device(bi, prm, s, x.data(), y.data(), rc.data());
+  std::vector<double> hx(n), hy(m), hrc(n);
+  x.download(hx.data(), n, s);
+  y.download(hy.data(), m, s);
+  rc.download(hrc.data(), n, s);
+  B200_CUDA_CHECK(cudaStreamSynchronize(s));
+  for (int b = 0; b < bi.count; ++b) {
+    lp_solution& o = out[ids[b]];
+    o.r            = rs[b];
+    o.r.x.assign(hx.begin() + bi.col_start[b], hx.begin() + bi.col_start[b + 1]);
+    o.r.rc.assign(hrc.begin() + bi.col_start[b], hrc.begin() + bi.col_start[b + 1]);
+    o.r.y.assign(hy.begin() + bi.row_start[b], hy.begin() + bi.row_start[b + 1]);
+  }
+}
+
+std::vector<lp_solution> solve_batch(const std::vector<const lp_problem*>& ps, const lp_settings& st)
+{
+  std::vector<lp_solution> out(ps.size());
+  std::vector<std::vector<double>> lo(ps.size()), up(ps.size());
+  std::vector<size_t> eligible;
+  for (size_t i = 0; i < ps.size(); ++i) {
+    try {
+      if (prepare_for_pdlp(*ps[i], st, lo[i], up[i], out[i])) eligible.push_back(i);
+    } catch (const std::exception& e) {
+      set_error(out[i], CUOPT_RUNTIME_ERROR, e.what());
+    }
+  }
+  const pdlp_params prm = params_from_settings(st);
+  // Chunks that fit the batch layout: at most 65535 instances and int32 totals.
+  size_t pos = 0;
+  while (pos < eligible.size()) {
+    std::vector<size_t> chunk;
+    int64_t m = 0, n = 0, nnz = 0;
+    while (pos < eligible.size() && chunk.size() < 65535) {
+      const lp_problem& p = *ps[eligible[pos]];
+      if (!chunk.empty() && (m + p.m >= INT_MAX || n + p.n >= INT_MAX ||
+                             nnz + p.row_off[p.m] >= INT_MAX))
+        break;
+      m += p.m;
+      n += p.n;
+      nnz += p.row_off[p.m];
+      chunk.push_back(eligible[pos++]);
+    }
+    try {
+      solve_batch_chunk(ps, chunk, lo, up, prm, out);
+    } catch (const std::bad_alloc&) {
+      for (size_t id : chunk) set_error(out[id], CUOPT_OUT_OF_MEMORY, "Memory allocation failed");
+    } catch (const std::invalid_argument& e) {
+      for (size_t id : chunk) set_error(out[id], CUOPT_VALIDATION_ERROR, e.what());
+    } catch (const std::exception& e) {
+      for (size_t id : chunk) set_error(out[id], CUOPT_RUNTIME_ERROR, e.what());
+    }
   }
   return out;
 }

@@ -81,6 +81,10 @@ pdlp_params params_from_settings(const lp_settings& s);
 // Full solve as done by cuOptSolve: validation, trivial cases, PDLP.
 lp_solution solve_problem(const lp_problem& p, const lp_settings& s);
 
+// Solves independent problems together: every problem that reaches PDLP joins one block-diagonal
+// batch (per-instance Stable3 state); the others are answered as solve_problem would.
+std::vector<lp_solution> solve_batch(const std::vector<const lp_problem*>& ps, const lp_settings& s);
+
 // MPS input / output (reference cpp/libmps_parser).  read_mps returns 0 or CUOPT_MPS_* codes.
 int read_mps(const std::string& path, lp_problem& out, std::string& err);
 int write_mps(const lp_problem& p, const std::string& path);

@@ -8,6 +8,7 @@
 #include "device_layout.cuh"
 #include "kernels.cuh"
 #include "pdlp_engine.hpp"
+#include "pdlp_schedule.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -21,35 +22,6 @@
 namespace cuopt_b200 {
 
 namespace {
-
-constexpr int kOptimal = 1, kIterationLimit = 4, kTimeLimit = 5, kNumericalError = 6,
-              kPrimalFeasible = 7, kNoTermination = 0;
-
-// Stable3 constants (reference solve.cu:167-209, pdlp_hyper_params.cuh:12-56,
-// pdlp_restart_strategy.cu:689-836, pdlp.cu:2620-2731).
-constexpr long kMajor                 = 200;
-constexpr double kArtificialRestart   = 0.36;
-constexpr double kSufficientReduction = 0.2;
-constexpr double kNecessaryReduction  = 0.8;
-constexpr double kKp = 0.99, kKi = 0.01, kKd = 0.0, kISmooth = 0.3;
-constexpr int kPowerMaxIters          = 5000;
-constexpr double kPowerTol            = 1e-4;
-constexpr double kStepScaling         = 0.998;
-constexpr int kRuizIterations         = 10;
-constexpr double kPcAlpha             = 1.0;
-
-long conditional_major(long k)  // reference utils.cuh:63-81
-{
-  long step = 10, threshold = 1000;
-  while (k >= threshold) {
-    step *= 10;
-    threshold *= 10;
-  }
-  return step;
-}
-
-bool is_check(long k) { return (k % kMajor == 0 && k > 0) || k <= 0 || k % conditional_major(k) == 0; }
-bool is_major_step(long k) { return ((k + 1) % kMajor == 0) || ((k + 2) % conditional_major(k + 2)) == 0; }
 
 double now_s()
 {
@@ -820,25 +792,6 @@ class engine {
 
 namespace {
 
-// The engine captures CUDA graphs, which the legacy default stream does not allow, so it always
-// works on its own non-blocking stream ordered after / before the caller's stream with events.
-struct joined_stream {
-  cudaStream_t caller, own = nullptr;
-  cudaEvent_t ev = nullptr;
-  explicit joined_stream(cudaStream_t c) : caller(c)
-  {
-    B200_CUDA_CHECK(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
-    B200_CUDA_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    B200_CUDA_CHECK(cudaEventRecord(ev, caller));
-    B200_CUDA_CHECK(cudaStreamWaitEvent(own, ev, 0));
-  }
-  ~joined_stream()
-  {
-    if (cudaEventRecord(ev, own) == cudaSuccess) cudaStreamWaitEvent(caller, ev, 0);
-    cudaEventDestroy(ev);
-    cudaStreamDestroy(own);
-  }
-};
 
 }  // namespace
 

@@ -77,7 +77,34 @@ struct lp_device_input {
 
 // Runs PDLP (Stable3) on the GPU from host arrays (uploads them, returns x / y / rc on the host).
 // Throws std::exception subclasses on CUDA or input errors.
+// A block-diagonal batch of `count` independent LPs on the device: the CSR concatenates the
+// instances' rows with global column indices; row_inst / col_inst give every user row / column
+// its instance (device); row_start / col_start (host, count + 1) delimit the instances.
+struct batch_device_input {
+  int count = 0;
+  int m = 0, n = 0;
+  const int* row_off   = nullptr;
+  const int* col_idx   = nullptr;
+  const double* val    = nullptr;
+  const double* c      = nullptr;
+  const double* con_lo = nullptr;
+  const double* con_up = nullptr;
+  const double* var_lo = nullptr;
+  const double* var_up = nullptr;
+  const int* row_inst  = nullptr;
+  const int* col_inst  = nullptr;
+  std::vector<int> row_start, col_start;
+  std::vector<double> obj_offset;
+  std::vector<char> maximize;
+};
+
 pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p);
+
+// Solves every instance of the batch with its own Stable3 state; x / y / reduced costs are written
+// to device arrays of the batch's total sizes (user order, instances concatenated).
+std::vector<pdlp_result> pdlp_batch_solve_device(const batch_device_input& in,
+                                                 const pdlp_params& p, cudaStream_t stream,
+                                                 double* x_out, double* y_out, double* rc_out);
 
 // Runs PDLP on device-resident arrays.  x_out (n), y_out (m), rc_out (n) are device arrays in the
 // user's order; the returned result carries statistics only (its x / y / rc stay empty).

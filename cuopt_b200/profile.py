@@ -5,7 +5,10 @@
 
 `solve`  runs one full solve to 1e-6 relative KKT from device-resident inputs (cuOptSolveDevice);
 `sweeps` prepares the LP and launches the two fused PDHG sweeps separately between CUDA events
-         (cuOptProfilePDHGSweeps).  Prints one JSON line with the timings.
+         (cuOptProfilePDHGSweeps).
+`batch`  (config c3) solves the 512-instance batch in one cuOptBatchSolve call and a sample of the
+         same instances one by one with cuOptSolve (FP64, 1e-6).
+Prints one JSON line with the timings.
 """
 from __future__ import annotations
 
@@ -40,7 +43,10 @@ def main() -> None:
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c1_small")
-    ap.add_argument("--mode", choices=["solve", "sweeps"], default="sweeps")
+    ap.add_argument("--mode", choices=["solve", "sweeps", "batch"], default="sweeps")
+    ap.add_argument("--count", type=int, default=512, help="batch mode: instances")
+    ap.add_argument("--sequential", type=int, default=64,
+                    help="batch mode: instances also solved one by one (timing sample)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--iterations", type=int, default=3)
     ap.add_argument("--tol", type=float, default=1e-6)
@@ -48,6 +54,9 @@ def main() -> None:
     ap.add_argument("--refine", type=int, default=0, help="FP64 refinement passes (mixed precision)")
     a = ap.parse_args()
 
+    if a.mode == "batch":
+        print(json.dumps(run_batch(a)))
+        return
     m, n, k, seed = CONFIGS[a.config]
     lp = gen.constructed_lp(m, n, k, seed=seed) if k else gen.skewed_lp(m, n, seed=seed)
     dev = torch.device("cuda", 0)
@@ -100,6 +109,60 @@ def main() -> None:
             sys.exit(1)
     L.cuOptDestroySolverSettings(C.byref(s))
     print(json.dumps(out))
+
+
+def run_batch(a) -> dict:
+    """Config 3: one batched solve of `count` uneven LPs vs the same LPs solved one at a time."""
+    import numpy as np
+
+    from cuopt_b200 import generators as gen
+    from cuopt_b200 import linear_programming as lpm
+
+    lps = gen.batch_lps(a.count, seed=3000)
+    dms = []
+    for lp in lps:
+        dm = lpm.DataModel()
+        dm.set_csr_constraint_matrix(lp.val, lp.col_idx, lp.row_off)
+        dm.set_objective_coefficients(lp.c)
+        dm.set_constraint_lower_bounds(lp.con_lo)
+        dm.set_constraint_upper_bounds(lp.con_up)
+        dm.set_variable_lower_bounds(lp.var_lo)
+        dm.set_variable_upper_bounds(lp.var_up)
+        dms.append(dm)
+    st = lpm.SolverSettings()
+    st.set_optimality_tolerance(a.tol)
+    st.set_parameter(lpm.CUOPT_METHOD, int(lpm.SolverMethod.PDLP))
+    st.set_parameter(lpm.CUOPT_LOG_TO_CONSOLE, False)
+    if a.time_limit > 0:
+        st.set_parameter(lpm.CUOPT_TIME_LIMIT, a.time_limit)
+    sols, batch_s = lpm.BatchSolve(dms, st)
+    status = [int(s.get_termination_status()) for s in sols]
+    iters = [s.get_lp_stats()["nb_iterations"] for s in sols]
+    obj_err = [abs(s.get_primal_objective() - lp.optimal_objective) / max(1.0, abs(lp.optimal_objective))
+               for s, lp in zip(sols, lps)]
+    out = {"config": "c3", "count": a.count, "m_total": int(sum(lp.m for lp in lps)),
+           "n_total": int(sum(lp.n for lp in lps)), "nnz_total": int(sum(lp.nnz for lp in lps)),
+           "batch_s": batch_s, "batch_lps_per_s": a.count / batch_s,
+           "optimal": status.count(1), "max_iterations": max(iters),
+           "mean_iterations": float(np.mean(iters)), "max_objective_rel_error": max(obj_err),
+           "batch_setup_s": sols[0].stats.get("setup_time"),
+           "iterations_p50_p90_p99": [float(np.percentile(iters, q)) for q in (50, 90, 99)],
+           "max_power_iterations": max(s.stats.get("power_iterations", 0) for s in sols)}
+    if a.sequential > 0:
+        pick = np.linspace(0, a.count - 1, min(a.sequential, a.count)).astype(int)
+        t0 = time.perf_counter()
+        seq_iters_equal = 0
+        for i in pick:
+            s1 = lpm.Solve(dms[i], st)
+            seq_iters_equal += int(s1.get_lp_stats()["nb_iterations"] == iters[i])
+        seq_s = time.perf_counter() - t0
+        out.update({"sequential_sample": int(len(pick)), "sequential_s": seq_s,
+                    "sequential_s_per_lp": seq_s / len(pick),
+                    "sequential_lps_per_s": len(pick) / seq_s,
+                    "sequential_same_iterations": seq_iters_equal,
+                    "speedup_batch_vs_sequential": (len(pick) / seq_s and
+                                                    (a.count / batch_s) / (len(pick) / seq_s))})
+    return out
 
 
 if __name__ == "__main__":

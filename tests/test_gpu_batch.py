@@ -1,0 +1,97 @@
+"""GPU parity tests of the batched PDLP (cuOptBatchSolve / BatchSolve): every instance of a
+block-diagonal batch must follow its own single-LP Stable3 trajectory.
+
+Reference for every expectation: the CPU oracle solving each instance alone (an FP64 restatement of
+the reference's Stable3 PDLP) and the optima known by construction.  Tolerances: iterates after the
+same number of iterations agree with the oracle to 1e-9 relative to the vector's magnitude
+(summation order differs); solved instances reach the relative KKT targets asked for.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from cuopt_b200 import generators as gen
+from cuopt_b200 import linear_programming as lpm
+from oracle import oracle as O
+from tests.helpers import datamodel_from_lp, oracle_view, rel, settings
+
+pytestmark = pytest.mark.gpu
+
+ITERATE_RTOL = 1e-9
+
+
+@pytest.fixture(scope="module")
+def instances():
+    """Uneven sizes, a maximisation with an offset, and one instance with long rows."""
+    lps = [gen.constructed_lp(m, int(2.5 * m), k, seed=50 + i)
+           for i, (m, k) in enumerate([(200, 6), (1300, 12), (450, 8), (3000, 9)])]
+    lps.append(gen.skewed_lp(400, 3000, seed=7, cap=3000))
+    return lps
+
+
+def _models(lps, maximize_index=None):
+    dms = []
+    for i, lp in enumerate(lps):
+        if i == maximize_index:
+            dm = datamodel_from_lp(lp, maximize=True, offset=1.25)
+            dm.set_objective_coefficients(-lp.c)
+        else:
+            dm = datamodel_from_lp(lp)
+        dms.append(dm)
+    return dms
+
+
+@pytest.mark.parametrize("k", [10, 200, 1000])
+def test_batch_iterates_match_single_oracle(instances, k):
+    dms = _models(instances)
+    sols, _ = lpm.BatchSolve(dms, settings(tol=1e-12, iteration_limit=k))
+    for lp, sol in zip(instances, sols):
+        res, x, y, rc = O.solve(lp, tol=1e-12, iteration_limit=k)
+        assert sol.get_termination_status() == lpm.LPTerminationStatus.IterationLimit
+        assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+        assert np.max(np.abs(sol.get_primal_solution() - x)) <= ITERATE_RTOL * (1 + np.abs(x).max())
+        assert np.max(np.abs(sol.get_dual_solution() - y)) <= ITERATE_RTOL * (1 + np.abs(y).max())
+        assert np.max(np.abs(sol.get_reduced_cost() - rc)) <= ITERATE_RTOL * (1 + np.abs(rc).max())
+        assert rel(sol.get_primal_objective(), res["primal_obj"]) <= 1e-9
+
+
+def test_batch_solves_to_tolerance_like_single_solves(instances):
+    """Each instance terminates Optimal at 1e-6 at the oracle's iteration count (±5 %), with its
+    own restarts; the constructed optima are recovered."""
+    lps = instances[:4]
+    dms = _models(lps, maximize_index=2)
+    sols, _ = lpm.BatchSolve(dms, settings(tol=1e-6))
+    for i, (lp, dm, sol) in enumerate(zip(lps, dms, sols)):
+        res, _, _, _ = O.solve(oracle_view(dm), tol=1e-6)
+        assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+        assert res["status"] == 1
+        assert abs(sol.get_lp_stats()["nb_iterations"] - res["iterations"]) <= \
+            0.05 * res["iterations"] + 10
+        want = -lp.optimal_objective + 1.25 if i == 2 else lp.optimal_objective
+        assert rel(sol.get_primal_objective(), want) <= 1e-5
+
+
+def test_batch_is_deterministic(instances):
+    dms = _models(instances)
+    a, _ = lpm.BatchSolve(dms, settings(tol=1e-12, iteration_limit=300))
+    b, _ = lpm.BatchSolve(dms, settings(tol=1e-12, iteration_limit=300))
+    for sa, sb in zip(a, b):
+        assert np.array_equal(sa.get_primal_solution(), sb.get_primal_solution())
+        assert np.array_equal(sa.get_dual_solution(), sb.get_dual_solution())
+
+
+def test_batch_mixes_special_cases(golden, golden_dir, instances):
+    """Problems that never reach PDLP (no constraints) are answered as single solves would."""
+    dms = [datamodel_from_lp(instances[0]),
+           lpm.ReadMps(golden_dir / "lp-model-no-constraints.mps"),
+           datamodel_from_lp(instances[2])]
+    s = settings(tol=1e-6, method=lpm.SolverMethod.Concurrent)
+    sols, _ = lpm.BatchSolve(dms, s)
+    assert sols[0].get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert sols[2].get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert sols[1].get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert not sols[1].get_solved_by_pdlp()
+    assert abs(sols[1].get_primal_objective() - golden["no_constraints_objective"]["value"]) <= 1e-4
+    single = lpm.Solve(datamodel_from_lp(instances[2]), s)
+    assert sols[2].get_lp_stats()["nb_iterations"] == single.get_lp_stats()["nb_iterations"]
