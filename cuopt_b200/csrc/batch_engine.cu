@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <limits>
 #include <map>
 #include <random>
@@ -388,40 +389,73 @@ __global__ void b_advance_kernel(pdlp_scalars* sc, const int* active, int count,
     if (active[b]) sc[b].t0 += steps;
 }
 
-// Power iteration per instance (reference pdlp.cu:2620-2731).
+// Power iteration per instance (reference pdlp.cu:2620-2731), one block per instance.
 struct b_power_state {
   double s2;
   double resid;
   int iters;
   int pad;
 };
-__global__ void b_power_normalize_kernel(const double* z, double* q, int m, const int* rinst,
-                                         const int* pactive, const double* sumsq)
+
+// Fixed-order block sum of per-thread values (compensated per thread, then a fixed tree).
+__device__ __forceinline__ double block_sum(const ksum& acc, double* sm)
 {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-    const int b = rinst[i];
-    if (!pactive[b]) continue;
-    q[i] = z[i] / sqrt(sumsq[b]);
+  sm[threadIdx.x] = acc.value();
+  __syncthreads();
+  for (int h = kBlock / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) sm[threadIdx.x] += sm[threadIdx.x + h];
+    __syncthreads();
   }
+  const double v = sm[0];
+  __syncthreads();
+  return v;
 }
-__global__ void b_power_residual_kernel(double* q, const double* z, int m, const int* rinst,
-                                        const int* pactive, const double* s2, double* rowbuf)
+
+// q = z / |z| over the instance's rows.
+__global__ void __launch_bounds__(kBlock) b_power_normalize_kernel(const double* z, double* q,
+                                                                   const int4* ranges,
+                                                                   const int* pactive)
 {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-    const int b = rinst[i];
-    if (!pactive[b]) continue;
-    const double v = q[i] * -s2[b] + z[i];
+  const int b = blockIdx.x;
+  if (!pactive[b]) return;
+  const int4 r = ranges[b];
+  __shared__ double sm[kBlock];
+  ksum acc;
+  for (int i = r.x + threadIdx.x; i < r.y; i += kBlock) acc.add(z[i] * z[i]);
+  for (int i = r.z + threadIdx.x; i < r.w; i += kBlock) acc.add(z[i] * z[i]);
+  const double nq = sqrt(block_sum(acc, sm));
+  for (int i = r.x + threadIdx.x; i < r.y; i += kBlock) q[i] = z[i] / nq;
+  for (int i = r.z + threadIdx.x; i < r.w; i += kBlock) q[i] = z[i] / nq;
+}
+
+// s2 = q . z (rowbuf holds q_i z_i); q <- q (-s2) + z; residual |q|; convergence test.
+__global__ void __launch_bounds__(kBlock)
+  b_power_update_kernel(double* q, const double* z, const double* rowbuf, const int4* ranges,
+                        int* pactive, b_power_state* ps, double tol, int* remaining)
+{
+  const int b = blockIdx.x;
+  if (!pactive[b]) return;
+  const int4 r = ranges[b];
+  __shared__ double sm[kBlock];
+  ksum a1;
+  for (int i = r.x + threadIdx.x; i < r.y; i += kBlock) a1.add(rowbuf[i]);
+  for (int i = r.z + threadIdx.x; i < r.w; i += kBlock) a1.add(rowbuf[i]);
+  const double s2 = block_sum(a1, sm);
+  ksum a2;
+  for (int i = r.x + threadIdx.x; i < r.y; i += kBlock) {
+    const double v = q[i] * -s2 + z[i];
     q[i]           = v;
-    rowbuf[i]      = v * v;
+    a2.add(v * v);
   }
-}
-__global__ void b_power_check_kernel(b_power_state* ps, int* pactive, const double* s2,
-                                     const double* rsq, int count, double tol, int* remaining)
-{
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < count; b += gridDim.x * blockDim.x) {
-    if (!pactive[b]) continue;
-    ps[b].s2    = s2[b];
-    ps[b].resid = sqrt(rsq[b]);
+  for (int i = r.z + threadIdx.x; i < r.w; i += kBlock) {
+    const double v = q[i] * -s2 + z[i];
+    q[i]           = v;
+    a2.add(v * v);
+  }
+  const double rsq = block_sum(a2, sm);
+  if (threadIdx.x == 0) {
+    ps[b].s2    = s2;
+    ps[b].resid = sqrt(rsq);
     ps[b].iters += 1;
     if (ps[b].resid < tol) {
       pactive[b] = 0;
@@ -724,56 +758,64 @@ class batch_engine {
     dbuf<b_power_state> ps(B_);
     ps.zero(s_);
     dbuf<int> pact(B_), remaining(1);
-    std::vector<int> ones(B_, 1);
-    pact.upload(ones.data(), B_, s_);
+    std::vector<int> pact_h(B_, 1);
+    pact.upload(pact_h.data(), B_, s_);
     remaining.upload(&B_, 1, s_);
-    const auto As  = bview<TX>(L_.A, As_.data());
-    const auto ATs = bview<TX>(L_.AT, ATs_.data());
     const inst_ctx rctx{rinst_.data(), pact.data(), nullptr};
     const inst_ctx cctx{cinst_.data(), pact.data(), nullptr};
-    double* sumsq = segout_.data();
-    double* s2    = segout_.data() + B_;
-    double* rsq   = segout_.data() + 2 * (size_t)B_;
     auto one_iteration = [&]() {
-      sq_diff_kernel<double><<<vgrid_, kBlock, 0, s_>>>(dz.data(), nullptr, m, rowbuf_.data());
-      seg_reduce_kernel<1><<<B_, kBlock, 0, s_>>>(rowbuf_.data(), stride_, rr_d_.data(),
-                                                 pact.data(), sumsq);
-      b_power_normalize_kernel<<<vgrid_, kBlock, 0, s_>>>(dz.data(), dq.data(), m, rinst_.data(),
-                                                          pact.data(), sumsq);
+      const auto As  = wview<TX>(true, As_.data());
+      const auto ATs = wview<TX>(false, ATs_.data());
+      b_power_normalize_kernel<<<B_, kBlock, 0, s_>>>(dz.data(), dq.data(), rr_d_.data(),
+                                                      pact.data());
       sell_map_kernel<TX, double, b_store_epi<double>><<<sell_grid(ATs), kBlock, 0, s_>>>(
         ATs, dq.data(), b_store_epi<double>{datq.data(), cctx}, partials_.data());
       sell_map_kernel<TX, double, b_power_z_epi><<<sell_grid(As), kBlock, 0, s_>>>(
         As, datq.data(), b_power_z_epi{dz.data(), dq.data(), rowbuf_.data(), rctx},
         partials_.data());
-      seg_reduce_kernel<1><<<B_, kBlock, 0, s_>>>(rowbuf_.data(), stride_, rr_d_.data(),
-                                                 pact.data(), s2);
-      b_power_residual_kernel<<<vgrid_, kBlock, 0, s_>>>(dq.data(), dz.data(), m, rinst_.data(),
-                                                         pact.data(), s2, rowbuf_.data());
-      seg_reduce_kernel<1><<<B_, kBlock, 0, s_>>>(rowbuf_.data(), stride_, rr_d_.data(),
-                                                 pact.data(), rsq);
-      b_power_check_kernel<<<ceil_div(B_, kBlock), kBlock, 0, s_>>>(
-        ps.data(), pact.data(), s2, rsq, B_, kPowerTol, remaining.data());
+      b_power_update_kernel<<<B_, kBlock, 0, s_>>>(dq.data(), dz.data(), rowbuf_.data(),
+                                                   rr_d_.data(), pact.data(), ps.data(),
+                                                   kPowerTol, remaining.data());
     };
-    cudaGraph_t graph;
-    cudaGraphExec_t exec;
-    B200_CUDA_CHECK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < 32; ++i) one_iteration();
-    B200_CUDA_CHECK(cudaStreamEndCapture(s_, &graph));
-    B200_CUDA_CHECK(cudaGraphInstantiate(&exec, graph, 0));
-    cudaGraphDestroy(graph);
-    int left = B_;
+    // Chunks of 32 iterations are captured into a graph.  When the instances still iterating are
+    // at most half of those the sweeps were last restricted to, the work lists shrink to them and
+    // the chunk is captured again.
+    cudaGraphExec_t exec = nullptr;
+    auto capture = [&]() {
+      if (exec) cudaGraphExecDestroy(exec);
+      cudaGraph_t graph;
+      B200_CUDA_CHECK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+      for (int i = 0; i < 32; ++i) one_iteration();
+      B200_CUDA_CHECK(cudaStreamEndCapture(s_, &graph));
+      B200_CUDA_CHECK(cudaGraphInstantiate(&exec, graph, 0));
+      cudaGraphDestroy(graph);
+    };
+    capture();
+    int left = B_, listed = B_;
     for (int done_iters = 0; done_iters < kPowerMaxIters; done_iters += 32) {
       if (kPowerMaxIters - done_iters < 32) {
         for (int i = 0; i < kPowerMaxIters - done_iters; ++i) one_iteration();
       } else {
         B200_CUDA_CHECK(cudaGraphLaunch(exec, s_));
       }
-      launches_ += 9.0 * std::min(32, kPowerMaxIters - done_iters);
+      launches_ += 4.0 * std::min(32, kPowerMaxIters - done_iters);
       remaining.download(&left, 1, s_);
       B200_CUDA_CHECK(cudaStreamSynchronize(s_));
       if (left == 0) break;
+      if (2 * left <= listed) {
+        pact.download(pact_h.data(), B_, s_);
+        B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+        rebuild_work(pact_h);
+        listed = left;
+        capture();
+        char what[96];
+        std::snprintf(what, sizeof what, "batch: power to %d its, %d instances left",
+                      done_iters + 32, left);
+        trace(what);
+      }
     }
     cudaGraphExecDestroy(exec);
+    clear_work();
     std::vector<b_power_state> h(B_);
     ps.download(h.data(), B_, s_);
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
@@ -785,6 +827,71 @@ class batch_engine {
     }
   }
 
+  // ---------------------------------------------------------------- work lists
+  // Sweeps over A (rows = constraints) and A^T (rows = variables), restricted to the listed long
+  // rows and slices once some instances have finished.
+  template <typename T>
+  dev_sell<T> wview(bool of_A, const T* vals) const
+  {
+    dev_sell<T> v = bview<T>(of_A ? L_.A : L_.AT, vals);
+    if (lists_on_) {
+      const work_list& w = of_A ? wa_ : wt_;
+      v.long_list        = w.longs.data();
+      v.slice_list       = w.slices.data();
+      v.work_long        = w.n_long;
+      v.work_slices      = w.n_slices;
+    }
+    return v;
+  }
+
+  struct work_list {
+    dbuf<int> longs, slices;
+    int n_long = 0, n_slices = 0;
+  };
+
+  void build_list(const std::vector<int4>& ranges, int n_long_rows, const std::vector<int>& act,
+                  work_list& w)
+  {
+    std::vector<int> longs, slices;
+    for (int b = 0; b < B_; ++b) {
+      if (!act[b]) continue;
+      const int4 r = ranges[b];
+      for (int i = r.x; i < r.y; ++i) longs.push_back(i);
+      if (r.z < r.w) {
+        const int first = (r.z - n_long_rows) / kWarp, last = (r.w - 1 - n_long_rows) / kWarp;
+        for (int q = first; q <= last; ++q)
+          if (slices.empty() || slices.back() < q) slices.push_back(q);
+      }
+    }
+    w.n_long   = (int)longs.size();
+    w.n_slices = (int)slices.size();
+    w.longs.resize(std::max<size_t>(longs.size(), 1));
+    w.slices.resize(std::max<size_t>(slices.size(), 1));
+    if (!longs.empty()) w.longs.upload(longs.data(), longs.size(), s_);
+    if (!slices.empty()) w.slices.upload(slices.data(), slices.size(), s_);
+  }
+
+  // Restricts the sweeps to the instances flagged in `act`; cached graphs are dropped because
+  // they hold the previous lists.
+  void rebuild_work(const std::vector<int>& act)
+  {
+    build_list(rranges_, L_.A.n_long, act, wa_);
+    build_list(cranges_, L_.AT.n_long, act, wt_);
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    lists_on_ = true;
+    drop_graphs();
+  }
+  void clear_work()
+  {
+    lists_on_ = false;
+    drop_graphs();
+  }
+  void drop_graphs()
+  {
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+  }
+
   // ---------------------------------------------------------------- iterations
   inst_ctx ctx_rows() const { return inst_ctx{rinst_.data(), active_d_.data(), sc_d_.data()}; }
   inst_ctx ctx_cols() const { return inst_ctx{cinst_.data(), active_d_.data(), sc_d_.data()}; }
@@ -792,7 +899,7 @@ class batch_engine {
   template <bool MAJOR, bool HALPERN, bool SAVE_ATY>
   void launch_primal(int it_off)
   {
-    const auto A = bview<TX>(L_.AT, ATs_.data());
+    const auto A = wview<TX>(false, ATs_.data());
     b_primal_epi<TX, MAJOR, HALPERN, SAVE_ATY> e{x_.data(),    cs_.data(),   ls_.data(),
                                                  us_.data(),   xa_.data(),   xbar_.data(),
                                                  x_.data(),    xhat_.data(), slack_.data(),
@@ -804,7 +911,7 @@ class batch_engine {
   template <bool MAJOR, bool HALPERN, bool FPE>
   void launch_dual(int it_off)
   {
-    const auto A = bview<TX>(L_.A, As_.data());
+    const auto A = wview<TX>(true, As_.data());
     b_dual_epi<TX, MAJOR, HALPERN, FPE> e{y_.data(),     lcs_.data(),  ucs_.data(),
                                           ya_.data(),    ybar_.data(), y_.data(),
                                           yhat_.data(),  rowbuf_.data(), ctx_rows(), it_off};
@@ -869,7 +976,7 @@ class batch_engine {
       xhat_.data(), yhat_.data(), slack_.data(), dc_.data(), dr_.data(), beta_d_.data(),
       gamma_d_.data(), cinst_.data(), rinst_.data(), active_d_.data(), n, m, xu_.data(), yu_.data(),
       su_.data());
-    const auto A = bview(L_.A, L_.A.val.data()), AT = bview(L_.AT, L_.AT.val.data());
+    const auto A = wview<double>(true, L_.A.val.data()), AT = wview<double>(false, L_.AT.val.data());
     sell_map_kernel<double, double, b_term_primal_epi><<<sell_grid(A), kBlock, 0, s_>>>(
       A, xu_.data(),
       b_term_primal_epi{lc64_.data(), uc64_.data(), yu_.data(), rowbuf_.data(), stride_,
@@ -934,7 +1041,7 @@ class batch_engine {
     std::vector<double> pid_sum(B_, 0.0), pid_last(B_, 0.0), best_gap(B_, inf);
     std::vector<long> since(B_, 0);
     std::vector<int> restarted(B_, 0);
-    int n_active = B_;
+    int n_active = B_, listed = B_;
     upload_scalars(since);
 
     for (long k = 0;;) {
@@ -962,6 +1069,14 @@ class batch_engine {
         }
         n_active = (int)std::count(active_h_.begin(), active_h_.end(), 1);
         if (n_active == 0) break;
+        if (2 * n_active <= listed) {
+          rebuild_work(active_h_);
+          listed = n_active;
+          char what[96];
+          std::snprintf(what, sizeof what, "batch: loop to %ld its, %d instances left", k,
+                        n_active);
+          trace(what);
+        }
 
         if (major) {
           // Restart distances of every active instance.
@@ -1059,7 +1174,7 @@ class batch_engine {
           launch_dual<false, false, true>(0);
         }
         seg_reduce<1>(true, 0, true);
-        const auto AT = bview<TX>(L_.AT, ATs_.data());
+        const auto AT = wview<TX>(false, ATs_.data());
         sell_map_kernel<TX, TX, b_fpe_epi<TX>><<<sell_grid(AT), kBlock, 0, s_>>>(
           AT, ybar_.data(),
           b_fpe_epi<TX>{aty_.data(), xbar_.data(), x_.data(), rowbuf_.data(), stride_, ctx_cols()},
@@ -1135,6 +1250,8 @@ class batch_engine {
   std::vector<int> restarts_, power_iters_, active_h_;
   std::vector<pdlp_result> results_;
   std::map<int, cudaGraphExec_t> graphs_;
+  work_list wa_, wt_;
+  bool lists_on_ = false;
 };
 
 

@@ -68,8 +68,8 @@ inline double* pinned_scratch()
   return p;
 }
 
-// The engines capture CUDA graphs, which the legacy default stream does not allow, so they
-// always work on its own non-blocking stream ordered after / before the caller's stream with events.
+// The engines capture CUDA graphs, which the legacy default stream does not allow, so they always
+// work on a non-blocking stream of their own, ordered after / before the caller's stream by events.
 struct joined_stream {
   cudaStream_t caller, own = nullptr;
   cudaEvent_t ev = nullptr;

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "host_io.hpp"
 #include "lp_model.hpp"
 
 using cuopt_b200::lp_problem;
@@ -27,25 +28,6 @@ using cuopt_b200::lp_solution;
 namespace {
 
 constexpr int kVersionMajor = 26, kVersionMinor = 4, kVersionPatch = 0;
-
-// Parallel host copy for large arrays (problem creation copies the user's arrays).
-void parallel_memcpy(void* dst, const void* src, size_t bytes)
-{
-  constexpr size_t kChunk = size_t(16) << 20;
-  const unsigned hw       = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
-  if (bytes < 2 * kChunk || hw == 1) {
-    std::memcpy(dst, src, bytes);
-    return;
-  }
-  std::vector<std::thread> pool;
-  for (unsigned t = 0; t < hw; ++t) {
-    const size_t lo = bytes * t / hw, hi = bytes * (t + 1) / hw;
-    pool.emplace_back([=] {
-      std::memcpy(static_cast<char*>(dst) + lo, static_cast<const char*>(src) + lo, hi - lo);
-    });
-  }
-  for (auto& th : pool) th.join();
-}
 
 // Copies n elements from a host or device pointer (the reference accepts both).
 template <typename T>
@@ -65,7 +47,7 @@ void copy_in(std::vector<T>& dst, const T* src, size_t n)
   }
   cudaGetLastError();  // clear a "no device" / "invalid value" answer for plain host memory
   dst.resize(n);
-  parallel_memcpy(dst.data(), src, n * sizeof(T));
+  cuopt_b200::parallel_memcpy(dst.data(), src, n * sizeof(T));
 }
 
 template <typename T>

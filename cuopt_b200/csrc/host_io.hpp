@@ -1,0 +1,135 @@
+// Host <-> device transfer helpers for host-resident problem data.
+//
+// Pageable cudaMemcpy runs through the driver's own small staging buffer and reaches only a few
+// GB/s.  staged_upload copies through two pinned buffers of its own instead: host threads fill one
+// buffer while the DMA engine drains the other, so large uploads run at host-memcpy speed.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "common.cuh"
+
+namespace cuopt_b200 {
+
+// memcpy split over up to 8 host threads for large copies.
+inline void parallel_memcpy(void* dst, const void* src, size_t bytes)
+{
+  constexpr size_t kChunk = size_t(8) << 20;
+  const unsigned hw       = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  const unsigned parts    = (unsigned)std::min<size_t>(hw, bytes / kChunk);
+  if (parts <= 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < parts; ++t) {
+    const size_t lo = bytes * t / parts, hi = bytes * (t + 1) / parts;
+    pool.emplace_back([=] {
+      std::memcpy(static_cast<char*>(dst) + lo, static_cast<const char*>(src) + lo, hi - lo);
+    });
+  }
+  for (auto& th : pool) th.join();
+}
+
+// Uploads host arrays to device memory through two pinned staging buffers (per host thread,
+// allocated once).  put() may return before the copy has reached the device; finish() (or the
+// destructor) waits for every copy issued.
+class staged_upload {
+ public:
+  explicit staged_upload(cudaStream_t s) : s_(s)
+  {
+    auto& st = state();
+    for (int i = 0; i < 2; ++i) {
+      if (!st.buf[i]) B200_CUDA_CHECK(cudaMallocHost(&st.buf[i], kStage));
+      if (!st.done[i]) B200_CUDA_CHECK(cudaEventCreateWithFlags(&st.done[i], cudaEventDisableTiming));
+    }
+  }
+  ~staged_upload()
+  {
+    try {
+      finish();
+    } catch (...) {
+    }
+  }
+  staged_upload(const staged_upload&)            = delete;
+  staged_upload& operator=(const staged_upload&) = delete;
+
+  template <typename T>
+  void put(T* dst, const T* src, size_t count)
+  {
+    put_bytes(dst, src, count * sizeof(T));
+  }
+
+  void put_bytes(void* dst, const void* src, size_t bytes)
+  {
+    auto* d       = static_cast<char*>(dst);
+    const auto* h = static_cast<const char*>(src);
+    while (bytes > 0) {
+      if (used_ == kStage) flush();
+      const size_t n = std::min(bytes, kStage - used_);
+      parallel_memcpy(state().buf[cur_] + used_, h, n);
+      pending_.push_back({d, used_, n});
+      used_ += n;
+      d += n;
+      h += n;
+      bytes -= n;
+    }
+  }
+
+  void finish()
+  {
+    flush();
+    auto& st = state();
+    for (int i = 0; i < 2; ++i)
+      if (armed_[i]) B200_CUDA_CHECK(cudaEventSynchronize(st.done[i]));
+    armed_[0] = armed_[1] = false;
+  }
+
+ private:
+  static constexpr size_t kStage = size_t(32) << 20;
+  struct piece {
+    char* dst;
+    size_t off, bytes;
+  };
+  struct buffers {
+    char* buf[2]        = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+  };
+  static buffers& state()
+  {
+    static thread_local buffers b;
+    return b;
+  }
+  // Issues the copies of the current buffer and switches to the other one (waiting until the
+  // DMA engine has drained it).
+  void flush()
+  {
+    if (pending_.empty()) return;
+    auto& st = state();
+    for (const piece& p : pending_)
+      B200_CUDA_CHECK(cudaMemcpyAsync(p.dst, st.buf[cur_] + p.off, p.bytes,
+                                      cudaMemcpyHostToDevice, s_));
+    B200_CUDA_CHECK(cudaEventRecord(st.done[cur_], s_));
+    armed_[cur_] = true;
+    pending_.clear();
+    cur_  = 1 - cur_;
+    used_ = 0;
+    if (armed_[cur_]) {
+      B200_CUDA_CHECK(cudaEventSynchronize(st.done[cur_]));
+      armed_[cur_] = false;
+    }
+  }
+
+  cudaStream_t s_;
+  int cur_         = 0;
+  size_t used_     = 0;
+  bool armed_[2]   = {false, false};
+  std::vector<piece> pending_;
+};
+
+}  // namespace cuopt_b200

@@ -27,13 +27,23 @@ struct dev_sell {
   const int64_t* slice_off;
   const int* idx;
   const T* val;
+  // Optional work lists (block-diagonal batches with finished instances): when set, a sweep visits
+  // only the listed long rows / slices, work_long / work_slices of them.
+  const int* long_list  = nullptr;
+  const int* slice_list = nullptr;
+  int work_long         = 0;
+  int work_slices       = 0;
+  B200_HD int long_count() const { return long_list ? work_long : n_long; }
+  B200_HD int slice_count() const { return slice_list ? work_slices : n_slices; }
 };
 
 B200_HD inline int long_blocks(int n_long) { return ceil_div(n_long, kWarpsPerBlock); }
+// Grid of sell_map_kernel (and of the setup kernels, which always see full views).
 template <typename T>
 inline int sell_grid(const dev_sell<T>& a)
 {
-  return long_blocks(a.n_long) + ceil_div(a.n_slices, kWarpsPerBlock);
+  const int g = long_blocks(a.long_count()) + ceil_div(a.slice_count(), kWarpsPerBlock);
+  return g > 0 ? g : 1;  // an empty work list still launches one (idle) block
 }
 
 // Scalars that change between iterations live on the device so captured graphs stay valid.
@@ -155,10 +165,11 @@ __global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
     return;
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int lb   = long_blocks(A.n_long);
+  const int lb   = long_blocks(A.long_count());
   if ((int)blockIdx.x < lb) {
-    const int row = blockIdx.x * kWarpsPerBlock + warp;
-    if (row < A.n_long && !skip_rows(epi, row, row)) {
+    const int q   = blockIdx.x * kWarpsPerBlock + warp;
+    const int row = q < A.long_count() ? (A.long_list ? A.long_list[q] : q) : 0;
+    if (q < A.long_count() && !skip_rows(epi, row, row)) {
       const auto pre  = epi.load(row);
       const int64_t b = A.long_off[row], e = A.long_off[row + 1];
       double acc      = 0.0;
@@ -168,8 +179,9 @@ __global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
       if (lane == 0) epi(row, acc, pre, red);
     }
   } else {
-    const int s = (blockIdx.x - lb) * kWarpsPerBlock + warp;
-    if (s < A.n_slices &&
+    const int q = (blockIdx.x - lb) * kWarpsPerBlock + warp;
+    const int s = q < A.slice_count() ? (A.slice_list ? A.slice_list[q] : q) : 0;
+    if (q < A.slice_count() &&
         !skip_rows(epi, A.n_long + s * kWarp, min(A.n_long + s * kWarp + kWarp, A.rows) - 1)) {
       const int row      = A.n_long + s * kWarp + lane;
       const bool valid   = row < A.rows;

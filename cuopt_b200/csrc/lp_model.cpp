@@ -9,10 +9,13 @@
 #include <cmath>
 #include <cstdio>
 #include <limits>
+#include <memory>
 #include <new>
 #include <stdexcept>
+#include <thread>
 
 #include "common.cuh"
+#include "host_io.hpp"
 
 namespace cuopt_b200 {
 
@@ -492,20 +495,28 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
     bi.maximize.push_back(p.maximize ? 1 : 0);
   }
   const int m = bi.row_start.back(), n = bi.col_start.back();
-  std::vector<int> off(m + 1), idx(std::max<int64_t>(nnz, 1)), rinst(m), cinst(n);
-  std::vector<double> val(std::max<int64_t>(nnz, 1)), c(n), clo(m), cup(m), vlo(n), vup(n);
-  for (int b = 0; b < bi.count; ++b) {
+  // Uninitialised host arrays (every element is written below; zero-filling 10^8 elements would
+  // cost as much as the copy itself).
+  const size_t nz = (size_t)std::max<int64_t>(nnz, 1);
+  std::unique_ptr<int[]> off(new int[m + 1]), idx(new int[nz]), rinst(new int[m]), cinst(new int[n]);
+  std::unique_ptr<double[]> val(new double[nz]), c(new double[n]), clo(new double[m]),
+    cup(new double[m]), vlo(new double[n]), vup(new double[n]);
+  off[0] = 0;
+  // Row offsets first (prefix over instances), then every instance's pieces in parallel.
+  std::vector<int> e0(bi.count + 1, 0);
+  for (int b = 0; b < bi.count; ++b) e0[b + 1] = e0[b] + ps[ids[b]]->row_off[ps[ids[b]]->m];
+  auto fill_instance = [&](int b) {
     const lp_problem& p = *ps[ids[b]];
-    const int r0 = bi.row_start[b], c0 = bi.col_start[b], e0 = off[r0];
+    const int r0 = bi.row_start[b], c0 = bi.col_start[b], base = e0[b];
     for (int i = 0; i < p.m; ++i) {
-      off[r0 + i + 1] = e0 + p.row_off[i + 1];
+      off[r0 + i + 1] = base + p.row_off[i + 1];
       clo[r0 + i]     = lo[ids[b]][i];
       cup[r0 + i]     = up[ids[b]][i];
       rinst[r0 + i]   = b;
     }
     for (int k = 0; k < p.row_off[p.m]; ++k) {
-      idx[e0 + k] = p.col_idx[k] + c0;
-      val[e0 + k] = p.val[k];
+      idx[base + k] = p.col_idx[k] + c0;
+      val[base + k] = p.val[k];
     }
     for (int j = 0; j < p.n; ++j) {
       c[c0 + j]     = p.c[j];
@@ -513,6 +524,15 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
       vup[c0 + j]   = p.var_up[j];
       cinst[c0 + j] = b;
     }
+  };
+  {
+    const int nt = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t)
+      pool.emplace_back([&, t] {
+        for (int b = t; b < bi.count; b += nt) fill_instance(b);
+      });
+    for (auto& th : pool) th.join();
   }
   trace("batch: concatenate");
   cudaStream_t s;
@@ -523,18 +543,24 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
   } guard{s};
   alloc_scope scope(s);
   configure_pool_once();
-  dbuf<int> doff(m + 1), didx(idx.size()), dri(m), dci(n);
-  dbuf<double> dval(val.size()), dc(n), dlo(m), dup(m), dvl(n), dvu(n), x(n), y(m), rc(n);
-  doff.upload(off.data(), m + 1, s);
-  didx.upload(idx.data(), idx.size(), s);
-  dval.upload(val.data(), val.size(), s);
-  dri.upload(rinst.data(), m, s);
-  dci.upload(cinst.data(), n, s);
-  dc.upload(c.data(), n, s);
-  dlo.upload(clo.data(), m, s);
-  dup.upload(cup.data(), m, s);
-  dvl.upload(vlo.data(), n, s);
-  dvu.upload(vup.data(), n, s);
+  dbuf<int> doff(m + 1), didx(nz), dri(m), dci(n);
+  dbuf<double> dval(nz), dc(n), dlo(m), dup(m), dvl(n), dvu(n), x(n), y(m), rc(n);
+  B200_CUDA_CHECK(cudaStreamSynchronize(s));
+  trace("batch: device allocation");
+  {
+    staged_upload h2d(s);
+    h2d.put(doff.data(), off.get(), m + 1);
+    h2d.put(didx.data(), idx.get(), nz);
+    h2d.put(dval.data(), val.get(), nz);
+    h2d.put(dri.data(), rinst.get(), m);
+    h2d.put(dci.data(), cinst.get(), n);
+    h2d.put(dc.data(), c.get(), n);
+    h2d.put(dlo.data(), clo.get(), m);
+    h2d.put(dup.data(), cup.get(), m);
+    h2d.put(dvl.data(), vlo.get(), n);
+    h2d.put(dvu.data(), vup.get(), n);
+    h2d.finish();
+  }
   bi.m        = m;
   bi.n        = n;
   bi.row_off  = doff.data();

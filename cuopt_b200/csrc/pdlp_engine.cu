@@ -6,6 +6,7 @@
 // is in the kernels of kernels.cuh.  Iterations that need neither a termination test, a "major"
 // step nor a fixed-point error are replayed from cached CUDA graphs of 2^k iterations.
 #include "device_layout.cuh"
+#include "host_io.hpp"
 #include "kernels.cuh"
 #include "pdlp_engine.hpp"
 #include "pdlp_schedule.hpp"
@@ -834,14 +835,18 @@ pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p)
   dbuf<int> off(m + 1), idx(std::max<int64_t>(nnz, 1));
   dbuf<double> val(std::max<int64_t>(nnz, 1)), c(n), lo(m), up(m), vl(n), vu(n), x(n), y(m), rc(n),
     ip, id;
-  off.upload(in.row_off, m + 1, s);
-  idx.upload(in.col_idx, nnz, s);
-  val.upload(in.val, nnz, s);
-  c.upload(in.c, n, s);
-  lo.upload(in.con_lo, m, s);
-  up.upload(in.con_up, m, s);
-  vl.upload(in.var_lo, n, s);
-  vu.upload(in.var_up, n, s);
+  {
+    staged_upload h2d(s);
+    h2d.put(off.data(), in.row_off, m + 1);
+    h2d.put(idx.data(), in.col_idx, nnz);
+    h2d.put(val.data(), in.val, nnz);
+    h2d.put(c.data(), in.c, n);
+    h2d.put(lo.data(), in.con_lo, m);
+    h2d.put(up.data(), in.con_up, m);
+    h2d.put(vl.data(), in.var_lo, n);
+    h2d.put(vu.data(), in.var_up, n);
+    h2d.finish();
+  }
   lp_device_input d;
   d.m = m;
   d.n = n;
