@@ -14,6 +14,9 @@ iterates, FP64 termination / restart / step ratio).  The same solve in plain FP6
             against the measured HBM copy bandwidth.
   cpu_baseline  the oracle (FP64 restatement of the same algorithm) on the host cores: a bounded
             number of PDHG iterations, scaled by the iterations the solve needs.
+  batch_c3  config 3: 512 seeded LPs of uneven sizes (m log-uniform in [200, 20000], n = 2.5 m,
+            6-12 non-zeros per column) solved in FP64 to 1e-6 by one cuOptBatchSolve call, against
+            a sample of the same LPs solved one by one with cuOptSolve.
 
 `--impl reference` times that CPU implementation alone (rank 0) on the same workload and metric.
 """
@@ -316,7 +319,7 @@ def run_b200(args):
             "speedup_mixed_vs_fp64": ms_fp64 / ms_mixed,
         }
 
-    # Mixed precision followed by FP64 iterative refinement to 1e-8 relative KKT
+    # Mixed precision to 1e-6, then FP64 continuation from that solution to 1e-8 relative KKT
     refine = None
     if not args.no_refine:
         s_ref = settings_handle(L, tol, 1, refine_passes=8, refine_tol=1e-8, time_limit=20.0)
@@ -390,6 +393,13 @@ def run_b200(args):
                          f"({s_iter * 1e3:.1f} ms each), scaled by the {iters} iterations of the FP64 solve",
                "pdhg_iter_per_s": 1.0 / s_iter}
 
+    # Config 3: 512 uneven FP64 LPs in one batched call vs the same LPs one by one (rank 0, N = 1).
+    batch = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        from cuopt_b200.profile import run_batch
+        batch = run_batch(argparse.Namespace(count=512, sequential=args.batch_sequential,
+                                             repeats=2, tol=1e-6, time_limit=120.0))
+
     value = world * 1000.0 / ms_mixed
     line = {
         "metric": METRIC, "value": value, "unit": "LPs/s to 1e-6 rel. KKT", "n_gpus": world,
@@ -404,7 +414,7 @@ def run_b200(args):
         "pdhg_iter_per_s": last_mixed["number_of_steps_taken"] / (last_mixed["loop_time"] or 1e-9),
         "setup_s": last_mixed["setup_time"], "loop_s": last_mixed["loop_time"],
         "objective_rel_error": obj_err_mixed, "kkt": kkt_mixed, "fp64": fp64,
-        "mixed_refined_to_1e-8": refine,
+        "mixed_refined_to_1e-8": refine, "batch_c3": batch,
         "roofline": roofline, "cpu_baseline": cpu,
         "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "LPs/s to 1e-6 rel. KKT",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
@@ -435,6 +445,9 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-refine", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-sequential", type=int, default=32,
+                    help="config-3 instances also solved one by one (timing sample)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

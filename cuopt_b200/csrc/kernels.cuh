@@ -720,43 +720,6 @@ __global__ void scale_initial_kernel(const double* v, const double* d, double fa
   }
 }
 
-// Correction LP of an iterative-refinement pass (FP64, unscaled, internal order):
-//   c' = dd (c - A^T y),  [l', u'] = dp ([l, u] - x),  [lc', uc'] = dp ([lc, uc] - A x).
-static __global__ void refine_vectors_kernel(const double* c0, const double* l0, const double* u0,
-                                      const double* lc0, const double* uc0, const double* x,
-                                      const double* ax, const double* aty, double dp, double dd,
-                                      int n, int m, double* c, double* l, double* u, double* lc,
-                                      double* uc)
-{
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x) {
-    if (i < n) {
-      c[i] = dd * (c0[i] - aty[i]);
-      l[i] = dp * (l0[i] - x[i]);
-      u[i] = dp * (u0[i] - x[i]);
-    } else {
-      const int r = i - n;
-      lc[r]       = dp * (lc0[r] - ax[r]);
-      uc[r]       = dp * (uc0[r] - ax[r]);
-    }
-  }
-}
-
-// x += z / dp, y += w / dd, s = s_w / dd (refinement update).
-static __global__ void refine_update_kernel(double* x, double* y, double* s, const double* z,
-                                     const double* w, const double* sw, double dp, double dd,
-                                     int n, int m)
-{
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x) {
-    if (i < n) {
-      x[i] += z[i] / dp;
-      s[i] = sw[i] / dd;
-    } else {
-      const int r = i - n;
-      y[r] += w[r] / dd;
-    }
-  }
-}
-
 // Elementwise helpers
 template <typename TX>
 __global__ void clamp_kernel(TX* x, const TX* l, const TX* u, int n)

@@ -41,11 +41,25 @@ struct conv_info {
   double l2_primal, l2_dual, primal_obj, dual_obj, gap, abs_obj;
 };
 
+// Iteration count and restart / PID state of the main loop (host side).
+struct loop_state {
+  long k = 0, since = 0;
+  double fpe        = std::numeric_limits<double>::quiet_NaN();
+  double fpe0       = std::numeric_limits<double>::quiet_NaN();
+  double last_trial = std::numeric_limits<double>::infinity();
+  double pid_sum = 0.0, pid_last = 0.0;
+  double best_gap = std::numeric_limits<double>::infinity();
+  bool fresh      = true;  // no iteration run yet: the loop starts by zeroing the step counter
+};
+
 template <typename TX>
 class engine {
+  template <typename>
+  friend class engine;
+
  public:
   engine(const lp_device_input& in, const pdlp_params& p, cudaStream_t s)
-    : in_(in), p_(p), s_(s), iteration_limit_(p.iteration_limit)
+    : in_(in), p_(p), s_(s)
   {
     int dev = 0;
     B200_CUDA_CHECK(cudaGetDevice(&dev));
@@ -76,7 +90,29 @@ class engine {
     }
     t_loop_ = now_s();
     loop(r);
-    if (p_.precision == 1 && p_.refinement_passes > 0 && r.status == kOptimal) refine(r);
+    write_outputs();
+    finish_times(r);
+    return r;
+  }
+
+  // FP64 continuation of a mixed-precision solve (used on engine<double>): takes over the layout,
+  // the scaling, the step size, the primal weight, the iterates, the Halpern anchor and the
+  // schedule / restart state of `mixed`, and resumes its iteration in FP64 at the check where it
+  // stopped, until the tolerances of this engine's parameters hold on the original LP.  Iteration
+  // counts, restarts and times continue those of the first solve.
+  template <typename TM>
+  pdlp_result continue_from(engine<TM>& mixed, const pdlp_result& first, double* x_out,
+                            double* y_out, double* rc_out)
+  {
+    alloc_scope scope(s_);
+    x_out_  = x_out;
+    y_out_  = y_out;
+    rc_out_ = rc_out;
+    adopt(mixed);
+    pdlp_result r;
+    loop(r);
+    r.power_iterations  = power_iters_;
+    r.refinement_passes = 1;
     write_outputs();
     finish_times(r);
     return r;
@@ -156,9 +192,71 @@ class engine {
     reset_iterates(true);
   }
 
+  // Takes the precision-independent state of another engine over (see continue_from).
+  template <typename TM>
+  void adopt(engine<TM>& o)
+  {
+    const int m = in_.m, n = in_.n;
+    t_start_     = o.t_start_;
+    t_loop_      = o.t_loop_;
+    sms_         = o.sms_;
+    vgrid_       = o.vgrid_;
+    L_           = std::move(o.L_);
+    c64_         = std::move(o.c64_);
+    l64_         = std::move(o.l64_);
+    u64_         = std::move(o.u64_);
+    lc64_        = std::move(o.lc64_);
+    uc64_        = std::move(o.uc64_);
+    dr_          = std::move(o.dr_);
+    dc_          = std::move(o.dc_);
+    partials_    = std::move(o.partials_);
+    dres_        = std::move(o.dres_);
+    scalars_     = std::move(o.scalars_);
+    xu_          = std::move(o.xu_);
+    yu_          = std::move(o.yu_);
+    su_          = std::move(o.su_);
+    obj_scale_   = o.obj_scale_;
+    obj_offset_  = o.obj_offset_;
+    eta_         = o.eta_;
+    omega_       = o.omega_;
+    best_omega_  = o.best_omega_;
+    power_iters_ = o.power_iters_;
+    restarts_    = o.restarts_;
+    launches_    = o.launches_;
+    sched_       = o.sched_;
+    // Scaled matrices and vectors in FP64, from the unscaled data and the shared scaling.
+    As_.resize(L_.A.stored());
+    ATs_.resize(L_.AT.stored());
+    scale_values_kernel<TX, false><<<sell_grid(view64(L_.A)), kBlock, 0, s_>>>(
+      view64(L_.A), dr_.data(), dc_.data(), As_.data());
+    scale_values_kernel<TX, true><<<sell_grid(view64(L_.AT)), kBlock, 0, s_>>>(
+      view64(L_.AT), dr_.data(), dc_.data(), ATs_.data());
+    launches_ += 2;
+    prepare_vectors();
+    // Iterates, anchors and the last averaged iterate, converted to FP64.
+    for (auto* b : {&x_, &xhat_, &slack_, &xbar_, &xa_, &aty_}) {
+      b->resize(n);
+      b->zero(s_);
+    }
+    for (auto* b : {&y_, &yhat_, &ybar_, &ya_}) {
+      b->resize(m);
+      b->zero(s_);
+    }
+    copy_convert_kernel<TM, TX><<<vgrid_, kBlock, 0, s_>>>(x_.data(), o.x_.data(), n);
+    copy_convert_kernel<TM, TX><<<vgrid_, kBlock, 0, s_>>>(xa_.data(), o.xa_.data(), n);
+    copy_convert_kernel<TM, TX><<<vgrid_, kBlock, 0, s_>>>(xhat_.data(), o.xhat_.data(), n);
+    copy_convert_kernel<TM, TX><<<vgrid_, kBlock, 0, s_>>>(slack_.data(), o.slack_.data(), n);
+    copy_convert_kernel<TM, TX><<<vgrid_, kBlock, 0, s_>>>(y_.data(), o.y_.data(), m);
+    copy_convert_kernel<TM, TX><<<vgrid_, kBlock, 0, s_>>>(ya_.data(), o.ya_.data(), m);
+    copy_convert_kernel<TM, TX><<<vgrid_, kBlock, 0, s_>>>(yhat_.data(), o.yhat_.data(), m);
+    launches_ += 7;
+    B200_LAUNCH_CHECK();
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+  }
+
   // Norms of the unscaled vectors and their scaled copies in the iterate precision (bound /
-  // objective rescaling recomputed, reference initial_scaling.cu:95-149, 417-569).  Called once
-  // for the LP and once per refinement pass for the correction LP; the matrix scaling is shared.
+  // objective rescaling recomputed, reference initial_scaling.cu:95-149, 417-569).  Called at setup
+  // and by an FP64 continuation that takes the scaling of a mixed-precision solve over.
   void prepare_vectors()
   {
     const int m = in_.m, n = in_.n;
@@ -454,104 +552,6 @@ class engine {
     B200_CUDA_CHECK(cudaMemcpyAsync(dst, src, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s_));
   }
 
-  // FP64 iterative refinement of a mixed-precision solution (x, y, s).  The correction LP
-  //   min (dd (c - A^T y))^T z   s.t.  dp (lc - A x) <= A z <= dp (uc - A x),  dp (l - x) <= z <= dp (u - x)
-  // has the same matrix, so the layout, the Ruiz / Pock-Chambolle scaling and the step size are
-  // reused; only the vectors are rebuilt.  Its solution (z, w, s_w) gives x += z / dp,
-  // y += w / dd, s = s_w / dd, with dp, dd the inverse primal / dual residual norms of the current
-  // point.  Passes stop once the original LP meets `refinement_tol`; a pass that does not improve
-  // the relative KKT error is discarded.
-  void refine(pdlp_result& r)
-  {
-    const int m = in_.m, n = in_.n;
-    dbuf<double> c0(n), l0(n), u0(n), lc0(m), uc0(m), X(n), Y(m), S(n), AX(m), ATY(n);
-    dbuf<double> Xb(n), Yb(m), Sb(n);
-    copy_d(c0.data(), c64_.data(), n);
-    copy_d(l0.data(), l64_.data(), n);
-    copy_d(u0.data(), u64_.data(), n);
-    copy_d(lc0.data(), lc64_.data(), m);
-    copy_d(uc0.data(), uc64_.data(), m);
-    copy_d(X.data(), xu_.data(), n);
-    copy_d(Y.data(), yu_.data(), m);
-    copy_d(S.data(), su_.data(), n);
-    const double scale0 = obj_scale_, offset0 = obj_offset_, cn0 = c_norm_, bn0 = b_norm_;
-    const double tol = p_.refinement_tol;
-    const auto A = view64(L_.A), AT = view64(L_.AT);
-    long total = r.iterations;
-    int passes = 0;
-    conv_info cv = evaluate_unscaled();
-    double best  = rel_kkt(cv, bn0, cn0);
-    // Each correction solve gets at most 4x the first solve's iterations (plus 1000), within what
-    // is left of the caller's iteration and time limits; a correction solve that stops on that
-    // budget still yields a candidate, but ends the refinement.
-    const long user_limit = p_.iteration_limit;
-    const long pass_cap   = 4 * (long)r.iterations + 1000;
-    bool more             = true;
-    while (more && passes < p_.refinement_passes && !meets(cv, tol) &&
-           now_s() - t_start_ < p_.time_limit && total < user_limit) {
-      const double dp = std::min(std::max(1.0 / std::max(cv.l2_primal, 1e-300), 1.0), 1e12);
-      const double dd = std::min(std::max(1.0 / std::max(cv.l2_dual, 1e-300), 1.0), 1e12);
-      sell_map_kernel<double, double, store_epi<double>><<<sell_grid(A), kBlock, 0, s_>>>(
-        A, X.data(), store_epi<double>{AX.data(), nullptr}, partials_.data());
-      sell_map_kernel<double, double, store_epi<double>><<<sell_grid(AT), kBlock, 0, s_>>>(
-        AT, Y.data(), store_epi<double>{ATY.data(), nullptr}, partials_.data());
-      refine_vectors_kernel<<<vgrid_, kBlock, 0, s_>>>(
-        c0.data(), l0.data(), u0.data(), lc0.data(), uc0.data(), X.data(), AX.data(), ATY.data(),
-        dp, dd, n, m, c64_.data(), l64_.data(), u64_.data(), lc64_.data(), uc64_.data());
-      launches_ += 3;
-      B200_LAUNCH_CHECK();
-      obj_scale_  = 1.0;
-      obj_offset_ = 0.0;
-      prepare_vectors();
-      reset_iterates(false);
-      pdlp_result rr;
-      iteration_limit_ = std::min(pass_cap, user_limit - total);
-      loop(rr);
-      iteration_limit_ = user_limit;
-      more             = rr.status == kOptimal;
-      total += rr.iterations;
-      ++passes;
-      // candidate = current + correction
-      copy_d(Xb.data(), X.data(), n);
-      copy_d(Yb.data(), Y.data(), m);
-      copy_d(Sb.data(), S.data(), n);
-      refine_update_kernel<<<vgrid_, kBlock, 0, s_>>>(Xb.data(), Yb.data(), Sb.data(), xu_.data(),
-                                                      yu_.data(), su_.data(), dp, dd, n, m);
-      ++launches_;
-      // evaluate the candidate on the original LP
-      copy_d(c64_.data(), c0.data(), n);
-      copy_d(l64_.data(), l0.data(), n);
-      copy_d(u64_.data(), u0.data(), n);
-      copy_d(lc64_.data(), lc0.data(), m);
-      copy_d(uc64_.data(), uc0.data(), m);
-      obj_scale_  = scale0;
-      obj_offset_ = offset0;
-      c_norm_     = cn0;
-      b_norm_     = bn0;
-      copy_d(xu_.data(), Xb.data(), n);
-      copy_d(yu_.data(), Yb.data(), m);
-      copy_d(su_.data(), Sb.data(), n);
-      const conv_info cand = evaluate_unscaled();
-      const double err     = rel_kkt(cand, bn0, cn0);
-      if (!(err < best)) break;  // no improvement: keep the previous point
-      best = err;
-      cv   = cand;
-      copy_d(X.data(), Xb.data(), n);
-      copy_d(Y.data(), Yb.data(), m);
-      copy_d(S.data(), Sb.data(), n);
-    }
-    // final point on the original LP
-    copy_d(xu_.data(), X.data(), n);
-    copy_d(yu_.data(), Y.data(), m);
-    copy_d(su_.data(), S.data(), n);
-    c_norm_ = cn0;
-    b_norm_ = bn0;
-    const long keep_iters = total;
-    finish(r, kOptimal, cv, keep_iters);
-    r.refinement_passes = passes;
-    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
-  }
-
   // Solution in the user's order; duals and reduced costs negated for maximisation
   // (reference solve.cu:584-588).
   void write_outputs()
@@ -576,15 +576,21 @@ class engine {
   void loop(pdlp_result& r)
   {
     const int m = in_.m, n = in_.n;
-    const double qnan = std::numeric_limits<double>::quiet_NaN();
-    const double inf  = std::numeric_limits<double>::infinity();
-    double fpe = qnan, fpe0 = qnan, last_trial = inf;
-    double pid_sum = 0.0, pid_last = 0.0, best_gap = inf;
-    long since = 0;
-    set_scalars(0);
+    const double inf = std::numeric_limits<double>::infinity();
+    // The schedule / restart state lives in sched_ so that an FP64 continuation resumes it.
+    long& k            = sched_.k;
+    long& since        = sched_.since;
+    double& fpe        = sched_.fpe;
+    double& fpe0       = sched_.fpe0;
+    double& last_trial = sched_.last_trial;
+    double& pid_sum    = sched_.pid_sum;
+    double& pid_last   = sched_.pid_last;
+    double& best_gap   = sched_.best_gap;
+    if (sched_.fresh) set_scalars(0);
+    sched_.fresh = false;
     const auto A = As_view(), AT = ATs_view();
 
-    for (long k = 0;;) {
+    for (;;) {
       const bool major = (k % kMajor == 0 && k > 0) || k <= 0;
       const bool cond  = (k % conditional_major(k)) == 0;
       bool restarted   = false;
@@ -602,7 +608,7 @@ class engine {
                       cv.dual_obj, cv.gap, cv.l2_primal, cv.l2_dual, now_s() - t_start_);
         if (k > 1 && status == kOptimal) return finish(r, kOptimal, cv, k);
         if (now_s() - t_start_ >= p_.time_limit) return finish(r, kTimeLimit, cv, k);
-        if (k >= iteration_limit_) return finish(r, kIterationLimit, cv, k);
+        if (k >= p_.iteration_limit) return finish(r, kIterationLimit, cv, k);
         if (!std::isfinite(cv.l2_primal) || !std::isfinite(cv.l2_dual))
           return finish(r, kNumericalError, cv, k);
 
@@ -722,7 +728,6 @@ class engine {
   const lp_device_input& in_;
   const pdlp_params& p_;
   cudaStream_t s_ = nullptr;
-  long iteration_limit_;  // limit of the running loop (lowered for correction solves)
   double *x_out_ = nullptr, *y_out_ = nullptr, *rc_out_ = nullptr;
   int sms_ = 148, vgrid_ = 592;
   double* hres_ = nullptr;
@@ -740,6 +745,7 @@ class engine {
 
   double obj_scale_ = 1.0, obj_offset_ = 0.0;
   double c_norm_ = 0, b_norm_ = 0, beta_ = 1, gamma_ = 1;
+  loop_state sched_;
   double eta_ = 0, omega_ = 1, best_omega_ = 1;
   int power_iters_ = 0, restarts_ = 0;
   double launches_ = 0;
@@ -791,18 +797,22 @@ class engine {
 
 }  // namespace
 
-namespace {
-
-
-}  // namespace
-
 pdlp_result pdlp_solve_device(const lp_device_input& in, const pdlp_params& p, cudaStream_t stream,
                               double* x_out, double* y_out, double* rc_out)
 {
   joined_stream js(stream);
   if (p.precision == 1) {
     engine<float> e(in, p, js.own);
-    return e.run(x_out, y_out, rc_out);
+    pdlp_result r = e.run(x_out, y_out, rc_out);
+    if (p.refinement_passes <= 0 || r.status != kOptimal) return r;
+    // FP64 continuation to the refinement tolerance, within what is left of the limits.
+    pdlp_params q     = p;
+    q.abs_primal      = q.rel_primal = p.refinement_tol;
+    q.abs_dual        = q.rel_dual = p.refinement_tol;
+    q.abs_gap         = q.rel_gap = p.refinement_tol;
+    q.iteration_limit = std::max<int64_t>(p.iteration_limit - r.iterations, 0);
+    engine<double> d(in, q, js.own);
+    return d.continue_from(e, r, x_out, y_out, rc_out);
   }
   engine<double> e(in, p, js.own);
   return e.run(x_out, y_out, rc_out);

@@ -47,11 +47,13 @@ def main() -> None:
     ap.add_argument("--count", type=int, default=512, help="batch mode: instances")
     ap.add_argument("--sequential", type=int, default=64,
                     help="batch mode: instances also solved one by one (timing sample)")
+    ap.add_argument("--repeats", type=int, default=2,
+                    help="batch mode: batched solves, the first one untimed (warm-up)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--iterations", type=int, default=3)
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--time-limit", type=float, default=0.0)
-    ap.add_argument("--refine", type=int, default=0, help="FP64 refinement passes (mixed precision)")
+    ap.add_argument("--refine", type=int, default=0, help="> 0: continue a mixed-precision solve in FP64 to 1e-8")
     a = ap.parse_args()
 
     if a.mode == "batch":
@@ -135,7 +137,11 @@ def run_batch(a) -> dict:
     st.set_parameter(lpm.CUOPT_LOG_TO_CONSOLE, False)
     if a.time_limit > 0:
         st.set_parameter(lpm.CUOPT_TIME_LIMIT, a.time_limit)
-    sols, batch_s = lpm.BatchSolve(dms, st)
+    times = []
+    for _ in range(max(1, a.repeats)):
+        sols, t = lpm.BatchSolve(dms, st)
+        times.append(t)
+    batch_s = min(times[1:]) if len(times) > 1 else times[0]
     status = [int(s.get_termination_status()) for s in sols]
     iters = [s.get_lp_stats()["nb_iterations"] for s in sols]
     obj_err = [abs(s.get_primal_objective() - lp.optimal_objective) / max(1.0, abs(lp.optimal_objective))
@@ -150,6 +156,7 @@ def run_batch(a) -> dict:
            "max_power_iterations": max(s.stats.get("power_iterations", 0) for s in sols)}
     if a.sequential > 0:
         pick = np.linspace(0, a.count - 1, min(a.sequential, a.count)).astype(int)
+        lpm.Solve(dms[pick[0]], st)  # warm-up
         t0 = time.perf_counter()
         seq_iters_equal = 0
         for i in pick:

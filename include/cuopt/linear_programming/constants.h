@@ -80,10 +80,11 @@
 
 /* Parameters added by this library (no counterpart in the reference).  "pdlp_precision" picks the
  * arithmetic of the PDHG iterations: 0 = FP64 throughout (the reference's behaviour, default),
- * 1 = mixed (FP32 matrix and iterates, FP64 termination/restart/step ratio, FP64 refinement).
- * "pdlp_refinement_passes" (default 0 = off) bounds the number of FP64 iterative-refinement passes
- * applied after a mixed-precision solve reached its tolerances; "pdlp_refinement_tolerance"
- * (default 1e-8) is the tolerance the refinement passes aim for on the original LP. */
+ * 1 = mixed (FP32 matrix and iterates, FP64 termination/restart/step ratio).
+ * "pdlp_refinement_passes" (default 0 = off; any positive value = on) makes a mixed-precision solve
+ * that reached its tolerances continue in FP64 from its solution (same scaling, step size and
+ * primal weight) until "pdlp_refinement_tolerance" (default 1e-8) holds for all six relative
+ * tolerances on the original LP, within the iteration and time limits. */
 #define CUOPT_PDLP_PRECISION            "pdlp_precision"
 #define CUOPT_PDLP_REFINEMENT_PASSES    "pdlp_refinement_passes"
 #define CUOPT_PDLP_REFINEMENT_TOLERANCE "pdlp_refinement_tolerance"
