@@ -42,6 +42,7 @@ class PDLPStatistics(C.Structure):
         ("setup_time", cuopt_float_t),
         ("loop_time", cuopt_float_t),
         ("kernel_launches", cuopt_float_t),
+        ("crossover", cuopt_int_t),
     ]
 
 

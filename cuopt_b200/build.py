@@ -80,7 +80,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     newest = max(o.stat().st_mtime for o in objs)
     if force or not LIB.exists() or LIB.stat().st_mtime < newest:
         cmd = [_nvcc(), *ARCH, "-shared", "-cudart", "static", "-ccbin", _host_cxx(),
-               "-Xcompiler", "-fPIC", "-o", str(LIB), *map(str, objs), "-lpthread"]
+               "-Xcompiler", "-fPIC", "-o", str(LIB), *map(str, objs), "-lpthread", "-ldl"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")

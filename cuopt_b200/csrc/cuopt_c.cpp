@@ -555,6 +555,7 @@ cuopt_int_t cuOptGetPDLPStatistics(cuOptSolution solution, cuOptPDLPStatistics* 
   st->setup_time                      = r.setup_time;
   st->loop_time                       = r.loop_time;
   st->kernel_launches                 = r.kernel_launches;
+  st->crossover                       = r.crossover ? 1 : 0;
   return CUOPT_SUCCESS;
 }
 
@@ -675,11 +676,40 @@ cuopt_int_t cuOptBatchSolve(const cuOptOptimizationProblem* problems, cuopt_int_
 }
 
 cuopt_int_t cuOptSolutionAdjoint(cuOptOptimizationProblem problem, cuOptSolution solution,
-                                 const cuopt_float_t* dl_dx, const cuopt_float_t*,
-                                 cuopt_float_t*, cuopt_float_t*, cuopt_float_t*, cuopt_float_t*)
+                                 const cuopt_float_t* dl_dx, const cuopt_float_t* dl_dy,
+                                 cuopt_float_t* dl_dc, cuopt_float_t* dl_dlower,
+                                 cuopt_float_t* dl_dupper, cuopt_float_t* dl_dvalues)
 {
   if (!problem || !solution || !dl_dx) return CUOPT_INVALID_ARGUMENT;
-  return CUOPT_INVALID_ARGUMENT;
+  const lp_solution* sol = R(solution);
+  if (sol->error_code != CUOPT_SUCCESS || sol->r.status != CUOPT_TERIMINATION_STATUS_OPTIMAL)
+    return CUOPT_INVALID_ARGUMENT;
+  const lp_problem& p = *P(problem);
+  if ((int)sol->r.x.size() != p.n || (int)sol->r.y.size() != p.m) return CUOPT_INVALID_ARGUMENT;
+  try {
+    std::vector<double> gx, gy;
+    copy_in(gx, dl_dx, p.n);
+    if (dl_dy) copy_in(gy, dl_dy, p.m);
+    std::vector<double> dc(dl_dc ? p.n : 0), dlo(dl_dlower ? p.m : 0), dup(dl_dupper ? p.m : 0),
+      dval(dl_dvalues ? p.val.size() : 0);
+    cuopt_b200::solution_adjoint(p, sol->r, gx.data(), dl_dy ? gy.data() : nullptr,
+                                 dl_dc ? dc.data() : nullptr, dl_dlower ? dlo.data() : nullptr,
+                                 dl_dupper ? dup.data() : nullptr,
+                                 dl_dvalues ? dval.data() : nullptr);
+    if (dl_dc) copy_out(dl_dc, dc);
+    if (dl_dlower) copy_out(dl_dlower, dlo);
+    if (dl_dupper) copy_out(dl_dupper, dup);
+    if (dl_dvalues) copy_out(dl_dvalues, dval);
+  } catch (const std::bad_alloc&) {
+    return CUOPT_OUT_OF_MEMORY;
+  } catch (const std::invalid_argument& e) {
+    std::fprintf(stderr, "cuOptSolutionAdjoint: %s\n", e.what());
+    return CUOPT_INVALID_ARGUMENT;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "cuOptSolutionAdjoint: %s\n", e.what());
+    return CUOPT_RUNTIME_ERROR;
+  }
+  return CUOPT_SUCCESS;
 }
 
 }  // extern "C"

@@ -455,6 +455,8 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
     trace("constraint bounds + checks");
     out.r         = pdlp_solve(in, prm);
     trace("pdlp_solve");
+    if (st.b(CUOPT_CROSSOVER) && out.r.status == CUOPT_TERIMINATION_STATUS_OPTIMAL)
+      out.r.crossover = vertex_polish(p, out.r);
     if (prm.log_to_console)
       std::printf("PDLP status %d  objective %+.10e  iterations %lld  time %.3fs\n", out.r.status,
                   out.r.primal_obj, (long long)out.r.iterations, out.r.solve_time);
@@ -479,7 +481,7 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
                               const std::vector<size_t>& ids,
                               const std::vector<std::vector<double>>& lo,
                               const std::vector<std::vector<double>>& up, const pdlp_params& prm,
-                              std::vector<lp_solution>& out)
+                              bool crossover, std::vector<lp_solution>& out)
 {
   batch_device_input bi;
   bi.count = (int)ids.size();
@@ -586,6 +588,8 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
     o.r.x.assign(hx.begin() + bi.col_start[b], hx.begin() + bi.col_start[b + 1]);
     o.r.rc.assign(hrc.begin() + bi.col_start[b], hrc.begin() + bi.col_start[b + 1]);
     o.r.y.assign(hy.begin() + bi.row_start[b], hy.begin() + bi.row_start[b + 1]);
+    if (crossover && o.r.status == CUOPT_TERIMINATION_STATUS_OPTIMAL)
+      o.r.crossover = vertex_polish(*ps[ids[b]], o.r);
   }
 }
 
@@ -618,7 +622,7 @@ std::vector<lp_solution> solve_batch(const std::vector<const lp_problem*>& ps, c
       chunk.push_back(eligible[pos++]);
     }
     try {
-      solve_batch_chunk(ps, chunk, lo, up, prm, out);
+      solve_batch_chunk(ps, chunk, lo, up, prm, st.b(CUOPT_CROSSOVER), out);
     } catch (const std::bad_alloc&) {
       for (size_t id : chunk) set_error(out[id], CUOPT_OUT_OF_MEMORY, "Memory allocation failed");
     } catch (const std::invalid_argument& e) {

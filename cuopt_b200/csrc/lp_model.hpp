@@ -86,6 +86,17 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& s);
 std::vector<lp_solution> solve_batch(const std::vector<const lp_problem*>& ps, const lp_settings& s);
 
 // MPS input / output (reference cpp/libmps_parser).  read_mps returns 0 or CUOPT_MPS_* codes.
+// Reverse-mode sensitivities of an optimal solution (see adjoint.cu): gx (n) and optional gy (m)
+// in; any of dc (n), dlo / dup (m, constraint bounds) and dval (nnz, CSR order) out.
+void solution_adjoint(const lp_problem& p, const pdlp_result& sol, const double* gx,
+                      const double* gy, double* dc, double* dlo, double* dup, double* dval);
+
+// Crossover to a vertex on the solution's active set (see adjoint.cu): when the free variables
+// and the constraints held at a bound form a square, non-singular system whose solution is primal
+// and dual feasible, the solution is replaced by that exact vertex and true is returned; otherwise
+// (a degenerate optimum) the solution is left unchanged.
+bool vertex_polish(const lp_problem& p, pdlp_result& r);
+
 int read_mps(const std::string& path, lp_problem& out, std::string& err);
 int write_mps(const lp_problem& p, const std::string& path);
 

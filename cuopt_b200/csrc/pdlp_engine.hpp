@@ -51,6 +51,7 @@ struct pdlp_result {
   double solve_time = 0, setup_time = 0, loop_time = 0;
   double step_size = 0, primal_weight = 0;
   int restarts = 0, power_iterations = 0, refinement_passes = 0;
+  bool crossover = false;  // the solution was replaced by the vertex of its active set
   double kernel_launches = 0;
 };
 

@@ -21,6 +21,8 @@ from __future__ import annotations
 
 from dataclasses import dataclass
 
+from typing import Optional
+
 import numpy as np
 
 
@@ -40,6 +42,7 @@ class LP:
     y_star: np.ndarray
     s_star: np.ndarray
     name: str = "lp"
+    basic: Optional[np.ndarray] = None  # basic columns of a non-degenerate vertex (vertex_lp)
 
     @property
     def nnz(self) -> int:
@@ -102,6 +105,48 @@ def constructed_lp(m: int, n: int, nnz_per_col: int = 8, seed: int = 0, upper: f
     lp.con_lo = b.copy()
     lp.con_up = b.copy()
     lp.c = lp.rmatvec(y) + s
+    return lp
+
+
+def vertex_lp(m: int, n: int, nnz_per_col: int = 8, seed: int = 0, upper: float = 10.0,
+              name: str = "vertex") -> LP:
+    """Config-4 generator: the config-0 recipe with a unique, non-degenerate optimal vertex.
+
+    m basic variables lie strictly inside [0, upper]; basic column basic[i] holds row i with a
+    value of magnitude in [1, 2], so the basis matrix is non-singular.  Every other variable sits
+    on a bound (80 % at 0, 20 % at `upper`) with a reduced cost of the matching sign and magnitude
+    in [0.1, 1], so the optimum is unique and its derivatives with respect to c, b and A exist.
+    """
+    rng = np.random.default_rng(seed)
+    rows = _distinct_rows_per_column(rng, m, n, nnz_per_col)
+    vals = rng.standard_normal((n, nnz_per_col))
+    basic = rng.permutation(n)[:m]
+    diag = np.arange(m)
+    pos = np.argmax(rows[basic] == diag[:, None], axis=1)
+    has = (rows[basic] == diag[:, None]).any(axis=1)
+    pos[~has] = 0
+    rows[basic[~has], 0] = diag[~has]
+    vals[basic, pos] = np.where(rng.random(m) < 0.5, -1.0, 1.0) * rng.uniform(1.0, 2.0, size=m)
+    cols = np.repeat(np.arange(n, dtype=np.int64), nnz_per_col)
+    row_off, col_idx, val = _csr_from_columns(m, n, rows.ravel(), cols, vals.ravel())
+    is_basic = np.zeros(n, dtype=bool)
+    is_basic[basic] = True
+    at_up = (~is_basic) & (rng.random(n) < 0.2)
+    x = np.zeros(n)
+    x[basic] = rng.uniform(0.5, upper - 0.5, size=m)
+    x[at_up] = upper
+    s = np.zeros(n)
+    at_lo = (~is_basic) & (~at_up)
+    s[at_lo] = rng.uniform(0.1, 1.0, size=int(at_lo.sum()))
+    s[at_up] = -rng.uniform(0.1, 1.0, size=int(at_up.sum()))
+    y = rng.standard_normal(m)
+    lp = LP(m, n, row_off, col_idx, val, np.zeros(n), np.zeros(m), np.zeros(m),
+            np.zeros(n), np.full(n, float(upper)), x, y, s, name)
+    b = lp.matvec(x)
+    lp.con_lo = b.copy()
+    lp.con_up = b.copy()
+    lp.c = lp.rmatvec(y) + s
+    lp.basic = np.sort(basic)
     return lp
 
 

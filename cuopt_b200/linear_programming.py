@@ -32,6 +32,7 @@ CUOPT_PRESOLVE = "presolve"
 CUOPT_LOG_TO_CONSOLE = "log_to_console"
 CUOPT_INFEASIBILITY_DETECTION = "infeasibility_detection"
 CUOPT_PER_CONSTRAINT_RESIDUAL = "per_constraint_residual"
+CUOPT_CROSSOVER = "crossover"
 # Additions of this library
 CUOPT_PDLP_PRECISION = "pdlp_precision"
 CUOPT_PDLP_REFINEMENT_PASSES = "pdlp_refinement_passes"

@@ -39,6 +39,7 @@ typedef struct {
   cuopt_float_t setup_time;     /* seconds spent before the first PDHG iteration */
   cuopt_float_t loop_time;      /* seconds spent in the iteration loop */
   cuopt_float_t kernel_launches; /* kernels this library launched for the solve */
+  cuopt_int_t crossover;         /* 1: the solution is the vertex of its active set ("crossover") */
 } cuOptPDLPStatistics;
 
 cuopt_int_t cuOptGetPDLPStatistics(cuOptSolution solution, cuOptPDLPStatistics* stats);
