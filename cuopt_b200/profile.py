@@ -8,6 +8,10 @@
          (cuOptProfilePDHGSweeps).
 `batch`  (config c3) solves the 512-instance batch in one cuOptBatchSolve call and a sample of the
          same instances one by one with cuOptSolve (FP64, 1e-6).
+`adjoint` (config c4) solves 64 non-degenerate 5000 x 10000 LPs in one batched call (crossover
+         on), back-propagates L = sum w * x* through the KKT adjoint, and checks the gradients
+         against the exact basis derivatives and against central differences (h = 1e-6) on random
+         coordinates of c, b and the A values.
 Prints one JSON line with the timings.
 """
 from __future__ import annotations
@@ -43,7 +47,11 @@ def main() -> None:
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c1_small")
-    ap.add_argument("--mode", choices=["solve", "sweeps", "batch"], default="sweeps")
+    ap.add_argument("--mode", choices=["solve", "sweeps", "batch", "adjoint"], default="sweeps")
+    ap.add_argument("--fd-instances", type=int, default=2,
+                    help="adjoint mode: instances checked by finite differences")
+    ap.add_argument("--fd-coords", type=int, default=32,
+                    help="adjoint mode: coordinates per kind (c, b, A) and instance")
     ap.add_argument("--count", type=int, default=512, help="batch mode: instances")
     ap.add_argument("--sequential", type=int, default=64,
                     help="batch mode: instances also solved one by one (timing sample)")
@@ -58,6 +66,9 @@ def main() -> None:
 
     if a.mode == "batch":
         print(json.dumps(run_batch(a)))
+        return
+    if a.mode == "adjoint":
+        print(json.dumps(run_adjoint(a)))
         return
     m, n, k, seed = CONFIGS[a.config]
     lp = gen.constructed_lp(m, n, k, seed=seed) if k else gen.skewed_lp(m, n, seed=seed)
@@ -170,6 +181,101 @@ def run_batch(a) -> dict:
                     "speedup_batch_vs_sequential": (len(pick) / seq_s and
                                                     (a.count / batch_s) / (len(pick) / seq_s))})
     return out
+
+
+def run_adjoint(a) -> dict:
+    """Config 4: batched forward solve + KKT-adjoint backward, checked two ways."""
+    import numpy as np
+    import scipy.sparse as sp
+    import torch
+    from scipy.sparse.linalg import splu
+
+    from cuopt_b200 import generators as gen
+    from cuopt_b200 import linear_programming as lpm
+    from cuopt_b200.torch_layer import LPInstance, lp_solve_batch
+
+    count = a.count
+    lps = [gen.vertex_lp(5000, 10000, 8, seed=4000 + i) for i in range(count)]
+    rng = np.random.default_rng(4)
+    ws = [rng.standard_normal(lp.n) for lp in lps]
+    dev = torch.device("cuda", 0)
+    f = lambda v: torch.tensor(v, device=dev, dtype=torch.float64)
+    i32 = lambda v: torch.tensor(v, device=dev, dtype=torch.int32)
+
+    def instance(lp, c=None, lo=None, up=None, val=None, grad=False):
+        t = LPInstance(f(lp.c if c is None else c), f(lp.con_lo if lo is None else lo),
+                       f(lp.con_up if up is None else up), f(lp.val if val is None else val),
+                       i32(lp.row_off), i32(lp.col_idx), f(lp.var_lo), f(lp.var_up))
+        if grad:
+            for x in (t.c, t.con_lo, t.con_up, t.values):
+                x.requires_grad_()
+        return t
+
+    st = lpm.SolverSettings()
+    st.set_optimality_tolerance(a.tol)
+    st.set_parameter(lpm.CUOPT_METHOD, int(lpm.SolverMethod.PDLP))
+    st.set_parameter(lpm.CUOPT_CROSSOVER, True)
+    st.set_parameter(lpm.CUOPT_LOG_TO_CONSOLE, False)
+    insts = [instance(lp, grad=True) for lp in lps]
+    lp_solve_batch([instance(lps[0])], st)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    outs = lp_solve_batch(insts, st)
+    torch.cuda.synchronize()
+    forward_s = time.perf_counter() - t0
+    loss = sum((f(w) * x).sum() for w, (x, _) in zip(ws, outs))
+    t0 = time.perf_counter()
+    loss.backward()
+    torch.cuda.synchronize()
+    backward_s = time.perf_counter() - t0
+
+    # Exact basis derivatives (an independent sparse LU of each basis).
+    err = {"c": 0.0, "b": 0.0, "A": 0.0}
+    rel = lambda g, e: float(np.abs(g - e).max() / max(1.0, np.abs(e).max()))
+    for lp, w, t in zip(lps, ws, insts):
+        A = sp.csr_matrix((lp.val, lp.col_idx, lp.row_off), shape=(lp.m, lp.n))
+        lam = splu(A[:, lp.basic].tocsc()).solve(w[lp.basic], trans="T")
+        rows = np.repeat(np.arange(lp.m), np.diff(lp.row_off))
+        dval = -lam[rows] * lp.x_star[lp.col_idx]
+        err["c"] = max(err["c"], float(np.abs(t.c.grad.cpu().numpy()).max()))
+        err["b"] = max(err["b"], rel((t.con_lo.grad + t.con_up.grad).cpu().numpy(), lam))
+        err["A"] = max(err["A"], rel(t.values.grad.cpu().numpy(), dval))
+
+    # Central differences through the solver (all perturbed LPs in one batched call).
+    h, fd_err, checked = 1e-6, 0.0, 0
+    pert, keys = [], []
+    for q in range(min(a.fd_instances, count)):
+        lp = lps[q]
+        picks = {"c": rng.choice(lp.n, a.fd_coords, replace=False),
+                 "b": rng.choice(lp.m, a.fd_coords, replace=False),
+                 "A": rng.choice(lp.nnz, a.fd_coords, replace=False)}
+        for kind, idx in picks.items():
+            for k in idx:
+                for sgn in (1.0, -1.0):
+                    c, lo, up, val = lp.c.copy(), lp.con_lo.copy(), lp.con_up.copy(), lp.val.copy()
+                    if kind == "c":
+                        c[k] += sgn * h
+                    elif kind == "b":
+                        lo[k] += sgn * h
+                        up[k] += sgn * h
+                    else:
+                        val[k] += sgn * h
+                    pert.append(instance(lp, c, lo, up, val))
+                    keys.append((q, kind, int(k), sgn))
+    res = lp_solve_batch(pert, st) if pert else []
+    vals = {key: float(x.detach().cpu().numpy() @ ws[key[0]]) for key, (x, _) in zip(keys, res)}
+    for (q, kind, k, sgn) in keys:
+        if sgn < 0:
+            continue
+        fd = (vals[(q, kind, k, 1.0)] - vals[(q, kind, k, -1.0)]) / (2 * h)
+        t = insts[q]
+        g = {"c": t.c.grad, "b": t.con_lo.grad + t.con_up.grad, "A": t.values.grad}[kind][k].item()
+        fd_err = max(fd_err, abs(fd - g) / (1.0 + abs(g)))
+        checked += 1
+    return {"config": "c4", "count": count, "m": 5000, "n": 10000, "forward_s": forward_s,
+            "backward_s": backward_s, "adjoint_ms_per_instance": backward_s * 1e3 / count,
+            "grad_vs_basis_max_rel_error": err, "fd_checked": checked, "fd_h": h,
+            "fd_max_rel_error": fd_err}
 
 
 if __name__ == "__main__":
