@@ -720,6 +720,101 @@ __global__ void scale_initial_kernel(const double* v, const double* d, double fa
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Infeasibility detection (reference infeasibility_information.cu:230-490, the cuPDLPx branch).
+// The rays are the step's deltas x_bar - x and y_bar - y in the scaled space, clamped to the
+// recession cones of the bounds.
+
+// d_j = clamp(x_bar_j - x_j) (>= 0 on a finite lower bound, <= 0 on a finite upper bound) and
+// cd_j = c_j d_j;  e_i = clamp(y_bar_i - y_i) (<= 0 without a finite lower bound, >= 0 without a
+// finite upper bound) and pe_i = max(e_i, 0) fin(lc_i) + min(e_i, 0) fin(uc_i).
+template <typename TX>
+__global__ void ray_vectors_kernel(const TX* x, const TX* xbar, const TX* l, const TX* u,
+                                   const TX* c, int n, const TX* y, const TX* ybar, const TX* lc,
+                                   const TX* uc, int m, double* d, double* cd, double* e,
+                                   double* pe)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x) {
+    if (i < n) {
+      double v = (double)xbar[i] - (double)x[i];
+      if (isfinite((double)l[i])) v = fmax(v, 0.0);
+      if (isfinite((double)u[i])) v = fmin(v, 0.0);
+      d[i]  = v;
+      cd[i] = (double)c[i] * v;
+    } else {
+      const int r = i - n;
+      double v    = (double)ybar[r] - (double)y[r];
+      if (!isfinite((double)lc[r])) v = fmin(v, 0.0);
+      if (!isfinite((double)uc[r])) v = fmax(v, 0.0);
+      e[r]  = v;
+      pe[r] = fmax(v, 0.0) * finite_or_zero((double)lc[r]) + fmin(v, 0.0) * finite_or_zero((double)uc[r]);
+    }
+  }
+}
+
+// Row i of A applied to d: violation of the primal ray, (max(-Ad, 0) [lc finite] +
+// max(Ad, 0) [uc finite]) dr_i with Ad scaled by 1 / |d|_inf.
+template <typename TX>
+struct ray_primal_epi {
+  static constexpr int kRed = 0;
+  const TX* lc;
+  const TX* uc;
+  const double* dr;
+  double inv_norm;
+  double* out;
+  struct pre_t {};
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ pre_t load(int) const { return pre_t{}; }
+  __device__ __forceinline__ void operator()(int i, double acc, const pre_t&, red_t<0>&) const
+  {
+    const double ad = acc * inv_norm;
+    out[i]          = (fmax(-ad, 0.0) * (isfinite((double)lc[i]) ? 1.0 : 0.0) +
+              fmax(ad, 0.0) * (isfinite((double)uc[i]) ? 1.0 : 0.0)) *
+             dr[i];
+  }
+};
+
+// Row j of A^T applied to e (g = (A^T e)_j): dual-slack objective term and dual-ray violation.
+template <typename TX>
+struct ray_dual_epi {
+  static constexpr int kRed = 0;
+  const TX* l;
+  const TX* u;
+  const double* dc;
+  double* slack_term;
+  double* violation;
+  struct pre_t {};
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ pre_t load(int) const { return pre_t{}; }
+  __device__ __forceinline__ void operator()(int j, double g, const pre_t&, red_t<0>&) const
+  {
+    const double lj = (double)l[j], uj = (double)u[j];
+    slack_term[j] = fmax(-g, 0.0) * finite_or_zero(lj) + fmin(-g, 0.0) * finite_or_zero(uj);
+    violation[j]  = (fmax(-g, 0.0) * (isfinite(lj) ? 0.0 : 1.0) -
+                    fmin(-g, 0.0) * (isfinite(uj) ? 0.0 : 1.0)) *
+                   dc[j];
+  }
+};
+
+// Per-block sum (MAX = false) or maximum of |a| (MAX = true) into partials[blockIdx.x].
+template <bool MAX>
+__global__ void __launch_bounds__(kBlock) block_stat_kernel(const double* a, int n, double* partials)
+{
+  __shared__ double sm[kBlock];
+  double v = 0.0;
+  for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock)
+    v = MAX ? fmax(v, fabs(a[i])) : v + a[i];
+  sm[threadIdx.x] = v;
+  __syncthreads();
+  for (int h = kBlock / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h)
+      sm[threadIdx.x] = MAX ? fmax(sm[threadIdx.x], sm[threadIdx.x + h])
+                            : sm[threadIdx.x] + sm[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = sm[0];
+}
+
 // Elementwise helpers
 template <typename TX>
 __global__ void clamp_kernel(TX* x, const TX* l, const TX* u, int n)

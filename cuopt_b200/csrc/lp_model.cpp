@@ -366,6 +366,9 @@ pdlp_params params_from_settings(const lp_settings& st)
   prm.refinement_passes = st.i(CUOPT_PDLP_REFINEMENT_PASSES);
   prm.refinement_tol    = st.f(CUOPT_PDLP_REFINEMENT_TOLERANCE);
   prm.log_to_console    = st.b(CUOPT_LOG_TO_CONSOLE);
+  prm.detect_infeasibility  = st.b(CUOPT_INFEASIBILITY_DETECTION);
+  prm.primal_infeasible_tol = st.f(CUOPT_PRIMAL_INFEASIBLE_TOLERANCE);
+  prm.dual_infeasible_tol   = st.f(CUOPT_DUAL_INFEASIBLE_TOLERANCE);
   return prm;
 }
 

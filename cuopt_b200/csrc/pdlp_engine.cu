@@ -50,6 +50,9 @@ struct loop_state {
   double pid_sum = 0.0, pid_last = 0.0;
   double best_gap = std::numeric_limits<double>::infinity();
   bool fresh      = true;  // no iteration run yet: the loop starts by zeroing the step counter
+  // Infeasibility test statistics (zero until first computed, then kept between computations).
+  double primal_ray_obj = 0.0, max_primal_ray_inf = 0.0;
+  double dual_ray_obj = 0.0, max_dual_ray_inf = 0.0;
 };
 
 template <typename TX>
@@ -572,6 +575,56 @@ class engine {
     r.loop_time    = t_loop_ > 0 ? t - t_loop_ : 0.0;
   }
 
+  // Host-side sum / maximum of block statistics (fixed order).
+  template <bool MAX>
+  double stat(const double* a, int count)
+  {
+    block_stat_kernel<MAX><<<vgrid_, kBlock, 0, s_>>>(a, count, partials_.data());
+    ++launches_;
+    B200_LAUNCH_CHECK();
+    std::vector<double> h(vgrid_);
+    B200_CUDA_CHECK(cudaMemcpyAsync(h.data(), partials_.data(), vgrid_ * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s_));
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    double v = 0.0;
+    for (double p : h) v = MAX ? std::max(v, p) : v + p;
+    return v;
+  }
+
+  // Ray statistics of the infeasibility test (reference infeasibility_information.cu:230-490,
+  // cuPDLPx branch) from x_bar - x and y_bar - y of the current step.
+  void ray_statistics()
+  {
+    const int m = in_.m, n = in_.n;
+    dbuf<double> d(n), cd(n), e(m), pe(m), vm(m), sn(n), vn(n);
+    ray_vectors_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(
+      x_.data(), xbar_.data(), ls_.data(), us_.data(), cs_.data(), n, y_.data(), ybar_.data(),
+      lcs_.data(), ucs_.data(), m, d.data(), cd.data(), e.data(), pe.data());
+    ++launches_;
+    B200_LAUNCH_CHECK();
+    const double nd = stat<true>(d.data(), n), ne = stat<true>(e.data(), m);
+    const double sum_cd = stat<false>(cd.data(), n), sum_ps = stat<false>(pe.data(), m);
+    const auto A = As_view(), AT = ATs_view();
+    sell_map_kernel<TX, double, ray_primal_epi<TX>><<<sell_grid(A), kBlock, 0, s_>>>(
+      A, d.data(),
+      ray_primal_epi<TX>{lcs_.data(), ucs_.data(), dr_.data(), nd > 0.0 ? 1.0 / nd : 1.0,
+                         vm.data()},
+      partials_.data());
+    sell_map_kernel<TX, double, ray_dual_epi<TX>><<<sell_grid(AT), kBlock, 0, s_>>>(
+      AT, e.data(), ray_dual_epi<TX>{ls_.data(), us_.data(), dc_.data(), sn.data(), vn.data()},
+      partials_.data());
+    launches_ += 2;
+    B200_LAUNCH_CHECK();
+    const double br  = beta_ * gamma_;
+    const double sum_ds = stat<false>(sn.data(), n);
+    const double mdi    = stat<true>(vn.data(), n);
+    sched_.max_primal_ray_inf = stat<true>(vm.data(), m);
+    sched_.primal_ray_obj     = (nd > 0.0 ? sum_cd / nd : sum_cd) / br;
+    const double sf = std::max(mdi, ne);
+    sched_.max_dual_ray_inf = sf > 0.0 ? mdi / sf : 0.0;
+    sched_.dual_ray_obj     = sf > 0.0 ? ((sum_ps + sum_ds) / br) / sf : 0.0;
+  }
+
   // ------------------------------------------------------------------ main loop
   void loop(pdlp_result& r)
   {
@@ -607,6 +660,16 @@ class engine {
           std::printf("%7ld %+.8e %+.8e  %8.2e   %8.2e     %8.2e   %.3fs\n", k, cv.primal_obj,
                       cv.dual_obj, cv.gap, cv.l2_primal, cv.l2_dual, now_s() - t_start_);
         if (k > 1 && status == kOptimal) return finish(r, kOptimal, cv, k);
+        // check_termination_criteria_kernel (reference termination_strategy.cu:354-376); Stable3
+        // returns any current infeasibility (never_restart_to_average, pdlp.cu:1089-1109).
+        if (p_.detect_infeasibility && status == kNoTermination) {
+          if (sched_.dual_ray_obj > 0.0 &&
+              sched_.max_dual_ray_inf / sched_.dual_ray_obj <= p_.primal_infeasible_tol)
+            return finish(r, kPrimalInfeasible, cv, k);
+          if (sched_.primal_ray_obj < 0.0 &&
+              sched_.max_primal_ray_inf / -sched_.primal_ray_obj <= p_.dual_infeasible_tol)
+            return finish(r, kDualInfeasible, cv, k);
+        }
         if (now_s() - t_start_ >= p_.time_limit) return finish(r, kTimeLimit, cv, k);
         if (k >= p_.iteration_limit) return finish(r, kIterationLimit, cv, k);
         if (!std::isfinite(cv.l2_primal) || !std::isfinite(cv.l2_dual))
@@ -699,6 +762,10 @@ class engine {
           AT, ybar_.data(), fpe_epi<TX>{aty_.data(), xbar_.data(), x_.data()}, partials_.data());
         finalize_sum_kernel<2><<<1, kBlock, 0, s_>>>(partials_.data(), sell_grid(AT),
                                                      dres_.data() + 9);
+        // Infeasibility information from this step's deltas, for the checks at iterations 200
+        // and 400 only (reference termination_strategy.cu:187-199).
+        if (p_.detect_infeasibility && (k + 1) % kMajor == 0 && (k + 1) < 3 * kMajor)
+          ray_statistics();
         halpern_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(x_.data(), xbar_.data(), xa_.data(), n,
                                                       y_.data(), ybar_.data(), ya_.data(), m,
                                                       scalars_.data());

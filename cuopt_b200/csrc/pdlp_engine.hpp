@@ -38,6 +38,10 @@ struct pdlp_params {
   int refinement_passes   = 0;
   double refinement_tol   = 1e-8;
   bool log_to_console     = false;
+  // Infeasibility detection (CUOPT_INFEASIBILITY_DETECTION and its two tolerances).
+  bool detect_infeasibility   = false;
+  double primal_infeasible_tol = 1e-10;
+  double dual_infeasible_tol   = 1e-10;
   std::vector<double> initial_primal;  // user order, optional
   std::vector<double> initial_dual;    // user order, optional
 };

@@ -4,7 +4,7 @@
 namespace cuopt_b200 {
 
 constexpr int kOptimal = 1, kIterationLimit = 4, kTimeLimit = 5, kNumericalError = 6,
-              kPrimalFeasible = 7, kNoTermination = 0;
+              kPrimalFeasible = 7, kNoTermination = 0, kPrimalInfeasible = 2, kDualInfeasible = 3;
 
 // Stable3 constants (reference solve.cu:167-209, pdlp_hyper_params.cuh:12-56,
 // pdlp_restart_strategy.cu:689-836, pdlp.cu:2620-2731).

@@ -26,7 +26,9 @@ class _Settings(C.Structure):
     _fields_ = [("abs_primal", C.c_double), ("rel_primal", C.c_double),
                 ("abs_dual", C.c_double), ("rel_dual", C.c_double),
                 ("abs_gap", C.c_double), ("rel_gap", C.c_double),
-                ("iteration_limit", C.c_long), ("time_limit", C.c_double), ("threads", C.c_int)]
+                ("iteration_limit", C.c_long), ("time_limit", C.c_double), ("threads", C.c_int),
+                ("detect_infeasibility", C.c_int), ("primal_infeasible_tolerance", C.c_double),
+                ("dual_infeasible_tolerance", C.c_double)]
 
 
 class _Result(C.Structure):
@@ -77,11 +79,13 @@ def _holder(lp):
                    getattr(lp, "obj_offset", 0.0), getattr(lp, "maximize", False))
 
 
-def solve(lp, tol=1e-4, iteration_limit=2**31 - 1, time_limit=1e300, threads=0):
+def solve(lp, tol=1e-4, iteration_limit=2**31 - 1, time_limit=1e300, threads=0,
+          detect_infeasibility=False, infeasible_tol=1e-10):
     """Runs the FP64 Stable3 restatement.  Returns (result dict, x, y, reduced_cost)."""
     h = _holder(lp)
     m, n = h.s.m, h.s.n
-    st = _Settings(tol, tol, tol, tol, tol, tol, int(iteration_limit), float(time_limit), int(threads))
+    st = _Settings(tol, tol, tol, tol, tol, tol, int(iteration_limit), float(time_limit), int(threads),
+                   int(bool(detect_infeasibility)), float(infeasible_tol), float(infeasible_tol))
     r = _Result()
     x, y, rc = np.zeros(n), np.zeros(m), np.zeros(n)
     lib().oracle_pdlp_solve(C.byref(h.s), C.byref(st), C.byref(r), x.ctypes.data, y.ctypes.data,

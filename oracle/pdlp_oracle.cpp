@@ -383,6 +383,8 @@ struct oracle_settings {
   long iteration_limit;
   double time_limit;
   int threads;
+  int detect_infeasibility;                                   // CUOPT_INFEASIBILITY_DETECTION
+  double primal_infeasible_tolerance, dual_infeasible_tolerance;
 };
 
 struct oracle_result {
@@ -423,7 +425,8 @@ lp_t build(const oracle_lp* in)
   return p;
 }
 
-enum { kNoTermination = 0, kOptimal = 1, kInfeasible = 2, kIterationLimit = 4, kTimeLimit = 5,
+enum { kNoTermination = 0, kOptimal = 1, kInfeasible = 2, kUnbounded = 3, kIterationLimit = 4,
+       kTimeLimit = 5,
        kNumericalError = 6, kPrimalFeasible = 7 };
 
 }  // namespace
@@ -516,6 +519,9 @@ int oracle_pdlp_solve(const oracle_lp* in, const oracle_settings* st, oracle_res
 
   const double qnan = std::numeric_limits<double>::quiet_NaN();
   double fpe = qnan, fpe0 = qnan, last_trial = kInf;
+  // Ray statistics of the infeasibility test (infeasibility_information.cu:220-490, cuPDLPx
+  // branch); zero until first computed, then kept between computations.
+  double primal_ray_obj = 0.0, max_primal_ray_inf = 0.0, dual_ray_obj = 0.0, max_dual_ray_inf = 0.0;
   double pid_sum = 0.0, pid_last = 0.0, best_gap = kInf;
   long iters_since_restart = 0;
   int restarts = 0;
@@ -559,6 +565,15 @@ int oracle_pdlp_solve(const oracle_lp* in, const oracle_settings* st, oracle_res
       else if (primal_ok)
         status = kPrimalFeasible;
       if (k > 1 && status == kOptimal) return finish(kOptimal, cv, k);
+      // check_termination_criteria_kernel (termination_strategy.cu:354-376); Stable3 returns any
+      // current infeasibility (never_restart_to_average, pdlp.cu:1089-1109).
+      if (st->detect_infeasibility && status == kNoTermination) {
+        if (dual_ray_obj > 0.0 && max_dual_ray_inf / dual_ray_obj <= st->primal_infeasible_tolerance)
+          return finish(kInfeasible, cv, k);
+        if (primal_ray_obj < 0.0 &&
+            max_primal_ray_inf / -primal_ray_obj <= st->dual_infeasible_tolerance)
+          return finish(kUnbounded, cv, k);
+      }
       if (elapsed() >= st->time_limit) return finish(kTimeLimit, cv, k);
       if (k >= st->iteration_limit) return finish(kIterationLimit, cv, k);
       rescale(s, x_hat, y_hat, slack);
@@ -649,6 +664,62 @@ int oracle_pdlp_solve(const oracle_lp* in, const oracle_settings* st, oracle_res
       const double movement = ndx * omega + ndy / omega;
       fpe = std::sqrt(movement + 2.0 * inter * eta);
       if (restarted[0]) fpe0 = fpe;
+      // Infeasibility information from the deltas of this step, for the checks at iterations 200
+      // and 400 only (termination_strategy.cu:187-199; infeasibility_information.cu:230-490).
+      if (st->detect_infeasibility && (k + 1) % h.major_iteration == 0 &&
+          (k + 1) < 3 * h.major_iteration) {
+        vec d(n), e(m), ad(m), ate(n);
+        for (int j = 0; j < n; ++j) {
+          double v = x_bar[j] - x[j];
+          if (std::isfinite(q.var_lo[j])) v = std::max(v, 0.0);
+          if (std::isfinite(q.var_up[j])) v = std::min(v, 0.0);
+          d[j] = v;
+        }
+        double nd = 0.0, ne = 0.0;
+        for (int j = 0; j < n; ++j) nd = std::max(nd, std::fabs(d[j]));
+        for (int i = 0; i < m; ++i) {
+          double v = y_bar[i] - y[i];
+          if (!std::isfinite(q.con_lo[i])) v = std::min(v, 0.0);
+          if (!std::isfinite(q.con_up[i])) v = std::max(v, 0.0);
+          e[i] = v;
+          ne   = std::max(ne, std::fabs(v));
+        }
+        if (nd > 0.0)
+          for (int j = 0; j < n; ++j) d[j] /= nd;
+        spmv(q.a, d.data(), ad.data());
+        spmv(q.at, e.data(), ate.data());
+        const double br = s.beta * s.gamma;
+        const auto fin  = [](double v) { return std::isfinite(v) ? v : 0.0; };
+        primal_ray_obj  = chunk_sum(n, [&](int j) { return q.c[j] * d[j]; }) / br;
+        const double sum_ps = chunk_sum(m, [&](int i) {
+          return std::max(e[i], 0.0) * fin(q.con_lo[i]) + std::min(e[i], 0.0) * fin(q.con_up[i]);
+        });
+        const double sum_ds = chunk_sum(n, [&](int j) {
+          return std::max(-ate[j], 0.0) * fin(q.var_lo[j]) + std::min(-ate[j], 0.0) * fin(q.var_up[j]);
+        });
+        max_primal_ray_inf = 0.0;
+        for (int i = 0; i < m; ++i) {
+          const double v = (std::max(-ad[i], 0.0) * (std::isfinite(q.con_lo[i]) ? 1.0 : 0.0) +
+                            std::max(ad[i], 0.0) * (std::isfinite(q.con_up[i]) ? 1.0 : 0.0)) *
+                           s.dr[i];
+          max_primal_ray_inf = std::max(max_primal_ray_inf, std::fabs(v));
+        }
+        double mdi = 0.0;
+        for (int j = 0; j < n; ++j) {
+          const double v = (std::max(-ate[j], 0.0) * (std::isfinite(q.var_lo[j]) ? 0.0 : 1.0) -
+                            std::min(-ate[j], 0.0) * (std::isfinite(q.var_up[j]) ? 0.0 : 1.0)) *
+                           s.dc[j];
+          mdi = std::max(mdi, std::fabs(v));
+        }
+        const double sf = std::max(mdi, ne);
+        if (sf > 0.0) {
+          max_dual_ray_inf = mdi / sf;
+          dual_ray_obj     = ((sum_ps + sum_ds) / br) / sf;
+        } else {
+          max_dual_ray_inf = 0.0;
+          dual_ray_obj     = 0.0;
+        }
+      }
     }
 
     // halpern_update (pdlp.cu:2506-2563)

@@ -56,3 +56,35 @@ def settings(tol=1e-4, iteration_limit=None, time_limit=None, precision=None, me
 
 def rel(a, b):
     return abs(a - b) / max(1.0, abs(b))
+
+
+def small_lp(rows, c, con_lo, con_up, var_lo, var_up):
+    """An LP view (as the oracle and datamodel_from_lp take it) from dense row lists
+    [[(column, value), ...], ...]."""
+    from types import SimpleNamespace
+    off, idx, val = [0], [], []
+    for r in rows:
+        for j, v in r:
+            idx.append(j)
+            val.append(v)
+        off.append(len(idx))
+    return SimpleNamespace(m=len(rows), n=len(c), row_off=np.array(off, np.int32),
+                           col_idx=np.array(idx, np.int32), val=np.array(val, float),
+                           c=np.array(c, float), con_lo=np.array(con_lo, float),
+                           con_up=np.array(con_up, float), var_lo=np.array(var_lo, float),
+                           var_up=np.array(var_up, float), obj_offset=0.0, maximize=False)
+
+
+def infeasible_cases(golden_dir):
+    """(name, lp view) pairs: a 2-row LP with no feasible point, and afiro with the variable bounds
+    of the reference's (disabled) infeasibility test (pdlp_test.cu:1289-1313: variables 1-7 in
+    [7, 8], variables 13-26 in [1, 5])."""
+    inf = np.inf
+    tiny = small_lp([[(0, 1.0), (1, 1.0)], [(0, 1.0), (1, -1.0)]], [1.0, 1.0], [-inf, -inf],
+                    [-1.0, 0.0], [0.0, 0.0], [inf, inf])
+    afiro = oracle_view(lpm.ReadMps(golden_dir / "afiro_original.mps"))
+    afiro.var_lo = afiro.var_lo.copy()
+    afiro.var_up = afiro.var_up.copy()
+    afiro.var_lo[1:8], afiro.var_up[1:8] = 7.0, 8.0
+    afiro.var_lo[13:27], afiro.var_up[13:27] = 1.0, 5.0
+    return [("two_rows", tiny), ("afiro_new_bounds", afiro)]

@@ -205,3 +205,15 @@ def test_repeat_solves_bitwise_identical():
     b = lpm.Solve(dm, settings(tol=1e-12, iteration_limit=300))
     assert np.array_equal(a.get_primal_solution(), b.get_primal_solution())
     assert np.array_equal(a.get_dual_solution(), b.get_dual_solution())
+
+
+def test_infeasibility_detection_matches_oracle(golden_dir):
+    """Infeasible LPs end PrimalInfeasible at the same check as in the oracle."""
+    from tests.helpers import infeasible_cases
+    for name, lp in infeasible_cases(golden_dir):
+        s = settings(tol=1e-6, iteration_limit=3000)
+        s.set_parameter(lpm.CUOPT_INFEASIBILITY_DETECTION, True)
+        sol = lpm.Solve(datamodel_from_lp(lp), s)
+        res, _, _, _ = O.solve(lp, tol=1e-6, iteration_limit=3000, detect_infeasibility=True)
+        assert int(sol.get_termination_status()) == res["status"] == 2, name
+        assert sol.get_lp_stats()["nb_iterations"] == res["iterations"], name

@@ -109,3 +109,19 @@ def test_highs_cross_check():
     assert rel(r.fun, lp.optimal_objective) <= 1e-9
     res, _, _, _ = O.solve(lp, tol=1e-8)
     assert rel(res["primal_obj"], r.fun) <= 1e-7
+
+
+def test_infeasibility_detection(golden_dir):
+    """With detection on, both infeasible cases end PrimalInfeasible at one of the two checks that
+    test it (iterations 200 and 400); with it off they run to the iteration limit, and a feasible
+    LP follows the same iterations either way."""
+    from tests.helpers import infeasible_cases, oracle_view
+    for name, lp in infeasible_cases(golden_dir):
+        res, _, _, _ = O.solve(lp, tol=1e-6, iteration_limit=3000, detect_infeasibility=True)
+        assert res["status"] == 2 and res["iterations"] in (200, 400), (name, res)
+        res, _, _, _ = O.solve(lp, tol=1e-6, iteration_limit=3000)
+        assert res["status"] == 4, name
+    afiro = oracle_view(lpm.ReadMps(golden_dir / "afiro_original.mps"))
+    a, _, _, _ = O.solve(afiro, tol=1e-6, detect_infeasibility=True)
+    b, _, _, _ = O.solve(afiro, tol=1e-6)
+    assert a["status"] == b["status"] == 1 and a["iterations"] == b["iterations"]
