@@ -19,7 +19,8 @@ class _LP(C.Structure):
                 ("row_off", C.c_void_p), ("col_idx", C.c_void_p), ("val", C.c_void_p),
                 ("c", C.c_void_p), ("con_lo", C.c_void_p), ("con_up", C.c_void_p),
                 ("var_lo", C.c_void_p), ("var_up", C.c_void_p),
-                ("obj_offset", C.c_double), ("maximize", C.c_int)]
+                ("obj_offset", C.c_double), ("maximize", C.c_int),
+                ("initial_primal", C.c_void_p), ("initial_dual", C.c_void_p)]
 
 
 class _Settings(C.Structure):
@@ -65,24 +66,29 @@ class _Holder:
     """Keeps the numpy arrays alive while the C struct points at them."""
 
     def __init__(self, row_off, col_idx, val, c, con_lo, con_up, var_lo, var_up, obj_offset=0.0,
-                 maximize=False):
+                 maximize=False, initial_primal=None, initial_dual=None):
         self.a = [np.ascontiguousarray(row_off, np.int32), np.ascontiguousarray(col_idx, np.int32)]
         self.a += [np.ascontiguousarray(v, np.float64) for v in (val, c, con_lo, con_up, var_lo, var_up)]
         p = [x.ctypes.data for x in self.a]
         m = len(self.a[0]) - 1
+        self.init = [None if v is None else np.ascontiguousarray(v, np.float64)
+                     for v in (initial_primal, initial_dual)]
         self.s = _LP(m, len(self.a[3]), int(self.a[0][-1]) if m >= 0 else 0, *p,
-                     float(obj_offset), int(bool(maximize)))
+                     float(obj_offset), int(bool(maximize)),
+                     *[None if v is None else v.ctypes.data for v in self.init])
 
 
-def _holder(lp):
+def _holder(lp, initial_primal=None, initial_dual=None):
     return _Holder(lp.row_off, lp.col_idx, lp.val, lp.c, lp.con_lo, lp.con_up, lp.var_lo, lp.var_up,
-                   getattr(lp, "obj_offset", 0.0), getattr(lp, "maximize", False))
+                   getattr(lp, "obj_offset", 0.0), getattr(lp, "maximize", False),
+                   initial_primal, initial_dual)
 
 
 def solve(lp, tol=1e-4, iteration_limit=2**31 - 1, time_limit=1e300, threads=0,
-          detect_infeasibility=False, infeasible_tol=1e-10):
-    """Runs the FP64 Stable3 restatement.  Returns (result dict, x, y, reduced_cost)."""
-    h = _holder(lp)
+          detect_infeasibility=False, infeasible_tol=1e-10, initial_primal=None, initial_dual=None):
+    """Runs the FP64 Stable3 restatement (optionally warm-started from an initial primal and / or
+    dual solution in the user's order).  Returns (result dict, x, y, reduced_cost)."""
+    h = _holder(lp, initial_primal, initial_dual)
     m, n = h.s.m, h.s.n
     st = _Settings(tol, tol, tol, tol, tol, tol, int(iteration_limit), float(time_limit), int(threads),
                    int(bool(detect_infeasibility)), float(infeasible_tol), float(infeasible_tol))

@@ -376,6 +376,8 @@ struct oracle_lp {
   const double* var_up;
   double obj_offset;
   int maximize;
+  const double* initial_primal;  // optional (n), user order; null: start from zero
+  const double* initial_dual;    // optional (m)
 };
 
 struct oracle_settings {
@@ -514,6 +516,19 @@ int oracle_pdlp_solve(const oracle_lp* in, const oracle_settings* st, oracle_res
 
   vec x(n, 0.0), y(m, 0.0), x_hat(n, 0.0), y_hat(m, 0.0), slack(n, 0.0), x_bar(n, 0.0),
     y_bar(m, 0.0), x_anchor(n, 0.0), y_anchor(m, 0.0), aty(n, 0.0), ax(m, 0.0), next_aty(n, 0.0);
+  // Initial solution (pdlp.cu:1236-1400, set_initial_primal_solution :305-330): x, the
+  // potential next iterate and the restart anchor take it, scaled by scale_solutions
+  // (initial_scaling.cu:571-640).
+  if (in->initial_primal)
+    for (int j = 0; j < n; ++j) {
+      const double v = s.dc[j] != 0 ? in->initial_primal[j] / s.dc[j] : in->initial_primal[j];
+      x[j] = x_hat[j] = x_anchor[j] = v * s.beta;
+    }
+  if (in->initial_dual)
+    for (int i = 0; i < m; ++i) {
+      const double v = s.dr[i] != 0 ? in->initial_dual[i] / s.dr[i] : in->initial_dual[i];
+      y[i] = y_hat[i] = y_anchor[i] = v * s.gamma;
+    }
   // project_initial_primal (pdlp.cu:2237-2262): only x, not the anchor
   for (int j = 0; j < n; ++j) x[j] = std::min(std::max(x[j], q.var_lo[j]), q.var_up[j]);
 

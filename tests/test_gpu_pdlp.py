@@ -217,3 +217,25 @@ def test_infeasibility_detection_matches_oracle(golden_dir):
         res, _, _, _ = O.solve(lp, tol=1e-6, iteration_limit=3000, detect_infeasibility=True)
         assert int(sol.get_termination_status()) == res["status"] == 2, name
         assert sol.get_lp_stats()["nb_iterations"] == res["iterations"], name
+
+
+def test_warm_start_matches_oracle(small_lp):
+    """An initial primal / dual solution gives the oracle's iterates, and a good one converges in
+    fewer iterations than the cold start."""
+    rng = np.random.default_rng(3)
+    x0 = small_lp.x_star + 1e-3 * rng.standard_normal(small_lp.n)
+    y0 = small_lp.y_star + 1e-3 * rng.standard_normal(small_lp.m)
+    dm = datamodel_from_lp(small_lp)
+    dm.set_initial_primal_solution(x0)
+    dm.set_initial_dual_solution(y0)
+    for k in (10, 200):
+        sol = lpm.Solve(dm, settings(tol=1e-12, iteration_limit=k))
+        res, x, y, _ = O.solve(small_lp, tol=1e-12, iteration_limit=k, initial_primal=x0,
+                               initial_dual=y0)
+        assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+        assert np.max(np.abs(sol.get_primal_solution() - x)) <= ITERATE_RTOL * (1 + np.abs(x).max())
+        assert np.max(np.abs(sol.get_dual_solution() - y)) <= ITERATE_RTOL * (1 + np.abs(y).max())
+    warm = lpm.Solve(dm, settings(tol=1e-6))
+    cold = lpm.Solve(datamodel_from_lp(small_lp), settings(tol=1e-6))
+    assert warm.get_termination_status() == cold.get_termination_status() == 1
+    assert warm.get_lp_stats()["nb_iterations"] < cold.get_lp_stats()["nb_iterations"]
