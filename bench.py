@@ -17,6 +17,9 @@ iterates, FP64 termination / restart / step ratio).  The same solve in plain FP6
   batch_c3  config 3: 512 seeded LPs of uneven sizes (m log-uniform in [200, 20000], n = 2.5 m,
             6-12 non-zeros per column) solved in FP64 to 1e-6 by one cuOptBatchSolve call, against
             a sample of the same LPs solved one by one with cuOptSolve.
+  adjoint_c4  config 4: 64 non-degenerate 5000 x 10000 LPs solved in one batched call with
+            crossover, L = sum w * x* back-propagated through the KKT adjoint, gradients checked
+            against the exact basis derivatives and central differences (h = 1e-6).
 
 `--impl reference` times that CPU implementation alone (rank 0) on the same workload and metric.
 """
@@ -399,6 +402,13 @@ def run_b200(args):
         from cuopt_b200.profile import run_batch
         batch = run_batch(argparse.Namespace(count=512, sequential=args.batch_sequential,
                                              repeats=2, tol=1e-6, time_limit=120.0))
+    # Config 4: 64 non-degenerate 5000 x 10000 LPs, batched forward (crossover) + KKT adjoint.
+    adjoint = None
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        from cuopt_b200.profile import run_adjoint
+        adjoint = run_adjoint(argparse.Namespace(count=64, tol=1e-6, fd_instances=1,
+                                                 fd_coords=args.adjoint_fd_coords,
+                                                 basis_checks=2))
 
     value = world * 1000.0 / ms_mixed
     line = {
@@ -414,7 +424,7 @@ def run_b200(args):
         "pdhg_iter_per_s": last_mixed["number_of_steps_taken"] / (last_mixed["loop_time"] or 1e-9),
         "setup_s": last_mixed["setup_time"], "loop_s": last_mixed["loop_time"],
         "objective_rel_error": obj_err_mixed, "kkt": kkt_mixed, "fp64": fp64,
-        "mixed_refined_to_1e-8": refine, "batch_c3": batch,
+        "mixed_refined_to_1e-8": refine, "batch_c3": batch, "adjoint_c4": adjoint,
         "roofline": roofline, "cpu_baseline": cpu,
         "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "LPs/s to 1e-6 rel. KKT",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
@@ -446,6 +456,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-refine", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-fd-coords", type=int, default=16,
+                    help="config-4 coordinates per kind checked by central differences")
     ap.add_argument("--batch-sequential", type=int, default=32,
                     help="config-3 instances also solved one by one (timing sample)")
     args = ap.parse_args()

@@ -30,8 +30,8 @@ namespace {
 constexpr int kVersionMajor = 26, kVersionMinor = 4, kVersionPatch = 0;
 
 // Copies n elements from a host or device pointer (the reference accepts both).
-template <typename T>
-void copy_in(std::vector<T>& dst, const T* src, size_t n)
+template <typename T, typename A>
+void copy_in(std::vector<T, A>& dst, const T* src, size_t n)
 {
   if (n == 0) {
     dst.clear();
@@ -50,8 +50,8 @@ void copy_in(std::vector<T>& dst, const T* src, size_t n)
   cuopt_b200::parallel_memcpy(dst.data(), src, n * sizeof(T));
 }
 
-template <typename T>
-void copy_out(T* dst, const std::vector<T>& src)
+template <typename T, typename A>
+void copy_out(T* dst, const std::vector<T, A>& src)
 {
   if (src.empty()) return;
   cudaPointerAttributes attr{};

@@ -570,6 +570,66 @@ static __global__ void power_check_kernel(power_state* ps, const double* s2, con
   if (ps->resid < tol) ps->done = 1;
 }
 
+// Golub-Kahan-Lanczos bidiagonalisation of the scaled A (the mixed-precision step size).  The
+// vectors are stored unnormalised; gk_state holds their norms: u has norm beta (beta_k), v has
+// norm alpha (alpha_{k-1}, or 0 before the first step).
+struct gk_state {
+  double beta;
+  double alpha;
+};
+
+// Row j of A^T applied to u:  p_j = (A^T u)_j / beta - beta v_j / alpha  (written over v_j).
+struct gk_primal_epi {
+  static constexpr int kRed = 1;
+  double* v;
+  const gk_state* st;
+  struct pre_t {
+    double v;
+  };
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ pre_t load(int j) const { return pre_t{v[j]}; }
+  __device__ __forceinline__ void operator()(int j, double acc, const pre_t& p, red_t<1>& r) const
+  {
+    const double b = st->beta, a = st->alpha;
+    const double pj = acc / b - (a > 0.0 ? b * (p.v / a) : 0.0);
+    v[j]            = pj;
+    r.v[0] += pj * pj;
+  }
+};
+
+// Row i of A applied to v:  q_i = (A v)_i / alpha - alpha u_i / beta  (written over u_i).
+struct gk_dual_epi {
+  static constexpr int kRed = 1;
+  double* u;
+  const gk_state* st;
+  struct pre_t {
+    double u;
+  };
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ pre_t load(int i) const { return pre_t{u[i]}; }
+  __device__ __forceinline__ void operator()(int i, double acc, const pre_t& p, red_t<1>& r) const
+  {
+    const double a = st->alpha, b = st->beta;
+    const double qi = acc / a - a * (p.u / b);
+    u[i]            = qi;
+    r.v[0] += qi * qi;
+  }
+};
+
+// Records a new norm: FIELD 0 sets alpha (history alphas[k]), FIELD 1 sets beta (betas[k + 1]).
+template <int FIELD>
+static __global__ void gk_record_kernel(gk_state* st, const double* sumsq, double* hist, int k)
+{
+  const double v = sqrt(*sumsq);
+  if (FIELD == 0) {
+    st->alpha = v;
+    hist[k]   = v;
+  } else {
+    st->beta    = v;
+    hist[k + 1] = v;
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Scaling (reference initial_scaling.cu:152-569).
 

@@ -26,8 +26,8 @@ constexpr double kInf = std::numeric_limits<double>::infinity();
 void lp_problem::constraint_bounds(std::vector<double>& lo, std::vector<double>& up) const
 {
   if (ranged) {
-    lo = con_lo;
-    up = con_up;
+    lo.assign(con_lo.begin(), con_lo.end());
+    up.assign(con_up.begin(), con_up.end());
     return;
   }
   lo.resize(m);

@@ -2,6 +2,8 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -11,18 +13,42 @@ namespace cuopt_b200 {
 
 // cuOptOptimizationProblem: the user's LP, copied at creation (reference optimization_problem_t,
 // cpp/include/cuopt/linear_programming/optimization_problem.hpp:160-319).
+// std::vector whose resize leaves new elements uninitialised: the problem arrays are always
+// overwritten right after they are sized, and zero-filling 10^8 elements first (single-threaded)
+// would cost as much as the copy itself.
+template <typename T>
+struct default_init_allocator : std::allocator<T> {
+  template <typename U>
+  struct rebind {
+    using other = default_init_allocator<U>;
+  };
+  using std::allocator<T>::allocator;
+  template <typename U>
+  void construct(U* p) noexcept
+  {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... Args>
+  void construct(U* p, Args&&... args)
+  {
+    ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+  }
+};
+template <typename T>
+using host_array = std::vector<T, default_init_allocator<T>>;
+
 struct lp_problem {
   int m = 0, n = 0;
   bool maximize     = false;
   double obj_offset = 0.0;
-  std::vector<double> c;
-  std::vector<int> row_off, col_idx;
-  std::vector<double> val;
+  host_array<double> c;
+  host_array<int> row_off, col_idx;
+  host_array<double> val;
   bool ranged = false;           // true: con_lo / con_up given; false: row_types + rhs
   std::vector<char> row_types;   // 'E' 'L' 'G'
-  std::vector<double> rhs;
-  std::vector<double> con_lo, con_up;
-  std::vector<double> var_lo, var_up;
+  host_array<double> rhs;
+  host_array<double> con_lo, con_up;
+  host_array<double> var_lo, var_up;
   std::vector<char> var_types;   // 'C' 'I'
   bool quadratic = false;
   std::vector<std::string> row_names, col_names;

@@ -232,15 +232,15 @@ int read_mps(const std::string& path, lp_problem& out, std::string& err)
   out.n          = n;
   out.maximize   = maximize;
   out.obj_offset = offset;
-  out.c          = cost;
-  out.var_lo     = lo;
-  out.var_up     = up;
+  out.c.assign(cost.begin(), cost.end());
+  out.var_lo.assign(lo.begin(), lo.end());
+  out.var_up.assign(up.begin(), up.end());
   out.var_types  = vtype;
   out.row_names  = row_names;
   out.col_names  = col_names;
   out.objective_name = obj_row;
   out.row_types  = row_types;
-  out.rhs        = rhs;
+  out.rhs.assign(rhs.begin(), rhs.end());
   out.ranged     = true;
   out.con_lo.resize(m);
   out.con_up.resize(m);

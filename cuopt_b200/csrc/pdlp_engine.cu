@@ -185,7 +185,10 @@ class engine {
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
     trace("engine: scaling");
     // Step size from the largest singular value of the scaled A (reference pdlp.cu:2620-2731).
-    power_iteration();
+    if (p_.precision == 1)
+      lanczos_step_size();
+    else
+      power_iteration();
     trace("engine: power iteration");
 
     xu_.resize(n);
@@ -408,6 +411,116 @@ class engine {
     cudaGraphExecDestroy(exec);
     power_iters_ = h.iters;
     eta_         = kStepScaling / std::sqrt(h.s2);
+  }
+
+  // Largest singular value of the scaled A by Golub-Kahan-Lanczos bidiagonalisation, used in
+  // mixed precision (where the iterates are not expected to match the FP64 reference path): the
+  // estimate sigma_max(B_k) of the bidiagonal B_k rises to sigma_max(A) within tens of matrix
+  // pairs, where the reference's power iteration (kept for FP64) takes hundreds.  Same start vector
+  // as the power iteration; stops when the estimate changes by less than 1e-10 relative.
+  void lanczos_step_size()
+  {
+    const int m = in_.m, n = in_.n;
+    std::vector<double> z0(m);
+    std::mt19937 gen(1);
+    std::normal_distribution<double> dist(0.0, 1.0);
+    for (int i = 0; i < m; ++i) z0[i] = dist(gen);
+    constexpr int kChunk = 16, kMaxSteps = 512;
+    dbuf<double> u(m), v(n), tmp(m), alphas(kMaxSteps + 1), betas(kMaxSteps + 2);
+    dbuf<gk_state> st(1);
+    tmp.upload(z0.data(), m, s_);
+    permute_gather(tmp.data(), L_.row_new2old.data(), m, 1.0, u.data(), s_);
+    v.zero(s_);
+    st.zero(s_);
+    double beta0 = 0.0;
+    {
+      vec_reduce_kernel<0, double><<<vgrid_, kBlock, 0, s_>>>(u.data(), nullptr, m,
+                                                              partials_.data(), nullptr);
+      finalize_sum_kernel<1><<<1, kBlock, 0, s_>>>(partials_.data(), vgrid_, dres_.data());
+      gk_record_kernel<1><<<1, 1, 0, s_>>>(st.data(), dres_.data(), betas.data(), -1);
+      launches_ += 3;
+      B200_LAUNCH_CHECK();
+      betas.download(&beta0, 1, s_);
+      B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    }
+    const auto As = view_of<TX>(L_.A, As_.data()), ATs = view_of<TX>(L_.AT, ATs_.data());
+    auto step = [&](int k) {
+      sell_map_kernel<TX, double, gk_primal_epi><<<sell_grid(ATs), kBlock, 0, s_>>>(
+        ATs, u.data(), gk_primal_epi{v.data(), st.data()}, partials_.data());
+      finalize_sum_kernel<1><<<1, kBlock, 0, s_>>>(partials_.data(), sell_grid(ATs),
+                                                   dres_.data());
+      gk_record_kernel<0><<<1, 1, 0, s_>>>(st.data(), dres_.data(), alphas.data(), k);
+      sell_map_kernel<TX, double, gk_dual_epi><<<sell_grid(As), kBlock, 0, s_>>>(
+        As, v.data(), gk_dual_epi{u.data(), st.data()}, partials_.data());
+      finalize_sum_kernel<1><<<1, kBlock, 0, s_>>>(partials_.data(), sell_grid(As),
+                                                   dres_.data() + 1);
+      gk_record_kernel<1><<<1, 1, 0, s_>>>(st.data(), dres_.data() + 1, betas.data(), k);
+    };
+    std::vector<double> ha(kMaxSteps + 1), hb(kMaxSteps + 2);
+    double sigma2 = 0.0, prev = -1.0;
+    int k = 0;
+    while (k < kMaxSteps) {
+      const int c = std::min(kChunk, kMaxSteps - k);
+      for (int i = 0; i < c; ++i) step(k + i);
+      launches_ += 6.0 * c;
+      B200_LAUNCH_CHECK();
+      k += c;
+      alphas.download(ha.data(), k, s_);
+      betas.download(hb.data(), k + 1, s_);
+      B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+      // betas[0] holds |z0| (written at index -1 + 1); the recurrence coefficients are betas[1..].
+      bool breakdown = false;
+      int used = k;
+      for (int j = 0; j < k; ++j)
+        if (!(ha[j] > 0.0) || !(hb[j + 1] > 0.0) || !std::isfinite(ha[j]) || !std::isfinite(hb[j + 1])) {
+          used      = j + 1;
+          breakdown = true;
+          break;
+        }
+      sigma2 = largest_bidiagonal_sigma2(ha.data(), hb.data() + 1, used);
+      if (breakdown || (prev > 0.0 && std::fabs(sigma2 - prev) <= 1e-10 * sigma2)) {
+        k = used;
+        break;
+      }
+      prev = sigma2;
+    }
+    (void)beta0;
+    power_iters_ = k;
+    eta_         = kStepScaling / std::sqrt(sigma2);
+  }
+
+  // sigma_max^2 of the (k+1) x k lower bidiagonal matrix with diagonal a[0..k-1] and subdiagonal
+  // b[0..k-1]: the largest eigenvalue of the tridiagonal B^T B, by Sturm-sequence bisection.
+  static double largest_bidiagonal_sigma2(const double* a, const double* b, int k)
+  {
+    if (k <= 0) return 0.0;
+    std::vector<double> d(k), e(std::max(k - 1, 0));
+    for (int j = 0; j < k; ++j) d[j] = a[j] * a[j] + b[j] * b[j];
+    for (int j = 0; j + 1 < k; ++j) e[j] = a[j + 1] * b[j];
+    double hi = 0.0;
+    for (int j = 0; j < k; ++j)
+      hi = std::max(hi, d[j] + (j > 0 ? std::fabs(e[j - 1]) : 0.0) + (j + 1 < k ? std::fabs(e[j]) : 0.0));
+    double lo = 0.0;
+    // count of eigenvalues below x (Sturm sequence of T - x I)
+    auto below = [&](double x) {
+      int cnt  = 0;
+      double q = d[0] - x;
+      if (q < 0) ++cnt;
+      for (int j = 1; j < k; ++j) {
+        const double prevq = q != 0.0 ? q : 1e-300;
+        q = d[j] - x - e[j - 1] * e[j - 1] / prevq;
+        if (q < 0) ++cnt;
+      }
+      return cnt;
+    };
+    for (int it = 0; it < 200 && hi - lo > 1e-15 * hi; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      if (below(mid) >= k)
+        hi = mid;
+      else
+        lo = mid;
+    }
+    return hi;
   }
 
   // ------------------------------------------------------------------ iteration kernels

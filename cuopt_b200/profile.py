@@ -52,6 +52,8 @@ def main() -> None:
                     help="adjoint mode: instances checked by finite differences")
     ap.add_argument("--fd-coords", type=int, default=32,
                     help="adjoint mode: coordinates per kind (c, b, A) and instance")
+    ap.add_argument("--basis-checks", type=int, default=4,
+                    help="adjoint mode: instances checked against exact basis derivatives")
     ap.add_argument("--count", type=int, default=512, help="batch mode: instances")
     ap.add_argument("--sequential", type=int, default=64,
                     help="batch mode: instances also solved one by one (timing sample)")
@@ -188,7 +190,6 @@ def run_adjoint(a) -> dict:
     import numpy as np
     import scipy.sparse as sp
     import torch
-    from scipy.sparse.linalg import splu
 
     from cuopt_b200 import generators as gen
     from cuopt_b200 import linear_programming as lpm
@@ -229,12 +230,14 @@ def run_adjoint(a) -> dict:
     torch.cuda.synchronize()
     backward_s = time.perf_counter() - t0
 
-    # Exact basis derivatives (an independent sparse LU of each basis).
+    # Exact basis derivatives (an independent dense LU of each basis on the host: these random
+    # sparse bases fill in almost completely, so a dense solve is the faster one).
     err = {"c": 0.0, "b": 0.0, "A": 0.0}
     rel = lambda g, e: float(np.abs(g - e).max() / max(1.0, np.abs(e).max()))
-    for lp, w, t in zip(lps, ws, insts):
+    nb = min(getattr(a, "basis_checks", 4), count)
+    for lp, w, t in zip(lps[:nb], ws[:nb], insts[:nb]):
         A = sp.csr_matrix((lp.val, lp.col_idx, lp.row_off), shape=(lp.m, lp.n))
-        lam = splu(A[:, lp.basic].tocsc()).solve(w[lp.basic], trans="T")
+        lam = np.linalg.solve(A[:, lp.basic].toarray().T, w[lp.basic])
         rows = np.repeat(np.arange(lp.m), np.diff(lp.row_off))
         dval = -lam[rows] * lp.x_star[lp.col_idx]
         err["c"] = max(err["c"], float(np.abs(t.c.grad.cpu().numpy()).max()))
@@ -274,7 +277,8 @@ def run_adjoint(a) -> dict:
         checked += 1
     return {"config": "c4", "count": count, "m": 5000, "n": 10000, "forward_s": forward_s,
             "backward_s": backward_s, "adjoint_ms_per_instance": backward_s * 1e3 / count,
-            "grad_vs_basis_max_rel_error": err, "fd_checked": checked, "fd_h": h,
+            "grad_vs_basis_max_rel_error": err, "basis_checked_instances": nb,
+            "fd_checked": checked, "fd_h": h,
             "fd_max_rel_error": fd_err}
 
 

@@ -239,3 +239,16 @@ def test_warm_start_matches_oracle(small_lp):
     cold = lpm.Solve(datamodel_from_lp(small_lp), settings(tol=1e-6))
     assert warm.get_termination_status() == cold.get_termination_status() == 1
     assert warm.get_lp_stats()["nb_iterations"] < cold.get_lp_stats()["nb_iterations"]
+
+
+@pytest.mark.parametrize("cfg", [(200, 500, 8, 11), (2000, 5000, 8, 0)])
+def test_mixed_step_size_from_lanczos_matches_power_iteration(cfg):
+    """Mixed precision takes sigma_max(A) from a Golub-Kahan-Lanczos bidiagonalisation; the step
+    size agrees with the FP64 power iteration's to 1e-5 relative (the power iteration stops at a
+    1e-4 residual, the FP32 matrix differs from the FP64 one in the 8th digit)."""
+    m, n, k, seed = cfg
+    dm = datamodel_from_lp(gen.constructed_lp(m, n, k, seed=seed))
+    a = lpm.Solve(dm, settings(tol=1e-12, iteration_limit=0, precision=1))
+    b = lpm.Solve(dm, settings(tol=1e-12, iteration_limit=0))
+    assert rel(a.stats["step_size"], b.stats["step_size"]) <= 1e-5
+    assert a.stats["power_iterations"] < b.stats["power_iterations"]
