@@ -100,8 +100,10 @@ cuopt_int_t cuOptProfilePDHGSweeps(cuopt_int_t num_constraints,
 /* Solve `count` independent LPs in one call.  The counterpart of the reference's
  * cuopt::cython::call_batch_solve (cpp/src/pdlp/utilities/cython_solve.cu:317-352, used by the
  * Python BatchSolve, python/cuopt/cuopt/linear_programming/solver/solver.py:109), which runs the
- * problems on up to four host threads.  Here all instances advance in one persistent device
- * launch with per-instance restart and termination.  solutions[i] receives the solution of
+ * problems on up to four host threads.  Here the instances form one block-diagonal LP: every PDHG
+ * sweep is one launch over all of them, each keeping its own scaling, step size, restarts and
+ * termination (and its single-solve iterates); finished instances drop out of the sweeps.
+ * solutions[i] receives the solution of
  * problems[i]; each must be released with cuOptDestroySolution.  Returns CUOPT_SUCCESS when every
  * instance ran (inspect each termination status), or the first error code. */
 cuopt_int_t cuOptBatchSolve(const cuOptOptimizationProblem* problems,
@@ -113,8 +115,11 @@ cuopt_int_t cuOptBatchSolve(const cuOptOptimizationProblem* problems,
  * Given dL/dx (size n) and optionally dL/dy (size m, may be NULL) at the solution returned by
  * cuOptSolve, computes dL/dc (n), dL/dlower and dL/dupper of the constraint bounds (m each) and
  * dL/dA for every stored non-zero of the constraint matrix (nnz, CSR order of the problem), by
- * implicit differentiation of the KKT conditions on the solution's active set.  Any output
- * pointer may be NULL.  Returns CUOPT_INVALID_ARGUMENT if the solution is not Optimal. */
+ * implicit differentiation of the KKT conditions on the solution's active set.  For a row whose
+ * bounds are equal, the gradient with respect to its right-hand side is in dl_dlower.  At a
+ * non-degenerate vertex these are the exact derivatives; otherwise those of the minimum-norm
+ * response.  Any output pointer may be NULL.  Returns CUOPT_INVALID_ARGUMENT if the solution is not
+ * Optimal (or the active set exceeds the dense limit). */
 cuopt_int_t cuOptSolutionAdjoint(cuOptOptimizationProblem problem,
                                  cuOptSolution solution,
                                  const cuopt_float_t* dl_dx,
