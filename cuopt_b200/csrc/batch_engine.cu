@@ -411,51 +411,96 @@ __device__ __forceinline__ double block_sum(const ksum& acc, double* sm)
   return v;
 }
 
-// q = z / |z| over the instance's rows.
-__global__ void __launch_bounds__(kBlock) b_power_normalize_kernel(const double* z, double* q,
-                                                                   const int4* ranges,
-                                                                   const int* pactive)
+// The power iteration's vector work is split into row chunks of at most kPowerChunk rows (each
+// inside one instance), so a large instance does not serialise a kernel on one block.  Chunk
+// partial sums are combined per instance in chunk order (deterministic).
+constexpr int kPowerChunk = 2048;
+
+// Thread 0's fixed-order sum of the partials of instance b's chunks, shared with the block.
+__device__ __forceinline__ double instance_total(const double* part, const int* chunk_off, int b,
+                                                 double* slot)
 {
-  const int b = blockIdx.x;
-  if (!pactive[b]) return;
-  const int4 r = ranges[b];
-  __shared__ double sm[kBlock];
-  ksum acc;
-  for (int i = r.x + threadIdx.x; i < r.y; i += kBlock) acc.add(z[i] * z[i]);
-  for (int i = r.z + threadIdx.x; i < r.w; i += kBlock) acc.add(z[i] * z[i]);
-  const double nq = sqrt(block_sum(acc, sm));
-  for (int i = r.x + threadIdx.x; i < r.y; i += kBlock) q[i] = z[i] / nq;
-  for (int i = r.z + threadIdx.x; i < r.w; i += kBlock) q[i] = z[i] / nq;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int c = chunk_off[b]; c < chunk_off[b + 1]; ++c) t += part[c];
+    *slot = t;
+  }
+  __syncthreads();
+  return *slot;
 }
 
-// s2 = q . z (rowbuf holds q_i z_i); q <- q (-s2) + z; residual |q|; convergence test.
-__global__ void __launch_bounds__(kBlock)
-  b_power_update_kernel(double* q, const double* z, const double* rowbuf, const int4* ranges,
-                        int* pactive, b_power_state* ps, double tol, int* remaining)
+// part[c] = sum of z^2 over chunk c.
+__global__ void __launch_bounds__(kBlock) b_chunk_sumsq_kernel(const int4* chunks, const int* pactive,
+                                                               const double* z, double* part)
 {
-  const int b = blockIdx.x;
-  if (!pactive[b]) return;
-  const int4 r = ranges[b];
+  const int4 ch = chunks[blockIdx.x];
+  if (!pactive[ch.x]) return;
   __shared__ double sm[kBlock];
-  ksum a1;
-  for (int i = r.x + threadIdx.x; i < r.y; i += kBlock) a1.add(rowbuf[i]);
-  for (int i = r.z + threadIdx.x; i < r.w; i += kBlock) a1.add(rowbuf[i]);
-  const double s2 = block_sum(a1, sm);
-  ksum a2;
-  for (int i = r.x + threadIdx.x; i < r.y; i += kBlock) {
+  ksum acc;
+  for (int i = ch.y + threadIdx.x; i < ch.z; i += kBlock) acc.add(z[i] * z[i]);
+  const double v = block_sum(acc, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+// q = z / |z| over chunk c (|z| of its instance).
+__global__ void __launch_bounds__(kBlock)
+  b_chunk_normalize_kernel(const int4* chunks, const int* chunk_off, const int* pactive,
+                           const double* part, const double* z, double* q)
+{
+  const int4 ch = chunks[blockIdx.x];
+  if (!pactive[ch.x]) return;
+  __shared__ double slot;
+  const double nq = sqrt(instance_total(part, chunk_off, ch.x, &slot));
+  for (int i = ch.y + threadIdx.x; i < ch.z; i += kBlock) q[i] = z[i] / nq;
+}
+
+// part[c] = sum of rowbuf (q_i z_i) over chunk c.
+__global__ void __launch_bounds__(kBlock) b_chunk_sum_kernel(const int4* chunks, const int* pactive,
+                                                             const double* v, double* part)
+{
+  const int4 ch = chunks[blockIdx.x];
+  if (!pactive[ch.x]) return;
+  __shared__ double sm[kBlock];
+  ksum acc;
+  for (int i = ch.y + threadIdx.x; i < ch.z; i += kBlock) acc.add(v[i]);
+  const double t = block_sum(acc, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// s2 = q . z of the instance;  q <- q (-s2) + z over chunk c;  part_r[c] = sum of the new q^2.
+__global__ void __launch_bounds__(kBlock)
+  b_chunk_residual_kernel(const int4* chunks, const int* chunk_off, const int* pactive,
+                          const double* part_s2, const double* z, double* q, double* part_r)
+{
+  const int4 ch = chunks[blockIdx.x];
+  if (!pactive[ch.x]) return;
+  __shared__ double slot;
+  __shared__ double sm[kBlock];
+  const double s2 = instance_total(part_s2, chunk_off, ch.x, &slot);
+  ksum acc;
+  for (int i = ch.y + threadIdx.x; i < ch.z; i += kBlock) {
     const double v = q[i] * -s2 + z[i];
     q[i]           = v;
-    a2.add(v * v);
+    acc.add(v * v);
   }
-  for (int i = r.z + threadIdx.x; i < r.w; i += kBlock) {
-    const double v = q[i] * -s2 + z[i];
-    q[i]           = v;
-    a2.add(v * v);
-  }
-  const double rsq = block_sum(a2, sm);
-  if (threadIdx.x == 0) {
+  const double t = block_sum(acc, sm);
+  if (threadIdx.x == 0) part_r[blockIdx.x] = t;
+}
+
+// Per instance: record sigma^2 and the residual, test convergence.
+__global__ void b_power_check_kernel(const int* chunk_off, int count, const double* part_s2,
+                                     const double* part_r, int* pactive, b_power_state* ps,
+                                     double tol, int* remaining)
+{
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < count; b += gridDim.x * blockDim.x) {
+    if (!pactive[b]) continue;
+    double s2 = 0.0, r = 0.0;
+    for (int c = chunk_off[b]; c < chunk_off[b + 1]; ++c) {
+      s2 += part_s2[c];
+      r += part_r[c];
+    }
     ps[b].s2    = s2;
-    ps[b].resid = sqrt(rsq);
+    ps[b].resid = sqrt(r);
     ps[b].iters += 1;
     if (ps[b].resid < tol) {
       pactive[b] = 0;
@@ -763,19 +808,46 @@ class batch_engine {
     remaining.upload(&B_, 1, s_);
     const inst_ctx rctx{rinst_.data(), pact.data(), nullptr};
     const inst_ctx cctx{cinst_.data(), pact.data(), nullptr};
+    // Row chunks of every instance for the vector work (see kPowerChunk).
+    std::vector<int4> chunks;
+    std::vector<int> chunk_off(B_ + 1, 0);
+    for (int b = 0; b < B_; ++b) {
+      chunk_off[b] = (int)chunks.size();
+      const int4 r = rranges_[b];
+      for (int lo = r.x; lo < r.y; lo += kPowerChunk)
+        chunks.push_back(int4{b, lo, std::min(lo + kPowerChunk, r.y), 0});
+      for (int lo = r.z; lo < r.w; lo += kPowerChunk)
+        chunks.push_back(int4{b, lo, std::min(lo + kPowerChunk, r.w), 0});
+    }
+    chunk_off[B_]     = (int)chunks.size();
+    const int nchunks = (int)chunks.size();
+    dbuf<int4> dchunks(std::max(nchunks, 1));
+    dbuf<int> dchunk_off(B_ + 1);
+    dbuf<double> part_z(std::max(nchunks, 1)), part_s2(std::max(nchunks, 1)),
+      part_r(std::max(nchunks, 1));
+    dchunks.upload(chunks.data(), nchunks, s_);
+    dchunk_off.upload(chunk_off.data(), B_ + 1, s_);
     auto one_iteration = [&]() {
       const auto As  = wview<TX>(true, As_.data());
       const auto ATs = wview<TX>(false, ATs_.data());
-      b_power_normalize_kernel<<<B_, kBlock, 0, s_>>>(dz.data(), dq.data(), rr_d_.data(),
-                                                      pact.data());
+      b_chunk_sumsq_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks.data(), pact.data(), dz.data(),
+                                                       part_z.data());
+      b_chunk_normalize_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks.data(), dchunk_off.data(),
+                                                           pact.data(), part_z.data(), dz.data(),
+                                                           dq.data());
       sell_map_kernel<TX, double, b_store_epi<double>><<<sell_grid(ATs), kBlock, 0, s_>>>(
         ATs, dq.data(), b_store_epi<double>{datq.data(), cctx}, partials_.data());
       sell_map_kernel<TX, double, b_power_z_epi><<<sell_grid(As), kBlock, 0, s_>>>(
         As, datq.data(), b_power_z_epi{dz.data(), dq.data(), rowbuf_.data(), rctx},
         partials_.data());
-      b_power_update_kernel<<<B_, kBlock, 0, s_>>>(dq.data(), dz.data(), rowbuf_.data(),
-                                                   rr_d_.data(), pact.data(), ps.data(),
-                                                   kPowerTol, remaining.data());
+      b_chunk_sum_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks.data(), pact.data(), rowbuf_.data(),
+                                                     part_s2.data());
+      b_chunk_residual_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks.data(), dchunk_off.data(),
+                                                          pact.data(), part_s2.data(), dz.data(),
+                                                          dq.data(), part_r.data());
+      b_power_check_kernel<<<ceil_div(B_, kBlock), kBlock, 0, s_>>>(
+        dchunk_off.data(), B_, part_s2.data(), part_r.data(), pact.data(), ps.data(), kPowerTol,
+        remaining.data());
     };
     // Chunks of 32 iterations are captured into a graph.  When the instances still iterating are
     // at most half of those the sweeps were last restricted to, the work lists shrink to them and
@@ -798,7 +870,7 @@ class batch_engine {
       } else {
         B200_CUDA_CHECK(cudaGraphLaunch(exec, s_));
       }
-      launches_ += 4.0 * std::min(32, kPowerMaxIters - done_iters);
+      launches_ += 7.0 * std::min(32, kPowerMaxIters - done_iters);
       remaining.download(&left, 1, s_);
       B200_CUDA_CHECK(cudaStreamSynchronize(s_));
       if (left == 0) break;

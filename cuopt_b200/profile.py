@@ -161,7 +161,7 @@ def run_batch(a) -> dict:
                for s, lp in zip(sols, lps)]
     out = {"config": "c3", "count": a.count, "m_total": int(sum(lp.m for lp in lps)),
            "n_total": int(sum(lp.n for lp in lps)), "nnz_total": int(sum(lp.nnz for lp in lps)),
-           "batch_s": batch_s, "batch_lps_per_s": a.count / batch_s,
+           "batch_s": batch_s, "batch_times_s": times, "batch_lps_per_s": a.count / batch_s,
            "optimal": status.count(1), "max_iterations": max(iters),
            "mean_iterations": float(np.mean(iters)), "max_objective_rel_error": max(obj_err),
            "batch_setup_s": sols[0].stats.get("setup_time"),
