@@ -4,12 +4,15 @@
 #include <cuopt/linear_programming/constants.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstdio>
+#include <exception>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <thread>
@@ -479,6 +482,9 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
   return out;
 }
 
+// Dense active-set factorisations (crossover, adjoint) run at most this many at a time.
+constexpr int kConcurrentPolish = 4;
+
 // One block-diagonal batch on the device (see pdlp_batch_solve_device).
 static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
                               const std::vector<size_t>& ids,
@@ -591,9 +597,30 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
     o.r.x.assign(hx.begin() + bi.col_start[b], hx.begin() + bi.col_start[b + 1]);
     o.r.rc.assign(hrc.begin() + bi.col_start[b], hrc.begin() + bi.col_start[b + 1]);
     o.r.y.assign(hy.begin() + bi.row_start[b], hy.begin() + bi.row_start[b + 1]);
-    if (crossover && o.r.status == CUOPT_TERIMINATION_STATUS_OPTIMAL)
-      o.r.crossover = vertex_polish(*ps[ids[b]], o.r);
   }
+  if (!crossover) return;
+  // Crossover of the Optimal instances on a few host threads: each polish runs its own stream and
+  // dense factorisation, so several overlap on the GPU.
+  std::atomic<int> next{0};
+  std::exception_ptr failure;
+  std::mutex failure_mu;
+  auto worker = [&]() {
+    for (int b; (b = next++) < bi.count;) {
+      lp_solution& o = out[ids[b]];
+      if (o.r.status != CUOPT_TERIMINATION_STATUS_OPTIMAL) continue;
+      try {
+        o.r.crossover = vertex_polish(*ps[ids[b]], o.r);
+      } catch (...) {
+        std::lock_guard<std::mutex> lock(failure_mu);
+        if (!failure) failure = std::current_exception();
+      }
+    }
+  };
+  const int nt = std::max(1, std::min(kConcurrentPolish, bi.count));
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t) pool.emplace_back(worker);
+  for (auto& th : pool) th.join();
+  if (failure) std::rethrow_exception(failure);
 }
 
 std::vector<lp_solution> solve_batch(const std::vector<const lp_problem*>& ps, const lp_settings& st)

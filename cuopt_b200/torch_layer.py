@@ -124,19 +124,35 @@ def _settings(settings: Optional[lpm.SolverSettings]) -> lpm.SolverSettings:
     return s
 
 
-class _Attach(torch.autograd.Function):
-    """Returns an already computed solution and routes its gradients through the KKT adjoint."""
+class _AttachBatch(torch.autograd.Function):
+    """Returns already computed solutions and routes their gradients through the KKT adjoint; the
+    adjoints of a batch run on a few host threads, so their factorisations overlap on the GPU."""
 
     @staticmethod
-    def forward(ctx, c, con_lo, con_up, values, solved: _Solved):
+    def forward(ctx, solved, *tensors):
         ctx.solved = solved
         ctx.set_materialize_grads(False)  # an unused output passes no gradient (NULL to the C API)
-        return solved.outputs()
+        out = []
+        for sv in solved:
+            out.extend(sv.outputs())
+        return tuple(out)
 
     @staticmethod
-    def backward(ctx, gx, gy):
-        dc, dlo, dup, dval = ctx.solved.adjoint(gx, gy)
-        return dc, dlo, dup, dval, None
+    def backward(ctx, *grads):
+        from concurrent.futures import ThreadPoolExecutor
+        pairs = [(grads[2 * i], grads[2 * i + 1]) for i in range(len(ctx.solved))]
+        jobs = [i for i, (gx, gy) in enumerate(pairs) if gx is not None or gy is not None]
+        results = [None] * len(ctx.solved)
+        with ThreadPoolExecutor(max_workers=min(_ADJOINT_THREADS, max(1, len(jobs)))) as ex:
+            for i, r in zip(jobs, ex.map(lambda i: ctx.solved[i].adjoint(*pairs[i]), jobs)):
+                results[i] = r
+        flat = [None]
+        for r in results:
+            flat.extend(r if r is not None else (None, None, None, None))
+        return tuple(flat)
+
+
+_ADJOINT_THREADS = 4
 
 
 def lp_solve(c, con_lo, con_up, values, row_offsets, column_indices, var_lo, var_up,
@@ -162,5 +178,6 @@ def lp_solve_batch(instances: Sequence[LPInstance],
             raise lpm.CuOptError(rc, "cuOptBatchSolve")
     finally:
         L.cuOptDestroySolverSettings(C.byref(s))
-    return [_Attach.apply(inst.c, inst.con_lo, inst.con_up, inst.values, sv)
-            for inst, sv in zip(instances, solved)]
+    tensors = [t for inst in instances for t in (inst.c, inst.con_lo, inst.con_up, inst.values)]
+    out = _AttachBatch.apply(solved, *tensors)
+    return [(out[2 * i], out[2 * i + 1]) for i in range(len(instances))]
