@@ -233,30 +233,47 @@ struct b_power_z_epi {
   }
 };
 
-// One block per instance: out[b K + q] = sum of plane q of rowbuf over the instance's two ranges
-// (long rows, sliced rows), in a fixed order (compensated per thread, then a fixed tree).
+// Rows of an instance are processed in chunks of at most kChunkRows (each inside one instance), so
+// a large instance does not serialise a kernel on one block.
+constexpr int kChunkRows = 2048;
+
+// Per-instance sums of row-buffer planes, for instances of any size: block c sums the K planes over its
+// chunk (instance chunks[c].x, rows [chunks[c].y, chunks[c].z)) into part[c K + q]; then one
+// thread per instance adds its chunks in chunk order.
 template <int K>
-__global__ void __launch_bounds__(kBlock) seg_reduce_kernel(const double* rowbuf, size_t stride,
-                                                            const int4* ranges, const int* want,
-                                                            double* out)
+__global__ void __launch_bounds__(kBlock) chunk_reduce_kernel(const double* rowbuf, size_t stride,
+                                                              const int4* chunks, const int* want,
+                                                              double* part)
 {
-  const int b = blockIdx.x;
-  if (want && !want[b]) return;
-  const int4 r = ranges[b];
+  const int4 ch = chunks[blockIdx.x];
+  if (want && !want[ch.x]) return;
   __shared__ double sm[kBlock];
   for (int q = 0; q < K; ++q) {
     const double* v = rowbuf + (size_t)q * stride;
     ksum acc;
-    for (int i = r.x + threadIdx.x; i < r.y; i += kBlock) acc.add(v[i]);
-    for (int i = r.z + threadIdx.x; i < r.w; i += kBlock) acc.add(v[i]);
+    for (int i = ch.y + threadIdx.x; i < ch.z; i += kBlock) acc.add(v[i]);
     sm[threadIdx.x] = acc.value();
     __syncthreads();
     for (int h = kBlock / 2; h > 0; h >>= 1) {
       if (threadIdx.x < h) sm[threadIdx.x] += sm[threadIdx.x + h];
       __syncthreads();
     }
-    if (threadIdx.x == 0) out[(size_t)b * K + q] = sm[0];
+    if (threadIdx.x == 0) part[(size_t)blockIdx.x * K + q] = sm[0];
     __syncthreads();
+  }
+}
+
+template <int K>
+__global__ void instance_reduce_kernel(const double* part, const int* chunk_off, int count,
+                                       const int* want, double* out)
+{
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < count; b += gridDim.x * blockDim.x) {
+    if (want && !want[b]) continue;
+    for (int q = 0; q < K; ++q) {
+      double t = 0.0;
+      for (int c = chunk_off[b]; c < chunk_off[b + 1]; ++c) t += part[(size_t)c * K + q];
+      out[(size_t)b * K + q] = t;
+    }
   }
 }
 
@@ -411,10 +428,8 @@ __device__ __forceinline__ double block_sum(const ksum& acc, double* sm)
   return v;
 }
 
-// The power iteration's vector work is split into row chunks of at most kPowerChunk rows (each
-// inside one instance), so a large instance does not serialise a kernel on one block.  Chunk
-// partial sums are combined per instance in chunk order (deterministic).
-constexpr int kPowerChunk = 2048;
+// The power iteration's vector work runs on the same row chunks; chunk partial sums are combined
+// per instance in chunk order (deterministic).
 
 // Thread 0's fixed-order sum of the partials of instance b's chunks, shared with the block.
 __device__ __forceinline__ double instance_total(const double* part, const int* chunk_off, int b,
@@ -588,6 +603,8 @@ class batch_engine {
     cr_d_.resize(B_);
     rr_d_.upload(rranges_.data(), B_, s_);
     cr_d_.upload(cranges_.data(), B_, s_);
+    build_chunks(rranges_, rows_);
+    build_chunks(cranges_, cols_);
 
     // Per-instance sign (maximisation) and objective scale / offset.
     std::vector<double> sgn(B_);
@@ -722,14 +739,48 @@ class batch_engine {
 
   // Per-instance sums of K planes of the row buffer over rows (ROWS) or columns; result in
   // segout_ + offset, optionally only for active instances.
+  // Row chunks of every instance (rows of A, or of A^T for the columns), see kChunkRows.
+  struct chunk_table {
+    dbuf<int4> chunks;
+    dbuf<int> offsets;
+    int count = 0;
+  };
+  void build_chunks(const std::vector<int4>& ranges, chunk_table& t)
+  {
+    std::vector<int4> chunks;
+    std::vector<int> off(B_ + 1, 0);
+    for (int b = 0; b < B_; ++b) {
+      off[b]       = (int)chunks.size();
+      const int4 r = ranges[b];
+      for (int lo = r.x; lo < r.y; lo += kChunkRows)
+        chunks.push_back(int4{b, lo, std::min(lo + kChunkRows, r.y), 0});
+      for (int lo = r.z; lo < r.w; lo += kChunkRows)
+        chunks.push_back(int4{b, lo, std::min(lo + kChunkRows, r.w), 0});
+    }
+    off[B_] = (int)chunks.size();
+    t.count = (int)chunks.size();
+    t.chunks.resize(std::max(t.count, 1));
+    t.offsets.resize(B_ + 1);
+    if (t.count > 0) t.chunks.upload(chunks.data(), t.count, s_);
+    t.offsets.upload(off.data(), B_ + 1, s_);
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+  }
+
+  // Per-instance sums of K planes of the row buffer over rows (ROWS) or columns; result in
+  // segout_ + offset, optionally only for active instances.
   template <int K>
   void seg_reduce(bool rows, size_t offset, bool only_active)
   {
-    seg_reduce_kernel<K><<<B_, kBlock, 0, s_>>>(rowbuf_.data(), stride_,
-                                               rows ? rr_d_.data() : cr_d_.data(),
-                                               only_active ? active_d_.data() : nullptr,
-                                               segout_.data() + offset);
-    ++launches_;
+    const chunk_table& t = rows ? rows_ : cols_;
+    const int* want      = only_active ? active_d_.data() : nullptr;
+    if (chunk_part_.size() < (size_t)std::max(rows_.count, cols_.count) * 3)
+      chunk_part_.resize((size_t)std::max({rows_.count, cols_.count, 1}) * 3);
+    if (t.count > 0)
+      chunk_reduce_kernel<K><<<t.count, kBlock, 0, s_>>>(rowbuf_.data(), stride_, t.chunks.data(),
+                                                         want, chunk_part_.data());
+    instance_reduce_kernel<K><<<ceil_div(B_, kBlock), kBlock, 0, s_>>>(
+      chunk_part_.data(), t.offsets.data(), B_, want, segout_.data() + offset);
+    launches_ += 2;
   }
   void fetch(size_t offset, size_t count, double* dst)
   {
@@ -808,31 +859,17 @@ class batch_engine {
     remaining.upload(&B_, 1, s_);
     const inst_ctx rctx{rinst_.data(), pact.data(), nullptr};
     const inst_ctx cctx{cinst_.data(), pact.data(), nullptr};
-    // Row chunks of every instance for the vector work (see kPowerChunk).
-    std::vector<int4> chunks;
-    std::vector<int> chunk_off(B_ + 1, 0);
-    for (int b = 0; b < B_; ++b) {
-      chunk_off[b] = (int)chunks.size();
-      const int4 r = rranges_[b];
-      for (int lo = r.x; lo < r.y; lo += kPowerChunk)
-        chunks.push_back(int4{b, lo, std::min(lo + kPowerChunk, r.y), 0});
-      for (int lo = r.z; lo < r.w; lo += kPowerChunk)
-        chunks.push_back(int4{b, lo, std::min(lo + kPowerChunk, r.w), 0});
-    }
-    chunk_off[B_]     = (int)chunks.size();
-    const int nchunks = (int)chunks.size();
-    dbuf<int4> dchunks(std::max(nchunks, 1));
-    dbuf<int> dchunk_off(B_ + 1);
+    const int nchunks = rows_.count;
     dbuf<double> part_z(std::max(nchunks, 1)), part_s2(std::max(nchunks, 1)),
       part_r(std::max(nchunks, 1));
-    dchunks.upload(chunks.data(), nchunks, s_);
-    dchunk_off.upload(chunk_off.data(), B_ + 1, s_);
+    const int4* dchunks_p   = rows_.chunks.data();
+    const int* dchunk_off_p = rows_.offsets.data();
     auto one_iteration = [&]() {
       const auto As  = wview<TX>(true, As_.data());
       const auto ATs = wview<TX>(false, ATs_.data());
-      b_chunk_sumsq_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks.data(), pact.data(), dz.data(),
+      b_chunk_sumsq_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks_p, pact.data(), dz.data(),
                                                        part_z.data());
-      b_chunk_normalize_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks.data(), dchunk_off.data(),
+      b_chunk_normalize_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks_p, dchunk_off_p,
                                                            pact.data(), part_z.data(), dz.data(),
                                                            dq.data());
       sell_map_kernel<TX, double, b_store_epi<double>><<<sell_grid(ATs), kBlock, 0, s_>>>(
@@ -840,13 +877,13 @@ class batch_engine {
       sell_map_kernel<TX, double, b_power_z_epi><<<sell_grid(As), kBlock, 0, s_>>>(
         As, datq.data(), b_power_z_epi{dz.data(), dq.data(), rowbuf_.data(), rctx},
         partials_.data());
-      b_chunk_sum_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks.data(), pact.data(), rowbuf_.data(),
+      b_chunk_sum_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks_p, pact.data(), rowbuf_.data(),
                                                      part_s2.data());
-      b_chunk_residual_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks.data(), dchunk_off.data(),
+      b_chunk_residual_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks_p, dchunk_off_p,
                                                           pact.data(), part_s2.data(), dz.data(),
                                                           dq.data(), part_r.data());
       b_power_check_kernel<<<ceil_div(B_, kBlock), kBlock, 0, s_>>>(
-        dchunk_off.data(), B_, part_s2.data(), part_r.data(), pact.data(), ps.data(), kPowerTol,
+        dchunk_off_p, B_, part_s2.data(), part_r.data(), pact.data(), ps.data(), kPowerTol,
         remaining.data());
     };
     // Chunks of 32 iterations are captured into a graph.  When the instances still iterating are
@@ -1324,6 +1361,8 @@ class batch_engine {
   std::map<int, cudaGraphExec_t> graphs_;
   work_list wa_, wt_;
   bool lists_on_ = false;
+  chunk_table rows_, cols_;
+  dbuf<double> chunk_part_;
 };
 
 

@@ -156,3 +156,21 @@ def test_adjoint_requires_an_optimal_solution(vlp):
     x, _ = lp_solve(**t, settings=s)
     with pytest.raises(lpm.CuOptError):
         x.sum().backward()
+
+
+def test_batched_backward_equals_single_backwards():
+    """lp_solve_batch back-propagates through one batched call (adjoints on host threads); the
+    gradients equal those of the instances solved and differentiated one at a time."""
+    from cuopt_b200.torch_layer import LPInstance, lp_solve, lp_solve_batch
+    lps = [gen.vertex_lp(150 + 50 * i, 300 + 100 * i, 6, seed=70 + i) for i in range(3)]
+    rng = np.random.default_rng(12)
+    ws = [rng.standard_normal(lp.n) for lp in lps]
+    batch_t = [_tensors(lp) for lp in lps]
+    outs = lp_solve_batch([LPInstance(**t) for t in batch_t], _settings())
+    sum((torch.tensor(w, device="cuda") * x).sum() for w, (x, _) in zip(ws, outs)).backward()
+    for lp, w, tb in zip(lps, ws, batch_t):
+        ts = _tensors(lp)
+        x, _ = lp_solve(**ts, settings=_settings())
+        (torch.tensor(w, device="cuda") * x).sum().backward()
+        for k in ("c", "con_lo", "con_up", "values"):
+            _close(tb[k].grad.cpu().numpy(), ts[k].grad.cpu().numpy(), 1e-9)
