@@ -120,6 +120,10 @@ SIGNATURES = {
     "cuOptBatchSolve": (cuopt_int_t, [C.POINTER(handle_t), cuopt_int_t, handle_t,
                                       C.POINTER(handle_t)]),
     "cuOptSolutionAdjoint": (cuopt_int_t, [handle_t, handle_t] + [C.c_void_p] * 6),
+    "cuOptSolveClimbers": (cuopt_int_t, [handle_t, handle_t, cuopt_int_t] + [C.c_void_p] * 3 +
+                           [C.POINTER(handle_t)]),
+    "cuOptBatchPDLPStrongBranching": (cuopt_int_t, [handle_t, handle_t, cuopt_int_t] +
+                                      [C.c_void_p] * 2 + [C.POINTER(handle_t)]),
     "cuOptComputeKKTErrorsNoAlloc": (cuopt_int_t, [cuopt_int_t, cuopt_int_t, cuopt_int_t,
                                                    cuopt_float_t] + [C.c_void_p] * 11),
 }

@@ -7,6 +7,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <limits>
@@ -673,6 +674,86 @@ cuopt_int_t cuOptBatchSolve(const cuOptOptimizationProblem* problems, cuopt_int_
     if (sol->error_code != CUOPT_SUCCESS && first_error == CUOPT_SUCCESS) first_error = sol->error_code;
   }
   return first_error;
+}
+
+namespace {
+cuopt_int_t climbers_to_solutions(std::vector<lp_solution>&& rs, cuOptSolution* solutions)
+{
+  cuopt_int_t first_error = CUOPT_SUCCESS;
+  for (size_t i = 0; i < rs.size(); ++i) {
+    auto* sol = new (std::nothrow) lp_solution(std::move(rs[i]));
+    if (!sol) {
+      for (size_t j = 0; j < i; ++j) cuOptDestroySolution(&solutions[j]);
+      return CUOPT_OUT_OF_MEMORY;
+    }
+    solutions[i] = sol;
+    if (sol->error_code != CUOPT_SUCCESS && first_error == CUOPT_SUCCESS)
+      first_error = sol->error_code;
+  }
+  return first_error;
+}
+}  // namespace
+
+cuopt_int_t cuOptSolveClimbers(cuOptOptimizationProblem problem, cuOptSolverSettings settings,
+                               cuopt_int_t count, const cuopt_int_t* variable_indices,
+                               const cuopt_float_t* lower_bounds,
+                               const cuopt_float_t* upper_bounds, cuOptSolution* solutions)
+{
+  if (!problem || !settings || !solutions || count <= 0 || !variable_indices || !lower_bounds ||
+      !upper_bounds)
+    return CUOPT_INVALID_ARGUMENT;
+  for (cuopt_int_t i = 0; i < count; ++i) solutions[i] = nullptr;
+  std::vector<int> var;
+  std::vector<double> lo, up;
+  try {
+    copy_in(var, variable_indices, count);
+    copy_in(lo, lower_bounds, count);
+    copy_in(up, upper_bounds, count);
+    return climbers_to_solutions(cuopt_b200::solve_climbers(*P(problem), *S(settings), var, lo, up),
+                                 solutions);
+  } catch (const std::bad_alloc&) {
+    return CUOPT_OUT_OF_MEMORY;
+  } catch (const std::exception&) {
+    return CUOPT_INVALID_ARGUMENT;
+  }
+}
+
+cuopt_int_t cuOptBatchPDLPStrongBranching(cuOptOptimizationProblem problem,
+                                          cuOptSolverSettings settings, cuopt_int_t count,
+                                          const cuopt_int_t* fractional,
+                                          const cuopt_float_t* root_solution,
+                                          cuOptSolution* solutions)
+{
+  if (!problem || !settings || !solutions || count <= 0 || !fractional || !root_solution)
+    return CUOPT_INVALID_ARGUMENT;
+  const lp_problem& p = *P(problem);
+  for (cuopt_int_t i = 0; i < 2 * count; ++i) solutions[i] = nullptr;
+  try {
+    std::vector<int> frac;
+    std::vector<double> root;
+    copy_in(frac, fractional, count);
+    copy_in(root, root_solution, count);
+    // Down branches (upper bound floor(x)) then up branches (lower bound ceil(x)), as
+    // batch_pdlp_solve builds them (reference solve.cu:884-919).
+    std::vector<int> var(2 * count);
+    std::vector<double> lo(2 * count), up(2 * count);
+    for (cuopt_int_t i = 0; i < count; ++i) {
+      const int j = frac[i];
+      if (j < 0 || j >= p.n) return CUOPT_INVALID_ARGUMENT;
+      var[i]         = j;
+      lo[i]          = p.var_lo[j];
+      up[i]          = std::floor(root[i]);
+      var[count + i] = j;
+      lo[count + i]  = std::ceil(root[i]);
+      up[count + i]  = p.var_up[j];
+    }
+    return climbers_to_solutions(cuopt_b200::solve_climbers(p, *S(settings), var, lo, up),
+                                 solutions);
+  } catch (const std::bad_alloc&) {
+    return CUOPT_OUT_OF_MEMORY;
+  } catch (const std::exception&) {
+    return CUOPT_INVALID_ARGUMENT;
+  }
 }
 
 cuopt_int_t cuOptSolutionAdjoint(cuOptOptimizationProblem problem, cuOptSolution solution,

@@ -664,4 +664,98 @@ std::vector<lp_solution> solve_batch(const std::vector<const lp_problem*>& ps, c
   return out;
 }
 
+std::vector<lp_solution> solve_climbers(const lp_problem& p, const lp_settings& st,
+                                        const std::vector<int>& var, const std::vector<double>& lo,
+                                        const std::vector<double>& up)
+{
+  const int count = (int)var.size();
+  std::vector<lp_solution> out(count);
+  for (int b = 0; b < count; ++b)
+    if (var[b] < 0 || var[b] >= p.n) {
+      for (auto& o : out) set_error(o, CUOPT_INVALID_ARGUMENT, "climber variable out of range");
+      return out;
+    }
+  auto modified = [&](int b) {
+    lp_problem q    = p;
+    q.var_lo[var[b]] = lo[b];
+    q.var_up[var[b]] = up[b];
+    return q;
+  };
+  std::vector<double> clo, cup;
+  lp_solution base;
+  bool reaches = false;
+  try {
+    reaches = prepare_for_pdlp(p, st, clo, cup, base);
+  } catch (const std::exception& e) {
+    set_error(base, CUOPT_RUNTIME_ERROR, e.what());
+  }
+  if (!reaches || base.error_code != CUOPT_SUCCESS) {
+    // The base LP does not go to PDLP (no constraints, validation error, ...): every climber is
+    // answered like a single solve of its LP.
+    for (int b = 0; b < count; ++b) out[b] = solve_problem(modified(b), st);
+    return out;
+  }
+  try {
+    const int m = p.m, n = p.n;
+    const int64_t nnz = p.row_off[m];
+    cudaStream_t s;
+    B200_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    struct stream_guard {
+      cudaStream_t s;
+      ~stream_guard() { cudaStreamDestroy(s); }
+    } guard{s};
+    alloc_scope scope(s);
+    configure_pool_once();
+    const size_t nz = (size_t)std::max<int64_t>(nnz, 1);
+    dbuf<int> doff(m + 1), didx(nz);
+    dbuf<double> dval(nz), dc(n), dlo(m), dup(m), dvl(n), dvu(n);
+    {
+      staged_upload h2d(s);
+      h2d.put(doff.data(), p.row_off.data(), m + 1);
+      h2d.put(didx.data(), p.col_idx.data(), nnz);
+      h2d.put(dval.data(), p.val.data(), nnz);
+      h2d.put(dc.data(), p.c.data(), n);
+      h2d.put(dlo.data(), clo.data(), m);
+      h2d.put(dup.data(), cup.data(), m);
+      h2d.put(dvl.data(), p.var_lo.data(), n);
+      h2d.put(dvu.data(), p.var_up.data(), n);
+      h2d.finish();
+    }
+    lp_device_input in;
+    in.m          = m;
+    in.n          = n;
+    in.row_off    = doff.data();
+    in.col_idx    = didx.data();
+    in.val        = dval.data();
+    in.c          = dc.data();
+    in.con_lo     = dlo.data();
+    in.con_up     = dup.data();
+    in.var_lo     = dvl.data();
+    in.var_up     = dvu.data();
+    in.obj_offset = p.obj_offset;
+    in.maximize   = p.maximize;
+    const pdlp_params prm = params_from_settings(st);
+    std::vector<double> hx((size_t)count * n), hy((size_t)count * m), hrc((size_t)count * n);
+    std::vector<pdlp_result> rs =
+      pdlp_climber_solve_device(in, prm, var, lo, up, s, hx.data(), hy.data(), hrc.data());
+    for (int b = 0; b < count; ++b) {
+      out[b].r = rs[b];
+      if (rs[b].status == CUOPT_TERIMINATION_STATUS_INFEASIBLE && rs[b].iterations == 0)
+        continue;  // crossing bounds: no solution vectors, as for a single solve
+      out[b].r.x.assign(hx.begin() + (size_t)b * n, hx.begin() + (size_t)(b + 1) * n);
+      out[b].r.rc.assign(hrc.begin() + (size_t)b * n, hrc.begin() + (size_t)(b + 1) * n);
+      out[b].r.y.assign(hy.begin() + (size_t)b * m, hy.begin() + (size_t)(b + 1) * m);
+      if (st.b(CUOPT_CROSSOVER) && out[b].r.status == CUOPT_TERIMINATION_STATUS_OPTIMAL)
+        out[b].r.crossover = vertex_polish(modified(b), out[b].r);
+    }
+  } catch (const std::bad_alloc&) {
+    for (auto& o : out) set_error(o, CUOPT_OUT_OF_MEMORY, "Memory allocation failed");
+  } catch (const std::invalid_argument& e) {
+    for (auto& o : out) set_error(o, CUOPT_VALIDATION_ERROR, e.what());
+  } catch (const std::exception& e) {
+    for (auto& o : out) set_error(o, CUOPT_RUNTIME_ERROR, e.what());
+  }
+  return out;
+}
+
 }  // namespace cuopt_b200

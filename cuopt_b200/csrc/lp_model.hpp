@@ -112,6 +112,12 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& s);
 std::vector<lp_solution> solve_batch(const std::vector<const lp_problem*>& ps, const lp_settings& s);
 
 // MPS input / output (reference cpp/libmps_parser).  read_mps returns 0 or CUOPT_MPS_* codes.
+// Climber batch (strong branching): the LP solved once per climber b with variable var[b] bounded
+// by [lo[b], up[b]]; all climbers share one matrix read per sweep (see climber_engine.cuh).
+std::vector<lp_solution> solve_climbers(const lp_problem& p, const lp_settings& s,
+                                        const std::vector<int>& var, const std::vector<double>& lo,
+                                        const std::vector<double>& up);
+
 // Reverse-mode sensitivities of an optimal solution (see adjoint.cu): gx (n) and optional gy (m)
 // in; any of dc (n), dlo / dup (m, constraint bounds) and dval (nnz, CSR order) out.
 void solution_adjoint(const lp_problem& p, const pdlp_result& sol, const double* gx,

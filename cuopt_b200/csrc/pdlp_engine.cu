@@ -55,10 +55,13 @@ struct loop_state {
   double dual_ray_obj = 0.0, max_dual_ray_inf = 0.0;
 };
 
+class climber_engine;
+
 template <typename TX>
 class engine {
   template <typename>
   friend class engine;
+  friend class climber_engine;
 
  public:
   engine(const lp_device_input& in, const pdlp_params& p, cudaStream_t s)
@@ -73,6 +76,14 @@ class engine {
   ~engine()
   {
     for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+  }
+
+  // Setup only (layout, scaling, step size): the base of a climber batch.
+  void prepare()
+  {
+    alloc_scope scope(s_);
+    t_start_ = now_s();
+    setup();
   }
 
   pdlp_result run(double* x_out, double* y_out, double* rc_out)
@@ -975,6 +986,8 @@ class engine {
   }
 };
 
+#include "climber_engine.cuh"
+
 }  // namespace
 
 pdlp_result pdlp_solve_device(const lp_device_input& in, const pdlp_params& p, cudaStream_t stream,
@@ -996,6 +1009,20 @@ pdlp_result pdlp_solve_device(const lp_device_input& in, const pdlp_params& p, c
   }
   engine<double> e(in, p, js.own);
   return e.run(x_out, y_out, rc_out);
+}
+
+std::vector<pdlp_result> pdlp_climber_solve_device(const lp_device_input& in, const pdlp_params& p,
+                                                   const std::vector<int>& var,
+                                                   const std::vector<double>& lo,
+                                                   const std::vector<double>& up,
+                                                   cudaStream_t stream, double* x_out,
+                                                   double* y_out, double* rc_out)
+{
+  joined_stream js(stream);
+  engine<double> base(in, p, js.own);
+  base.prepare();
+  climber_engine ce(base, p, var, lo, up);
+  return ce.run(x_out, y_out, rc_out);
 }
 
 sweep_profile pdlp_profile_sweeps(const lp_device_input& in, const pdlp_params& p,

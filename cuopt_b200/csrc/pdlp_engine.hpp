@@ -117,6 +117,16 @@ pdlp_result pdlp_solve_device(const lp_device_input& in, const pdlp_params& p, c
                               double* x_out, double* y_out, double* rc_out);
 
 // Times `iterations` plain iterations sweep by sweep (see cuOptProfilePDHGSweeps).
+// Climber batch (strong branching): the LP of `in` solved once per climber b with variable var[b]
+// (user order) bounded by [lo[b], up[b]] instead; FP64.  x_out (B x n), y_out (B x m) and rc_out
+// (B x n) are host arrays, climber-major, user order.
+std::vector<pdlp_result> pdlp_climber_solve_device(const lp_device_input& in, const pdlp_params& p,
+                                                   const std::vector<int>& var,
+                                                   const std::vector<double>& lo,
+                                                   const std::vector<double>& up,
+                                                   cudaStream_t stream, double* x_out,
+                                                   double* y_out, double* rc_out);
+
 sweep_profile pdlp_profile_sweeps(const lp_device_input& in, const pdlp_params& p,
                                   cudaStream_t stream, int iterations);
 

@@ -449,3 +449,55 @@ def ReadMps(path: str) -> DataModel:
         return dm
     finally:
         L.cuOptDestroyProblem(C.byref(h))
+
+
+def _solve_climbers(call, data_model, count, arrays, solver_settings):
+    import time
+
+    L = lib()
+    settings = solver_settings or SolverSettings()
+    prob = data_model._create()
+    s = settings._create()
+    sols = (handle_t * count)()
+    keep = [np.ascontiguousarray(a) for a in arrays]
+    try:
+        t0 = time.perf_counter()
+        call(L, prob, s, sols, [C.c_void_p(a.ctypes.data) for a in keep])
+        elapsed = time.perf_counter() - t0
+        out = [_read_solution(handle_t(sols[i]), data_model.n_constraints, data_model.n_variables)
+               if sols[i] else None for i in range(count)]
+        return out, elapsed
+    finally:
+        for i in range(count):
+            h = handle_t(sols[i])
+            if h:
+                L.cuOptDestroySolution(C.byref(h))
+        L.cuOptDestroyProblem(C.byref(prob))
+        L.cuOptDestroySolverSettings(C.byref(s))
+
+
+def SolveClimbers(data_model, variable_indices, lower_bounds, upper_bounds,
+                  solver_settings: SolverSettings | None = None):
+    """Solves copies of one LP that differ only in one variable's bounds each (the reference's
+    new_bounds batch, solve.cu:740-882): copy i bounds variable_indices[i] by
+    [lower_bounds[i], upper_bounds[i]].  Returns (solutions, time)."""
+    idx = np.asarray(variable_indices, dtype=np.int32)
+    lo = np.asarray(lower_bounds, dtype=np.float64)
+    up = np.asarray(upper_bounds, dtype=np.float64)
+    n = len(idx)
+    return _solve_climbers(
+        lambda L, p, s, sols, a: L.cuOptSolveClimbers(p, s, n, a[0], a[1], a[2], sols),
+        data_model, n, [idx, lo, up], solver_settings)
+
+
+def BatchPDLPStrongBranching(data_model, fractional, root_solution,
+                             solver_settings: SolverSettings | None = None):
+    """Strong branching (the reference's batch_pdlp_solve, solve.cu:884-919): the down branches
+    (x_j <= floor(root_j)) of every fractional variable, then the up branches (x_j >= ceil(root_j)).
+    Returns (solutions, time) with 2 * len(fractional) solutions."""
+    frac = np.asarray(fractional, dtype=np.int32)
+    root = np.asarray(root_solution, dtype=np.float64)
+    n = len(frac)
+    return _solve_climbers(
+        lambda L, p, s, sols, a: L.cuOptBatchPDLPStrongBranching(p, s, n, a[0], a[1], sols),
+        data_model, 2 * n, [frac, root], solver_settings)

@@ -111,6 +111,32 @@ cuopt_int_t cuOptBatchSolve(const cuOptOptimizationProblem* problems,
                             cuOptSolverSettings settings,
                             cuOptSolution* solutions);
 
+/* Climber batch (strong branching): solves `count` copies of `problem` that differ only in the
+ * bounds of one variable each: copy i has variable variable_indices[i] bounded by
+ * [lower_bounds[i], upper_bounds[i]].  Counterpart of the reference's pdlp_solver_settings_t::
+ * new_bounds with solve_lp in batch mode (cpp/src/pdlp/solve.cu:740-882).  All copies share one
+ * read of the matrix per PDHG sweep; each follows the iterates of a single solve of its LP (FP64).
+ * solutions[i] receives copy i's solution (release with cuOptDestroySolution).  Returns
+ * CUOPT_SUCCESS or the first error code. */
+cuopt_int_t cuOptSolveClimbers(cuOptOptimizationProblem problem,
+                               cuOptSolverSettings settings,
+                               cuopt_int_t count,
+                               const cuopt_int_t* variable_indices,
+                               const cuopt_float_t* lower_bounds,
+                               const cuopt_float_t* upper_bounds,
+                               cuOptSolution* solutions);
+
+/* Strong branching on `count` fractional variables (counterpart of the reference's
+ * batch_pdlp_solve, cpp/src/pdlp/solve.cu:884-919): solutions[0 .. count) are the down branches
+ * (fractional[i] bounded above by floor(root_solution[i])), solutions[count .. 2 count) the up
+ * branches (bounded below by ceil(root_solution[i])); `solutions` holds 2 * count handles. */
+cuopt_int_t cuOptBatchPDLPStrongBranching(cuOptOptimizationProblem problem,
+                                          cuOptSolverSettings settings,
+                                          cuopt_int_t count,
+                                          const cuopt_int_t* fractional,
+                                          const cuopt_float_t* root_solution,
+                                          cuOptSolution* solutions);
+
 /* Reverse-mode sensitivity of an optimal LP solution (no counterpart in the reference).
  * Given dL/dx (size n) and optionally dL/dy (size m, may be NULL) at the solution returned by
  * cuOptSolve, computes dL/dc (n), dL/dlower and dL/dupper of the constraint bounds (m each) and

@@ -1,0 +1,115 @@
+"""GPU tests of the climber batch (cuOptSolveClimbers / cuOptBatchPDLPStrongBranching): copies of
+one LP that differ in one variable's bounds each, swept together through one matrix read.
+
+Reference for every expectation: the CPU oracle solving each modified LP alone, and the reference's
+own batch test (pdlp_test.cu:1450-1535: identical climbers on afiro give bitwise identical
+results, all Optimal at afiro's objective).  Tolerances: iterates after the same number of
+iterations agree with the oracle to 1e-9 relative to the vector's magnitude.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from cuopt_b200 import generators as gen
+from cuopt_b200 import linear_programming as lpm
+from oracle import oracle as O
+from tests.helpers import datamodel_from_lp, oracle_view, rel, settings
+
+pytestmark = pytest.mark.gpu
+
+ITERATE_RTOL = 1e-9
+
+
+def _climbers(lp, count, seed):
+    rng = np.random.default_rng(seed)
+    var = rng.choice(lp.n, count, replace=False)
+    lo = lp.var_lo[var].copy()
+    up = np.minimum(lp.var_up[var], rng.uniform(0.5, 3.0, count))  # tighter upper bounds
+    return var, lo, up
+
+
+def _modified(lp, j, lo, up):
+    from dataclasses import replace
+    q = replace(lp, var_lo=lp.var_lo.copy(), var_up=lp.var_up.copy())
+    q.var_lo[j], q.var_up[j] = lo, up
+    return q
+
+
+@pytest.fixture(scope="module")
+def base_lp():
+    return gen.constructed_lp(200, 500, 8, seed=11)
+
+
+@pytest.mark.parametrize("k", [10, 200, 600])
+def test_climber_iterates_match_single_oracle(base_lp, k):
+    """11 climbers (two groups of eight, one partly filled) follow the oracle's solves of their
+    modified LPs."""
+    var, lo, up = _climbers(base_lp, 11, seed=3)
+    sols, _ = lpm.SolveClimbers(datamodel_from_lp(base_lp), var, lo, up,
+                                settings(tol=1e-12, iteration_limit=k))
+    for b, sol in enumerate(sols):
+        res, x, y, rc = O.solve(_modified(base_lp, var[b], lo[b], up[b]), tol=1e-12,
+                                iteration_limit=k)
+        assert sol.get_termination_status() == lpm.LPTerminationStatus.IterationLimit
+        assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+        assert np.max(np.abs(sol.get_primal_solution() - x)) <= ITERATE_RTOL * (1 + np.abs(x).max())
+        assert np.max(np.abs(sol.get_dual_solution() - y)) <= ITERATE_RTOL * (1 + np.abs(y).max())
+        assert np.max(np.abs(sol.get_reduced_cost() - rc)) <= ITERATE_RTOL * (1 + np.abs(rc).max())
+
+
+def test_climbers_solve_to_tolerance_like_single_solves(base_lp):
+    var, lo, up = _climbers(base_lp, 6, seed=4)
+    sols, _ = lpm.SolveClimbers(datamodel_from_lp(base_lp), var, lo, up, settings(tol=1e-6))
+    for b, sol in enumerate(sols):
+        res, _, _, _ = O.solve(_modified(base_lp, var[b], lo[b], up[b]), tol=1e-6)
+        assert int(sol.get_termination_status()) == res["status"] == 1
+        assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+        assert rel(sol.get_primal_objective(), res["primal_obj"]) <= 1e-8
+
+
+def test_identical_afiro_climbers_are_bitwise_identical(golden, golden_dir):
+    """pdlp_test.cu:1450-1535 (big_batch_afiro, here 24 climbers): every climber keeps variable 0's
+    own bounds; all are Optimal at afiro's objective with bitwise identical results."""
+    dm = lpm.ReadMps(golden_dir / "afiro_original.mps")
+    v = oracle_view(dm)
+    count = 24
+    sols, _ = lpm.SolveClimbers(dm, np.zeros(count, np.int32), np.full(count, v.var_lo[0]),
+                                np.full(count, v.var_up[0]), settings(tol=1e-4))
+    g = golden["afiro_objective"]
+    ref = sols[0]
+    assert ref.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert rel(ref.get_primal_objective(), g["value"]) <= g["rel_tol"]
+    for sol in sols[1:]:
+        assert sol.get_termination_status() == ref.get_termination_status()
+        assert sol.get_primal_objective() == ref.get_primal_objective()
+        assert sol.get_dual_objective() == ref.get_dual_objective()
+        assert sol.get_lp_stats()["nb_iterations"] == ref.get_lp_stats()["nb_iterations"]
+        assert np.array_equal(sol.get_primal_solution(), ref.get_primal_solution())
+        assert np.array_equal(sol.get_dual_solution(), ref.get_dual_solution())
+    single = lpm.Solve(dm, settings(tol=1e-4))
+    assert single.get_lp_stats()["nb_iterations"] == ref.get_lp_stats()["nb_iterations"]
+
+
+def test_strong_branching_builds_down_then_up_branches(base_lp):
+    """batch_pdlp_solve's climbers: x_j <= floor(root_j) for every fractional j, then
+    x_j >= ceil(root_j); each matches the oracle's solve of that branch."""
+    rng = np.random.default_rng(5)
+    frac = rng.choice(base_lp.n, 3, replace=False)
+    root = base_lp.x_star[frac] + 0.5
+    sols, _ = lpm.BatchPDLPStrongBranching(datamodel_from_lp(base_lp), frac, root,
+                                           settings(tol=1e-12, iteration_limit=200))
+    assert len(sols) == 6
+    for i, j in enumerate(frac):
+        for sol, (lo, up) in ((sols[i], (base_lp.var_lo[j], np.floor(root[i]))),
+                              (sols[3 + i], (np.ceil(root[i]), base_lp.var_up[j]))):
+            res, x, _, _ = O.solve(_modified(base_lp, j, lo, up), tol=1e-12, iteration_limit=200)
+            assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+            assert np.max(np.abs(sol.get_primal_solution() - x)) <= ITERATE_RTOL * (1 + np.abs(x).max())
+
+
+def test_crossing_climber_is_infeasible(base_lp):
+    sols, _ = lpm.SolveClimbers(datamodel_from_lp(base_lp), [0, 1], [5.0, base_lp.var_lo[1]],
+                                [1.0, base_lp.var_up[1]], settings(tol=1e-6))
+    assert sols[0].get_termination_status() == lpm.LPTerminationStatus.PrimalInfeasible
+    assert sols[1].get_termination_status() == lpm.LPTerminationStatus.Optimal
