@@ -29,14 +29,23 @@ __device__ __forceinline__ void gather_group(const double* __restrict__ p, doubl
   }
 }
 
-// acc[b] = sum_k A[r,k] g[idx[r,k] * ld + g0 + b] for the kGroup climbers of group g0, then
-// epi(r, acc, pre, red).
+// acc[b] = sum_k A[r,k] g[idx[r,k] * ld + g0 + b] for the kGroup climbers of a group, then
+// epi(r, acc, pre, red).  One launch covers the n_groups groups listed in `groups`: block
+// q * n_groups + i sweeps matrix block q for group groups[i] (its g0 replaces the epilogue's), so
+// the blocks that read one stretch of the matrix run side by side and share it through L2.  The
+// block sums of group g go to partials + g * pstride.
 template <class Epi>
 __global__ void __launch_bounds__(kBlock) mm_sweep_kernel(const dev_sell<double> A,
                                                           const double* __restrict__ g, int ld,
-                                                          int g0, Epi epi, double* partials)
+                                                          const int* __restrict__ groups,
+                                                          int n_groups, Epi epi, double* partials,
+                                                          size_t pstride)
 {
   constexpr int K = Epi::kRed;
+  const int grp = groups[blockIdx.x % n_groups];
+  const int xb  = (int)(blockIdx.x / n_groups);
+  const int g0  = grp * kGroup;
+  epi.ctx.g0    = g0;
   red_t<K> red;
 #pragma unroll
   for (int q = 0; q < (K > 0 ? K : 1); ++q) red.v[q] = 0.0;
@@ -45,8 +54,8 @@ __global__ void __launch_bounds__(kBlock) mm_sweep_kernel(const dev_sell<double>
   double acc[kGroup];
 #pragma unroll
   for (int b = 0; b < kGroup; ++b) acc[b] = 0.0;
-  if ((int)blockIdx.x < lb) {
-    const int row = blockIdx.x * kWarpsPerBlock + warp;
+  if (xb < lb) {
+    const int row = xb * kWarpsPerBlock + warp;
     if (row < A.n_long) {
       const auto pre = epi.load(row);
       for (int64_t k = A.long_off[row] + lane; k < A.long_off[row + 1]; k += kWarp) {
@@ -61,7 +70,7 @@ __global__ void __launch_bounds__(kBlock) mm_sweep_kernel(const dev_sell<double>
       if (lane == 0) epi(row, acc, pre, red);
     }
   } else {
-    const int s = (blockIdx.x - lb) * kWarpsPerBlock + warp;
+    const int s = (xb - lb) * kWarpsPerBlock + warp;
     if (s < A.n_slices) {
       const int row      = A.n_long + s * kWarp + lane;
       const bool valid   = row < A.rows;
@@ -88,7 +97,17 @@ __global__ void __launch_bounds__(kBlock) mm_sweep_kernel(const dev_sell<double>
       if (valid) epi(row, acc, pre, red);
     }
   }
-  block_reduce_store<K>(red, partials);
+  block_reduce_store<K>(red, partials + (size_t)grp * pstride, xb);
+}
+
+// out[g * stride + q] = the ordered sum of group g's block sums, one block per listed group.
+template <int K>
+__global__ void __launch_bounds__(kBlock) mm_finalize_kernel(const double* partials, size_t pstride,
+                                                             int nblocks, const int* groups,
+                                                             double* out, int stride)
+{
+  const int grp = groups[blockIdx.x];
+  ordered_block_sum<K>(partials + (size_t)grp * pstride, nblocks, out + (size_t)grp * stride);
 }
 
 // Per-climber state shared by the climber epilogues.
@@ -335,22 +354,27 @@ __global__ void mm_advance_kernel(pdlp_scalars* sc, const int* active, int count
     if (active[b]) sc[b].t0 += steps;
 }
 
-// Per-block partial sums of (a - b)^2 for the kGroup climbers of group g0 over `rows` rows.
+// Per-block partial sums of (a - b)^2 over `rows` rows for the kGroup climbers of every listed
+// group (blocks laid out as in mm_sweep_kernel).
 __global__ void __launch_bounds__(kBlock) mm_sqdiff_kernel(const double* a, const double* b,
-                                                           int rows, int ld, int g0,
-                                                           double* partials)
+                                                           int rows, int ld, const int* groups,
+                                                           int n_groups, double* partials,
+                                                           size_t pstride)
 {
+  const int grp = groups[blockIdx.x % n_groups];
+  const int xb = (int)(blockIdx.x / n_groups), nxb = (int)(gridDim.x / n_groups);
+  const int g0 = grp * kGroup;
   red_t<kGroup> r;
 #pragma unroll
   for (int q = 0; q < kGroup; ++q) r.v[q] = 0.0;
-  for (int i = blockIdx.x * kBlock + threadIdx.x; i < rows; i += gridDim.x * kBlock) {
+  for (int i = xb * kBlock + threadIdx.x; i < rows; i += nxb * kBlock) {
     double va[kGroup], vb[kGroup];
     gather_group(a + (size_t)i * ld + g0, va);
     gather_group(b + (size_t)i * ld + g0, vb);
 #pragma unroll
     for (int q = 0; q < kGroup; ++q) r.v[q] += (va[q] - vb[q]) * (va[q] - vb[q]);
   }
-  block_reduce_store<kGroup>(r, partials);
+  block_reduce_store<kGroup>(r, partials + (size_t)grp * pstride, xb);
 }
 
 // x = clamp(0, l, u) with the climbers' overrides (project_initial_primal).
@@ -376,7 +400,7 @@ class climber_engine {
   {
     ld_     = std::max(kGroup, (B_ + kGroup - 1) / kGroup * kGroup);
     groups_ = ld_ / kGroup;
-    B200_CUDA_CHECK(cudaMallocHost(&hbuf_, sizeof(double) * 4 * (size_t)ld_ + 64));
+    B200_CUDA_CHECK(cudaMallocHost(&hbuf_, sizeof(double) * 6 * (size_t)ld_ + 64));
     var_ = var;
     lo_  = lo;
     up_  = up;
@@ -434,6 +458,8 @@ class climber_engine {
     for (int b : crossing_) active_h_[b] = 0;  // crossing bounds: Infeasible without iterating
     active_d_.resize(ld_);
     active_d_.upload(active_h_.data(), ld_, s_);
+    groups_d_.resize(groups_);
+    refresh_groups();
     for (auto* v : {&x_, &xhat_, &slack_, &xbar_, &xa_, &aty_, &xu_, &su_}) {
       v->resize(nx);
       v->zero(s_);
@@ -451,7 +477,8 @@ class climber_engine {
     restarts_.assign(ld_, 0);
     const int g =
       std::max({sell_grid(view64(e_.L_.A)), sell_grid(view64(e_.L_.AT)), e_.vgrid_});
-    partials_.resize((size_t)g * 3 * kGroup);
+    pstride_ = (size_t)g * 3 * kGroup;
+    partials_.resize(pstride_ * groups_);
     dres_.resize((size_t)6 * ld_);
     B200_LAUNCH_CHECK();
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
@@ -463,31 +490,43 @@ class climber_engine {
       if (active_h_[b]) return true;
     return false;
   }
-  mm_ctx ctx(int g) const { return mm_ctx{ld_, g * kGroup, sc_d_.data(), active_d_.data()}; }
-
-  template <bool MAJOR, bool HALPERN, bool SAVE_ATY>
-  void launch_primal(int g, int it_off)
+  // The list of groups with an active climber, on the device for the sweeps (captured graphs see
+  // it by address: they are dropped whenever it changes).
+  void refresh_groups()
   {
-    const auto A = view_of<double>(e_.L_.AT, e_.ATs_.data());
-    mm_primal_epi<MAJOR, HALPERN, SAVE_ATY> ep{x_.data(),     xa_.data(),    e_.cs_.data(),
-                                               e_.ls_.data(), e_.us_.data(), xbar_.data(),
-                                               x_.data(),     xhat_.data(),  slack_.data(),
-                                               aty_.data(),   ovr_.data(),   ctx(g),
-                                               it_off};
-    mm_sweep_kernel<<<sell_grid(A), kBlock, 0, s_>>>(A, y_.data(), ld_, g * kGroup, ep,
-                                                     partials_.data());
+    groups_h_.clear();
+    for (int g = 0; g < groups_; ++g)
+      if (group_active(g)) groups_h_.push_back(g);
+    if (!groups_h_.empty()) groups_d_.upload(groups_h_.data(), groups_h_.size(), s_);
+  }
+  int n_act() const { return (int)groups_h_.size(); }
+  // g0 is set per block by the kernels.
+  mm_ctx ctx() const { return mm_ctx{ld_, 0, sc_d_.data(), active_d_.data()}; }
+  template <class Epi>
+  void sweep(const dev_sell<double>& A, const double* g, const Epi& ep)
+  {
+    if (n_act() == 0) return;
+    mm_sweep_kernel<<<sell_grid(A) * n_act(), kBlock, 0, s_>>>(
+      A, g, ld_, groups_d_.data(), n_act(), ep, partials_.data(), pstride_);
     ++launches_;
   }
+
+  template <bool MAJOR, bool HALPERN, bool SAVE_ATY>
+  void launch_primal(int it_off)
+  {
+    const auto A = view_of<double>(e_.L_.AT, e_.ATs_.data());
+    sweep(A, y_.data(),
+          mm_primal_epi<MAJOR, HALPERN, SAVE_ATY>{
+            x_.data(), xa_.data(), e_.cs_.data(), e_.ls_.data(), e_.us_.data(), xbar_.data(),
+            x_.data(), xhat_.data(), slack_.data(), aty_.data(), ovr_.data(), ctx(), it_off});
+  }
   template <bool MAJOR, bool HALPERN, bool FPE>
-  void launch_dual(int g, int it_off)
+  void launch_dual(int it_off)
   {
     const auto A = view_of<double>(e_.L_.A, e_.As_.data());
-    mm_dual_epi<MAJOR, HALPERN, FPE> ed{y_.data(),    ya_.data(),    e_.lcs_.data(),
-                                        e_.ucs_.data(), ybar_.data(), y_.data(),
-                                        yhat_.data(), ctx(g),        it_off};
-    mm_sweep_kernel<<<sell_grid(A), kBlock, 0, s_>>>(A, xbar_.data(), ld_, g * kGroup, ed,
-                                                     partials_.data());
-    ++launches_;
+    sweep(A, xbar_.data(),
+          mm_dual_epi<MAJOR, HALPERN, FPE>{y_.data(), ya_.data(), e_.lcs_.data(), e_.ucs_.data(),
+                                           ybar_.data(), y_.data(), yhat_.data(), ctx(), it_off});
   }
   void advance(int steps)
   {
@@ -498,10 +537,8 @@ class climber_engine {
   void plain_iterations(int L)
   {
     for (int i = 0; i < L; ++i) {
-      for (int g = 0; g < groups_; ++g)
-        if (group_active(g)) launch_primal<false, true, false>(g, i);
-      for (int g = 0; g < groups_; ++g)
-        if (group_active(g)) launch_dual<false, true, false>(g, i);
+      launch_primal<false, true, false>(i);
+      launch_dual<false, true, false>(i);
     }
     advance(L);
   }
@@ -523,9 +560,7 @@ class climber_engine {
           it = graphs_.emplace(L, ex).first;
         }
         B200_CUDA_CHECK(cudaGraphLaunch(it->second, s_));
-        int active_groups = 0;
-        for (int g = 0; g < groups_; ++g) active_groups += group_active(g);
-        launches_ += 2.0 * L * active_groups + 1.0;
+        launches_ += 2.0 * L + 1.0;
         R -= L;
       }
     }
@@ -546,12 +581,24 @@ class climber_engine {
     active_d_.upload(active_h_.data(), ld_, s_);
   }
 
-  // Sums K x kGroup values per climber of group g from the sweep partials into dres_ + off.
+  // Sums the K values per block of every listed group g from the partials into
+  // dres_ + off + g * stride.
   template <int K>
-  void finalize(int nblocks, size_t off)
+  void finalize(int nblocks, size_t off, int stride)
   {
-    finalize_sum_kernel<K><<<1, kBlock, 0, s_>>>(partials_.data(), nblocks, dres_.data() + off);
+    if (n_act() == 0) return;
+    mm_finalize_kernel<K><<<n_act(), kBlock, 0, s_>>>(partials_.data(), pstride_, nblocks,
+                                                      groups_d_.data(), dres_.data() + off, stride);
     ++launches_;
+  }
+  // Sums of (a - b)^2 per climber over `rows` rows into dres_ + off + climber.
+  void sqdiff(const double* a, const double* b, int rows, size_t off)
+  {
+    if (n_act() == 0) return;
+    mm_sqdiff_kernel<<<e_.vgrid_ * n_act(), kBlock, 0, s_>>>(a, b, rows, ld_, groups_d_.data(),
+                                                            n_act(), partials_.data(), pstride_);
+    ++launches_;
+    finalize<kGroup>(e_.vgrid_, off, kGroup);
   }
   void fetch(size_t count)
   {
@@ -570,28 +617,22 @@ class climber_engine {
     ++launches_;
     const auto A = view64(e_.L_.A), AT = view64(e_.L_.AT);
     std::vector<conv_info> cv(ld_);
-    for (int g = 0; g < groups_; ++g) {
-      if (!group_active(g)) continue;
-      mm_sweep_kernel<<<sell_grid(A), kBlock, 0, s_>>>(
-        A, xu_.data(), ld_, g * kGroup,
-        mm_term_primal_epi{e_.lc64_.data(), e_.uc64_.data(), yu_.data(), ctx(g)},
-        partials_.data());
-      finalize<2 * kGroup>(sell_grid(A), 0);
-      mm_sweep_kernel<<<sell_grid(AT), kBlock, 0, s_>>>(
-        AT, yu_.data(), ld_, g * kGroup,
-        mm_term_dual_epi{e_.c64_.data(), xu_.data(), su_.data(), ctx(g)}, partials_.data());
-      finalize<3 * kGroup>(sell_grid(AT), 2 * kGroup);
-      launches_ += 2;
-      B200_LAUNCH_CHECK();
-      fetch(5 * kGroup);
+    sweep(A, xu_.data(), mm_term_primal_epi{e_.lc64_.data(), e_.uc64_.data(), yu_.data(), ctx()});
+    finalize<2 * kGroup>(sell_grid(A), 0, 5 * kGroup);
+    sweep(AT, yu_.data(), mm_term_dual_epi{e_.c64_.data(), xu_.data(), su_.data(), ctx()});
+    finalize<3 * kGroup>(sell_grid(AT), 2 * kGroup, 5 * kGroup);
+    B200_LAUNCH_CHECK();
+    fetch(5 * (size_t)ld_);
+    for (int g : groups_h_) {
+      const double* h = hbuf_ + (size_t)g * 5 * kGroup;
       for (int q = 0; q < kGroup; ++q) {
         const int b = g * kGroup + q;
         if (!active_h_[b]) continue;
         conv_info& c = cv[b];
-        c.l2_primal  = std::sqrt(hbuf_[q]);
-        c.l2_dual    = std::sqrt(hbuf_[2 * kGroup + q]);
-        c.primal_obj = hbuf_[3 * kGroup + q];
-        c.dual_obj   = hbuf_[4 * kGroup + q] + hbuf_[kGroup + q];
+        c.l2_primal  = std::sqrt(h[q]);
+        c.l2_dual    = std::sqrt(h[2 * kGroup + q]);
+        c.primal_obj = h[3 * kGroup + q];
+        c.dual_obj   = h[4 * kGroup + q] + h[kGroup + q];
         if (e_.obj_scale_ != 1.0 || e_.obj_offset_ != 0.0) {
           c.primal_obj = e_.obj_scale_ * (c.primal_obj + e_.obj_offset_);
           c.dual_obj   = e_.obj_scale_ * (c.dual_obj + e_.obj_offset_);
@@ -673,20 +714,15 @@ class climber_engine {
             groups_seen[g] = 0;
             groups_changed = true;
           }
-        if (groups_changed) drop_graphs();
+        if (groups_changed) {
+          drop_graphs();
+          refresh_groups();
+        }
         active_d_.upload(active_h_.data(), ld_, s_);
 
         if (major) {
-          for (int g = 0; g < groups_; ++g) {
-            if (!group_active(g)) continue;
-            mm_sqdiff_kernel<<<e_.vgrid_, kBlock, 0, s_>>>(xa_.data(), xhat_.data(), n, ld_,
-                                                           g * kGroup, partials_.data());
-            finalize<kGroup>(e_.vgrid_, (size_t)g * kGroup);
-            mm_sqdiff_kernel<<<e_.vgrid_, kBlock, 0, s_>>>(ya_.data(), yhat_.data(), m, ld_,
-                                                           g * kGroup, partials_.data());
-            finalize<kGroup>(e_.vgrid_, (size_t)ld_ + g * kGroup);
-            launches_ += 2;
-          }
+          sqdiff(xa_.data(), xhat_.data(), n, 0);
+          sqdiff(ya_.data(), yhat_.data(), m, (size_t)ld_);
           B200_LAUNCH_CHECK();
           fetch(2 * (size_t)ld_);
           for (int b = 0; b < B_; ++b) {
@@ -764,24 +800,18 @@ class climber_engine {
       }
 
       if (fpe_all || any_restart) {
+        const auto A = view_of<double>(e_.L_.A, e_.As_.data());
         const auto AT = view_of<double>(e_.L_.AT, e_.ATs_.data());
-        for (int g = 0; g < groups_; ++g) {
-          if (!group_active(g)) continue;
-          if (mstep) {
-            launch_primal<true, false, true>(g, 0);
-            launch_dual<true, false, true>(g, 0);
-          } else {
-            launch_primal<false, false, true>(g, 0);
-            launch_dual<false, false, true>(g, 0);
-          }
-          finalize<kGroup>(sell_grid(view_of<double>(e_.L_.A, e_.As_.data())),
-                           (size_t)g * kGroup);
-          mm_sweep_kernel<<<sell_grid(AT), kBlock, 0, s_>>>(
-            AT, ybar_.data(), ld_, g * kGroup, mm_fpe_epi{aty_.data(), xbar_.data(), x_.data(), ctx(g)},
-            partials_.data());
-          finalize<2 * kGroup>(sell_grid(AT), (size_t)ld_ + 2 * g * kGroup);
-          ++launches_;
+        if (mstep) {
+          launch_primal<true, false, true>(0);
+          launch_dual<true, false, true>(0);
+        } else {
+          launch_primal<false, false, true>(0);
+          launch_dual<false, false, true>(0);
         }
+        finalize<kGroup>(sell_grid(A), 0, kGroup);
+        sweep(AT, ybar_.data(), mm_fpe_epi{aty_.data(), xbar_.data(), x_.data(), ctx()});
+        finalize<2 * kGroup>(sell_grid(AT), (size_t)ld_, 2 * kGroup);
         mm_halpern_kernel<<<e_.vgrid_, kBlock, 0, s_>>>(x_.data(), xbar_.data(), xa_.data(), nx,
                                                         y_.data(), ybar_.data(), ya_.data(), ny,
                                                         ld_, active_d_.data(), sc_d_.data());
@@ -800,10 +830,8 @@ class climber_engine {
           if (restarted[b]) fpe0[b] = fpe[b];
         }
       } else {
-        for (int g = 0; g < groups_; ++g)
-          if (group_active(g)) launch_primal<true, true, false>(g, 0);
-        for (int g = 0; g < groups_; ++g)
-          if (group_active(g)) launch_dual<true, true, false>(g, 0);
+        launch_primal<true, true, false>(0);
+        launch_dual<true, true, false>(0);
         advance(1);
         B200_LAUNCH_CHECK();
       }
@@ -848,7 +876,9 @@ class climber_engine {
   std::vector<double> omega_, best_omega_;
   std::vector<pdlp_result> results_;
   dbuf<climber_bound> ovr_;
-  dbuf<int> active_d_, flags_;
+  dbuf<int> active_d_, flags_, groups_d_;
+  std::vector<int> groups_h_;
+  size_t pstride_ = 0;
   dbuf<pdlp_scalars> sc_d_;
   dbuf<double> x_, xhat_, slack_, xbar_, xa_, aty_, y_, yhat_, ybar_, ya_, xu_, yu_, su_;
   dbuf<double> partials_, dres_;

@@ -66,9 +66,9 @@ struct red_t {
   double v[K > 0 ? K : 1];
 };
 
-// Block reduction of K doubles; thread 0 writes partials[blockIdx.x * K + r].
+// Block reduction of K doubles; threads 0..K-1 write partials[slot * K + r].
 template <int K>
-__device__ __forceinline__ void block_reduce_store(red_t<K>& r, double* partials)
+__device__ __forceinline__ void block_reduce_store(red_t<K>& r, double* partials, int slot)
 {
   if constexpr (K > 0) {
     __shared__ double sm[kWarpsPerBlock][K];
@@ -83,15 +83,19 @@ __device__ __forceinline__ void block_reduce_store(red_t<K>& r, double* partials
       double s = 0.0;
 #pragma unroll
       for (int w = 0; w < kWarpsPerBlock; ++w) s += sm[w][threadIdx.x];
-      partials[(size_t)blockIdx.x * K + threadIdx.x] = s;
+      partials[(size_t)slot * K + threadIdx.x] = s;
     }
   }
 }
-
-// out[q] = sum over blocks of partials[b*K+q] (single block, ordered, compensated).
 template <int K>
-__global__ void __launch_bounds__(kBlock) finalize_sum_kernel(const double* partials, int nblocks,
-                                                              double* out)
+__device__ __forceinline__ void block_reduce_store(red_t<K>& r, double* partials)
+{
+  block_reduce_store<K>(r, partials, (int)blockIdx.x);
+}
+
+// out[q] = sum over blocks of partials[b*K+q], summed by one block (ordered, compensated).
+template <int K>
+__device__ __forceinline__ void ordered_block_sum(const double* partials, int nblocks, double* out)
 {
   __shared__ double sm[kBlock];
   for (int q = 0; q < K; ++q) {
@@ -106,6 +110,12 @@ __global__ void __launch_bounds__(kBlock) finalize_sum_kernel(const double* part
     if (threadIdx.x == 0) out[q] = sm[0];
     __syncthreads();
   }
+}
+template <int K>
+__global__ void __launch_bounds__(kBlock) finalize_sum_kernel(const double* partials, int nblocks,
+                                                              double* out)
+{
+  ordered_block_sum<K>(partials, nblocks, out);
 }
 
 // 4 consecutive values of one lane chunk (16-byte aligned), streamed with evict-first loads.

@@ -12,6 +12,9 @@
          on), back-propagates L = sum w * x* through the KKT adjoint, and checks the gradients
          against the exact basis derivatives and against central differences (h = 1e-6) on random
          coordinates of c, b and the A values.
+`climbers` solves `count` copies of one LP (the config's) that differ in one variable's upper
+         bound each with one cuOptSolveClimbers call (FP64), and a sample of the same copies one
+         by one with cuOptSolve.
 Prints one JSON line with the timings.
 """
 from __future__ import annotations
@@ -47,7 +50,7 @@ def main() -> None:
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c1_small")
-    ap.add_argument("--mode", choices=["solve", "sweeps", "batch", "adjoint"], default="sweeps")
+    ap.add_argument("--mode", choices=["solve", "sweeps", "batch", "adjoint", "climbers"], default="sweeps")
     ap.add_argument("--fd-instances", type=int, default=2,
                     help="adjoint mode: instances checked by finite differences")
     ap.add_argument("--fd-coords", type=int, default=32,
@@ -71,6 +74,9 @@ def main() -> None:
         return
     if a.mode == "adjoint":
         print(json.dumps(run_adjoint(a)))
+        return
+    if a.mode == "climbers":
+        print(json.dumps(run_climbers(a)))
         return
     m, n, k, seed = CONFIGS[a.config]
     lp = gen.constructed_lp(m, n, k, seed=seed) if k else gen.skewed_lp(m, n, seed=seed)
@@ -280,6 +286,70 @@ def run_adjoint(a) -> dict:
             "grad_vs_basis_max_rel_error": err, "basis_checked_instances": nb,
             "fd_checked": checked, "fd_h": h,
             "fd_max_rel_error": fd_err}
+
+
+def run_climbers(a) -> dict:
+    """Strong-branching shape: `count` climbers of one LP in one call vs the same LPs one by one."""
+    import numpy as np
+
+    from cuopt_b200 import generators as gen
+    from cuopt_b200 import linear_programming as lpm
+
+    m, n, k, seed = CONFIGS[a.config]
+    lp = gen.constructed_lp(m, n, k, seed=seed) if k else gen.skewed_lp(m, n, seed=seed)
+    rng = np.random.default_rng(7)
+    var = rng.choice(n, a.count, replace=False).astype(np.int32)
+    lo = lp.var_lo[var].copy()
+    up = np.minimum(lp.var_up[var], rng.uniform(0.5, 3.0, a.count))
+
+    def model(j=None, l=None, u=None):
+        dm = lpm.DataModel()
+        dm.set_csr_constraint_matrix(lp.val, lp.col_idx, lp.row_off)
+        dm.set_objective_coefficients(lp.c)
+        dm.set_constraint_lower_bounds(lp.con_lo)
+        dm.set_constraint_upper_bounds(lp.con_up)
+        vl, vu = lp.var_lo.copy(), lp.var_up.copy()
+        if j is not None:
+            vl[j], vu[j] = l, u
+        dm.set_variable_lower_bounds(vl)
+        dm.set_variable_upper_bounds(vu)
+        return dm
+
+    st = lpm.SolverSettings()
+    st.set_optimality_tolerance(a.tol)
+    st.set_parameter(lpm.CUOPT_METHOD, int(lpm.SolverMethod.PDLP))
+    st.set_parameter(lpm.CUOPT_LOG_TO_CONSOLE, False)
+    if a.time_limit > 0:
+        st.set_parameter(lpm.CUOPT_TIME_LIMIT, a.time_limit)
+    base = model()
+    times = []
+    for _ in range(max(1, a.repeats)):
+        sols, t = lpm.SolveClimbers(base, var, lo, up, st)
+        times.append(t)
+    batch_s = min(times[1:]) if len(times) > 1 else times[0]
+    status = [int(s.get_termination_status()) for s in sols]
+    iters = [s.get_lp_stats()["nb_iterations"] for s in sols]
+    out = {"config": a.config, "m": m, "n": n, "nnz": lp.nnz, "climbers": a.count,
+           "climbers_s": batch_s, "climbers_times_s": times, "climbers_per_s": a.count / batch_s,
+           "optimal": status.count(1), "max_iterations": max(iters),
+           "mean_iterations": float(np.mean(iters))}
+    if a.sequential > 0:
+        pick = np.linspace(0, a.count - 1, min(a.sequential, a.count)).astype(int)
+        dms = [model(var[i], lo[i], up[i]) for i in pick]
+        lpm.Solve(dms[0], st)  # warm-up
+        t0 = time.perf_counter()
+        same, seq_iters = 0, []
+        for i, dm in zip(pick, dms):
+            s1 = lpm.Solve(dm, st)
+            seq_iters.append(s1.get_lp_stats()["nb_iterations"])
+            same += int(seq_iters[-1] == iters[i])
+        seq_s = time.perf_counter() - t0
+        out.update({"sequential_sample": int(len(pick)), "sequential_s_per_lp": seq_s / len(pick),
+                    "sequential_lps_per_s": len(pick) / seq_s,
+                    "sequential_same_iterations": same,
+                    "sequential_mean_iterations": float(np.mean(seq_iters)),
+                    "speedup_climbers_vs_sequential": (a.count / batch_s) / (len(pick) / seq_s)})
+    return out
 
 
 if __name__ == "__main__":
