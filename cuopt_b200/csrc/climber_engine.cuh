@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(kBlock) mm_sqdiff_kernel(const double* a, cons
   block_reduce_store<kGroup>(r, partials + (size_t)grp * pstride, xb);
 }
 
-// x = clamp(0, l, u) with the climbers' overrides (project_initial_primal).
+// x = clamp(x, l, u) with the climbers' overrides (project_initial_primal).
 __global__ void mm_initial_primal_kernel(double* x, const double* l, const double* u, int n, int ld,
                                          const climber_bound* ovr)
 {
@@ -386,7 +386,20 @@ __global__ void mm_initial_primal_kernel(double* x, const double* l, const doubl
     const int b = (int)(e % ld), j = (int)(e / ld);
     const climber_bound o = ovr[b];
     const double lo = o.col == j ? o.l : l[j], hi = o.col == j ? o.u : u[j];
-    x[e]            = fmin(fmax(0.0, lo), hi);
+    x[e]            = fmin(fmax(x[e], lo), hi);
+  }
+}
+
+// a = b = c = src broadcast to every climber (element e = row * ld + climber).
+__global__ void mm_broadcast_kernel(const double* src, int rows, int ld, double* a, double* b,
+                                    double* c)
+{
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < (size_t)rows * ld;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const double v = src[e / ld];
+    a[e]           = v;
+    b[e]           = v;
+    c[e]           = v;
   }
 }
 
@@ -468,12 +481,25 @@ class climber_engine {
       v->resize(ny);
       v->zero(s_);
     }
+    // A warm start (the caller's initial solution, scaled by the base engine into x_hat and y_hat
+    // of the base) starts every climber at the same point, as the reference's batch does with
+    // its initial solution; the primal is then projected onto each climber's bounds.
+    if (e_.in_.initial_primal) {
+      mm_broadcast_kernel<<<e_.vgrid_, kBlock, 0, s_>>>(e_.xhat_.data(), n, ld_, x_.data(),
+                                                        xhat_.data(), xa_.data());
+      ++launches_;
+    }
+    if (e_.in_.initial_dual) {
+      mm_broadcast_kernel<<<e_.vgrid_, kBlock, 0, s_>>>(e_.yhat_.data(), m, ld_, y_.data(),
+                                                        yhat_.data(), ya_.data());
+      ++launches_;
+    }
     mm_initial_primal_kernel<<<e_.vgrid_, kBlock, 0, s_>>>(x_.data(), e_.ls_.data(),
                                                            e_.us_.data(), n, ld_, ovr_.data());
     ++launches_;
     sc_d_.resize(ld_);
-    omega_.assign(ld_, 1.0);
-    best_omega_.assign(ld_, 1.0);
+    omega_.assign(ld_, e_.omega_);
+    best_omega_.assign(ld_, e_.best_omega_);
     restarts_.assign(ld_, 0);
     const int g =
       std::max({sell_grid(view64(e_.L_.A)), sell_grid(view64(e_.L_.AT)), e_.vgrid_});

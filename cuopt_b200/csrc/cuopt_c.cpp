@@ -733,21 +733,12 @@ cuopt_int_t cuOptBatchPDLPStrongBranching(cuOptOptimizationProblem problem,
     std::vector<double> root;
     copy_in(frac, fractional, count);
     copy_in(root, root_solution, count);
-    // Down branches (upper bound floor(x)) then up branches (lower bound ceil(x)), as
-    // batch_pdlp_solve builds them (reference solve.cu:884-919).
-    std::vector<int> var(2 * count);
-    std::vector<double> lo(2 * count), up(2 * count);
-    for (cuopt_int_t i = 0; i < count; ++i) {
-      const int j = frac[i];
-      if (j < 0 || j >= p.n) return CUOPT_INVALID_ARGUMENT;
-      var[i]         = j;
-      lo[i]          = p.var_lo[j];
-      up[i]          = std::floor(root[i]);
-      var[count + i] = j;
-      lo[count + i]  = std::ceil(root[i]);
-      up[count + i]  = p.var_up[j];
-    }
-    return climbers_to_solutions(cuopt_b200::solve_climbers(p, *S(settings), var, lo, up),
+    for (cuopt_int_t i = 0; i < count; ++i)
+      if (frac[i] < 0 || frac[i] >= p.n) return CUOPT_INVALID_ARGUMENT;
+    // Down branches (upper bound floor(x)) then up branches (lower bound ceil(x)), started from a
+    // solve of the LP itself, as batch_pdlp_solve / run_batch_pdlp do (reference
+    // solve.cu:743-919).
+    return climbers_to_solutions(cuopt_b200::solve_strong_branching(p, *S(settings), frac, root),
                                  solutions);
   } catch (const std::bad_alloc&) {
     return CUOPT_OUT_OF_MEMORY;

@@ -666,7 +666,7 @@ std::vector<lp_solution> solve_batch(const std::vector<const lp_problem*>& ps, c
 
 std::vector<lp_solution> solve_climbers(const lp_problem& p, const lp_settings& st,
                                         const std::vector<int>& var, const std::vector<double>& lo,
-                                        const std::vector<double>& up)
+                                        const std::vector<double>& up, const climber_start* start)
 {
   const int count = (int)var.size();
   std::vector<lp_solution> out(count);
@@ -734,7 +734,24 @@ std::vector<lp_solution> solve_climbers(const lp_problem& p, const lp_settings& 
     in.var_up     = dvu.data();
     in.obj_offset = p.obj_offset;
     in.maximize   = p.maximize;
-    const pdlp_params prm = params_from_settings(st);
+    pdlp_params prm = params_from_settings(st);
+    const std::vector<double>* x0 = start ? &start->x : &st.initial_primal;
+    const std::vector<double>* y0 = start ? &start->y : &st.initial_dual;
+    if (start) {
+      prm.initial_step_size     = start->step_size;
+      prm.initial_primal_weight = start->primal_weight;
+    }
+    dbuf<double> dx0, dy0;
+    if ((int)x0->size() == n) {
+      dx0.resize(n);
+      dx0.upload(x0->data(), n, s);
+      in.initial_primal = dx0.data();
+    }
+    if ((int)y0->size() == m) {
+      dy0.resize(m);
+      dy0.upload(y0->data(), m, s);
+      in.initial_dual = dy0.data();
+    }
     std::vector<double> hx((size_t)count * n), hy((size_t)count * m), hrc((size_t)count * n);
     std::vector<pdlp_result> rs =
       pdlp_climber_solve_device(in, prm, var, lo, up, s, hx.data(), hy.data(), hrc.data());
@@ -756,6 +773,47 @@ std::vector<lp_solution> solve_climbers(const lp_problem& p, const lp_settings& 
     for (auto& o : out) set_error(o, CUOPT_RUNTIME_ERROR, e.what());
   }
   return out;
+}
+
+std::vector<lp_solution> solve_strong_branching(const lp_problem& p, const lp_settings& st,
+                                                const std::vector<int>& frac,
+                                                const std::vector<double>& root)
+{
+  const int count = (int)frac.size();
+  std::vector<int> var(2 * (size_t)count);
+  std::vector<double> lo(2 * (size_t)count), up(2 * (size_t)count);
+  for (int i = 0; i < count; ++i) {
+    const int j = frac[i];
+    if (j < 0 || j >= p.n) {
+      std::vector<lp_solution> out(2 * (size_t)count);
+      for (auto& o : out) set_error(o, CUOPT_INVALID_ARGUMENT, "fractional variable out of range");
+      return out;
+    }
+    var[i]         = j;
+    lo[i]          = p.var_lo[j];
+    up[i]          = std::floor(root[i]);
+    var[count + i] = j;
+    lo[count + i]  = std::ceil(root[i]);
+    up[count + i]  = p.var_up[j];
+  }
+  // The settings run_batch_pdlp gives both solves (solve.cu:795-834).
+  lp_settings sb = st;
+  sb.set_int(CUOPT_METHOD, CUOPT_METHOD_PDLP);
+  sb.set_int(CUOPT_PDLP_SOLVER_MODE, CUOPT_PDLP_SOLVER_MODE_STABLE3);
+  sb.set_bool(CUOPT_INFEASIBILITY_DETECTION, false);
+  sb.set_int(CUOPT_ITERATION_LIMIT, 100000);
+  lp_settings base_settings = sb;
+  base_settings.set_bool(CUOPT_CROSSOVER, false);
+  const lp_solution base = solve_problem(p, base_settings);
+  climber_start start;
+  if (base.error_code == CUOPT_SUCCESS && base.solved_by_pdlp && (int)base.r.x.size() == p.n &&
+      (int)base.r.y.size() == p.m) {
+    start.x             = base.r.x;
+    start.y             = base.r.y;
+    start.step_size     = base.r.step_size;
+    start.primal_weight = base.r.primal_weight;
+  }
+  return solve_climbers(p, sb, var, lo, up, start.x.empty() ? nullptr : &start);
 }
 
 }  // namespace cuopt_b200

@@ -111,12 +111,30 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& s);
 // batch (per-instance Stable3 state); the others are answered as solve_problem would.
 std::vector<lp_solution> solve_batch(const std::vector<const lp_problem*>& ps, const lp_settings& s);
 
-// MPS input / output (reference cpp/libmps_parser).  read_mps returns 0 or CUOPT_MPS_* codes.
-// Climber batch (strong branching): the LP solved once per climber b with variable var[b] bounded
-// by [lo[b], up[b]]; all climbers share one matrix read per sweep (see climber_engine.cuh).
+// Starting point shared by the climbers of a batch: an initial solution in the user's order, and
+// optionally the step size and primal weight to start from (NaN: computed / 1).
+struct climber_start {
+  std::vector<double> x, y;
+  double step_size     = std::numeric_limits<double>::quiet_NaN();
+  double primal_weight = std::numeric_limits<double>::quiet_NaN();
+};
+
+// Climber batch: the LP solved once per climber b with variable var[b] bounded by [lo[b], up[b]];
+// all climbers share one matrix read per sweep (see climber_engine.cuh).  Without `start`, the
+// settings' initial solution (if any) is every climber's starting point.
 std::vector<lp_solution> solve_climbers(const lp_problem& p, const lp_settings& s,
                                         const std::vector<int>& var, const std::vector<double>& lo,
-                                        const std::vector<double>& up);
+                                        const std::vector<double>& up,
+                                        const climber_start* start = nullptr);
+
+// Strong branching as the reference's batch_pdlp_solve / run_batch_pdlp do it
+// (cpp/src/pdlp/solve.cu:743-919): the LP is solved once (Stable3, no infeasibility detection,
+// iteration limit 100000), then the down branches (var[i] <= floor(root[i])) and the up branches
+// (var[i] >= ceil(root[i])) run as one climber batch started from that solution, its step size and
+// its primal weight, under the same limits.
+std::vector<lp_solution> solve_strong_branching(const lp_problem& p, const lp_settings& s,
+                                                const std::vector<int>& frac,
+                                                const std::vector<double>& root);
 
 // Reverse-mode sensitivities of an optimal solution (see adjoint.cu): gx (n) and optional gy (m)
 // in; any of dc (n), dlo / dup (m, constraint bounds) and dval (nnz, CSR order) out.
@@ -129,6 +147,7 @@ void solution_adjoint(const lp_problem& p, const pdlp_result& sol, const double*
 // (a degenerate optimum) the solution is left unchanged.
 bool vertex_polish(const lp_problem& p, pdlp_result& r);
 
+// MPS input / output (reference cpp/libmps_parser).  read_mps returns 0 or CUOPT_MPS_* codes.
 int read_mps(const std::string& path, lp_problem& out, std::string& err);
 int write_mps(const lp_problem& p, const std::string& path);
 

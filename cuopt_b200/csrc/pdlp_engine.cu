@@ -195,8 +195,11 @@ class engine {
     prepare_vectors();
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
     trace("engine: scaling");
-    // Step size from the largest singular value of the scaled A (reference pdlp.cu:2620-2731).
-    if (p_.precision == 1)
+    // Step size from the largest singular value of the scaled A (reference pdlp.cu:2620-2731),
+    // unless the caller gives it (pdlp.cu:2036-2059).
+    if (std::isfinite(p_.initial_step_size))
+      eta_ = p_.initial_step_size;
+    else if (p_.precision == 1)
       lanczos_step_size();
     else
       power_iteration();
@@ -304,8 +307,11 @@ class engine {
   void reset_iterates(bool with_initial)
   {
     const int m = in_.m, n = in_.n;
-    omega_      = 1.0;  // bound_objective_rescaling => primal weight 1 (pdlp.cu:2799-2810)
-    best_omega_ = 1.0;
+    // bound_objective_rescaling => primal weight 1 (pdlp.cu:2799-2810); a given initial weight
+    // replaces it and the PID controller's best weight (pdlp.cu:2061-2083).
+    omega_      = with_initial && std::isfinite(p_.initial_primal_weight) ? p_.initial_primal_weight
+                                                                          : 1.0;
+    best_omega_ = omega_;
     restarts_   = 0;
     for (auto* b : {&x_, &xhat_, &slack_, &xbar_, &xa_, &aty_}) {
       b->resize(n);

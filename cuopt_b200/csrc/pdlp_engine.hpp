@@ -8,6 +8,7 @@
 
 #include <cstdint>
 #include <string>
+#include <limits>
 #include <vector>
 
 namespace cuopt_b200 {
@@ -44,6 +45,11 @@ struct pdlp_params {
   double dual_infeasible_tol   = 1e-10;
   std::vector<double> initial_primal;  // user order, optional
   std::vector<double> initial_dual;    // user order, optional
+  // Given by the warm start of a strong-branching batch (the reference's run_batch_pdlp,
+  // cpp/src/pdlp/solve.cu:743-882, and pdlp.cu:2027-2083): a finite step size replaces the power
+  // iteration, a finite primal weight the initial 1 (and the best weight of the PID controller).
+  double initial_step_size     = std::numeric_limits<double>::quiet_NaN();
+  double initial_primal_weight = std::numeric_limits<double>::quiet_NaN();
 };
 
 struct pdlp_result {

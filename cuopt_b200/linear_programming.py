@@ -461,6 +461,7 @@ def _solve_climbers(call, data_model, count, arrays, solver_settings):
     sols = (handle_t * count)()
     keep = [np.ascontiguousarray(a) for a in arrays]
     try:
+        _apply_initial(s, data_model)
         t0 = time.perf_counter()
         call(L, prob, s, sols, [C.c_void_p(a.ctypes.data) for a in keep])
         elapsed = time.perf_counter() - t0
@@ -480,7 +481,8 @@ def SolveClimbers(data_model, variable_indices, lower_bounds, upper_bounds,
                   solver_settings: SolverSettings | None = None):
     """Solves copies of one LP that differ only in one variable's bounds each (the reference's
     new_bounds batch, solve.cu:740-882): copy i bounds variable_indices[i] by
-    [lower_bounds[i], upper_bounds[i]].  Returns (solutions, time)."""
+    [lower_bounds[i], upper_bounds[i]].  An initial solution set on the data model is every copy's
+    starting point.  Returns (solutions, time)."""
     idx = np.asarray(variable_indices, dtype=np.int32)
     lo = np.asarray(lower_bounds, dtype=np.float64)
     up = np.asarray(upper_bounds, dtype=np.float64)
@@ -492,9 +494,11 @@ def SolveClimbers(data_model, variable_indices, lower_bounds, upper_bounds,
 
 def BatchPDLPStrongBranching(data_model, fractional, root_solution,
                              solver_settings: SolverSettings | None = None):
-    """Strong branching (the reference's batch_pdlp_solve, solve.cu:884-919): the down branches
-    (x_j <= floor(root_j)) of every fractional variable, then the up branches (x_j >= ceil(root_j)).
-    Returns (solutions, time) with 2 * len(fractional) solutions."""
+    """Strong branching (the reference's batch_pdlp_solve, solve.cu:743-919): the down branches
+    (x_j <= floor(root_j)) of every fractional variable, then the up branches (x_j >= ceil(root_j)),
+    all started from a solve of the LP itself (its solution, step size and primal weight; iteration
+    limit 100000, no infeasibility detection).  Returns (solutions, time) with 2 * len(fractional)
+    solutions."""
     frac = np.asarray(fractional, dtype=np.int32)
     root = np.asarray(root_solution, dtype=np.float64)
     n = len(frac)

@@ -14,7 +14,9 @@
          coordinates of c, b and the A values.
 `climbers` solves `count` copies of one LP (the config's) that differ in one variable's upper
          bound each with one cuOptSolveClimbers call (FP64), and a sample of the same copies one
-         by one with cuOptSolve.
+         by one with cuOptSolve.  With --strong-branching: cuOptBatchPDLPStrongBranching on
+         count / 2 fractional variables (a solve of the LP, then `count` warm-started branches),
+         against the same branches solved one by one from the LP's solution.
 Prints one JSON line with the timings.
 """
 from __future__ import annotations
@@ -66,6 +68,8 @@ def main() -> None:
     ap.add_argument("--iterations", type=int, default=3)
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--time-limit", type=float, default=0.0)
+    ap.add_argument("--strong-branching", action="store_true",
+                    help="climbers mode: time cuOptBatchPDLPStrongBranching instead")
     ap.add_argument("--refine", type=int, default=0, help="> 0: continue a mixed-precision solve in FP64 to 1e-8")
     a = ap.parse_args()
 
@@ -322,22 +326,41 @@ def run_climbers(a) -> dict:
     if a.time_limit > 0:
         st.set_parameter(lpm.CUOPT_TIME_LIMIT, a.time_limit)
     base = model()
+    if a.strong_branching:
+        frac = var[: a.count // 2]
+        root = np.minimum(lp.x_star[frac], lp.var_up[frac] - 1.0) + 0.5
+        var = np.concatenate([frac, frac])
+        lo = np.concatenate([lp.var_lo[frac], np.ceil(root)])
+        up = np.concatenate([np.floor(root), lp.var_up[frac]])
+        run = lambda: lpm.BatchPDLPStrongBranching(base, frac, root, st)
+    else:
+        run = lambda: lpm.SolveClimbers(base, var, lo, up, st)
     times = []
     for _ in range(max(1, a.repeats)):
-        sols, t = lpm.SolveClimbers(base, var, lo, up, st)
+        sols, t = run()
         times.append(t)
     batch_s = min(times[1:]) if len(times) > 1 else times[0]
     status = [int(s.get_termination_status()) for s in sols]
     iters = [s.get_lp_stats()["nb_iterations"] for s in sols]
-    out = {"config": a.config, "m": m, "n": n, "nnz": lp.nnz, "climbers": a.count,
-           "climbers_s": batch_s, "climbers_times_s": times, "climbers_per_s": a.count / batch_s,
+    out = {"config": a.config, "m": m, "n": n, "nnz": lp.nnz, "climbers": len(sols),
+           "strong_branching": bool(a.strong_branching),
+           "climbers_s": batch_s, "climbers_times_s": times, "climbers_per_s": len(sols) / batch_s,
            "optimal": status.count(1), "max_iterations": max(iters),
            "mean_iterations": float(np.mean(iters))}
     if a.sequential > 0:
-        pick = np.linspace(0, a.count - 1, min(a.sequential, a.count)).astype(int)
+        pick = np.linspace(0, len(sols) - 1, min(a.sequential, len(sols))).astype(int)
         dms = [model(var[i], lo[i], up[i]) for i in pick]
-        lpm.Solve(dms[0], st)  # warm-up
         t0 = time.perf_counter()
+        if a.strong_branching:
+            # One solve of the LP, then each branch from its solution (single solves recompute the
+            # step size and start at primal weight 1).
+            root_sol = lpm.Solve(base, st)
+            for dm in dms:
+                dm.set_initial_primal_solution(root_sol.get_primal_solution())
+                dm.set_initial_dual_solution(root_sol.get_dual_solution())
+        else:
+            lpm.Solve(dms[0], st)  # warm-up
+            t0 = time.perf_counter()
         same, seq_iters = 0, []
         for i, dm in zip(pick, dms):
             s1 = lpm.Solve(dm, st)
@@ -348,7 +371,7 @@ def run_climbers(a) -> dict:
                     "sequential_lps_per_s": len(pick) / seq_s,
                     "sequential_same_iterations": same,
                     "sequential_mean_iterations": float(np.mean(seq_iters)),
-                    "speedup_climbers_vs_sequential": (a.count / batch_s) / (len(pick) / seq_s)})
+                    "speedup_climbers_vs_sequential": (len(sols) / batch_s) / (len(pick) / seq_s)})
     return out
 
 

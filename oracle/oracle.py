@@ -20,7 +20,8 @@ class _LP(C.Structure):
                 ("c", C.c_void_p), ("con_lo", C.c_void_p), ("con_up", C.c_void_p),
                 ("var_lo", C.c_void_p), ("var_up", C.c_void_p),
                 ("obj_offset", C.c_double), ("maximize", C.c_int),
-                ("initial_primal", C.c_void_p), ("initial_dual", C.c_void_p)]
+                ("initial_primal", C.c_void_p), ("initial_dual", C.c_void_p),
+                ("initial_step_size", C.c_double), ("initial_primal_weight", C.c_double)]
 
 
 class _Settings(C.Structure):
@@ -66,7 +67,8 @@ class _Holder:
     """Keeps the numpy arrays alive while the C struct points at them."""
 
     def __init__(self, row_off, col_idx, val, c, con_lo, con_up, var_lo, var_up, obj_offset=0.0,
-                 maximize=False, initial_primal=None, initial_dual=None):
+                 maximize=False, initial_primal=None, initial_dual=None, initial_step_size=None,
+                 initial_primal_weight=None):
         self.a = [np.ascontiguousarray(row_off, np.int32), np.ascontiguousarray(col_idx, np.int32)]
         self.a += [np.ascontiguousarray(v, np.float64) for v in (val, c, con_lo, con_up, var_lo, var_up)]
         p = [x.ctypes.data for x in self.a]
@@ -75,20 +77,25 @@ class _Holder:
                      for v in (initial_primal, initial_dual)]
         self.s = _LP(m, len(self.a[3]), int(self.a[0][-1]) if m >= 0 else 0, *p,
                      float(obj_offset), int(bool(maximize)),
-                     *[None if v is None else v.ctypes.data for v in self.init])
+                     *[None if v is None else v.ctypes.data for v in self.init],
+                     *[float("nan") if v is None else float(v)
+                       for v in (initial_step_size, initial_primal_weight)])
 
 
-def _holder(lp, initial_primal=None, initial_dual=None):
+def _holder(lp, initial_primal=None, initial_dual=None, initial_step_size=None,
+            initial_primal_weight=None):
     return _Holder(lp.row_off, lp.col_idx, lp.val, lp.c, lp.con_lo, lp.con_up, lp.var_lo, lp.var_up,
                    getattr(lp, "obj_offset", 0.0), getattr(lp, "maximize", False),
-                   initial_primal, initial_dual)
+                   initial_primal, initial_dual, initial_step_size, initial_primal_weight)
 
 
 def solve(lp, tol=1e-4, iteration_limit=2**31 - 1, time_limit=1e300, threads=0,
-          detect_infeasibility=False, infeasible_tol=1e-10, initial_primal=None, initial_dual=None):
+          detect_infeasibility=False, infeasible_tol=1e-10, initial_primal=None, initial_dual=None,
+          initial_step_size=None, initial_primal_weight=None):
     """Runs the FP64 Stable3 restatement (optionally warm-started from an initial primal and / or
-    dual solution in the user's order).  Returns (result dict, x, y, reduced_cost)."""
-    h = _holder(lp, initial_primal, initial_dual)
+    dual solution in the user's order, and from a given step size and primal weight).  Returns
+    (result dict, x, y, reduced_cost)."""
+    h = _holder(lp, initial_primal, initial_dual, initial_step_size, initial_primal_weight)
     m, n = h.s.m, h.s.n
     st = _Settings(tol, tol, tol, tol, tol, tol, int(iteration_limit), float(time_limit), int(threads),
                    int(bool(detect_infeasibility)), float(infeasible_tol), float(infeasible_tol))
@@ -98,6 +105,32 @@ def solve(lp, tol=1e-4, iteration_limit=2**31 - 1, time_limit=1e300, threads=0,
                             rc.ctypes.data)
     res = {f: getattr(r, f) for f, _ in _Result._fields_}
     return res, x, y, rc
+
+
+def strong_branching(lp, fractional, root, tol=1e-4, time_limit=1e300, threads=0):
+    """The reference's batch_pdlp_solve (solve.cu:743-919) restated on the oracle: the LP solved
+    once (iteration limit 100000, no infeasibility detection), then every down branch
+    (x_j <= floor(root)) and up branch (x_j >= ceil(root)) solved from that solution, its step size
+    and its primal weight under the same limits.  Returns a list of (result, x, y, rc), down
+    branches first."""
+    import copy
+    base, x0, y0, _ = solve(lp, tol=tol, iteration_limit=100000, time_limit=time_limit,
+                            threads=threads)
+    out = []
+    for down in (True, False):
+        for j, r in zip(fractional, root):
+            q = copy.copy(lp)
+            q.var_lo = np.array(lp.var_lo, dtype=np.float64)
+            q.var_up = np.array(lp.var_up, dtype=np.float64)
+            if down:
+                q.var_up[j] = np.floor(r)
+            else:
+                q.var_lo[j] = np.ceil(r)
+            out.append(solve(q, tol=tol, iteration_limit=100000, time_limit=time_limit,
+                             threads=threads, initial_primal=x0, initial_dual=y0,
+                             initial_step_size=base["step_size"],
+                             initial_primal_weight=base["primal_weight"]))
+    return out
 
 
 def initial_step_and_weight(lp, mode: int = 4):

@@ -378,6 +378,11 @@ struct oracle_lp {
   int maximize;
   const double* initial_primal;  // optional (n), user order; null: start from zero
   const double* initial_dual;    // optional (m)
+  // Optional (NaN: not given): a step size that replaces the power iteration and a primal weight
+  // that replaces the initial 1, as the reference's strong-branching batch passes them
+  // (solve.cu:835-842, pdlp.cu:2027-2083).
+  double initial_step_size;
+  double initial_primal_weight;
 };
 
 struct oracle_settings {
@@ -501,13 +506,17 @@ int oracle_pdlp_solve(const oracle_lp* in, const oracle_settings* st, oracle_res
   const double c_norm = nrm2(p.c);
   const double b_norm = bound_norm(p.con_lo, p.con_up);
 
-  // Initial primal weight before scaling: bound_objective_rescaling => 1 (pdlp.cu:2799-2810)
-  double omega = 1.0, best_omega = 1.0;
+  // Initial primal weight before scaling: bound_objective_rescaling => 1 (pdlp.cu:2799-2810),
+  // unless one is given; it also seeds the PID controller's best weight (pdlp.cu:2061-2083).
+  double omega = std::isfinite(in->initial_primal_weight) ? in->initial_primal_weight : 1.0;
+  double best_omega = omega;
   scaling_t s  = compute_scaling(p, h);
   lp_t q       = scale_problem(p, s, h);
   int piters   = 0;
-  double s2    = power_iteration(q, &piters);
-  const double eta = 0.998 / std::sqrt(s2);
+  // A given step size skips compute_initial_step_size (pdlp.cu:2036-2059).
+  const double eta = std::isfinite(in->initial_step_size)
+                       ? in->initial_step_size
+                       : 0.998 / std::sqrt(power_iteration(q, &piters));
   if (!(std::isfinite(eta) && eta > 0)) {
     res->status = kNumericalError;
     return 0;

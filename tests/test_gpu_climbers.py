@@ -1,10 +1,12 @@
 """GPU tests of the climber batch (cuOptSolveClimbers / cuOptBatchPDLPStrongBranching): copies of
 one LP that differ in one variable's bounds each, swept together through one matrix read.
 
-Reference for every expectation: the CPU oracle solving each modified LP alone, and the reference's
-own batch test (pdlp_test.cu:1450-1535: identical climbers on afiro give bitwise identical
-results, all Optimal at afiro's objective).  Tolerances: iterates after the same number of
-iterations agree with the oracle to 1e-9 relative to the vector's magnitude.
+Reference for every expectation: the CPU oracle solving each modified LP alone (for strong
+branching, its restatement of batch_pdlp_solve: a solve of the LP, then warm-started branches), and
+the reference's own batch test (pdlp_test.cu:1450-1535: identical climbers on afiro give bitwise
+identical results, all Optimal at afiro's objective).  Tolerances: iterates after the same number
+of iterations agree with the oracle to 1e-9 relative to the vector's magnitude; solutions at the
+1e-6 termination of a strong-branching batch to 1e-7.
 """
 from __future__ import annotations
 
@@ -92,20 +94,48 @@ def test_identical_afiro_climbers_are_bitwise_identical(golden, golden_dir):
 
 
 def test_strong_branching_builds_down_then_up_branches(base_lp):
-    """batch_pdlp_solve's climbers: x_j <= floor(root_j) for every fractional j, then
-    x_j >= ceil(root_j); each matches the oracle's solve of that branch."""
+    """batch_pdlp_solve / run_batch_pdlp (solve.cu:743-919): the LP is solved first, then
+    x_j <= floor(root_j) for every fractional j and x_j >= ceil(root_j), each started from that
+    solution, its step size and primal weight; each matches the oracle's restatement."""
     rng = np.random.default_rng(5)
     frac = rng.choice(base_lp.n, 3, replace=False)
     root = base_lp.x_star[frac] + 0.5
     sols, _ = lpm.BatchPDLPStrongBranching(datamodel_from_lp(base_lp), frac, root,
-                                           settings(tol=1e-12, iteration_limit=200))
-    assert len(sols) == 6
-    for i, j in enumerate(frac):
-        for sol, (lo, up) in ((sols[i], (base_lp.var_lo[j], np.floor(root[i]))),
-                              (sols[3 + i], (np.ceil(root[i]), base_lp.var_up[j]))):
-            res, x, _, _ = O.solve(_modified(base_lp, j, lo, up), tol=1e-12, iteration_limit=200)
-            assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
-            assert np.max(np.abs(sol.get_primal_solution() - x)) <= ITERATE_RTOL * (1 + np.abs(x).max())
+                                           settings(tol=1e-6))
+    ref = O.strong_branching(base_lp, frac, root, tol=1e-6)
+    assert len(sols) == len(ref) == 6
+    for i, (sol, (res, x, y, _)) in enumerate(zip(sols, ref)):
+        j = frac[i % 3]
+        xj = sol.get_primal_solution()[j]
+        assert int(sol.get_termination_status()) == res["status"] == 1
+        assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+        assert sol.stats["power_iterations"] == 0
+        assert np.max(np.abs(sol.get_primal_solution() - x)) <= 1e-7 * (1 + np.abs(x).max())
+        assert np.max(np.abs(sol.get_dual_solution() - y)) <= 1e-7 * (1 + np.abs(y).max())
+        if i < 3:
+            assert xj <= np.floor(root[i]) + 1e-6
+        else:
+            assert xj >= np.ceil(root[i - 3]) - 1e-6
+
+
+@pytest.mark.parametrize("k", [10, 400])
+def test_climbers_start_from_the_initial_solution(base_lp, k):
+    """An initial solution on the data model starts every climber (as new_bounds with an initial
+    solution does in the reference's batch): iterates follow the oracle's warm-started solves."""
+    rng = np.random.default_rng(8)
+    x0 = base_lp.x_star + 0.05 * rng.standard_normal(base_lp.n)
+    y0 = base_lp.y_star + 0.05 * rng.standard_normal(base_lp.m)
+    var, lo, up = _climbers(base_lp, 9, seed=6)
+    dm = datamodel_from_lp(base_lp)
+    dm.set_initial_primal_solution(x0)
+    dm.set_initial_dual_solution(y0)
+    sols, _ = lpm.SolveClimbers(dm, var, lo, up, settings(tol=1e-12, iteration_limit=k))
+    for b, sol in enumerate(sols):
+        res, x, y, _ = O.solve(_modified(base_lp, var[b], lo[b], up[b]), tol=1e-12,
+                               iteration_limit=k, initial_primal=x0, initial_dual=y0)
+        assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+        assert np.max(np.abs(sol.get_primal_solution() - x)) <= ITERATE_RTOL * (1 + np.abs(x).max())
+        assert np.max(np.abs(sol.get_dual_solution() - y)) <= ITERATE_RTOL * (1 + np.abs(y).max())
 
 
 def test_crossing_climber_is_infeasible(base_lp):

@@ -138,3 +138,38 @@ def test_warm_start_from_a_nearby_point_converges_faster():
     warm, _, _, _ = O.solve(lp, tol=1e-6, initial_primal=x0, initial_dual=y0)
     assert cold["status"] == warm["status"] == 1
     assert warm["iterations"] < cold["iterations"]
+
+
+def test_given_step_size_and_primal_weight():
+    """A step size and primal weight passed in (as the strong-branching batch passes them)
+    replace the power iteration and the initial weight: passing the values the solver computes
+    itself changes nothing, and no power iteration runs."""
+    lp = gen.constructed_lp(200, 500, 8, seed=11)
+    cold, xc, yc, _ = O.solve(lp, tol=1e-12, iteration_limit=300)
+    step, weight = O.initial_step_and_weight(lp)
+    given, xg, yg, _ = O.solve(lp, tol=1e-12, iteration_limit=300, initial_step_size=step,
+                               initial_primal_weight=weight)
+    assert given["power_iterations"] == 0 < cold["power_iterations"]
+    assert given["step_size"] == cold["step_size"]
+    assert np.array_equal(xg, xc) and np.array_equal(yg, yc)
+    other, _, _, _ = O.solve(lp, tol=1e-12, iteration_limit=300, initial_step_size=0.5 * step,
+                             initial_primal_weight=2.0)
+    assert other["step_size"] == 0.5 * step
+
+
+def test_strong_branching_restatement():
+    """batch_pdlp_solve on the oracle: every branch starts from the LP's own solution; branches
+    that keep the LP's optimum feasible finish within a few checks."""
+    lp = gen.constructed_lp(200, 500, 8, seed=11)
+    rng = np.random.default_rng(5)
+    frac = rng.choice(lp.n, 3, replace=False)
+    root = lp.x_star[frac] + 0.5
+    out = O.strong_branching(lp, frac, root, tol=1e-6)
+    assert len(out) == 6
+    for i, (res, x, _, _) in enumerate(out):
+        j = frac[i % 3]
+        assert res["status"] == 1 and res["power_iterations"] == 0
+        if i < 3:
+            assert x[j] <= np.floor(root[i]) + 1e-6
+        else:
+            assert x[j] >= np.ceil(root[i - 3]) - 1e-6
