@@ -68,6 +68,7 @@ def main() -> None:
     ap.add_argument("--iterations", type=int, default=3)
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--time-limit", type=float, default=0.0)
+    ap.add_argument("--iteration-limit", type=int, default=0, help="climbers mode: > 0 caps iterations")
     ap.add_argument("--strong-branching", action="store_true",
                     help="climbers mode: time cuOptBatchPDLPStrongBranching instead")
     ap.add_argument("--refine", type=int, default=0, help="> 0: continue a mixed-precision solve in FP64 to 1e-8")
@@ -325,6 +326,8 @@ def run_climbers(a) -> dict:
     st.set_parameter(lpm.CUOPT_LOG_TO_CONSOLE, False)
     if a.time_limit > 0:
         st.set_parameter(lpm.CUOPT_TIME_LIMIT, a.time_limit)
+    if a.iteration_limit > 0:
+        st.set_parameter(lpm.CUOPT_ITERATION_LIMIT, a.iteration_limit)
     base = model()
     if a.strong_branching:
         frac = var[: a.count // 2]

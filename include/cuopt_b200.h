@@ -114,10 +114,11 @@ cuopt_int_t cuOptBatchSolve(const cuOptOptimizationProblem* problems,
 /* Climber batch (strong branching): solves `count` copies of `problem` that differ only in the
  * bounds of one variable each: copy i has variable variable_indices[i] bounded by
  * [lower_bounds[i], upper_bounds[i]].  Counterpart of the reference's pdlp_solver_settings_t::
- * new_bounds with solve_lp in batch mode (cpp/src/pdlp/solve.cu:740-882).  All copies share one
- * read of the matrix per PDHG sweep; each follows the iterates of a single solve of its LP (FP64).
- * solutions[i] receives copy i's solution (release with cuOptDestroySolution).  Returns
- * CUOPT_SUCCESS or the first error code. */
+ * new_bounds with solve_lp in batch mode (cpp/src/pdlp/solve.cu:1124-1342, pdlp.cu:1447-1746).
+ * All copies share one read of the matrix per PDHG sweep; each follows the iterates of a single
+ * solve of its LP (FP64), starting from the settings' initial solution when one is set.  A copy
+ * whose bounds cross is PrimalInfeasible without iterating.  solutions[i] receives copy i's
+ * solution (release with cuOptDestroySolution).  Returns CUOPT_SUCCESS or the first error code. */
 cuopt_int_t cuOptSolveClimbers(cuOptOptimizationProblem problem,
                                cuOptSolverSettings settings,
                                cuopt_int_t count,
@@ -127,9 +128,12 @@ cuopt_int_t cuOptSolveClimbers(cuOptOptimizationProblem problem,
                                cuOptSolution* solutions);
 
 /* Strong branching on `count` fractional variables (counterpart of the reference's
- * batch_pdlp_solve, cpp/src/pdlp/solve.cu:884-919): solutions[0 .. count) are the down branches
- * (fractional[i] bounded above by floor(root_solution[i])), solutions[count .. 2 count) the up
- * branches (bounded below by ceil(root_solution[i])); `solutions` holds 2 * count handles. */
+ * batch_pdlp_solve and run_batch_pdlp, cpp/src/pdlp/solve.cu:743-919): solutions[0 .. count) are
+ * the down branches (fractional[i] bounded above by floor(root_solution[i])),
+ * solutions[count .. 2 count) the up branches (bounded below by ceil(root_solution[i]));
+ * `solutions` holds 2 * count handles.  As in the reference, the LP itself is solved first
+ * (Stable3, no infeasibility detection, iteration limit 100000) and every branch starts from its
+ * solution, step size and primal weight, under the same limits. */
 cuopt_int_t cuOptBatchPDLPStrongBranching(cuOptOptimizationProblem problem,
                                           cuOptSolverSettings settings,
                                           cuopt_int_t count,

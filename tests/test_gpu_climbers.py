@@ -32,8 +32,9 @@ def _climbers(lp, count, seed):
 
 
 def _modified(lp, j, lo, up):
-    from dataclasses import replace
-    q = replace(lp, var_lo=lp.var_lo.copy(), var_up=lp.var_up.copy())
+    import copy
+    q = copy.copy(lp)
+    q.var_lo, q.var_up = np.array(lp.var_lo, dtype=np.float64), np.array(lp.var_up, dtype=np.float64)
     q.var_lo[j], q.var_up[j] = lo, up
     return q
 
@@ -143,3 +144,33 @@ def test_crossing_climber_is_infeasible(base_lp):
                                 [1.0, base_lp.var_up[1]], settings(tol=1e-6))
     assert sols[0].get_termination_status() == lpm.LPTerminationStatus.PrimalInfeasible
     assert sols[1].get_termination_status() == lpm.LPTerminationStatus.Optimal
+
+
+def test_afiro_strong_branching_like_the_reference(golden_dir):
+    """pdlp_test.cu:1615-1720 (strong_branching_test): afiro, fractional {1, 2, 4} at
+    {0.891, 0.109, 0.636429}.  Every branch has the status of the single solve of its LP and an
+    objective within 1e-1 of it (the reference's tolerance), consistent with its own x; the
+    new_bounds batch (cuOptSolveClimbers, cold start) agrees the same way.  Beyond the reference:
+    each branch takes the oracle's iteration count."""
+    dm = lpm.ReadMps(golden_dir / "afiro_original.mps")
+    v = oracle_view(dm)
+    frac, root = [1, 2, 4], [0.891, 0.109, 0.636429]
+    s = settings(tol=1e-4)
+    sols, _ = lpm.BatchPDLPStrongBranching(dm, frac, root, s)
+    var = frac + frac
+    lo = [v.var_lo[j] for j in frac] + [np.ceil(r) for r in root]
+    up = [np.floor(r) for r in root] + [v.var_up[j] for j in frac]
+    cold, _ = lpm.SolveClimbers(dm, var, lo, up, s)
+    ref = O.strong_branching(v, frac, root, tol=1e-4)
+    assert len(sols) == len(cold) == 6
+    for i in range(6):
+        q = _modified(v, var[i], lo[i], up[i])
+        single = lpm.Solve(datamodel_from_lp(q, offset=v.obj_offset), s)
+        for sol in (sols[i], cold[i]):
+            assert sol.get_termination_status() == single.get_termination_status()
+            assert abs(sol.get_primal_objective() - single.get_primal_objective()) <= 1e-1
+            x = sol.get_primal_solution()
+            assert abs(float(v.c @ x) + v.obj_offset - sol.get_primal_objective()) <= \
+                1e-9 * (1 + abs(sol.get_primal_objective()))
+            assert lo[i] - 1e-9 <= x[var[i]] <= up[i] + 1e-9
+        assert sols[i].get_lp_stats()["nb_iterations"] == ref[i][0]["iterations"]
