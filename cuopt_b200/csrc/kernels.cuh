@@ -66,8 +66,9 @@ struct red_t {
   double v[K > 0 ? K : 1];
 };
 
-// Block reduction of K doubles; threads 0..K-1 write partials[slot * K + r].
-template <int K>
+// Block reduction of K doubles (sums, or maxima when MAX); threads 0..K-1 write
+// partials[slot * K + r].
+template <int K, bool MAX = false>
 __device__ __forceinline__ void block_reduce_store(red_t<K>& r, double* partials, int slot)
 {
   if constexpr (K > 0) {
@@ -75,23 +76,31 @@ __device__ __forceinline__ void block_reduce_store(red_t<K>& r, double* partials
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int q = 0; q < K; ++q) {
-      double v = warp_sum(r.v[q]);
+      double v = MAX ? warp_max(r.v[q]) : warp_sum(r.v[q]);
       if (lane == 0) sm[warp][q] = v;
     }
     __syncthreads();
     if (threadIdx.x < K) {
-      double s = 0.0;
+      double s = MAX ? sm[0][threadIdx.x] : 0.0;
 #pragma unroll
-      for (int w = 0; w < kWarpsPerBlock; ++w) s += sm[w][threadIdx.x];
+      for (int w = 0; w < kWarpsPerBlock; ++w)
+        s = MAX ? fmax(s, sm[w][threadIdx.x]) : s + sm[w][threadIdx.x];
       partials[(size_t)slot * K + threadIdx.x] = s;
     }
   }
 }
-template <int K>
+template <int K, bool MAX = false>
 __device__ __forceinline__ void block_reduce_store(red_t<K>& r, double* partials)
 {
-  block_reduce_store<K>(r, partials, (int)blockIdx.x);
+  block_reduce_store<K, MAX>(r, partials, (int)blockIdx.x);
 }
+
+// Epilogues may declare `static constexpr bool kMaxRed = true`: their block values are then
+// combined by maxima instead of sums.
+template <class E, class = void>
+struct has_max_red : std::false_type {};
+template <class E>
+struct has_max_red<E, std::void_t<decltype(E::kMaxRed)>> : std::bool_constant<E::kMaxRed> {};
 
 // out[q] = sum over blocks of partials[b*K+q], summed by one block (ordered, compensated).
 template <int K>
@@ -116,6 +125,26 @@ __global__ void __launch_bounds__(kBlock) finalize_sum_kernel(const double* part
                                                               double* out)
 {
   ordered_block_sum<K>(partials, nblocks, out);
+}
+
+// out[q] = max over blocks of partials[b*K+q] (single block).
+template <int K>
+__global__ void __launch_bounds__(kBlock) finalize_max_kernel(const double* partials, int nblocks,
+                                                              double* out)
+{
+  __shared__ double sm[kBlock];
+  for (int q = 0; q < K; ++q) {
+    double v = -INFINITY;
+    for (int b = threadIdx.x; b < nblocks; b += kBlock) v = fmax(v, partials[(size_t)b * K + q]);
+    sm[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = kBlock / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + s]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[q] = sm[0];
+    __syncthreads();
+  }
 }
 
 // 4 consecutive values of one lane chunk (16-byte aligned), streamed with evict-first loads.
@@ -171,7 +200,7 @@ __global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
   for (int q = 0; q < (K > 0 ? K : 1); ++q) red.v[q] = 0.0;
   if (epi.skip()) {
     // Uniform early exit (e.g. converged power iteration): every block still stores zeros.
-    block_reduce_store<K>(red, partials);
+    block_reduce_store<K, has_max_red<Epi>::value>(red, partials);
     return;
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -233,7 +262,7 @@ __global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
       if (valid) epi(row, acc, pre, red);
     }
   }
-  block_reduce_store<K>(red, partials);
+  block_reduce_store<K, has_max_red<Epi>::value>(red, partials);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -465,6 +494,48 @@ struct term_dual_epi {
     r.v[0] += rd * rd;
     r.v[1] += cj * xj;
     r.v[2] += sj * xj;
+  }
+};
+
+// Per-constraint forms of the residuals (per_constraint_residual; reference
+// convergence_information.cu:390-420, 453-470 with relative_residual_t, utils.cuh:578-590):
+// max(0, max_i r_p,i - rel * max(|l_i|, |u_i|) over the finite bounds (combine_finite_abs_bounds,
+// utils.cuh:180-188)) over the rows of A, and max(0, max_j r_d,j - rel * c_j) over the rows of A^T.
+struct term_linf_primal_epi {
+  static constexpr int kRed     = 1;
+  static constexpr bool kMaxRed = true;
+  const double* lc;
+  const double* uc;
+  double rel;
+  struct pre_t {
+    double l, u;
+  };
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ pre_t load(int i) const { return pre_t{lc[i], uc[i]}; }
+  __device__ __forceinline__ void operator()(int, double ax, const pre_t& p, red_t<1>& r) const
+  {
+    const double rp = ax - fmax(p.l, fmin(ax, p.u));
+    double cb       = 0.0;
+    if (isfinite(p.u)) cb = fmax(cb, fabs(p.u));
+    if (isfinite(p.l)) cb = fmax(cb, fabs(p.l));
+    r.v[0] = fmax(r.v[0], rp - rel * cb);
+  }
+};
+struct term_linf_dual_epi {
+  static constexpr int kRed     = 1;
+  static constexpr bool kMaxRed = true;
+  const double* c;
+  const double* s;
+  double rel;
+  struct pre_t {
+    double c, s;
+  };
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ pre_t load(int j) const { return pre_t{c[j], s[j]}; }
+  __device__ __forceinline__ void operator()(int, double aty, const pre_t& p, red_t<1>& r) const
+  {
+    const double rd = (p.c - aty) - p.s;
+    r.v[0]          = fmax(r.v[0], rd - rel * p.c);
   }
 };
 

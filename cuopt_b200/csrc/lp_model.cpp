@@ -370,6 +370,7 @@ pdlp_params params_from_settings(const lp_settings& st)
   prm.refinement_tol    = st.f(CUOPT_PDLP_REFINEMENT_TOLERANCE);
   prm.log_to_console    = st.b(CUOPT_LOG_TO_CONSOLE);
   prm.detect_infeasibility  = st.b(CUOPT_INFEASIBILITY_DETECTION);
+  prm.per_constraint_residual = st.b(CUOPT_PER_CONSTRAINT_RESIDUAL);
   prm.primal_infeasible_tol = st.f(CUOPT_PRIMAL_INFEASIBLE_TOLERANCE);
   prm.dual_infeasible_tol   = st.f(CUOPT_DUAL_INFEASIBLE_TOLERANCE);
   return prm;
@@ -626,6 +627,12 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
 std::vector<lp_solution> solve_batch(const std::vector<const lp_problem*>& ps, const lp_settings& st)
 {
   std::vector<lp_solution> out(ps.size());
+  // The block-diagonal batch evaluates l2 residuals only; the per-constraint criterion solves the
+  // problems one at a time, as the reference's batch of independent solves does.
+  if (st.b(CUOPT_PER_CONSTRAINT_RESIDUAL)) {
+    for (size_t i = 0; i < ps.size(); ++i) out[i] = solve_problem(*ps[i], st);
+    return out;
+  }
   std::vector<std::vector<double>> lo(ps.size()), up(ps.size());
   std::vector<size_t> eligible;
   for (size_t i = 0; i < ps.size(); ++i) {
@@ -670,6 +677,11 @@ std::vector<lp_solution> solve_climbers(const lp_problem& p, const lp_settings& 
 {
   const int count = (int)var.size();
   std::vector<lp_solution> out(count);
+  if (st.b(CUOPT_PER_CONSTRAINT_RESIDUAL)) {  // as the reference (convergence_information.cu:393-395)
+    for (auto& o : out)
+      set_error(o, CUOPT_VALIDATION_ERROR, "Batch mode not supported for per_constraint_residual");
+    return out;
+  }
   for (int b = 0; b < count; ++b)
     if (var[b] < 0 || var[b] >= p.n) {
       for (auto& o : out) set_error(o, CUOPT_INVALID_ARGUMENT, "climber variable out of range");

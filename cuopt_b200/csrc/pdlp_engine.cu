@@ -39,6 +39,7 @@ inline dev_sell<double> view64(const dev_matrix& M) { return view_of<double>(M, 
 
 struct conv_info {
   double l2_primal, l2_dual, primal_obj, dual_obj, gap, abs_obj;
+  double linf_primal = 0, linf_dual = 0;  // per-constraint forms, when asked for
 };
 
 // Iteration count and restart / PID state of the main loop (host side).
@@ -634,11 +635,30 @@ class engine {
     finalize_sum_kernel<3><<<1, kBlock, 0, s_>>>(partials_.data(), sell_grid(AT),
                                                  dres_.data() + 2);
     launches_ += 4;
+    int nres = 5;
+    if (p_.per_constraint_residual) {
+      sell_map_kernel<double, double, term_linf_primal_epi><<<sell_grid(A), kBlock, 0, s_>>>(
+        A, xu_.data(), term_linf_primal_epi{lc64_.data(), uc64_.data(), p_.rel_primal},
+        partials_.data());
+      finalize_max_kernel<1><<<1, kBlock, 0, s_>>>(partials_.data(), sell_grid(A),
+                                                   dres_.data() + 5);
+      sell_map_kernel<double, double, term_linf_dual_epi><<<sell_grid(AT), kBlock, 0, s_>>>(
+        AT, yu_.data(), term_linf_dual_epi{c64_.data(), su_.data(), p_.rel_dual},
+        partials_.data());
+      finalize_max_kernel<1><<<1, kBlock, 0, s_>>>(partials_.data(), sell_grid(AT),
+                                                   dres_.data() + 6);
+      launches_ += 4;
+      nres = 7;
+    }
     B200_LAUNCH_CHECK();
     B200_CUDA_CHECK(
-      cudaMemcpyAsync(hres_, dres_.data(), 5 * sizeof(double), cudaMemcpyDeviceToHost, s_));
+      cudaMemcpyAsync(hres_, dres_.data(), nres * sizeof(double), cudaMemcpyDeviceToHost, s_));
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
     conv_info cv;
+    if (p_.per_constraint_residual) {
+      cv.linf_primal = hres_[5];
+      cv.linf_dual   = hres_[6];
+    }
     cv.l2_primal  = std::sqrt(hres_[0]);
     cv.l2_dual    = std::sqrt(hres_[2]);
     cv.primal_obj = hres_[3];
@@ -658,8 +678,10 @@ class engine {
     r.iterations = k;
     r.primal_obj = cv.primal_obj;
     r.dual_obj   = cv.dual_obj;
-    r.l2_primal  = cv.l2_primal;
-    r.l2_dual    = cv.l2_dual;
+    // With per_constraint_residual the statistics carry the per-constraint forms (reference
+    // termination_strategy.cu:540-566).
+    r.l2_primal  = p_.per_constraint_residual ? cv.linf_primal : cv.l2_primal;
+    r.l2_dual    = p_.per_constraint_residual ? cv.linf_dual : cv.l2_dual;
     r.rel_primal = cv.l2_primal / (1.0 + b_norm_);
     r.rel_dual   = cv.l2_dual / (1.0 + c_norm_);
     r.gap        = cv.gap;
@@ -779,10 +801,14 @@ class engine {
       bool restarted   = false;
       if (major || cond) {
         const conv_info cv = evaluate();
-        const bool primal_ok = cv.l2_primal <= p_.abs_primal + p_.rel_primal * b_norm_;
+        // check_termination_criteria_kernel (reference termination_strategy.cu:311-352)
+        const bool pcr       = p_.per_constraint_residual;
+        const bool primal_ok = pcr ? cv.linf_primal <= p_.abs_primal
+                                   : cv.l2_primal <= p_.abs_primal + p_.rel_primal * b_norm_;
+        const bool dual_ok   = pcr ? cv.linf_dual <= p_.abs_dual
+                                   : cv.l2_dual <= p_.abs_dual + p_.rel_dual * c_norm_;
         int status           = kNoTermination;
-        if (cv.l2_dual <= p_.abs_dual + p_.rel_dual * c_norm_ && primal_ok &&
-            cv.gap <= p_.abs_gap + p_.rel_gap * cv.abs_obj)
+        if (dual_ok && primal_ok && cv.gap <= p_.abs_gap + p_.rel_gap * cv.abs_obj)
           status = kOptimal;
         else if (primal_ok)
           status = kPrimalFeasible;

@@ -43,6 +43,9 @@ struct pdlp_params {
   bool detect_infeasibility   = false;
   double primal_infeasible_tol = 1e-10;
   double dual_infeasible_tol   = 1e-10;
+  // CUOPT_PER_CONSTRAINT_RESIDUAL: the primal / dual tests (and the reported residuals) use the
+  // per-constraint maxima instead of the l2 norms.
+  bool per_constraint_residual = false;
   std::vector<double> initial_primal;  // user order, optional
   std::vector<double> initial_dual;    // user order, optional
   // Given by the warm start of a strong-branching batch (the reference's run_batch_pdlp,

@@ -30,7 +30,7 @@ class _Settings(C.Structure):
                 ("abs_gap", C.c_double), ("rel_gap", C.c_double),
                 ("iteration_limit", C.c_long), ("time_limit", C.c_double), ("threads", C.c_int),
                 ("detect_infeasibility", C.c_int), ("primal_infeasible_tolerance", C.c_double),
-                ("dual_infeasible_tolerance", C.c_double)]
+                ("dual_infeasible_tolerance", C.c_double), ("per_constraint_residual", C.c_int)]
 
 
 class _Result(C.Structure):
@@ -91,14 +91,15 @@ def _holder(lp, initial_primal=None, initial_dual=None, initial_step_size=None,
 
 def solve(lp, tol=1e-4, iteration_limit=2**31 - 1, time_limit=1e300, threads=0,
           detect_infeasibility=False, infeasible_tol=1e-10, initial_primal=None, initial_dual=None,
-          initial_step_size=None, initial_primal_weight=None):
+          initial_step_size=None, initial_primal_weight=None, per_constraint_residual=False):
     """Runs the FP64 Stable3 restatement (optionally warm-started from an initial primal and / or
     dual solution in the user's order, and from a given step size and primal weight).  Returns
     (result dict, x, y, reduced_cost)."""
     h = _holder(lp, initial_primal, initial_dual, initial_step_size, initial_primal_weight)
     m, n = h.s.m, h.s.n
     st = _Settings(tol, tol, tol, tol, tol, tol, int(iteration_limit), float(time_limit), int(threads),
-                   int(bool(detect_infeasibility)), float(infeasible_tol), float(infeasible_tol))
+                   int(bool(detect_infeasibility)), float(infeasible_tol), float(infeasible_tol),
+                   int(bool(per_constraint_residual)))
     r = _Result()
     x, y, rc = np.zeros(n), np.zeros(m), np.zeros(n)
     lib().oracle_pdlp_solve(C.byref(h.s), C.byref(st), C.byref(r), x.ctypes.data, y.ctypes.data,

@@ -329,10 +329,15 @@ double power_iteration(const lp_t& q, int* iters_out)
 
 struct conv_t {
   double l2_primal = 0, l2_dual = 0, primal_obj = 0, dual_obj = 0, gap = 0, abs_obj = 0;
+  // per_constraint_residual: max(0, max_i r_i - rel * rhs_i), rhs = combined bound / c_j
+  double linf_primal = 0, linf_dual = 0;
 };
 
-// compute_convergence_information for the reflected variant (convergence_information.cu:327-811)
-conv_t convergence(const lp_t& p, const vec& x, const vec& y, const vec& slack)
+// compute_convergence_information for the reflected variant (convergence_information.cu:327-811);
+// the per-constraint forms follow :390-420, :453-470 with relative_residual_t (utils.cuh:578-590)
+// and combine_finite_abs_bounds (utils.cuh:180-188).
+conv_t convergence(const lp_t& p, const vec& x, const vec& y, const vec& slack, double rel_primal,
+                   double rel_dual)
 {
   const int m = p.a.rows, n = p.a.cols;
   conv_t r;
@@ -349,6 +354,13 @@ conv_t convergence(const lp_t& p, const vec& x, const vec& y, const vec& slack)
   spmv(p.at, y.data(), aty.data());
   for (int j = 0; j < n; ++j) rd[j] = (p.c[j] - aty[j]) - slack[j];
   r.l2_dual = nrm2(rd);
+  for (int i = 0; i < m; ++i) {
+    double cb = 0.0;
+    if (std::isfinite(p.con_up[i])) cb = std::max(cb, std::fabs(p.con_up[i]));
+    if (std::isfinite(p.con_lo[i])) cb = std::max(cb, std::fabs(p.con_lo[i]));
+    r.linf_primal = std::max(r.linf_primal, rp[i] - rel_primal * cb);
+  }
+  for (int j = 0; j < n; ++j) r.linf_dual = std::max(r.linf_dual, rd[j] - rel_dual * p.c[j]);
   r.dual_obj =
     dot(slack, x) + chunk_sum(m, [&](int i) { return pslack[i]; });
   if (p.obj_scale != 1.0 || p.obj_offset != 0.0) {
@@ -392,6 +404,7 @@ struct oracle_settings {
   int threads;
   int detect_infeasibility;                                   // CUOPT_INFEASIBILITY_DETECTION
   double primal_infeasible_tolerance, dual_infeasible_tolerance;
+  int per_constraint_residual;                                // CUOPT_PER_CONSTRAINT_RESIDUAL
 };
 
 struct oracle_result {
@@ -555,8 +568,10 @@ int oracle_pdlp_solve(const oracle_lp* in, const oracle_settings* st, oracle_res
     res->iterations  = (int)internal_iters;
     res->primal_obj  = cv.primal_obj;
     res->dual_obj    = cv.dual_obj;
-    res->l2_primal   = cv.l2_primal;
-    res->l2_dual     = cv.l2_dual;
+    // With per_constraint_residual the statistics carry the per-constraint forms
+    // (termination_strategy.cu:540-566).
+    res->l2_primal   = st->per_constraint_residual ? cv.linf_primal : cv.l2_primal;
+    res->l2_dual     = st->per_constraint_residual ? cv.linf_dual : cv.l2_dual;
     res->rel_primal  = cv.l2_primal / (1.0 + b_norm);
     res->rel_dual    = cv.l2_dual / (1.0 + c_norm);
     res->gap         = cv.gap;
@@ -580,11 +595,15 @@ int oracle_pdlp_solve(const oracle_lp* in, const oracle_settings* st, oracle_res
     std::vector<int> restarted(1, 0);
     if (is_major || is_cond) {
       unscale(s, x_hat, y_hat, slack);
-      conv_t cv = convergence(p, x_hat, y_hat, slack);
+      conv_t cv = convergence(p, x_hat, y_hat, slack, st->rel_primal, st->rel_dual);
       int status = kNoTermination;
-      const bool primal_ok = cv.l2_primal <= st->abs_primal + st->rel_primal * b_norm;
-      if (cv.l2_dual <= st->abs_dual + st->rel_dual * c_norm && primal_ok &&
-          cv.gap <= st->abs_gap + st->rel_gap * cv.abs_obj)
+      // check_termination_criteria_kernel (termination_strategy.cu:311-352)
+      const bool pcr       = st->per_constraint_residual != 0;
+      const bool primal_ok = pcr ? cv.linf_primal <= st->abs_primal
+                                 : cv.l2_primal <= st->abs_primal + st->rel_primal * b_norm;
+      const bool dual_ok   = pcr ? cv.linf_dual <= st->abs_dual
+                                 : cv.l2_dual <= st->abs_dual + st->rel_dual * c_norm;
+      if (dual_ok && primal_ok && cv.gap <= st->abs_gap + st->rel_gap * cv.abs_obj)
         status = kOptimal;
       else if (primal_ok)
         status = kPrimalFeasible;

@@ -252,3 +252,59 @@ def test_mixed_step_size_from_lanczos_matches_power_iteration(cfg):
     b = lpm.Solve(dm, settings(tol=1e-12, iteration_limit=0))
     assert rel(a.stats["step_size"], b.stats["step_size"]) <= 1e-5
     assert a.stats["power_iterations"] < b.stats["power_iterations"]
+
+
+def _pcr_settings(tol, iteration_limit=None, on=True):
+    s = settings(tol=tol, iteration_limit=iteration_limit)
+    s.set_parameter(lpm.CUOPT_PER_CONSTRAINT_RESIDUAL, bool(on))
+    return s
+
+
+def test_per_constraint_residual_on_the_reference_point():
+    """pdlp_test.cu:640-733: A = I (3 x 3), 0 <= Ax <= 0, c = 0; at x = (0.02, 0.03, 0.1) the
+    per-constraint primal residual is exactly 0.1 while the l2 one is 0.106."""
+    from types import SimpleNamespace
+    z = np.zeros(3)
+    lp = SimpleNamespace(row_off=np.arange(4), col_idx=np.arange(3), val=np.ones(3), c=z,
+                         con_lo=z, con_up=z, var_lo=np.full(3, -np.inf), var_up=np.full(3, np.inf))
+    dm = datamodel_from_lp(lp)
+    dm.set_initial_primal_solution(np.array([0.02, 0.03, 0.1]))
+    pcr = lpm.Solve(dm, _pcr_settings(0.1, iteration_limit=0))
+    l2 = lpm.Solve(dm, _pcr_settings(0.1, iteration_limit=0, on=False))
+    assert pcr.get_lp_stats()["primal_residual"] == 0.1
+    assert l2.get_lp_stats()["primal_residual"] == np.sqrt(0.02 ** 2 + 0.03 ** 2 + 0.1 ** 2)
+
+
+@pytest.mark.parametrize("scale_c", [1.0, 0.05])
+def test_per_constraint_residual_matches_oracle(small_lp, scale_c):
+    """The per-constraint criterion (CUOPT_PER_CONSTRAINT_RESIDUAL) stops at the oracle's
+    iteration with the oracle's status and reported maxima.  With c as generated its dual form
+    cannot be met (it subtracts rel * c_j with c_j's sign, as the reference does); with c scaled
+    to |c_j| < 1 the solve ends Optimal."""
+    from dataclasses import replace
+    lp = replace(small_lp, c=small_lp.c * scale_c)
+    tol = 1e-4
+    sol = lpm.Solve(datamodel_from_lp(lp), _pcr_settings(tol, iteration_limit=3000))
+    res, x, _, _ = O.solve(lp, tol=tol, iteration_limit=3000, per_constraint_residual=True)
+    assert int(sol.get_termination_status()) == res["status"] == (4 if scale_c == 1.0 else 1)
+    assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+    st = sol.get_lp_stats()
+    assert abs(st["primal_residual"] - res["l2_primal"]) <= 1e-9 * (1e-3 + res["l2_primal"])
+    assert abs(st["dual_residual"] - res["l2_dual"]) <= 1e-9 * (1e-3 + res["l2_dual"])
+    assert np.max(np.abs(sol.get_primal_solution() - x)) <= ITERATE_RTOL * (1 + np.abs(x).max())
+
+
+def test_per_constraint_residual_in_batches(small_lp):
+    """cuOptBatchSolve solves the problems one at a time under the per-constraint criterion (the
+    reference's batch is independent solves); climber batches reject it, as the reference's batch
+    mode does (convergence_information.cu:393-395)."""
+    from dataclasses import replace
+    lp = replace(small_lp, c=small_lp.c * 0.05)
+    s = _pcr_settings(1e-4, iteration_limit=3000)
+    sols, _ = lpm.BatchSolve([datamodel_from_lp(lp), datamodel_from_lp(lp)], s)
+    single = lpm.Solve(datamodel_from_lp(lp), s)
+    for sol in sols:
+        assert sol.get_termination_status() == single.get_termination_status()
+        assert np.array_equal(sol.get_primal_solution(), single.get_primal_solution())
+    climbers, _ = lpm.SolveClimbers(datamodel_from_lp(lp), [0], [lp.var_lo[0]], [lp.var_up[0]], s)
+    assert climbers[0].get_error_status() == 4  # CUOPT_VALIDATION_ERROR

@@ -173,3 +173,46 @@ def test_strong_branching_restatement():
             assert x[j] <= np.floor(root[i]) + 1e-6
         else:
             assert x[j] >= np.ceil(root[i - 3]) - 1e-6
+
+
+def _identity_lp():
+    """pdlp_test.cu:640-733: A = I (3 x 3), 0 <= Ax <= 0, c = 0, free variables."""
+    from types import SimpleNamespace
+    z = np.zeros(3)
+    return SimpleNamespace(row_off=np.arange(4), col_idx=np.arange(3), val=np.ones(3), c=z,
+                           con_lo=z, con_up=z, var_lo=np.full(3, -np.inf),
+                           var_up=np.full(3, np.inf), obj_offset=0.0, maximize=False, m=3, n=3)
+
+
+def test_per_constraint_residual_on_the_reference_point():
+    """pdlp_test.cu:640-733: at x = (0.02, 0.03, 0.1) the per-constraint primal residual is
+    exactly 0.1 (and passes an absolute tolerance of 0.1) while the l2 residual is 0.106."""
+    x0 = np.array([0.02, 0.03, 0.1])
+    pcr, _, _, _ = O.solve(_identity_lp(), tol=0.1, iteration_limit=0, initial_primal=x0,
+                           per_constraint_residual=True)
+    l2, _, _, _ = O.solve(_identity_lp(), tol=0.1, iteration_limit=0, initial_primal=x0)
+    assert pcr["l2_primal"] == 0.1
+    assert l2["l2_primal"] == np.sqrt(0.02 ** 2 + 0.03 ** 2 + 0.1 ** 2) > 0.1
+
+
+def test_per_constraint_residual_solve():
+    """Under the per-constraint criterion the reported residuals are the per-constraint maxima of
+    the returned point (checked here in numpy).  The dual form subtracts rel * c_j with the sign of
+    c_j, as the reference does, so with c_j < -1 it stays above the tolerance: this LP runs to its
+    iteration limit."""
+    lp = gen.constructed_lp(200, 500, 8, seed=11)
+    tol = 1e-3
+    res, x, y, rc = O.solve(lp, tol=tol, iteration_limit=1000, time_limit=30,
+                            per_constraint_residual=True)
+    assert res["status"] == 4
+    A = np.zeros((lp.m, lp.n))
+    rows = np.repeat(np.arange(lp.m), np.diff(lp.row_off))
+    A[rows, lp.col_idx] = lp.val
+    ax = A @ x
+    rp = ax - np.clip(ax, lp.con_lo, lp.con_up)
+    cb = np.maximum(np.where(np.isfinite(lp.con_up), np.abs(lp.con_up), 0),
+                    np.where(np.isfinite(lp.con_lo), np.abs(lp.con_lo), 0))
+    rd = (lp.c - A.T @ y) - rc
+    assert abs(res["l2_primal"] - max(0.0, np.max(rp - tol * cb))) <= 1e-12
+    assert abs(res["l2_dual"] - max(0.0, np.max(rd - tol * lp.c))) <= 1e-12
+    assert res["l2_dual"] > tol < tol * np.max(-lp.c)
