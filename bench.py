@@ -17,6 +17,8 @@ iterates, FP64 termination / restart / step ratio).  The same solve in plain FP6
   batch_c3  config 3: 512 seeded LPs of uneven sizes (m log-uniform in [200, 20000], n = 2.5 m,
             6-12 non-zeros per column) solved in FP64 to 1e-6 by one cuOptBatchSolve call, against
             a sample of the same LPs solved one by one with cuOptSolve.
+  batch_c3_mixed  the same in mixed precision (batch and single solves): Lanczos step sizes, FP32
+            sweeps; an instance whose FP32 iterates stall is solved again in FP64.
   adjoint_c4  config 4: 64 non-degenerate 5000 x 10000 LPs solved in one batched call with
             crossover, L = sum w * x* back-propagated through the KKT adjoint, gradients checked
             against the exact basis derivatives and central differences (h = 1e-6).
@@ -396,12 +398,16 @@ def run_b200(args):
                          f"({s_iter * 1e3:.1f} ms each), scaled by the {iters} iterations of the FP64 solve",
                "pdhg_iter_per_s": 1.0 / s_iter}
 
-    # Config 3: 512 uneven FP64 LPs in one batched call vs the same LPs one by one (rank 0, N = 1).
-    batch = None
+    # Config 3: 512 uneven FP64 LPs in one batched call vs the same LPs one by one (rank 0, N = 1),
+    # then the same in mixed precision.
+    batch = batch_mixed = None
     if rank == 0 and world == 1 and not args.no_batch:
         from cuopt_b200.profile import run_batch
         batch = run_batch(argparse.Namespace(count=512, sequential=args.batch_sequential,
                                              repeats=2, tol=1e-6, time_limit=120.0))
+        batch_mixed = run_batch(argparse.Namespace(count=512, sequential=args.batch_sequential,
+                                                   repeats=2, tol=1e-6, time_limit=120.0,
+                                                   batch_precision="mixed"))
     # Config 4: 64 non-degenerate 5000 x 10000 LPs, batched forward (crossover) + KKT adjoint.
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint:
@@ -424,7 +430,8 @@ def run_b200(args):
         "pdhg_iter_per_s": last_mixed["number_of_steps_taken"] / (last_mixed["loop_time"] or 1e-9),
         "setup_s": last_mixed["setup_time"], "loop_s": last_mixed["loop_time"],
         "objective_rel_error": obj_err_mixed, "kkt": kkt_mixed, "fp64": fp64,
-        "mixed_refined_to_1e-8": refine, "batch_c3": batch, "adjoint_c4": adjoint,
+        "mixed_refined_to_1e-8": refine, "batch_c3": batch, "batch_c3_mixed": batch_mixed,
+        "adjoint_c4": adjoint,
         "roofline": roofline, "cpu_baseline": cpu,
         "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "LPs/s to 1e-6 rel. KKT",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,

@@ -524,6 +524,83 @@ __global__ void b_power_check_kernel(const int* chunk_off, int count, const doub
   }
 }
 
+// Golub-Kahan-Lanczos step size per instance (mixed precision), the single engine's
+// lanczos_step_size run on every instance at once: u and v hold the unnormalised Lanczos vectors,
+// st[b] their norms, and rowbuf the squares of the new vector for the per-instance norms.
+struct b_gk_state {
+  double beta;
+  double alpha;
+};
+
+// Row j of A^T applied to u:  p_j = (A^T u)_j / beta - beta v_j / alpha  (written over v_j).
+struct b_gk_primal_epi {
+  static constexpr int kRed = 0;
+  double* v;
+  double* rowbuf;
+  const b_gk_state* st;
+  inst_ctx ctx;
+  struct pre_t {
+    double v;
+    int b;
+  };
+  __device__ bool skip() const { return false; }
+  __device__ bool skip_range(int r0, int r1) const { return ctx.all_frozen(r0, r1); }
+  __device__ __forceinline__ pre_t load(int j) const { return pre_t{v[j], ctx.inst[j]}; }
+  __device__ __forceinline__ void operator()(int j, double acc, const pre_t& p, red_t<0>&) const
+  {
+    if (!ctx.active[p.b]) return;
+    const double b = st[p.b].beta, a = st[p.b].alpha;
+    const double pj = acc / b - (a > 0.0 ? b * (p.v / a) : 0.0);
+    v[j]            = pj;
+    rowbuf[j]       = pj * pj;
+  }
+};
+
+// Row i of A applied to v:  q_i = (A v)_i / alpha - alpha u_i / beta  (written over u_i).
+struct b_gk_dual_epi {
+  static constexpr int kRed = 0;
+  double* u;
+  double* rowbuf;
+  const b_gk_state* st;
+  inst_ctx ctx;
+  struct pre_t {
+    double u;
+    int b;
+  };
+  __device__ bool skip() const { return false; }
+  __device__ bool skip_range(int r0, int r1) const { return ctx.all_frozen(r0, r1); }
+  __device__ __forceinline__ pre_t load(int i) const { return pre_t{u[i], ctx.inst[i]}; }
+  __device__ __forceinline__ void operator()(int i, double acc, const pre_t& p, red_t<0>&) const
+  {
+    if (!ctx.active[p.b]) return;
+    const double a = st[p.b].alpha, b = st[p.b].beta;
+    const double qi = acc / a - a * (p.u / b);
+    u[i]            = qi;
+    rowbuf[i]       = qi * qi;
+  }
+};
+
+// Per iterating instance b, the norm of its new vector from the chunk sums: FIELD 0 sets alpha
+// (hist[k * count + b]), FIELD 1 sets beta (hist[(k + 1) * count + b]).
+template <int FIELD>
+__global__ void b_gk_record_kernel(const int* chunk_off, int count, const double* part,
+                                   const int* active, b_gk_state* st, double* hist, int k)
+{
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < count; b += gridDim.x * blockDim.x) {
+    if (!active[b]) continue;
+    double t = 0.0;
+    for (int c = chunk_off[b]; c < chunk_off[b + 1]; ++c) t += part[c];
+    const double v = sqrt(t);
+    if (FIELD == 0) {
+      st[b].alpha                     = v;
+      hist[(size_t)k * count + b]     = v;
+    } else {
+      st[b].beta                      = v;
+      hist[(size_t)(k + 1) * count + b] = v;
+    }
+  }
+}
+
 // ------------------------------------------------------------------------------------------------
 // Host side
 
@@ -672,8 +749,13 @@ class batch_engine {
     trace("batch: ranges + scaling");
     prepare_vectors();
     trace("batch: vectors");
-    power_iteration();
-    trace("batch: power iteration");
+    // Step size from the largest singular value of each scaled instance: the power iteration
+    // (reference pdlp.cu:2620-2731), or Golub-Kahan-Lanczos in mixed precision, as single solves.
+    if (p_.precision == 1)
+      lanczos_step_size();
+    else
+      power_iteration();
+    trace("batch: step size");
 
     xu_.resize(n);
     su_.resize(n);
@@ -732,9 +814,9 @@ class batch_engine {
 
   void fill(double* p, int n, double v)
   {
-    std::vector<double> h(n, v);
-    B200_CUDA_CHECK(cudaMemcpyAsync(p, h.data(), n * sizeof(double), cudaMemcpyHostToDevice, s_));
-    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    fill_kernel<<<vgrid_, kBlock, 0, s_>>>(p, n, v);
+    ++launches_;
+    B200_LAUNCH_CHECK();
   }
 
   // Per-instance sums of K planes of the row buffer over rows (ROWS) or columns; result in
@@ -933,6 +1015,113 @@ class batch_engine {
     for (int b = 0; b < B_; ++b) {
       eta_[b]         = kStepScaling / std::sqrt(h[b].s2);
       power_iters_[b] = h[b].iters;
+    }
+  }
+
+  // Golub-Kahan-Lanczos on every instance (the single engine's lanczos_step_size, per instance):
+  // chunks of kLanczosChunk steps; after each chunk an instance whose sigma_max^2 estimate moved by
+  // at most kLanczosTol (relative), or whose recurrence broke down, stops, and the sweeps shrink
+  // to the instances still iterating once they are at most half of those listed.
+  void lanczos_step_size()
+  {
+    const int m = in_.m, n = in_.n;
+    const int ld = kLanczosMaxSteps + 2;  // history rows (steps), each B_ wide
+    std::vector<double> z0(m);
+    for (int b = 0; b < B_; ++b) {
+      std::mt19937 gen(1);
+      std::normal_distribution<double> dist(0.0, 1.0);
+      for (int i = in_.row_start[b]; i < in_.row_start[b + 1]; ++i) z0[i] = dist(gen);
+    }
+    dbuf<double> u(m), v(n), tmp(m), alphas((size_t)B_ * ld), betas((size_t)B_ * ld);
+    dbuf<b_gk_state> st(B_);
+    tmp.upload(z0.data(), m, s_);
+    permute_gather(tmp.data(), L_.row_new2old.data(), m, 1.0, u.data(), s_);
+    v.zero(s_);
+    st.zero(s_);
+    dbuf<int> pact(B_);
+    std::vector<int> pact_h(B_, 1);
+    pact.upload(pact_h.data(), B_, s_);
+    const inst_ctx rctx{rinst_.data(), pact.data(), nullptr};
+    const inst_ctx cctx{cinst_.data(), pact.data(), nullptr};
+    dbuf<double> part_r(std::max(rows_.count, 1)), part_c(std::max(cols_.count, 1));
+    // beta_0 = |z0| per instance (betas[b * ld + 0])
+    b_chunk_sumsq_kernel<<<rows_.count, kBlock, 0, s_>>>(rows_.chunks.data(), pact.data(),
+                                                        u.data(), part_r.data());
+    b_gk_record_kernel<1><<<ceil_div(B_, kBlock), kBlock, 0, s_>>>(
+      rows_.offsets.data(), B_, part_r.data(), pact.data(), st.data(), betas.data(), -1);
+    launches_ += 2;
+    B200_LAUNCH_CHECK();
+    auto step = [&](int k) {
+      const auto As  = wview<TX>(true, As_.data());
+      const auto ATs = wview<TX>(false, ATs_.data());
+      sell_map_kernel<TX, double, b_gk_primal_epi><<<sell_grid(ATs), kBlock, 0, s_>>>(
+        ATs, u.data(), b_gk_primal_epi{v.data(), rowbuf_.data(), st.data(), cctx},
+        partials_.data());
+      b_chunk_sum_kernel<<<cols_.count, kBlock, 0, s_>>>(cols_.chunks.data(), pact.data(),
+                                                         rowbuf_.data(), part_c.data());
+      b_gk_record_kernel<0><<<ceil_div(B_, kBlock), kBlock, 0, s_>>>(
+        cols_.offsets.data(), B_, part_c.data(), pact.data(), st.data(), alphas.data(), k);
+      sell_map_kernel<TX, double, b_gk_dual_epi><<<sell_grid(As), kBlock, 0, s_>>>(
+        As, v.data(), b_gk_dual_epi{u.data(), rowbuf_.data(), st.data(), rctx},
+        partials_.data());
+      b_chunk_sum_kernel<<<rows_.count, kBlock, 0, s_>>>(rows_.chunks.data(), pact.data(),
+                                                         rowbuf_.data(), part_r.data());
+      b_gk_record_kernel<1><<<ceil_div(B_, kBlock), kBlock, 0, s_>>>(
+        rows_.offsets.data(), B_, part_r.data(), pact.data(), st.data(), betas.data(), k);
+    };
+    std::vector<double> ha((size_t)B_ * ld), hb((size_t)B_ * ld), prev(B_, -1.0), sigma2(B_, 0.0);
+    std::vector<double> a(ld), bb(ld);
+    eta_.assign(B_, 0.0);
+    power_iters_.assign(B_, 0);
+    int left = B_, listed = B_, k = 0;
+    while (left > 0 && k < kLanczosMaxSteps) {
+      const int c = std::min(kLanczosChunk, kLanczosMaxSteps - k);
+      for (int i = 0; i < c; ++i) step(k + i);
+      launches_ += 6.0 * c;
+      B200_LAUNCH_CHECK();
+      k += c;
+      alphas.download(ha.data(), (size_t)k * B_, s_);
+      betas.download(hb.data(), (size_t)(k + 1) * B_, s_);
+      B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+      for (int b = 0; b < B_; ++b) {
+        if (!pact_h[b]) continue;
+        // betas[0] holds |z0|; the recurrence coefficients are betas[1..].
+        for (int j = 0; j < k; ++j) a[j] = ha[(size_t)j * B_ + b];
+        for (int j = 0; j <= k; ++j) bb[j] = hb[(size_t)j * B_ + b];
+        bool breakdown = false;
+        int used         = k;
+        for (int j = 0; j < k; ++j)
+          if (!(a[j] > 0.0) || !(bb[j + 1] > 0.0) || !std::isfinite(a[j]) ||
+              !std::isfinite(bb[j + 1])) {
+            used      = j + 1;
+            breakdown = true;
+            break;
+          }
+        sigma2[b] = largest_bidiagonal_sigma2(a.data(), bb.data() + 1, used);
+        const bool done = breakdown || k >= kLanczosMaxSteps ||
+                          (prev[b] > 0.0 && std::fabs(sigma2[b] - prev[b]) <= kLanczosTol * sigma2[b]);
+        prev[b] = sigma2[b];
+        if (done) {
+          pact_h[b]        = 0;
+          power_iters_[b]  = used;
+          --left;
+        }
+      }
+      if (left == 0) break;
+      pact.upload(pact_h.data(), B_, s_);
+      if (2 * left <= listed) {
+        rebuild_work(pact_h);
+        listed = left;
+        char what[96];
+        std::snprintf(what, sizeof what, "batch: lanczos to %d steps, %d instances left", k,
+                      left);
+        trace(what);
+      }
+    }
+    clear_work();
+    for (int b = 0; b < B_; ++b) {
+      if (pact_h[b]) power_iters_[b] = k;  // step limit reached
+      eta_[b] = kStepScaling / std::sqrt(sigma2[b]);
     }
   }
 
@@ -1150,6 +1339,9 @@ class batch_engine {
     std::vector<double> pid_sum(B_, 0.0), pid_last(B_, 0.0), best_gap(B_, inf);
     std::vector<long> since(B_, 0);
     std::vector<int> restarted(B_, 0);
+    // Stall test of mixed precision (per instance; see kStallWindow).
+    std::vector<double> stall_ref(B_, std::numeric_limits<double>::infinity());
+    std::vector<long> stall_k(B_, 0);
     int n_active = B_, listed = B_;
     upload_scalars(since);
 
@@ -1175,6 +1367,16 @@ class batch_engine {
             finish(b, kIterationLimit, c, k);
           else if (!std::isfinite(c.l2_primal) || !std::isfinite(c.l2_dual))
             finish(b, kNumericalError, c, k);
+          else if (std::is_same_v<TX, float>) {
+            const double q = termination_distance(
+              c.l2_primal, p_.abs_primal + p_.rel_primal * b_norm_[b], c.l2_dual,
+              p_.abs_dual + p_.rel_dual * c_norm_[b], c.gap, p_.abs_gap + p_.rel_gap * c.abs_obj);
+            if (q <= 0.5 * stall_ref[b]) {
+              stall_ref[b] = q;
+              stall_k[b]   = k;
+            } else if (k - stall_k[b] >= kStallWindow)
+              finish(b, kStalled, c, k);
+          }
         }
         n_active = (int)std::count(active_h_.begin(), active_h_.end(), 1);
         if (n_active == 0) break;

@@ -99,6 +99,15 @@ inline void trace(const char* what)
   last = t;
 }
 
+// trace() once the stream's work so far has finished (no synchronisation unless tracing).
+inline void trace_sync(cudaStream_t s, const char* what)
+{
+  static const bool on = std::getenv("CUOPT_B200_TRACE") != nullptr;
+  if (!on) return;
+  cudaStreamSynchronize(s);
+  trace(what);
+}
+
 // Device buffer owning `n` elements of T (stream-ordered allocation on alloc_stream_ref()).
 template <typename T>
 class dbuf {

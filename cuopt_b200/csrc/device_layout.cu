@@ -297,11 +297,13 @@ void build_device_layout(int m, int n, const int* d_off, const int* d_idx, const
                                   cudaMemcpyDeviceToHost, s));
   B200_CUDA_CHECK(cudaStreamSynchronize(s));
   if (hcount[1]) throw std::invalid_argument("constraint matrix column index out of range");
+  trace_sync(s, "layout: lengths");
 
   const int a_long = order_items(rlen.data(), p.row_inst, m, p, s, tmp, out.row_new2old,
                                  out.row_old2new, counters.data(), hcount);
   const int t_long = order_items(clen.data(), p.col_inst, n, p, s, tmp, out.col_new2old,
                                  out.col_old2new, counters.data(), hcount);
+  trace_sync(s, "layout: relabelling");
 
   // Internal A (CSR) ----------------------------------------------------------------------
   dbuf<int> alen(m + 1), aoff(m + 1);
@@ -319,6 +321,7 @@ void build_device_layout(int m, int n, const int* d_off, const int* d_idx, const
     aidx.data(), aval.data(), asrc.data(), arow.data());
   B200_LAUNCH_CHECK();
 
+  trace_sync(s, "layout: internal A");
   // Internal A^T (CSR) by a stable sort of the entries on their internal column ----------------
   dbuf<int> tlen(n + 1), toff(n + 1), pos_in(nz), pos_out(nz), key_out(nz);
   gather_len_kernel<<<grid_for(n + 1), kT, 0, s>>>(clen.data(), out.col_new2old.data(), n,
@@ -344,8 +347,11 @@ void build_device_layout(int m, int n, const int* d_off, const int* d_idx, const
     B200_LAUNCH_CHECK();
   }
 
+  trace_sync(s, "layout: internal A^T");
   to_sell(m, n, a_long, aoff.data(), aidx.data(), aval.data(), asrc.data(), nnz, s, tmp, out.A);
+  trace_sync(s, "layout: sliced A");
   to_sell(n, m, t_long, toff.data(), tidx.data(), tval.data(), tsrc.data(), nnz, s, tmp, out.AT);
+  trace_sync(s, "layout: sliced A^T");
   B200_CUDA_CHECK(cudaStreamSynchronize(s));
 }
 

@@ -127,6 +127,12 @@ __global__ void __launch_bounds__(kBlock) finalize_sum_kernel(const double* part
   ordered_block_sum<K>(partials, nblocks, out);
 }
 
+// p[0 .. n) = v.
+static __global__ void fill_kernel(double* p, int n, double v)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
 // out[q] = max over blocks of partials[b*K+q] (single block).
 template <int K>
 __global__ void __launch_bounds__(kBlock) finalize_max_kernel(const double* partials, int nblocks,

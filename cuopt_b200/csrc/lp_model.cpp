@@ -19,6 +19,7 @@
 
 #include "common.cuh"
 #include "host_io.hpp"
+#include "pdlp_schedule.hpp"
 
 namespace cuopt_b200 {
 
@@ -493,6 +494,7 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
                               const std::vector<std::vector<double>>& up, const pdlp_params& prm,
                               bool crossover, std::vector<lp_solution>& out)
 {
+  const auto t_chunk = std::chrono::steady_clock::now();
   batch_device_input bi;
   bi.count = (int)ids.size();
   bi.row_start.assign(1, 0);
@@ -598,6 +600,20 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
     o.r.x.assign(hx.begin() + bi.col_start[b], hx.begin() + bi.col_start[b + 1]);
     o.r.rc.assign(hrc.begin() + bi.col_start[b], hrc.begin() + bi.col_start[b + 1]);
     o.r.y.assign(hy.begin() + bi.row_start[b], hy.begin() + bi.row_start[b + 1]);
+  }
+  // Instances whose FP32 iterates stalled are solved again, together, in FP64 (their single
+  // solves would continue in FP64 from the stalled state instead).
+  std::vector<size_t> stalled;
+  for (int b = 0; b < bi.count; ++b)
+    if (rs[b].status == kStalled) stalled.push_back(ids[b]);
+  if (!stalled.empty()) {
+    pdlp_params q = prm;
+    q.precision   = 0;
+    q.time_limit  = std::max(
+      0.0, prm.time_limit -
+             std::chrono::duration<double>(std::chrono::steady_clock::now() - t_chunk).count());
+    solve_batch_chunk(ps, stalled, lo, up, q, false, out);
+    for (size_t id : stalled) out[id].r.refinement_passes = 1;
   }
   if (!crossover) return;
   // Crossover of the Optimal instances on a few host threads: each polish runs its own stream and

@@ -54,6 +54,9 @@ struct loop_state {
   // Infeasibility test statistics (zero until first computed, then kept between computations).
   double primal_ray_obj = 0.0, max_primal_ray_inf = 0.0;
   double dual_ray_obj = 0.0, max_dual_ray_inf = 0.0;
+  // Stall test of mixed precision: reference distance and the iteration it was reached.
+  double stall_ref = std::numeric_limits<double>::infinity();
+  long stall_k     = 0;
 };
 
 class climber_engine;
@@ -354,9 +357,9 @@ class engine {
 
   void fill(double* p, int n, double v)
   {
-    std::vector<double> h(n, v);
-    B200_CUDA_CHECK(cudaMemcpyAsync(p, h.data(), n * sizeof(double), cudaMemcpyHostToDevice, s_));
-    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    fill_kernel<<<vgrid_, kBlock, 0, s_>>>(p, n, v);
+    ++launches_;
+    B200_LAUNCH_CHECK();
   }
 
   // Sum reduction of a vector expression (see vec_reduce_kernel) returned to the host.
@@ -443,7 +446,7 @@ class engine {
     std::mt19937 gen(1);
     std::normal_distribution<double> dist(0.0, 1.0);
     for (int i = 0; i < m; ++i) z0[i] = dist(gen);
-    constexpr int kChunk = 16, kMaxSteps = 512;
+    constexpr int kChunk = kLanczosChunk, kMaxSteps = kLanczosMaxSteps;
     dbuf<double> u(m), v(n), tmp(m), alphas(kMaxSteps + 1), betas(kMaxSteps + 2);
     dbuf<gk_state> st(1);
     tmp.upload(z0.data(), m, s_);
@@ -496,7 +499,7 @@ class engine {
           break;
         }
       sigma2 = largest_bidiagonal_sigma2(ha.data(), hb.data() + 1, used);
-      if (breakdown || (prev > 0.0 && std::fabs(sigma2 - prev) <= 1e-10 * sigma2)) {
+      if (breakdown || (prev > 0.0 && std::fabs(sigma2 - prev) <= kLanczosTol * sigma2)) {
         k = used;
         break;
       }
@@ -505,40 +508,6 @@ class engine {
     (void)beta0;
     power_iters_ = k;
     eta_         = kStepScaling / std::sqrt(sigma2);
-  }
-
-  // sigma_max^2 of the (k+1) x k lower bidiagonal matrix with diagonal a[0..k-1] and subdiagonal
-  // b[0..k-1]: the largest eigenvalue of the tridiagonal B^T B, by Sturm-sequence bisection.
-  static double largest_bidiagonal_sigma2(const double* a, const double* b, int k)
-  {
-    if (k <= 0) return 0.0;
-    std::vector<double> d(k), e(std::max(k - 1, 0));
-    for (int j = 0; j < k; ++j) d[j] = a[j] * a[j] + b[j] * b[j];
-    for (int j = 0; j + 1 < k; ++j) e[j] = a[j + 1] * b[j];
-    double hi = 0.0;
-    for (int j = 0; j < k; ++j)
-      hi = std::max(hi, d[j] + (j > 0 ? std::fabs(e[j - 1]) : 0.0) + (j + 1 < k ? std::fabs(e[j]) : 0.0));
-    double lo = 0.0;
-    // count of eigenvalues below x (Sturm sequence of T - x I)
-    auto below = [&](double x) {
-      int cnt  = 0;
-      double q = d[0] - x;
-      if (q < 0) ++cnt;
-      for (int j = 1; j < k; ++j) {
-        const double prevq = q != 0.0 ? q : 1e-300;
-        q = d[j] - x - e[j - 1] * e[j - 1] / prevq;
-        if (q < 0) ++cnt;
-      }
-      return cnt;
-    };
-    for (int it = 0; it < 200 && hi - lo > 1e-15 * hi; ++it) {
-      const double mid = 0.5 * (lo + hi);
-      if (below(mid) >= k)
-        hi = mid;
-      else
-        lo = mid;
-    }
-    return hi;
   }
 
   // ------------------------------------------------------------------ iteration kernels
@@ -830,6 +799,18 @@ class engine {
         if (k >= p_.iteration_limit) return finish(r, kIterationLimit, cv, k);
         if (!std::isfinite(cv.l2_primal) || !std::isfinite(cv.l2_dual))
           return finish(r, kNumericalError, cv, k);
+        if constexpr (std::is_same_v<TX, float>) {
+          const double q = termination_distance(
+            pcr ? cv.linf_primal : cv.l2_primal,
+            pcr ? p_.abs_primal : p_.abs_primal + p_.rel_primal * b_norm_,
+            pcr ? cv.linf_dual : cv.l2_dual, pcr ? p_.abs_dual : p_.abs_dual + p_.rel_dual * c_norm_,
+            cv.gap, p_.abs_gap + p_.rel_gap * cv.abs_obj);
+          if (q <= 0.5 * sched_.stall_ref) {
+            sched_.stall_ref = q;
+            sched_.stall_k   = k;
+          } else if (k - sched_.stall_k >= kStallWindow)
+            return finish(r, kStalled, cv, k);
+        }
 
         if (major) {
           // should_cupdlpx_restart (reference pdlp_restart_strategy.cu:689-754)
@@ -1029,13 +1010,17 @@ pdlp_result pdlp_solve_device(const lp_device_input& in, const pdlp_params& p, c
   if (p.precision == 1) {
     engine<float> e(in, p, js.own);
     pdlp_result r = e.run(x_out, y_out, rc_out);
-    if (p.refinement_passes <= 0 || r.status != kOptimal) return r;
-    // FP64 continuation to the refinement tolerance, within what is left of the limits.
-    pdlp_params q     = p;
-    q.abs_primal      = q.rel_primal = p.refinement_tol;
-    q.abs_dual        = q.rel_dual = p.refinement_tol;
-    q.abs_gap         = q.rel_gap = p.refinement_tol;
-    q.iteration_limit = std::max<int64_t>(p.iteration_limit - r.iterations, 0);
+    const bool stalled = r.status == kStalled;
+    if (!stalled && (p.refinement_passes <= 0 || r.status != kOptimal)) return r;
+    // FP64 continuation: to the refinement tolerance when one is asked for, else (a stalled mixed
+    // solve) to the solve's own tolerances.  It resumes the iteration count, so the limits stay
+    // those of the solve.
+    pdlp_params q = p;
+    if (p.refinement_passes > 0) {
+      q.abs_primal = q.rel_primal = p.refinement_tol;
+      q.abs_dual = q.rel_dual = p.refinement_tol;
+      q.abs_gap = q.rel_gap = p.refinement_tol;
+    }
     engine<double> d(in, q, js.own);
     return d.continue_from(e, r, x_out, y_out, rc_out);
   }

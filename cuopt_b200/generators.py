@@ -209,13 +209,26 @@ def skewed_lp(m: int, n: int, seed: int = 2000, zipf_a: float = 1.3, cap: int = 
     return lp
 
 
-def batch_lps(count: int = 512, seed: int = 3000, m_lo: int = 200, m_hi: int = 20000):
-    """Config-3 generator: `count` config-0 LPs of uneven sizes."""
+def _batch_shapes(count, seed, m_lo, m_hi):
     rng = np.random.default_rng(seed)
     ms = np.exp(rng.uniform(np.log(m_lo), np.log(m_hi), size=count)).astype(int)
     ks = rng.integers(6, 13, size=count)
+    return ms, ks
+
+
+def batch_lps(count: int = 512, seed: int = 3000, m_lo: int = 200, m_hi: int = 20000):
+    """Config-3 generator: `count` config-0 LPs of uneven sizes."""
+    ms, ks = _batch_shapes(count, seed, m_lo, m_hi)
     return [constructed_lp(int(m), int(2.5 * m), int(k), seed=seed + 1 + i, name=f"batch{i}")
             for i, (m, k) in enumerate(zip(ms, ks))]
+
+
+def batch_instance(i: int, count: int = 512, seed: int = 3000, m_lo: int = 200,
+                   m_hi: int = 20000):
+    """Instance i of batch_lps(count, seed, ...) alone."""
+    ms, ks = _batch_shapes(count, seed, m_lo, m_hi)
+    return constructed_lp(int(ms[i]), int(2.5 * ms[i]), int(ks[i]), seed=seed + 1 + i,
+                          name=f"batch{i}")
 
 
 def kkt_relative_error(lp: LP, x: np.ndarray, y: np.ndarray) -> dict:

@@ -7,7 +7,8 @@
 `sweeps` prepares the LP and launches the two fused PDHG sweeps separately between CUDA events
          (cuOptProfilePDHGSweeps).
 `batch`  (config c3) solves the 512-instance batch in one cuOptBatchSolve call and a sample of the
-         same instances one by one with cuOptSolve (FP64, 1e-6).
+         same instances one by one with cuOptSolve (1e-6; FP64, or mixed precision with
+         --batch-precision mixed, for both).
 `adjoint` (config c4) solves 64 non-degenerate 5000 x 10000 LPs in one batched call (crossover
          on), back-propagates L = sum w * x* through the KKT adjoint, and checks the gradients
          against the exact basis derivatives and against central differences (h = 1e-6) on random
@@ -65,6 +66,7 @@ def main() -> None:
     ap.add_argument("--repeats", type=int, default=2,
                     help="batch mode: batched solves, the first one untimed (warm-up)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--batch-precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--iterations", type=int, default=3)
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--time-limit", type=float, default=0.0)
@@ -159,6 +161,8 @@ def run_batch(a) -> dict:
     st.set_optimality_tolerance(a.tol)
     st.set_parameter(lpm.CUOPT_METHOD, int(lpm.SolverMethod.PDLP))
     st.set_parameter(lpm.CUOPT_LOG_TO_CONSOLE, False)
+    precision = getattr(a, "batch_precision", "fp64")
+    st.set_parameter(lpm.CUOPT_PDLP_PRECISION, 1 if precision == "mixed" else 0)
     if a.time_limit > 0:
         st.set_parameter(lpm.CUOPT_TIME_LIMIT, a.time_limit)
     times = []
@@ -170,14 +174,16 @@ def run_batch(a) -> dict:
     iters = [s.get_lp_stats()["nb_iterations"] for s in sols]
     obj_err = [abs(s.get_primal_objective() - lp.optimal_objective) / max(1.0, abs(lp.optimal_objective))
                for s, lp in zip(sols, lps)]
-    out = {"config": "c3", "count": a.count, "m_total": int(sum(lp.m for lp in lps)),
+    out = {"config": "c3", "precision": precision, "count": a.count,
+           "m_total": int(sum(lp.m for lp in lps)),
            "n_total": int(sum(lp.n for lp in lps)), "nnz_total": int(sum(lp.nnz for lp in lps)),
            "batch_s": batch_s, "batch_times_s": times, "batch_lps_per_s": a.count / batch_s,
            "optimal": status.count(1), "max_iterations": max(iters),
            "mean_iterations": float(np.mean(iters)), "max_objective_rel_error": max(obj_err),
            "batch_setup_s": sols[0].stats.get("setup_time"),
            "iterations_p50_p90_p99": [float(np.percentile(iters, q)) for q in (50, 90, 99)],
-           "max_power_iterations": max(s.stats.get("power_iterations", 0) for s in sols)}
+           "max_power_iterations": max(s.stats.get("power_iterations", 0) for s in sols),
+           "fp64_resolved": sum(int(s.stats.get("refinement_passes", 0) > 0) for s in sols)}
     if a.sequential > 0:
         pick = np.linspace(0, a.count - 1, min(a.sequential, a.count)).astype(int)
         lpm.Solve(dms[pick[0]], st)  # warm-up

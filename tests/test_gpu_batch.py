@@ -95,3 +95,23 @@ def test_batch_mixes_special_cases(golden, golden_dir, instances):
     assert abs(sols[1].get_primal_objective() - golden["no_constraints_objective"]["value"]) <= 1e-4
     single = lpm.Solve(datamodel_from_lp(instances[2]), s)
     assert sols[2].get_lp_stats()["nb_iterations"] == single.get_lp_stats()["nb_iterations"]
+
+
+def test_mixed_batch_follows_single_mixed_solves(instances):
+    """In mixed precision every instance takes its step size from Golub-Kahan-Lanczos, as a single
+    mixed solve does: the same number of Lanczos steps and the same step size (1e-12 relative;
+    summation order differs), Optimal at 1e-6 with the single solve's iteration count (±5 %) and
+    the constructed optimum."""
+    lps = instances[:4]
+    dms = _models(lps)
+    s = settings(tol=1e-6, precision=1)
+    sols, _ = lpm.BatchSolve(dms, s)
+    for lp, dm, sol in zip(lps, dms, sols):
+        single = lpm.Solve(dm, s)
+        assert sol.get_termination_status() == single.get_termination_status() == \
+            lpm.LPTerminationStatus.Optimal
+        assert sol.stats["power_iterations"] == single.stats["power_iterations"] > 0
+        assert rel(sol.stats["step_size"], single.stats["step_size"]) <= 1e-12
+        si, bi = single.get_lp_stats()["nb_iterations"], sol.get_lp_stats()["nb_iterations"]
+        assert abs(bi - si) <= 0.05 * si + 10
+        assert rel(sol.get_primal_objective(), lp.optimal_objective) <= 1e-5

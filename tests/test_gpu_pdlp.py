@@ -308,3 +308,25 @@ def test_per_constraint_residual_in_batches(small_lp):
         assert np.array_equal(sol.get_primal_solution(), single.get_primal_solution())
     climbers, _ = lpm.SolveClimbers(datamodel_from_lp(lp), [0], [lp.var_lo[0]], [lp.var_up[0]], s)
     assert climbers[0].get_error_status() == 4  # CUOPT_VALIDATION_ERROR
+
+
+def test_mixed_precision_stall_continues_in_fp64():
+    """Config-3 instance 458: its FP32 iterates stall with the relative gap near 1e-4 (after which
+    the primal weight drifts), so a mixed solve continues in FP64 from its own state and ends
+    Optimal at 1e-6 with the constructed optimum (refinement_passes = 1), as the FP64 solve does.
+    In a mixed batch the stalled instance is solved again in FP64; the others stay mixed."""
+    lp = gen.batch_instance(458)
+    dm = datamodel_from_lp(lp)
+    mixed = lpm.Solve(dm, settings(tol=1e-6, precision=1, time_limit=60))
+    fp64 = lpm.Solve(dm, settings(tol=1e-6, precision=0, time_limit=60))
+    assert mixed.get_termination_status() == fp64.get_termination_status() == \
+        lpm.LPTerminationStatus.Optimal
+    assert mixed.stats["refinement_passes"] == 1
+    assert rel(mixed.get_primal_objective(), lp.optimal_objective) <= 1e-5
+    other = gen.batch_instance(0)
+    sols, _ = lpm.BatchSolve([dm, datamodel_from_lp(other)],
+                             settings(tol=1e-6, precision=1, time_limit=60))
+    assert [int(s.get_termination_status()) for s in sols] == [1, 1]
+    assert [s.stats["refinement_passes"] for s in sols] == [1, 0]
+    assert rel(sols[0].get_primal_objective(), lp.optimal_objective) <= 1e-5
+    assert rel(sols[1].get_primal_objective(), other.optimal_objective) <= 1e-5
