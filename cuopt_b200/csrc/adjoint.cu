@@ -149,9 +149,10 @@ struct active_set {
   std::vector<char> rkind;  // per row: 0 inactive, 1 lower bound (or equality), 2 upper bound
 };
 
+template <class X>
 active_set classify(const lp_problem& p, const std::vector<double>& lo,
-                    const std::vector<double>& up, const std::vector<double>& x,
-                    const std::vector<double>& ax, double bound_tol, double row_tol)
+                    const std::vector<double>& up, const X& x, const std::vector<double>& ax,
+                    double bound_tol, double row_tol)
 {
   active_set a;
   a.fpos.assign(p.n, -1);
@@ -184,7 +185,8 @@ active_set classify(const lp_problem& p, const std::vector<double>& lo,
   return a;
 }
 
-std::vector<double> row_products(const lp_problem& p, const std::vector<double>& x)
+template <class X>
+std::vector<double> row_products(const lp_problem& p, const X& x)
 {
   std::vector<double> ax(p.m, 0.0);
   for (int i = 0; i < p.m; ++i)
@@ -348,8 +350,8 @@ void solution_adjoint(const lp_problem& p, const pdlp_result& sol, const double*
     throw std::invalid_argument("adjoint: the solution holds no primal / dual vectors");
   std::vector<double> lo, up;
   p.constraint_bounds(lo, up);
-  const std::vector<double>& x = sol.x;
-  const std::vector<double>& y = sol.y;
+  const host_array<double>& x = sol.x;
+  const host_array<double>& y = sol.y;
   const active_set a = classify(p, lo, up, x, row_products(p, x), kBoundTol, kActiveTol);
   const int nr = (int)a.R.size(), nf = (int)a.F.size();
 
@@ -427,7 +429,7 @@ bool vertex_polish(const lp_problem& p, pdlp_result& r)
     yR = sys.solve_transposed(cF);
   }
   // Candidate vertex; accepted only if primal and dual feasible.
-  std::vector<double> x = r.x, y(m, 0.0);
+  std::vector<double> x(r.x.begin(), r.x.end()), y(m, 0.0);
   for (int q = 0; q < nf; ++q) x[a.F[q]] = xF[q];
   for (int q = 0; q < nr; ++q) y[a.R[q]] = yR[q];
   for (int j : a.F) {
@@ -465,7 +467,7 @@ bool vertex_polish(const lp_problem& p, pdlp_result& r)
             std::min(y[i], 0.0) * (std::isfinite(up[i]) ? up[i] : 0.0);
   for (int j = 0; j < n; ++j) dobj += s[j] * x[j];
   dobj = sgn * dobj;
-  r.x = x;
+  r.x.assign(x.begin(), x.end());
   r.y.resize(m);
   r.rc.resize(n);
   for (int i = 0; i < m; ++i) r.y[i] = sgn * y[i];

@@ -924,12 +924,14 @@ class batch_engine {
   void power_iteration()
   {
     const int m = in_.m, n = in_.n;
+    // Every instance starts from the first m_b values of the std::mt19937(1) normal sequence.
     std::vector<double> z0(m);
-    for (int b = 0; b < B_; ++b) {
-      std::mt19937 gen(1);
-      std::normal_distribution<double> dist(0.0, 1.0);
-      for (int i = in_.row_start[b]; i < in_.row_start[b + 1]; ++i) z0[i] = dist(gen);
-    }
+    int max_rows = 0;
+    for (int b = 0; b < B_; ++b) max_rows = std::max(max_rows, in_.row_start[b + 1] - in_.row_start[b]);
+    const auto seq = power_start_sequence(max_rows);
+    for (int b = 0; b < B_; ++b)
+      std::copy(seq->begin(), seq->begin() + (in_.row_start[b + 1] - in_.row_start[b]),
+                z0.begin() + in_.row_start[b]);
     dbuf<double> dz(m), dq(m), datq(n);
     dq.upload(z0.data(), m, s_);
     permute_gather(dq.data(), L_.row_new2old.data(), m, 1.0, dz.data(), s_);
@@ -1026,12 +1028,14 @@ class batch_engine {
   {
     const int m = in_.m, n = in_.n;
     const int ld = kLanczosMaxSteps + 2;  // history rows (steps), each B_ wide
+    // Every instance starts from the first m_b values of the std::mt19937(1) normal sequence.
     std::vector<double> z0(m);
-    for (int b = 0; b < B_; ++b) {
-      std::mt19937 gen(1);
-      std::normal_distribution<double> dist(0.0, 1.0);
-      for (int i = in_.row_start[b]; i < in_.row_start[b + 1]; ++i) z0[i] = dist(gen);
-    }
+    int max_rows = 0;
+    for (int b = 0; b < B_; ++b) max_rows = std::max(max_rows, in_.row_start[b + 1] - in_.row_start[b]);
+    const auto seq = power_start_sequence(max_rows);
+    for (int b = 0; b < B_; ++b)
+      std::copy(seq->begin(), seq->begin() + (in_.row_start[b + 1] - in_.row_start[b]),
+                z0.begin() + in_.row_start[b]);
     dbuf<double> u(m), v(n), tmp(m), alphas((size_t)B_ * ld), betas((size_t)B_ * ld);
     dbuf<b_gk_state> st(B_);
     tmp.upload(z0.data(), m, s_);

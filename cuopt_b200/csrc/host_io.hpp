@@ -36,19 +36,28 @@ inline void parallel_memcpy(void* dst, const void* src, size_t bytes)
   for (auto& th : pool) th.join();
 }
 
-// Uploads host arrays to device memory through two pinned staging buffers (per host thread,
-// allocated once).  put() may return before the copy has reached the device; finish() (or the
+// Two pinned staging buffers per host thread (allocated once), shared by staged_upload and
+// staged_download.
+constexpr size_t kStageBytes = size_t(32) << 20;
+struct staging_buffers {
+  char* buf[2]        = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+};
+inline staging_buffers& staging()
+{
+  static thread_local staging_buffers b;
+  for (int i = 0; i < 2; ++i) {
+    if (!b.buf[i]) B200_CUDA_CHECK(cudaMallocHost(&b.buf[i], kStageBytes));
+    if (!b.done[i]) B200_CUDA_CHECK(cudaEventCreateWithFlags(&b.done[i], cudaEventDisableTiming));
+  }
+  return b;
+}
+
+// Uploads host arrays to device memory through the pinned staging buffers.  put() may return before the copy has reached the device; finish() (or the
 // destructor) waits for every copy issued.
 class staged_upload {
  public:
-  explicit staged_upload(cudaStream_t s) : s_(s)
-  {
-    auto& st = state();
-    for (int i = 0; i < 2; ++i) {
-      if (!st.buf[i]) B200_CUDA_CHECK(cudaMallocHost(&st.buf[i], kStage));
-      if (!st.done[i]) B200_CUDA_CHECK(cudaEventCreateWithFlags(&st.done[i], cudaEventDisableTiming));
-    }
-  }
+  explicit staged_upload(cudaStream_t s) : s_(s) { staging(); }
   ~staged_upload()
   {
     try {
@@ -91,20 +100,12 @@ class staged_upload {
   }
 
  private:
-  static constexpr size_t kStage = size_t(32) << 20;
+  static constexpr size_t kStage = kStageBytes;
   struct piece {
     char* dst;
     size_t off, bytes;
   };
-  struct buffers {
-    char* buf[2]        = {nullptr, nullptr};
-    cudaEvent_t done[2] = {nullptr, nullptr};
-  };
-  static buffers& state()
-  {
-    static thread_local buffers b;
-    return b;
-  }
+  static staging_buffers& state() { return staging(); }
   // Issues the copies of the current buffer and switches to the other one (waiting until the
   // DMA engine has drained it).
   void flush()
@@ -131,5 +132,35 @@ class staged_upload {
   bool armed_[2]   = {false, false};
   std::vector<piece> pending_;
 };
+
+// Copies `bytes` of device memory to host memory through the pinned staging buffers, after the
+// work already queued on `s`: the DMA engine fills one buffer while host threads empty the other.
+// Returns when the host copy is complete.
+inline void staged_download(void* dst, const void* src, size_t bytes, cudaStream_t s)
+{
+  if (bytes == 0) return;
+  auto& st      = staging();
+  auto* d       = static_cast<char*>(dst);
+  const auto* h = static_cast<const char*>(src);
+  size_t off    = 0;
+  int cur       = 0;
+  size_t n      = std::min(bytes, kStageBytes);
+  B200_CUDA_CHECK(cudaMemcpyAsync(st.buf[cur], h, n, cudaMemcpyDeviceToHost, s));
+  B200_CUDA_CHECK(cudaEventRecord(st.done[cur], s));
+  for (;;) {
+    const size_t next = off + n;
+    const size_t nn   = std::min(bytes - next, kStageBytes);
+    if (nn > 0) {
+      B200_CUDA_CHECK(cudaMemcpyAsync(st.buf[1 - cur], h + next, nn, cudaMemcpyDeviceToHost, s));
+      B200_CUDA_CHECK(cudaEventRecord(st.done[1 - cur], s));
+    }
+    B200_CUDA_CHECK(cudaEventSynchronize(st.done[cur]));
+    parallel_memcpy(d + off, st.buf[cur], n);
+    if (nn == 0) break;
+    off = next;
+    n   = nn;
+    cur = 1 - cur;
+  }
+}
 
 }  // namespace cuopt_b200

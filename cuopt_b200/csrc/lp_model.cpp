@@ -377,11 +377,19 @@ pdlp_params params_from_settings(const lp_settings& st)
   return prm;
 }
 
+// Constraint bounds as PDLP takes them: a ranged problem's own arrays, otherwise built from the
+// row types and right-hand sides.
+struct row_bounds {
+  const double* lo = nullptr;
+  const double* up = nullptr;
+  std::vector<double> lo_store, up_store;
+};
+
 // The checks and special cases that come before PDLP (reference solve.cu:1124-1342 and
-// problem_checking.cu).  Returns true when the problem goes to PDLP with constraint bounds lo / up;
+// problem_checking.cu).  Returns true when the problem goes to PDLP with constraint bounds `rb`;
 // otherwise `out` already holds the answer.
-static bool prepare_for_pdlp(const lp_problem& p, const lp_settings& st, std::vector<double>& lo,
-                             std::vector<double>& up, lp_solution& out)
+static bool prepare_for_pdlp(const lp_problem& p, const lp_settings& st, row_bounds& rb,
+                             lp_solution& out)
 {
   const auto t0 = std::chrono::steady_clock::now();
   if (p.quadratic) {
@@ -401,7 +409,16 @@ static bool prepare_for_pdlp(const lp_problem& p, const lp_settings& st, std::ve
     return false;
   }
   trace("validate_problem");
-  p.constraint_bounds(lo, up);
+  if (p.ranged) {
+    rb.lo = p.con_lo.data();
+    rb.up = p.con_up.data();
+  } else {
+    p.constraint_bounds(rb.lo_store, rb.up_store);
+    rb.lo = rb.lo_store.data();
+    rb.up = rb.up_store.data();
+  }
+  const double* lo = rb.lo;
+  const double* up = rb.up;
   // has_crossing_bounds (reference problem_checking.cu:316-339)
   for (int j = 0; j < p.n; ++j)
     if (!(p.var_up[j] >= p.var_lo[j])) {
@@ -442,8 +459,8 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
   lp_solution out;
   trace("solve_problem: start");
   try {
-    std::vector<double> lo, up;
-    if (!prepare_for_pdlp(p, st, lo, up, out)) return out;
+    row_bounds rb;
+    if (!prepare_for_pdlp(p, st, rb, out)) return out;
     pdlp_params prm = params_from_settings(st);
     if ((int)st.initial_primal.size() == p.n) prm.initial_primal = st.initial_primal;
     if ((int)st.initial_dual.size() == p.m) prm.initial_dual = st.initial_dual;
@@ -454,8 +471,8 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
     in.col_idx    = p.col_idx.data();
     in.val        = p.val.data();
     in.c          = p.c.data();
-    in.con_lo     = lo.data();
-    in.con_up     = up.data();
+    in.con_lo     = rb.lo;
+    in.con_up     = rb.up;
     in.var_lo     = p.var_lo.data();
     in.var_up     = p.var_up.data();
     in.obj_offset = p.obj_offset;
@@ -489,9 +506,8 @@ constexpr int kConcurrentPolish = 4;
 
 // One block-diagonal batch on the device (see pdlp_batch_solve_device).
 static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
-                              const std::vector<size_t>& ids,
-                              const std::vector<std::vector<double>>& lo,
-                              const std::vector<std::vector<double>>& up, const pdlp_params& prm,
+                              const std::vector<size_t>& ids, const std::vector<row_bounds>& rb,
+                              const pdlp_params& prm,
                               bool crossover, std::vector<lp_solution>& out)
 {
   const auto t_chunk = std::chrono::steady_clock::now();
@@ -512,9 +528,8 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
   // Uninitialised host arrays (every element is written below; zero-filling 10^8 elements would
   // cost as much as the copy itself).
   const size_t nz = (size_t)std::max<int64_t>(nnz, 1);
-  std::unique_ptr<int[]> off(new int[m + 1]), idx(new int[nz]), rinst(new int[m]), cinst(new int[n]);
-  std::unique_ptr<double[]> val(new double[nz]), c(new double[n]), clo(new double[m]),
-    cup(new double[m]), vlo(new double[n]), vup(new double[n]);
+  host_array<int> off(m + 1), idx(nz), rinst(m), cinst(n);
+  host_array<double> val(nz), c(n), clo(m), cup(m), vlo(n), vup(n);
   off[0] = 0;
   // Row offsets first (prefix over instances), then every instance's pieces in parallel.
   std::vector<int> e0(bi.count + 1, 0);
@@ -524,8 +539,8 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
     const int r0 = bi.row_start[b], c0 = bi.col_start[b], base = e0[b];
     for (int i = 0; i < p.m; ++i) {
       off[r0 + i + 1] = base + p.row_off[i + 1];
-      clo[r0 + i]     = lo[ids[b]][i];
-      cup[r0 + i]     = up[ids[b]][i];
+      clo[r0 + i]     = rb[ids[b]].lo[i];
+      cup[r0 + i]     = rb[ids[b]].up[i];
       rinst[r0 + i]   = b;
     }
     for (int k = 0; k < p.row_off[p.m]; ++k) {
@@ -563,16 +578,16 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
   trace("batch: device allocation");
   {
     staged_upload h2d(s);
-    h2d.put(doff.data(), off.get(), m + 1);
-    h2d.put(didx.data(), idx.get(), nz);
-    h2d.put(dval.data(), val.get(), nz);
-    h2d.put(dri.data(), rinst.get(), m);
-    h2d.put(dci.data(), cinst.get(), n);
-    h2d.put(dc.data(), c.get(), n);
-    h2d.put(dlo.data(), clo.get(), m);
-    h2d.put(dup.data(), cup.get(), m);
-    h2d.put(dvl.data(), vlo.get(), n);
-    h2d.put(dvu.data(), vup.get(), n);
+    h2d.put(doff.data(), off.data(), m + 1);
+    h2d.put(didx.data(), idx.data(), nz);
+    h2d.put(dval.data(), val.data(), nz);
+    h2d.put(dri.data(), rinst.data(), m);
+    h2d.put(dci.data(), cinst.data(), n);
+    h2d.put(dc.data(), c.data(), n);
+    h2d.put(dlo.data(), clo.data(), m);
+    h2d.put(dup.data(), cup.data(), m);
+    h2d.put(dvl.data(), vlo.data(), n);
+    h2d.put(dvu.data(), vup.data(), n);
     h2d.finish();
   }
   bi.m        = m;
@@ -589,11 +604,10 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
   bi.col_inst = dci.data();
   trace("batch: upload");
   std::vector<pdlp_result> rs = pdlp_batch_solve_device(bi, prm, s, x.data(), y.data(), rc.data());
-  std::vector<double> hx(n), hy(m), hrc(n);
-  x.download(hx.data(), n, s);
-  y.download(hy.data(), m, s);
-  rc.download(hrc.data(), n, s);
-  B200_CUDA_CHECK(cudaStreamSynchronize(s));
+  host_array<double> hx(n), hy(m), hrc(n);
+  staged_download(hx.data(), x.data(), n * sizeof(double), s);
+  staged_download(hy.data(), y.data(), m * sizeof(double), s);
+  staged_download(hrc.data(), rc.data(), n * sizeof(double), s);
   for (int b = 0; b < bi.count; ++b) {
     lp_solution& o = out[ids[b]];
     o.r            = rs[b];
@@ -612,7 +626,7 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
     q.time_limit  = std::max(
       0.0, prm.time_limit -
              std::chrono::duration<double>(std::chrono::steady_clock::now() - t_chunk).count());
-    solve_batch_chunk(ps, stalled, lo, up, q, false, out);
+    solve_batch_chunk(ps, stalled, rb, q, false, out);
     for (size_t id : stalled) out[id].r.refinement_passes = 1;
   }
   if (!crossover) return;
@@ -649,11 +663,11 @@ std::vector<lp_solution> solve_batch(const std::vector<const lp_problem*>& ps, c
     for (size_t i = 0; i < ps.size(); ++i) out[i] = solve_problem(*ps[i], st);
     return out;
   }
-  std::vector<std::vector<double>> lo(ps.size()), up(ps.size());
+  std::vector<row_bounds> rb(ps.size());
   std::vector<size_t> eligible;
   for (size_t i = 0; i < ps.size(); ++i) {
     try {
-      if (prepare_for_pdlp(*ps[i], st, lo[i], up[i], out[i])) eligible.push_back(i);
+      if (prepare_for_pdlp(*ps[i], st, rb[i], out[i])) eligible.push_back(i);
     } catch (const std::exception& e) {
       set_error(out[i], CUOPT_RUNTIME_ERROR, e.what());
     }
@@ -675,7 +689,7 @@ std::vector<lp_solution> solve_batch(const std::vector<const lp_problem*>& ps, c
       chunk.push_back(eligible[pos++]);
     }
     try {
-      solve_batch_chunk(ps, chunk, lo, up, prm, st.b(CUOPT_CROSSOVER), out);
+      solve_batch_chunk(ps, chunk, rb, prm, st.b(CUOPT_CROSSOVER), out);
     } catch (const std::bad_alloc&) {
       for (size_t id : chunk) set_error(out[id], CUOPT_OUT_OF_MEMORY, "Memory allocation failed");
     } catch (const std::invalid_argument& e) {
@@ -709,11 +723,11 @@ std::vector<lp_solution> solve_climbers(const lp_problem& p, const lp_settings& 
     q.var_up[var[b]] = up[b];
     return q;
   };
-  std::vector<double> clo, cup;
+  row_bounds rb;
   lp_solution base;
   bool reaches = false;
   try {
-    reaches = prepare_for_pdlp(p, st, clo, cup, base);
+    reaches = prepare_for_pdlp(p, st, rb, base);
   } catch (const std::exception& e) {
     set_error(base, CUOPT_RUNTIME_ERROR, e.what());
   }
@@ -743,8 +757,8 @@ std::vector<lp_solution> solve_climbers(const lp_problem& p, const lp_settings& 
       h2d.put(didx.data(), p.col_idx.data(), nnz);
       h2d.put(dval.data(), p.val.data(), nnz);
       h2d.put(dc.data(), p.c.data(), n);
-      h2d.put(dlo.data(), clo.data(), m);
-      h2d.put(dup.data(), cup.data(), m);
+      h2d.put(dlo.data(), rb.lo, m);
+      h2d.put(dup.data(), rb.up, m);
       h2d.put(dvl.data(), p.var_lo.data(), n);
       h2d.put(dvu.data(), p.var_up.data(), n);
       h2d.finish();
@@ -836,8 +850,8 @@ std::vector<lp_solution> solve_strong_branching(const lp_problem& p, const lp_se
   climber_start start;
   if (base.error_code == CUOPT_SUCCESS && base.solved_by_pdlp && (int)base.r.x.size() == p.n &&
       (int)base.r.y.size() == p.m) {
-    start.x             = base.r.x;
-    start.y             = base.r.y;
+    start.x.assign(base.r.x.begin(), base.r.x.end());
+    start.y.assign(base.r.y.begin(), base.r.y.end());
     start.step_size     = base.r.step_size;
     start.primal_weight = base.r.primal_weight;
   }

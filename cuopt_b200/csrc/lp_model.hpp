@@ -13,29 +13,7 @@ namespace cuopt_b200 {
 
 // cuOptOptimizationProblem: the user's LP, copied at creation (reference optimization_problem_t,
 // cpp/include/cuopt/linear_programming/optimization_problem.hpp:160-319).
-// std::vector whose resize leaves new elements uninitialised: the problem arrays are always
-// overwritten right after they are sized, and zero-filling 10^8 elements first (single-threaded)
-// would cost as much as the copy itself.
-template <typename T>
-struct default_init_allocator : std::allocator<T> {
-  template <typename U>
-  struct rebind {
-    using other = default_init_allocator<U>;
-  };
-  using std::allocator<T>::allocator;
-  template <typename U>
-  void construct(U* p) noexcept
-  {
-    ::new (static_cast<void*>(p)) U;
-  }
-  template <typename U, typename... Args>
-  void construct(U* p, Args&&... args)
-  {
-    ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
-  }
-};
-template <typename T>
-using host_array = std::vector<T, default_init_allocator<T>>;
+
 
 struct lp_problem {
   int m = 0, n = 0;

@@ -379,10 +379,8 @@ class engine {
   {
     const int m = in_.m, n = in_.n;
     // Start vector: std::mt19937(1) normals in the user's constraint order (pdlp.cu:2632-2638).
-    std::vector<double> z0(m);
-    std::mt19937 gen(1);
-    std::normal_distribution<double> dist(0.0, 1.0);
-    for (int i = 0; i < m; ++i) z0[i] = dist(gen);
+    const auto seq          = power_start_sequence(m);
+    const std::vector<double>& z0 = *seq;
     dbuf<double> dz(m), dq(m), datq(n);
     dbuf<power_state> ps(1);
     ps.zero(s_);
@@ -442,10 +440,8 @@ class engine {
   void lanczos_step_size()
   {
     const int m = in_.m, n = in_.n;
-    std::vector<double> z0(m);
-    std::mt19937 gen(1);
-    std::normal_distribution<double> dist(0.0, 1.0);
-    for (int i = 0; i < m; ++i) z0[i] = dist(gen);
+    const auto seq          = power_start_sequence(m);
+    const std::vector<double>& z0 = *seq;
     constexpr int kChunk = kLanczosChunk, kMaxSteps = kLanczosMaxSteps;
     dbuf<double> u(m), v(n), tmp(m), alphas(kMaxSteps + 1), betas(kMaxSteps + 2);
     dbuf<gk_state> st(1);
@@ -1111,10 +1107,9 @@ pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p)
     r.x.resize(n);
     r.y.resize(m);
     r.rc.resize(n);
-    x.download(r.x.data(), n, s);
-    y.download(r.y.data(), m, s);
-    rc.download(r.rc.data(), n, s);
-    B200_CUDA_CHECK(cudaStreamSynchronize(s));
+    staged_download(r.x.data(), x.data(), n * sizeof(double), s);
+    staged_download(r.y.data(), y.data(), m * sizeof(double), s);
+    staged_download(r.rc.data(), rc.data(), n * sizeof(double), s);
   }
   return r;
 }

@@ -11,6 +11,8 @@
 #include <limits>
 #include <vector>
 
+#include "host_array.hpp"
+
 namespace cuopt_b200 {
 
 // The LP as handed over by the C interface: user order, minimise or maximise,
@@ -57,7 +59,7 @@ struct pdlp_params {
 
 struct pdlp_result {
   int status = 0;  // CUOPT_TERIMINATION_STATUS_*
-  std::vector<double> x, y, rc;
+  host_array<double> x, y, rc;  // user order
   int64_t iterations = 0;
   double primal_obj = 0, dual_obj = 0;
   double l2_primal = 0, l2_dual = 0, rel_primal = 0, rel_dual = 0, gap = 0, rel_gap = 0;

@@ -3,6 +3,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <memory>
+#include <mutex>
+#include <random>
 #include <vector>
 
 namespace cuopt_b200 {
@@ -83,6 +86,24 @@ inline double largest_bidiagonal_sigma2(const double* a, const double* b, int k)
       lo = mid;
   }
   return hi;
+}
+
+// Start vector of the step-size iterations: normals of std::mt19937(1) (reference
+// pdlp.cu:2632-2638).  The sequence does not depend on the LP, so its values are generated once
+// per process and shared; a solve (or batch instance) with m rows takes the first m.
+inline std::shared_ptr<const std::vector<double>> power_start_sequence(size_t count)
+{
+  static std::mutex mu;
+  static std::shared_ptr<const std::vector<double>> cached;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!cached || cached->size() < count) {
+    auto v = std::make_shared<std::vector<double>>(count);
+    std::mt19937 gen(1);
+    std::normal_distribution<double> dist(0.0, 1.0);
+    for (auto& x : *v) x = dist(gen);
+    cached = std::move(v);
+  }
+  return cached;
 }
 
 // Stopping rule of the Golub-Kahan-Lanczos step size: steps run in chunks of kLanczosChunk; after
