@@ -404,9 +404,9 @@ def run_b200(args):
     if rank == 0 and world == 1 and not args.no_batch:
         from cuopt_b200.profile import run_batch
         batch = run_batch(argparse.Namespace(count=512, sequential=args.batch_sequential,
-                                             repeats=2, tol=1e-6, time_limit=120.0))
+                                             repeats=3, tol=1e-6, time_limit=120.0))
         batch_mixed = run_batch(argparse.Namespace(count=512, sequential=args.batch_sequential,
-                                                   repeats=2, tol=1e-6, time_limit=120.0,
+                                                   repeats=3, tol=1e-6, time_limit=120.0,
                                                    batch_precision="mixed"))
     # Config 4: 64 non-degenerate 5000 x 10000 LPs, batched forward (crossover) + KKT adjoint.
     adjoint = None

@@ -69,10 +69,99 @@ lp_problem* P(cuOptOptimizationProblem p) { return static_cast<lp_problem*>(p); 
 lp_settings* S(cuOptSolverSettings s) { return static_cast<lp_settings*>(s); }
 lp_solution* R(cuOptSolution s) { return static_cast<lp_solution*>(s); }
 
+// Device copy of a new problem's arrays (see device_problem), started before the host copies
+// when every array is pinned host memory or memory of the current device, so that the DMA engine
+// reads them while host threads make the library's own copies.  finish() waits for it (the caller
+// may free its arrays once the create call returns); on any failure there is simply no copy.
+class device_copy {
+ public:
+  struct array {
+    const void* src;
+    size_t bytes;
+  };
+  explicit device_copy(const std::vector<array>& arrays)
+  {
+    if (!start(arrays)) fail();
+  }
+  ~device_copy()
+  {
+    if (s_) {
+      cudaStreamSynchronize(s_);
+      cudaStreamDestroy(s_);
+    }
+  }
+  // The copy's arrays in the order given, once they have arrived (null: no copy).
+  std::shared_ptr<cuopt_b200::device_problem> finish(std::vector<void*>& dst)
+  {
+    if (!s_ || !dev_) return nullptr;
+    const bool ok = cudaStreamSynchronize(s_) == cudaSuccess;
+    cudaStreamDestroy(s_);
+    s_ = nullptr;
+    if (!ok) {
+      fail();
+      return nullptr;
+    }
+    dst = dst_;
+    return std::move(dev_);
+  }
+
+ private:
+  bool start(const std::vector<array>& arrays)
+  {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    size_t total = 0;
+    for (const array& a : arrays) {
+      if (!a.src || a.bytes == 0) continue;
+      cudaPointerAttributes attr{};
+      if (cudaPointerGetAttributes(&attr, a.src) != cudaSuccess) return false;
+      const bool pinned = attr.type == cudaMemoryTypeHost;
+      const bool local  = attr.type == cudaMemoryTypeDevice && attr.device == dev;
+      if (!pinned && !local) return false;
+      total += (a.bytes + 255) / 256 * 256;
+    }
+    if (total == 0) return true;
+    cuopt_b200::configure_pool_once();
+    if (cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking) != cudaSuccess) {
+      s_ = nullptr;
+      return false;
+    }
+    dev_         = std::make_shared<cuopt_b200::device_problem>();
+    dev_->device = dev;
+    if (cudaMallocAsync(&dev_->base, total, s_) != cudaSuccess) {
+      dev_->base = nullptr;
+      return false;
+    }
+    size_t at = 0;
+    for (const array& a : arrays) {
+      void* dst = nullptr;
+      if (a.src && a.bytes) {
+        dst = static_cast<char*>(dev_->base) + at;
+        if (cudaMemcpyAsync(dst, a.src, a.bytes, cudaMemcpyDefault, s_) != cudaSuccess)
+          return false;
+        at += (a.bytes + 255) / 256 * 256;
+      }
+      dst_.push_back(dst);
+    }
+    return true;
+  }
+  // No copy: copies in flight finish before the allocation is released.
+  void fail()
+  {
+    if (s_) cudaStreamSynchronize(s_);
+    cudaGetLastError();
+    dev_.reset();
+  }
+  cudaStream_t s_ = nullptr;
+  std::shared_ptr<cuopt_b200::device_problem> dev_;
+  std::vector<void*> dst_;
+};
+
 cuopt_int_t create_common(cuopt_int_t m, cuopt_int_t n, cuopt_int_t sense, cuopt_float_t offset,
                           const cuopt_float_t* c, const cuopt_int_t* off, const cuopt_int_t* idx,
                           const cuopt_float_t* val, const cuopt_float_t* vlo,
-                          const cuopt_float_t* vup, const char* vtypes, lp_problem* p)
+                          const cuopt_float_t* vup, const char* vtypes, const cuopt_float_t* clo,
+                          const cuopt_float_t* cup, lp_problem* p)
 {
   if (m < 0 || n < 0) return CUOPT_INVALID_ARGUMENT;
   p->m          = m;
@@ -83,10 +172,36 @@ cuopt_int_t create_common(cuopt_int_t m, cuopt_int_t n, cuopt_int_t sense, cuopt
   copy_in(p->row_off, off, (size_t)m + 1);
   const int64_t nnz = p->row_off[m];
   if (nnz < 0) return CUOPT_INVALID_ARGUMENT;
+  const bool ranged = clo && cup;
+  device_copy copy({{off, ((size_t)m + 1) * sizeof(int)},
+                    {idx, (size_t)nnz * sizeof(int)},
+                    {val, (size_t)nnz * sizeof(double)},
+                    {c, (size_t)n * sizeof(double)},
+                    {vlo, (size_t)n * sizeof(double)},
+                    {vup, (size_t)n * sizeof(double)},
+                    {ranged ? clo : nullptr, (size_t)m * sizeof(double)},
+                    {ranged ? cup : nullptr, (size_t)m * sizeof(double)}});
   copy_in(p->col_idx, idx, (size_t)nnz);
   copy_in(p->val, val, (size_t)nnz);
   copy_in(p->var_lo, vlo, n);
   copy_in(p->var_up, vup, n);
+  if (ranged) {
+    p->ranged = true;
+    copy_in(p->con_lo, clo, m);
+    copy_in(p->con_up, cup, m);
+  }
+  std::vector<void*> d;
+  if (auto dp = copy.finish(d); dp && m > 0 && n > 0 && nnz > 0) {
+    dp->row_off = static_cast<const int*>(d[0]);
+    dp->col_idx = static_cast<const int*>(d[1]);
+    dp->val     = static_cast<const double*>(d[2]);
+    dp->c       = static_cast<const double*>(d[3]);
+    dp->var_lo  = static_cast<const double*>(d[4]);
+    dp->var_up  = static_cast<const double*>(d[5]);
+    dp->con_lo  = static_cast<const double*>(d[6]);
+    dp->con_up  = static_cast<const double*>(d[7]);
+    p->dev.p    = std::move(dp);
+  }
   if (vtypes) {
     std::vector<char> t;
     copy_in(t, vtypes, n);
@@ -160,7 +275,7 @@ cuopt_int_t cuOptCreateProblem(cuopt_int_t num_constraints, cuopt_int_t num_vari
                                    objective_offset, objective_coefficients,
                                    constraint_matrix_row_offsets, constraint_matrix_column_indices,
                                    constraint_matrix_coefficent_values, lower_bounds, upper_bounds,
-                                   variable_types, p);
+                                   variable_types, nullptr, nullptr, p);
     if (rc != CUOPT_SUCCESS) {
       delete p;
       return rc;
@@ -201,14 +316,12 @@ cuopt_int_t cuOptCreateRangedProblem(cuopt_int_t num_constraints, cuopt_int_t nu
       create_common(num_constraints, num_variables, objective_sense, objective_offset,
                     objective_coefficients, constraint_matrix_row_offsets,
                     constraint_matrix_column_indices, constraint_matrix_coefficients,
-                    variable_lower_bounds, variable_upper_bounds, variable_types, p);
+                    variable_lower_bounds, variable_upper_bounds, variable_types,
+                    constraint_lower_bounds, constraint_upper_bounds, p);
     if (rc != CUOPT_SUCCESS) {
       delete p;
       return rc;
     }
-    p->ranged = true;
-    copy_in(p->con_lo, constraint_lower_bounds, num_constraints);
-    copy_in(p->con_up, constraint_upper_bounds, num_constraints);
   } catch (const std::exception&) {
     delete p;
     return CUOPT_INVALID_ARGUMENT;

@@ -448,6 +448,21 @@ static bool prepare_for_pdlp(const lp_problem& p, const lp_settings& st, row_bou
   return true;
 }
 
+device_problem::~device_problem()
+{
+  if (!base) return;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != device) cudaSetDevice(device);
+  cudaStream_t s;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess) {
+    cudaFreeAsync(base, s);
+    cudaStreamDestroy(s);
+  }
+  if (cur >= 0 && cur != device) cudaSetDevice(cur);
+  cudaGetLastError();
+}
+
 static void set_error(lp_solution& out, int code, const char* what)
 {
   out.error_code    = code;
@@ -465,6 +480,7 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
     if ((int)st.initial_primal.size() == p.n) prm.initial_primal = st.initial_primal;
     if ((int)st.initial_dual.size() == p.m) prm.initial_dual = st.initial_dual;
     lp_input in;
+    in.dev        = p.dev.p.get();
     in.m          = p.m;
     in.n          = p.n;
     in.row_off    = p.row_off.data();

@@ -31,6 +31,20 @@ struct lp_problem {
   bool quadratic = false;
   std::vector<std::string> row_names, col_names;
   std::string name, objective_name;
+  // Device copy made at creation (see device_problem).  A copy of the problem (e.g. one with a
+  // variable's bounds changed) does not share it.
+  struct mirror_ref {
+    std::shared_ptr<const device_problem> p;
+    mirror_ref() = default;
+    mirror_ref(const mirror_ref&) {}
+    mirror_ref& operator=(const mirror_ref&)
+    {
+      p.reset();
+      return *this;
+    }
+    mirror_ref(mirror_ref&&) noexcept            = default;
+    mirror_ref& operator=(mirror_ref&&) noexcept = default;
+  } dev;
 
   // Constraint bounds as PDLP sees them (reference problem_helpers.cuh:26-51).
   void constraint_bounds(std::vector<double>& lo, std::vector<double>& up) const;

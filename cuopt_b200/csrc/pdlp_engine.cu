@@ -1062,32 +1062,35 @@ pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p)
   configure_pool_once();
   const int m = in.m, n = in.n;
   const int64_t nnz = in.row_off[m];
-  dbuf<int> off(m + 1), idx(std::max<int64_t>(nnz, 1));
-  dbuf<double> val(std::max<int64_t>(nnz, 1)), c(n), lo(m), up(m), vl(n), vu(n), x(n), y(m), rc(n),
-    ip, id;
+  // A device copy made at problem creation (same device) replaces the upload of its arrays.
+  const device_problem* dv = in.dev;
+  if (dv) {
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != dv->device) dv = nullptr;
+  }
+  dbuf<int> off, idx;
+  dbuf<double> val, c, lo, up, vl, vu, x(n), y(m), rc(n), ip, id;
+  lp_device_input d;
   {
     staged_upload h2d(s);
-    h2d.put(off.data(), in.row_off, m + 1);
-    h2d.put(idx.data(), in.col_idx, nnz);
-    h2d.put(val.data(), in.val, nnz);
-    h2d.put(c.data(), in.c, n);
-    h2d.put(lo.data(), in.con_lo, m);
-    h2d.put(up.data(), in.con_up, m);
-    h2d.put(vl.data(), in.var_lo, n);
-    h2d.put(vu.data(), in.var_up, n);
+    auto put = [&](auto& buf, const auto* host, const auto* mirrored, int64_t count) {
+      if (mirrored) return mirrored;
+      buf.resize((size_t)std::max<int64_t>(count, 1));
+      h2d.put(buf.data(), host, (size_t)count);
+      return static_cast<decltype(mirrored)>(buf.data());
+    };
+    d.row_off = put(off, in.row_off, dv ? dv->row_off : nullptr, m + 1);
+    d.col_idx = put(idx, in.col_idx, dv ? dv->col_idx : nullptr, nnz);
+    d.val     = put(val, in.val, dv ? dv->val : nullptr, nnz);
+    d.c       = put(c, in.c, dv ? dv->c : nullptr, n);
+    d.con_lo  = put(lo, in.con_lo, dv ? dv->con_lo : nullptr, m);
+    d.con_up  = put(up, in.con_up, dv ? dv->con_up : nullptr, m);
+    d.var_lo  = put(vl, in.var_lo, dv ? dv->var_lo : nullptr, n);
+    d.var_up  = put(vu, in.var_up, dv ? dv->var_up : nullptr, n);
     h2d.finish();
   }
-  lp_device_input d;
-  d.m = m;
-  d.n = n;
-  d.row_off = off.data();
-  d.col_idx = idx.data();
-  d.val     = val.data();
-  d.c       = c.data();
-  d.con_lo  = lo.data();
-  d.con_up  = up.data();
-  d.var_lo  = vl.data();
-  d.var_up  = vu.data();
+  d.m          = m;
+  d.n          = n;
   d.obj_offset = in.obj_offset;
   d.maximize   = in.maximize;
   if ((int)p.initial_primal.size() == n) {

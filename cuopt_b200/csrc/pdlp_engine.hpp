@@ -17,7 +17,26 @@ namespace cuopt_b200 {
 
 // The LP as handed over by the C interface: user order, minimise or maximise,
 // con_lo <= A x <= con_up, var_lo <= x <= var_up.
+// Device copies of a problem's arrays in the user's order, made when the problem is created from
+// pinned host memory or device memory (the reference keeps its problems on the device too); a
+// host-path solve on the same device reads them instead of uploading.  Null members were not
+// copied.  The arrays live in one allocation, released with the object.
+struct device_problem {
+  int device         = -1;
+  void* base         = nullptr;
+  const int* row_off = nullptr;
+  const int* col_idx = nullptr;
+  const double* val  = nullptr;
+  const double* c = nullptr, *var_lo = nullptr, *var_up = nullptr;
+  const double* con_lo = nullptr, *con_up = nullptr;
+  device_problem() = default;
+  device_problem(const device_problem&)            = delete;
+  device_problem& operator=(const device_problem&) = delete;
+  ~device_problem();
+};
+
 struct lp_input {
+  const device_problem* dev = nullptr;  // optional device copy of the arrays below
   int m = 0, n = 0;
   const int* row_off    = nullptr;  // m + 1
   const int* col_idx    = nullptr;  // nnz

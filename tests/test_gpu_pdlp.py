@@ -330,3 +330,49 @@ def test_mixed_precision_stall_continues_in_fp64():
     assert [s.stats["refinement_passes"] for s in sols] == [1, 0]
     assert rel(sols[0].get_primal_objective(), lp.optimal_objective) <= 1e-5
     assert rel(sols[1].get_primal_objective(), other.optimal_objective) <= 1e-5
+
+
+def test_problem_from_pinned_or_device_arrays_solves_identically(small_lp):
+    """cuOptCreateRangedProblem from pinned host arrays (or device arrays) keeps a device copy made
+    while the library copies the arrays, and cuOptSolve reads it instead of uploading: the result
+    is bitwise that of the same problem created from pageable arrays."""
+    import ctypes as C
+    torch = pytest.importorskip("torch")
+    from cuopt_b200._lib import lib
+    L = lib()
+    lp = small_lp
+    arrays = [(lp.c, np.float64), (lp.row_off, np.int32), (lp.col_idx, np.int32),
+              (lp.val, np.float64), (lp.con_lo, np.float64), (lp.con_up, np.float64),
+              (lp.var_lo, np.float64), (lp.var_up, np.float64)]
+    s = settings(tol=1e-8)._create()
+
+    def solve(kind):
+        if kind == "pageable":
+            bufs = [np.ascontiguousarray(a, dtype=dt) for a, dt in arrays]
+            ptrs = [C.c_void_p(b.ctypes.data) for b in bufs]
+        else:
+            bufs = [torch.as_tensor(np.ascontiguousarray(a, dtype=dt)) for a, dt in arrays]
+            bufs = [b.pin_memory() if kind == "pinned" else b.cuda() for b in bufs]
+            ptrs = [C.c_void_p(b.data_ptr()) for b in bufs]
+        h, sol = C.c_void_p(), C.c_void_p()
+        assert L.cuOptCreateRangedProblem(lp.m, lp.n, 1, 0.0, *ptrs, b"C" * lp.n, C.byref(h)) == 0
+        del bufs  # the library holds its own copies
+        assert L.cuOptSolve(h, s, C.byref(sol)) == 0
+        x, y = np.zeros(lp.n), np.zeros(lp.m)
+        L.cuOptGetPrimalSolution(sol, C.c_void_p(x.ctypes.data))
+        L.cuOptGetDualSolution(sol, C.c_void_p(y.ctypes.data))
+        status = C.c_int32()
+        L.cuOptGetTerminationStatus(sol, C.byref(status))
+        L.cuOptDestroySolution(C.byref(sol))
+        L.cuOptDestroyProblem(C.byref(h))
+        return status.value, x, y
+
+    try:
+        ref = solve("pageable")
+        assert ref[0] == 1
+        for kind in ("pinned", "device"):
+            got = solve(kind)
+            assert got[0] == ref[0]
+            assert np.array_equal(got[1], ref[1]) and np.array_equal(got[2], ref[2])
+    finally:
+        L.cuOptDestroySolverSettings(C.byref(s))
