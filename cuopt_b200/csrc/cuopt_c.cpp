@@ -62,7 +62,7 @@ void copy_out(T* dst, const std::vector<T, A>& src)
     return;
   }
   cudaGetLastError();
-  std::memcpy(dst, src.data(), src.size() * sizeof(T));
+  cuopt_b200::parallel_memcpy(dst, src.data(), src.size() * sizeof(T));
 }
 
 lp_problem* P(cuOptOptimizationProblem p) { return static_cast<lp_problem*>(p); }

@@ -19,7 +19,7 @@ namespace cuopt_b200 {
 // memcpy split over up to 8 host threads for large copies.
 inline void parallel_memcpy(void* dst, const void* src, size_t bytes)
 {
-  constexpr size_t kChunk = size_t(8) << 20;
+  constexpr size_t kChunk = size_t(2) << 20;  // at least this much per thread
   const unsigned hw       = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
   const unsigned parts    = (unsigned)std::min<size_t>(hw, bytes / kChunk);
   if (parts <= 1) {
@@ -134,22 +134,23 @@ class staged_upload {
 };
 
 // Copies `bytes` of device memory to host memory through the pinned staging buffers, after the
-// work already queued on `s`: the DMA engine fills one buffer while host threads empty the other.
-// Returns when the host copy is complete.
+// work already queued on `s`: the DMA engine fills one buffer while host threads empty the other,
+// in pieces of kPiece bytes so the two overlap.  Returns when the host copy is complete.
 inline void staged_download(void* dst, const void* src, size_t bytes, cudaStream_t s)
 {
+  constexpr size_t kPiece = size_t(8) << 20;
   if (bytes == 0) return;
   auto& st      = staging();
   auto* d       = static_cast<char*>(dst);
   const auto* h = static_cast<const char*>(src);
   size_t off    = 0;
   int cur       = 0;
-  size_t n      = std::min(bytes, kStageBytes);
+  size_t n      = std::min(bytes, kPiece);
   B200_CUDA_CHECK(cudaMemcpyAsync(st.buf[cur], h, n, cudaMemcpyDeviceToHost, s));
   B200_CUDA_CHECK(cudaEventRecord(st.done[cur], s));
   for (;;) {
     const size_t next = off + n;
-    const size_t nn   = std::min(bytes - next, kStageBytes);
+    const size_t nn   = std::min(bytes - next, kPiece);
     if (nn > 0) {
       B200_CUDA_CHECK(cudaMemcpyAsync(st.buf[1 - cur], h + next, nn, cudaMemcpyDeviceToHost, s));
       B200_CUDA_CHECK(cudaEventRecord(st.done[1 - cur], s));
