@@ -355,6 +355,34 @@ void build_device_layout(int m, int n, const int* d_off, const int* d_idx, const
   B200_CUDA_CHECK(cudaStreamSynchronize(s));
 }
 
+// One block per instance b of a batch whose arrays were uploaded instance by instance: row
+// offsets and column indices become global (row_off[r0 + i + 1] += first non-zero of b;
+// col_idx += first column of b) and every row / column records its instance.
+__global__ void rebase_batch_kernel(const int* row_start, const int* col_start,
+                                    const int* nnz_start, int* row_off, int* col_idx,
+                                    int* row_inst, int* col_inst)
+{
+  const int b  = blockIdx.x;
+  const int e0 = nnz_start[b], c0 = col_start[b];
+  for (int i = row_start[b] + threadIdx.x; i < row_start[b + 1]; i += blockDim.x) {
+    row_off[i + 1] += e0;
+    row_inst[i] = b;
+  }
+  for (int j = c0 + threadIdx.x; j < col_start[b + 1]; j += blockDim.x) col_inst[j] = b;
+  for (int k = e0 + threadIdx.x; k < nnz_start[b + 1]; k += blockDim.x) col_idx[k] += c0;
+}
+
+void rebase_batch_arrays(int count, const int* row_start, const int* col_start,
+                         const int* nnz_start, int* row_off, int* col_idx, int* row_inst,
+                         int* col_inst, cudaStream_t s)
+{
+  B200_CUDA_CHECK(cudaMemsetAsync(row_off, 0, sizeof(int), s));
+  if (count > 0)
+    rebase_batch_kernel<<<count, kT, 0, s>>>(row_start, col_start, nnz_start, row_off, col_idx,
+                                             row_inst, col_inst);
+  B200_LAUNCH_CHECK();
+}
+
 void permute_gather(const double* src, const int* perm, int count, double sign, double* dst,
                     cudaStream_t s)
 {

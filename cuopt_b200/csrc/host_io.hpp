@@ -36,6 +36,36 @@ inline void parallel_memcpy(void* dst, const void* src, size_t bytes)
   for (auto& th : pool) th.join();
 }
 
+// Copies the pieces one after another into dst, split over up to 8 host threads by bytes (a
+// thread's range may cover many small pieces or part of a large one).
+struct host_piece {
+  const void* src;
+  size_t bytes;
+};
+inline void parallel_gather(char* dst, const host_piece* pieces, size_t count, size_t total)
+{
+  constexpr size_t kPerThread = size_t(2) << 20;
+  const unsigned hw    = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  const unsigned parts = (unsigned)std::max<size_t>(1, std::min<size_t>(hw, total / kPerThread));
+  auto copy_range = [&](size_t lo, size_t hi) {  // bytes [lo, hi) of the concatenation
+    size_t at = 0;
+    for (size_t i = 0; i < count && at < hi; ++i) {
+      const size_t b = pieces[i].bytes, s0 = std::max(lo, at), s1 = std::min(hi, at + b);
+      if (s0 < s1)
+        std::memcpy(dst + s0, static_cast<const char*>(pieces[i].src) + (s0 - at), s1 - s0);
+      at += b;
+    }
+  };
+  if (parts <= 1) {
+    copy_range(0, total);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < parts; ++t)
+    pool.emplace_back(copy_range, total * t / parts, total * (t + 1) / parts);
+  for (auto& th : pool) th.join();
+}
+
 // Two pinned staging buffers per host thread (allocated once), shared by staged_upload and
 // staged_download.
 constexpr size_t kStageBytes = size_t(32) << 20;
@@ -87,6 +117,39 @@ class staged_upload {
       d += n;
       h += n;
       bytes -= n;
+    }
+  }
+
+  // Uploads the pieces, in order, to consecutive device memory from dst (inside one allocation),
+  // filling the staging buffers with all host threads.
+  void put_gather(void* dst, const std::vector<host_piece>& pieces)
+  {
+    auto* d = static_cast<char*>(dst);
+    std::vector<host_piece> window;
+    size_t i = 0, skip = 0;  // next piece, bytes of it already sent
+    while (i < pieces.size()) {
+      if (used_ == kStage) flush();
+      const size_t space = kStage - used_;
+      size_t filled      = 0;
+      window.clear();
+      while (i < pieces.size() && filled < space) {
+        const size_t rest = pieces[i].bytes - skip;
+        const size_t take = std::min(rest, space - filled);
+        if (take > 0)
+          window.push_back({static_cast<const char*>(pieces[i].src) + skip, take});
+        filled += take;
+        if (take == rest) {
+          ++i;
+          skip = 0;
+        } else {
+          skip += take;
+        }
+      }
+      if (filled == 0) continue;
+      parallel_gather(state().buf[cur_] + used_, window.data(), window.size(), filled);
+      pending_.push_back({d, used_, filled});
+      used_ += filled;
+      d += filled;
     }
   }
 

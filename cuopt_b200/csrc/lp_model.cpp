@@ -541,45 +541,9 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
     bi.maximize.push_back(p.maximize ? 1 : 0);
   }
   const int m = bi.row_start.back(), n = bi.col_start.back();
-  // Uninitialised host arrays (every element is written below; zero-filling 10^8 elements would
-  // cost as much as the copy itself).
   const size_t nz = (size_t)std::max<int64_t>(nnz, 1);
-  host_array<int> off(m + 1), idx(nz), rinst(m), cinst(n);
-  host_array<double> val(nz), c(n), clo(m), cup(m), vlo(n), vup(n);
-  off[0] = 0;
-  // Row offsets first (prefix over instances), then every instance's pieces in parallel.
   std::vector<int> e0(bi.count + 1, 0);
   for (int b = 0; b < bi.count; ++b) e0[b + 1] = e0[b] + ps[ids[b]]->row_off[ps[ids[b]]->m];
-  auto fill_instance = [&](int b) {
-    const lp_problem& p = *ps[ids[b]];
-    const int r0 = bi.row_start[b], c0 = bi.col_start[b], base = e0[b];
-    for (int i = 0; i < p.m; ++i) {
-      off[r0 + i + 1] = base + p.row_off[i + 1];
-      clo[r0 + i]     = rb[ids[b]].lo[i];
-      cup[r0 + i]     = rb[ids[b]].up[i];
-      rinst[r0 + i]   = b;
-    }
-    for (int k = 0; k < p.row_off[p.m]; ++k) {
-      idx[base + k] = p.col_idx[k] + c0;
-      val[base + k] = p.val[k];
-    }
-    for (int j = 0; j < p.n; ++j) {
-      c[c0 + j]     = p.c[j];
-      vlo[c0 + j]   = p.var_lo[j];
-      vup[c0 + j]   = p.var_up[j];
-      cinst[c0 + j] = b;
-    }
-  };
-  {
-    const int nt = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
-    std::vector<std::thread> pool;
-    for (int t = 0; t < nt; ++t)
-      pool.emplace_back([&, t] {
-        for (int b = t; b < bi.count; b += nt) fill_instance(b);
-      });
-    for (auto& th : pool) th.join();
-  }
-  trace("batch: concatenate");
   cudaStream_t s;
   B200_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   struct stream_guard {
@@ -588,24 +552,52 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
   } guard{s};
   alloc_scope scope(s);
   configure_pool_once();
-  dbuf<int> doff(m + 1), didx(nz), dri(m), dci(n);
+  dbuf<int> doff(m + 1), didx(nz), dri(m), dci(n), drs(bi.count + 1), dcs(bi.count + 1),
+    des(bi.count + 1);
   dbuf<double> dval(nz), dc(n), dlo(m), dup(m), dvl(n), dvu(n), x(n), y(m), rc(n);
   B200_CUDA_CHECK(cudaStreamSynchronize(s));
   trace("batch: device allocation");
   {
+    // Every instance's arrays go straight to their place in the batch arrays (consecutive
+    // instances of one array travel as one copy); offsets, indices and instance ids are made
+    // global on the device.
     staged_upload h2d(s);
-    h2d.put(doff.data(), off.data(), m + 1);
-    h2d.put(didx.data(), idx.data(), nz);
-    h2d.put(dval.data(), val.data(), nz);
-    h2d.put(dri.data(), rinst.data(), m);
-    h2d.put(dci.data(), cinst.data(), n);
-    h2d.put(dc.data(), c.data(), n);
-    h2d.put(dlo.data(), clo.data(), m);
-    h2d.put(dup.data(), cup.data(), m);
-    h2d.put(dvl.data(), vlo.data(), n);
-    h2d.put(dvu.data(), vup.data(), n);
+    std::vector<host_piece> pieces(bi.count);
+    auto gather = [&](auto* dst, auto&& piece_of) {
+      for (int b = 0; b < bi.count; ++b) pieces[b] = piece_of(*ps[ids[b]], b);
+      h2d.put_gather(dst, pieces);
+    };
+    gather(doff.data() + 1, [&](const lp_problem& p, int) {
+      return host_piece{p.row_off.data() + 1, (size_t)p.m * sizeof(int)};
+    });
+    gather(didx.data(), [&](const lp_problem& p, int) {
+      return host_piece{p.col_idx.data(), (size_t)p.row_off[p.m] * sizeof(int)};
+    });
+    gather(dval.data(), [&](const lp_problem& p, int) {
+      return host_piece{p.val.data(), (size_t)p.row_off[p.m] * sizeof(double)};
+    });
+    gather(dc.data(), [&](const lp_problem& p, int) {
+      return host_piece{p.c.data(), (size_t)p.n * sizeof(double)};
+    });
+    gather(dlo.data(), [&](const lp_problem& p, int b) {
+      return host_piece{rb[ids[b]].lo, (size_t)p.m * sizeof(double)};
+    });
+    gather(dup.data(), [&](const lp_problem& p, int b) {
+      return host_piece{rb[ids[b]].up, (size_t)p.m * sizeof(double)};
+    });
+    gather(dvl.data(), [&](const lp_problem& p, int) {
+      return host_piece{p.var_lo.data(), (size_t)p.n * sizeof(double)};
+    });
+    gather(dvu.data(), [&](const lp_problem& p, int) {
+      return host_piece{p.var_up.data(), (size_t)p.n * sizeof(double)};
+    });
+    h2d.put(drs.data(), bi.row_start.data(), bi.count + 1);
+    h2d.put(dcs.data(), bi.col_start.data(), bi.count + 1);
+    h2d.put(des.data(), e0.data(), bi.count + 1);
     h2d.finish();
   }
+  rebase_batch_arrays(bi.count, drs.data(), dcs.data(), des.data(), doff.data(), didx.data(),
+                      dri.data(), dci.data(), s);
   bi.m        = m;
   bi.n        = n;
   bi.row_off  = doff.data();

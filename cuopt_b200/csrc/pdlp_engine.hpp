@@ -133,6 +133,13 @@ struct batch_device_input {
   std::vector<char> maximize;
 };
 
+// Arrays of a batch uploaded instance by instance (instance b's rows from row_start[b], columns
+// from col_start[b], non-zeros from nnz_start[b]; all three device arrays of count + 1 entries):
+// makes the row offsets and column indices global and fills the instance of every row / column.
+void rebase_batch_arrays(int count, const int* row_start, const int* col_start,
+                         const int* nnz_start, int* row_off, int* col_idx, int* row_inst,
+                         int* col_inst, cudaStream_t s);
+
 pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p);
 
 // Solves every instance of the batch with its own Stable3 state; x / y / reduced costs are written
