@@ -220,6 +220,14 @@ def cpu_sample(lp, target_s: float, threads: int):
     return t / iters, iters
 
 
+def bench_config(args, lp, world):
+    """The workload both arms report (the reference arm times the same one on the host)."""
+    return {"workload": f"{args.config}: {lp.m}x{lp.n} LP, {lp.nnz} nnz, Stable3 PDLP to 1e-6 "
+                        "relative KKT, mixed precision", "replicas": world,
+            "l2": "inputs larger than L2 (matrix 16M nnz, >= 190 MB per copy)",
+            "parallelism": f"replicas x{world}"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -240,7 +248,7 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * s_iter * iters_needed, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{args.config}: {lp.m}x{lp.n} LP, {lp.nnz} nnz, Stable3 PDLP to 1e-6"},
+        "config": bench_config(args, lp, 1),
         "cpu_baseline": {"value": value, "unit": "LPs/s to 1e-6 rel. KKT", "cores": threads,
                          "kind": "port",
                          "sample": f"oracle FP64 PDHG, {n} iterations per step on {threads} threads, "
@@ -422,10 +430,7 @@ def run_b200(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 mixed",
         "data": "synthetic (seeded generator, optimum known by construction)",
-        "config": {"workload": f"{args.config}: {lp.m}x{lp.n} LP, {lp.nnz} nnz, Stable3 PDLP to 1e-6 "
-                               "relative KKT, mixed precision", "replicas": world,
-                   "l2": "inputs larger than L2 (matrix 16M nnz, >= 190 MB per copy)",
-                   "parallelism": f"replicas x{world}"},
+        "config": bench_config(args, lp, world),
         "status": status_mixed, "iterations": last_mixed["number_of_steps_taken"],
         "pdhg_iter_per_s": last_mixed["number_of_steps_taken"] / (last_mixed["loop_time"] or 1e-9),
         "setup_s": last_mixed["setup_time"], "loop_s": last_mixed["loop_time"],
