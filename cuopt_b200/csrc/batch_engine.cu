@@ -400,6 +400,20 @@ __global__ void b_restart_kernel(TX* x, TX* xa, const TX* xhat, int n, TX* y, TX
   }
 }
 
+// Warm start: a = b = c = v / d (v / d = v where d = 0) times the instance's factor f[inst].
+template <typename TX>
+__global__ void b_scale_initial_kernel(const double* v, const double* d, const int* inst,
+                                       const double* f, int n, TX* a, TX* b, TX* c)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double s = d[i] != 0.0 ? v[i] / d[i] : v[i];
+    const TX w     = (TX)(s * f[inst[i]]);
+    a[i]           = w;
+    b[i]           = w;
+    c[i]           = w;
+  }
+}
+
 __global__ void b_advance_kernel(pdlp_scalars* sc, const int* active, int count, int steps)
 {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < count; b += gridDim.x * blockDim.x)
@@ -751,7 +765,10 @@ class batch_engine {
     trace("batch: vectors");
     // Step size from the largest singular value of each scaled instance: the power iteration
     // (reference pdlp.cu:2620-2731), or Golub-Kahan-Lanczos in mixed precision, as single solves.
-    if (p_.precision == 1)
+    if ((int)in_.initial_step.size() == B_) {
+      eta_ = in_.initial_step;
+      power_iters_.assign(B_, 0);
+    } else if (p_.precision == 1)
       lanczos_step_size();
     else
       power_iteration();
@@ -764,8 +781,11 @@ class batch_engine {
     su_.zero(s_);
     yu_.zero(s_);
     sc_d_.resize(B_);
-    omega_.assign(B_, 1.0);
-    best_omega_.assign(B_, 1.0);
+    if ((int)in_.initial_weight.size() == B_)
+      omega_ = in_.initial_weight;
+    else
+      omega_.assign(B_, 1.0);
+    best_omega_ = omega_;
     restarts_.assign(B_, 0);
     for (auto* b : {&x_, &xhat_, &slack_, &xbar_, &xa_, &aty_}) {
       b->resize(n);
@@ -774,6 +794,24 @@ class batch_engine {
     for (auto* b : {&y_, &yhat_, &ybar_, &ya_}) {
       b->resize(m);
       b->zero(s_);
+    }
+    // Warm start: iterate, anchor and x_hat from the initial solution in the scaled space (the
+    // single engine's load_initial_solution, per instance).
+    if (in_.initial_primal) {
+      dbuf<double> v(n);
+      permute_gather(in_.initial_primal, L_.col_new2old.data(), n, 1.0, v.data(), s_);
+      b_scale_initial_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(v.data(), dc_.data(), cinst_.data(),
+                                                            beta_d_.data(), n, x_.data(),
+                                                            xhat_.data(), xa_.data());
+      B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    }
+    if (in_.initial_dual) {
+      dbuf<double> v(m);
+      permute_gather(in_.initial_dual, L_.row_new2old.data(), m, 1.0, v.data(), s_);
+      b_scale_initial_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(v.data(), dr_.data(), rinst_.data(),
+                                                            gamma_d_.data(), m, y_.data(),
+                                                            yhat_.data(), ya_.data());
+      B200_CUDA_CHECK(cudaStreamSynchronize(s_));
     }
     clamp_kernel<TX><<<vgrid_, kBlock, 0, s_>>>(x_.data(), ls_.data(), us_.data(), n);
     launches_ += 1;

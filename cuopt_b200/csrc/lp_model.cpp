@@ -520,11 +520,19 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
 // Dense active-set factorisations (crossover, adjoint) run at most this many at a time.
 constexpr int kConcurrentPolish = 4;
 
-// One block-diagonal batch on the device (see pdlp_batch_solve_device).
+// Starting point of one instance: its solution (user order; duals in the solver's sign
+// convention), step size and primal weight.
+struct batch_warm {
+  host_array<double> x, y;
+  double step = 0.0, weight = 1.0;
+};
+
+// One block-diagonal batch on the device (see pdlp_batch_solve_device); `warm`, when given, holds
+// a starting point per instance of `ids`.
 static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
                               const std::vector<size_t>& ids, const std::vector<row_bounds>& rb,
-                              const pdlp_params& prm,
-                              bool crossover, std::vector<lp_solution>& out)
+                              const pdlp_params& prm, bool crossover, std::vector<lp_solution>& out,
+                              const std::vector<batch_warm>* warm = nullptr)
 {
   const auto t_chunk = std::chrono::steady_clock::now();
   batch_device_input bi;
@@ -554,7 +562,11 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
   configure_pool_once();
   dbuf<int> doff(m + 1), didx(nz), dri(m), dci(n), drs(bi.count + 1), dcs(bi.count + 1),
     des(bi.count + 1);
-  dbuf<double> dval(nz), dc(n), dlo(m), dup(m), dvl(n), dvu(n), x(n), y(m), rc(n);
+  dbuf<double> dval(nz), dc(n), dlo(m), dup(m), dvl(n), dvu(n), x(n), y(m), rc(n), dx0, dy0;
+  if (warm) {
+    dx0.resize(n);
+    dy0.resize(m);
+  }
   B200_CUDA_CHECK(cudaStreamSynchronize(s));
   trace("batch: device allocation");
   {
@@ -591,6 +603,20 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
     gather(dvu.data(), [&](const lp_problem& p, int) {
       return host_piece{p.var_up.data(), (size_t)p.n * sizeof(double)};
     });
+    if (warm) {
+      gather(dx0.data(), [&](const lp_problem& p, int b) {
+        return host_piece{(*warm)[b].x.data(), (size_t)p.n * sizeof(double)};
+      });
+      gather(dy0.data(), [&](const lp_problem& p, int b) {
+        return host_piece{(*warm)[b].y.data(), (size_t)p.m * sizeof(double)};
+      });
+      bi.initial_primal = dx0.data();
+      bi.initial_dual   = dy0.data();
+      for (const batch_warm& w : *warm) {
+        bi.initial_step.push_back(w.step);
+        bi.initial_weight.push_back(w.weight);
+      }
+    }
     h2d.put(drs.data(), bi.row_start.data(), bi.count + 1);
     h2d.put(dcs.data(), bi.col_start.data(), bi.count + 1);
     h2d.put(des.data(), e0.data(), bi.count + 1);
@@ -623,19 +649,37 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
     o.r.rc.assign(hrc.begin() + bi.col_start[b], hrc.begin() + bi.col_start[b + 1]);
     o.r.y.assign(hy.begin() + bi.row_start[b], hy.begin() + bi.row_start[b + 1]);
   }
-  // Instances whose FP32 iterates stalled are solved again, together, in FP64 (their single
-  // solves would continue in FP64 from the stalled state instead).
+  // Instances whose FP32 iterates stalled continue, together, in FP64 from where they stopped:
+  // their solutions, step sizes and primal weights start an FP64 batch.
   std::vector<size_t> stalled;
+  std::vector<batch_warm> restart;
   for (int b = 0; b < bi.count; ++b)
-    if (rs[b].status == kStalled) stalled.push_back(ids[b]);
+    if (rs[b].status == kStalled) {
+      const lp_solution& o = out[ids[b]];
+      batch_warm w;
+      w.x.assign(o.r.x.begin(), o.r.x.end());
+      w.y.assign(o.r.y.begin(), o.r.y.end());
+      if (bi.maximize[b])  // returned duals are negated for maximisation
+        for (double& v : w.y) v = -v;
+      w.step   = rs[b].step_size;
+      w.weight = rs[b].primal_weight;
+      stalled.push_back(ids[b]);
+      restart.push_back(std::move(w));
+    }
   if (!stalled.empty()) {
     pdlp_params q = prm;
     q.precision   = 0;
     q.time_limit  = std::max(
       0.0, prm.time_limit -
              std::chrono::duration<double>(std::chrono::steady_clock::now() - t_chunk).count());
-    solve_batch_chunk(ps, stalled, rb, q, false, out);
-    for (size_t id : stalled) out[id].r.refinement_passes = 1;
+    std::vector<int64_t> mixed_iters;
+    for (int b = 0; b < bi.count; ++b)
+      if (rs[b].status == kStalled) mixed_iters.push_back(rs[b].iterations);
+    solve_batch_chunk(ps, stalled, rb, q, false, out, &restart);
+    for (size_t i = 0; i < stalled.size(); ++i) {
+      out[stalled[i]].r.refinement_passes = 1;
+      out[stalled[i]].r.iterations += mixed_iters[i];
+    }
   }
   if (!crossover) return;
   // Crossover of the Optimal instances on a few host threads: each polish runs its own stream and

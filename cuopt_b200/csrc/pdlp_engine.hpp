@@ -131,6 +131,12 @@ struct batch_device_input {
   std::vector<int> row_start, col_start;
   std::vector<double> obj_offset;
   std::vector<char> maximize;
+  // Optional warm start (used to continue instances whose FP32 iterates stalled, in FP64):
+  // initial primal / dual solutions in the batch's user order (device, n / m; duals in the
+  // solver's sign convention), and per instance the step size and primal weight to start from.
+  const double* initial_primal = nullptr;
+  const double* initial_dual   = nullptr;
+  std::vector<double> initial_step, initial_weight;
 };
 
 // Arrays of a batch uploaded instance by instance (instance b's rows from row_start[b], columns
