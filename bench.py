@@ -18,7 +18,9 @@ iterates, FP64 termination / restart / step ratio).  The same solve in plain FP6
             6-12 non-zeros per column) solved in FP64 to 1e-6 by one cuOptBatchSolve call, against
             a sample of the same LPs solved one by one with cuOptSolve.
   batch_c3_mixed  the same in mixed precision (batch and single solves): Lanczos step sizes, FP32
-            sweeps; an instance whose FP32 iterates stall is solved again in FP64.
+            sweeps; an instance whose FP32 iterates stall continues in FP64.  Config 3 as
+            specified (FP32 bulk against plain FP64 solves one by one) is its
+            speedup_vs_sequential_fp64.
   adjoint_c4  config 4: 64 non-degenerate 5000 x 10000 LPs solved in one batched call with
             crossover, L = sum w * x* back-propagated through the KKT adjoint, gradients checked
             against the exact basis derivatives and central differences (h = 1e-6).
@@ -416,6 +418,10 @@ def run_b200(args):
         batch_mixed = run_batch(argparse.Namespace(count=512, sequential=args.batch_sequential,
                                                    repeats=3, tol=1e-6, time_limit=120.0,
                                                    batch_precision="mixed"))
+        # Config 3 as specified: the FP32-bulk batch against plain FP64 solves one by one.
+        if batch.get("sequential_lps_per_s"):
+            batch_mixed["speedup_vs_sequential_fp64"] = (batch_mixed["batch_lps_per_s"] /
+                                                         batch["sequential_lps_per_s"])
     # Config 4: 64 non-degenerate 5000 x 10000 LPs, batched forward (crossover) + KKT adjoint.
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint:
