@@ -159,8 +159,13 @@ def _truncated_zipf(rng: np.random.Generator, a: float, cap: int, size: int) -> 
 
 
 def skewed_lp(m: int, n: int, seed: int = 2000, zipf_a: float = 1.3, cap: int = 5000,
-              name: str = "skewed") -> LP:
-    """Config-2 generator (row lengths Zipf(a) on [1, cap], mixed senses, free columns)."""
+              name: str = "skewed", explicit_slacks: bool = False) -> LP:
+    """Config-2 generator (row lengths Zipf(a) on [1, cap], mixed senses, free columns).
+
+    With explicit_slacks, every '<=' row gets a slack column (coefficient +1, bounds [0, inf),
+    cost 0) and becomes an equality, as the config-2 workload is specified (n grows by the number
+    of such rows); the constructed optimum carries over (slack = the row's slack, reduced cost
+    -y_i)."""
     rng = np.random.default_rng(seed)
     lens = np.minimum(_truncated_zipf(rng, zipf_a, cap, m), n)
     rows = np.repeat(np.arange(m, dtype=np.int64), lens)
@@ -206,6 +211,19 @@ def skewed_lp(m: int, n: int, seed: int = 2000, zipf_a: float = 1.3, cap: int = 
     lp.con_up = ax + slack
     lp.y_star = y
     lp.c = lp.rmatvec(y) + s
+    if explicit_slacks:
+        le = ~eq
+        k = int(le.sum())
+        ends = lp.row_off[1:].astype(np.int64)[le]
+        col_idx = np.insert(lp.col_idx, ends, (n + np.arange(k)).astype(np.int32))
+        val = np.insert(lp.val, ends, 1.0)
+        row_off = (lp.row_off.astype(np.int64) +
+                   np.concatenate([[0], np.cumsum(le)])).astype(np.int32)
+        b = lp.con_up
+        lp = LP(m, n + k, row_off, col_idx.astype(np.int32), val,
+                np.concatenate([lp.c, np.zeros(k)]), b.copy(), b.copy(),
+                np.concatenate([lb, np.zeros(k)]), np.concatenate([ub, np.full(k, np.inf)]),
+                np.concatenate([x, slack[le]]), y, np.concatenate([s, -y[le]]), name)
     return lp
 
 

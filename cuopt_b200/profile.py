@@ -38,7 +38,7 @@ CONFIGS = {
     "c0": (2_000, 5_000, 8, 0),
     "c1": (1_000_000, 2_000_000, 8, 1000),
     "c1_small": (750_000, 1_500_000, 8, 1000),
-    "c2": (500_000, 1_500_000, 0, 2000),
+    "c2": (500_000, 1_500_000, 0, 2000),  # + one slack column per '<=' row (n = 1.75M)
     "c2_small": (50_000, 150_000, 0, 2000),
     "c4": (5_000, 10_000, 8, 4000),
 }
@@ -86,7 +86,8 @@ def main() -> None:
         print(json.dumps(run_climbers(a)))
         return
     m, n, k, seed = CONFIGS[a.config]
-    lp = gen.constructed_lp(m, n, k, seed=seed) if k else gen.skewed_lp(m, n, seed=seed)
+    lp = (gen.constructed_lp(m, n, k, seed=seed) if k
+          else gen.skewed_lp(m, n, seed=seed, explicit_slacks=True))
     dev = torch.device("cuda", 0)
     t = lambda x, dt: torch.as_tensor(np.ascontiguousarray(x), device=dev, dtype=dt)
     arrs = [t(lp.c, torch.float64), t(lp.row_off, torch.int32), t(lp.col_idx, torch.int32),
@@ -307,7 +308,8 @@ def run_climbers(a) -> dict:
     from cuopt_b200 import linear_programming as lpm
 
     m, n, k, seed = CONFIGS[a.config]
-    lp = gen.constructed_lp(m, n, k, seed=seed) if k else gen.skewed_lp(m, n, seed=seed)
+    lp = (gen.constructed_lp(m, n, k, seed=seed) if k
+          else gen.skewed_lp(m, n, seed=seed, explicit_slacks=True))
     rng = np.random.default_rng(7)
     var = rng.choice(n, a.count, replace=False).astype(np.int32)
     lo = lp.var_lo[var].copy()

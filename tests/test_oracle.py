@@ -216,3 +216,18 @@ def test_per_constraint_residual_solve():
     assert abs(res["l2_primal"] - max(0.0, np.max(rp - tol * cb))) <= 1e-12
     assert abs(res["l2_dual"] - max(0.0, np.max(rd - tol * lp.c))) <= 1e-12
     assert res["l2_dual"] > tol < tol * np.max(-lp.c)
+
+
+def test_skewed_generator_with_explicit_slacks():
+    """Config 2 as specified: one slack column per '<=' row, every row an equality; the
+    constructed optimum stays exact and the objective is unchanged."""
+    a = gen.skewed_lp(2000, 6000, seed=7, cap=500)
+    b = gen.skewed_lp(2000, 6000, seed=7, cap=500, explicit_slacks=True)
+    k = int(np.sum(~np.isfinite(a.con_lo)))
+    assert b.n == a.n + k and b.nnz == a.nnz + k
+    assert np.array_equal(b.con_lo, b.con_up)
+    e = gen.kkt_relative_error(b, b.x_star, b.y_star)
+    assert e["rel_primal"] <= 1e-12 and e["rel_dual"] <= 1e-12 and e["rel_gap"] <= 1e-12
+    assert b.optimal_objective == a.optimal_objective
+    res, _, _, _ = O.solve(b, tol=1e-4, iteration_limit=20000, time_limit=60)
+    assert res["status"] == 1
