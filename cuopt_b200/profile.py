@@ -88,6 +88,7 @@ def main() -> None:
     m, n, k, seed = CONFIGS[a.config]
     lp = (gen.constructed_lp(m, n, k, seed=seed) if k
           else gen.skewed_lp(m, n, seed=seed, explicit_slacks=True))
+    m, n = lp.m, lp.n  # config 2 adds slack columns
     dev = torch.device("cuda", 0)
     t = lambda x, dt: torch.as_tensor(np.ascontiguousarray(x), device=dev, dtype=dt)
     arrs = [t(lp.c, torch.float64), t(lp.row_off, torch.int32), t(lp.col_idx, torch.int32),
@@ -310,6 +311,7 @@ def run_climbers(a) -> dict:
     m, n, k, seed = CONFIGS[a.config]
     lp = (gen.constructed_lp(m, n, k, seed=seed) if k
           else gen.skewed_lp(m, n, seed=seed, explicit_slacks=True))
+    m, n = lp.m, lp.n
     rng = np.random.default_rng(7)
     var = rng.choice(n, a.count, replace=False).astype(np.int32)
     lo = lp.var_lo[var].copy()
