@@ -13,7 +13,8 @@ Workloads (sizes are parameters so the tests can run them small):
                    uniform rows, N(0,1) values; 30% of x* at 0, the rest U(0.5, 5).
   skewed_lp        config 2: Zipf(1.3) row lengths on [1, 5000], uniform columns, log-uniform
                    magnitudes in [1e-3, 1e3] with random signs, 50% 'E' / 50% 'L' rows
-                   (the slack of an 'L' row is implicit), bounds [0, U(1,100)], 10% free columns.
+                   (a slack column each with explicit_slacks, as config 2 is specified;
+                   otherwise a ranged row), bounds [0, U(1,100)], 10% free columns.
   batch_lps        config 3: many config-0 LPs with m log-uniform in [200, 20000], n = 2.5 m,
                    non-zeros per column uniform in 6..12.
 """
