@@ -262,30 +262,49 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+class Replicas:
+    """Replica plumbing (one process per GPU, every rank solves its own copy of the workload, no
+    data-path collective): a barrier around the timed region and the max over ranks of a time.
+    backend "nccl" with a CUDA device on the GPU box, "gloo" on CPU (tests)."""
+
+    def __init__(self, world: int, rank: int, device=None, backend: str = "nccl",
+                 timeout_s: float = 600.0):
+        import torch
+        import torch.distributed as dist
+        self.world, self.rank, self.device = world, rank, device
+        self._torch, self._dist = torch, dist
+        if world > 1:
+            import datetime
+            kw = {"device_id": device} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s),
+                                    world_size=world, rank=rank, **kw)
+
+    def barrier(self):
+        if self.world > 1:
+            self._dist.barrier()
+
+    def max(self, v: float) -> float:
+        if self.world == 1:
+            return v
+        t = self._torch.tensor([v], device=self.device, dtype=self._torch.float64)
+        self._dist.all_reduce(t, op=self._dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self._dist.destroy_process_group()
+
+
 def run_b200(args):
     import torch
-    import torch.distributed as dist
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=device)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], device=device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    replicas = Replicas(world, rank, device, "nccl")
+    barrier, max_over_ranks = replicas.barrier, replicas.max
 
     from cuopt_b200._lib import lib
     from cuopt_b200 import generators as gen
@@ -453,8 +472,7 @@ def run_b200(args):
         print(json.dumps(line), flush=True)
     L.cuOptDestroySolverSettings(C.byref(s_mixed))
     L.cuOptDestroySolverSettings(C.byref(s_fp64))
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.close()
 
 
 def main():
