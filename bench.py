@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """PDLP benchmark on one B200 (or N replicas under torchrun).
 
-Workload (default, config 1): the seeded 1,000,000 x 2,000,000 LP with 8 non-zeros per column
+Workload (default, c1): the seeded 1,000,000 x 2,000,000 LP with 8 non-zeros per column
 (16M non-zeros), equality rows, bounds [0, 10], optimum known by construction.  One "step" is one
 full solve to 1e-6 relative KKT (all six tolerances 1e-6), mixed precision (FP32 matrix and
 iterates, FP64 termination / restart / step ratio).  The same solve in plain FP64 is timed beside it.
@@ -14,14 +14,14 @@ iterates, FP64 termination / restart / step ratio).  The same solve in plain FP6
             against the measured HBM copy bandwidth.
   cpu_baseline  the oracle (FP64 restatement of the same algorithm) on the host cores: a bounded
             number of PDHG iterations, scaled by the iterations the solve needs.
-  batch_c3  config 3: 512 seeded LPs of uneven sizes (m log-uniform in [200, 20000], n = 2.5 m,
+  batch_c3  512 seeded LPs of uneven sizes (m log-uniform in [200, 20000], n = 2.5 m,
             6-12 non-zeros per column) solved in FP64 to 1e-6 by one cuOptBatchSolve call, against
             a sample of the same LPs solved one by one with cuOptSolve.
   batch_c3_mixed  the same in mixed precision (batch and single solves): Lanczos step sizes, FP32
-            sweeps; an instance whose FP32 iterates stall continues in FP64.  Config 3 as
+            sweeps; an instance whose FP32 iterates stall continues in FP64.  The batch as
             specified (FP32 bulk against plain FP64 solves one by one) is its
             speedup_vs_sequential_fp64.
-  adjoint_c4  config 4: 64 non-degenerate 5000 x 10000 LPs solved in one batched call with
+  adjoint_c4  64 non-degenerate 5000 x 10000 LPs solved in one batched call with
             crossover, L = sum w * x* back-propagated through the KKT adjoint, gradients checked
             against the exact basis derivatives and central differences (h = 1e-6).
 
@@ -52,7 +52,7 @@ CONFIGS = {
     "c0": (2_000, 5_000, 8, 0),
     "c1_small": (750_000, 1_500_000, 8, 1000),
 }
-# FP64 Stable3 iterations to 1e-6 on config 1 (the oracle and the GPU FP64 path follow the same
+# FP64 Stable3 iterations to 1e-6 on the 1M x 2M LP (the oracle and the GPU FP64 path follow the same
 # iterates; measured by the FP64 leg of this benchmark on a B200).  Used only to scale the CPU
 # per-iteration time of the reference arm into the LPs/s unit.
 FP64_ITERATIONS_C1 = 1700
@@ -427,7 +427,7 @@ def run_b200(args):
                          f"({s_iter * 1e3:.1f} ms each), scaled by the {iters} iterations of the FP64 solve",
                "pdhg_iter_per_s": 1.0 / s_iter}
 
-    # Config 3: 512 uneven FP64 LPs in one batched call vs the same LPs one by one (rank 0, N = 1),
+    # 512 uneven FP64 LPs in one batched call vs the same LPs one by one (rank 0, N = 1),
     # then the same in mixed precision.
     batch = batch_mixed = None
     if rank == 0 and world == 1 and not args.no_batch:
@@ -437,11 +437,11 @@ def run_b200(args):
         batch_mixed = run_batch(argparse.Namespace(count=512, sequential=args.batch_sequential,
                                                    repeats=3, tol=1e-6, time_limit=120.0,
                                                    batch_precision="mixed"))
-        # Config 3 as specified: the FP32-bulk batch against plain FP64 solves one by one.
+        # The batch as specified: the FP32-bulk batch against plain FP64 solves one by one.
         if batch.get("sequential_lps_per_s"):
             batch_mixed["speedup_vs_sequential_fp64"] = (batch_mixed["batch_lps_per_s"] /
                                                          batch["sequential_lps_per_s"])
-    # Config 4: 64 non-degenerate 5000 x 10000 LPs, batched forward (crossover) + KKT adjoint.
+    # 64 non-degenerate 5000 x 10000 LPs, batched forward (crossover) + KKT adjoint.
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint:
         from cuopt_b200.profile import run_adjoint
@@ -494,9 +494,9 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adjoint-fd-coords", type=int, default=16,
-                    help="config-4 coordinates per kind checked by central differences")
+                    help="adjoint batch: coordinates per kind checked by central differences")
     ap.add_argument("--batch-sequential", type=int, default=32,
-                    help="config-3 instances also solved one by one (timing sample)")
+                    help="512-LP batch: instances also solved one by one (timing sample)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

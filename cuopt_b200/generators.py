@@ -9,13 +9,13 @@ So c.x* is the optimal objective.  Random numbers come from numpy's PCG64 seeded
 ``config_id * 1000 + instance``.
 
 Workloads (sizes are parameters so the tests can run them small):
-  constructed_lp   config 0 / 1 / 4: equality rows, [0, 10] bounds, k non-zeros per column at
+  constructed_lp   the 2000 x 5000 and 1M x 2M LPs: equality rows, [0, 10] bounds, k non-zeros per column at
                    uniform rows, N(0,1) values; 30% of x* at 0, the rest U(0.5, 5).
-  skewed_lp        config 2: Zipf(1.3) row lengths on [1, 5000], uniform columns, log-uniform
+  skewed_lp        the 500k-row skewed LP: Zipf(1.3) row lengths on [1, 5000], uniform columns, log-uniform
                    magnitudes in [1e-3, 1e3] with random signs, 50% 'E' / 50% 'L' rows
-                   (a slack column each with explicit_slacks, as config 2 is specified;
+                   (a slack column each with explicit_slacks, as that workload is specified;
                    otherwise a ranged row), bounds [0, U(1,100)], 10% free columns.
-  batch_lps        config 3: many config-0 LPs with m log-uniform in [200, 20000], n = 2.5 m,
+  batch_lps        the 512-LP batch: constructed_lp instances with m log-uniform in [200, 20000], n = 2.5 m,
                    non-zeros per column uniform in 6..12.
 """
 from __future__ import annotations
@@ -89,7 +89,7 @@ def _distinct_rows_per_column(rng: np.random.Generator, m: int, n: int, k: int) 
 
 def constructed_lp(m: int, n: int, nnz_per_col: int = 8, seed: int = 0, upper: float = 10.0,
                    name: str = "constructed") -> LP:
-    """Config-0 generator: min c.x s.t. A x = b, 0 <= x <= upper, optimum known."""
+    """min c.x s.t. A x = b, 0 <= x <= upper, with a constructed (degenerate) optimum."""
     rng = np.random.default_rng(seed)
     rows = _distinct_rows_per_column(rng, m, n, nnz_per_col)
     vals = rng.standard_normal((n, nnz_per_col))
@@ -111,7 +111,7 @@ def constructed_lp(m: int, n: int, nnz_per_col: int = 8, seed: int = 0, upper: f
 
 def vertex_lp(m: int, n: int, nnz_per_col: int = 8, seed: int = 0, upper: float = 10.0,
               name: str = "vertex") -> LP:
-    """Config-4 generator: the config-0 recipe with a unique, non-degenerate optimal vertex.
+    """The constructed_lp recipe with a unique, non-degenerate optimal vertex (the adjoint batch).
 
     m basic variables lie strictly inside [0, upper]; basic column basic[i] holds row i with a
     value of magnitude in [1, 2], so the basis matrix is non-singular.  Every other variable sits
@@ -161,10 +161,10 @@ def _truncated_zipf(rng: np.random.Generator, a: float, cap: int, size: int) -> 
 
 def skewed_lp(m: int, n: int, seed: int = 2000, zipf_a: float = 1.3, cap: int = 5000,
               name: str = "skewed", explicit_slacks: bool = False) -> LP:
-    """Config-2 generator (row lengths Zipf(a) on [1, cap], mixed senses, free columns).
+    """Skewed-sparsity LP (row lengths Zipf(a) on [1, cap], mixed senses, free columns).
 
     With explicit_slacks, every '<=' row gets a slack column (coefficient +1, bounds [0, inf),
-    cost 0) and becomes an equality, as the config-2 workload is specified (n grows by the number
+    cost 0) and becomes an equality, as the 500k-row skewed workload is specified (n grows by the number
     of such rows); the constructed optimum carries over (slack = the row's slack, reduced cost
     -y_i)."""
     rng = np.random.default_rng(seed)
@@ -236,7 +236,7 @@ def _batch_shapes(count, seed, m_lo, m_hi):
 
 
 def batch_lps(count: int = 512, seed: int = 3000, m_lo: int = 200, m_hi: int = 20000):
-    """Config-3 generator: `count` config-0 LPs of uneven sizes."""
+    """The batch workload: `count` constructed_lp instances of uneven sizes."""
     ms, ks = _batch_shapes(count, seed, m_lo, m_hi)
     return [constructed_lp(int(m), int(2.5 * m), int(k), seed=seed + 1 + i, name=f"batch{i}")
             for i, (m, k) in enumerate(zip(ms, ks))]

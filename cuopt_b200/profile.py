@@ -88,7 +88,7 @@ def main() -> None:
     m, n, k, seed = CONFIGS[a.config]
     lp = (gen.constructed_lp(m, n, k, seed=seed) if k
           else gen.skewed_lp(m, n, seed=seed, explicit_slacks=True))
-    m, n = lp.m, lp.n  # config 2 adds slack columns
+    m, n = lp.m, lp.n  # the skewed LP adds slack columns
     dev = torch.device("cuda", 0)
     t = lambda x, dt: torch.as_tensor(np.ascontiguousarray(x), device=dev, dtype=dt)
     arrs = [t(lp.c, torch.float64), t(lp.row_off, torch.int32), t(lp.col_idx, torch.int32),
@@ -142,7 +142,7 @@ def main() -> None:
 
 
 def run_batch(a) -> dict:
-    """Config 3: one batched solve of `count` uneven LPs vs the same LPs solved one at a time."""
+    """The 512-LP batch: one batched solve of `count` uneven LPs vs the same LPs one at a time."""
     import numpy as np
 
     from cuopt_b200 import generators as gen
@@ -205,7 +205,7 @@ def run_batch(a) -> dict:
 
 
 def run_adjoint(a) -> dict:
-    """Config 4: batched forward solve + KKT-adjoint backward, checked two ways."""
+    """64 x (5000 x 10000) vertex LPs: batched forward solve + KKT-adjoint backward, checked two ways."""
     import numpy as np
     import scipy.sparse as sp
     import torch

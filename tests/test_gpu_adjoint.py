@@ -138,7 +138,7 @@ def test_finite_differences_through_the_solver(vlp):
 
 
 def test_adjoint_on_a_degenerate_optimum_is_finite():
-    """The config-0 generator has a dual-degenerate optimum (more free variables than rows): the
+    """constructed_lp has a dual-degenerate optimum (more free variables than rows): the
     adjoint falls back to the least-squares response and stays finite."""
     from cuopt_b200.torch_layer import lp_solve
     lp = gen.constructed_lp(200, 500, 8, seed=11)

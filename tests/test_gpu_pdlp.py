@@ -61,7 +61,7 @@ def test_solve_matches_oracle_and_optimum(small_lp):
 
 
 def test_config0_full_size():
-    """Config 0 (2000 x 5000, 8 nnz / column): Optimal at 1e-6, objective within 1e-6 of the
+    """The 2000 x 5000 LP (8 nnz / column): Optimal at 1e-6, objective within 1e-6 of the
     constructed optimum relative to its magnitude, same status and iteration count as the oracle."""
     lp = gen.constructed_lp(2000, 5000, 8, seed=0)
     sol = lpm.Solve(datamodel_from_lp(lp), settings(tol=1e-6))
@@ -311,7 +311,7 @@ def test_per_constraint_residual_in_batches(small_lp):
 
 
 def test_mixed_precision_stall_continues_in_fp64():
-    """Config-3 instance 458: its FP32 iterates stall with the relative gap near 1e-4 (after which
+    """Instance 458 of the 512-LP batch (2539 x 6347): its FP32 iterates stall with the relative gap near 1e-4 (after which
     the primal weight drifts), so a mixed solve continues in FP64 from its own state and ends
     Optimal at 1e-6 with the constructed optimum (refinement_passes = 1), as the FP64 solve does.
     In a mixed batch the stalled instance is solved again in FP64; the others stay mixed."""

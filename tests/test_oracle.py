@@ -63,8 +63,8 @@ def test_constructed_optimum_small(seed):
     assert kkt["rel_primal"] <= 1e-7 and kkt["rel_gap"] <= 1e-7
 
 
-def test_constructed_optimum_config0():
-    """Config 0 (2000 x 5000) to 1e-6: objective within 1e-6 relative of the constructed optimum."""
+def test_constructed_optimum_2000x5000():
+    """The 2000 x 5000 LP to 1e-6: objective within 1e-6 relative of the constructed optimum."""
     lp = gen.constructed_lp(2000, 5000, 8, seed=0)
     res, x, y, _ = O.solve(lp, tol=1e-6)
     assert res["status"] == 1
@@ -219,7 +219,7 @@ def test_per_constraint_residual_solve():
 
 
 def test_skewed_generator_with_explicit_slacks():
-    """Config 2 as specified: one slack column per '<=' row, every row an equality; the
+    """The skewed LP as specified: one slack column per '<=' row, every row an equality; the
     constructed optimum stays exact and the objective is unchanged."""
     a = gen.skewed_lp(2000, 6000, seed=7, cap=500)
     b = gen.skewed_lp(2000, 6000, seed=7, cap=500, explicit_slacks=True)
