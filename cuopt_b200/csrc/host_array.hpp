@@ -6,16 +6,70 @@
 #include <cstddef>
 #include <cstdlib>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <utility>
 #include <vector>
 
 namespace cuopt_b200 {
 
+// Large host blocks (2 MiB aligned, advised as transparent huge pages) with a bounded cache of
+// freed ones: a block of the same rounded size is handed out again with its pages already
+// faulted in, instead of being returned to the system and zeroed again on first touch (a
+// problem, its solution and a batch's arrays are typically allocated at the same sizes solve
+// after solve).  At most kCacheBytes are kept.
+class huge_blocks {
+ public:
+  static constexpr std::size_t kAlign = std::size_t(2) << 20, kCacheBytes = std::size_t(1) << 30;
+  static void* get(std::size_t rounded)
+  {
+    {
+      auto& c = cache();
+      std::lock_guard<std::mutex> lock(c.mu);
+      for (std::size_t i = 0; i < c.blocks.size(); ++i)
+        if (c.blocks[i].second == rounded) {
+          void* p = c.blocks[i].first;
+          c.blocks[i] = c.blocks.back();
+          c.blocks.pop_back();
+          c.bytes -= rounded;
+          return p;
+        }
+    }
+    void* p = std::aligned_alloc(kAlign, rounded);
+    if (!p) throw std::bad_alloc();
+    madvise(p, rounded, MADV_HUGEPAGE);
+    return p;
+  }
+  static void put(void* p, std::size_t rounded)
+  {
+    auto& c = cache();
+    {
+      std::lock_guard<std::mutex> lock(c.mu);
+      if (c.bytes + rounded <= kCacheBytes) {
+        c.blocks.emplace_back(p, rounded);
+        c.bytes += rounded;
+        return;
+      }
+    }
+    std::free(p);
+  }
+
+ private:
+  struct state {
+    std::mutex mu;
+    std::vector<std::pair<void*, std::size_t>> blocks;
+    std::size_t bytes = 0;
+  };
+  static state& cache()
+  {
+    static state* s = new state;  // never destroyed: arrays may be released during exit
+    return *s;
+  }
+};
+
 // std::vector whose resize leaves new elements uninitialised: the problem arrays are always
 // overwritten right after they are sized, and zero-filling 10^8 elements first (single-threaded)
-// would cost as much as the copy itself.  Arrays of 4 MiB or more are 2 MiB aligned and advised
-// as transparent huge pages, which halves the page-fault cost of filling fresh memory.
+// would cost as much as the copy itself.  Arrays of 4 MiB or more come from huge_blocks.
 template <typename T>
 struct default_init_allocator : std::allocator<T> {
   template <typename U>
@@ -28,18 +82,15 @@ struct default_init_allocator : std::allocator<T> {
   {
     const std::size_t bytes = n * sizeof(T);
     if (bytes < kHugeMin) return std::allocator<T>::allocate(n);
-    const std::size_t rounded = (bytes + kHuge - 1) / kHuge * kHuge;
-    void* p                   = std::aligned_alloc(kHuge, rounded);
-    if (!p) throw std::bad_alloc();
-    madvise(p, rounded, MADV_HUGEPAGE);
-    return static_cast<T*>(p);
+    return static_cast<T*>(huge_blocks::get((bytes + kHuge - 1) / kHuge * kHuge));
   }
   void deallocate(T* p, std::size_t n)
   {
-    if (n * sizeof(T) < kHugeMin)
+    const std::size_t bytes = n * sizeof(T);
+    if (bytes < kHugeMin)
       std::allocator<T>::deallocate(p, n);
     else
-      std::free(p);
+      huge_blocks::put(p, (bytes + kHuge - 1) / kHuge * kHuge);
   }
   template <typename U>
   void construct(U* p) noexcept
