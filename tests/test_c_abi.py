@@ -228,3 +228,26 @@ def test_product_path_fails_loudly_without_library(tmp_path, monkeypatch):
     monkeypatch.setattr(L, "LIB_PATH", tmp_path / "missing.so")
     with pytest.raises(ImportError):
         L.lib()
+
+
+def _build_c_caller(tmp_path):
+    """Compiles tests/c_api/solve_lp.c, a plain C caller of cuopt_c.h, against this library."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    root = Path(__file__).resolve().parents[1]
+    exe = tmp_path / "solve_lp"
+    cmd = [cc, "-std=c11", "-Wall", "-Werror", "-I", str(root / "include"),
+           str(root / "tests" / "c_api" / "solve_lp.c"), "-o", str(exe),
+           "-L", str(LIB_PATH.parent), "-lcuopt_b200", f"-Wl,-rpath,{LIB_PATH.parent}", "-lm"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
+    return exe
+
+
+def test_c_caller_compiles_and_links(tmp_path):
+    """A C program written against cuopt_c.h builds and links against libcuopt_b200.so as it
+    would against the reference's libcuopt."""
+    assert _build_c_caller(tmp_path).exists()

@@ -376,3 +376,20 @@ def test_problem_from_pinned_or_device_arrays_solves_identically(small_lp):
             assert np.array_equal(got[1], ref[1]) and np.array_equal(got[2], ref[2])
     finally:
         L.cuOptDestroySolverSettings(C.byref(s))
+
+
+def test_c_caller_solves(golden, golden_dir, tmp_path):
+    """The plain C caller (tests/c_api/solve_lp.c) solves afiro from its MPS file and a ranged
+    maximisation built from arrays: both Optimal, afiro at its golden objective, the ranged LP at
+    its optimum 11."""
+    import subprocess
+    from tests.test_c_abi import _build_c_caller
+    exe = _build_c_caller(tmp_path)
+    res = subprocess.run([str(exe), str(golden_dir / "afiro_original.mps")], capture_output=True,
+                         text=True, timeout=120)
+    assert res.returncode == 0, res.stderr
+    lines = {l.split()[0]: l.split()[1:] for l in res.stdout.splitlines()}
+    assert int(lines["mps"][0]) == 1 and int(lines["ranged"][0]) == 1
+    g = golden["afiro_objective"]
+    assert rel(float(lines["mps"][1]), g["value"]) <= g["rel_tol"]
+    assert abs(float(lines["ranged"][1]) - 11.0) <= 1e-5
