@@ -393,3 +393,24 @@ def test_c_caller_solves(golden, golden_dir, tmp_path):
     g = golden["afiro_objective"]
     assert rel(float(lines["mps"][1]), g["value"]) <= g["rel_tol"]
     assert abs(float(lines["ranged"][1]) - 11.0) <= 1e-5
+
+
+def test_concurrent_solves_on_host_threads_match_sequential():
+    """Solves of different problems may run on different host threads at once (the reference's
+    threading contract: each problem on its own stream, cuopt_c_internal.hpp:20-29); each result is
+    bitwise the sequential one."""
+    from concurrent.futures import ThreadPoolExecutor
+    lps = [gen.constructed_lp(300 + 100 * i, 800 + 200 * i, 8, seed=90 + i) for i in range(4)]
+    s = settings(tol=1e-6)
+
+    def run(lp):
+        sol = lpm.Solve(datamodel_from_lp(lp), s)
+        return (int(sol.get_termination_status()), sol.get_lp_stats()["nb_iterations"],
+                sol.get_primal_solution(), sol.get_dual_solution())
+
+    seq = [run(lp) for lp in lps]
+    with ThreadPoolExecutor(max_workers=4) as ex:
+        par = list(ex.map(run, lps))
+    for a, b in zip(seq, par):
+        assert a[0] == b[0] == 1 and a[1] == b[1]
+        assert np.array_equal(a[2], b[2]) and np.array_equal(a[3], b[3])
