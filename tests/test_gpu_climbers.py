@@ -62,7 +62,13 @@ def test_climber_iterates_match_single_oracle(base_lp, k):
 
 
 def test_climbers_solve_to_tolerance_like_single_solves(base_lp):
-    var, lo, up = _climbers(base_lp, 6, seed=4)
+    """12 climbers in two groups of eight whose upper bounds cut into the optimum: the second
+    group is done at 610 iterations while two climbers of the first need 620 and 640, so the
+    sweeps drop a group mid-solve.  Each climber stops where the oracle's solve of its LP stops."""
+    rng = np.random.default_rng(5)
+    var = rng.choice(np.where(base_lp.x_star > 2.0)[0], 12, replace=False)
+    lo = base_lp.var_lo[var].copy()
+    up = base_lp.x_star[var] * rng.uniform(0.05, 0.6, 12)
     sols, _ = lpm.SolveClimbers(datamodel_from_lp(base_lp), var, lo, up, settings(tol=1e-6))
     for b, sol in enumerate(sols):
         res, _, _, _ = O.solve(_modified(base_lp, var[b], lo[b], up[b]), tol=1e-6)
