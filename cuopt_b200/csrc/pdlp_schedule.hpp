@@ -108,7 +108,10 @@ inline std::shared_ptr<const std::vector<double>> power_start_sequence(size_t co
 
 // Stopping rule of the Golub-Kahan-Lanczos step size: steps run in chunks of kLanczosChunk; after
 // each chunk sigma_max^2 of the bidiagonal so far is compared with the previous chunk's value.
+// The estimate approaches sigma_max from below, so the step 0.998 / sigma keeps a margin of 2e-3
+// over the stability limit; a relative change of 1e-8 leaves it untouched (on the 1M x 2M LP the
+// step agrees with that of 1e-10 to ten digits, in 64 steps instead of 80).
 constexpr int kLanczosChunk = 16, kLanczosMaxSteps = 512;
-constexpr double kLanczosTol = 1e-10;
+constexpr double kLanczosTol = 1e-8;
 
 }  // namespace cuopt_b200
