@@ -291,13 +291,36 @@ bool lp_settings::b(const char* name) const
 
 // ------------------------------------------------------------------------------------------
 
+// True when bad(i) holds for some i in [0, count), tested on up to 8 host threads for large counts.
+template <class Pred>
+static bool any_of_index(int64_t count, Pred bad)
+{
+  constexpr int64_t kPerThread = int64_t(1) << 18;
+  const int nt = (int)std::min<int64_t>(std::max(1u, std::min(8u, std::thread::hardware_concurrency())),
+                                        std::max<int64_t>(1, count / kPerThread));
+  if (nt <= 1) {
+    for (int64_t i = 0; i < count; ++i)
+      if (bad(i)) return true;
+    return false;
+  }
+  std::atomic<bool> found{false};
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t)
+    pool.emplace_back([&, t] {
+      for (int64_t i = count * t / nt, e = count * (t + 1) / nt; i < e && !found.load(); ++i)
+        if (bad(i)) found = true;
+    });
+  for (auto& th : pool) th.join();
+  return found.load();
+}
+
 std::string validate_problem(const lp_problem& p)
 {
   if (p.m < 0 || p.n < 0) return "Negative problem dimensions.";
   if ((int)p.row_off.size() != p.m + 1) return "A_offsets must have num_constraints + 1 entries.";
   if (p.row_off[0] != 0) return "A_offsets first value should be 0.";
-  for (int i = 0; i < p.m; ++i)
-    if (p.row_off[i + 1] < p.row_off[i]) return "A_offsets values must in an increasing order.";
+  if (any_of_index(p.m, [&](int64_t i) { return p.row_off[i + 1] < p.row_off[i]; }))
+    return "A_offsets values must in an increasing order.";
   const int64_t nnz = p.row_off[p.m];
   if ((int64_t)p.col_idx.size() != nnz || (int64_t)p.val.size() != nnz)
     return "A_index and A_values must have same sizes.";
@@ -420,17 +443,11 @@ static bool prepare_for_pdlp(const lp_problem& p, const lp_settings& st, row_bou
   const double* lo = rb.lo;
   const double* up = rb.up;
   // has_crossing_bounds (reference problem_checking.cu:316-339)
-  for (int j = 0; j < p.n; ++j)
-    if (!(p.var_up[j] >= p.var_lo[j])) {
-      out.r.status = CUOPT_TERIMINATION_STATUS_INFEASIBLE;
-      return false;
-    }
-  if (p.ranged)
-    for (int i = 0; i < p.m; ++i)
-      if (!(up[i] >= lo[i])) {
-        out.r.status = CUOPT_TERIMINATION_STATUS_INFEASIBLE;
-        return false;
-      }
+  if (any_of_index(p.n, [&](int64_t j) { return !(p.var_up[j] >= p.var_lo[j]); }) ||
+      (p.ranged && any_of_index(p.m, [&](int64_t i) { return !(up[i] >= lo[i]); }))) {
+    out.r.status = CUOPT_TERIMINATION_STATUS_INFEASIBLE;
+    return false;
+  }
   const int method = st.i(CUOPT_METHOD);
   if (p.m == 0) {
     if (method == CUOPT_METHOD_PDLP) {
