@@ -601,7 +601,11 @@ cuopt_int_t cuOptGetErrorString(cuOptSolution solution, char* buf, cuopt_int_t s
 cuopt_int_t cuOptGetPrimalSolution(cuOptSolution solution, cuopt_float_t* v)
 {
   CHECK2(solution, v);
-  copy_out(v, R(solution)->r.x);
+  const auto& r = R(solution)->r;
+  if (r.dev)
+    cuopt_b200::copy_solution_vector(r, 0, v);
+  else
+    copy_out(v, r.x);
   return CUOPT_SUCCESS;
 }
 cuopt_int_t cuOptGetObjectiveValue(cuOptSolution solution, cuopt_float_t* v)
@@ -629,7 +633,11 @@ cuopt_int_t cuOptGetSolutionBound(cuOptSolution solution, cuopt_float_t* v)
 cuopt_int_t cuOptGetDualSolution(cuOptSolution solution, cuopt_float_t* v)
 {
   CHECK2(solution, v);
-  copy_out(v, R(solution)->r.y);
+  const auto& r = R(solution)->r;
+  if (r.dev)
+    cuopt_b200::copy_solution_vector(r, 1, v);
+  else
+    copy_out(v, r.y);
   return CUOPT_SUCCESS;
 }
 cuopt_int_t cuOptGetDualObjectiveValue(cuOptSolution solution, cuopt_float_t* v)
@@ -641,7 +649,11 @@ cuopt_int_t cuOptGetDualObjectiveValue(cuOptSolution solution, cuopt_float_t* v)
 cuopt_int_t cuOptGetReducedCosts(cuOptSolution solution, cuopt_float_t* v)
 {
   CHECK2(solution, v);
-  copy_out(v, R(solution)->r.rc);
+  const auto& r = R(solution)->r;
+  if (r.dev)
+    cuopt_b200::copy_solution_vector(r, 2, v);
+  else
+    copy_out(v, r.rc);
   return CUOPT_SUCCESS;
 }
 
@@ -866,10 +878,15 @@ cuopt_int_t cuOptSolutionAdjoint(cuOptOptimizationProblem problem, cuOptSolution
                                  cuopt_float_t* dl_dupper, cuopt_float_t* dl_dvalues)
 {
   if (!problem || !solution || !dl_dx) return CUOPT_INVALID_ARGUMENT;
-  const lp_solution* sol = R(solution);
+  lp_solution* sol = R(solution);
   if (sol->error_code != CUOPT_SUCCESS || sol->r.status != CUOPT_TERIMINATION_STATUS_OPTIMAL)
     return CUOPT_INVALID_ARGUMENT;
   const lp_problem& p = *P(problem);
+  try {
+    cuopt_b200::ensure_host(sol->r);
+  } catch (const std::exception&) {
+    return CUOPT_RUNTIME_ERROR;
+  }
   if ((int)sol->r.x.size() != p.n || (int)sol->r.y.size() != p.m) return CUOPT_INVALID_ARGUMENT;
   try {
     std::vector<double> gx, gy;

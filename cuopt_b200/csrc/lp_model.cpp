@@ -513,8 +513,10 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
     trace("constraint bounds + checks");
     out.r         = pdlp_solve(in, prm);
     trace("pdlp_solve");
-    if (st.b(CUOPT_CROSSOVER) && out.r.status == CUOPT_TERIMINATION_STATUS_OPTIMAL)
+    if (st.b(CUOPT_CROSSOVER) && out.r.status == CUOPT_TERIMINATION_STATUS_OPTIMAL) {
+      ensure_host(out.r);
       out.r.crossover = vertex_polish(p, out.r);
+    }
     if (prm.log_to_console)
       std::printf("PDLP status %d  objective %+.10e  iterations %lld  time %.3fs\n", out.r.status,
                   out.r.primal_obj, (long long)out.r.iterations, out.r.solve_time);
@@ -915,7 +917,8 @@ std::vector<lp_solution> solve_strong_branching(const lp_problem& p, const lp_se
   sb.set_int(CUOPT_ITERATION_LIMIT, 100000);
   lp_settings base_settings = sb;
   base_settings.set_bool(CUOPT_CROSSOVER, false);
-  const lp_solution base = solve_problem(p, base_settings);
+  lp_solution base = solve_problem(p, base_settings);
+  ensure_host(base.r);
   climber_start start;
   if (base.error_code == CUOPT_SUCCESS && base.solved_by_pdlp && (int)base.r.x.size() == p.n &&
       (int)base.r.y.size() == p.m) {

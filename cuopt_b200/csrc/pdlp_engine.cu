@@ -1050,13 +1050,86 @@ sweep_profile pdlp_profile_sweeps(const lp_device_input& in, const pdlp_params& 
   return e.profile(iterations);
 }
 
+device_solution::~device_solution()
+{
+  if (!base) return;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != device) cudaSetDevice(device);
+  cudaStream_t s;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess) {
+    cudaFreeAsync(base, s);
+    cudaStreamDestroy(s);
+  }
+  if (cur >= 0 && cur != device) cudaSetDevice(cur);
+  cudaGetLastError();
+}
+
+namespace {
+// Makes d's device current for the lifetime of the object.
+struct on_device {
+  int prev = -1, dev;
+  explicit on_device(int d) : dev(d)
+  {
+    cudaGetDevice(&prev);
+    if (prev != dev) B200_CUDA_CHECK(cudaSetDevice(dev));
+  }
+  ~on_device()
+  {
+    if (prev >= 0 && prev != dev) cudaSetDevice(prev);
+  }
+};
+}  // namespace
+
+void ensure_host(pdlp_result& r)
+{
+  if (!r.dev) return;
+  const device_solution& d = *r.dev;
+  on_device scope(d.device);
+  cudaStream_t s;
+  B200_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  r.x.resize(d.n);
+  r.y.resize(d.m);
+  r.rc.resize(d.n);
+  staged_download(r.x.data(), d.x, (size_t)d.n * sizeof(double), s);
+  staged_download(r.y.data(), d.y, (size_t)d.m * sizeof(double), s);
+  staged_download(r.rc.data(), d.rc, (size_t)d.n * sizeof(double), s);
+  cudaStreamDestroy(s);
+  r.dev.reset();
+}
+
+void copy_solution_vector(const pdlp_result& r, int which, double* dst)
+{
+  const device_solution& d = *r.dev;
+  const double* src  = which == 0 ? d.x : which == 1 ? d.y : d.rc;
+  const size_t bytes = (size_t)(which == 1 ? d.m : d.n) * sizeof(double);
+  if (bytes == 0) return;
+  on_device scope(d.device);
+  cudaPointerAttributes attr{};
+  const bool dma = cudaPointerGetAttributes(&attr, dst) == cudaSuccess &&
+                   attr.type != cudaMemoryTypeUnregistered;
+  cudaGetLastError();
+  if (dma) {  // pinned host or device memory: one copy
+    B200_CUDA_CHECK(cudaMemcpy(dst, src, bytes, cudaMemcpyDefault));
+    return;
+  }
+  cudaStream_t s;
+  B200_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  staged_download(dst, src, bytes, s);
+  cudaStreamDestroy(s);
+}
+
 pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p)
 {
   cudaStream_t s;
   B200_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  struct stream_guard {
+  struct stream_guard {  // the stream's work ends before its buffers are released
     cudaStream_t s;
-    ~stream_guard() { cudaStreamDestroy(s); }
+    ~stream_guard()
+    {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
   } guard{s};
   alloc_scope scope(s);
   configure_pool_once();
@@ -1069,7 +1142,16 @@ pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p)
     if (cudaGetDevice(&cur) != cudaSuccess || cur != dv->device) dv = nullptr;
   }
   dbuf<int> off, idx;
-  dbuf<double> val, c, lo, up, vl, vu, x(n), y(m), rc(n), ip, id;
+  dbuf<double> val, c, lo, up, vl, vu, ip, id;
+  // The solution stays on the device (one allocation for x, reduced costs and y).
+  auto sol = std::make_shared<device_solution>();
+  B200_CUDA_CHECK(cudaGetDevice(&sol->device));
+  sol->n = n;
+  sol->m = m;
+  B200_CUDA_CHECK(cudaMallocAsync(&sol->base, (2 * (size_t)n + m) * sizeof(double), s));
+  sol->x  = static_cast<double*>(sol->base);
+  sol->rc = sol->x + n;
+  sol->y  = sol->rc + n;
   lp_device_input d;
   {
     staged_upload h2d(s);
@@ -1104,16 +1186,10 @@ pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p)
     d.initial_dual = id.data();
   }
   trace("host path: upload");
-  pdlp_result r = pdlp_solve_device(d, p, s, x.data(), y.data(), rc.data());
+  pdlp_result r = pdlp_solve_device(d, p, s, sol->x, sol->y, sol->rc);
+  B200_CUDA_CHECK(cudaStreamSynchronize(s));
   trace("host path: device solve");
-  if (r.status != kNumericalError || r.iterations > 0) {
-    r.x.resize(n);
-    r.y.resize(m);
-    r.rc.resize(n);
-    staged_download(r.x.data(), x.data(), n * sizeof(double), s);
-    staged_download(r.y.data(), y.data(), m * sizeof(double), s);
-    staged_download(r.rc.data(), rc.data(), n * sizeof(double), s);
-  }
+  if (r.status != kNumericalError || r.iterations > 0) r.dev = std::move(sol);
   return r;
 }
 

@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <string>
 #include <limits>
+#include <memory>
 #include <vector>
 
 #include "host_array.hpp"
@@ -76,9 +77,26 @@ struct pdlp_params {
   double initial_primal_weight = std::numeric_limits<double>::quiet_NaN();
 };
 
+// A solution's x, y and reduced costs left on the device by a host-path solve (user order, the
+// signs the user sees), as the reference keeps its solutions: getters copy from it straight to the
+// caller's buffer, and host code that needs the vectors downloads them first (ensure_host).
+struct device_solution {
+  int device    = -1;
+  void* base    = nullptr;
+  double* x     = nullptr;
+  double* y     = nullptr;
+  double* rc    = nullptr;
+  int n = 0, m = 0;
+  device_solution() = default;
+  device_solution(const device_solution&)            = delete;
+  device_solution& operator=(const device_solution&) = delete;
+  ~device_solution();
+};
+
 struct pdlp_result {
   int status = 0;  // CUOPT_TERIMINATION_STATUS_*
-  host_array<double> x, y, rc;  // user order
+  host_array<double> x, y, rc;  // user order (empty while they are only on the device, `dev`)
+  std::shared_ptr<const device_solution> dev;
   int64_t iterations = 0;
   double primal_obj = 0, dual_obj = 0;
   double l2_primal = 0, l2_dual = 0, rel_primal = 0, rel_dual = 0, gap = 0, rel_gap = 0;
@@ -172,5 +190,12 @@ std::vector<pdlp_result> pdlp_climber_solve_device(const lp_device_input& in, co
 
 sweep_profile pdlp_profile_sweeps(const lp_device_input& in, const pdlp_params& p,
                                   cudaStream_t stream, int iterations);
+
+// Fills r.x / r.y / r.rc from r.dev when the vectors are only on the device (then drops it).
+void ensure_host(pdlp_result& r);
+
+// Copies r's x (which 0), y (1) or reduced costs (2) to dst (host or device memory of any kind),
+// from the device when the vectors are there.
+void copy_solution_vector(const pdlp_result& r, int which, double* dst);
 
 }  // namespace cuopt_b200
