@@ -65,6 +65,19 @@ void copy_out(T* dst, const std::vector<T, A>& src)
   cuopt_b200::parallel_memcpy(dst, src.data(), src.size() * sizeof(T));
 }
 
+// Runs the body of a C entry point; no exception crosses the C ABI (they become return codes).
+template <class F>
+cuopt_int_t guarded(F&& body) noexcept
+{
+  try {
+    return body();
+  } catch (const std::bad_alloc&) {
+    return CUOPT_OUT_OF_MEMORY;
+  } catch (...) {
+    return CUOPT_RUNTIME_ERROR;
+  }
+}
+
 lp_problem* P(cuOptOptimizationProblem p) { return static_cast<lp_problem*>(p); }
 lp_settings* S(cuOptSolverSettings s) { return static_cast<lp_settings*>(s); }
 lp_solution* R(cuOptSolution s) { return static_cast<lp_solution*>(s); }
@@ -235,7 +248,7 @@ cuopt_int_t cuOptReadProblem(const char* filename, cuOptOptimizationProblem* pro
   auto* p = new (std::nothrow) lp_problem();
   if (!p) return CUOPT_OUT_OF_MEMORY;
   std::string err;
-  int rc = cuopt_b200::read_mps(filename, *p, err);
+  const cuopt_int_t rc = guarded([&] { return (cuopt_int_t)cuopt_b200::read_mps(filename, *p, err); });
   if (rc != CUOPT_SUCCESS) {
     delete p;
     *problem_ptr = nullptr;
@@ -250,7 +263,7 @@ cuopt_int_t cuOptWriteProblem(cuOptOptimizationProblem problem, const char* file
 {
   if (!problem || !filename || std::strlen(filename) == 0) return CUOPT_INVALID_ARGUMENT;
   if (format != CUOPT_FILE_FORMAT_MPS) return CUOPT_INVALID_ARGUMENT;
-  return cuopt_b200::write_mps(*P(problem), filename);
+  return guarded([&] { return (cuopt_int_t)cuopt_b200::write_mps(*P(problem), filename); });
 }
 
 cuopt_int_t cuOptCreateProblem(cuopt_int_t num_constraints, cuopt_int_t num_variables,
@@ -567,7 +580,14 @@ cuopt_int_t cuOptSolve(cuOptOptimizationProblem problem, cuOptSolverSettings set
   auto* sol = new (std::nothrow) lp_solution();
   if (!sol) return CUOPT_OUT_OF_MEMORY;
   cuopt_b200::trace("cuOptSolve: enter");
-  *sol          = cuopt_b200::solve_problem(*P(problem), *S(settings));
+  const cuopt_int_t rc = guarded([&] {
+    *sol = cuopt_b200::solve_problem(*P(problem), *S(settings));
+    return CUOPT_SUCCESS;
+  });
+  if (rc != CUOPT_SUCCESS) {
+    delete sol;
+    return rc;
+  }
   cuopt_b200::trace("cuOptSolve: solve_problem");
   *solution_ptr = sol;
   return sol->error_code;
@@ -601,12 +621,14 @@ cuopt_int_t cuOptGetErrorString(cuOptSolution solution, char* buf, cuopt_int_t s
 cuopt_int_t cuOptGetPrimalSolution(cuOptSolution solution, cuopt_float_t* v)
 {
   CHECK2(solution, v);
-  const auto& r = R(solution)->r;
-  if (r.dev)
-    cuopt_b200::copy_solution_vector(r, 0, v);
-  else
-    copy_out(v, r.x);
-  return CUOPT_SUCCESS;
+  return guarded([&] {
+    const auto& r = R(solution)->r;
+    if (r.dev)
+      cuopt_b200::copy_solution_vector(r, 0, v);
+    else
+      copy_out(v, r.x);
+    return CUOPT_SUCCESS;
+  });
 }
 cuopt_int_t cuOptGetObjectiveValue(cuOptSolution solution, cuopt_float_t* v)
 {
@@ -633,12 +655,14 @@ cuopt_int_t cuOptGetSolutionBound(cuOptSolution solution, cuopt_float_t* v)
 cuopt_int_t cuOptGetDualSolution(cuOptSolution solution, cuopt_float_t* v)
 {
   CHECK2(solution, v);
-  const auto& r = R(solution)->r;
-  if (r.dev)
-    cuopt_b200::copy_solution_vector(r, 1, v);
-  else
-    copy_out(v, r.y);
-  return CUOPT_SUCCESS;
+  return guarded([&] {
+    const auto& r = R(solution)->r;
+    if (r.dev)
+      cuopt_b200::copy_solution_vector(r, 1, v);
+    else
+      copy_out(v, r.y);
+    return CUOPT_SUCCESS;
+  });
 }
 cuopt_int_t cuOptGetDualObjectiveValue(cuOptSolution solution, cuopt_float_t* v)
 {
@@ -649,12 +673,14 @@ cuopt_int_t cuOptGetDualObjectiveValue(cuOptSolution solution, cuopt_float_t* v)
 cuopt_int_t cuOptGetReducedCosts(cuOptSolution solution, cuopt_float_t* v)
 {
   CHECK2(solution, v);
-  const auto& r = R(solution)->r;
-  if (r.dev)
-    cuopt_b200::copy_solution_vector(r, 2, v);
-  else
-    copy_out(v, r.rc);
-  return CUOPT_SUCCESS;
+  return guarded([&] {
+    const auto& r = R(solution)->r;
+    if (r.dev)
+      cuopt_b200::copy_solution_vector(r, 2, v);
+    else
+      copy_out(v, r.rc);
+    return CUOPT_SUCCESS;
+  });
 }
 
 cuopt_int_t cuOptGetPDLPStatistics(cuOptSolution solution, cuOptPDLPStatistics* st)

@@ -26,13 +26,17 @@ inline void parallel_memcpy(void* dst, const void* src, size_t bytes)
     std::memcpy(dst, src, bytes);
     return;
   }
-  std::vector<std::thread> pool;
-  for (unsigned t = 0; t < parts; ++t) {
+  auto part = [=](unsigned t) {
     const size_t lo = bytes * t / parts, hi = bytes * (t + 1) / parts;
-    pool.emplace_back([=] {
-      std::memcpy(static_cast<char*>(dst) + lo, static_cast<const char*>(src) + lo, hi - lo);
-    });
+    std::memcpy(static_cast<char*>(dst) + lo, static_cast<const char*>(src) + lo, hi - lo);
+  };
+  std::vector<std::thread> pool;
+  unsigned started = 0;
+  try {
+    for (; started < parts; ++started) pool.emplace_back(part, started);
+  } catch (...) {  // no thread to spare: the rest is copied here
   }
+  for (unsigned t = started; t < parts; ++t) part(t);
   for (auto& th : pool) th.join();
 }
 
@@ -61,8 +65,13 @@ inline void parallel_gather(char* dst, const host_piece* pieces, size_t count, s
     return;
   }
   std::vector<std::thread> pool;
-  for (unsigned t = 0; t < parts; ++t)
-    pool.emplace_back(copy_range, total * t / parts, total * (t + 1) / parts);
+  unsigned started = 0;
+  try {
+    for (; started < parts; ++started)
+      pool.emplace_back(copy_range, total * started / parts, total * (started + 1) / parts);
+  } catch (...) {  // no thread to spare: the rest is copied here
+  }
+  for (unsigned t = started; t < parts; ++t) copy_range(total * t / parts, total * (t + 1) / parts);
   for (auto& th : pool) th.join();
 }
 

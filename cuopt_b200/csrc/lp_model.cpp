@@ -304,12 +304,17 @@ static bool any_of_index(int64_t count, Pred bad)
     return false;
   }
   std::atomic<bool> found{false};
+  auto part = [&](int t) {
+    for (int64_t i = count * t / nt, e = count * (t + 1) / nt; i < e && !found.load(); ++i)
+      if (bad(i)) found = true;
+  };
   std::vector<std::thread> pool;
-  for (int t = 0; t < nt; ++t)
-    pool.emplace_back([&, t] {
-      for (int64_t i = count * t / nt, e = count * (t + 1) / nt; i < e && !found.load(); ++i)
-        if (bad(i)) found = true;
-    });
+  int started = 0;
+  try {
+    for (; started < nt; ++started) pool.emplace_back(part, started);
+  } catch (...) {  // no thread to spare: the rest is tested here
+  }
+  for (int t = started; t < nt; ++t) part(t);
   for (auto& th : pool) th.join();
   return found.load();
 }
