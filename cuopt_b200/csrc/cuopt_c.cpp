@@ -813,6 +813,8 @@ cuopt_int_t cuOptBatchSolve(const cuOptOptimizationProblem* problems, cuopt_int_
     rs = cuopt_b200::solve_batch(ps, *S(settings));
   } catch (const std::bad_alloc&) {
     return CUOPT_OUT_OF_MEMORY;
+  } catch (...) {
+    return CUOPT_RUNTIME_ERROR;
   }
   cuopt_int_t first_error = CUOPT_SUCCESS;
   for (cuopt_int_t i = 0; i < count; ++i) {
