@@ -251,3 +251,39 @@ def test_c_caller_compiles_and_links(tmp_path):
     """A C program written against cuopt_c.h builds and links against libcuopt_b200.so as it
     would against the reference's libcuopt."""
     assert _build_c_caller(tmp_path).exists()
+
+
+def test_large_problem_checks_without_gpu():
+    """The pre-solve checks split large arrays over host threads: a decreasing row offset near the
+    end of 600 000 rows is a validation error, and a crossing bound near the end of 600 000
+    variables (or of the ranged rows) ends Infeasible, all before any device work."""
+    L = lib()
+    s = _settings()
+    p = lambda a: C.c_void_p(a.ctypes.data)
+    m = n = 600_000
+
+    def solve(off, vlo, vup, clo, cup):
+        idx, val = np.arange(n, dtype=np.int32), np.ones(n)
+        h, sol = C.c_void_p(), C.c_void_p()
+        assert L.cuOptCreateRangedProblem(m, n, 1, 0.0, p(np.ones(n)), p(off), p(idx), p(val),
+                                          p(clo), p(cup), p(vlo), p(vup), b"C" * n,
+                                          C.byref(h)) == 0
+        rc = L.cuOptSolve(h, s, C.byref(sol))
+        st = C.c_int32()
+        L.cuOptGetTerminationStatus(sol, C.byref(st))
+        L.cuOptDestroySolution(C.byref(sol))
+        L.cuOptDestroyProblem(C.byref(h))
+        return rc, st.value
+
+    off = np.arange(m + 1, dtype=np.int32)
+    vlo, vup, clo, cup = np.zeros(n), np.ones(n), np.zeros(m), np.ones(m)
+    bad_off = off.copy()
+    bad_off[m - 3] = bad_off[m - 2] + 1  # offsets decrease at row m - 3
+    assert solve(bad_off, vlo, vup, clo, cup)[0] == 4  # CUOPT_VALIDATION_ERROR
+    bad_vup = vup.copy()
+    bad_vup[n - 5] = -1.0
+    assert solve(off, vlo, bad_vup, clo, cup) == (0, 2)  # Infeasible
+    bad_cup = cup.copy()
+    bad_cup[m - 7] = -1.0
+    assert solve(off, vlo, vup, clo, bad_cup) == (0, 2)
+    L.cuOptDestroySolverSettings(C.byref(s))
