@@ -231,3 +231,20 @@ def test_skewed_generator_with_explicit_slacks():
     assert b.optimal_objective == a.optimal_objective
     res, _, _, _ = O.solve(b, tol=1e-4, iteration_limit=20000, time_limit=60)
     assert res["status"] == 1
+
+
+def test_tiny_lp_of_the_reference_python_tests():
+    """test_lp_solver.py:46-80: x <= 1 twice, min x over x >= 0.  Optimal with x = 0, zero
+    residuals, objectives and gap (the reference runs it in Stable2 because its Stable3 loops on
+    it; the Stable3 restatement ends Optimal at the first check after iteration 1)."""
+    from types import SimpleNamespace
+    inf = np.inf
+    lp = SimpleNamespace(row_off=np.array([0, 1, 2]), col_idx=np.array([0, 0]),
+                         val=np.array([1.0, 1.0]), c=np.array([1.0]),
+                         con_lo=np.array([-inf, -inf]), con_up=np.array([1.0, 1.0]),
+                         var_lo=np.array([0.0]), var_up=np.array([inf]), obj_offset=0.0,
+                         maximize=False)
+    res, x, y, _ = O.solve(lp, tol=1e-2, iteration_limit=10000, time_limit=10)
+    assert res["status"] == 1
+    assert x[0] == 0.0 and res["primal_obj"] == 0.0 and res["dual_obj"] == 0.0
+    assert res["l2_primal"] == 0.0 and res["l2_dual"] == 0.0 and res["gap"] == 0.0
