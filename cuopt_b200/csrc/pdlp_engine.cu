@@ -1121,6 +1121,9 @@ void copy_solution_vector(const pdlp_result& r, int which, double* dst)
 
 pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p)
 {
+  // Declared before the stream guard, so that on an early exit the stream's work has ended (the
+  // guard synchronises) before the solution's memory is released.
+  auto sol = std::make_shared<device_solution>();
   cudaStream_t s;
   B200_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   struct stream_guard {  // the stream's work ends before its buffers are released
@@ -1144,7 +1147,6 @@ pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p)
   dbuf<int> off, idx;
   dbuf<double> val, c, lo, up, vl, vu, ip, id;
   // The solution stays on the device (one allocation for x, reduced costs and y).
-  auto sol = std::make_shared<device_solution>();
   B200_CUDA_CHECK(cudaGetDevice(&sol->device));
   sol->n = n;
   sol->m = m;
