@@ -1079,6 +1079,16 @@ struct on_device {
     if (prev >= 0 && prev != dev) cudaSetDevice(prev);
   }
 };
+// A non-blocking stream for the lifetime of the object (synchronised before it is destroyed).
+struct temp_stream {
+  cudaStream_t s = nullptr;
+  temp_stream() { B200_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+  ~temp_stream()
+  {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+};
 }  // namespace
 
 void ensure_host(pdlp_result& r)
@@ -1086,15 +1096,13 @@ void ensure_host(pdlp_result& r)
   if (!r.dev) return;
   const device_solution& d = *r.dev;
   on_device scope(d.device);
-  cudaStream_t s;
-  B200_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  temp_stream ts;
   r.x.resize(d.n);
   r.y.resize(d.m);
   r.rc.resize(d.n);
-  staged_download(r.x.data(), d.x, (size_t)d.n * sizeof(double), s);
-  staged_download(r.y.data(), d.y, (size_t)d.m * sizeof(double), s);
-  staged_download(r.rc.data(), d.rc, (size_t)d.n * sizeof(double), s);
-  cudaStreamDestroy(s);
+  staged_download(r.x.data(), d.x, (size_t)d.n * sizeof(double), ts.s);
+  staged_download(r.y.data(), d.y, (size_t)d.m * sizeof(double), ts.s);
+  staged_download(r.rc.data(), d.rc, (size_t)d.n * sizeof(double), ts.s);
   r.dev.reset();
 }
 
@@ -1113,10 +1121,8 @@ void copy_solution_vector(const pdlp_result& r, int which, double* dst)
     B200_CUDA_CHECK(cudaMemcpy(dst, src, bytes, cudaMemcpyDefault));
     return;
   }
-  cudaStream_t s;
-  B200_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  staged_download(dst, src, bytes, s);
-  cudaStreamDestroy(s);
+  temp_stream ts;
+  staged_download(dst, src, bytes, ts.s);
 }
 
 pdlp_result pdlp_solve(const lp_input& in, const pdlp_params& p)
