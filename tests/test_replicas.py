@@ -64,3 +64,29 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch):
     monkeypatch.setattr(bench, "make_lp", lambda *a: called.append(a))
     assert bench.run_reference(None) is None
     assert not called
+
+
+def test_reference_arm_prints_one_contract_line():
+    """`bench.py --impl reference` prints one JSON line with the contract's keys, on the small
+    2000 x 5000 workload (the oracle's FP64 PDHG iterations on the host)."""
+    import json
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    res = subprocess.run([sys.executable, str(root / "bench.py"), "--impl", "reference",
+                          "--config", "c0", "--steps", "1", "--warmup", "1",
+                          "--cpu-seconds", "1"], capture_output=True, text=True, timeout=300,
+                         cwd=root, env={**os.environ, "RANK": "0", "WORLD_SIZE": "1"})
+    assert res.returncode == 0, res.stderr
+    lines = [l for l in res.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+              "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
+              "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["value"] > 0 and d["higher_is_better"] is True
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert "2000x5000" in d["config"]["workload"]
