@@ -86,6 +86,9 @@ def ShardedBatchSolve(data_model_list, solver_settings: lpm.SolverSettings | Non
     every rank (host objects, after the solves); without it the entries solved on other ranks are
     None.  An error on any rank is raised on every rank after the exchange, so no rank is left
     waiting in a collective.  Without an initialised process group this is `BatchSolve`.
+
+    The solve runs on the calling thread's current CUDA device; with an NCCL group, set it to the
+    rank's own GPU first (`torch.cuda.set_device`), which the object collectives also need.
     """
     import torch.distributed as dist
 
