@@ -287,3 +287,27 @@ def test_large_problem_checks_without_gpu():
     bad_cup[m - 7] = -1.0
     assert solve(off, vlo, vup, clo, bad_cup) == (0, 2)
     L.cuOptDestroySolverSettings(C.byref(s))
+
+
+def test_without_a_gpu_every_solve_reports_a_cuda_error():
+    """No CPU fallback: without a device, the single, batch, climber and strong-branching solves
+    end with RuntimeError and a CUDA error message, and return no solution values."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from cuopt_b200 import generators as gen
+    from tests.helpers import datamodel_from_lp
+    lp = gen.constructed_lp(50, 120, 4, seed=1)
+    dm = datamodel_from_lp(lp)
+    s = _py_settings()
+    sols = [lpm.Solve(dm, s)]
+    sols += lpm.BatchSolve([dm, dm], s)[0]
+    sols += lpm.SolveClimbers(dm, [0, 1], [0.0, 0.0], [1.0, 1.0], s)[0]
+    sols += lpm.BatchPDLPStrongBranching(dm, [2], [0.5] + [0.0] * (lp.n - 1), s)[0]
+    assert len(sols) == 7
+    for sol in sols:
+        assert sol is not None
+        assert sol.get_error_status() == lpm.ErrorStatus.RuntimeError
+        assert "CUDA" in sol.get_error_message()
+        assert sol.get_termination_status() == lpm.LPTerminationStatus.NoTermination
+        assert not np.any(sol.get_primal_solution())
