@@ -119,8 +119,7 @@ class engine {
   // stopped, until the tolerances of this engine's parameters hold on the original LP.  Iteration
   // counts, restarts and times continue those of the first solve.
   template <typename TM>
-  pdlp_result continue_from(engine<TM>& mixed, const pdlp_result& first, double* x_out,
-                            double* y_out, double* rc_out)
+  pdlp_result continue_from(engine<TM>& mixed, double* x_out, double* y_out, double* rc_out)
   {
     alloc_scope scope(s_);
     x_out_  = x_out;
@@ -1018,7 +1017,7 @@ pdlp_result pdlp_solve_device(const lp_device_input& in, const pdlp_params& p, c
       q.abs_gap = q.rel_gap = p.refinement_tol;
     }
     engine<double> d(in, q, js.own);
-    return d.continue_from(e, r, x_out, y_out, rc_out);
+    return d.continue_from(e, x_out, y_out, rc_out);
   }
   engine<double> e(in, p, js.own);
   return e.run(x_out, y_out, rc_out);
