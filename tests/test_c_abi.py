@@ -311,3 +311,38 @@ def test_without_a_gpu_every_solve_reports_a_cuda_error():
         assert "CUDA" in sol.get_error_message()
         assert sol.get_termination_status() == lpm.LPTerminationStatus.NoTermination
         assert not np.any(sol.get_primal_solution())
+
+
+def test_large_problem_roundtrips_through_the_getters():
+    """Arrays of several MiB (the library's huge-page blocks and threaded copies) come back from
+    the getters exactly as given, also after freed blocks have been reused by a second problem."""
+    L = lib()
+    p = lambda a: C.c_void_p(a.ctypes.data)
+    rng = np.random.default_rng(11)
+    m, n, per_row = 400_000, 700_000, 3
+    nnz = m * per_row
+    for rep in range(2):
+        off = np.arange(0, nnz + 1, per_row, dtype=np.int32)
+        idx = rng.integers(0, n, nnz).astype(np.int32)
+        val = rng.standard_normal(nnz)
+        c, vlo, vup = rng.standard_normal(n), -rng.random(n), rng.random(n) + 1.0
+        clo, cup = -rng.random(m) - rep, rng.random(m)
+        h = C.c_void_p()
+        assert L.cuOptCreateRangedProblem(m, n, -1, 0.5 * rep, p(c), p(off), p(idx), p(val),
+                                          p(clo), p(cup), p(vlo), p(vup), b"C" * n,
+                                          C.byref(h)) == 0
+        got_off, got_idx = np.empty(m + 1, np.int32), np.empty(nnz, np.int32)
+        got_val, got_c = np.empty(nnz), np.empty(n)
+        got = {k: np.empty(len(v)) for k, v in
+               (("clo", clo), ("cup", cup), ("vlo", vlo), ("vup", vup))}
+        assert L.cuOptGetConstraintMatrix(h, p(got_off), p(got_idx), p(got_val)) == 0
+        assert L.cuOptGetObjectiveCoefficients(h, p(got_c)) == 0
+        assert L.cuOptGetConstraintLowerBounds(h, p(got["clo"])) == 0
+        assert L.cuOptGetConstraintUpperBounds(h, p(got["cup"])) == 0
+        assert L.cuOptGetVariableLowerBounds(h, p(got["vlo"])) == 0
+        assert L.cuOptGetVariableUpperBounds(h, p(got["vup"])) == 0
+        assert np.array_equal(got_off, off) and np.array_equal(got_idx, idx)
+        assert np.array_equal(got_val, val) and np.array_equal(got_c, c)
+        for k, v in (("clo", clo), ("cup", cup), ("vlo", vlo), ("vup", vup)):
+            assert np.array_equal(got[k], v), k
+        L.cuOptDestroyProblem(C.byref(h))
