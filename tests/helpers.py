@@ -88,3 +88,50 @@ def infeasible_cases(golden_dir):
     afiro.var_lo[1:8], afiro.var_up[1:8] = 7.0, 8.0
     afiro.var_lo[13:27], afiro.var_up[13:27] = 1.0, 5.0
     return [("two_rows", tiny), ("afiro_new_bounds", afiro)]
+
+
+# Small LPs written out in the reference's own tests, restated as DataModels.
+
+def reference_ranged_lp() -> lpm.DataModel:
+    """max 5x + 8y  s.t.  2x + 3y <= 12,  3x + y <= 6,  2 <= x + 2y <= 8,  0 <= x, y <= 10
+    (cpp/tests/linear_programming/c_api_tests/c_api_test.c:927-1041; optimum 32)."""
+    dm = lpm.DataModel()
+    dm.set_maximize(True)
+    dm.set_csr_constraint_matrix([2.0, 3.0, 3.0, 1.0, 1.0, 2.0], [0, 1, 0, 1, 0, 1], [0, 2, 4, 6])
+    dm.set_objective_coefficients([5.0, 8.0])
+    dm.set_constraint_lower_bounds([-np.inf, -np.inf, 2.0])
+    dm.set_constraint_upper_bounds([12.0, 6.0, 8.0])
+    dm.set_variable_lower_bounds([0.0, 0.0])
+    dm.set_variable_upper_bounds([10.0, 10.0])
+    return dm
+
+
+MAXIMIZE_DUAL_RHS = np.array([1.0, 55.0, 3.0])
+
+
+def reference_maximize_dual_lp() -> lpm.DataModel:
+    """max 4x1 + x2 + 5x3 + 3x4  s.t.  x1 - x2 - x3 + 3x4 <= 1,  5x1 + x2 + 3x3 + 8x4 <= 55,
+    -x1 + 2x2 + 3x3 - 5x4 <= 3,  x >= 0 (c_api_test.c:1461-1614: the objective equals the dual
+    objective sum_i y_i rhs_i)."""
+    dm = lpm.DataModel()
+    dm.set_maximize(True)
+    dm.set_csr_constraint_matrix([1.0, -1.0, -1.0, 3.0, 5.0, 1.0, 3.0, 8.0, -1.0, 2.0, 3.0, -5.0],
+                                 [0, 1, 2, 3] * 3, [0, 4, 8, 12])
+    dm.set_objective_coefficients([4.0, 1.0, 5.0, 3.0])
+    dm.set_constraint_bounds(MAXIMIZE_DUAL_RHS)
+    dm.set_row_types(["L", "L", "L"])
+    dm.set_variable_lower_bounds([0.0] * 4)
+    dm.set_variable_upper_bounds([np.inf] * 4)
+    return dm
+
+
+def chess_set_lp() -> lpm.DataModel:
+    """max 5xs + 20xl  s.t.  xs + 3xl <= 200,  3xs + 2xl <= 160,  x >= 0
+    (cpp/tests/dual_simplex/unit_tests/solve.cpp:23-94; optimum 1333.33 at (0, 66.6667))."""
+    dm = lpm.DataModel()
+    dm.set_maximize(True)
+    dm.set_csr_constraint_matrix([1.0, 3.0, 3.0, 2.0], [0, 1, 0, 1], [0, 2, 4])
+    dm.set_objective_coefficients([5.0, 20.0])
+    dm.set_constraint_bounds([200.0, 160.0])
+    dm.set_row_types(["L", "L"])
+    return dm

@@ -1,0 +1,51 @@
+"""GPU tests on the small LPs written out in the reference's own tests: the ranged C API problem
+(c_api_tests.cpp:105-112), the maximisation whose objective must equal its dual objective
+(c_api_tests.cpp:149-165) and the chess-set LP (dual_simplex/unit_tests/solve.cpp:23-94).
+
+Each is solved through the C-ABI and checked against the golden values of those tests (with their
+tolerances) and against the oracle: same status and iteration count, objective within 1e-9
+relative (FP64 path; summation order differs).
+"""
+from __future__ import annotations
+
+import pytest
+
+from cuopt_b200 import linear_programming as lpm
+from oracle import oracle as O
+from tests.helpers import (MAXIMIZE_DUAL_RHS, chess_set_lp, oracle_view, reference_maximize_dual_lp,
+                           reference_ranged_lp, rel, settings)
+
+pytestmark = pytest.mark.gpu
+
+
+def _solve_both(dm, tol, method=None):
+    sol = lpm.Solve(dm, settings(tol=tol, method=method))
+    res, x, y, _ = O.solve(oracle_view(dm), tol=tol)
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert res["status"] == 1
+    assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+    assert rel(sol.get_primal_objective(), res["primal_obj"]) <= 1e-9
+    return sol
+
+
+@pytest.mark.parametrize("tol", [1e-4, 1e-8])
+def test_reference_ranged_problem(golden, tol):
+    g = golden["ranged_problem_objective"]
+    sol = _solve_both(reference_ranged_lp(), tol)
+    assert abs(sol.get_primal_objective() - g["value"]) <= g["abs_tol"]
+
+
+@pytest.mark.parametrize("method", [lpm.SolverMethod.Concurrent, lpm.SolverMethod.PDLP])
+def test_reference_maximize_dual_variables(golden, method):
+    g = golden["maximize_dual_objective_match"]
+    sol = _solve_both(reference_maximize_dual_lp(), 1e-4, method)
+    dual_objective = sol.get_dual_solution() @ MAXIMIZE_DUAL_RHS
+    assert abs(sol.get_primal_objective() - dual_objective) <= g["abs_tol"]
+
+
+def test_chess_set(golden):
+    g = golden["chess_set_dual_simplex"]
+    sol = _solve_both(chess_set_lp(), 1e-8)
+    x = sol.get_primal_solution()
+    assert abs(sol.get_primal_objective() - g["objective"]) <= 1e-2
+    assert abs(x[0] - g["x"][0]) <= 1e-6 and abs(x[1] - g["x"][1]) <= 1e-3

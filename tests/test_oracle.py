@@ -11,7 +11,8 @@ import pytest
 from cuopt_b200 import generators as gen
 from cuopt_b200 import linear_programming as lpm
 from oracle import oracle as O
-from tests.helpers import oracle_view, rel
+from tests.helpers import (MAXIMIZE_DUAL_RHS, chess_set_lp, oracle_view, reference_maximize_dual_lp,
+                           reference_ranged_lp, rel)
 
 
 def test_methodical1_initial_step_and_weight_match_reference_golden(golden, golden_dir):
@@ -248,3 +249,33 @@ def test_tiny_lp_of_the_reference_python_tests():
     assert res["status"] == 1
     assert x[0] == 0.0 and res["primal_obj"] == 0.0 and res["dual_obj"] == 0.0
     assert res["l2_primal"] == 0.0 and res["l2_dual"] == 0.0 and res["gap"] == 0.0
+
+
+@pytest.mark.parametrize("tol", [1e-4, 1e-6, 1e-8])
+def test_reference_ranged_problem(golden, tol):
+    """c_api_tests.cpp:105-112: Optimal with objective 32 within 1e-3."""
+    g = golden["ranged_problem_objective"]
+    res, _, _, _ = O.solve(oracle_view(reference_ranged_lp()), tol=tol)
+    assert res["status"] == 1
+    assert abs(res["primal_obj"] - g["value"]) <= g["abs_tol"]
+
+
+def test_reference_maximize_dual_variables(golden):
+    """c_api_tests.cpp:149-165: for a maximisation, the objective equals sum_i y_i rhs_i within
+    1e-2 (the PDLP tolerance there) at the default tolerance, which pins the sign of the duals."""
+    g = golden["maximize_dual_objective_match"]
+    res, x, y, _ = O.solve(oracle_view(reference_maximize_dual_lp()), tol=1e-4)
+    assert res["status"] == 1
+    assert abs(res["primal_obj"] - y @ MAXIMIZE_DUAL_RHS) <= g["abs_tol"]
+    assert (y >= 0).all()
+
+
+@pytest.mark.parametrize("tol", [1e-6, 1e-8])
+def test_chess_set(golden, tol):
+    """dual_simplex/unit_tests/solve.cpp:86-88: objective 1333.33 (1e-2), x = (0 (1e-6), 66.6667
+    (1e-3))."""
+    g = golden["chess_set_dual_simplex"]
+    res, x, _, _ = O.solve(oracle_view(chess_set_lp()), tol=tol)
+    assert res["status"] == 1
+    assert abs(res["primal_obj"] - g["objective"]) <= 1e-2
+    assert abs(x[0] - g["x"][0]) <= 1e-6 and abs(x[1] - g["x"][1]) <= 1e-3
