@@ -135,3 +135,34 @@ def chess_set_lp() -> lpm.DataModel:
     dm.set_constraint_bounds([200.0, 160.0])
     dm.set_row_types(["L", "L"])
     return dm
+
+
+def with_variable_bounds(view, j, lo, up):
+    """A copy of an oracle view whose variable j has the bounds [lo, up] (a climber's LP)."""
+    import copy
+    q = copy.copy(view)
+    q.var_lo = np.array(view.var_lo, dtype=np.float64)
+    q.var_up = np.array(view.var_up, dtype=np.float64)
+    q.var_lo[j], q.var_up[j] = lo, up
+    return q
+
+
+def highs_objective(view):
+    """Optimal objective of an oracle view by SciPy HiGHS (a third-party cross-check)."""
+    from scipy.optimize import linprog
+    from scipy.sparse import csr_matrix
+
+    A = csr_matrix((view.val, view.col_idx, view.row_off), shape=(view.m, view.n))
+    lo, up = np.asarray(view.con_lo), np.asarray(view.con_up)
+    eq = lo == up
+    ub_rows = np.isfinite(up) & ~eq
+    lb_rows = np.isfinite(lo) & ~eq
+    from scipy.sparse import vstack
+    A_ub = vstack([A[ub_rows], -A[lb_rows]])
+    b_ub = np.concatenate([up[ub_rows], -lo[lb_rows]])
+    bounds = [(l, None if np.isinf(u) else u) for l, u in zip(view.var_lo, view.var_up)]
+    sign = -1.0 if view.maximize else 1.0
+    r = linprog(sign * np.asarray(view.c), A_ub=A_ub, b_ub=b_ub, A_eq=A[eq], b_eq=lo[eq],
+                bounds=bounds, method="highs")
+    assert r.status == 0, r.message
+    return sign * r.fun + view.obj_offset

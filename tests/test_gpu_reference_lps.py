@@ -49,3 +49,31 @@ def test_chess_set(golden):
     x = sol.get_primal_solution()
     assert abs(sol.get_primal_objective() - g["objective"]) <= 1e-2
     assert abs(x[0] - g["x"][0]) <= 1e-6 and abs(x[1] - g["x"][1]) <= 1e-3
+
+
+def test_afiro_climbers_with_different_bounds_like_the_reference(golden, golden_dir):
+    """pdlp_test.cu:1194-1287 (more_complex_batch_different_bounds): five afiro climbers, #1 with
+    variable 5 in [4, 5] and #3 with variable 1 in [-7, 13], the others unchanged.  All are
+    Optimal; #0, #2 and #4 have the same objective, at afiro's; #1 and #3 stop where the oracle's
+    solves of their LPs stop, at the same objective (1e-8 relative)."""
+    import numpy as np
+
+    from tests.helpers import with_variable_bounds
+
+    dm = lpm.ReadMps(golden_dir / "afiro_original.mps")
+    v = oracle_view(dm)
+    var = np.array([0, 5, 0, 1, 0], np.int32)
+    lo = np.array([v.var_lo[0], 4.0, v.var_lo[0], -7.0, v.var_lo[0]])
+    up = np.array([v.var_up[0], 5.0, v.var_up[0], 13.0, v.var_up[0]])
+    sols, _ = lpm.SolveClimbers(dm, var, lo, up, settings(tol=1e-4))
+    for sol in sols:
+        assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    g = golden["afiro_objective"]
+    assert rel(sols[0].get_primal_objective(), g["value"]) <= g["rel_tol"]
+    assert sols[0].get_primal_objective() == sols[2].get_primal_objective() == \
+        sols[4].get_primal_objective()
+    for b in (1, 3):
+        res, _, _, _ = O.solve(with_variable_bounds(v, var[b], lo[b], up[b]), tol=1e-4)
+        assert res["status"] == 1
+        assert sols[b].get_lp_stats()["nb_iterations"] == res["iterations"]
+        assert rel(sols[b].get_primal_objective(), res["primal_obj"]) <= 1e-8

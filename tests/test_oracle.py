@@ -279,3 +279,15 @@ def test_chess_set(golden, tol):
     assert res["status"] == 1
     assert abs(res["primal_obj"] - g["objective"]) <= 1e-2
     assert abs(x[0] - g["x"][0]) <= 1e-6 and abs(x[1] - g["x"][1]) <= 1e-3
+
+
+@pytest.mark.parametrize("j,lo,up", [(5, 4.0, 5.0), (1, -7.0, 13.0)])
+def test_afiro_with_the_reference_batch_tests_bounds(golden_dir, j, lo, up):
+    """The climbers of pdlp_test.cu:1138-1287 (afiro with variable 5 in [4, 5], or variable 1 in
+    [-7, 13]) solve Optimal on the oracle, at HiGHS's optimum (1e-7 relative at 1e-8 tolerance)."""
+    pytest.importorskip("scipy")
+    from tests.helpers import highs_objective, with_variable_bounds
+    q = with_variable_bounds(oracle_view(lpm.ReadMps(golden_dir / "afiro_original.mps")), j, lo, up)
+    res, _, _, _ = O.solve(q, tol=1e-8)
+    assert res["status"] == 1
+    assert rel(res["primal_obj"], highs_objective(q)) <= 1e-7
