@@ -14,7 +14,8 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 DATASETS = ["afiro_original.mps", "good-max.mps", "max_offset.mps", "lp-model-no-constraints.mps",
-            "empty_matrix.mps", "lp_model_with_var_bounds.mps", "good-mps-fixed-ranges.mps"]
+            "empty_matrix.mps", "lp_model_with_var_bounds.mps", "good-mps-fixed-ranges.mps",
+            "good-mps-some-var-bounds.mps", "good-mps-1.mps"]
 
 GOLDEN = {
     "afiro_objective": {
@@ -46,6 +47,22 @@ GOLDEN = {
         "abs_tol": 1e-2,
         "source": "cpp/tests/linear_programming/c_api_tests/c_api_tests.cpp:149-165, "
                   "c_api_test.c:1461-1614"},
+    "many_different_bounds": {
+        "variable": 0, "upper": 10.0,
+        "lower": [-133.0, None, -133.0, None, -183.0, -233.0, None, -1033.0, -1033.0, -1283.0,
+                  -2533.0, None, None],
+        "constraint_tol": 1e-8,
+        "note": "None keeps the variable's own bounds; every climber as its single solve, with "
+                "constraint violations under constraint_tol",
+        "source": "cpp/tests/linear_programming/pdlp_test.cu:1720-1804 (good-mps-some-var-bounds)"},
+    "some_climber_hit_iteration_limit": {
+        "variable": 0, "upper": 10.0, "lower": [-2533.0, None], "iteration_limit": 500,
+        "statuses": ["IterationLimit", "Optimal"],
+        "note": "the test's comment: one climber converges within the limit, the other hits it",
+        "source": "cpp/tests/linear_programming/pdlp_test.cu:1806-1885"},
+    "good_mps_1_optimal": {
+        "tol": 1e-2, "status": "Optimal",
+        "source": "python/cuopt/cuopt/tests/linear_programming/test_lp_solver.py:82-89"},
     "chess_set_dual_simplex": {
         "objective": 1333.333333, "x": [0.0, 66.666667], "tol": 1e-5,
         "source": "cpp/tests/dual_simplex/unit_tests/solve.cpp:23-94"},

@@ -77,3 +77,61 @@ def test_afiro_climbers_with_different_bounds_like_the_reference(golden, golden_
         assert res["status"] == 1
         assert sols[b].get_lp_stats()["nb_iterations"] == res["iterations"]
         assert rel(sols[b].get_primal_objective(), res["primal_obj"]) <= 1e-8
+
+
+def _variant_bounds(view, g):
+    import numpy as np
+    j = g["variable"]
+    lo = np.array([view.var_lo[j] if v is None else v for v in g["lower"]])
+    up = np.array([view.var_up[j] if v is None else g["upper"] for v in g["lower"]])
+    return np.full(len(lo), j, np.int32), lo, up
+
+
+def test_many_different_bounds_climbers(golden, golden_dir):
+    """pdlp_test.cu:1720-1804: 13 climbers of good-mps-some-var-bounds (two groups of eight, from
+    210 to about 16 000 iterations) each end as the oracle's solve of its LP does: same status,
+    iteration count within 5 %, the optimum (HiGHS) within 1e-3 relative, constraint violations
+    under 1e-8."""
+    import numpy as np
+    from scipy.sparse import csr_matrix
+
+    from tests.helpers import highs_objective, with_variable_bounds
+
+    g = golden["many_different_bounds"]
+    dm = lpm.ReadMps(golden_dir / "good-mps-some-var-bounds.mps")
+    v = oracle_view(dm)
+    var, lo, up = _variant_bounds(v, g)
+    sols, _ = lpm.SolveClimbers(dm, var, lo, up, settings(tol=1e-4))
+    A = csr_matrix((v.val, v.col_idx, v.row_off), shape=(v.m, v.n))
+    for b, sol in enumerate(sols):
+        q = with_variable_bounds(v, var[b], lo[b], up[b])
+        res, _, _, _ = O.solve(q, tol=1e-4)
+        assert int(sol.get_termination_status()) == res["status"] == 1
+        it = sol.get_lp_stats()["nb_iterations"]
+        assert abs(it - res["iterations"]) <= 0.05 * res["iterations"] + 10
+        assert rel(sol.get_primal_objective(), highs_objective(q)) <= 1e-3
+        x = sol.get_primal_solution()
+        ax = A @ x
+        viol = max(np.max(np.maximum(0.0, ax - q.con_up)), np.max(np.maximum(0.0, q.con_lo - ax)),
+                   np.max(np.maximum(0.0, q.var_lo - x)), np.max(np.maximum(0.0, x - q.var_up)))
+        assert viol <= g["constraint_tol"]
+
+
+def test_some_climber_hits_the_iteration_limit(golden, golden_dir):
+    """pdlp_test.cu:1806-1885: at 500 iterations one climber hits the limit and the other is
+    Optimal, with the oracle's iteration count and objective (1e-8 relative)."""
+    from tests.helpers import with_variable_bounds
+
+    g = golden["some_climber_hit_iteration_limit"]
+    dm = lpm.ReadMps(golden_dir / "good-mps-some-var-bounds.mps")
+    v = oracle_view(dm)
+    var, lo, up = _variant_bounds(v, g)
+    sols, _ = lpm.SolveClimbers(dm, var, lo, up,
+                                settings(tol=1e-4, iteration_limit=g["iteration_limit"]))
+    for b, (sol, status) in enumerate(zip(sols, g["statuses"])):
+        assert sol.get_termination_status() == lpm.LPTerminationStatus[status]
+        if status == "Optimal":
+            res, _, _, _ = O.solve(with_variable_bounds(v, var[b], lo[b], up[b]), tol=1e-4,
+                                   iteration_limit=g["iteration_limit"])
+            assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+            assert rel(sol.get_primal_objective(), res["primal_obj"]) <= 1e-8

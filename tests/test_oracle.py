@@ -291,3 +291,48 @@ def test_afiro_with_the_reference_batch_tests_bounds(golden_dir, j, lo, up):
     res, _, _, _ = O.solve(q, tol=1e-8)
     assert res["status"] == 1
     assert rel(res["primal_obj"], highs_objective(q)) <= 1e-7
+
+
+def _bound_variants(view, g):
+    from tests.helpers import with_variable_bounds
+    j = g["variable"]
+    return [view if lo is None else with_variable_bounds(view, j, lo, g["upper"]) for lo in g["lower"]]
+
+
+def _violation(q, x):
+    from scipy.sparse import csr_matrix
+    ax = csr_matrix((q.val, q.col_idx, q.row_off), shape=(q.m, q.n)) @ x
+    return max(np.max(np.maximum(0.0, ax - q.con_up)), np.max(np.maximum(0.0, q.con_lo - ax)),
+               np.max(np.maximum(0.0, q.var_lo - x)), np.max(np.maximum(0.0, x - q.var_up)))
+
+
+def test_many_different_bounds(golden, golden_dir):
+    """pdlp_test.cu:1720-1804: the 13 bound variants of good-mps-some-var-bounds solve Optimal with
+    constraint violations under 1e-8, at HiGHS's optimum (1e-9 relative)."""
+    pytest.importorskip("scipy")
+    from tests.helpers import highs_objective
+    g = golden["many_different_bounds"]
+    view = oracle_view(lpm.ReadMps(golden_dir / "good-mps-some-var-bounds.mps"))
+    for q in _bound_variants(view, g):
+        res, x, _, _ = O.solve(q)
+        assert res["status"] == 1
+        assert _violation(q, x) <= g["constraint_tol"]
+        assert rel(res["primal_obj"], highs_objective(q)) <= 1e-9
+
+
+def test_some_climber_hits_the_iteration_limit(golden, golden_dir):
+    """pdlp_test.cu:1806-1885: at 500 iterations the variant with variable 0 down to -2533 hits the
+    limit, the unchanged LP is Optimal."""
+    g = golden["some_climber_hit_iteration_limit"]
+    view = oracle_view(lpm.ReadMps(golden_dir / "good-mps-some-var-bounds.mps"))
+    want = {"IterationLimit": 4, "Optimal": 1}
+    for q, status in zip(_bound_variants(view, g), g["statuses"]):
+        res, _, _, _ = O.solve(q, iteration_limit=g["iteration_limit"])
+        assert res["status"] == want[status]
+
+
+def test_good_mps_1(golden, golden_dir):
+    """test_lp_solver.py:82-89: good-mps-1 is Optimal at tolerance 1e-2."""
+    g = golden["good_mps_1_optimal"]
+    res, _, _, _ = O.solve(oracle_view(lpm.ReadMps(golden_dir / "good-mps-1.mps")), tol=g["tol"])
+    assert res["status"] == 1
