@@ -91,13 +91,17 @@ def _holder(lp, initial_primal=None, initial_dual=None, initial_step_size=None,
 
 def solve(lp, tol=1e-4, iteration_limit=2**31 - 1, time_limit=1e300, threads=0,
           detect_infeasibility=False, infeasible_tol=1e-10, initial_primal=None, initial_dual=None,
-          initial_step_size=None, initial_primal_weight=None, per_constraint_residual=False):
+          initial_step_size=None, initial_primal_weight=None, per_constraint_residual=False,
+          abs_tol=None, rel_tol=None):
     """Runs the FP64 Stable3 restatement (optionally warm-started from an initial primal and / or
-    dual solution in the user's order, and from a given step size and primal weight).  Returns
-    (result dict, x, y, reduced_cost)."""
+    dual solution in the user's order, and from a given step size and primal weight).  `tol` sets
+    the six absolute and relative tolerances; `abs_tol` / `rel_tol` override the absolute or the
+    relative ones.  Returns (result dict, x, y, reduced_cost)."""
     h = _holder(lp, initial_primal, initial_dual, initial_step_size, initial_primal_weight)
     m, n = h.s.m, h.s.n
-    st = _Settings(tol, tol, tol, tol, tol, tol, int(iteration_limit), float(time_limit), int(threads),
+    at = tol if abs_tol is None else abs_tol
+    rt = tol if rel_tol is None else rel_tol
+    st = _Settings(at, rt, at, rt, at, rt, int(iteration_limit), float(time_limit), int(threads),
                    int(bool(detect_infeasibility)), float(infeasible_tol), float(infeasible_tol),
                    int(bool(per_constraint_residual)))
     r = _Result()

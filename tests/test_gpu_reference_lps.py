@@ -135,3 +135,49 @@ def test_some_climber_hits_the_iteration_limit(golden, golden_dir):
                                    iteration_limit=g["iteration_limit"])
             assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
             assert rel(sol.get_primal_objective(), res["primal_obj"]) <= 1e-8
+
+
+def _afiro(golden_dir):
+    return lpm.ReadMps(golden_dir / "afiro_original.mps")
+
+
+def test_afiro_at_the_minimal_absolute_tolerance(golden, golden_dir):
+    """pdlp_test.cu:76-100: absolute tolerances 1e-12, relative 0: Optimal at afiro's objective
+    (1 %)."""
+    s = settings(tol=1e-4)
+    for name in ("absolute_primal_tolerance", "absolute_dual_tolerance", "absolute_gap_tolerance"):
+        s.set_parameter(name, 1e-12)
+    for name in ("relative_primal_tolerance", "relative_dual_tolerance", "relative_gap_tolerance"):
+        s.set_parameter(name, 0.0)
+    s.set_parameter(lpm.CUOPT_TIME_LIMIT, 120.0)
+    sol = lpm.Solve(_afiro(golden_dir), s)
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert rel(sol.get_primal_objective(), golden["afiro_objective"]["value"]) <= 0.01
+
+
+def test_afiro_from_an_all_ones_primal(golden, golden_dir):
+    """pdlp_test.cu:102-122: started from x = 1: Optimal at afiro's objective (1 %), where the
+    oracle's warm-started solve stops."""
+    import numpy as np
+
+    dm = _afiro(golden_dir)
+    dm.set_initial_primal_solution(np.ones(dm.n_variables))
+    sol = lpm.Solve(dm, settings(tol=1e-4))
+    res, _, _, _ = O.solve(oracle_view(dm), initial_primal=np.ones(dm.n_variables))
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert rel(sol.get_primal_objective(), golden["afiro_objective"]["value"]) <= 0.01
+    assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+
+
+def test_afiro_iteration_limit_returns_the_current_iterate(golden_dir):
+    """pdlp_test.cu:124-147: 10 iterations at tolerance 0 end IterationLimit with the current primal
+    iterate, the oracle's to 1e-9."""
+    import numpy as np
+
+    dm = _afiro(golden_dir)
+    sol = lpm.Solve(dm, settings(tol=0.0, iteration_limit=10))
+    res, x, _, _ = O.solve(oracle_view(dm), tol=0.0, iteration_limit=10)
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.IterationLimit
+    got = sol.get_primal_solution()
+    assert np.any(got != 0.0)
+    assert np.max(np.abs(got - x)) <= 1e-9 * (1 + np.abs(x).max())

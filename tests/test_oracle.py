@@ -336,3 +336,30 @@ def test_good_mps_1(golden, golden_dir):
     g = golden["good_mps_1_optimal"]
     res, _, _, _ = O.solve(oracle_view(lpm.ReadMps(golden_dir / "good-mps-1.mps")), tol=g["tol"])
     assert res["status"] == 1
+
+
+def test_afiro_at_the_minimal_absolute_tolerance(golden, golden_dir):
+    """pdlp_test.cu:76-100: absolute tolerances at their minimum 1e-12 and relative ones 0 still end
+    Optimal, at afiro's objective (1 %)."""
+    v = oracle_view(lpm.ReadMps(golden_dir / "afiro_original.mps"))
+    res, _, _, _ = O.solve(v, abs_tol=1e-12, rel_tol=0.0, time_limit=120)
+    assert res["status"] == 1
+    assert rel(res["primal_obj"], golden["afiro_objective"]["value"]) <= 0.01
+    assert res["l2_primal"] <= 1e-12 and res["l2_dual"] <= 1e-12
+
+
+def test_afiro_from_an_all_ones_primal(golden, golden_dir):
+    """pdlp_test.cu:102-122: started from x = 1, afiro ends Optimal at its objective (1 %)."""
+    v = oracle_view(lpm.ReadMps(golden_dir / "afiro_original.mps"))
+    res, _, _, _ = O.solve(v, initial_primal=np.ones(v.n))
+    assert res["status"] == 1
+    assert rel(res["primal_obj"], golden["afiro_objective"]["value"]) <= 0.01
+
+
+def test_afiro_iteration_limit_returns_the_current_iterate(golden_dir):
+    """pdlp_test.cu:124-147: 10 iterations with tolerance 0 end IterationLimit with the current
+    (non-zero) primal iterate."""
+    v = oracle_view(lpm.ReadMps(golden_dir / "afiro_original.mps"))
+    res, x, _, _ = O.solve(v, tol=0.0, iteration_limit=10)
+    assert res["status"] == 4 and res["iterations"] == 10
+    assert np.any(x != 0.0)
