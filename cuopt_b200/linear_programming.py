@@ -6,6 +6,8 @@ Counterparts (python/cuopt/cuopt/linear_programming/ in the reference):
   Solve           solver/solver.py:13-106
   BatchSolve      solver/solver.py:109-160
   Solution        solution/solution.py:55-393         (getters, get_lp_stats)
+  PDLPWarmStartData  cpp/include/cuopt/linear_programming/pdlp/pdlp_warm_start_data.hpp
+                  (returned; rejected by the Stable3 solve as in pdlp.cu:176-181)
 Every call goes through libcuopt_b200.so; arrays are copied into the library, as in the reference.
 """
 from __future__ import annotations
@@ -264,6 +266,17 @@ class SolverSettings:
         for n in _TOLERANCE_NAMES:
             self.params[n] = float(eps_optimal)
 
+    def set_pdlp_warm_start_data(self, pdlp_warm_start_data):
+        """PDLP solver state from a previous solve (reference solver_settings.py:183-207).  The
+        reference resumes from it in Stable2 only (pdlp.cu:176-181); this library runs every mode
+        as Stable3, so a solve given it ends NoTermination with a validation error, as a Stable3
+        solve does in the reference.  Start from a previous solution with
+        DataModel.set_initial_primal_solution / set_initial_dual_solution instead."""
+        self.pdlp_warm_start_data = pdlp_warm_start_data
+
+    def get_pdlp_warm_start_data(self):
+        return getattr(self, "pdlp_warm_start_data", None)
+
     def _create(self) -> handle_t:
         L = lib()
         h = handle_t()
@@ -281,6 +294,24 @@ class SolverSettings:
                 L.cuOptDestroySolverSettings(C.byref(h))
                 _check(rc, f"set parameter {name}")
         return h
+
+
+class PDLPWarmStartData:
+    """The PDLP state a solve ends with (reference pdlp_warm_start_data.hpp): the current
+    iterates, the step size, the primal weight and the iteration counts.  The restart-state
+    vectors are those iterates."""
+
+    def __init__(self, primal, dual, step_size, primal_weight, iterations):
+        self.current_primal_solution = np.asarray(primal, dtype=np.float64)
+        self.current_dual_solution = np.asarray(dual, dtype=np.float64)
+        self.initial_primal_average = self.current_primal_solution
+        self.initial_dual_average = self.current_dual_solution
+        self.last_restart_duality_gap_primal_solution = self.current_primal_solution
+        self.last_restart_duality_gap_dual_solution = self.current_dual_solution
+        self.initial_step_size = float(step_size)
+        self.initial_primal_weight = float(primal_weight)
+        self.total_pdlp_iterations = int(iterations)
+        self.total_pdhg_iterations = int(iterations)
 
 
 class Solution:
@@ -332,6 +363,16 @@ class Solution:
     def get_solved_by_pdlp(self):
         return self.solved_by_pdlp
 
+    def get_pdlp_warm_start_data(self):
+        """The solve's final PDLP state (reference solution.py:338-346); None when the LP was not
+        solved by PDLP."""
+        if not self.solved_by_pdlp or self.error_status != ErrorStatus.Success:
+            return None
+        return PDLPWarmStartData(self.primal_solution, self.dual_solution,
+                                 self.stats.get("step_size", 0.0),
+                                 self.stats.get("primal_weight", 0.0),
+                                 self.stats.get("number_of_steps_taken", 0))
+
     def get_lp_stats(self):
         return {
             "primal_residual": self.stats.get("l2_primal_residual"),
@@ -371,10 +412,23 @@ def _apply_initial(settings_h: handle_t, data_model: DataModel) -> None:
                "cuOptSetInitialDualSolution")
 
 
+def _warm_start_rejected(data_model: DataModel) -> Solution:
+    """The reference's answer to PDLP warm-start data outside Stable2 (pdlp.cu:179-181): a
+    validation error, termination status NoTermination, zero vectors."""
+    m, n = data_model.n_constraints, data_model.n_variables
+    return Solution(np.zeros(n), np.zeros(m), np.zeros(n), int(LPTerminationStatus.NoTermination),
+                    int(ErrorStatus.ValidationError),
+                    "Only Stable2 mode supported for warm start (this library runs Stable3; start "
+                    "from a solution with set_initial_primal_solution / "
+                    "set_initial_dual_solution)", {"solved_by_pdlp": 0})
+
+
 def Solve(data_model: DataModel, solver_settings: SolverSettings | None = None) -> Solution:
     """Solves one LP (reference solver.py:13-106)."""
     L = lib()
     settings = solver_settings or SolverSettings()
+    if settings.get_pdlp_warm_start_data() is not None:
+        return _warm_start_rejected(data_model)
     p = data_model._create()
     s = settings._create()
     sol = handle_t()
@@ -394,6 +448,9 @@ def BatchSolve(data_model_list, solver_settings: SolverSettings | None = None):
 
     L = lib()
     settings = solver_settings or SolverSettings()
+    if settings.get_pdlp_warm_start_data() is not None:
+        raise CuOptError(int(ErrorStatus.ValidationError),
+                         "BatchSolve (PDLP warm-start data cannot be used with a batch)")
     probs = (handle_t * len(data_model_list))()
     sols = (handle_t * len(data_model_list))()
     for i, dm in enumerate(data_model_list):
@@ -456,6 +513,9 @@ def _solve_climbers(call, data_model, count, arrays, solver_settings):
 
     L = lib()
     settings = solver_settings or SolverSettings()
+    if settings.get_pdlp_warm_start_data() is not None:
+        raise CuOptError(int(ErrorStatus.ValidationError),
+                         "climber batch (batch mode not supported for PDLP warm-start data)")
     prob = data_model._create()
     s = settings._create()
     sols = (handle_t * count)()
