@@ -7,8 +7,20 @@
 //   * BOUNDS LO/UP/FX/FR/MI/PL/BV/LI/UI; an UP bound below 0 on a variable without an earlier
 //     bound sets the lower bound to -inf (:1386-1393);
 //   * default variable bounds [0, +inf); MARKER INTORG/INTEND marks integer columns.
-// Tokens are whitespace separated (free MPS); fixed-format files whose names contain no blanks
-// read the same way.  Compressed files are not supported.
+// Records follow the reference's free-format rules (cuOptReadProblem parses free MPS,
+// cpp/src/pdlp/cuopt_c.cpp:103-107), which fixed-format files without blanks in names also meet:
+//   * a line starting with '*' or '$' is a comment; in a data line a field starting with '$'
+//     ends the record (:594-597, 974-978, 1077-1082, 1133-1154, 1196);
+//   * a line starting with anything but a blank opens a section (:599);
+//   * OBJNAME (on its line or the next) names the objective and must come before ROWS
+//     (:1262-1281); further N rows are ignored, with their COLUMNS entries (:840-859, 1005);
+//   * duplicate rows and columns whose entries are not contiguous are errors (:863, 913);
+//   * RHS records name a set unless the first field is a row or the objective (:1050-1060);
+//     RANGES records always name a set (:1192-1193); a BOUNDS record leaves the set name out
+//     when its second field is a column, and may define a column (:1136-1167);
+//   * OBJSENSE takes MIN / MINIMIZE / MAX / MAXIMIZE only (:257-270);
+//   * an objective row and the ROWS, COLUMNS and RHS sections are required (:772-780).
+// Compressed files are not supported.
 #include <cuopt/linear_programming/constants.h>
 
 #include <cmath>
@@ -29,12 +41,21 @@ namespace {
 
 constexpr double kInf = std::numeric_limits<double>::infinity();
 
-std::vector<std::string> split(const std::string& line)
+// Whitespace-separated fields up to the first one that starts with '$' (the rest of the line is a
+// comment); `cut` tells whether such a field was met.
+std::vector<std::string> split(const std::string& line, bool& cut)
 {
   std::vector<std::string> t;
   std::istringstream ss(line);
   std::string w;
-  while (ss >> w) t.push_back(w);
+  cut = false;
+  while (ss >> w) {
+    if (w[0] == '$') {
+      cut = true;
+      break;
+    }
+    t.push_back(w);
+  }
   return t;
 }
 
@@ -58,8 +79,10 @@ int read_mps(const std::string& path, lp_problem& out, std::string& err)
     err = "Error opening MPS file";
     return CUOPT_MPS_FILE_ERROR;
   }
-  enum sec { NONE, NAME, OBJSENSE, ROWS, COLUMNS, RHS, RANGES, BOUNDS, END } cur = NONE;
+  enum sec { NONE, NAME, OBJSENSE, OBJNAME, ROWS, COLUMNS, RHS, RANGES, BOUNDS, END } cur = NONE;
   std::string obj_row;
+  std::set<std::string> ignored_obj;  // N rows after the objective
+  bool seen_rows = false, seen_columns = false, seen_rhs = false;
   std::vector<std::string> row_names;
   std::vector<char> row_types;
   std::unordered_map<std::string, int> row_id, col_id;
@@ -90,14 +113,25 @@ int read_mps(const std::string& path, lp_problem& out, std::string& err)
     vtype.push_back(integer_block ? 'I' : 'C');
     return id;
   };
+  auto set_sense = [&](const std::string& w) {
+    if (w == "MIN" || w == "MINIMIZE") maximize = false;
+    else if (w == "MAX" || w == "MAXIMIZE") maximize = true;
+    else return false;
+    return true;
+  };
+  auto set_objname = [&](const std::string& w) {
+    if (!obj_row.empty()) return false;  // OBJNAME must precede ROWS
+    obj_row = w;
+    return true;
+  };
   while (std::getline(f, line)) {
     ++lineno;
     if (!line.empty() && line.back() == '\r') line.pop_back();
-    if (line.empty() || line[0] == '*') continue;
-    auto tok = split(line);
+    if (line.empty() || line[0] == '*' || line[0] == '$') continue;
+    bool cut  = false;
+    auto tok  = split(line, cut);
     if (tok.empty()) continue;
-    const bool header = !std::isspace((unsigned char)line[0]);
-    if (header) {
+    if (line[0] != ' ') {
       const std::string& h = tok[0];
       if (h == "NAME") {
         cur = NAME;
@@ -106,12 +140,23 @@ int read_mps(const std::string& path, lp_problem& out, std::string& err)
       }
       if (h == "OBJSENSE") {
         cur = OBJSENSE;
-        if (tok.size() > 1) maximize = (tok[1] == "MAX" || tok[1] == "MAXIMIZE");
+        if (tok.size() > 1 && !set_sense(tok[1])) return fail("Bad OBJSENSE " + tok[1]);
         continue;
       }
-      if (h == "ROWS") { cur = ROWS; continue; }
-      if (h == "COLUMNS") { cur = COLUMNS; continue; }
-      if (h == "RHS") { cur = RHS; continue; }
+      if (h == "OBJNAME") {
+        cur = OBJNAME;
+        if (tok.size() > 1 && !set_objname(tok[1]))
+          return fail("OBJNAME must come before the ROWS section");
+        continue;
+      }
+      if (h == "ROWS") { cur = ROWS; seen_rows = true; continue; }
+      if (h == "COLUMNS") { cur = COLUMNS; seen_columns = true; continue; }
+      if (h == "RHS") {
+        cur      = RHS;
+        seen_rhs = true;
+        if (rhs.empty()) rhs.assign(row_names.size(), 0.0);
+        continue;
+      }
       if (h == "RANGES") {
         cur = RANGES;
         ranges.assign(row_names.size(), unset);
@@ -119,25 +164,26 @@ int read_mps(const std::string& path, lp_problem& out, std::string& err)
       }
       if (h == "BOUNDS") { cur = BOUNDS; continue; }
       if (h == "ENDATA") { cur = END; break; }
-      if (h == "OBJSENSE" || h == "MAX" || h == "MIN" || h == "MAXIMIZE" || h == "MINIMIZE") {
-        if (cur == OBJSENSE) maximize = (h == "MAX" || h == "MAXIMIZE");
-        continue;
-      }
-      if (cur != OBJSENSE) return fail("Unknown section " + h);
+      return fail("Unknown section " + h);
     }
     switch (cur) {
       case OBJSENSE:
-        maximize = (tok[0] == "MAX" || tok[0] == "MAXIMIZE");
+        if (!set_sense(tok[0])) return fail("Bad OBJSENSE " + tok[0]);
+        break;
+      case OBJNAME:
+        if (!set_objname(tok[0])) return fail("OBJNAME must come before the ROWS section");
         break;
       case ROWS: {
         if (tok.size() < 2) return fail("Bad ROWS line");
         const std::string& t = tok[0];
         if (t == "N") {
           if (obj_row.empty()) obj_row = tok[1];
+          else if (tok[1] != obj_row) ignored_obj.insert(tok[1]);
           break;
         }
         if (t != "E" && t != "L" && t != "G") return fail("Bad row type " + t);
-        row_id.emplace(tok[1], (int)row_names.size());
+        if (!row_id.emplace(tok[1], (int)row_names.size()).second)
+          return fail("Duplicate row " + tok[1]);
         row_names.push_back(tok[1]);
         row_types.push_back(t[0]);
         break;
@@ -148,7 +194,11 @@ int read_mps(const std::string& path, lp_problem& out, std::string& err)
           if (tok[2] == "'INTEND'") integer_block = false;
           break;
         }
-        if (tok.size() < 3 || tok.size() % 2 == 0) return fail("Bad COLUMNS line");
+        // A record cut short by a comment after the column name only names the column.
+        if (tok.size() % 2 == 0) return fail("Bad COLUMNS line");
+        auto known = col_id.find(tok[0]);
+        if (known != col_id.end() && known->second != (int)col_names.size() - 1)
+          return fail("Entries of column " + tok[0] + " are not contiguous");
         const int j = col_of(tok[0]);
         for (size_t q = 1; q + 1 < tok.size(); q += 2) {
           double v;
@@ -157,6 +207,7 @@ int read_mps(const std::string& path, lp_problem& out, std::string& err)
             cost[j] = v;
             continue;
           }
+          if (ignored_obj.count(tok[q])) continue;
           auto it = row_id.find(tok[q]);
           if (it == row_id.end()) return fail("Unknown row " + tok[q]);
           cols[j].emplace_back(it->second, v);
@@ -165,13 +216,15 @@ int read_mps(const std::string& path, lp_problem& out, std::string& err)
       }
       case RHS:
       case RANGES: {
-        if (cur == RHS && rhs.empty()) rhs.assign(row_names.size(), 0.0);
-        size_t q = (tok.size() % 2 == 1) ? 1 : 0;  // optional set name
+        size_t q;
+        if (cur == RHS) q = (tok[0] == obj_row || row_id.count(tok[0])) ? 0 : 1;
+        else q = 1;
+        if ((tok.size() - q) % 2 != 0) return fail("Bad RHS/RANGES line");  // tok.size() >= 1 >= q
         for (; q + 1 < tok.size(); q += 2) {
           double v;
           if (!to_double(tok[q + 1], v)) return fail("Bad value in RHS/RANGES");
-          if (tok[q] == obj_row) {
-            if (cur == RHS) offset = -v;
+          if (cur == RHS && tok[q] == obj_row) {
+            offset = -v;
             continue;
           }
           auto it = row_id.find(tok[q]);
@@ -183,20 +236,19 @@ int read_mps(const std::string& path, lp_problem& out, std::string& err)
       case BOUNDS: {
         const std::string& t = tok[0];
         const bool novalue   = (t == "FR" || t == "MI" || t == "PL" || t == "BV");
-        std::string cname;
-        double v = 0.0;
-        if (novalue) {
-          if (tok.size() < 2) return fail("Bad BOUNDS line");
-          cname = tok.size() >= 3 ? tok[2] : tok[1];
-        } else {
-          if (tok.size() < 3) return fail("Bad BOUNDS line");
-          cname                 = tok.size() >= 4 ? tok[2] : tok[1];
-          const std::string& vs = tok.size() >= 4 ? tok[3] : tok[2];
-          if (!to_double(vs, v)) return fail("Bad value in BOUNDS");
+        // The bound set name is left out when the second field is a column.
+        const size_t vi = (tok.size() > 1 && col_id.count(tok[1])) ? 1 : 2;
+        if (tok.size() <= vi) {
+          if (cut) break;  // the column field is a comment
+          return fail("Bad BOUNDS line");
         }
-        auto it = col_id.find(cname);
-        if (it == col_id.end()) return fail("Unknown column " + cname);
-        const int j = it->second;
+        const std::string cname = tok[vi];
+        double v                = 0.0;
+        if (!novalue) {
+          if (tok.size() <= vi + 1) return fail("Bad BOUNDS line");
+          if (!to_double(tok[vi + 1], v)) return fail("Bad value in BOUNDS");
+        }
+        const int j = col_of(cname);  // a column named only here has no entries
         if (t == "LO") lo[j] = v;
         else if (t == "UP" || t == "UI") {
           up[j] = v;
@@ -226,6 +278,10 @@ int read_mps(const std::string& path, lp_problem& out, std::string& err)
       default: return fail("Data outside a section");
     }
   }
+  if (obj_row.empty()) return fail("No objective row");
+  if (!seen_rows) return fail("ROWS section missing");
+  if (!seen_columns) return fail("COLUMNS section missing");
+  if (!seen_rhs) return fail("RHS section missing");
   const int m = (int)row_names.size(), n = (int)col_names.size();
   if (rhs.empty()) rhs.assign(m, 0.0);
   out.m          = m;

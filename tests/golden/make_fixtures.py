@@ -3,6 +3,7 @@ reference tree is available; the fixtures are committed so tests never read the 
 
 Fixtures:
   *.mps           copies of the reference's small LP datasets (datasets/linear_programming/)
+  mps/*.mps       the reference's MPS parser test datasets (same folder)
   golden.json     expected values taken from the reference's own tests, with their source lines.
 """
 from __future__ import annotations
@@ -16,6 +17,19 @@ HERE = Path(__file__).resolve().parent
 DATASETS = ["afiro_original.mps", "good-max.mps", "max_offset.mps", "lp-model-no-constraints.mps",
             "empty_matrix.mps", "lp_model_with_var_bounds.mps", "good-mps-fixed-ranges.mps",
             "good-mps-some-var-bounds.mps", "good-mps-1.mps"]
+
+# The reference's MPS parser test datasets (cpp/libmps_parser/tests/mps_parser_test.cpp), copied
+# into mps/: every bad file must be rejected, the good ones read to the values in golden.json.
+MPS_PARSER_DATASETS = (
+    [f"bad-mps-{i}.mps" for i in range(1, 16) if i != 8]
+    + ["bad-mps-bound-1.mps", "bad-mps-bound-2.mps", "bad-mps-fixed-objname-after-rows.mps",
+       "bad-mps-fixed-ranges-name.mps", "bad-mps-fixed-ranges-value.mps", "good-fixed-mps-2.mps",
+       "good-mps-1-clrf.mps", "good-mps-1-comments.mps", "free-format-mps-1.mps",
+       "good-mps-fixed-empty-name.mps", "good-mps-fixed-no-name.mps",
+       "good-mps-fixed-two-objectives.mps", "good-mps-fixed-two-objectives-objname.mps",
+       "good-mps-fixed-two-objectives-objname-next-line.mps", "good-mps-fixed-var.mps",
+       "good-mps-free-var.mps", "good-mps-lower-bound-inf-var.mps",
+       "good-mps-upper-bound-inf-var.mps", "good-mps-rhs-cost.mps", "good-mps-free-ranges.mps"])
 
 GOLDEN = {
     "afiro_objective": {
@@ -63,6 +77,44 @@ GOLDEN = {
     "good_mps_1_optimal": {
         "tol": 1e-2, "status": "Optimal",
         "source": "python/cuopt/cuopt/tests/linear_programming/test_lp_solver.py:82-89"},
+    "mps_parser": {
+        "source": "cpp/libmps_parser/tests/mps_parser_test.cpp (free format, as cuOptReadProblem "
+                  "reads: cpp/src/pdlp/cuopt_c.cpp:103-107)",
+        "rejected": ["bad-mps-%d.mps" % i for i in range(1, 16) if i != 8]
+        + ["bad-mps-bound-1.mps", "bad-mps-bound-2.mps", "bad-mps-fixed-objname-after-rows.mps",
+           "bad-mps-fixed-ranges-name.mps", "bad-mps-fixed-ranges-value.mps",
+           "good-fixed-mps-2.mps"],
+        "good-1": {"files": ["good-mps-1.mps", "good-mps-1-clrf.mps", "free-format-mps-1.mps",
+                             "good-mps-fixed-empty-name.mps", "good-mps-fixed-no-name.mps",
+                             "good-mps-fixed-two-objectives.mps"],
+                   "row_offsets": [0, 2, 4], "columns": [0, 1, 0, 1],
+                   "values": [3.0, 4.0, 2.7, 10.1], "rhs": [5.4, 4.9], "c": [0.2, 0.1],
+                   "sense": "LL", "lines": "59-93, 95-129, 249-263, 201-211, 505-512"},
+        "comments": {"file": "good-mps-1-comments.mps", "row_offsets": [0, 2, 3],
+                     "columns": [0, 1, 0], "values": [3.0, 4.0, 2.7], "rhs": [5.4, 4.9],
+                     "c": [0.2, 0.1], "lines": "167-199"},
+        "objname": {"files": ["good-mps-fixed-two-objectives-objname.mps",
+                              "good-mps-fixed-two-objectives-objname-next-line.mps"],
+                    "c": [0.0, 0.0], "lines": "514-530 (objective COST6679327, no entries)"},
+        "var_bounds": {
+            "lp_model_with_var_bounds.mps": {"lower": [0.0, 1.0], "upper": [1.0, 2.0],
+                                             "c": [2.0, -1.0], "rhs": [3.0], "lines": "303-333"},
+            "free-format-mps-1.mps": {"lower": [0.0, 0.0], "upper": ["inf", "inf"],
+                                      "lines": "335-344"},
+            "good-mps-some-var-bounds.mps": {"lower": [-1.0, 0.0], "upper": ["inf", 2.0],
+                                             "lines": "346-355"},
+            "good-mps-fixed-var.mps": {"lower": [2.0, 0.0], "upper": [2.0, "inf"],
+                                       "lines": "357-366"},
+            "good-mps-free-var.mps": {"lower": ["-inf", 0.0], "upper": ["inf", "inf"],
+                                      "lines": "368-377"},
+            "good-mps-lower-bound-inf-var.mps": {"lower": ["-inf", 0.0], "upper": ["inf", "inf"],
+                                                 "lines": "379-388"},
+            "good-mps-upper-bound-inf-var.mps": {"lower": [0.0, 0.0], "upper": ["inf", "inf"],
+                                                 "lines": "396-405"}},
+        "rhs_cost_offset": {"file": "good-mps-rhs-cost.mps", "value": -5.0, "lines": "390-394"},
+        "ranges": {"files": ["good-mps-fixed-ranges.mps", "good-mps-free-ranges.mps"],
+                   "lower": [1.2, 1.5, 7.9, 3.5, 3.9, 4.9], "upper": [5.4, 4.9, 9.5, 6.9, 3.9, 4.9],
+                   "lines": "407-503"}},
     "chess_set_dual_simplex": {
         "objective": 1333.333333, "x": [0.0, 66.666667], "tol": 1e-5,
         "source": "cpp/tests/dual_simplex/unit_tests/solve.cpp:23-94"},
@@ -73,6 +125,9 @@ def main(ref_root: str = "/root/reference") -> None:
     src = Path(ref_root) / "datasets" / "linear_programming"
     for name in DATASETS:
         shutil.copyfile(src / name, HERE / name)
+    (HERE / "mps").mkdir(exist_ok=True)
+    for name in MPS_PARSER_DATASETS:
+        shutil.copyfile(src / name, HERE / "mps" / name)
     (HERE / "golden.json").write_text(json.dumps(GOLDEN, indent=2) + "\n")
     print("wrote", len(DATASETS), "datasets and golden.json to", HERE)
 
