@@ -19,7 +19,8 @@
 //     RANGES records always name a set (:1192-1193); a BOUNDS record leaves the set name out
 //     when its second field is a column, and may define a column (:1136-1167);
 //   * OBJSENSE takes MIN / MINIMIZE / MAX / MAXIMIZE only (:257-270);
-//   * an objective row and the ROWS, COLUMNS and RHS sections are required (:772-780).
+//   * an objective row and the ROWS, COLUMNS and RHS sections are required (:772-780);
+//   * integer columns without any bound get [0, 1] (:801-806).
 // Compressed files are not supported.
 #include <cuopt/linear_programming/constants.h>
 
@@ -282,6 +283,12 @@ int read_mps(const std::string& path, lp_problem& out, std::string& err)
   if (!seen_rows) return fail("ROWS section missing");
   if (!seen_columns) return fail("COLUMNS section missing");
   if (!seen_rhs) return fail("RHS section missing");
+  // Integer columns without any bound are binary (reference mps_parser.cpp:801-806).
+  for (int j = 0; j < (int)col_names.size(); ++j)
+    if (vtype[j] == 'I' && !bounded.count(j)) {
+      lo[j] = 0.0;
+      up[j] = 1.0;
+    }
   const int m = (int)row_names.size(), n = (int)col_names.size();
   if (rhs.empty()) rhs.assign(m, 0.0);
   out.m          = m;

@@ -31,6 +31,9 @@ MPS_PARSER_DATASETS = (
        "good-mps-free-var.mps", "good-mps-lower-bound-inf-var.mps",
        "good-mps-upper-bound-inf-var.mps", "good-mps-rhs-cost.mps", "good-mps-free-ranges.mps"])
 
+MPS_PARSER_MIP_DATASETS = ["good-mip-mps-1.mps", "good-mip-mps-1-no-mark.mps",
+                           "good-mip-mps-no-bounds.mps", "good-mip-mps-partial-bounds.mps"]
+
 GOLDEN = {
     "afiro_objective": {
         "value": -464.7531, "rel_tol": 0.01,
@@ -112,6 +115,18 @@ GOLDEN = {
             "good-mps-upper-bound-inf-var.mps": {"lower": [0.0, 0.0], "upper": ["inf", "inf"],
                                                  "lines": "396-405"}},
         "rhs_cost_offset": {"file": "good-mps-rhs-cost.mps", "value": -5.0, "lines": "390-394"},
+        "mip": {
+            "good-mip-mps-1.mps": {"types": "II", "lower": [0.0, 0.0], "upper": [10.0, 10.0],
+                                   "lines": "567-617"},
+            "good-mip-mps-1-no-mark.mps": {"types": "II", "lower": [0.0, 0.0],
+                                           "upper": [10.0, 10.0], "lines": "619-656"},
+            "good-mip-mps-no-bounds.mps": {"types": "IC", "lower": [0.0, 0.0],
+                                           "upper": [1.0, "inf"], "lines": "658-702"},
+            "good-mip-mps-partial-bounds.mps": {"types": "IC", "lower": [0.0, 0.0],
+                                                "upper": [1.0, 10.0], "lines": "704-748"},
+            "row_offsets": [0, 2, 4], "columns": [0, 1, 0, 1],
+            "values": [8000.0, 4000.0, 15.0, 30.0], "rhs": [40000.0, 200.0], "c": [100.0, 150.0],
+            "maximize": True},
         "ranges": {"files": ["good-mps-fixed-ranges.mps", "good-mps-free-ranges.mps"],
                    "lower": [1.2, 1.5, 7.9, 3.5, 3.9, 4.9], "upper": [5.4, 4.9, 9.5, 6.9, 3.9, 4.9],
                    "lines": "407-503"}},
@@ -128,6 +143,8 @@ def main(ref_root: str = "/root/reference") -> None:
     (HERE / "mps").mkdir(exist_ok=True)
     for name in MPS_PARSER_DATASETS:
         shutil.copyfile(src / name, HERE / "mps" / name)
+    for name in MPS_PARSER_MIP_DATASETS:
+        shutil.copyfile(src.parent / "mixed_integer_programming" / name, HERE / "mps" / name)
     (HERE / "golden.json").write_text(json.dumps(GOLDEN, indent=2) + "\n")
     print("wrote", len(DATASETS), "datasets and golden.json to", HERE)
 

@@ -167,3 +167,25 @@ def test_ranges_fixed_and_free(golden, golden_dir):
             lo, up = p.row_bounds()
             np.testing.assert_allclose(lo, g["lower"], rtol=0, atol=1e-12)
             np.testing.assert_allclose(up, g["upper"], rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", ["good-mip-mps-1.mps", "good-mip-mps-1-no-mark.mps",
+                                  "good-mip-mps-no-bounds.mps", "good-mip-mps-partial-bounds.mps"])
+def test_integer_markers_and_their_default_bounds(golden, golden_dir, name):
+    """mps_parser_test.cpp:567-748: columns between INTORG / INTEND markers are integer; UI bounds;
+    integer columns with no bound at all get [0, 1]; OBJSENSE MAX on its own line."""
+    g = golden["mps_parser"]["mip"]
+    want = g[name]
+    with _Problem(_path(golden_dir, name)) as p:
+        assert p.rc == 0
+        off, idx, val = p.matrix()
+        assert off.tolist() == g["row_offsets"] and idx.tolist() == g["columns"]
+        assert val.tolist() == g["values"]
+        assert p.rhs().tolist() == g["rhs"] and p.c().tolist() == g["c"]
+        assert p._int(p.L.cuOptGetObjectiveSense) == (-1 if g["maximize"] else 1)
+        types = C.create_string_buffer(2)
+        assert p.L.cuOptGetVariableTypes(p.h, types) == 0
+        assert types.raw.decode() == want["types"]
+        lo, up = p.bounds()
+        assert lo.tolist() == [_num(v) for v in want["lower"]]
+        assert up.tolist() == [_num(v) for v in want["upper"]]
