@@ -581,7 +581,15 @@ cuopt_int_t cuOptSolve(cuOptOptimizationProblem problem, cuOptSolverSettings set
   if (!sol) return CUOPT_OUT_OF_MEMORY;
   cuopt_b200::trace("cuOptSolve: enter");
   const cuopt_int_t rc = guarded([&] {
+    // user_problem_file / solution_file, as the reference's solve_lp writes them
+    // (cpp/src/pdlp/solve.cu:1282-1284, 1327-1329).
+    std::string problem_file, solution_file;
+    S(settings)->get_as_string(CUOPT_USER_PROBLEM_FILE, problem_file);
+    S(settings)->get_as_string(CUOPT_SOLUTION_FILE, solution_file);
+    if (!problem_file.empty()) cuopt_b200::write_mps(*P(problem), problem_file);
     *sol = cuopt_b200::solve_problem(*P(problem), *S(settings));
+    if (!solution_file.empty() && sol->error_code == CUOPT_SUCCESS)
+      cuopt_b200::write_sol_file(*P(problem), *sol, solution_file);
     return CUOPT_SUCCESS;
   });
   if (rc != CUOPT_SUCCESS) {

@@ -142,5 +142,10 @@ bool vertex_polish(const lp_problem& p, pdlp_result& r);
 // MPS input / output (reference cpp/libmps_parser).  read_mps returns 0 or CUOPT_MPS_* codes.
 int read_mps(const std::string& path, lp_problem& out, std::string& err);
 int write_mps(const lp_problem& p, const std::string& path);
+// The reference's .sol output of a single solve (pdlp/solver_solution.cu:428-448,
+// math_optimization/solution_writer.cu:16-40): "# Status: ..." (Optimal, Primal Feasible, or
+// Infeasible for every other status) and, when feasible, "# Objective value: ..." and one
+// "name value" line per named column.
+int write_sol_file(const lp_problem& p, lp_solution& s, const std::string& path);
 
 }  // namespace cuopt_b200

@@ -344,6 +344,26 @@ int read_mps(const std::string& path, lp_problem& out, std::string& err)
   return CUOPT_SUCCESS;
 }
 
+int write_sol_file(const lp_problem& p, lp_solution& s, const std::string& path)
+{
+  std::ofstream f(path);
+  if (!f.is_open()) return CUOPT_INVALID_ARGUMENT;
+  const int st        = s.r.status;
+  const bool feasible = st == CUOPT_TERIMINATION_STATUS_OPTIMAL ||
+                        st == CUOPT_TERIMINATION_STATUS_PRIMAL_FEASIBLE;
+  f.precision(std::numeric_limits<double>::max_digits10 + 1);
+  f << "# Status: "
+    << (st == CUOPT_TERIMINATION_STATUS_OPTIMAL ? "Optimal"
+                                                : (feasible ? "Primal Feasible" : "Infeasible"))
+    << "\n";
+  if (!feasible) return CUOPT_SUCCESS;
+  f << "# Objective value: " << s.r.primal_obj << "\n";
+  ensure_host(s.r);
+  for (size_t j = 0; j < p.col_names.size() && j < s.r.x.size(); ++j)
+    f << p.col_names[j] << " " << s.r.x[j] << "\n";
+  return f.good() ? CUOPT_SUCCESS : CUOPT_INVALID_ARGUMENT;
+}
+
 int write_mps(const lp_problem& p, const std::string& path)
 {
   std::FILE* f = std::fopen(path.c_str(), "w");

@@ -189,3 +189,42 @@ def test_integer_markers_and_their_default_bounds(golden, golden_dir, name):
         lo, up = p.bounds()
         assert lo.tolist() == [_num(v) for v in want["lower"]]
         assert up.tolist() == [_num(v) for v in want["upper"]]
+
+
+def test_user_problem_file_is_written_before_the_solve(golden_dir, tmp_path):
+    """solve.cu:1282-1284: with user_problem_file set, the solve first writes the problem as MPS
+    (here the solve itself needs a GPU; the file is written before it starts)."""
+    from cuopt_b200 import linear_programming as lpm
+    out = tmp_path / "afiro_out.mps"
+    s = lpm.SolverSettings()
+    s.set_parameter("user_problem_file", str(out))
+    lpm.Solve(lpm.ReadMps(golden_dir / "afiro_original.mps"), s)
+    a, b = lpm.ReadMps(golden_dir / "afiro_original.mps"), lpm.ReadMps(out)
+    for k in ("A_offsets", "A_indices", "A_values", "c", "constraint_lower_bounds",
+              "constraint_upper_bounds", "variable_lower_bounds", "variable_upper_bounds"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+
+
+def test_solution_file(golden_dir, tmp_path):
+    """solver_solution.cu:428-448, solution_writer.cu:16-40: the status line, the objective and one
+    'name value' line per column (the no-constraints LP, solved in closed form on the host)."""
+    from cuopt_b200 import linear_programming as lpm
+    out = tmp_path / "x.sol"
+    s = lpm.SolverSettings()
+    s.set_parameter(lpm.CUOPT_METHOD, int(lpm.SolverMethod.Concurrent))
+    s.set_parameter("solution_file", str(out))
+    with _Problem(golden_dir / "lp-model-no-constraints.mps") as p:  # keeps the column names
+        assert p.rc == 0
+        sh, sol = s._create(), C.c_void_p()
+        try:
+            assert p.L.cuOptSolve(p.h, sh, C.byref(sol)) == 0
+            st = C.c_int32()
+            p.L.cuOptGetTerminationStatus(sol, C.byref(st))
+            assert st.value == 1
+        finally:
+            p.L.cuOptDestroySolution(C.byref(sol))
+            p.L.cuOptDestroySolverSettings(C.byref(sh))
+    lines = out.read_text().splitlines()
+    assert lines[0] == "# Status: Optimal"
+    assert float(lines[1].split(":")[1]) == 1.0
+    assert lines[2].split()[0] == "x1" and float(lines[2].split()[1]) == 1.0
