@@ -346,3 +346,23 @@ def test_large_problem_roundtrips_through_the_getters():
         for k, v in (("clo", clo), ("cup", cup), ("vlo", vlo), ("vup", vup)):
             assert np.array_equal(got[k], v), k
         L.cuOptDestroyProblem(C.byref(h))
+
+
+def test_reference_invalid_bounds_lp_is_infeasible():
+    """c_api_test.c:1043-1175 (test_invalid_bounds, LP case): 0.2 <= x <= 0.5 as rows, variable
+    bounds [1, 0]: cuOptSolve succeeds with termination status Infeasible, before any device work."""
+    L = lib()
+    p = lambda a: C.c_void_p(a.ctypes.data)
+    off, idx, val = np.array([0, 1, 2], np.int32), np.zeros(2, np.int32), np.ones(2)
+    clo, cup = np.array([0.2, -np.inf]), np.array([np.inf, 0.5])
+    vlo, vup, c = np.array([1.0]), np.array([0.0]), np.array([2.0])
+    h, s, sol = C.c_void_p(), _settings(), C.c_void_p()
+    assert L.cuOptCreateRangedProblem(2, 1, 1, 0.0, p(c), p(off), p(idx), p(val), p(clo), p(cup),
+                                      p(vlo), p(vup), b"C", C.byref(h)) == 0
+    assert L.cuOptSolve(h, s, C.byref(sol)) == 0
+    st = C.c_int32()
+    assert L.cuOptGetTerminationStatus(sol, C.byref(st)) == 0
+    assert st.value == 2  # CUOPT_TERIMINATION_STATUS_INFEASIBLE
+    L.cuOptDestroySolution(C.byref(sol))
+    L.cuOptDestroyProblem(C.byref(h))
+    L.cuOptDestroySolverSettings(C.byref(s))
