@@ -18,15 +18,19 @@
 //   g_na_aty      A^T y accumulator, kNaMaxCols doubles (4 MiB): bounds num_variables;
 //                 must be zero before the row pass (cleared by a memset on every call);
 //   g_na_partials per-block partial sums of the two passes, written in full before they are read;
-//   g_na_bad      count of column indices outside [0, n); must be zero before the row pass
-//                 (cleared on every call).
+//   g_na_bad      count of malformed entries (column indices outside [0, n), rows whose offsets
+//                 decrease or start below 0); must be zero before the row pass (cleared on every
+//                 call).
 // Because the scratch is one static copy per device, calls that overlap in time on the same
 // device (different streams or host threads without ordering between them) race on it and give
-// wrong results; callers must order them.
+// wrong results; callers must order them.  A^T y is accumulated with double-precision atomics, so
+// the dual residual and the quantities derived from it may differ in the last bits between calls.
+// The scratch belongs to this library's device code, which the CUDA runtime loads on a device at
+// the first call that needs it (lazily, by default): that first call is when the static arrays take
+// their device memory.
 #include <math_constants.h>
 
 #include <cstdio>
-#include <mutex>
 
 #include <cuopt_b200.h>
 
@@ -41,7 +45,6 @@ constexpr int kNaMaxCols     = 1 << 19;  // 524,288 columns
 constexpr int kNaBlocks  = 592;      // 148 SMs x 4 resident blocks; fixed so partials fit
 constexpr int kNaRowRed  = 3;        // row pass: |r_p|^2, dual row term, |b|^2
 constexpr int kNaColRed  = 4;        // column pass: |r_d|^2, c.x, rc.x, |c|^2
-constexpr int kNaMaxDevices = 64;
 
 static __device__ __align__(256) double g_na_aty[kNaMaxCols];
 static __device__ __align__(256) double g_na_partials[kNaBlocks * (kNaRowRed + kNaColRed)];
@@ -88,6 +91,10 @@ __global__ void __launch_bounds__(kBlock)
   const int nw   = gridDim.x * kWarpsPerBlock;
   for (int i = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); i < m; i += nw) {
     const int b = off[i], e = off[i + 1];
+    if (b < 0 || e < b) {  // malformed offsets: counted, the row is skipped
+      if (lane == 0) atomicAdd(s.bad, 1u);
+      continue;
+    }
     const double yi = y[i];
     double ax       = 0.0;
     for (int k = b + lane; k < e; k += kWarp) {
@@ -167,23 +174,17 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-// Device addresses of the static scratch, looked up once per device (with that device current).
+// Device addresses of the static scratch on the current device.  Looked up on every call (a host
+// query that allocates nothing), so that a device reset or a new primary context, after which the
+// module is loaded again at new addresses, never leaves a stale address behind.
 bool scratch_for_current_device(na_scratch& out, int& dev)
 {
-  static std::mutex mu;
-  static bool ready[kNaMaxDevices] = {};
-  static na_scratch table[kNaMaxDevices];
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices) return false;
-  std::lock_guard<std::mutex> lock(mu);
-  if (!ready[dev]) {
-    na_scratch s{};
-    if (cudaGetSymbolAddress((void**)&s.aty, g_na_aty) != cudaSuccess) return false;
-    if (cudaGetSymbolAddress((void**)&s.partials, g_na_partials) != cudaSuccess) return false;
-    if (cudaGetSymbolAddress((void**)&s.bad, g_na_bad) != cudaSuccess) return false;
-    table[dev] = s;
-    ready[dev] = true;
-  }
-  out = table[dev];
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  na_scratch s{};
+  if (cudaGetSymbolAddress((void**)&s.aty, g_na_aty) != cudaSuccess) return false;
+  if (cudaGetSymbolAddress((void**)&s.partials, g_na_partials) != cudaSuccess) return false;
+  if (cudaGetSymbolAddress((void**)&s.bad, g_na_bad) != cudaSuccess) return false;
+  out = s;
   return true;
 }
 

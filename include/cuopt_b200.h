@@ -164,14 +164,21 @@ cuopt_int_t cuOptSolutionAdjoint(cuOptOptimizationProblem problem,
  * (d_primal n, d_dual m, d_reduced_cost n, signs as cuOptSolveDevice returns them), writes to the
  * device array d_out (9 doubles), in stream order: l2 primal residual, l2 dual residual, primal
  * objective, dual objective, gap, relative primal residual, relative dual residual, relative gap
- * (the quantities of cuOptPDLPStatistics), and the count of column indices outside [0, n) (when it
- * is non-zero the eight values are NaN).  For callers that cannot allocate: a memory pool that is
- * already fully reserved, or a loop that must not pay cudaMalloc's implicit synchronisation.
- * Scratch is a fixed static device array: num_variables may be at most 524288 (larger sizes
- * return CUOPT_INVALID_ARGUMENT with a message on stderr); constraints and non-zeros are not
- * bounded.  The first call on a device looks up the scratch addresses (setup), so make it before
- * any stream capture.  Calls that overlap in time on one device share the scratch and race; order
- * them. */
+ * (the quantities of cuOptPDLPStatistics), and the count of malformed entries found (column
+ * indices outside [0, n), rows whose offsets decrease or start below 0; when it is non-zero the
+ * eight values are NaN).  d_row_offsets must start at 0 and end at the length of d_column_indices
+ * and d_values: offsets past the arrays' end cannot be detected and are read as given.
+ * For callers that cannot allocate: a memory pool that is already fully reserved, or a loop that
+ * must not pay cudaMalloc's implicit synchronisation.
+ * Scratch is a fixed static device array (about 4 MiB) held by every device that loads this
+ * library until the process exits: num_variables may be at most 524288 (larger sizes return
+ * CUOPT_INVALID_ARGUMENT with a message on stderr); constraints and non-zeros are not bounded.
+ * The CUDA runtime loads the library's device code on a device at the first call that needs it,
+ * so the first call on a device is when the static scratch takes its device memory: make it
+ * before reserving the rest of the device's memory, and before any stream capture.  Calls that
+ * overlap in time on one device share the scratch and race; order them.  A^T y is summed with
+ * double-precision atomics, so the dual residual, the relative dual residual and the values
+ * derived from them are not bit-reproducible between calls (they agree to rounding). */
 cuopt_int_t cuOptComputeKKTErrorsNoAlloc(cuopt_int_t num_constraints,
                                          cuopt_int_t num_variables,
                                          cuopt_int_t objective_sense,

@@ -2,9 +2,11 @@
 
 It must report, for the point cuOptSolveDevice returns, the residuals, objectives and gap that
 cuOptSolveDevice itself reports in its statistics, on two calls in a row (its static scratch is
-cleared on every call).  Tolerances: residual norms and relative errors within 1e-7 relative
-(summation order and the atomic A^T y accumulation differ), objectives within 1e-10 relative, the
-gap within 1e-10 x (1 + |primal| + |dual|).
+cleared on every call); flag malformed column indices and row offsets with NaN outputs and a
+count, and clear that count on the next call; and leave the device's free memory unchanged.
+Tolerances: residual norms and relative errors within 1e-7 relative (summation order and the
+atomic A^T y accumulation differ), objectives within 1e-10 relative, the gap within
+1e-10 x (1 + |primal| + |dual|).
 
 The file name keeps it last in collection order, after the tests that use the allocating paths.
 """
@@ -65,13 +67,15 @@ def _solve(L, torch, d, lp, sense, offset, settings):
     return st, status.value
 
 
-def _no_alloc(L, torch, d, lp, sense, offset, n=None):
-    out = torch.full((9,), -1.0, device="cuda", dtype=torch.float64)
+def _no_alloc(L, torch, d, lp, sense, offset, n=None, out=None, idx=None, off=None):
+    if out is None:
+        out = torch.full((9,), -1.0, device="cuda", dtype=torch.float64)
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     rc = L.cuOptComputeKKTErrorsNoAlloc(lp.m, lp.n if n is None else n, sense, offset, _p(d["c"]),
-                                        _p(d["off"]), _p(d["idx"]), _p(d["val"]), _p(d["lo"]),
-                                        _p(d["up"]), _p(d["x"]), _p(d["y"]), _p(d["rc"]), stream,
-                                        _p(out))
+                                        _p(d["off"] if off is None else off),
+                                        _p(d["idx"] if idx is None else idx), _p(d["val"]),
+                                        _p(d["lo"]), _p(d["up"]), _p(d["x"]), _p(d["y"]),
+                                        _p(d["rc"]), stream, _p(out))
     torch.cuda.synchronize()
     return rc, out.cpu().numpy()
 
@@ -116,3 +120,70 @@ def test_no_alloc_rejects_too_many_variables():
     rc, out = _no_alloc(L, torch, d, lp, 1, 0.0, n=MAX_COLS + 1)
     assert rc == 1  # CUOPT_INVALID_ARGUMENT, before any device work
     assert np.all(out == -1.0)
+
+
+def _solved_c0(L, torch):
+    lp = gen.constructed_lp(2000, 5000, 8, seed=0)
+    d = _device(lp, torch)
+    s = _settings(L, 1e-6)
+    try:
+        st, status = _solve(L, torch, d, lp, 1, 0.0, s)
+    finally:
+        L.cuOptDestroySolverSettings(C.byref(s))
+    assert status == 1
+    return lp, d, st
+
+
+def test_no_alloc_flags_bad_column_then_clears():
+    """A column index equal to n is counted and skipped (NaN outputs); the next call with the
+    original indices starts from a cleared count and gives the solver's statistics again."""
+    torch = pytest.importorskip("torch")
+    L = lib()
+    lp, d, st = _solved_c0(L, torch)
+    bad_idx = d["idx"].clone()
+    bad_idx[123] = lp.n
+    rc, out = _no_alloc(L, torch, d, lp, 1, 0.0, idx=bad_idx)
+    assert rc == 0
+    assert out[8] == 1.0
+    assert np.all(np.isnan(out[:8]))
+    rc, out = _no_alloc(L, torch, d, lp, 1, 0.0)
+    assert rc == 0
+    _check(st, out)
+
+
+def test_no_alloc_flags_decreasing_row_offsets():
+    """Row 5 given an end offset below its start is counted and skipped; every access stays inside
+    the arrays (the neighbouring rows only grow or shrink within them)."""
+    torch = pytest.importorskip("torch")
+    L = lib()
+    lp, d, st = _solved_c0(L, torch)
+    off = d["off"].clone()
+    assert int(off[5]) > 0
+    off[6] = off[5] - 1
+    rc, out = _no_alloc(L, torch, d, lp, 1, 0.0, off=off)
+    assert rc == 0
+    assert out[8] == 1.0
+    assert np.all(np.isnan(out[:8]))
+    rc, out = _no_alloc(L, torch, d, lp, 1, 0.0)
+    assert rc == 0
+    _check(st, out)
+
+
+def test_no_alloc_leaves_free_memory_unchanged():
+    """After a first call (which loads the library's device code and its static scratch), further
+    calls take no device memory: the device's free bytes are the same before and after them."""
+    torch = pytest.importorskip("torch")
+    L = lib()
+    lp, d, st = _solved_c0(L, torch)
+    out = torch.full((9,), -1.0, device="cuda", dtype=torch.float64)
+    rc, _ = _no_alloc(L, torch, d, lp, 1, 0.0, out=out)
+    assert rc == 0
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        rc, res = _no_alloc(L, torch, d, lp, 1, 0.0, out=out)
+        assert rc == 0
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+    _check(st, res)
