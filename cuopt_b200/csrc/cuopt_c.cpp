@@ -746,6 +746,8 @@ cuopt_int_t cuOptSolveDevice(cuopt_int_t m, cuopt_int_t n, cuopt_int_t sense, cu
     in.var_up     = d_vup;
     in.obj_offset = offset;
     in.maximize   = sense == CUOPT_MAXIMIZE;
+    const std::string mode_err = cuopt_b200::solver_mode_error(*S(settings));
+    if (!mode_err.empty()) throw std::invalid_argument(mode_err);
     cuopt_b200::pdlp_params prm = cuopt_b200::params_from_settings(*S(settings));
     prm.log_to_console          = false;
     sol.r = cuopt_b200::pdlp_solve_device(in, prm, static_cast<cudaStream_t>(stream), d_x, d_y, d_rc);

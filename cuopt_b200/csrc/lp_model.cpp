@@ -383,6 +383,18 @@ lp_solution solve_without_constraints(const lp_problem& p)
 
 }  // namespace
 
+std::string solver_mode_error(const lp_settings& st)
+{
+  // Only Stable3, the reference's default mode (solve.cu:167-209), is built; the others need the
+  // adaptive step size (adaptive_step_size_strategy.cu:168-270) and the KKT / trust-region
+  // restarts, which are not.  Asking for them is an error rather than a silent substitution.
+  const int mode = st.i(CUOPT_PDLP_SOLVER_MODE);
+  if (mode == CUOPT_PDLP_SOLVER_MODE_STABLE3) return {};
+  static const char* names[] = {"Stable1", "Stable2", "Methodical1", "Fast1"};
+  return std::string("pdlp_solver_mode ") + (mode >= 0 && mode < 4 ? names[mode] : "?") +
+         " is not available in this library (only Stable3, the default, is built)";
+}
+
 pdlp_params params_from_settings(const lp_settings& st)
 {
   pdlp_params prm;
@@ -431,6 +443,7 @@ static bool prepare_for_pdlp(const lp_problem& p, const lp_settings& st, row_bou
     return false;
   }
   std::string err = validate_problem(p);
+  if (err.empty()) err = solver_mode_error(st);
   if (!err.empty()) {
     out.error_code    = CUOPT_VALIDATION_ERROR;
     out.error_message = err;

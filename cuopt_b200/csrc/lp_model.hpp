@@ -95,6 +95,8 @@ std::string validate_problem(const lp_problem& p);
 
 // Solver parameters from the settings registry.
 pdlp_params params_from_settings(const lp_settings& s);
+// Non-empty (a validation message) when the settings ask for a PDLP mode that is not built.
+std::string solver_mode_error(const lp_settings& s);
 
 // Full solve as done by cuOptSolve: validation, trivial cases, PDLP.
 lp_solution solve_problem(const lp_problem& p, const lp_settings& s);

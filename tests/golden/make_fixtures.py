@@ -1,5 +1,6 @@
 """Regenerates the golden fixtures in this folder from the reference project (run where the
-reference tree is available; the fixtures are committed so tests never read the reference).
+reference tree is available, with its root as the one argument; the fixtures are committed so
+tests never read the reference).
 
 Fixtures:
   *.mps           copies of the reference's small LP datasets (datasets/linear_programming/)
@@ -136,7 +137,8 @@ GOLDEN = {
 }
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str) -> None:
+    """ref_root: the root of the reference project's source tree (holds datasets/)."""
     src = Path(ref_root) / "datasets" / "linear_programming"
     for name in DATASETS:
         shutil.copyfile(src / name, HERE / name)
@@ -150,4 +152,6 @@ def main(ref_root: str = "/root/reference") -> None:
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_fixtures.py <reference project root>")
+    main(sys.argv[1])

@@ -46,3 +46,19 @@ def test_batch_solve_with_warm_start_data_raises():
         lpm.BatchSolve([chess_set_lp(), chess_set_lp()], s)
     with pytest.raises(lpm.CuOptError):
         lpm.SolveClimbers(chess_set_lp(), [0], [0.0], [1.0], s)
+
+
+@pytest.mark.parametrize("mode,name", [(0, "Stable1"), (1, "Stable2"), (2, "Methodical1"),
+                                       (3, "Fast1")])
+def test_unbuilt_solver_modes_are_rejected(mode, name):
+    """Only Stable3 is built: a solve or a batch that asks for another mode ends with a validation
+    error naming the mode (before any device work), instead of being solved as Stable3."""
+    s = lpm.SolverSettings()
+    s.set_parameter(lpm.CUOPT_PDLP_SOLVER_MODE, mode)
+    s.set_parameter(lpm.CUOPT_LOG_TO_CONSOLE, False)
+    sol = lpm.Solve(chess_set_lp(), s)
+    assert sol.get_error_status() == lpm.ErrorStatus.ValidationError
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.NoTermination
+    assert name in sol.get_error_message()
+    sols, _ = lpm.BatchSolve([chess_set_lp(), chess_set_lp()], s)
+    assert all(x.get_error_status() == lpm.ErrorStatus.ValidationError for x in sols)
