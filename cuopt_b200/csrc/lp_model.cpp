@@ -687,11 +687,14 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
     o.r.y.assign(hy.begin() + bi.row_start[b], hy.begin() + bi.row_start[b + 1]);
   }
   // Instances whose FP32 iterates stalled continue, together, in FP64 from where they stopped:
-  // their solutions, step sizes and primal weights start an FP64 batch.
+  // their solutions, step sizes and primal weights start an FP64 batch.  With refinement asked
+  // for (pdlp_refinement_passes > 0), the Optimal instances of a mixed batch continue with them,
+  // and all of them to the refinement tolerance, as a single solve's FP64 continuation does.
+  const bool refine = prm.precision == 1 && prm.refinement_passes > 0;
   std::vector<size_t> stalled;
   std::vector<batch_warm> restart;
   for (int b = 0; b < bi.count; ++b)
-    if (rs[b].status == kStalled) {
+    if (rs[b].status == kStalled || (refine && rs[b].status == kOptimal)) {
       const lp_solution& o = out[ids[b]];
       batch_warm w;
       w.x.assign(o.r.x.begin(), o.r.x.end());
@@ -706,12 +709,18 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
   if (!stalled.empty()) {
     pdlp_params q = prm;
     q.precision   = 0;
+    if (refine) {
+      q.abs_primal = q.rel_primal = prm.refinement_tol;
+      q.abs_dual = q.rel_dual = prm.refinement_tol;
+      q.abs_gap = q.rel_gap = prm.refinement_tol;
+    }
     q.time_limit  = std::max(
       0.0, prm.time_limit -
              std::chrono::duration<double>(std::chrono::steady_clock::now() - t_chunk).count());
     std::vector<int64_t> mixed_iters;
     for (int b = 0; b < bi.count; ++b)
-      if (rs[b].status == kStalled) mixed_iters.push_back(rs[b].iterations);
+      if (rs[b].status == kStalled || (refine && rs[b].status == kOptimal))
+        mixed_iters.push_back(rs[b].iterations);
     solve_batch_chunk(ps, stalled, rb, q, false, out, &restart);
     for (size_t i = 0; i < stalled.size(); ++i) {
       out[stalled[i]].r.refinement_passes = 1;

@@ -18,6 +18,8 @@
          by one with cuOptSolve.  With --strong-branching: cuOptBatchPDLPStrongBranching on
          count / 2 fractional variables (a solve of the LP, then `count` warm-started branches),
          against the same branches solved one by one from the LP's solution.
+`gather`  measures the random-gather ceiling (cuOptProfileGatherRate) for the config's two gathered
+         vectors (y in the primal sweep, x_bar in the dual sweep) in FP32 and FP64.
 Prints one JSON line with the timings.
 """
 from __future__ import annotations
@@ -53,7 +55,8 @@ def main() -> None:
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c1_small")
-    ap.add_argument("--mode", choices=["solve", "sweeps", "batch", "adjoint", "climbers"], default="sweeps")
+    ap.add_argument("--mode", choices=["solve", "sweeps", "batch", "adjoint", "climbers", "gather"],
+                    default="sweeps")
     ap.add_argument("--fd-instances", type=int, default=2,
                     help="adjoint mode: instances checked by finite differences")
     ap.add_argument("--fd-coords", type=int, default=32,
@@ -84,6 +87,9 @@ def main() -> None:
         return
     if a.mode == "climbers":
         print(json.dumps(run_climbers(a)))
+        return
+    if a.mode == "gather":
+        print(json.dumps(run_gather(a)))
         return
     m, n, k, seed = CONFIGS[a.config]
     lp = (gen.constructed_lp(m, n, k, seed=seed) if k
@@ -141,6 +147,36 @@ def main() -> None:
     print(json.dumps(out))
 
 
+def gather_rates(m: int, n: int, nnz: int, stream) -> dict:
+    """Best random-gather rates (gathers/s) for vectors of m and n elements, 4 and 8 bytes."""
+    from cuopt_b200._lib import lib
+
+    L = lib()
+    out = {}
+    for name, length in (("primal_gather_y", m), ("dual_gather_xbar", n)):
+        for eb in (4, 8):
+            rate, chunks = C.c_double(), C.c_int32()
+            code = L.cuOptProfileGatherRate(length, 4 * nnz, eb, stream, C.byref(rate),
+                                            C.byref(chunks))
+            if code != 0:
+                raise RuntimeError(f"cuOptProfileGatherRate returned {code}")
+            out[f"{name}_fp{8 * eb}"] = {"gathers_per_s": rate.value, "chunks_in_flight": chunks.value}
+    return out
+
+
+def run_gather(a) -> dict:
+    import torch
+
+    m, n, k, _ = CONFIGS[a.config]
+    nnz = n * k if k else 75_000_000
+    stream = C.c_void_p(torch.cuda.current_stream(torch.device("cuda", 0)).cuda_stream)
+    res = gather_rates(m, n, nnz, stream)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    for v in res.values():
+        v["per_sm_per_cycle_at_1965mhz"] = v["gathers_per_s"] / sms / 1.965e9
+    return {"config": a.config, "m": m, "n": n, "gathers": 4 * nnz, "sms": sms, "rates": res}
+
+
 def run_batch(a) -> dict:
     """The 512-LP batch: one batched solve of `count` uneven LPs vs the same LPs one at a time."""
     import numpy as np
@@ -165,6 +201,8 @@ def run_batch(a) -> dict:
     st.set_parameter(lpm.CUOPT_LOG_TO_CONSOLE, False)
     precision = getattr(a, "batch_precision", "fp64")
     st.set_parameter(lpm.CUOPT_PDLP_PRECISION, 1 if precision == "mixed" else 0)
+    if a.refine:
+        st.set_parameter(lpm.CUOPT_PDLP_REFINEMENT_PASSES, a.refine)
     if a.time_limit > 0:
         st.set_parameter(lpm.CUOPT_TIME_LIMIT, a.time_limit)
     times = []
@@ -176,7 +214,12 @@ def run_batch(a) -> dict:
     iters = [s.get_lp_stats()["nb_iterations"] for s in sols]
     obj_err = [abs(s.get_primal_objective() - lp.optimal_objective) / max(1.0, abs(lp.optimal_objective))
                for s, lp in zip(sols, lps)]
-    out = {"config": "c3", "precision": precision, "count": a.count,
+    kkt = [max(s.stats.get("l2_relative_primal_residual", 0.0),
+               s.stats.get("l2_relative_dual_residual", 0.0), s.stats.get("relative_gap", 0.0))
+           for s in sols]
+    worst = sorted(range(len(sols)), key=lambda i: -obj_err[i])[:8]
+    out = {"config": "c3", "precision": precision, "count": a.count, "tolerance": a.tol,
+           "refined_to": 1e-8 if (a.refine and precision == "mixed") else None,
            "m_total": int(sum(lp.m for lp in lps)),
            "n_total": int(sum(lp.n for lp in lps)), "nnz_total": int(sum(lp.nnz for lp in lps)),
            "batch_s": batch_s, "batch_times_s": times, "batch_lps_per_s": a.count / batch_s,
@@ -185,7 +228,14 @@ def run_batch(a) -> dict:
            "batch_setup_s": sols[0].stats.get("setup_time"),
            "iterations_p50_p90_p99": [float(np.percentile(iters, q)) for q in (50, 90, 99)],
            "max_power_iterations": max(s.stats.get("power_iterations", 0) for s in sols),
-           "fp64_resolved": sum(int(s.stats.get("refinement_passes", 0) > 0) for s in sols)}
+           "fp64_resolved": sum(int(s.stats.get("refinement_passes", 0) > 0) for s in sols),
+           "max_relative_kkt": max(kkt),
+           "objective_rel_error_over_1e-6": sum(int(e > 1e-6) for e in obj_err),
+           "worst_instances": [{"i": i, "m": lps[i].m, "status": status[i], "iterations": iters[i],
+                                "objective_rel_error": obj_err[i], "relative_kkt": kkt[i],
+                                "optimal_objective": lps[i].optimal_objective,
+                                "fp64_continued": int(sols[i].stats.get("refinement_passes", 0) > 0)}
+                               for i in worst]}
     if a.sequential > 0:
         pick = np.linspace(0, a.count - 1, min(a.sequential, a.count)).astype(int)
         lpm.Solve(dms[pick[0]], st)  # warm-up

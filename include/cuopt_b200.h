@@ -72,6 +72,19 @@ cuopt_int_t cuOptSolveDevice(cuopt_int_t num_constraints,
                              cuOptPDLPStatistics* stats,
                              cuopt_int_t* termination_status);
 
+/* Measurement hook (no counterpart in the reference): the random-gather ceiling of the device.
+ * Streams `gathers` random int32 indices into a vector of `vector_length` elements of
+ * `element_bytes` (4 or 8) bytes, in the sliced-ELL sweeps' chunk shape (a warp reads 32 lanes x 4
+ * indices with evict-first loads, then gathers the elements they name), with 1, 2, 4 and 8 chunks
+ * in flight per thread.  Returns the best rate in gathers per second and the chunk count that gave
+ * it.  On uniformly random sparsity this rate, not HBM bandwidth, bounds the fused sweeps. */
+cuopt_int_t cuOptProfileGatherRate(cuopt_int_t vector_length,
+                                   int64_t gathers,
+                                   cuopt_int_t element_bytes,
+                                   void* stream,
+                                   cuopt_float_t* gathers_per_second,
+                                   cuopt_int_t* chunks_in_flight);
+
 /* Measurement hook (no counterpart in the reference): prepares the device-resident LP exactly as
  * cuOptSolveDevice does, then runs `iterations` plain PDHG iterations launching the two fused
  * sweeps separately between CUDA events on `stream`.  Returns the mean device time of one primal
