@@ -10,22 +10,29 @@ iterates, FP64 termination / restart / step ratio).  The same solve in plain FP6
           solve's stream, max over ranks; the matrices (>= 200 MB each) exceed the 126 MB L2.
   e2e     the same through the reference-compatible C API with host buffers
           (cuOptCreateRangedProblem + cuOptSolve + cuOptGet* including the H2D / D2H copies).
-  roofline  the dominant fused PDHG sweep, timed per launch with CUDA events (cuOptProfilePDHGSweeps)
-            against the measured HBM copy bandwidth.
-  cpu_baseline  the oracle (FP64 restatement of the same algorithm) on the host cores: a bounded
-            number of PDHG iterations, scaled by the iterations the solve needs.
+  roofline  the dominant fused PDHG sweep, timed per launch with CUDA events
+            (cuOptProfilePDHGSweeps), against the measured HBM copy bandwidth; beside it, the
+            sweep's gathers per second against the measured random-gather ceiling
+            (cuOptProfileGatherRate), the bound of sweeps over uniformly random sparsity.
+  parity  every leg reports its relative KKT, its objective error against the optimum known by
+          construction, and its gap to the FP64 oracle (the CPU restatement of the reference's
+          algorithm: solved live for the CPU baseline, else tests/golden/oracle_results.json).
+          An objective within 1e-6 is met by the legs refined to 1e-8 relative KKT; 1e-6 KKT
+          alone does not bound it.
+  cpu_baseline  whole FP64 oracle solves of the workload on all host threads (scaling, step size,
+            termination checks, restarts; no extrapolation).
+  c0      the 2000 x 5000 LP (L2-resident, launch-bound): time to 1e-6, iterations/s and the
+          host/graph overhead per iteration beyond the two sweeps' device time.
   batch_c3  512 seeded LPs of uneven sizes (m log-uniform in [200, 20000], n = 2.5 m,
-            6-12 non-zeros per column) solved in FP64 to 1e-6 by one cuOptBatchSolve call, against
-            a sample of the same LPs solved one by one with cuOptSolve.
-  batch_c3_mixed  the same in mixed precision (batch and single solves): Lanczos step sizes, FP32
-            sweeps; an instance whose FP32 iterates stall continues in FP64.  The batch as
-            specified (FP32 bulk against plain FP64 solves one by one) is its
-            speedup_vs_sequential_fp64.
+            6-12 non-zeros per column) in one cuOptBatchSolve call, against all 512 solved one by
+            one with cuOptSolve: FP64 at 1e-6 and 1e-8, mixed precision at 1e-6 and refined in
+            FP64 to 1e-8.
   adjoint_c4  64 non-degenerate 5000 x 10000 LPs solved in one batched call with
-            crossover, L = sum w * x* back-propagated through the KKT adjoint, gradients checked
-            against the exact basis derivatives and central differences (h = 1e-6).
+            crossover, L = sum w * x* back-propagated through the matrix-free KKT adjoint,
+            gradients checked against every instance's exact derivatives and central differences
+            (h = 1e-6, 32 coordinates of each of c, b and A per instance).
 
-`--impl reference` times that CPU implementation alone (rank 0) on the same workload and metric.
+`--impl reference` times the CPU oracle alone (rank 0) on the same workload and metric.
 """
 from __future__ import annotations
 
@@ -46,16 +53,14 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "time-to-1e-6 KKT & PDHG iter/s (mixed vs FP64); batched LPs/s; SpMV GB/s"
+UNIT = "LPs/s to 1e-6 rel. KKT"
 CONFIGS = {
     # name: (m, n, nnz per column, seed)
     "c1": (1_000_000, 2_000_000, 8, 1000),
     "c0": (2_000, 5_000, 8, 0),
     "c1_small": (750_000, 1_500_000, 8, 1000),
 }
-# FP64 Stable3 iterations to 1e-6 on the 1M x 2M LP (the oracle and the GPU FP64 path follow the same
-# iterates; measured by the FP64 leg of this benchmark on a B200).  Used only to scale the CPU
-# per-iteration time of the reference arm into the LPs/s unit.
-FP64_ITERATIONS_C1 = 1700
+ORACLE_FIXTURE = ROOT / "tests" / "golden" / "oracle_results.json"
 
 
 def _peaks():
@@ -72,6 +77,14 @@ def _traffic(kernel: str, precision: str):
         return None
     d = json.loads(p.read_text())
     return d.get(f"{kernel}_{precision}")
+
+
+def _oracle_fixture():
+    return json.loads(ORACLE_FIXTURE.read_text()) if ORACLE_FIXTURE.exists() else None
+
+
+def rel_err(a: float, b: float) -> float:
+    return abs(a - b) / max(1.0, abs(b))
 
 
 class ClockSampler:
@@ -213,19 +226,30 @@ def solve_e2e(L, lp, pinned, settings):
     return status.value
 
 
-def cpu_sample(lp, target_s: float, threads: int):
-    """Seconds per PDHG iteration of the oracle on the host cores (bounded sample)."""
+def oracle_solves(lp, steps: int, warmup: int, budget_s: float, threads: int, tol: float = 1e-6):
+    """Whole FP64 oracle solves of `lp` to `tol` (scaling, step size, termination checks,
+    restarts) on `threads` host threads.  Warm-up: `warmup` bounded runs of 20 iterations.  Timed:
+    up to `steps` solves, stopping early once the next one would end past `budget_s` (the first
+    always runs).  Returns (seconds per solve, solves timed, last result dict)."""
     from oracle import oracle as O
-    t2 = O.pdhg_seconds(lp, 2, threads)
-    iters = int(max(3, min(200, target_s / max(t2 / 2, 1e-6))))
-    t = O.pdhg_seconds(lp, iters, threads)
-    return t / iters, iters
+    for _ in range(warmup):
+        O.solve(lp, tol=tol, iteration_limit=20, threads=threads)
+    times, res = [], None
+    t_all = time.perf_counter()
+    for _ in range(max(1, steps)):
+        t0 = time.perf_counter()
+        res, _, _, _ = O.solve(lp, tol=tol, threads=threads)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_all + times[-1] > budget_s:
+            break
+    return float(np.mean(times)), len(times), res
 
 
 def bench_config(args, lp, world):
-    """The workload both arms report (the reference arm times the same one on the host)."""
+    """The workload both arms report (the reference arm times the same one on the host); the
+    arithmetic each arm uses is in its own `dtype` / `precision` keys."""
     return {"workload": f"{args.config}: {lp.m}x{lp.n} LP, {lp.nnz} nnz, Stable3 PDLP to 1e-6 "
-                        "relative KKT, mixed precision", "replicas": world,
+                        "relative KKT", "replicas": world,
             "l2": "inputs larger than L2 (matrix 16M nnz, >= 190 MB per copy)",
             "parallelism": f"replicas x{world}"}
 
@@ -237,27 +261,24 @@ def run_reference(args):
     from oracle import oracle as O
     lp = make_lp(args.config)
     threads = O.max_threads()
-    iters_needed = args.cpu_iterations or FP64_ITERATIONS_C1 or 10000
-    samples = []
-    for i in range(args.warmup + args.steps):
-        s_per_iter, n = cpu_sample(lp, args.cpu_seconds / max(1, args.warmup + args.steps), threads)
-        if i >= args.warmup:
-            samples.append(s_per_iter)
-    s_iter = float(np.mean(samples))
-    value = 1.0 / (s_iter * iters_needed)
+    s, timed, res = oracle_solves(lp, args.steps, args.warmup, args.reference_seconds, threads)
+    value = 1.0 / s
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "LPs/s to 1e-6 rel. KKT",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * s_iter * iters_needed, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": timed, "steps_requested": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * s, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "precision": "fp64",
+        "data": "synthetic (seeded generator, optimum known by construction)",
         "config": bench_config(args, lp, 1),
-        "cpu_baseline": {"value": value, "unit": "LPs/s to 1e-6 rel. KKT", "cores": threads,
-                         "kind": "port",
-                         "sample": f"oracle FP64 PDHG, {n} iterations per step on {threads} threads, "
-                                   f"{s_iter * 1e3:.1f} ms/iteration x {iters_needed} iterations"},
-        "e2e": {"value": value, "unit": "LPs/s to 1e-6 rel. KKT", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
-        "pdhg_iter_per_s": 1.0 / s_iter,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{timed} whole FP64 oracle solve(s) of the workload to 1e-6 "
+                                   f"relative KKT on {threads} threads ({s:.2f} s each; warm-up: "
+                                   f"{args.warmup} runs of 20 iterations); steps past a "
+                                   f"{args.reference_seconds:.0f} s budget are not run"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "status": res["status"], "iterations": res["iterations"],
+        "pdhg_iter_per_s": res["iterations"] / s,
+        "objective_rel_error": rel_err(res["primal_obj"], lp.optimal_objective),
     }
     print(json.dumps(line), flush=True)
 
@@ -295,6 +316,81 @@ class Replicas:
             self._dist.destroy_process_group()
 
 
+def parity(lp, st, oracle=None):
+    """Per-result correctness record: relative KKT (reported by the solver), objective error
+    against the constructed optimum, and (when the oracle's result at the same tolerance is given)
+    the gap to the FP64 oracle's objective, status and iteration count."""
+    out = {"status": st[0], "iterations": st[1]["number_of_steps_taken"],
+           "relative_kkt": max(st[1]["l2_relative_primal_residual"],
+                               st[1]["l2_relative_dual_residual"], st[1]["relative_gap"]),
+           "objective_rel_error": rel_err(st[1]["primal_objective"], lp.optimal_objective)}
+    if oracle is not None:
+        out["objective_rel_error_vs_oracle"] = rel_err(st[1]["primal_objective"],
+                                                       oracle["primal_objective"])
+        out["oracle_status"] = oracle["status"]
+        out["oracle_iterations"] = oracle["iterations"]
+    return out
+
+
+def batch_parity(res: dict, lps, oracle_batch, tol_key: str) -> dict:
+    """Summary of a batch's per-instance results against the oracle fixture at its tolerance."""
+    inst = res.pop("instances")
+    out = {"instances": len(lps)}
+    if oracle_batch is None:
+        return out
+    want = [o[tol_key] for o in oracle_batch]
+    out["status_equal_oracle"] = sum(int(a == w["status"]) for a, w in zip(inst["status"], want))
+    out["iterations_equal_oracle"] = sum(int(a == w["iterations"])
+                                         for a, w in zip(inst["iterations"], want))
+    out["max_objective_rel_error_vs_oracle"] = max(
+        rel_err(a, w["primal_objective"]) for a, w in zip(inst["primal_objective"], want))
+    return out
+
+
+def run_c0(L, torch, device, sptr, args, O=None):
+    """The 2000 x 5000 LP: time to 1e-6 (FP64 and mixed) from device-resident inputs, iterations
+    per second, and the per-iteration overhead beyond the sweeps' device time."""
+    lp = make_lp("c0")
+    dlp = DeviceLP(lp, torch, device)
+    stream = torch.cuda.current_stream(device)
+    ref = None
+    out = {"config": "c0", "m": lp.m, "n": lp.n, "nnz": lp.nnz}
+    if O is not None:
+        r, _, _, _ = O.solve(lp, tol=1e-6)
+        ref = {"status": r["status"], "iterations": r["iterations"], "primal_objective": r["primal_obj"]}
+    for prec, name in ((0, "fp64"), (1, "mixed")):
+        sh = settings_handle(L, 1e-6, prec)
+        for _ in range(3):
+            solve_device(L, dlp, sh, sptr)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sts = [solve_device(L, dlp, sh, sptr) for _ in range(args.c0_steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.c0_steps
+        a, b, ba, bb = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        assert L.cuOptProfilePDHGSweeps(lp.m, lp.n, *dlp.ptrs(), sh, C.c_void_p(sptr), 200,
+                                        C.byref(a), C.byref(b), C.byref(ba), C.byref(bb)) == 0
+        L.cuOptDestroySolverSettings(C.byref(sh))
+        st = sts[-1][1]
+        it = st["number_of_steps_taken"]
+        us_iter = 1e6 * st["loop_time"] / max(it, 1)
+        out[name] = {"ms_per_solve": ms, "lps_per_s": 1000.0 / ms,
+                     "pdhg_iter_per_s": it / (st["loop_time"] or 1e-9),
+                     "setup_ms": 1e3 * st["setup_time"],
+                     "us_per_iteration": us_iter,
+                     "sweeps_us_per_iteration": 1e3 * (a.value + b.value),
+                     "overhead_us_per_iteration": us_iter - 1e3 * (a.value + b.value),
+                     **parity(lp, sts[-1], ref if name == "fp64" else None)}
+    if O is not None:
+        s, timed, _ = oracle_solves(lp, 3, 1, 30.0, O.max_threads())
+        out["cpu_baseline"] = {"value": 1.0 / s, "unit": UNIT, "cores": O.max_threads(),
+                               "kind": "port",
+                               "sample": f"{timed} whole FP64 oracle solves ({s * 1e3:.0f} ms each)"}
+    return out
+
+
 def run_b200(args):
     import torch
 
@@ -307,7 +403,6 @@ def run_b200(args):
     barrier, max_over_ranks = replicas.barrier, replicas.max
 
     from cuopt_b200._lib import lib
-    from cuopt_b200 import generators as gen
     L = lib()
     lp = make_lp(args.config)
     dlp = DeviceLP(lp, torch, device)
@@ -316,6 +411,9 @@ def run_b200(args):
     tol = 1e-6
     s_mixed = settings_handle(L, tol, 1)
     s_fp64 = settings_handle(L, tol, 0)
+    fixture = _oracle_fixture()
+    fx_single = (fixture or {}).get("single", {}).get(args.config)
+    lone = rank == 0 and world == 1
 
     def timed(settings, steps, warmup):
         for _ in range(warmup):
@@ -327,8 +425,7 @@ def run_b200(args):
         with ClockSampler(local) as clk:
             ev0.record(stream)
             for _ in range(steps):
-                status, st = solve_device(L, dlp, settings, sptr)
-                stats.append((status, st))
+                stats.append(solve_device(L, dlp, settings, sptr))
             ev1.record(stream)
             torch.cuda.synchronize()
         barrier()
@@ -336,48 +433,42 @@ def run_b200(args):
         return max_over_ranks(ms), stats, clk.summary()
 
     ms_mixed, st_mixed, clocks = timed(s_mixed, args.steps, args.warmup)
-    status_mixed, last_mixed = st_mixed[-1]
-    kkt_mixed = gen.kkt_relative_error(lp, dlp.x.cpu().numpy(), dlp.y.cpu().numpy())
-    obj_err_mixed = abs(last_mixed["primal_objective"] - lp.optimal_objective) / abs(lp.optimal_objective)
+    last_mixed = st_mixed[-1][1]
+    fx6 = fx_single["1e-06"] if fx_single else None
+    fx8 = fx_single["1e-08"] if fx_single else None
+    mixed = parity(lp, st_mixed[-1], fx6)
+
     fp64 = None
     if not args.no_fp64:
         ms_fp64, st_fp64, _ = timed(s_fp64, max(1, args.fp64_steps), max(1, args.fp64_warmup))
-        status_fp64, last_fp64 = st_fp64[-1]
-        fp64 = {
-            "ms_per_solve": ms_fp64, "status": status_fp64,
-            "iterations": last_fp64["number_of_steps_taken"],
-            "pdhg_iter_per_s": last_fp64["number_of_steps_taken"] / (last_fp64["loop_time"] or 1e-9),
-            "setup_s": last_fp64["setup_time"],
-            "objective_rel_error": abs(last_fp64["primal_objective"] - lp.optimal_objective)
-            / abs(lp.optimal_objective),
-            "speedup_mixed_vs_fp64": ms_fp64 / ms_mixed,
-        }
+        last_fp64 = st_fp64[-1][1]
+        fp64 = {"ms_per_solve": ms_fp64,
+                "pdhg_iter_per_s": last_fp64["number_of_steps_taken"] / (last_fp64["loop_time"] or 1e-9),
+                "setup_s": last_fp64["setup_time"], "speedup_mixed_vs_fp64": ms_fp64 / ms_mixed,
+                **parity(lp, st_fp64[-1], fx6)}
 
-    # Mixed precision to 1e-6, then FP64 continuation from that solution to 1e-8 relative KKT
-    refine = None
+    # 1e-8 relative KKT: mixed precision to 1e-6 continued in FP64, and FP64 from the start.
+    refine = fp64_8 = None
     if not args.no_refine:
-        s_ref = settings_handle(L, tol, 1, refine_passes=8, refine_tol=1e-8, time_limit=20.0)
+        s_ref = settings_handle(L, tol, 1, refine_passes=1, refine_tol=1e-8, time_limit=60.0)
         ms_ref, st_ref, _ = timed(s_ref, 1, 1)
         L.cuOptDestroySolverSettings(C.byref(s_ref))
-        status_ref, last_ref = st_ref[-1]
-        kkt_ref = gen.kkt_relative_error(lp, dlp.x.cpu().numpy(), dlp.y.cpu().numpy())
-        refine = {"ms_per_solve": ms_ref, "status": status_ref,
-                  "iterations": last_ref["number_of_steps_taken"],
-                  "refinement_passes": last_ref["refinement_passes"],
-                  "rel_primal": last_ref["l2_relative_primal_residual"],
-                  "rel_dual": last_ref["l2_relative_dual_residual"],
-                  "rel_gap": last_ref["relative_gap"], "kkt_check": kkt_ref,
-                  "objective_rel_error": abs(last_ref["primal_objective"] - lp.optimal_objective)
-                  / abs(lp.optimal_objective)}
+        refine = {"ms_per_solve": ms_ref, "refinement_passes": st_ref[-1][1]["refinement_passes"],
+                  **parity(lp, st_ref[-1], fx8)}
+        s_f8 = settings_handle(L, 1e-8, 0, time_limit=60.0)
+        ms_f8, st_f8, _ = timed(s_f8, 1, 1)
+        L.cuOptDestroySolverSettings(C.byref(s_f8))
+        fp64_8 = {"ms_per_solve": ms_f8, **parity(lp, st_f8[-1], fx8)}
+        refine["speedup_vs_fp64_to_1e-8"] = ms_f8 / ms_ref
 
     # Roofline of the dominant fused sweep (mixed precision = the headline path)
     prof = {}
     for prec, name in ((1, "mixed"), (0, "fp64")):
         a, b, ba, bb = C.c_double(), C.c_double(), C.c_double(), C.c_double()
         sh = settings_handle(L, tol, prec)
-        p = dlp.ptrs()
-        rc = L.cuOptProfilePDHGSweeps(lp.m, lp.n, *p, sh, C.c_void_p(sptr), args.profile_iters,
-                                      C.byref(a), C.byref(b), C.byref(ba), C.byref(bb))
+        rc = L.cuOptProfilePDHGSweeps(lp.m, lp.n, *dlp.ptrs(), sh, C.c_void_p(sptr),
+                                      args.profile_iters, C.byref(a), C.byref(b), C.byref(ba),
+                                      C.byref(bb))
         L.cuOptDestroySolverSettings(C.byref(sh))
         assert rc == 0, rc
         prof[name] = {"primal_sweep_ms": a.value, "dual_sweep_ms": b.value,
@@ -386,10 +477,18 @@ def run_b200(args):
     pm = prof["mixed"]
     dom = "dual" if pm["dual_sweep_ms"] >= pm["primal_sweep_ms"] else "primal"
     achieved = pm[f"{dom}_sweep_bytes"] / (pm[f"{dom}_sweep_ms"] * 1e-3) / 1e9
+    from cuopt_b200.profile import gather_rates
+    rates = gather_rates(lp.m, lp.n, lp.nnz, C.c_void_p(sptr))
+    g_peak = rates["dual_gather_xbar_fp32" if dom == "dual" else "primal_gather_y_fp32"]["gathers_per_s"]
+    g_ach = lp.nnz / (pm[f"{dom}_sweep_ms"] * 1e-3)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind,
                 "kernel": f"{dom} sweep (sell_map_kernel, mixed precision)",
                 "traffic": _traffic(dom, "mixed"),
+                "gather": {"achieved": g_ach / 1e9, "peak": g_peak / 1e9, "unit": "G gathers/s",
+                           "frac": g_ach / g_peak, "peak_kind": "measured live (cuOptProfileGatherRate)",
+                           "hbm_frac_at_gather_peak": pm[f"{dom}_sweep_bytes"] / (lp.nnz / g_peak) / 1e9 / peak},
+                "gather_ceilings": rates,
                 "iteration_achieved_gbs_mixed": (pm["primal_sweep_bytes"] + pm["dual_sweep_bytes"])
                 / ((pm["primal_sweep_ms"] + pm["dual_sweep_ms"]) * 1e-3) / 1e9,
                 "iteration_achieved_gbs_fp64": (prof["fp64"]["primal_sweep_bytes"] + prof["fp64"]["dual_sweep_bytes"])
@@ -407,65 +506,90 @@ def run_b200(args):
     solve_e2e(L, lp, pinned, s_mixed)
     barrier()
     torch.cuda.synchronize()
+    e2e_steps = args.e2e_steps or args.steps
     t0 = time.perf_counter()
-    e2e_status = [solve_e2e(L, lp, pinned, s_mixed) for _ in range(args.e2e_steps)]
+    e2e_status = [solve_e2e(L, lp, pinned, s_mixed) for _ in range(e2e_steps)]
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.e2e_steps)
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / e2e_steps)
     h2d = (lp.m + 1) * 4 + lp.nnz * 12 + lp.n * 8 * 3 + lp.m * 8 * 2
     d2h = (2 * lp.n + lp.m) * 8
 
-    # CPU baseline (rank 0, N = 1 only)
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    O = None
+    if lone and not args.no_cpu:
         from oracle import oracle as O
-        threads = O.max_threads()
-        s_iter, n = cpu_sample(lp, args.cpu_seconds, threads)
-        iters = fp64["iterations"] if fp64 else last_mixed["number_of_steps_taken"]
-        cpu = {"value": 1.0 / (s_iter * iters), "unit": "LPs/s to 1e-6 rel. KKT", "cores": threads,
-               "kind": "port",
-               "sample": f"oracle FP64 PDHG iterations: {n} on {threads} threads "
-                         f"({s_iter * 1e3:.1f} ms each), scaled by the {iters} iterations of the FP64 solve",
-               "pdhg_iter_per_s": 1.0 / s_iter}
 
-    # 512 uneven FP64 LPs in one batched call vs the same LPs one by one (rank 0, N = 1),
-    # then the same in mixed precision.
+    # CPU baseline (rank 0, N = 1 only): whole FP64 oracle solves of the workload.
+    cpu = None
+    if O is not None:
+        threads = O.max_threads()
+        s, timed_n, res = oracle_solves(lp, 1, 1, args.cpu_seconds, threads)
+        cpu = {"value": 1.0 / s, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{timed_n} whole FP64 oracle solve(s) of the workload to 1e-6 relative "
+                         f"KKT on {threads} threads ({s:.2f} s each)",
+               "status": res["status"], "iterations": res["iterations"],
+               "pdhg_iter_per_s": res["iterations"] / s}
+        live = {"status": res["status"], "iterations": res["iterations"],
+                "primal_objective": res["primal_obj"]}
+        if fp64 is not None:
+            fp64["live_oracle"] = {k: parity(lp, st_fp64[-1], live)[k] for k in
+                                   ("objective_rel_error_vs_oracle", "oracle_status",
+                                    "oracle_iterations")}
+        mixed["objective_rel_error_vs_live_oracle"] = rel_err(last_mixed["primal_objective"],
+                                                              res["primal_obj"])
+
+    c0 = run_c0(L, torch, device, sptr, args, O) if lone and not args.no_c0 else None
+
+    # 512 uneven LPs in one batched call vs all of them one by one (rank 0, N = 1): FP64 at 1e-6
+    # and 1e-8, mixed precision at 1e-6 and refined in FP64 to 1e-8.
     batch = batch_mixed = None
-    if rank == 0 and world == 1 and not args.no_batch:
-        from cuopt_b200.profile import run_batch
-        batch = run_batch(argparse.Namespace(count=512, sequential=args.batch_sequential,
-                                             repeats=3, tol=1e-6, time_limit=120.0))
-        batch_mixed = run_batch(argparse.Namespace(count=512, sequential=args.batch_sequential,
-                                                   repeats=3, tol=1e-6, time_limit=120.0,
-                                                   batch_precision="mixed"))
+    if lone and not args.no_batch:
+        from cuopt_b200.profile import batch_models, run_batch
+        models = batch_models(512)
+        ob = (fixture or {}).get("batch")
+        ns = lambda **kw: argparse.Namespace(count=512, time_limit=120.0, per_instance=True, **kw)
+        batch = run_batch(ns(sequential=args.batch_sequential, repeats=3, tol=1e-6,
+                             batch_precision="fp64"), models)
+        batch["parity"] = batch_parity(batch, models[0], ob, "1e-06")
+        b8 = run_batch(ns(sequential=0, repeats=2, tol=1e-8, batch_precision="fp64"), models)
+        b8["parity"] = batch_parity(b8, models[0], ob, "1e-08")
+        batch["fp64_to_1e-8"] = b8
+        batch_mixed = run_batch(ns(sequential=args.batch_sequential, repeats=3, tol=1e-6,
+                                   batch_precision="mixed"), models)
+        batch_mixed["parity"] = batch_parity(batch_mixed, models[0], None, "1e-06")
+        br = run_batch(ns(sequential=0, repeats=2, tol=1e-6, batch_precision="mixed", refine=1),
+                       models)
+        br["parity"] = batch_parity(br, models[0], ob, "1e-08")
+        batch_mixed["refined_to_1e-8"] = br
         # The batch as specified: the FP32-bulk batch against plain FP64 solves one by one.
         if batch.get("sequential_lps_per_s"):
             batch_mixed["speedup_vs_sequential_fp64"] = (batch_mixed["batch_lps_per_s"] /
                                                          batch["sequential_lps_per_s"])
     # 64 non-degenerate 5000 x 10000 LPs, batched forward (crossover) + KKT adjoint.
     adjoint = None
-    if rank == 0 and world == 1 and not args.no_adjoint:
+    if lone and not args.no_adjoint:
         from cuopt_b200.profile import run_adjoint
-        adjoint = run_adjoint(argparse.Namespace(count=64, tol=1e-6, fd_instances=1,
-                                                 fd_coords=args.adjoint_fd_coords,
-                                                 basis_checks=2))
+        adjoint = run_adjoint(argparse.Namespace(count=64, tol=1e-6,
+                                                 fd_coords=args.adjoint_fd_coords, fd_solver=2))
 
     value = world * 1000.0 / ms_mixed
     line = {
-        "metric": METRIC, "value": value, "unit": "LPs/s to 1e-6 rel. KKT", "n_gpus": world,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 mixed",
+        "precision": "mixed (FP32 matrix and iterates, FP64 termination / restart / step ratio)",
         "data": "synthetic (seeded generator, optimum known by construction)",
         "config": bench_config(args, lp, world),
-        "status": status_mixed, "iterations": last_mixed["number_of_steps_taken"],
         "pdhg_iter_per_s": last_mixed["number_of_steps_taken"] / (last_mixed["loop_time"] or 1e-9),
         "setup_s": last_mixed["setup_time"], "loop_s": last_mixed["loop_time"],
-        "objective_rel_error": obj_err_mixed, "kkt": kkt_mixed, "fp64": fp64,
-        "mixed_refined_to_1e-8": refine, "batch_c3": batch, "batch_c3_mixed": batch_mixed,
-        "adjoint_c4": adjoint,
+        **mixed, "fp64": fp64, "mixed_refined_to_1e-8": refine, "fp64_to_1e-8": fp64_8,
+        "objective_bound": "1e-6 relative KKT does not bound the objective error by 1e-6 (the "
+                           "oracle itself is 6.8e-6 off on batch instance 284 at 1e-6); the legs "
+                           "refined to 1e-8 are the ones held to 1e-6",
+        "c0": c0, "batch_c3": batch, "batch_c3_mixed": batch_mixed, "adjoint_c4": adjoint,
         "roofline": roofline, "cpu_baseline": cpu,
-        "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "LPs/s to 1e-6 rel. KKT",
+        "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-                "status": e2e_status},
+                "steps": e2e_steps, "status": e2e_status},
         "clocks": clocks, "gpu_launches": int(sum(st["kernel_launches"] for _, st in st_mixed)),
     }
     if rank == 0:
@@ -478,25 +602,29 @@ def run_b200(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c1")
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--fp64-warmup", type=int, default=1)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="0: as many as --steps")
+    ap.add_argument("--c0-steps", type=int, default=10)
     ap.add_argument("--profile-iters", type=int, default=50)
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--cpu-iterations", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=60.0,
+                    help="GPU arm: time budget of the whole-solve CPU baseline")
+    ap.add_argument("--reference-seconds", type=float, default=120.0,
+                    help="reference arm: time budget of its timed whole solves")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-refine", action="store_true")
+    ap.add_argument("--no-c0", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
-    ap.add_argument("--adjoint-fd-coords", type=int, default=16,
+    ap.add_argument("--adjoint-fd-coords", type=int, default=32,
                     help="adjoint batch: coordinates per kind checked by central differences")
-    ap.add_argument("--batch-sequential", type=int, default=32,
-                    help="512-LP batch: instances also solved one by one (timing sample)")
+    ap.add_argument("--batch-sequential", type=int, default=512,
+                    help="512-LP batch: instances also solved one by one")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -122,6 +122,7 @@ SIGNATURES = {
     "cuOptBatchSolve": (cuopt_int_t, [C.POINTER(handle_t), cuopt_int_t, handle_t,
                                       C.POINTER(handle_t)]),
     "cuOptSolutionAdjoint": (cuopt_int_t, [handle_t, handle_t] + [C.c_void_p] * 6),
+    "cuOptSolutionAdjointBatch": (cuopt_int_t, [cuopt_int_t] + [C.c_void_p] * 8),
     "cuOptSolveClimbers": (cuopt_int_t, [handle_t, handle_t, cuopt_int_t] + [C.c_void_p] * 3 +
                            [C.POINTER(handle_t)]),
     "cuOptBatchPDLPStrongBranching": (cuopt_int_t, [handle_t, handle_t, cuopt_int_t] +

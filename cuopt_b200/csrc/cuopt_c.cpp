@@ -910,6 +910,62 @@ cuopt_int_t cuOptBatchPDLPStrongBranching(cuOptOptimizationProblem problem,
   }
 }
 
+cuopt_int_t cuOptSolutionAdjointBatch(cuopt_int_t count, const cuOptOptimizationProblem* problems,
+                                      const cuOptSolution* solutions,
+                                      const cuopt_float_t* const* dl_dx,
+                                      const cuopt_float_t* const* dl_dy,
+                                      cuopt_float_t* const* dl_dc, cuopt_float_t* const* dl_dlower,
+                                      cuopt_float_t* const* dl_dupper,
+                                      cuopt_float_t* const* dl_dvalues)
+{
+  if (count < 0 || (count > 0 && (!problems || !solutions || !dl_dx)))
+    return CUOPT_INVALID_ARGUMENT;
+  struct host_grads {
+    std::vector<double> gx, gy, dc, dlo, dup, dval;
+  };
+  std::vector<host_grads> g(count);
+  std::vector<cuopt_b200::adjoint_job> jobs;
+  try {
+    for (int i = 0; i < count; ++i) {
+      if (!problems[i] || !solutions[i] || !dl_dx[i]) return CUOPT_INVALID_ARGUMENT;
+      lp_solution* sol = R(solutions[i]);
+      if (sol->error_code != CUOPT_SUCCESS || sol->r.status != CUOPT_TERIMINATION_STATUS_OPTIMAL)
+        return CUOPT_INVALID_ARGUMENT;
+      const lp_problem& p = *P(problems[i]);
+      cuopt_b200::ensure_host(sol->r);
+      if ((int)sol->r.x.size() != p.n || (int)sol->r.y.size() != p.m) return CUOPT_INVALID_ARGUMENT;
+      host_grads& h = g[i];
+      copy_in(h.gx, dl_dx[i], p.n);
+      const bool has_gy = dl_dy && dl_dy[i];
+      if (has_gy) copy_in(h.gy, dl_dy[i], p.m);
+      h.dc.resize(dl_dc && dl_dc[i] ? p.n : 0);
+      h.dlo.resize(dl_dlower && dl_dlower[i] ? p.m : 0);
+      h.dup.resize(dl_dupper && dl_dupper[i] ? p.m : 0);
+      h.dval.resize(dl_dvalues && dl_dvalues[i] ? p.val.size() : 0);
+      jobs.push_back(cuopt_b200::adjoint_job{
+        &p, &sol->r, h.gx.data(), has_gy ? h.gy.data() : nullptr,
+        h.dc.empty() ? nullptr : h.dc.data(), h.dlo.empty() ? nullptr : h.dlo.data(),
+        h.dup.empty() ? nullptr : h.dup.data(), h.dval.empty() ? nullptr : h.dval.data()});
+    }
+    cuopt_b200::solution_adjoint_batch(jobs);
+    for (int i = 0; i < count; ++i) {
+      if (!g[i].dc.empty()) copy_out(dl_dc[i], g[i].dc);
+      if (!g[i].dlo.empty()) copy_out(dl_dlower[i], g[i].dlo);
+      if (!g[i].dup.empty()) copy_out(dl_dupper[i], g[i].dup);
+      if (!g[i].dval.empty()) copy_out(dl_dvalues[i], g[i].dval);
+    }
+  } catch (const std::bad_alloc&) {
+    return CUOPT_OUT_OF_MEMORY;
+  } catch (const std::invalid_argument& e) {
+    std::fprintf(stderr, "cuOptSolutionAdjointBatch: %s\n", e.what());
+    return CUOPT_INVALID_ARGUMENT;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "cuOptSolutionAdjointBatch: %s\n", e.what());
+    return CUOPT_RUNTIME_ERROR;
+  }
+  return CUOPT_SUCCESS;
+}
+
 cuopt_int_t cuOptSolutionAdjoint(cuOptOptimizationProblem problem, cuOptSolution solution,
                                  const cuopt_float_t* dl_dx, const cuopt_float_t* dl_dy,
                                  cuopt_float_t* dl_dc, cuopt_float_t* dl_dlower,

@@ -113,6 +113,8 @@ lp_settings::lp_settings()
     {CUOPT_PDLP_PRECISION, CUOPT_PDLP_PRECISION_FP64, CUOPT_PDLP_PRECISION_MIXED,
      CUOPT_PDLP_PRECISION_FP64},
     {CUOPT_PDLP_REFINEMENT_PASSES, 0, 64, 0},
+    {CUOPT_PDLP_TILED_SWEEPS, CUOPT_PDLP_TILED_SWEEPS_AUTO, CUOPT_PDLP_TILED_SWEEPS_ON,
+     CUOPT_PDLP_TILED_SWEEPS_AUTO},
   };
   bparams = {
     {CUOPT_INFEASIBILITY_DETECTION, false}, {CUOPT_STRICT_INFEASIBILITY, false},
@@ -409,6 +411,7 @@ pdlp_params params_from_settings(const lp_settings& st)
   prm.precision         = st.i(CUOPT_PDLP_PRECISION);
   prm.refinement_passes = st.i(CUOPT_PDLP_REFINEMENT_PASSES);
   prm.refinement_tol    = st.f(CUOPT_PDLP_REFINEMENT_TOLERANCE);
+  prm.tiled_sweeps      = st.i(CUOPT_PDLP_TILED_SWEEPS);
   prm.log_to_console    = st.b(CUOPT_LOG_TO_CONSOLE);
   prm.detect_infeasibility  = st.b(CUOPT_INFEASIBILITY_DETECTION);
   prm.per_constraint_residual = st.b(CUOPT_PER_CONSTRAINT_RESIDUAL);
@@ -553,9 +556,6 @@ lp_solution solve_problem(const lp_problem& p, const lp_settings& st)
   }
   return out;
 }
-
-// Dense active-set factorisations (crossover, adjoint) run at most this many at a time.
-constexpr int kConcurrentPolish = 4;
 
 // Starting point of one instance: its solution (user order; duals in the solver's sign
 // convention), step size and primal weight.
@@ -728,28 +728,17 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
     }
   }
   if (!crossover) return;
-  // Crossover of the Optimal instances on a few host threads: each polish runs its own stream and
-  // dense factorisation, so several overlap on the GPU.
-  std::atomic<int> next{0};
-  std::exception_ptr failure;
-  std::mutex failure_mu;
-  auto worker = [&]() {
-    for (int b; (b = next++) < bi.count;) {
-      lp_solution& o = out[ids[b]];
-      if (o.r.status != CUOPT_TERIMINATION_STATUS_OPTIMAL) continue;
-      try {
-        o.r.crossover = vertex_polish(*ps[ids[b]], o.r);
-      } catch (...) {
-        std::lock_guard<std::mutex> lock(failure_mu);
-        if (!failure) failure = std::current_exception();
-      }
-    }
-  };
-  const int nt = std::max(1, std::min(kConcurrentPolish, bi.count));
-  std::vector<std::thread> pool;
-  for (int t = 0; t < nt; ++t) pool.emplace_back(worker);
-  for (auto& th : pool) th.join();
-  if (failure) std::rethrow_exception(failure);
+  // Crossover of the Optimal instances: all their active-set solves in one launch.
+  std::vector<const lp_problem*> pp;
+  std::vector<pdlp_result*> rr;
+  for (int b = 0; b < bi.count; ++b) {
+    lp_solution& o = out[ids[b]];
+    if (o.r.status != CUOPT_TERIMINATION_STATUS_OPTIMAL) continue;
+    pp.push_back(ps[ids[b]]);
+    rr.push_back(&o.r);
+  }
+  const std::vector<bool> polished = vertex_polish_batch(pp, rr);
+  for (size_t k = 0; k < rr.size(); ++k) rr[k]->crossover = polished[k];
 }
 
 std::vector<lp_solution> solve_batch(const std::vector<const lp_problem*>& ps, const lp_settings& st)
@@ -902,8 +891,23 @@ std::vector<lp_solution> solve_climbers(const lp_problem& p, const lp_settings& 
       out[b].r.x.assign(hx.begin() + (size_t)b * n, hx.begin() + (size_t)(b + 1) * n);
       out[b].r.rc.assign(hrc.begin() + (size_t)b * n, hrc.begin() + (size_t)(b + 1) * n);
       out[b].r.y.assign(hy.begin() + (size_t)b * m, hy.begin() + (size_t)(b + 1) * m);
-      if (st.b(CUOPT_CROSSOVER) && out[b].r.status == CUOPT_TERIMINATION_STATUS_OPTIMAL)
-        out[b].r.crossover = vertex_polish(modified(b), out[b].r);
+    }
+    if (st.b(CUOPT_CROSSOVER)) {  // all the Optimal climbers' active-set solves in one launch
+      std::vector<lp_problem> mods;
+      std::vector<int> which;
+      for (int b = 0; b < count; ++b)
+        if (out[b].r.status == CUOPT_TERIMINATION_STATUS_OPTIMAL && !out[b].r.x.empty()) {
+          mods.push_back(modified(b));
+          which.push_back(b);
+        }
+      std::vector<const lp_problem*> pp;
+      std::vector<pdlp_result*> rr;
+      for (size_t k = 0; k < which.size(); ++k) {
+        pp.push_back(&mods[k]);
+        rr.push_back(&out[which[k]].r);
+      }
+      const std::vector<bool> polished = vertex_polish_batch(pp, rr);
+      for (size_t k = 0; k < which.size(); ++k) out[which[k]].r.crossover = polished[k];
     }
   } catch (const std::bad_alloc&) {
     for (auto& o : out) set_error(o, CUOPT_OUT_OF_MEMORY, "Memory allocation failed");

@@ -134,12 +134,24 @@ std::vector<lp_solution> solve_strong_branching(const lp_problem& p, const lp_se
 // in; any of dc (n), dlo / dup (m, constraint bounds) and dval (nnz, CSR order) out.
 void solution_adjoint(const lp_problem& p, const pdlp_result& sol, const double* gx,
                       const double* gy, double* dc, double* dlo, double* dup, double* dval);
+// The same for many solutions at once: every active-set solve of the batch runs in one launch.
+struct adjoint_job {
+  const lp_problem* p;
+  const pdlp_result* sol;
+  const double* gx;
+  const double* gy;
+  double *dc, *dlo, *dup, *dval;
+};
+void solution_adjoint_batch(const std::vector<adjoint_job>& jobs);
 
 // Crossover to a vertex on the solution's active set (see adjoint.cu): when the free variables
 // and the constraints held at a bound form a square, non-singular system whose solution is primal
 // and dual feasible, the solution is replaced by that exact vertex and true is returned; otherwise
 // (a degenerate optimum) the solution is left unchanged.
 bool vertex_polish(const lp_problem& p, pdlp_result& r);
+// vertex_polish of many solutions, with all their active-set solves in one launch.
+std::vector<bool> vertex_polish_batch(const std::vector<const lp_problem*>& ps,
+                                      const std::vector<pdlp_result*>& rs);
 
 // MPS input / output (reference cpp/libmps_parser).  read_mps returns 0 or CUOPT_MPS_* codes.
 int read_mps(const std::string& path, lp_problem& out, std::string& err);

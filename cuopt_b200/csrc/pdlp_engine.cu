@@ -10,6 +10,7 @@
 #include "kernels.cuh"
 #include "pdlp_engine.hpp"
 #include "pdlp_schedule.hpp"
+#include "tile_sweep.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -213,6 +214,10 @@ class engine {
     yu_.resize(m);
     scalars_.resize(1);
     reset_iterates(true);
+    if constexpr (std::is_same_v<TX, float>) {
+      if (tune_tiles()) reset_iterates(true);  // the timed sweeps moved the iterates
+      trace("engine: sweep autotuning");
+    }
   }
 
   // Takes the precision-independent state of another engine over (see continue_from).
@@ -316,12 +321,13 @@ class engine {
                                                                           : 1.0;
     best_omega_ = omega_;
     restarts_   = 0;
+    // Four elements of zero padding: the tiled sweeps copy the gathered vectors in 16-byte units.
     for (auto* b : {&x_, &xhat_, &slack_, &xbar_, &xa_, &aty_}) {
-      b->resize(n);
+      b->resize((size_t)n + 4);
       b->zero(s_);
     }
     for (auto* b : {&y_, &yhat_, &ybar_, &ya_}) {
-      b->resize(m);
+      b->resize((size_t)m + 4);
       b->zero(s_);
     }
     if (with_initial && (in_.initial_primal || in_.initial_dual)) load_initial_solution();
@@ -533,11 +539,141 @@ class engine {
     ++launches_;
   }
 
+  // Tiled forms of the plain (non-major, Halpern) sweeps: the tile kernel's partial sums, then the
+  // epilogue row pass with the same functor as the sliced-ELL sweep.
+  void launch_primal_tiled(int it_off)
+  {
+    const tile_view T = view_of(tAT_);
+    tile_sweep_kernel<<<T.row_blocks * T.groups, kTileThreads, tAT_.smem_bytes(), s_>>>(
+      T, y_.data(), tpart_.data(), terr_.data());
+    primal_epi<TX, false, true, false> e{x_.data(),   cs_.data(),   ls_.data(),   us_.data(),
+                                         xa_.data(),  xbar_.data(), x_.data(),    xhat_.data(),
+                                         slack_.data(), aty_.data(), scalars_.data(), it_off};
+    tile_epilogue_kernel<decltype(e)><<<epi_grid(in_.n), kBlock, 0, s_>>>(
+      in_.n, T.groups, tpart_.data(), e, partials_.data());
+    launches_ += 2;
+  }
+  void launch_dual_tiled(int it_off)
+  {
+    const tile_view T = view_of(tA_);
+    tile_sweep_kernel<<<T.row_blocks * T.groups, kTileThreads, tA_.smem_bytes(), s_>>>(
+      T, xbar_.data(), tpart_.data(), terr_.data());
+    dual_epi<TX, false, true, false> e{y_.data(),    lcs_.data(), ucs_.data(),     ya_.data(),
+                                       ybar_.data(), y_.data(),   yhat_.data(),    scalars_.data(),
+                                       it_off};
+    tile_epilogue_kernel<decltype(e)><<<epi_grid(in_.m), kBlock, 0, s_>>>(
+      in_.m, T.groups, tpart_.data(), e, partials_.data());
+    launches_ += 2;
+  }
+  int epi_grid(int rows) const { return std::max(1, std::min(ceil_div(rows, kBlock), vgrid_)); }
+
+  // Autotuning of the mixed-precision sweeps (pdlp_tiled_sweeps = -1): builds the tiled copies of
+  // A and A^T where they apply, times each plain sweep both ways (one warm-up and three timed
+  // launches each, CUDA events on the solve's stream) and keeps the faster form per sweep.  With
+  // pdlp_tiled_sweeps = 1 the tiled form is used wherever it was built, with 0 never.  Returns true
+  // when sweeps were launched (the caller then resets the iterates).
+  bool tune_tiles()
+  {
+    tile_primal_ = tile_dual_ = false;
+    if (p_.tiled_sweeps == 0) return false;
+    int dev = 0, optin = 0;
+    B200_CUDA_CHECK(cudaGetDevice(&dev));
+    B200_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t limit = (size_t)optin - 64;  // the two mbarriers of the static shared memory
+    // Worth trying only when a row block's panel copies stay within a few matrix reads.
+    auto worth = [&](const tile_matrix& t, int64_t nnz) {
+      return p_.tiled_sweeps == 1 || t.staging_bytes() <= 4.0 * (double)nnz * 8.0;
+    };
+    const int64_t nnz = L_.nnz;
+    bool have_a = build_tile_matrix(L_.A, As_.data(), sms_, limit, s_, tA_) && worth(tA_, nnz);
+    bool have_t = build_tile_matrix(L_.AT, ATs_.data(), sms_, limit, s_, tAT_) && worth(tAT_, nnz);
+    if (!have_a) tA_ = tile_matrix{};
+    if (!have_t) tAT_ = tile_matrix{};
+    if (!have_a && !have_t) return false;
+    const size_t smem = std::max(have_a ? tA_.smem_bytes() : 0, have_t ? tAT_.smem_bytes() : 0);
+    B200_CUDA_CHECK(cudaFuncSetAttribute(tile_sweep_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    tpart_.resize(std::max(have_a ? (size_t)tA_.groups * in_.m : 1,
+                           have_t ? (size_t)tAT_.groups * in_.n : 1));
+    terr_.resize(1);
+    terr_.zero(s_);
+    if (p_.tiled_sweeps == 1) {
+      tile_primal_ = have_t;
+      tile_dual_   = have_a;
+      return false;
+    }
+    set_scalars(0);
+    cudaEvent_t e0, e1;
+    B200_CUDA_CHECK(cudaEventCreate(&e0));
+    B200_CUDA_CHECK(cudaEventCreate(&e1));
+    auto time_of = [&](auto&& launch) {
+      launch();
+      B200_CUDA_CHECK(cudaEventRecord(e0, s_));
+      for (int i = 0; i < 3; ++i) launch();
+      B200_CUDA_CHECK(cudaEventRecord(e1, s_));
+      B200_CUDA_CHECK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      B200_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+      return (double)ms;
+    };
+    if (have_t) {
+      const double sell = time_of([&] { launch_primal<false, true, false>(0); });
+      const double tile = time_of([&] { launch_primal_tiled(0); });
+      tile_primal_      = tile < sell;
+      tune_ms_[0] = sell / 3, tune_ms_[1] = tile / 3;
+    }
+    if (have_a) {
+      const double sell = time_of([&] { launch_dual<false, true, false>(0); });
+      const double tile = time_of([&] { launch_dual_tiled(0); });
+      tile_dual_        = tile < sell;
+      tune_ms_[2] = sell / 3, tune_ms_[3] = tile / 3;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check_tile_error();
+    if (!tile_primal_) tAT_ = tile_matrix{};
+    if (!tile_dual_) tA_ = tile_matrix{};
+    if (std::getenv("CUOPT_B200_TRACE"))
+      std::fprintf(stderr,
+                   "[cuopt_b200] sweep autotune: primal sell %.4f tiled %.4f ms -> %s; dual sell "
+                   "%.4f tiled %.4f ms -> %s\n",
+                   tune_ms_[0], tune_ms_[1], tile_primal_ ? "tiled" : "sell", tune_ms_[2],
+                   tune_ms_[3], tile_dual_ ? "tiled" : "sell");
+    return true;
+  }
+
+  // A tiled sweep whose panel copy did not complete in its bounded wait reports it here (read at
+  // every termination check, where the host synchronises anyway).
+  void check_tile_error()
+  {
+    if (!(tile_primal_ || tile_dual_) || terr_.size() == 0) return;
+    int e = 0;
+    B200_CUDA_CHECK(cudaMemcpyAsync(&e, terr_.data(), sizeof(int), cudaMemcpyDeviceToHost, s_));
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    if (e) throw cuda_error("tiled sweep: a panel copy did not complete within its wait limit");
+  }
+
+  // The plain (non-major, Halpern) sweeps in the form the autotuner chose.
+  void plain_primal(int it_off)
+  {
+    if constexpr (std::is_same_v<TX, float>) {
+      if (tile_primal_) return launch_primal_tiled(it_off);
+    }
+    launch_primal<false, true, false>(it_off);
+  }
+  void plain_dual(int it_off)
+  {
+    if constexpr (std::is_same_v<TX, float>) {
+      if (tile_dual_) return launch_dual_tiled(it_off);
+    }
+    launch_dual<false, true, false>(it_off);
+  }
+
   void plain_iterations(int L)  // L fused iterations, then t0 += L
   {
     for (int i = 0; i < L; ++i) {
-      launch_primal<false, true, false>(i);
-      launch_dual<false, true, false>(i);
+      plain_primal(i);
+      plain_dual(i);
     }
     advance_kernel<<<1, 1, 0, s_>>>(scalars_.data(), L);
     ++launches_;
@@ -618,6 +754,7 @@ class engine {
     B200_CUDA_CHECK(
       cudaMemcpyAsync(hres_, dres_.data(), nres * sizeof(double), cudaMemcpyDeviceToHost, s_));
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    if constexpr (std::is_same_v<TX, float>) check_tile_error();
     conv_info cv;
     if (p_.per_constraint_residual) {
       cv.linf_primal = hres_[5];
@@ -941,6 +1078,13 @@ class engine {
   dbuf<double> partials_, dres_;
   dbuf<pdlp_scalars> scalars_;
   std::map<int, cudaGraphExec_t> graphs_;
+  // Tiled sweeps (mixed precision): the tiled copies of A (dual sweep) and A^T (primal sweep), the
+  // form each plain sweep uses, the groups' partial sums and the bounded-wait error flag.
+  tile_matrix tA_, tAT_;
+  bool tile_primal_ = false, tile_dual_ = false;
+  dbuf<float> tpart_;
+  dbuf<int> terr_;
+  double tune_ms_[4] = {0, 0, 0, 0};
 
   double obj_scale_ = 1.0, obj_offset_ = 0.0;
   double c_norm_ = 0, b_norm_ = 0, beta_ = 1, gamma_ = 1;
@@ -961,45 +1105,16 @@ class engine {
     const auto A = As_view(), AT = ATs_view();
     std::vector<cudaEvent_t> ev(3 * iterations);
     for (auto& e : ev) B200_CUDA_CHECK(cudaEventCreate(&e));
-    // With CUOPT_B200_L2_PERSIST set, each sweep runs with an L2 persisting access window on the
-    // vector it gathers (y for the primal sweep, x_bar for the dual sweep).
-    const bool persist = std::getenv("CUOPT_B200_L2_PERSIST") != nullptr;
-    auto window = [&](const void* base, size_t bytes) {
-      if (!persist) return;
-      cudaStreamAttrValue v{};
-      v.accessPolicyWindow.base_ptr  = const_cast<void*>(base);
-      v.accessPolicyWindow.num_bytes = bytes;
-      v.accessPolicyWindow.hitRatio  = 1.0f;
-      v.accessPolicyWindow.hitProp   = cudaAccessPropertyPersisting;
-      v.accessPolicyWindow.missProp  = cudaAccessPropertyStreaming;
-      B200_CUDA_CHECK(cudaStreamSetAttribute(s_, cudaStreamAttributeAccessPolicyWindow, &v));
-    };
-    if (persist) {
-      int dev = 0, max_persist = 0, max_window = 0;
-      B200_CUDA_CHECK(cudaGetDevice(&dev));
-      B200_CUDA_CHECK(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev));
-      B200_CUDA_CHECK(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev));
-      B200_CUDA_CHECK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, (size_t)max_persist));
-      std::fprintf(stderr, "[cuopt_b200] L2 persisting carve-out %d bytes, window limit %d bytes\n",
-                   max_persist, max_window);
-    }
     for (int i = 0; i < 3; ++i) plain_iterations(1);  // warm-up
     for (int i = 0; i < iterations; ++i) {
       B200_CUDA_CHECK(cudaEventRecord(ev[3 * i], s_));
-      window(y_.data(), (size_t)m * sizeof(TX));
-      launch_primal<false, true, false>(0);
+      plain_primal(0);
       B200_CUDA_CHECK(cudaEventRecord(ev[3 * i + 1], s_));
-      window(xbar_.data(), (size_t)n * sizeof(TX));
-      launch_dual<false, true, false>(0);
+      plain_dual(0);
       B200_CUDA_CHECK(cudaEventRecord(ev[3 * i + 2], s_));
       advance_kernel<<<1, 1, 0, s_>>>(scalars_.data(), 1);
     }
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
-    if (persist) {
-      window(nullptr, 0);
-      B200_CUDA_CHECK(cudaCtxResetPersistingL2Cache());
-      B200_CUDA_CHECK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0));
-    }
     sweep_profile p;
     for (int i = 0; i < iterations; ++i) {
       float a = 0, b = 0;

@@ -59,6 +59,7 @@ struct pdlp_params {
   double time_limit       = 1e300;
   int precision           = 0;  // 0 FP64, 1 mixed FP32/FP64
   int refinement_passes   = 0;
+  int tiled_sweeps        = -1;  // mixed precision: -1 autotuned, 0 sliced ELL only, 1 tiled
   double refinement_tol   = 1e-8;
   bool log_to_console     = false;
   // Infeasibility detection (CUOPT_INFEASIBILITY_DETECTION and its two tolerances).

@@ -10,9 +10,10 @@
          same instances one by one with cuOptSolve (1e-6; FP64, or mixed precision with
          --batch-precision mixed, for both).
 `adjoint` (config c4) solves 64 non-degenerate 5000 x 10000 LPs in one batched call (crossover
-         on), back-propagates L = sum w * x* through the KKT adjoint, and checks the gradients
-         against the exact basis derivatives and against central differences (h = 1e-6) on random
-         coordinates of c, b and the A values.
+         on), back-propagates L = sum w * x* through the matrix-free KKT adjoint, and checks the
+         gradients of every instance against its vertex's exact derivatives and against central
+         differences (h = 1e-6) of the vertex map on random coordinates of c, b and the A values,
+         and a few instances' against central differences through the full solver.
 `climbers` solves `count` copies of one LP (the config's) that differ in one variable's upper
          bound each with one cuOptSolveClimbers call (FP64), and a sample of the same copies one
          by one with cuOptSolve.  With --strong-branching: cuOptBatchPDLPStrongBranching on
@@ -57,12 +58,10 @@ def main() -> None:
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c1_small")
     ap.add_argument("--mode", choices=["solve", "sweeps", "batch", "adjoint", "climbers", "gather"],
                     default="sweeps")
-    ap.add_argument("--fd-instances", type=int, default=2,
-                    help="adjoint mode: instances checked by finite differences")
+    ap.add_argument("--fd-solver", type=int, default=2,
+                    help="adjoint mode: instances also differenced through the full solver")
     ap.add_argument("--fd-coords", type=int, default=32,
                     help="adjoint mode: coordinates per kind (c, b, A) and instance")
-    ap.add_argument("--basis-checks", type=int, default=4,
-                    help="adjoint mode: instances checked against exact basis derivatives")
     ap.add_argument("--count", type=int, default=512, help="batch mode: instances")
     ap.add_argument("--sequential", type=int, default=64,
                     help="batch mode: instances also solved one by one (timing sample)")
@@ -77,6 +76,8 @@ def main() -> None:
     ap.add_argument("--strong-branching", action="store_true",
                     help="climbers mode: time cuOptBatchPDLPStrongBranching instead")
     ap.add_argument("--refine", type=int, default=0, help="> 0: continue a mixed-precision solve in FP64 to 1e-8")
+    ap.add_argument("--tiled", type=int, default=-1, choices=[-1, 0, 1],
+                    help="pdlp_tiled_sweeps: -1 autotuned, 0 sliced ELL only, 1 tiled where possible")
     a = ap.parse_args()
 
     if a.mode == "batch":
@@ -108,6 +109,7 @@ def main() -> None:
                  "relative_dual_tolerance", "absolute_gap_tolerance", "relative_gap_tolerance"):
         L.cuOptSetFloatParameter(s, name.encode(), a.tol)
     L.cuOptSetIntegerParameter(s, b"pdlp_precision", 1 if a.precision == "mixed" else 0)
+    L.cuOptSetIntegerParameter(s, b"pdlp_tiled_sweeps", a.tiled)
     L.cuOptSetParameter(s, b"log_to_console", b"false")
     if a.time_limit > 0:
         L.cuOptSetFloatParameter(s, b"time_limit", a.time_limit)
@@ -177,14 +179,12 @@ def run_gather(a) -> dict:
     return {"config": a.config, "m": m, "n": n, "gathers": 4 * nnz, "sms": sms, "rates": res}
 
 
-def run_batch(a) -> dict:
-    """The 512-LP batch: one batched solve of `count` uneven LPs vs the same LPs one at a time."""
-    import numpy as np
-
+def batch_models(count: int = 512):
+    """The 512-LP batch workload (generators.batch_lps) and its DataModels."""
     from cuopt_b200 import generators as gen
     from cuopt_b200 import linear_programming as lpm
 
-    lps = gen.batch_lps(a.count, seed=3000)
+    lps = gen.batch_lps(count, seed=3000)
     dms = []
     for lp in lps:
         dm = lpm.DataModel()
@@ -195,13 +195,25 @@ def run_batch(a) -> dict:
         dm.set_variable_lower_bounds(lp.var_lo)
         dm.set_variable_upper_bounds(lp.var_up)
         dms.append(dm)
+    return lps, dms
+
+
+def run_batch(a, models=None) -> dict:
+    """The 512-LP batch: one batched solve of `count` uneven LPs vs the same LPs one at a time.
+    `models` (lps, dms) reuses generated instances; with a.per_instance the result also holds every
+    instance's status, iteration count and primal objective."""
+    import numpy as np
+
+    from cuopt_b200 import linear_programming as lpm
+
+    lps, dms = models if models is not None else batch_models(a.count)
     st = lpm.SolverSettings()
     st.set_optimality_tolerance(a.tol)
     st.set_parameter(lpm.CUOPT_METHOD, int(lpm.SolverMethod.PDLP))
     st.set_parameter(lpm.CUOPT_LOG_TO_CONSOLE, False)
     precision = getattr(a, "batch_precision", "fp64")
     st.set_parameter(lpm.CUOPT_PDLP_PRECISION, 1 if precision == "mixed" else 0)
-    if a.refine:
+    if getattr(a, "refine", 0):
         st.set_parameter(lpm.CUOPT_PDLP_REFINEMENT_PASSES, a.refine)
     if a.time_limit > 0:
         st.set_parameter(lpm.CUOPT_TIME_LIMIT, a.time_limit)
@@ -219,7 +231,7 @@ def run_batch(a) -> dict:
            for s in sols]
     worst = sorted(range(len(sols)), key=lambda i: -obj_err[i])[:8]
     out = {"config": "c3", "precision": precision, "count": a.count, "tolerance": a.tol,
-           "refined_to": 1e-8 if (a.refine and precision == "mixed") else None,
+           "refined_to": 1e-8 if (getattr(a, "refine", 0) and precision == "mixed") else None,
            "m_total": int(sum(lp.m for lp in lps)),
            "n_total": int(sum(lp.n for lp in lps)), "nnz_total": int(sum(lp.nnz for lp in lps)),
            "batch_s": batch_s, "batch_times_s": times, "batch_lps_per_s": a.count / batch_s,
@@ -236,6 +248,10 @@ def run_batch(a) -> dict:
                                 "optimal_objective": lps[i].optimal_objective,
                                 "fp64_continued": int(sols[i].stats.get("refinement_passes", 0) > 0)}
                                for i in worst]}
+    if getattr(a, "per_instance", False):
+        out["instances"] = {"status": status, "iterations": iters,
+                            "primal_objective": [s.get_primal_objective() for s in sols],
+                            "relative_kkt": kkt}
     if a.sequential > 0:
         pick = np.linspace(0, a.count - 1, min(a.sequential, a.count)).astype(int)
         lpm.Solve(dms[pick[0]], st)  # warm-up
@@ -254,10 +270,77 @@ def run_batch(a) -> dict:
     return out
 
 
-def run_adjoint(a) -> dict:
-    """64 x (5000 x 10000) vertex LPs: batched forward solve + KKT-adjoint backward, checked two ways."""
+def _vertex_map_oracle(lp, w, h, picks, dev):
+    """Exact derivatives of L = w.x* at the vertex of a vertex_lp, and central differences of the
+    vertex map x*(c, b, A) (the solution of the same basis under the perturbed data) at the picked
+    coordinates.  Test oracle: a dense FP64 LU of the basis on the GPU (torch), each perturbed
+    vertex solved with it plus three steps of iterative refinement against the perturbed basis."""
     import numpy as np
     import scipy.sparse as sp
+    import torch
+
+    A = sp.csr_matrix((lp.val, lp.col_idx, lp.row_off), shape=(lp.m, lp.n))
+    basic = lp.basic
+    nonb = np.setdiff1d(np.arange(lp.n), basic)
+    pos = np.full(lp.n, -1)
+    pos[basic] = np.arange(lp.m)
+    t = lambda v: torch.tensor(np.asarray(v, dtype=np.float64), device=dev)
+    Bc = A[:, basic].tocoo()
+    B = torch.zeros(lp.m, lp.m, dtype=torch.float64, device=dev)
+    B[torch.tensor(Bc.row, device=dev, dtype=torch.int64),
+      torch.tensor(Bc.col, device=dev, dtype=torch.int64)] = t(Bc.data)
+    LU, piv = torch.linalg.lu_factor(B)
+    solve = lambda R: torch.linalg.lu_solve(LU, piv, R)
+    rhs0 = t(lp.con_lo - A[:, nonb] @ lp.x_star[nonb])
+    xB0 = solve(rhs0[:, None])[:, 0]
+    wB = t(w[basic])
+    lam = torch.linalg.lu_solve(LU, piv, wB[:, None], adjoint=True)[:, 0].cpu().numpy()
+    rows = np.repeat(np.arange(lp.m), np.diff(lp.row_off))
+    exact = {"c": np.zeros(lp.n), "b": lam, "A": -lam[rows] * lp.x_star[lp.col_idx]}
+    fd = {"c": np.zeros(len(picks["c"]))}  # the vertex does not depend on c
+    # b: rhs +- h e_i (linear in b)
+    kb = picks["b"]
+    R = rhs0[:, None].repeat(1, 2 * len(kb))
+    for q, i in enumerate(kb):
+        R[i, 2 * q] += h
+        R[i, 2 * q + 1] -= h
+    L = wB @ solve(R)
+    fd["b"] = ((L[0::2] - L[1::2]) / (2 * h)).cpu().numpy()
+    # A values: a column of N moves the right-hand side; a basic column perturbs the basis.
+    ka = picks["A"]
+    P = 2 * len(ka)
+    R = rhs0[:, None].repeat(1, P)
+    ii, kk, dd = [], [], []
+    for q, e in enumerate(ka):
+        i, j = int(rows[e]), int(lp.col_idx[e])
+        for sgn, col in ((1.0, 2 * q), (-1.0, 2 * q + 1)):
+            if pos[j] < 0:
+                R[i, col] -= sgn * h * lp.x_star[j]
+                ii.append(i), kk.append(0), dd.append(0.0)
+            else:
+                ii.append(i), kk.append(int(pos[j])), dd.append(sgn * h)
+    ii = torch.tensor(ii, device=dev, dtype=torch.int64)
+    kk = torch.tensor(kk, device=dev, dtype=torch.int64)
+    dd = torch.tensor(dd, device=dev, dtype=torch.float64)
+    cols = torch.arange(P, device=dev)
+    X = solve(R)
+    for _ in range(3):
+        res = R - B @ X
+        res[ii, cols] -= dd * X[kk, cols]
+        X = X + solve(res)
+    L = wB @ X
+    fd["A"] = ((L[0::2] - L[1::2]) / (2 * h)).cpu().numpy()
+    return exact, fd, xB0.cpu().numpy()
+
+
+def run_adjoint(a) -> dict:
+    """64 x (5000 x 10000) vertex LPs: batched forward solve with crossover, the matrix-free KKT
+    adjoint backward (cuOptSolutionAdjointBatch), checked against the exact derivatives of every
+    instance's vertex and against central differences (h = 1e-6) of the vertex map on
+    a.fd_coords coordinates of each of c, b and the A values of every instance; a.fd_solver
+    instances are also differenced through the full solver (perturbed LPs re-solved with
+    crossover)."""
+    import numpy as np
     import torch
 
     from cuopt_b200 import generators as gen
@@ -287,7 +370,9 @@ def run_adjoint(a) -> dict:
     st.set_parameter(lpm.CUOPT_CROSSOVER, True)
     st.set_parameter(lpm.CUOPT_LOG_TO_CONSOLE, False)
     insts = [instance(lp, grad=True) for lp in lps]
-    lp_solve_batch([instance(lps[0])], st)  # warm-up
+    warm = instance(lps[0], grad=True)
+    (x0, _), = lp_solve_batch([warm], st)  # warm-up (forward and backward)
+    (f(ws[0]) * x0).sum().backward()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     outs = lp_solve_batch(insts, st)
@@ -299,30 +384,40 @@ def run_adjoint(a) -> dict:
     torch.cuda.synchronize()
     backward_s = time.perf_counter() - t0
 
-    # Exact basis derivatives (an independent dense LU of each basis on the host: these random
-    # sparse bases fill in almost completely, so a dense solve is the faster one).
-    err = {"c": 0.0, "b": 0.0, "A": 0.0}
-    rel = lambda g, e: float(np.abs(g - e).max() / max(1.0, np.abs(e).max()))
-    nb = min(getattr(a, "basis_checks", 4), count)
-    for lp, w, t in zip(lps[:nb], ws[:nb], insts[:nb]):
-        A = sp.csr_matrix((lp.val, lp.col_idx, lp.row_off), shape=(lp.m, lp.n))
-        lam = np.linalg.solve(A[:, lp.basic].toarray().T, w[lp.basic])
-        rows = np.repeat(np.arange(lp.m), np.diff(lp.row_off))
-        dval = -lam[rows] * lp.x_star[lp.col_idx]
-        err["c"] = max(err["c"], float(np.abs(t.c.grad.cpu().numpy()).max()))
-        err["b"] = max(err["b"], rel((t.con_lo.grad + t.con_up.grad).cpu().numpy(), lam))
-        err["A"] = max(err["A"], rel(t.values.grad.cpu().numpy(), dval))
-
-    # Central differences through the solver (all perturbed LPs in one batched call).
-    h, fd_err, checked = 1e-6, 0.0, 0
-    pert, keys = [], []
-    for q in range(min(a.fd_instances, count)):
-        lp = lps[q]
+    h = 1e-6
+    vertex_err, basis_err, fd_err, checked = 0.0, {"c": 0.0, "b": 0.0, "A": 0.0}, 0.0, 0
+    worst = None
+    picks_all = []
+    for q, (lp, w, t) in enumerate(zip(lps, ws, insts)):
         picks = {"c": rng.choice(lp.n, a.fd_coords, replace=False),
                  "b": rng.choice(lp.m, a.fd_coords, replace=False),
                  "A": rng.choice(lp.nnz, a.fd_coords, replace=False)}
-        for kind, idx in picks.items():
-            for k in idx:
+        picks_all.append(picks)
+        exact, fd, xB = _vertex_map_oracle(lp, w, h, picks, dev)
+        x = outs[q][0].detach().cpu().numpy()
+        vertex_err = max(vertex_err, float(np.abs(x[lp.basic] - xB).max() / max(1.0, np.abs(xB).max())))
+        grads = {"c": t.c.grad.cpu().numpy(), "b": (t.con_lo.grad + t.con_up.grad).cpu().numpy(),
+                 "A": t.values.grad.cpu().numpy()}
+        for kind in ("c", "b", "A"):
+            e = exact[kind]
+            basis_err[kind] = max(basis_err[kind],
+                                  float(np.abs(grads[kind] - e).max() / max(1.0, np.abs(e).max())))
+            for k, d in zip(picks[kind], fd[kind]):
+                g = grads[kind][k]
+                err = abs(d - g) / (1.0 + abs(g))
+                if err > fd_err:
+                    fd_err, worst = err, {"instance": q, "kind": kind, "coordinate": int(k),
+                                          "fd": float(d), "gradient": float(g)}
+                checked += 1
+
+    # Central differences through the solver (perturbed LPs re-solved with crossover, in one
+    # batched call) on the first a.fd_solver instances, a few coordinates each.
+    solver_err, solver_checked = 0.0, 0
+    pert, keys = [], []
+    for q in range(min(a.fd_solver, count)):
+        lp = lps[q]
+        for kind in ("c", "b", "A"):
+            for k in picks_all[q][kind][:4]:
                 for sgn in (1.0, -1.0):
                     c, lo, up, val = lp.c.copy(), lp.con_lo.copy(), lp.con_up.copy(), lp.val.copy()
                     if kind == "c":
@@ -334,21 +429,28 @@ def run_adjoint(a) -> dict:
                         val[k] += sgn * h
                     pert.append(instance(lp, c, lo, up, val))
                     keys.append((q, kind, int(k), sgn))
-    res = lp_solve_batch(pert, st) if pert else []
-    vals = {key: float(x.detach().cpu().numpy() @ ws[key[0]]) for key, (x, _) in zip(keys, res)}
-    for (q, kind, k, sgn) in keys:
-        if sgn < 0:
-            continue
-        fd = (vals[(q, kind, k, 1.0)] - vals[(q, kind, k, -1.0)]) / (2 * h)
-        t = insts[q]
-        g = {"c": t.c.grad, "b": t.con_lo.grad + t.con_up.grad, "A": t.values.grad}[kind][k].item()
-        fd_err = max(fd_err, abs(fd - g) / (1.0 + abs(g)))
-        checked += 1
+    if pert:
+        res = lp_solve_batch(pert, st)
+        vals = {key: float(x.detach().cpu().numpy() @ ws[key[0]]) for key, (x, _) in zip(keys, res)}
+        for (q, kind, k, sgn) in keys:
+            if sgn < 0:
+                continue
+            fdv = (vals[(q, kind, k, 1.0)] - vals[(q, kind, k, -1.0)]) / (2 * h)
+            t = insts[q]
+            g = {"c": t.c.grad, "b": t.con_lo.grad + t.con_up.grad, "A": t.values.grad}[kind][k].item()
+            solver_err = max(solver_err, abs(fdv - g) / (1.0 + abs(g)))
+            solver_checked += 1
     return {"config": "c4", "count": count, "m": 5000, "n": 10000, "forward_s": forward_s,
             "backward_s": backward_s, "adjoint_ms_per_instance": backward_s * 1e3 / count,
-            "grad_vs_basis_max_rel_error": err, "basis_checked_instances": nb,
-            "fd_checked": checked, "fd_h": h,
-            "fd_max_rel_error": fd_err}
+            "backward": "matrix-free LSQR on the GPU (cuOptSolutionAdjointBatch), one thread block "
+                        "per active-set system; no dense factorisation",
+            "crossover_vertex_max_rel_error": vertex_err,
+            "grad_vs_exact_max_rel_error": basis_err, "exact_checked_instances": count,
+            "fd_h": h, "fd_checked": checked, "fd_max_rel_error": fd_err, "fd_worst": worst,
+            "fd_of": "the vertex map (perturbed vertices solved by a dense FP64 LU with refinement "
+                     "on the GPU, a test oracle)",
+            "fd_through_solver_checked": solver_checked,
+            "fd_through_solver_max_rel_error": solver_err}
 
 
 def run_climbers(a) -> dict:

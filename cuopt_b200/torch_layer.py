@@ -5,7 +5,8 @@
 solves  min c.x  s.t.  con_lo <= A x <= con_up,  var_lo <= x <= var_up  (A in CSR: values,
 column_indices, row_offsets; int32 indices) with the library's PDLP and returns the primal and
 dual solutions as float64 tensors on the device of `c`.  Backward is the KKT adjoint of the
-optimal solution (cuOptSolutionAdjoint): gradients flow to c, con_lo, con_up and values; the CSR
+optimal solution (cuOptSolutionAdjointBatch: matrix-free LSQR solves with the active-set matrix
+on the GPU, one thread block per system): gradients flow to c, con_lo, con_up and values; the CSR
 structure and the variable bounds are constants.  At a non-degenerate vertex these are the exact
 derivatives of the solution map; elsewhere they are those of its minimum-norm response.
 
@@ -86,23 +87,6 @@ class _Solved:
         self.status = status.value
         return x, y
 
-    def adjoint(self, gx: Optional[torch.Tensor], gy: Optional[torch.Tensor]):
-        L = lib()
-        dev = self.device
-        gx = (torch.zeros(self.n, dtype=torch.float64, device=dev) if gx is None
-              else _contig(gx, torch.float64))
-        gy = None if gy is None else _contig(gy, torch.float64)
-        dc = torch.empty(self.n, dtype=torch.float64, device=dev)
-        dlo = torch.empty(self.m, dtype=torch.float64, device=dev)
-        dup = torch.empty(self.m, dtype=torch.float64, device=dev)
-        dval = torch.empty(self.nnz, dtype=torch.float64, device=dev)
-        rc = L.cuOptSolutionAdjoint(self.problem, self.solution, _ptr(gx),
-                                    _ptr(gy) if gy is not None else None, _ptr(dc), _ptr(dlo),
-                                    _ptr(dup), _ptr(dval))
-        if rc != 0:
-            raise lpm.CuOptError(rc, "cuOptSolutionAdjoint (the solution must be Optimal)")
-        return dc, dlo, dup, dval
-
     def __del__(self):
         try:
             L = lib()
@@ -124,9 +108,47 @@ def _settings(settings: Optional[lpm.SolverSettings]) -> lpm.SolverSettings:
     return s
 
 
+def _adjoint_batch(solved, pairs):
+    """cuOptSolutionAdjointBatch over the solutions with a gradient: all their active-set solves in
+    one launch.  Returns one (dc, dlo, dup, dval) tuple per solution (None without a gradient)."""
+    L = lib()
+    jobs = [i for i, (gx, gy) in enumerate(pairs) if gx is not None or gy is not None]
+    results = [None] * len(solved)
+    if not jobs:
+        return results
+    keep, ptrs = [], {k: [] for k in ("gx", "gy", "dc", "dlo", "dup", "dval")}
+    for i in jobs:
+        sv, (gx, gy) = solved[i], pairs[i]
+        dev = sv.device
+        gx = (torch.zeros(sv.n, dtype=torch.float64, device=dev) if gx is None
+              else _contig(gx, torch.float64))
+        gy = None if gy is None else _contig(gy, torch.float64)
+        outs = (torch.empty(sv.n, dtype=torch.float64, device=dev),
+                torch.empty(sv.m, dtype=torch.float64, device=dev),
+                torch.empty(sv.m, dtype=torch.float64, device=dev),
+                torch.empty(sv.nnz, dtype=torch.float64, device=dev))
+        keep.append((gx, gy))
+        results[i] = outs
+        ptrs["gx"].append(gx.data_ptr())
+        ptrs["gy"].append(gy.data_ptr() if gy is not None else None)
+        for k, t in zip(("dc", "dlo", "dup", "dval"), outs):
+            ptrs[k].append(t.data_ptr())
+    arr = lambda vals: (C.c_void_p * len(vals))(*vals)
+    probs = (handle_t * len(jobs))(*[solved[i].problem.value for i in jobs])
+    sols = (handle_t * len(jobs))(*[solved[i].solution.value for i in jobs])
+    if any(t is not None and t.is_cuda for t, _ in keep):
+        torch.cuda.synchronize()  # the gradients are complete before the library reads them
+    rc = L.cuOptSolutionAdjointBatch(len(jobs), probs, sols, arr(ptrs["gx"]), arr(ptrs["gy"]),
+                                     arr(ptrs["dc"]), arr(ptrs["dlo"]), arr(ptrs["dup"]),
+                                     arr(ptrs["dval"]))
+    if rc != 0:
+        raise lpm.CuOptError(rc, "cuOptSolutionAdjointBatch (every solution must be Optimal)")
+    return results
+
+
 class _AttachBatch(torch.autograd.Function):
     """Returns already computed solutions and routes their gradients through the KKT adjoint; the
-    adjoints of a batch run on a few host threads, so their factorisations overlap on the GPU."""
+    adjoints of a batch are one cuOptSolutionAdjointBatch call."""
 
     @staticmethod
     def forward(ctx, solved, *tensors):
@@ -139,20 +161,12 @@ class _AttachBatch(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, *grads):
-        from concurrent.futures import ThreadPoolExecutor
         pairs = [(grads[2 * i], grads[2 * i + 1]) for i in range(len(ctx.solved))]
-        jobs = [i for i, (gx, gy) in enumerate(pairs) if gx is not None or gy is not None]
-        results = [None] * len(ctx.solved)
-        with ThreadPoolExecutor(max_workers=min(_ADJOINT_THREADS, max(1, len(jobs)))) as ex:
-            for i, r in zip(jobs, ex.map(lambda i: ctx.solved[i].adjoint(*pairs[i]), jobs)):
-                results[i] = r
+        results = _adjoint_batch(ctx.solved, pairs)
         flat = [None]
         for r in results:
             flat.extend(r if r is not None else (None, None, None, None))
         return tuple(flat)
-
-
-_ADJOINT_THREADS = 4
 
 
 def lp_solve(c, con_lo, con_up, values, row_offsets, column_indices, var_lo, var_up,

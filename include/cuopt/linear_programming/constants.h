@@ -88,8 +88,14 @@
 #define CUOPT_PDLP_PRECISION            "pdlp_precision"
 #define CUOPT_PDLP_REFINEMENT_PASSES    "pdlp_refinement_passes"
 #define CUOPT_PDLP_REFINEMENT_TOLERANCE "pdlp_refinement_tolerance"
+#define CUOPT_PDLP_TILED_SWEEPS         "pdlp_tiled_sweeps"
 #define CUOPT_PDLP_PRECISION_FP64  0
 #define CUOPT_PDLP_PRECISION_MIXED 1
+/* pdlp_tiled_sweeps (mixed precision): -1 chooses per sweep by timing both forms at setup,
+ * 0 always uses the sliced-ELL sweeps, 1 uses the tiled sweeps wherever the matrix allows them */
+#define CUOPT_PDLP_TILED_SWEEPS_AUTO -1
+#define CUOPT_PDLP_TILED_SWEEPS_OFF  0
+#define CUOPT_PDLP_TILED_SWEEPS_ON   1
 
 #define CUOPT_MODE_OPPORTUNISTIC 0
 #define CUOPT_MODE_DETERMINISTIC 1

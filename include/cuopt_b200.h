@@ -161,8 +161,9 @@ cuopt_int_t cuOptBatchPDLPStrongBranching(cuOptOptimizationProblem problem,
  * implicit differentiation of the KKT conditions on the solution's active set.  For a row whose
  * bounds are equal, the gradient with respect to its right-hand side is in dl_dlower.  At a
  * non-degenerate vertex these are the exact derivatives; otherwise those of the minimum-norm
- * response.  Any output pointer may be NULL.  Returns CUOPT_INVALID_ARGUMENT if the solution is not
- * Optimal (or the active set exceeds the dense limit). */
+ * response (in the equilibrated variables).  The active-set solves are matrix-free: LSQR on the
+ * GPU, one thread block per system.  Any output pointer may be NULL.  Returns
+ * CUOPT_INVALID_ARGUMENT if the solution is not Optimal. */
 cuopt_int_t cuOptSolutionAdjoint(cuOptOptimizationProblem problem,
                                  cuOptSolution solution,
                                  const cuopt_float_t* dl_dx,
@@ -171,6 +172,21 @@ cuopt_int_t cuOptSolutionAdjoint(cuOptOptimizationProblem problem,
                                  cuopt_float_t* dl_dlower,
                                  cuopt_float_t* dl_dupper,
                                  cuopt_float_t* dl_dvalues);
+
+/* cuOptSolutionAdjoint for `count` (problem, solution) pairs at once (no counterpart in the
+ * reference): every pointer argument is an array of `count` pointers with the meaning of the single
+ * call's argument (dl_dx[i] required; dl_dy, the output arrays, or any of their entries may be
+ * NULL).  All the active-set solves of the batch run in one launch, one thread block each.
+ * Returns CUOPT_INVALID_ARGUMENT (and writes nothing) if any solution is not Optimal. */
+cuopt_int_t cuOptSolutionAdjointBatch(cuopt_int_t count,
+                                      const cuOptOptimizationProblem* problems,
+                                      const cuOptSolution* solutions,
+                                      const cuopt_float_t* const* dl_dx,
+                                      const cuopt_float_t* const* dl_dy,
+                                      cuopt_float_t* const* dl_dc,
+                                      cuopt_float_t* const* dl_dlower,
+                                      cuopt_float_t* const* dl_dupper,
+                                      cuopt_float_t* const* dl_dvalues);
 
 /* KKT errors of a given point, computed without allocating device memory (no counterpart in the
  * reference).  For an LP in device memory (user's CSR order, as for cuOptSolveDevice) and a point

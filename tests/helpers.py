@@ -58,6 +58,39 @@ def rel(a, b):
     return abs(a - b) / max(1.0, abs(b))
 
 
+# The objective bound the results are held to: within 1e-6 relative (to max(1, |optimum|)) of the
+# optimum known by construction and of the FP64 oracle.  A solve to 1e-6 relative KKT does not
+# imply it: the residuals are relative to |b| and |c| while the objective can be far smaller, so
+# the oracle itself ends 6.8e-6 off on instance 284 of the 512-LP batch at 1e-6 (pinned in
+# test_oracle.py).  Tests of the bound therefore solve to 1e-8 relative KKT: FP64 at 1e-8, or
+# mixed precision at 1e-6 continued in FP64 to 1e-8 (refined_settings).
+OBJ_RTOL = 1e-6
+REFINED_TOL = 1e-8
+
+
+def refined_settings(**kw) -> lpm.SolverSettings:
+    """Mixed precision to 1e-6 relative KKT, then the FP64 continuation to 1e-8."""
+    s = settings(tol=1e-6, precision=1, **kw)
+    s.set_parameter(lpm.CUOPT_PDLP_REFINEMENT_PASSES, 1)
+    s.set_parameter(lpm.CUOPT_PDLP_REFINEMENT_TOLERANCE, REFINED_TOL)
+    return s
+
+
+def relative_kkt(sol) -> float:
+    """Largest of the three relative KKT errors a solution reports."""
+    st = sol.stats
+    return max(st["l2_relative_primal_residual"], st["l2_relative_dual_residual"],
+               st["relative_gap"])
+
+
+def oracle_results():
+    """The oracle's results on the benchmark workloads (tests/golden/oracle_results.json, written
+    by tests/golden/make_oracle_fixtures.py)."""
+    import json
+    from pathlib import Path
+    return json.loads((Path(__file__).resolve().parent / "golden" / "oracle_results.json").read_text())
+
+
 def small_lp(rows, c, con_lo, con_up, var_lo, var_up):
     """An LP view (as the oracle and datamodel_from_lp take it) from dense row lists
     [[(column, value), ...], ...]."""

@@ -1,5 +1,6 @@
-"""GPU tests of the KKT adjoint (cuOptSolutionAdjoint), the torch layer over it, and the vertex
-crossover.
+"""GPU tests of the matrix-free KKT adjoint (cuOptSolutionAdjointBatch: LSQR on the GPU, one
+thread block per active-set system), the torch layer over it, and the vertex crossover (the same
+LSQR solves).
 
 References: the constructed optimum of generators.vertex_lp (unique and non-degenerate, with a
 known basis), the exact derivatives of that vertex computed from a sparse LU of its basis (SciPy,
@@ -159,8 +160,9 @@ def test_adjoint_requires_an_optimal_solution(vlp):
 
 
 def test_batched_backward_equals_single_backwards():
-    """lp_solve_batch back-propagates through one batched call (adjoints on host threads); the
-    gradients equal those of the instances solved and differentiated one at a time."""
+    """lp_solve_batch back-propagates through one cuOptSolutionAdjointBatch call (every active-set
+    system in one launch); the gradients equal those of the instances solved and differentiated one
+    at a time (each system's LSQR runs alone in its thread block, so the batch does not change it)."""
     from cuopt_b200.torch_layer import LPInstance, lp_solve, lp_solve_batch
     lps = [gen.vertex_lp(150 + 50 * i, 300 + 100 * i, 6, seed=70 + i) for i in range(3)]
     rng = np.random.default_rng(12)
@@ -174,3 +176,22 @@ def test_batched_backward_equals_single_backwards():
         (torch.tensor(w, device="cuda") * x).sum().backward()
         for k in ("c", "con_lo", "con_up", "values"):
             _close(tb[k].grad.cpu().numpy(), ts[k].grad.cpu().numpy(), 1e-9)
+
+
+def test_c4_shape_adjoint_against_vertex_map():
+    """Four 5000 x 10000 vertex LPs (the 64-LP adjoint workload's shape) through the bench's own
+    check: batched forward with crossover, the batched matrix-free backward of L = w.x*, then
+    (a) the crossover vertex equals each LP's constructed vertex to 1e-9, (b) the gradients equal
+    the exact derivatives of the vertex to 1e-7 (relative to their largest magnitude), and
+    (c) central differences (h = 1e-6) of the vertex map on 32 coordinates of each of c, b and the
+    A values per instance agree to 1e-4 (|fd - g| / (1 + |g|)), as do differences through the full
+    solver on one instance."""
+    import argparse
+    from cuopt_b200.profile import run_adjoint
+    r = run_adjoint(argparse.Namespace(count=4, tol=1e-6, fd_coords=32, fd_solver=1))
+    assert r["crossover_vertex_max_rel_error"] <= 1e-9
+    assert max(r["grad_vs_exact_max_rel_error"].values()) <= 1e-7
+    assert r["fd_checked"] == 4 * 3 * 32
+    assert r["fd_max_rel_error"] <= 1e-4, r["fd_worst"]
+    assert r["fd_through_solver_checked"] == 12
+    assert r["fd_through_solver_max_rel_error"] <= 1e-4

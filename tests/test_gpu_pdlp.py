@@ -6,7 +6,9 @@ values of the reference's own tests (tests/golden/golden.json).
 
 Floating-point tolerances (FP64 path): iterates after the same number of iterations agree with the
 oracle to 1e-9 relative (summation order differs), objectives to 1e-9 relative, and solved
-problems reach the relative KKT targets asked for.
+problems reach the relative KKT targets asked for.  Objectives are held to OBJ_RTOL = 1e-6
+relative of the constructed optimum and of the FP64 oracle on solves to 1e-8 relative KKT (FP64, or
+mixed precision refined in FP64): 1e-6 KKT alone does not bound the objective error by 1e-6.
 """
 from __future__ import annotations
 
@@ -16,7 +18,8 @@ import pytest
 from cuopt_b200 import generators as gen
 from cuopt_b200 import linear_programming as lpm
 from oracle import oracle as O
-from tests.helpers import datamodel_from_lp, oracle_view, rel, settings
+from tests.helpers import (OBJ_RTOL, REFINED_TOL, datamodel_from_lp, oracle_results, oracle_view,
+                           refined_settings, rel, relative_kkt, settings)
 
 pytestmark = pytest.mark.gpu
 
@@ -48,29 +51,44 @@ def test_iterates_match_oracle(small_lp, k):
 
 
 def test_solve_matches_oracle_and_optimum(small_lp):
+    """At 1e-6: the oracle's status, iteration count and objective (1e-9 relative) and relative KKT
+    <= 1e-6; at 1e-8: the constructed optimum and the oracle's objective within OBJ_RTOL."""
     dm = datamodel_from_lp(small_lp)
     sol = lpm.Solve(dm, settings(tol=1e-6))
     res, x, y, _ = O.solve(small_lp, tol=1e-6)
     assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
     assert res["status"] == 1
-    assert abs(sol.get_lp_stats()["nb_iterations"] - res["iterations"]) <= 0.05 * res["iterations"]
-    opt = small_lp.optimal_objective
-    assert rel(sol.get_primal_objective(), opt) <= 1e-5
+    assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+    assert rel(sol.get_primal_objective(), res["primal_obj"]) <= 1e-9
+    assert relative_kkt(sol) <= 1e-6
     kkt = gen.kkt_relative_error(small_lp, sol.get_primal_solution(), sol.get_dual_solution())
     assert kkt["rel_primal"] <= 1e-6 and kkt["rel_gap"] <= 1e-6
+    tight = lpm.Solve(dm, settings(tol=REFINED_TOL))
+    res8, _, _, _ = O.solve(small_lp, tol=REFINED_TOL)
+    assert rel(tight.get_primal_objective(), small_lp.optimal_objective) <= OBJ_RTOL
+    assert rel(tight.get_primal_objective(), res8["primal_obj"]) <= 1e-9
 
 
 def test_config0_full_size():
-    """The 2000 x 5000 LP (8 nnz / column): Optimal at 1e-6, objective within 1e-6 of the
-    constructed optimum relative to its magnitude, same status and iteration count as the oracle."""
+    """The 2000 x 5000 LP (8 nnz / column): Optimal at 1e-6 with the oracle's status, iteration
+    count and objective (1e-9); at 1e-8, FP64 and mixed precision refined in FP64 both give the
+    constructed optimum and the oracle's objective within OBJ_RTOL."""
     lp = gen.constructed_lp(2000, 5000, 8, seed=0)
-    sol = lpm.Solve(datamodel_from_lp(lp), settings(tol=1e-6))
+    dm = datamodel_from_lp(lp)
+    sol = lpm.Solve(dm, settings(tol=1e-6))
     res, _, _, _ = O.solve(lp, tol=1e-6)
     assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal == res["status"]
-    assert abs(sol.get_lp_stats()["nb_iterations"] - res["iterations"]) <= 0.05 * res["iterations"]
-    assert rel(sol.get_primal_objective(), lp.optimal_objective) <= 1e-5
+    assert sol.get_lp_stats()["nb_iterations"] == res["iterations"]
+    assert rel(sol.get_primal_objective(), res["primal_obj"]) <= 1e-9
     kkt = gen.kkt_relative_error(lp, sol.get_primal_solution(), sol.get_dual_solution())
     assert max(kkt["rel_primal"], kkt["rel_gap"]) <= 1e-6
+    res8, _, _, _ = O.solve(lp, tol=REFINED_TOL)
+    for s in (settings(tol=REFINED_TOL), refined_settings()):
+        tight = lpm.Solve(dm, s)
+        assert tight.get_termination_status() == lpm.LPTerminationStatus.Optimal
+        assert relative_kkt(tight) <= REFINED_TOL
+        assert rel(tight.get_primal_objective(), lp.optimal_objective) <= OBJ_RTOL
+        assert rel(tight.get_primal_objective(), res8["primal_obj"]) <= OBJ_RTOL
 
 
 def test_afiro_objective(golden, golden_dir):
@@ -127,18 +145,30 @@ def test_inequality_and_free_rows_match_oracle():
 def test_maximize_offset_matches_oracle(small_lp):
     dm = datamodel_from_lp(small_lp, maximize=True, offset=3.5)
     dm.set_objective_coefficients(-small_lp.c)
-    sol = lpm.Solve(dm, settings(tol=1e-6))
-    res, x, y, _ = O.solve(oracle_view(dm), tol=1e-6)
+    sol = lpm.Solve(dm, settings(tol=REFINED_TOL))
+    res, x, y, _ = O.solve(oracle_view(dm), tol=REFINED_TOL)
     assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
     assert rel(sol.get_primal_objective(), res["primal_obj"]) <= 1e-8
-    assert rel(sol.get_primal_objective(), -small_lp.optimal_objective + 3.5) <= 1e-5
+    assert rel(sol.get_primal_objective(), -small_lp.optimal_objective + 3.5) <= OBJ_RTOL
     np.testing.assert_allclose(sol.get_dual_solution(), y, atol=1e-7 * (1 + np.abs(y).max()))
 
 
 def test_mixed_precision_reaches_tolerance(small_lp):
-    sol = lpm.Solve(datamodel_from_lp(small_lp), settings(tol=1e-4, precision=1))
+    """Mixed precision at 1e-6: Optimal with relative KKT <= 1e-6 on the returned FP64 point
+    (reported and recomputed on the host); refined in FP64 to 1e-8: the constructed optimum and the
+    oracle's 1e-8 objective within OBJ_RTOL."""
+    dm = datamodel_from_lp(small_lp)
+    sol = lpm.Solve(dm, settings(tol=1e-6, precision=1))
     assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
-    assert rel(sol.get_primal_objective(), small_lp.optimal_objective) <= 1e-3
+    assert relative_kkt(sol) <= 1e-6
+    kkt = gen.kkt_relative_error(small_lp, sol.get_primal_solution(), sol.get_dual_solution())
+    assert kkt["rel_primal"] <= 1e-6 and kkt["rel_gap"] <= 1e-6
+    ref = lpm.Solve(dm, refined_settings())
+    res8, _, _, _ = O.solve(small_lp, tol=REFINED_TOL)
+    assert ref.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert relative_kkt(ref) <= REFINED_TOL
+    assert rel(ref.get_primal_objective(), small_lp.optimal_objective) <= OBJ_RTOL
+    assert rel(ref.get_primal_objective(), res8["primal_obj"]) <= OBJ_RTOL
 
 
 def test_mixed_precision_refinement_reaches_1e8():
@@ -322,14 +352,21 @@ def test_mixed_precision_stall_continues_in_fp64():
     assert mixed.get_termination_status() == fp64.get_termination_status() == \
         lpm.LPTerminationStatus.Optimal
     assert mixed.stats["refinement_passes"] == 1
-    assert rel(mixed.get_primal_objective(), lp.optimal_objective) <= 1e-5
+    assert relative_kkt(mixed) <= 1e-6 and relative_kkt(fp64) <= 1e-6
     other = gen.batch_instance(0)
     sols, _ = lpm.BatchSolve([dm, datamodel_from_lp(other)],
                              settings(tol=1e-6, precision=1, time_limit=60))
     assert [int(s.get_termination_status()) for s in sols] == [1, 1]
     assert [s.stats["refinement_passes"] for s in sols] == [1, 0]
-    assert rel(sols[0].get_primal_objective(), lp.optimal_objective) <= 1e-5
-    assert rel(sols[1].get_primal_objective(), other.optimal_objective) <= 1e-5
+    assert max(relative_kkt(s) for s in sols) <= 1e-6
+    # Refined to 1e-8, alone and in a batch: the constructed optima within OBJ_RTOL.
+    ref = lpm.Solve(dm, refined_settings(time_limit=60))
+    assert rel(ref.get_primal_objective(), lp.optimal_objective) <= OBJ_RTOL
+    sols, _ = lpm.BatchSolve([dm, datamodel_from_lp(other)], refined_settings(time_limit=60))
+    assert [s.stats["refinement_passes"] for s in sols] == [1, 1]
+    assert max(relative_kkt(s) for s in sols) <= REFINED_TOL
+    assert rel(sols[0].get_primal_objective(), lp.optimal_objective) <= OBJ_RTOL
+    assert rel(sols[1].get_primal_objective(), other.optimal_objective) <= OBJ_RTOL
 
 
 def test_problem_from_pinned_or_device_arrays_solves_identically(small_lp):
@@ -414,3 +451,59 @@ def test_concurrent_solves_on_host_threads_match_sequential():
     for a, b in zip(seq, par):
         assert a[0] == b[0] == 1 and a[1] == b[1]
         assert np.array_equal(a[2], b[2]) and np.array_equal(a[3], b[3])
+
+
+def test_c1_small_matches_oracle_fixture():
+    """The 750k x 1.5M constructed LP (12M non-zeros, the 1M x 2M workload's generator): FP64 at
+    1e-6 ends with the oracle's status, iteration count and objective (1e-9 relative;
+    tests/golden/oracle_results.json); mixed precision at 1e-6 reaches relative KKT <= 1e-6; FP64
+    at 1e-8 and mixed precision refined in FP64 to 1e-8 give the constructed optimum and the
+    oracle's 1e-8 objective within OBJ_RTOL."""
+    fx = oracle_results()["single"]["c1_small"]
+    lp = gen.constructed_lp(fx["m"], fx["n"], 8, seed=fx["seed"])
+    assert rel(lp.optimal_objective, fx["optimal_objective"]) <= 1e-12
+    dm = datamodel_from_lp(lp)
+    fp64 = lpm.Solve(dm, settings(tol=1e-6, time_limit=120))
+    want = fx["1e-06"]
+    assert int(fp64.get_termination_status()) == want["status"] == 1
+    assert fp64.get_lp_stats()["nb_iterations"] == want["iterations"]
+    assert rel(fp64.get_primal_objective(), want["primal_objective"]) <= 1e-9
+    mixed = lpm.Solve(dm, settings(tol=1e-6, precision=1, time_limit=120))
+    assert mixed.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert relative_kkt(mixed) <= 1e-6
+    want8 = fx["1e-08"]
+    for s in (settings(tol=REFINED_TOL, time_limit=120), refined_settings(time_limit=120)):
+        sol = lpm.Solve(dm, s)
+        assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+        assert relative_kkt(sol) <= REFINED_TOL
+        assert rel(sol.get_primal_objective(), lp.optimal_objective) <= OBJ_RTOL
+        assert rel(sol.get_primal_objective(), want8["primal_objective"]) <= OBJ_RTOL
+
+
+@pytest.mark.parametrize("shape", [(2000, 5000, 8, 0), (60_000, 150_000, 8, 5)])
+def test_tiled_sweeps_follow_sliced_sweeps(shape):
+    """Mixed precision with the tiled sweeps forced on (pdlp_tiled_sweeps = 1: panels of the
+    gathered vector in shared memory, FP32 row sums) against the sliced-ELL sweeps (0): after 150
+    iterations (before the first restart decision) the iterates agree to 1e-4 relative to their
+    scale (the two sum in different orders and precisions, so they drift apart at FP32 rounding),
+    and both solves end Optimal at 1e-6 with relative KKT <= 1e-6; the autotuned default (-1) ends
+    Optimal too."""
+    m, n, k, seed = shape
+    lp = gen.constructed_lp(m, n, k, seed=seed)
+    dm = datamodel_from_lp(lp)
+    runs = {}
+    for tiled in (0, 1):
+        s = settings(tol=1e-12, iteration_limit=150, precision=1)
+        s.set_parameter(lpm.CUOPT_PDLP_TILED_SWEEPS, tiled)
+        runs[tiled] = lpm.Solve(dm, s)
+    a, b = runs[0], runs[1]
+    assert a.get_lp_stats()["nb_iterations"] == b.get_lp_stats()["nb_iterations"] == 150
+    for u, v in ((a.get_primal_solution(), b.get_primal_solution()),
+                 (a.get_dual_solution(), b.get_dual_solution())):
+        assert np.max(np.abs(u - v)) <= 1e-4 * (1.0 + np.max(np.abs(u)))
+    for tiled in (0, 1, -1):
+        s = settings(tol=1e-6, precision=1, time_limit=60)
+        s.set_parameter(lpm.CUOPT_PDLP_TILED_SWEEPS, tiled)
+        sol = lpm.Solve(dm, s)
+        assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+        assert relative_kkt(sol) <= 1e-6

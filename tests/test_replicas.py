@@ -68,15 +68,16 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch):
 
 def test_reference_arm_prints_one_contract_line():
     """`bench.py --impl reference` prints one JSON line with the contract's keys, on the small
-    2000 x 5000 workload (the oracle's FP64 PDHG iterations on the host)."""
+    2000 x 5000 workload (whole FP64 oracle solves on the host, the Optimal status and the
+    objective error against the constructed optimum recorded)."""
     import json
     import subprocess
     import sys
     from pathlib import Path
     root = Path(__file__).resolve().parents[1]
     res = subprocess.run([sys.executable, str(root / "bench.py"), "--impl", "reference",
-                          "--config", "c0", "--steps", "1", "--warmup", "1",
-                          "--cpu-seconds", "1"], capture_output=True, text=True, timeout=300,
+                          "--config", "c0", "--steps", "2", "--warmup", "1",
+                          "--reference-seconds", "60"], capture_output=True, text=True, timeout=300,
                          cwd=root, env={**os.environ, "RANK": "0", "WORLD_SIZE": "1"})
     assert res.returncode == 0, res.stderr
     lines = [l for l in res.stdout.splitlines() if l.startswith("{")]
@@ -90,3 +91,5 @@ def test_reference_arm_prints_one_contract_line():
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert "2000x5000" in d["config"]["workload"]
+    assert 1 <= d["steps"] <= 2 and d["steps_requested"] == 2 and d["dtype"] == "f64"
+    assert d["status"] == 1 and d["objective_rel_error"] < 1e-4
