@@ -21,8 +21,9 @@ iterates, FP64 termination / restart / step ratio).  The same solve in plain FP6
           alone does not bound it.
   cpu_baseline  whole FP64 oracle solves of the workload on all host threads (scaling, step size,
             termination checks, restarts; no extrapolation).
-  c0      the 2000 x 5000 LP (L2-resident, launch-bound): time to 1e-6, iterations/s and the
-          host/graph overhead per iteration beyond the two sweeps' device time.
+  c0      the 2000 x 5000 LP (L2-resident, launch-bound): time to 1e-6, iterations/s, time and
+          launches per iteration (plain iterations replay CUDA graphs), against the reference's own
+          CPU dual simplex (time-limited) and the oracle.
   batch_c3  512 seeded LPs of uneven sizes (m log-uniform in [200, 20000], n = 2.5 m,
             6-12 non-zeros per column) in one cuOptBatchSolve call, against all 512 solved one by
             one with cuOptSolve: FP64 at 1e-6 and 1e-8, mixed precision at 1e-6 and refined in
@@ -369,25 +370,38 @@ def run_c0(L, torch, device, sptr, args, O=None):
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.c0_steps
-        a, b, ba, bb = C.c_double(), C.c_double(), C.c_double(), C.c_double()
-        assert L.cuOptProfilePDHGSweeps(lp.m, lp.n, *dlp.ptrs(), sh, C.c_void_p(sptr), 200,
-                                        C.byref(a), C.byref(b), C.byref(ba), C.byref(bb)) == 0
         L.cuOptDestroySolverSettings(C.byref(sh))
         st = sts[-1][1]
         it = st["number_of_steps_taken"]
-        us_iter = 1e6 * st["loop_time"] / max(it, 1)
         out[name] = {"ms_per_solve": ms, "lps_per_s": 1000.0 / ms,
                      "pdhg_iter_per_s": it / (st["loop_time"] or 1e-9),
                      "setup_ms": 1e3 * st["setup_time"],
-                     "us_per_iteration": us_iter,
-                     "sweeps_us_per_iteration": 1e3 * (a.value + b.value),
-                     "overhead_us_per_iteration": us_iter - 1e3 * (a.value + b.value),
+                     "us_per_iteration": 1e6 * st["loop_time"] / max(it, 1),
+                     "kernel_launches_per_iteration": st["kernel_launches"] / max(it, 1),
                      **parity(lp, sts[-1], ref if name == "fp64" else None)}
     if O is not None:
         s, timed, _ = oracle_solves(lp, 3, 1, 30.0, O.max_threads())
-        out["cpu_baseline"] = {"value": 1.0 / s, "unit": UNIT, "cores": O.max_threads(),
-                               "kind": "port",
-                               "sample": f"{timed} whole FP64 oracle solves ({s * 1e3:.0f} ms each)"}
+        out["cpu_baseline_port"] = {"value": 1.0 / s, "unit": UNIT, "cores": O.max_threads(),
+                                    "kind": "port",
+                                    "sample": f"{timed} whole FP64 oracle PDLP solves "
+                                              f"({s * 1e3:.0f} ms each)"}
+        from oracle import ref_simplex as R
+        if R.available():
+            # The reference's own CPU dual simplex (solve_linear_program), compiled from its
+            # sources, under a time limit: its status, time, residual and objective error.
+            res, _ = R.solve(lp, time_limit=args.simplex_seconds,
+                             timeout=args.simplex_seconds + 120)
+            out["cpu_baseline"] = {
+                "value": (1.0 / res["solve_seconds"]) if res["status"] == "OPTIMAL" else 0.0,
+                "unit": UNIT, "cores": res["threads"], "kind": "reference",
+                "sample": f"one solve_linear_program call (the reference's CPU dual simplex) "
+                          f"with a {args.simplex_seconds:.0f} s time limit",
+                "status": res["status"], "solve_seconds": res["solve_seconds"],
+                "primal_residual": res["primal_residual"],
+                "objective_rel_error": rel_err(res["objective"], lp.optimal_objective)}
+        else:
+            out["cpu_baseline"] = {**out["cpu_baseline_port"],
+                                   "note": "oracle/_ref/ref_dual_simplex not built"}
     return out
 
 
@@ -610,6 +624,8 @@ def main():
     ap.add_argument("--fp64-warmup", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=0, help="0: as many as --steps")
     ap.add_argument("--c0-steps", type=int, default=10)
+    ap.add_argument("--simplex-seconds", type=float, default=60.0,
+                    help="c0 leg: time limit of the reference's CPU dual simplex")
     ap.add_argument("--profile-iters", type=int, default=50)
     ap.add_argument("--cpu-seconds", type=float, default=60.0,
                     help="GPU arm: time budget of the whole-solve CPU baseline")

@@ -42,6 +42,9 @@ constexpr double kPolishFeasTol  = 1e-9;
 // LSQR tolerance (atol = btol) of the active-set solves: close to FP64 resolution, so that
 // square systems are solved to the accuracy of a direct factorisation.
 constexpr double kSolveTol = 1e-14;
+// Iterative-refinement steps of the vertex polish (its vertex is returned as the solution, so it
+// is solved to FP64 resolution; the adjoint's multipliers need no refinement).
+constexpr int kPolishRefinements = 2;
 // Variables strictly inside their bounds (F) and constraints held at a bound (R) at a point x.
 struct active_set {
   std::vector<int> F, R, fpos, rpos;
@@ -231,6 +234,38 @@ struct scoped_stream {
   ~scoped_stream() { cudaStreamDestroy(s); }
 };
 
+// b - Op z with the row sums accumulated in long double (the residual of a refinement step).
+std::vector<double> residual(const lsqr_problem& q, const std::vector<double>& z)
+{
+  std::vector<double> r(q.rows);
+  for (int i = 0; i < q.rows; ++i) {
+    long double acc = q.b[i];
+    for (int64_t e = q.off[i]; e < q.off[i + 1]; ++e) acc -= (long double)q.val[e] * z[q.idx[e]];
+    r[i] = (double)acc;
+  }
+  return r;
+}
+
+std::vector<lsqr_result> solve_all(const std::vector<lsqr_problem>& sys);
+
+// `rounds` steps of iterative refinement of every solution: LSQR on the residual system, added
+// back.  Each step multiplies the error by about LSQR's relative accuracy on the system.
+void refine(const std::vector<lsqr_problem>& sys, std::vector<lsqr_result>& res, int rounds)
+{
+  for (int round = 0; round < rounds && !sys.empty(); ++round) {
+    std::vector<lsqr_problem> corr(sys.size());
+    for (size_t q = 0; q < sys.size(); ++q) {
+      corr[q]   = sys[q];
+      corr[q].b = residual(sys[q], res[q].z);
+    }
+    const std::vector<lsqr_result> d = solve_all(corr);
+    for (size_t q = 0; q < sys.size(); ++q) {
+      for (size_t j = 0; j < res[q].z.size(); ++j) res[q].z[j] += d[q].z[j];
+      if (d[q].flag == 3) res[q].flag = 3;
+    }
+  }
+}
+
 std::vector<lsqr_result> solve_all(const std::vector<lsqr_problem>& sys)
 {
   if (sys.empty()) return {};
@@ -351,7 +386,8 @@ std::vector<bool> vertex_polish_batch(const std::vector<const lp_problem*>& ps,
     P.ys = (int)sys.size();
     sys.push_back(active_operator(p, P.a, true, std::move(cF)));
   }
-  const std::vector<lsqr_result> res = solve_all(sys);
+  std::vector<lsqr_result> res = solve_all(sys);
+  refine(sys, res, kPolishRefinements);
   for (size_t t = 0; t < count; ++t) {
     prepared& P = prep[t];
     if (P.xs < 0) continue;

@@ -19,7 +19,9 @@
 #include <limits>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <random>
+#include <tuple>
 
 namespace cuopt_b200 {
 
@@ -61,6 +63,20 @@ struct loop_state {
 };
 
 class climber_engine;
+
+// Autotuning decisions of the mixed-precision sweeps, per problem shape (m, n, nnz) and device,
+// for the life of the process: (tiled primal sweep, tiled dual sweep).
+using tune_key = std::tuple<int, int, int64_t, int>;
+std::map<tune_key, std::pair<bool, bool>>& tune_cache()
+{
+  static std::map<tune_key, std::pair<bool, bool>> c;
+  return c;
+}
+std::mutex& tune_mutex()
+{
+  static std::mutex mu;
+  return mu;
+}
 
 template <typename TX>
 class engine {
@@ -580,13 +596,29 @@ class engine {
     B200_CUDA_CHECK(cudaGetDevice(&dev));
     B200_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     const size_t limit = (size_t)optin - 64;  // the two mbarriers of the static shared memory
+    // A shape tuned before in this process reuses its decision: only the tiled copies it chose
+    // are built, and nothing is timed.
+    const tune_key key{in_.m, in_.n, L_.nnz, dev};
+    bool want_a = true, want_t = true, cached = false;
+    if (p_.tiled_sweeps == -1) {
+      std::lock_guard<std::mutex> lock(tune_mutex());
+      auto it = tune_cache().find(key);
+      if (it != tune_cache().end()) {
+        cached = true;
+        want_t = it->second.first;
+        want_a = it->second.second;
+      }
+    }
+    if (cached && !want_a && !want_t) return false;
     // Worth trying only when a row block's panel copies stay within a few matrix reads.
     auto worth = [&](const tile_matrix& t, int64_t nnz) {
       return p_.tiled_sweeps == 1 || t.staging_bytes() <= 4.0 * (double)nnz * 8.0;
     };
     const int64_t nnz = L_.nnz;
-    bool have_a = build_tile_matrix(L_.A, As_.data(), sms_, limit, s_, tA_) && worth(tA_, nnz);
-    bool have_t = build_tile_matrix(L_.AT, ATs_.data(), sms_, limit, s_, tAT_) && worth(tAT_, nnz);
+    bool have_a = want_a && build_tile_matrix(L_.A, As_.data(), sms_, limit, s_, tA_) &&
+                  worth(tA_, nnz);
+    bool have_t = want_t && build_tile_matrix(L_.AT, ATs_.data(), sms_, limit, s_, tAT_) &&
+                  worth(tAT_, nnz);
     if (!have_a) tA_ = tile_matrix{};
     if (!have_t) tAT_ = tile_matrix{};
     if (!have_a && !have_t) return false;
@@ -597,7 +629,7 @@ class engine {
                            have_t ? (size_t)tAT_.groups * in_.n : 1));
     terr_.resize(1);
     terr_.zero(s_);
-    if (p_.tiled_sweeps == 1) {
+    if (p_.tiled_sweeps == 1 || cached) {
       tile_primal_ = have_t;
       tile_dual_   = have_a;
       return false;
@@ -633,6 +665,10 @@ class engine {
     check_tile_error();
     if (!tile_primal_) tAT_ = tile_matrix{};
     if (!tile_dual_) tA_ = tile_matrix{};
+    {
+      std::lock_guard<std::mutex> lock(tune_mutex());
+      tune_cache()[key] = {tile_primal_, tile_dual_};
+    }
     if (std::getenv("CUOPT_B200_TRACE"))
       std::fprintf(stderr,
                    "[cuopt_b200] sweep autotune: primal sell %.4f tiled %.4f ms -> %s; dual sell "

@@ -107,35 +107,71 @@ __global__ void __launch_bounds__(kTileThreads, 1)
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int kWarps = kTileThreads / kWarp;
+  // The first kTilePrefetch chunks of a warp in a tile are loaded one tile ahead, into registers,
+  // so their HBM latency overlaps the previous tile's work; further chunks load on demand.
+  constexpr int kTilePrefetch = 4;
+  uint32_t ck[kTilePrefetch], nk[kTilePrefetch];
+  float cv[kTilePrefetch], nv[kTilePrefetch];
+  auto prefetch = [&](int p, uint32_t(&k)[kTilePrefetch], float(&v)[kTilePrefetch]) {
+    int64_t e0 = 0, e1 = 0;
+    if (p < p1) {
+      const int64_t t = (int64_t)rb * T.panels + p;
+      e0 = T.tile_off[t];
+      e1 = T.tile_off[t + 1];
+    }
+#pragma unroll
+    for (int i = 0; i < kTilePrefetch; ++i) {
+      const int64_t e = e0 + ((int64_t)warp + (int64_t)i * kWarps) * kWarp;
+      if (e < e1) {
+        k[i] = __ldcs(T.key + e + lane);
+        v[i] = __ldcs(T.val + e + lane);
+      } else {
+        k[i] = kTilePadRow << kTileColBits;
+        v[i] = 0.0f;
+      }
+    }
+  };
+  // One 32-entry chunk: products with the panel, summed per row run, added to the row's sum.
+  auto chunk = [&](const float* panel, uint32_t kk, float v) {
+    const int r = (int)(kk >> kTileColBits);
+    if (__all_sync(0xffffffffu, r == (int)kTilePadRow)) return;  // nothing loaded into this chunk
+    float s      = v * panel[kk & ((1u << kTileColBits) - 1)];
+    const int rn = __shfl_down_sync(0xffffffffu, r, 1);
+    // Segmented inclusive sum over the chunk's row runs (rows are sorted inside a chunk), only
+    // when some row has more than one entry in it.
+    if (__any_sync(0xffffffffu, lane < 31 && rn == r)) {
+#pragma unroll
+      for (int d = 1; d < kWarp; d <<= 1) {
+        const float o = __shfl_up_sync(0xffffffffu, s, d);
+        const int ro  = __shfl_up_sync(0xffffffffu, r, d);
+        if (lane >= d && ro == r) s += o;
+      }
+    }
+    if ((lane == 31 || rn != r) && r != (int)kTilePadRow) acc[r] += s;
+  };
   bool ok = true;
+  prefetch(p0, ck, cv);
   for (int p = p0; p < p1; ++p) {
     const int k = p - p0, b = k & 1;
+    prefetch(p + 1, nk, nv);
     ok = tile_mbar_wait(&bar[b], (uint32_t)((k >> 1) & 1), err) && ok;
     const float* panel = b ? buf1 : buf0;
-    const int64_t t    = (int64_t)rb * T.panels + p;
-    const int64_t e1   = T.tile_off[t + 1];
-    for (int64_t e = T.tile_off[t] + (int64_t)warp * kWarp; e < e1; e += (int64_t)kWarps * kWarp) {
-      const uint32_t kk = __ldcs(T.key + e + lane);
-      const float v     = __ldcs(T.val + e + lane);
-      const int r       = (int)(kk >> kTileColBits);
-      float s           = v * panel[kk & ((1u << kTileColBits) - 1)];
-      const int rn      = __shfl_down_sync(0xffffffffu, r, 1);
-      // Segmented inclusive sum over the chunk's row runs (rows are sorted inside a chunk), only
-      // when some row has more than one entry in it.
-      if (__any_sync(0xffffffffu, lane < 31 && rn == r)) {
 #pragma unroll
-        for (int d = 1; d < kWarp; d <<= 1) {
-          const float o = __shfl_up_sync(0xffffffffu, s, d);
-          const int ro  = __shfl_up_sync(0xffffffffu, r, d);
-          if (lane >= d && ro == r) s += o;
-        }
-      }
-      if ((lane == 31 || rn != r) && r != (int)kTilePadRow) acc[r] += s;
-    }
+    for (int i = 0; i < kTilePrefetch; ++i) chunk(panel, ck[i], cv[i]);
+    const int64_t t  = (int64_t)rb * T.panels + p;
+    const int64_t e1 = T.tile_off[t + 1];
+    for (int64_t e = T.tile_off[t] + ((int64_t)warp + (int64_t)kTilePrefetch * kWarps) * kWarp;
+         e < e1; e += (int64_t)kWarps * kWarp)
+      chunk(panel, __ldcs(T.key + e + lane), __ldcs(T.val + e + lane));
     __syncthreads();
     if (threadIdx.x == 0 && p + 2 < p1) {
       issue(p + 2, b);
       ++(b ? issued1 : issued0);
+    }
+#pragma unroll
+    for (int i = 0; i < kTilePrefetch; ++i) {
+      ck[i] = nk[i];
+      cv[i] = nv[i];
     }
   }
   if (!ok && threadIdx.x == 0) {

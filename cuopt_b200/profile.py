@@ -273,8 +273,11 @@ def run_batch(a, models=None) -> dict:
 def _vertex_map_oracle(lp, w, h, picks, dev):
     """Exact derivatives of L = w.x* at the vertex of a vertex_lp, and central differences of the
     vertex map x*(c, b, A) (the solution of the same basis under the perturbed data) at the picked
-    coordinates.  Test oracle: a dense FP64 LU of the basis on the GPU (torch), each perturbed
-    vertex solved with it plus three steps of iterative refinement against the perturbed basis."""
+    coordinates.  Test oracle: a dense FP64 LU of the basis on the GPU (torch).  Each perturbed
+    vertex is x0 + dx, with dx solved from the perturbation itself (B' dx = r0 + d_rhs - dB x0,
+    r0 the unperturbed residual) by the LU plus three steps of iterative refinement against the
+    perturbed basis, so the difference L(+h) - L(-h) = w.(dx+ - dx-) carries no cancellation of two
+    full solves."""
     import numpy as np
     import scipy.sparse as sp
     import torch
@@ -292,45 +295,53 @@ def _vertex_map_oracle(lp, w, h, picks, dev):
     LU, piv = torch.linalg.lu_factor(B)
     solve = lambda R: torch.linalg.lu_solve(LU, piv, R)
     rhs0 = t(lp.con_lo - A[:, nonb] @ lp.x_star[nonb])
-    xB0 = solve(rhs0[:, None])[:, 0]
+    x0 = solve(rhs0[:, None])
+    for _ in range(2):
+        x0 = x0 + solve(rhs0[:, None] - B @ x0)
+    r0 = (rhs0[:, None] - B @ x0)[:, 0]
+    x0 = x0[:, 0]
     wB = t(w[basic])
     lam = torch.linalg.lu_solve(LU, piv, wB[:, None], adjoint=True)[:, 0].cpu().numpy()
     rows = np.repeat(np.arange(lp.m), np.diff(lp.row_off))
     exact = {"c": np.zeros(lp.n), "b": lam, "A": -lam[rows] * lp.x_star[lp.col_idx]}
+    x0h = x0.cpu().numpy()
+
+    def diff(cols):
+        """cols: (row i, basis position k or -1, delta d, rhs change g) per perturbed vertex;
+        returns w_B . dx for each."""
+        P = len(cols)
+        R = r0[:, None].repeat(1, P).clone()
+        ii = torch.tensor([c[0] for c in cols], device=dev, dtype=torch.int64)
+        kk = torch.tensor([max(c[1], 0) for c in cols], device=dev, dtype=torch.int64)
+        dd = torch.tensor([c[2] if c[1] >= 0 else 0.0 for c in cols], device=dev,
+                          dtype=torch.float64)
+        gg = torch.tensor([c[3] for c in cols], device=dev, dtype=torch.float64)
+        ar = torch.arange(P, device=dev)
+        R[ii, ar] += gg - dd * x0[kk]  # r0 + d_rhs - dB x0
+        X = solve(R)
+        for _ in range(3):
+            res = R - B @ X
+            res[ii, ar] -= dd * X[kk, ar]
+            X = X + solve(res)
+        return wB @ X
+
     fd = {"c": np.zeros(len(picks["c"]))}  # the vertex does not depend on c
-    # b: rhs +- h e_i (linear in b)
-    kb = picks["b"]
-    R = rhs0[:, None].repeat(1, 2 * len(kb))
-    for q, i in enumerate(kb):
-        R[i, 2 * q] += h
-        R[i, 2 * q + 1] -= h
-    L = wB @ solve(R)
+    cols = []
+    for i in picks["b"]:
+        cols += [(int(i), -1, 0.0, h), (int(i), -1, 0.0, -h)]
+    L = diff(cols)
     fd["b"] = ((L[0::2] - L[1::2]) / (2 * h)).cpu().numpy()
-    # A values: a column of N moves the right-hand side; a basic column perturbs the basis.
-    ka = picks["A"]
-    P = 2 * len(ka)
-    R = rhs0[:, None].repeat(1, P)
-    ii, kk, dd = [], [], []
-    for q, e in enumerate(ka):
+    cols = []
+    for e in picks["A"]:
         i, j = int(rows[e]), int(lp.col_idx[e])
-        for sgn, col in ((1.0, 2 * q), (-1.0, 2 * q + 1)):
+        for sgn in (1.0, -1.0):
             if pos[j] < 0:
-                R[i, col] -= sgn * h * lp.x_star[j]
-                ii.append(i), kk.append(0), dd.append(0.0)
+                cols.append((i, -1, 0.0, -sgn * h * lp.x_star[j]))
             else:
-                ii.append(i), kk.append(int(pos[j])), dd.append(sgn * h)
-    ii = torch.tensor(ii, device=dev, dtype=torch.int64)
-    kk = torch.tensor(kk, device=dev, dtype=torch.int64)
-    dd = torch.tensor(dd, device=dev, dtype=torch.float64)
-    cols = torch.arange(P, device=dev)
-    X = solve(R)
-    for _ in range(3):
-        res = R - B @ X
-        res[ii, cols] -= dd * X[kk, cols]
-        X = X + solve(res)
-    L = wB @ X
+                cols.append((i, int(pos[j]), sgn * h, 0.0))
+    L = diff(cols)
     fd["A"] = ((L[0::2] - L[1::2]) / (2 * h)).cpu().numpy()
-    return exact, fd, xB0.cpu().numpy()
+    return exact, fd, x0h
 
 
 def run_adjoint(a) -> dict:

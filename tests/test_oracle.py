@@ -395,3 +395,34 @@ def test_oracle_fixture_entries_reproduce(i):
         assert res["status"] == want["status"]
         assert res["iterations"] == want["iterations"]
         assert abs(res["primal_obj"] - want["primal_objective"]) <= 1e-12 * max(1.0, abs(want["primal_objective"]))
+
+
+_ref_missing = pytest.mark.skipif(
+    not __import__("oracle.ref_simplex", fromlist=["available"]).available(),
+    reason="oracle/_ref/ref_dual_simplex not built (make -C oracle ref REF=<reference root>)")
+
+
+@_ref_missing
+def test_reference_dual_simplex_chess_set(golden):
+    """The reference's own CPU dual simplex, compiled from its sources, reproduces the known answer
+    of its unit test (cpp/tests/dual_simplex/unit_tests/solve.cpp:86-88): 1333.33 at (0, 66.6667)."""
+    from oracle import ref_simplex as R
+    g = golden["chess_set_dual_simplex"]
+    v = oracle_view(chess_set_lp())
+    res, x = R.solve(v, maximize=bool(v.maximize))
+    assert res["status"] == "OPTIMAL"
+    assert abs(res["objective"] - g["objective"]) <= g["tol"] * abs(g["objective"])
+    assert np.allclose(x, g["x"], atol=1e-4)
+
+
+@_ref_missing
+def test_reference_dual_simplex_agrees_with_the_oracle_on_a_small_lp():
+    """On a 60 x 150 constructed LP the reference dual simplex and the FP64 PDLP oracle (1e-9)
+    reach the constructed optimum."""
+    from oracle import ref_simplex as R
+    lp = gen.constructed_lp(60, 150, 6, seed=3)
+    res, x = R.solve(lp)
+    o, _, _, _ = O.solve(lp, tol=1e-9)
+    assert res["status"] == "OPTIMAL" and o["status"] == 1
+    assert abs(res["objective"] - lp.optimal_objective) <= 1e-6 * abs(lp.optimal_objective)
+    assert abs(o["primal_obj"] - lp.optimal_objective) <= 1e-6 * abs(lp.optimal_objective)
