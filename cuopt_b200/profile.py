@@ -72,7 +72,8 @@ def main() -> None:
     ap.add_argument("--iterations", type=int, default=3)
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--time-limit", type=float, default=0.0)
-    ap.add_argument("--iteration-limit", type=int, default=0, help="climbers mode: > 0 caps iterations")
+    ap.add_argument("--iteration-limit", type=int, default=0,
+                    help="solve and climbers modes: > 0 caps iterations")
     ap.add_argument("--strong-branching", action="store_true",
                     help="climbers mode: time cuOptBatchPDLPStrongBranching instead")
     ap.add_argument("--refine", type=int, default=0, help="> 0: continue a mixed-precision solve in FP64 to 1e-8")
@@ -113,6 +114,8 @@ def main() -> None:
     L.cuOptSetParameter(s, b"log_to_console", b"false")
     if a.time_limit > 0:
         L.cuOptSetFloatParameter(s, b"time_limit", a.time_limit)
+    if a.iteration_limit > 0:
+        L.cuOptSetIntegerParameter(s, b"iteration_limit", a.iteration_limit)
     if a.refine:
         L.cuOptSetIntegerParameter(s, b"pdlp_refinement_passes", a.refine)
     stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
