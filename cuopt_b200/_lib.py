@@ -119,6 +119,8 @@ SIGNATURES = {
                                [C.POINTER(C.c_double)] * 4),
     "cuOptProfileGatherRate": (cuopt_int_t, [cuopt_int_t, C.c_int64, cuopt_int_t, C.c_void_p,
                                              C.POINTER(C.c_double), C.POINTER(cuopt_int_t)]),
+    "cuOptProfileScatterRate": (cuopt_int_t, [cuopt_int_t, C.c_int64, cuopt_int_t, C.c_void_p,
+                                              C.POINTER(C.c_double), C.POINTER(cuopt_int_t)]),
     "cuOptBatchSolve": (cuopt_int_t, [C.POINTER(handle_t), cuopt_int_t, handle_t,
                                       C.POINTER(handle_t)]),
     "cuOptSolutionAdjoint": (cuopt_int_t, [handle_t, handle_t] + [C.c_void_p] * 6),

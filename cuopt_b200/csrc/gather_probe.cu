@@ -72,6 +72,35 @@ __global__ void __launch_bounds__(kProbeBlock)
   if (lane == 0) sink[w] = acc;
 }
 
+// The scatter counterpart: each gathered index instead receives an atomic add (the result is not
+// used, so it compiles to a fire-and-forget reduction).
+template <typename T, int CHUNKS>
+__global__ void __launch_bounds__(kProbeBlock)
+  probe_scatter_kernel(const int* __restrict__ idx, int64_t rows, T* __restrict__ g,
+                       double* __restrict__ sink)
+{
+  const int lane   = threadIdx.x & 31;
+  const int64_t w  = (blockIdx.x * (int64_t)kProbeBlock + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * kProbeBlock) >> 5;
+  for (int64_t r = w * CHUNKS; r < rows; r += nw * CHUNKS) {
+    int4 ix[CHUNKS];
+#pragma unroll
+    for (int c = 0; c < CHUNKS; ++c)
+      ix[c] = r + c < rows ? __ldcs(reinterpret_cast<const int4*>(idx + ((r + c) * 32 + lane) * 4))
+                           : make_int4(0, 0, 0, 0);
+#pragma unroll
+    for (int c = 0; c < CHUNKS; ++c) {
+      if (r + c >= rows) continue;
+      atomicAdd(g + ix[c].x, (T)1);
+      atomicAdd(g + ix[c].y, (T)1);
+      atomicAdd(g + ix[c].z, (T)1);
+      atomicAdd(g + ix[c].w, (T)1);
+    }
+  }
+  (void)lane;
+  (void)sink;
+}
+
 template <typename T, int CHUNKS>
 float time_probe(const int* idx, int64_t rows, const T* g, double* sink, int grid, cudaStream_t s,
                  int repeats)
@@ -92,6 +121,47 @@ float time_probe(const int* idx, int64_t rows, const T* g, double* sink, int gri
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   return ms / repeats;
+}
+
+template <typename T, int CHUNKS>
+float time_scatter(const int* idx, int64_t rows, T* g, double* sink, int grid, cudaStream_t s,
+                   int repeats)
+{
+  cudaEvent_t a, b;
+  B200_CUDA_CHECK(cudaEventCreate(&a));
+  B200_CUDA_CHECK(cudaEventCreate(&b));
+  for (int i = 0; i < 3; ++i)
+    probe_scatter_kernel<T, CHUNKS><<<grid, kProbeBlock, 0, s>>>(idx, rows, g, sink);
+  B200_LAUNCH_CHECK();
+  B200_CUDA_CHECK(cudaEventRecord(a, s));
+  for (int i = 0; i < repeats; ++i)
+    probe_scatter_kernel<T, CHUNKS><<<grid, kProbeBlock, 0, s>>>(idx, rows, g, sink);
+  B200_CUDA_CHECK(cudaEventRecord(b, s));
+  B200_CUDA_CHECK(cudaEventSynchronize(b));
+  float ms = 0.f;
+  B200_CUDA_CHECK(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return ms / repeats;
+}
+
+template <typename T>
+double best_scatter_rate(const int* idx, int64_t rows, T* g, double* sink, int grid,
+                         cudaStream_t s, int repeats, int* best_chunks)
+{
+  const double n = (double)rows * 128.0;
+  double best    = 0.0;
+  const float t[3] = {time_scatter<T, 1>(idx, rows, g, sink, grid, s, repeats),
+                      time_scatter<T, 2>(idx, rows, g, sink, grid, s, repeats),
+                      time_scatter<T, 4>(idx, rows, g, sink, grid, s, repeats)};
+  for (int k = 0; k < 3; ++k) {
+    const double rate = n / (t[k] * 1e-3);
+    if (rate > best) {
+      best         = rate;
+      *best_chunks = 1 << k;
+    }
+  }
+  return best;
 }
 
 template <typename T>
@@ -153,6 +223,47 @@ extern "C" cuopt_int_t cuOptProfileGatherRate(cuopt_int_t vector_length, int64_t
     B200_CUDA_CHECK(cudaStreamSynchronize(s));
   } catch (const std::exception& e) {
     std::fprintf(stderr, "cuOptProfileGatherRate: %s\n", e.what());
+    return CUOPT_RUNTIME_ERROR;
+  }
+  return CUOPT_SUCCESS;
+}
+
+extern "C" cuopt_int_t cuOptProfileScatterRate(cuopt_int_t vector_length, int64_t scatters,
+                                               cuopt_int_t element_bytes, void* stream,
+                                               cuopt_float_t* scatters_per_second,
+                                               cuopt_int_t* chunks_in_flight)
+{
+  using namespace cuopt_b200;
+  if (vector_length <= 0 || scatters < 128 || !scatters_per_second || !chunks_in_flight ||
+      (element_bytes != 4 && element_bytes != 8))
+    return CUOPT_INVALID_ARGUMENT;
+  try {
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int dev = 0, sms = 148;
+    B200_CUDA_CHECK(cudaGetDevice(&dev));
+    B200_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t rows = scatters / 128;
+    const int grid     = sms * 8;
+    alloc_scope scope(s);
+    dbuf<int> idx((size_t)rows * 128);
+    dbuf<double> sink((size_t)grid * (kProbeBlock / 32));
+    probe_fill_kernel<<<sms * 8, kProbeBlock, 0, s>>>(idx.data(), rows * 128, vector_length,
+                                                       0x5eedull);
+    B200_LAUNCH_CHECK();
+    if (element_bytes == 4) {
+      dbuf<float> g(vector_length);
+      g.zero(s);
+      *scatters_per_second = best_scatter_rate<float>(idx.data(), rows, g.data(), sink.data(),
+                                                      grid, s, 10, chunks_in_flight);
+    } else {
+      dbuf<double> g(vector_length);
+      g.zero(s);
+      *scatters_per_second = best_scatter_rate<double>(idx.data(), rows, g.data(), sink.data(),
+                                                       grid, s, 10, chunks_in_flight);
+    }
+    B200_CUDA_CHECK(cudaStreamSynchronize(s));
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "cuOptProfileScatterRate: %s\n", e.what());
     return CUOPT_RUNTIME_ERROR;
   }
   return CUOPT_SUCCESS;

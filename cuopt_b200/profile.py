@@ -176,9 +176,20 @@ def run_gather(a) -> dict:
     nnz = n * k if k else 75_000_000
     stream = C.c_void_p(torch.cuda.current_stream(torch.device("cuda", 0)).cuda_stream)
     res = gather_rates(m, n, nnz, stream)
+    from cuopt_b200._lib import lib
+    L = lib()
+    for name, length in (("primal_scatter_y", m), ("dual_scatter_ax", m)):
+        for eb in (4, 8):
+            rate, chunks = C.c_double(), C.c_int32()
+            if L.cuOptProfileScatterRate(length, 4 * nnz, eb, stream, C.byref(rate),
+                                         C.byref(chunks)) != 0:
+                raise RuntimeError("cuOptProfileScatterRate failed")
+            res[f"{name}_fp{8 * eb}"] = {"scatters_per_s": rate.value,
+                                          "chunks_in_flight": chunks.value}
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     for v in res.values():
-        v["per_sm_per_cycle_at_1965mhz"] = v["gathers_per_s"] / sms / 1.965e9
+        rate = v.get("gathers_per_s", v.get("scatters_per_s"))
+        v["per_sm_per_cycle_at_1965mhz"] = rate / sms / 1.965e9
     return {"config": a.config, "m": m, "n": n, "gathers": 4 * nnz, "sms": sms, "rates": res}
 
 

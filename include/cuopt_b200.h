@@ -72,6 +72,18 @@ cuopt_int_t cuOptSolveDevice(cuopt_int_t num_constraints,
                              cuOptPDLPStatistics* stats,
                              cuopt_int_t* termination_status);
 
+/* Measurement hook (no counterpart in the reference): the same index stream as
+ * cuOptProfileGatherRate, but every index receives an atomic add whose result is unused (a
+ * fire-and-forget reduction into the vector), with 1, 2 and 4 chunks in flight.  Returns the best
+ * rate in reductions per second: the rate a sweep that scatters its products instead of gathering
+ * its operand would face. */
+cuopt_int_t cuOptProfileScatterRate(cuopt_int_t vector_length,
+                                    int64_t scatters,
+                                    cuopt_int_t element_bytes,
+                                    void* stream,
+                                    cuopt_float_t* scatters_per_second,
+                                    cuopt_int_t* chunks_in_flight);
+
 /* Measurement hook (no counterpart in the reference): the random-gather ceiling of the device.
  * Streams `gathers` random int32 indices into a vector of `vector_length` elements of
  * `element_bytes` (4 or 8) bytes, in the sliced-ELL sweeps' chunk shape (a warp reads 32 lanes x 4
