@@ -206,6 +206,25 @@ def solve_device(L, dlp, settings, stream_ptr):
     return status.value, {f: getattr(st, f) for f, _ in PDLPStatistics._fields_}
 
 
+def form_info(st):
+    """The form of the plain iterations a solve used and the cycle timings the choice was made on
+    (pdlp_persistent_iterations = -1: CUDA graphs against the persistent cooperative kernel)."""
+    return {"form": {0: "graphs", 1: "persistent"}.get(st["plain_iteration_form"], "undecided"),
+            "persistent_blocks": st["persistent_blocks"],
+            "us_per_iteration_graphs": st["plain_iteration_us_graphs"],
+            "us_per_iteration_persistent": st["plain_iteration_us_persistent"]}
+
+
+def grid_barrier_costs(L):
+    """Microseconds per grid barrier of the persistent kernel, alone (cuOptProbeGridBarrier)."""
+    out = {}
+    for blocks in (20, 148, 296, 740):
+        st, ms = C.c_int32(), C.c_double()
+        if L.cuOptProbeGridBarrier(blocks, 2000, 0, 5000.0, None, C.byref(st), C.byref(ms)) == 0:
+            out[str(blocks)] = 1e3 * ms.value / 2000 if st.value == 0 else None
+    return out
+
+
 def solve_e2e(L, lp, pinned, settings):
     """One solve through the reference-compatible C API from (pinned) host buffers."""
     h = C.c_void_p()
@@ -378,6 +397,7 @@ def run_c0(L, torch, device, sptr, args, O=None):
                      "setup_ms": 1e3 * st["setup_time"],
                      "us_per_iteration": 1e6 * st["loop_time"] / max(it, 1),
                      "kernel_launches_per_iteration": st["kernel_launches"] / max(it, 1),
+                     "iteration_loop": form_info(st),
                      **parity(lp, sts[-1], ref if name == "fp64" else None)}
     if O is not None:
         s, timed, _ = oracle_solves(lp, 3, 1, 30.0, O.max_threads())
@@ -599,6 +619,7 @@ def run_b200(args):
         "objective_bound": "1e-6 relative KKT does not bound the objective error by 1e-6 (the "
                            "oracle itself is 6.8e-6 off on batch instance 284 at 1e-6); the legs "
                            "refined to 1e-8 are the ones held to 1e-6",
+        "iteration_loop": {**form_info(last_mixed), "grid_barrier_us": grid_barrier_costs(L)},
         "c0": c0, "batch_c3": batch, "batch_c3_mixed": batch_mixed, "adjoint_c4": adjoint,
         "roofline": roofline, "cpu_baseline": cpu,
         "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT,

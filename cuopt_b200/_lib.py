@@ -43,6 +43,10 @@ class PDLPStatistics(C.Structure):
         ("loop_time", cuopt_float_t),
         ("kernel_launches", cuopt_float_t),
         ("crossover", cuopt_int_t),
+        ("plain_iteration_form", cuopt_int_t),
+        ("persistent_blocks", cuopt_int_t),
+        ("plain_iteration_us_graphs", cuopt_float_t),
+        ("plain_iteration_us_persistent", cuopt_float_t),
     ]
 
 
@@ -121,6 +125,9 @@ SIGNATURES = {
                                              C.POINTER(C.c_double), C.POINTER(cuopt_int_t)]),
     "cuOptProfileScatterRate": (cuopt_int_t, [cuopt_int_t, C.c_int64, cuopt_int_t, C.c_void_p,
                                               C.POINTER(C.c_double), C.POINTER(cuopt_int_t)]),
+    "cuOptProbeGridBarrier": (cuopt_int_t, [cuopt_int_t, cuopt_int_t, cuopt_int_t, C.c_double,
+                                            C.c_void_p, C.POINTER(cuopt_int_t),
+                                            C.POINTER(C.c_double)]),
     "cuOptBatchSolve": (cuopt_int_t, [C.POINTER(handle_t), cuopt_int_t, handle_t,
                                       C.POINTER(handle_t)]),
     "cuOptSolutionAdjoint": (cuopt_int_t, [handle_t, handle_t] + [C.c_void_p] * 6),

@@ -18,6 +18,7 @@
 #include "kernels.cuh"
 #include "pdlp_engine.hpp"
 #include "pdlp_schedule.hpp"
+#include "plain_form.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -632,11 +633,13 @@ class batch_engine {
     B200_CUDA_CHECK(cudaGetDevice(&dev));
     B200_CUDA_CHECK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
     B200_CUDA_CHECK(cudaMallocHost(&hbuf_, sizeof(double) * 8 * (size_t)std::max(B_, 1)));
+    B200_CUDA_CHECK(cudaMallocHost(&hstatus_, sizeof(int)));
   }
   ~batch_engine()
   {
     for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
     cudaFreeHost(hbuf_);
+    cudaFreeHost(hstatus_);
   }
 
   std::vector<pdlp_result> run(double* x_out, double* y_out, double* rc_out)
@@ -645,6 +648,7 @@ class batch_engine {
     t_start_ = now_s();
     results_.assign(B_, pdlp_result{});
     setup();
+    init_plain_form(B_);
     t_loop_ = now_s();
     loop();
     trace("batch: loop");
@@ -655,6 +659,10 @@ class batch_engine {
       results_[b].loop_time       = results_[b].solve_time - (t_loop_ - t_start_);
       results_[b].kernel_launches = launches_;
       results_[b].power_iterations = power_iters_[b];
+      results_[b].plain_form          = first_form_;
+      results_[b].persistent_blocks   = first_blocks_;
+      results_[b].us_plain_graphs     = first_us_[0];
+      results_[b].us_plain_persistent = first_us_[1];
     }
     (void)t;
     return results_;
@@ -906,7 +914,18 @@ class batch_engine {
   {
     B200_CUDA_CHECK(cudaMemcpyAsync(dst, segout_.data() + offset, count * sizeof(double),
                                     cudaMemcpyDeviceToHost, s_));
+    if (persist_used_)
+      B200_CUDA_CHECK(cudaMemcpyAsync(hstatus_, &pctl_.data()->status, sizeof(int),
+                                      cudaMemcpyDeviceToHost, s_));
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    if (persist_used_) {
+      persist_used_ = false;
+      if (*hstatus_ != 0)
+        throw cuda_error(*hstatus_ == kBarrierTimedOut
+                           ? "persistent batch iterations: a grid barrier passed its deadline"
+                           : "persistent batch iterations: a grid barrier passed its poll limit");
+    }
+    collect_form_timing();
   }
 
   void prepare_vectors()
@@ -1220,11 +1239,13 @@ class batch_engine {
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
     lists_on_ = true;
     drop_graphs();
+    init_plain_form((int)std::count(act.begin(), act.end(), 1));
   }
   void clear_work()
   {
     lists_on_ = false;
     drop_graphs();
+    init_plain_form(B_);
   }
   void drop_graphs()
   {
@@ -1273,8 +1294,110 @@ class batch_engine {
     }
     advance(L);
   }
-  void run_plain(long R)
+  // ---------------------------------------------------------------- persistent plain iterations
+  // The same choice as for single solves (plain_form.hpp), made again for every work list: the
+  // sweeps shrink as instances finish, and the cost of kernel boundaries grows relative to them.
+  using persist_pe = b_primal_epi<TX, false, true, false>;
+  using persist_de = b_dual_epi<TX, false, true, false>;
+  static const void* persistent_fn()
   {
+    return (const void*)persistent_plain_kernel<TX, persist_pe, persist_de, advance_active>;
+  }
+  void init_plain_form(int n_active)
+  {
+    int dev = 0, coop = 0, per_sm = 0;
+    B200_CUDA_CHECK(cudaGetDevice(&dev));
+    B200_CUDA_CHECK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    B200_CUDA_CHECK(
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_fn(), kBlock, 0));
+    const int need = std::max(sell_grid(wview<TX>(false, ATs_.data())),
+                              sell_grid(wview<TX>(true, As_.data())));
+    persist_grid_  = std::min(need, per_sm * sms_);
+    if (pctl_.size() == 0) {
+      pctl_.resize(1);
+      pctl_.zero(s_);
+    }
+    form_active_ = n_active;
+    cycle_open_  = false;
+    ++form_epochs_;
+    form_.reset(p_.persistent, -1, coop && persist_grid_ > 0);
+    if (n_active == B_ && form_.decided()) {  // forced (or the only form available)
+      first_form_   = form_.chosen();
+      first_blocks_ = persist_grid_;
+    }
+  }
+  void trace_form()
+  {
+    if (form_active_ == B_ && first_form_ < 0) {
+      first_form_    = form_.chosen();
+      first_us_[0]   = form_.us_per_iteration(0);
+      first_us_[1]   = form_.us_per_iteration(1);
+      first_blocks_  = persist_grid_;
+    }
+    if (std::getenv("CUOPT_B200_TRACE"))
+      std::fprintf(stderr,
+                   "[cuopt_b200] batch plain iterations (%d instances): graphs %.2f us, "
+                   "persistent (%d blocks) %.2f us per iteration -> %s\n",
+                   form_active_, form_.us_per_iteration(0), persist_grid_,
+                   form_.us_per_iteration(1), form_.chosen() ? "persistent" : "graphs");
+  }
+  void collect_form_timing()
+  {
+    const bool before = form_.decided();
+    form_.collect();
+    if (!before && form_.decided()) trace_form();
+  }
+  // Returns true for the first launch of the engine (which may include loading the kernel).
+  bool launch_persistent(int L)
+  {
+    const auto AT = wview<TX>(false, ATs_.data()), A = wview<TX>(true, As_.data());
+    persist_pe pe{x_.data(),   cs_.data(),   ls_.data(),    us_.data(),  xa_.data(),
+                  xbar_.data(), x_.data(),   xhat_.data(),  slack_.data(), aty_.data(),
+                  ctx_cols(),  0};
+    persist_de de{y_.data(),    lcs_.data(),  ucs_.data(),    ya_.data(), ybar_.data(),
+                  y_.data(),    yhat_.data(), rowbuf_.data(), ctx_rows(), 0};
+    advance_active adv{sc_d_.data(), active_d_.data(), B_};
+    int gp = sell_grid(AT), gd = sell_grid(A);
+    const TX* y    = y_.data();
+    const TX* xb   = xbar_.data();
+    persist_ctl* c = pctl_.data();
+    unsigned long long budget = kPersistBudgetNs;
+    B200_CUDA_CHECK(cudaMemsetAsync(&c->arrivals, 0, sizeof(unsigned), s_));
+    void* args[] = {(void*)&AT, (void*)&A, (void*)&y, (void*)&xb, (void*)&pe, (void*)&de,
+                    (void*)&adv, (void*)&L, (void*)&gp, (void*)&gd, (void*)&c, (void*)&budget};
+    B200_CUDA_CHECK(cudaLaunchCooperativeKernel(persistent_fn(), dim3(persist_grid_),
+                                                dim3(kBlock), args, 0, s_));
+    ++launches_;
+    persist_used_ = true;
+    return persist_launches_++ == 0;
+  }
+
+  // A timing cycle runs from the first plain run after a termination check to the next check:
+  // all its plain runs use one form, and its events bracket everything the GPU does in between
+  // (major steps, fixed-point errors and every launch boundary), so the forms are compared on
+  // what they cost the loop.
+  void run_plain(long R, long k)
+  {
+    if (!cycle_open_) {
+      cycle_form_     = form_.next();
+      cycle_k0_       = k;
+      cycle_one_time_ = false;
+      cycle_open_     = true;
+      form_.begin(s_);
+    }
+    cycle_one_time_ |= cycle_form_ == 1 ? launch_persistent((int)R) : run_graphs(R);
+  }
+  void close_cycle(long k)
+  {
+    if (!cycle_open_) return;
+    cycle_open_ = false;
+    form_.end(s_, cycle_form_, k - cycle_k0_, cycle_one_time_);
+  }
+
+  // Returns true when a graph had to be captured and instantiated first.
+  bool run_graphs(long R)
+  {
+    bool built = false;
     for (int L = 128; L >= 1; L >>= 1) {
       while (R >= L) {
         auto it = graphs_.find(L);
@@ -1289,12 +1412,14 @@ class batch_engine {
           B200_CUDA_CHECK(cudaGraphInstantiate(&e, g, 0));
           cudaGraphDestroy(g);
           it = graphs_.emplace(L, e).first;
+          built = true;
         }
         B200_CUDA_CHECK(cudaGraphLaunch(it->second, s_));
         launches_ += 2.0 * L + 1.0;
         R -= L;
       }
     }
+    return built;
   }
 
   void upload_scalars(const std::vector<long>& since)
@@ -1393,6 +1518,7 @@ class batch_engine {
       std::fill(restarted.begin(), restarted.end(), 0);
       bool any_restart = false;
       if (major || cond) {
+        close_cycle(k);
         const std::vector<inst_conv> cv = evaluate();
         const bool out_of_time = now_s() - t_start_ >= p_.time_limit;
         for (int b = 0; b < B_; ++b) {
@@ -1509,7 +1635,7 @@ class batch_engine {
           if (is_check(kk) || is_major_step(kk) || ((kk + 1) % kMajor == 0)) break;
           ++R;
         }
-        run_plain(R);
+        run_plain(R, k);
         k += R;
         for (int b = 0; b < B_; ++b)
           if (active_h_[b]) since[b] += R;
@@ -1607,6 +1733,20 @@ class batch_engine {
   bool lists_on_ = false;
   chunk_table rows_, cols_;
   dbuf<double> chunk_part_;
+  // Persistent plain iterations: control block, grid, the choice of form for the current work
+  // list, and the choice made while every instance ran (reported in the results).
+  dbuf<persist_ctl> pctl_;
+  int* hstatus_      = nullptr;
+  bool cycle_open_ = false, cycle_one_time_ = false;
+  int cycle_form_  = 0;
+  long cycle_k0_   = 0;
+  int persist_grid_  = 0;
+  bool persist_used_ = false;
+  long persist_launches_ = 0;
+  plain_form_tuner form_;
+  int form_active_ = 0, form_epochs_ = 0;
+  int first_form_ = -1, first_blocks_ = 0;
+  double first_us_[2] = {0, 0};
 };
 
 

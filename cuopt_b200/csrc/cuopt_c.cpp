@@ -716,6 +716,10 @@ cuopt_int_t cuOptGetPDLPStatistics(cuOptSolution solution, cuOptPDLPStatistics* 
   st->loop_time                       = r.loop_time;
   st->kernel_launches                 = r.kernel_launches;
   st->crossover                       = r.crossover ? 1 : 0;
+  st->plain_iteration_form            = r.plain_form;
+  st->persistent_blocks               = r.persistent_blocks;
+  st->plain_iteration_us_graphs       = r.us_plain_graphs;
+  st->plain_iteration_us_persistent   = r.us_plain_persistent;
   return CUOPT_SUCCESS;
 }
 

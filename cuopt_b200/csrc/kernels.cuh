@@ -195,10 +195,23 @@ __device__ __forceinline__ bool skip_rows(const Epi& epi, int r0, int r1)
 // Generic fused sweep: acc_r = sum_k A[r,k] * g[idx[r,k]], then epi(r, acc_r, pre, red).
 // The epilogue's per-row operands (`pre`) are loaded before the matrix loop so their memory latency
 // overlaps the gathers.  Sliced rows are read in 4-element lane chunks, two chunks in flight.
-template <typename TM, typename TG, class Epi>
-__global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
-                                                          const TG* __restrict__ g, Epi epi,
-                                                          double* partials)
+// `vb` is the block's index in the sweep's grid (blockIdx.x, or a virtual index in a persistent
+// kernel that walks the grid).
+// Gathered-vector loads.  A kernel that writes the gathered vector itself (the persistent
+// iterations below) reads it through L2 (ld.global.cg), which its grid barrier keeps coherent;
+// every other sweep may use the read-only path.
+template <bool COH, typename T>
+__device__ __forceinline__ T gather_load(const T* __restrict__ g, int i)
+{
+  if constexpr (COH)
+    return __ldcg(g + i);
+  else
+    return g[i];
+}
+
+template <typename TM, typename TG, class Epi, bool COH = false>
+__device__ __forceinline__ void sell_map_block(const dev_sell<TM>& A, const TG* __restrict__ g,
+                                               const Epi& epi, double* partials, int vb)
 {
   constexpr int K = Epi::kRed;
   red_t<K> red;
@@ -206,25 +219,25 @@ __global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
   for (int q = 0; q < (K > 0 ? K : 1); ++q) red.v[q] = 0.0;
   if (epi.skip()) {
     // Uniform early exit (e.g. converged power iteration): every block still stores zeros.
-    block_reduce_store<K, has_max_red<Epi>::value>(red, partials);
+    block_reduce_store<K, has_max_red<Epi>::value>(red, partials, vb);
     return;
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int lb   = long_blocks(A.long_count());
-  if ((int)blockIdx.x < lb) {
-    const int q   = blockIdx.x * kWarpsPerBlock + warp;
+  if (vb < lb) {
+    const int q   = vb * kWarpsPerBlock + warp;
     const int row = q < A.long_count() ? (A.long_list ? A.long_list[q] : q) : 0;
     if (q < A.long_count() && !skip_rows(epi, row, row)) {
       const auto pre  = epi.load(row);
       const int64_t b = A.long_off[row], e = A.long_off[row + 1];
       double acc      = 0.0;
       for (int64_t k = b + lane; k < e; k += kWarp)
-        acc += (double)ld_stream(A.val + k) * (double)g[ld_stream(A.idx + k)];
+        acc += (double)ld_stream(A.val + k) * (double)gather_load<COH>(g, ld_stream(A.idx + k));
       acc = warp_sum(acc);
       if (lane == 0) epi(row, acc, pre, red);
     }
   } else {
-    const int q = (blockIdx.x - lb) * kWarpsPerBlock + warp;
+    const int q = (vb - lb) * kWarpsPerBlock + warp;
     const int s = q < A.slice_count() ? (A.slice_list ? A.slice_list[q] : q) : 0;
     if (q < A.slice_count() &&
         !skip_rows(epi, A.n_long + s * kWarp, min(A.n_long + s * kWarp + kWarp, A.rows) - 1)) {
@@ -242,8 +255,10 @@ __global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
         double v0[4], v1[4];
         load_chunk(v, v0);
         load_chunk(v + 32 * kChunk, v1);
-        const TG g0 = g[i0.x], g1 = g[i0.y], g2 = g[i0.z], g3 = g[i0.w];
-        const TG g4 = g[i1.x], g5 = g[i1.y], g6 = g[i1.z], g7 = g[i1.w];
+        const TG g0 = gather_load<COH>(g, i0.x), g1 = gather_load<COH>(g, i0.y);
+        const TG g2 = gather_load<COH>(g, i0.z), g3 = gather_load<COH>(g, i0.w);
+        const TG g4 = gather_load<COH>(g, i1.x), g5 = gather_load<COH>(g, i1.y);
+        const TG g6 = gather_load<COH>(g, i1.z), g7 = gather_load<COH>(g, i1.w);
         acc += v0[0] * (double)g0;
         acc += v0[1] * (double)g1;
         acc += v0[2] * (double)g2;
@@ -259,7 +274,8 @@ __global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
         const int4 i0 = load_idx_chunk(ix);
         double v0[4];
         load_chunk(v, v0);
-        const TG g0 = g[i0.x], g1 = g[i0.y], g2 = g[i0.z], g3 = g[i0.w];
+        const TG g0 = gather_load<COH>(g, i0.x), g1 = gather_load<COH>(g, i0.y);
+        const TG g2 = gather_load<COH>(g, i0.z), g3 = gather_load<COH>(g, i0.w);
         acc += v0[0] * (double)g0;
         acc += v0[1] * (double)g1;
         acc += v0[2] * (double)g2;
@@ -268,7 +284,152 @@ __global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
       if (valid) epi(row, acc, pre, red);
     }
   }
-  block_reduce_store<K, has_max_red<Epi>::value>(red, partials);
+  block_reduce_store<K, has_max_red<Epi>::value>(red, partials, vb);
+}
+
+template <typename TM, typename TG, class Epi>
+__global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
+                                                          const TG* __restrict__ g, Epi epi,
+                                                          double* partials)
+{
+  sell_map_block(A, g, epi, partials, (int)blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Persistent plain iterations: one cooperative launch runs L primal / dual sweep pairs with a
+// grid-wide barrier after each sweep, instead of 2L kernel nodes of a CUDA graph.  Block b takes
+// the sweep's virtual blocks b, b + gridDim.x, ... in both sweeps of every iteration, so each row's
+// own iterates are read back by the thread that wrote them; the gathered vectors, written by other
+// blocks, are read through L2.
+//
+// Every wait is bounded: a barrier that is not reached before the launch's deadline (read from
+// %globaltimer) or within kBarrierPolls polls stores a status in the control block and every block
+// returns; the host reads the status at its next synchronisation and fails the solve.
+
+struct persist_ctl {
+  unsigned arrivals;  // barrier arrivals of the current launch (zeroed before each launch)
+  int status;         // 0, or kBarrierTimedOut / kBarrierPollLimit
+};
+constexpr int kBarrierTimedOut  = 1;
+constexpr int kBarrierPollLimit = 2;
+constexpr unsigned kBarrierPolls = 1u << 24;
+// Deadline of one persistent launch of the solvers (at most 255 iterations): far above any
+// legitimate run, it only bounds a launch whose grid barrier could not complete.
+constexpr unsigned long long kPersistBudgetNs = 30ull * 1000 * 1000 * 1000;
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p)
+{
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void red_release_gpu_add(unsigned* p, unsigned v)
+{
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_relaxed_gpu(const int* p)
+{
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Arrive and wait until `target` arrivals have been counted.  Returns false (uniformly across
+// the block) when the wait gave up or another block's wait already had.  The block's writes reach
+// thread 0 through the block barrier; its arrival is a release at GPU scope (cumulative over
+// them), and the poll that sees the last arrival an acquire, after which the block barrier hands
+// the other blocks' writes on to every thread.
+__device__ __forceinline__ bool persist_barrier(persist_ctl* c, unsigned target,
+                                                unsigned long long deadline)
+{
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    red_release_gpu_add(&c->arrivals, 1u);
+    int st = 0;
+    for (unsigned polls = 0;; ++polls) {
+      if (ld_acquire_gpu(&c->arrivals) >= target) break;
+      if ((st = ld_relaxed_gpu(&c->status)) != 0) break;
+      if (polls >= kBarrierPolls) {
+        st = kBarrierPollLimit;
+        atomicCAS(&c->status, 0, st);
+        break;
+      }
+      if ((polls & 15) == 15 && global_ns() > deadline) {
+        st = kBarrierTimedOut;
+        atomicCAS(&c->status, 0, st);
+        break;
+      }
+    }
+    ok = st == 0;
+  }
+  __syncthreads();
+  return ok;
+}
+
+// Block 0's closing step of a persistent launch (after the last barrier): the iteration counter
+// of the one LP, or of every active instance of a batch, moves on by L.
+struct advance_one {
+  pdlp_scalars* st;
+  __device__ void operator()(int steps) const
+  {
+    if (threadIdx.x == 0) st->t0 += steps;
+  }
+};
+struct advance_active {
+  pdlp_scalars* sc;
+  const int* active;
+  int count;
+  __device__ void operator()(int steps) const
+  {
+    for (int b = threadIdx.x; b < count; b += blockDim.x)
+      if (active[b]) sc[b].t0 += steps;
+  }
+};
+
+template <typename TX, class PE, class DE, class ADV>
+__global__ void __launch_bounds__(kBlock)
+  persistent_plain_kernel(const dev_sell<TX> AT, const dev_sell<TX> A, const TX* y, const TX* xbar,
+                          PE pe, DE de, ADV adv, int L, int grid_p, int grid_d, persist_ctl* ctl,
+                          unsigned long long budget_ns)
+{
+  const unsigned long long deadline = global_ns() + budget_ns;
+  unsigned target                   = 0;
+  for (int i = 0; i < L; ++i) {
+    pe.it_off = i;
+    for (int vb = blockIdx.x; vb < grid_p; vb += gridDim.x)
+      sell_map_block<TX, TX, PE, true>(AT, y, pe, nullptr, vb);
+    target += gridDim.x;
+    if (!persist_barrier(ctl, target, deadline)) return;
+    de.it_off = i;
+    for (int vb = blockIdx.x; vb < grid_d; vb += gridDim.x)
+      sell_map_block<TX, TX, DE, true>(A, xbar, de, nullptr, vb);
+    target += gridDim.x;
+    if (!persist_barrier(ctl, target, deadline)) return;
+  }
+  if (blockIdx.x == 0) adv(L);
+}
+
+// The barrier alone, for measuring its cost and for checking that a wait which cannot complete
+// (`unreachable` > 0 asks for more arrivals than the grid has blocks) ends with a status instead
+// of hanging: `rounds` barriers, then block 0 records the elapsed nanoseconds.
+static __global__ void persist_barrier_probe_kernel(persist_ctl* ctl, int rounds, unsigned unreachable,
+                                                    unsigned long long budget_ns,
+                                                    unsigned long long* elapsed)
+{
+  const unsigned long long t0 = global_ns(), deadline = t0 + budget_ns;
+  unsigned target = 0;
+  for (int r = 0; r < rounds; ++r) {
+    target += gridDim.x;
+    if (!persist_barrier(ctl, target + unreachable, deadline)) break;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *elapsed = global_ns() - t0;
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -115,6 +115,8 @@ lp_settings::lp_settings()
     {CUOPT_PDLP_REFINEMENT_PASSES, 0, 64, 0},
     {CUOPT_PDLP_TILED_SWEEPS, CUOPT_PDLP_TILED_SWEEPS_AUTO, CUOPT_PDLP_TILED_SWEEPS_ON,
      CUOPT_PDLP_TILED_SWEEPS_AUTO},
+    {CUOPT_PDLP_PERSISTENT_ITERATIONS, CUOPT_PDLP_PERSISTENT_ITERATIONS_AUTO,
+     CUOPT_PDLP_PERSISTENT_ITERATIONS_ON, CUOPT_PDLP_PERSISTENT_ITERATIONS_AUTO},
   };
   bparams = {
     {CUOPT_INFEASIBILITY_DETECTION, false}, {CUOPT_STRICT_INFEASIBILITY, false},
@@ -412,6 +414,7 @@ pdlp_params params_from_settings(const lp_settings& st)
   prm.refinement_passes = st.i(CUOPT_PDLP_REFINEMENT_PASSES);
   prm.refinement_tol    = st.f(CUOPT_PDLP_REFINEMENT_TOLERANCE);
   prm.tiled_sweeps      = st.i(CUOPT_PDLP_TILED_SWEEPS);
+  prm.persistent        = st.i(CUOPT_PDLP_PERSISTENT_ITERATIONS);
   prm.log_to_console    = st.b(CUOPT_LOG_TO_CONSOLE);
   prm.detect_infeasibility  = st.b(CUOPT_INFEASIBILITY_DETECTION);
   prm.per_constraint_residual = st.b(CUOPT_PER_CONSTRAINT_RESIDUAL);

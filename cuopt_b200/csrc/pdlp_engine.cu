@@ -4,18 +4,21 @@
 // (cpp/src/pdlp/pdlp.cu:2013-2457).  The host keeps the scalar state that the reference keeps on
 // the host (restart decision, PID primal weight, fixed-point errors); all vector and matrix work
 // is in the kernels of kernels.cuh.  Iterations that need neither a termination test, a "major"
-// step nor a fixed-point error are replayed from cached CUDA graphs of 2^k iterations.
+// step nor a fixed-point error are replayed from cached CUDA graphs of 2^k iterations, or run by one
+// persistent cooperative launch, whichever form timed faster on the solve's first runs.
 #include "device_layout.cuh"
 #include "host_io.hpp"
 #include "kernels.cuh"
 #include "pdlp_engine.hpp"
 #include "pdlp_schedule.hpp"
+#include "plain_form.hpp"
 #include "tile_sweep.cuh"
 
 #include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <limits>
 #include <map>
 #include <memory>
@@ -76,6 +79,19 @@ std::mutex& tune_mutex()
 {
   static std::mutex mu;
   return mu;
+}
+// Form of the plain iterations (0 CUDA graphs, 1 persistent kernel) chosen by timing, per problem
+// shape (m, n, nnz), device and iterate precision (bytes), for the life of the process.
+// The timings it was chosen by are kept with it (microseconds per plain iteration).
+using form_key = std::tuple<int, int, int64_t, int, int>;
+struct form_choice {
+  int form;
+  double us_graphs, us_persistent;
+};
+std::map<form_key, form_choice>& form_cache()
+{
+  static std::map<form_key, form_choice> c;
+  return c;
 }
 
 template <typename TX>
@@ -234,6 +250,7 @@ class engine {
       if (tune_tiles()) reset_iterates(true);  // the timed sweeps moved the iterates
       trace("engine: sweep autotuning");
     }
+    init_plain_form();
   }
 
   // Takes the precision-independent state of another engine over (see continue_from).
@@ -296,6 +313,7 @@ class engine {
     launches_ += 7;
     B200_LAUNCH_CHECK();
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    init_plain_form();
   }
 
   // Norms of the unscaled vectors and their scaled copies in the iterate precision (bound /
@@ -715,8 +733,116 @@ class engine {
     ++launches_;
   }
 
-  void run_plain(long R)
+  // ------------------------------------------------------------------ persistent plain iterations
+  using persist_pe = primal_epi<TX, false, true, false>;
+  using persist_de = dual_epi<TX, false, true, false>;
+  static const void* persistent_fn()
   {
+    return (const void*)persistent_plain_kernel<TX, persist_pe, persist_de, advance_one>;
+  }
+
+  // Sizes the persistent launch (all co-resident blocks, at most one per virtual block of the
+  // larger sweep) and sets up the choice of form for this solve.
+  void init_plain_form()
+  {
+    int dev = 0, coop = 0, per_sm = 0;
+    B200_CUDA_CHECK(cudaGetDevice(&dev));
+    B200_CUDA_CHECK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    B200_CUDA_CHECK(
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_fn(), kBlock, 0));
+    const int need = std::max(sell_grid(ATs_view()), sell_grid(As_view()));
+    persist_grid_  = std::min(need, per_sm * sms_);
+    // The persistent kernel runs the sliced-ELL sweeps only.
+    const bool ok = coop && persist_grid_ > 0 && !tile_primal_ && !tile_dual_;
+    pctl_.resize(1);
+    pctl_.zero(s_);
+    form_key_     = form_key{in_.m, in_.n, L_.nnz, dev, (int)sizeof(TX)};
+    int known     = -1;
+    form_us_[0] = form_us_[1] = 0.0;
+    if (p_.persistent == -1) {
+      std::lock_guard<std::mutex> lock(tune_mutex());
+      auto it = form_cache().find(form_key_);
+      if (it != form_cache().end()) {
+        known       = it->second.form;
+        form_us_[0] = it->second.us_graphs;
+        form_us_[1] = it->second.us_persistent;
+      }
+    }
+    cycle_open_ = false;
+    form_.reset(p_.persistent, known, ok);
+  }
+
+  // Returns true for the first launch of the engine (which may include loading the kernel).
+  bool launch_persistent(int L)
+  {
+    const auto AT = ATs_view(), A = As_view();
+    persist_pe pe{x_.data(),   cs_.data(),   ls_.data(),    us_.data(),  xa_.data(),
+                  xbar_.data(), x_.data(),   xhat_.data(),  slack_.data(), aty_.data(),
+                  scalars_.data(), 0};
+    persist_de de{y_.data(),    lcs_.data(), ucs_.data(),  ya_.data(),      ybar_.data(),
+                  y_.data(),    yhat_.data(), scalars_.data(), 0};
+    advance_one adv{scalars_.data()};
+    int gp = sell_grid(AT), gd = sell_grid(A);
+    const TX* y    = y_.data();
+    const TX* xb   = xbar_.data();
+    persist_ctl* c = pctl_.data();
+    unsigned long long budget = kPersistBudgetNs;
+    B200_CUDA_CHECK(cudaMemsetAsync(&c->arrivals, 0, sizeof(unsigned), s_));
+    void* args[] = {(void*)&AT, (void*)&A, (void*)&y, (void*)&xb, (void*)&pe, (void*)&de,
+                    (void*)&adv, (void*)&L, (void*)&gp, (void*)&gd, (void*)&c, (void*)&budget};
+    B200_CUDA_CHECK(cudaLaunchCooperativeKernel(persistent_fn(), dim3(persist_grid_),
+                                                dim3(kBlock), args, 0, s_));
+    ++launches_;
+    return persist_launches_++ == 0;
+  }
+
+  // After a synchronisation: timings of the forms, and the decision once made.
+  void collect_form_timing()
+  {
+    const bool before = form_.decided();
+    form_.collect();
+    if (!before && form_.decided()) {
+      form_us_[0] = form_.us_per_iteration(0);
+      form_us_[1] = form_.us_per_iteration(1);
+      {
+        std::lock_guard<std::mutex> lock(tune_mutex());
+        form_cache()[form_key_] = form_choice{form_.chosen(), form_us_[0], form_us_[1]};
+      }
+      if (std::getenv("CUOPT_B200_TRACE"))
+        std::fprintf(stderr,
+                     "[cuopt_b200] plain iterations: graphs %.2f us, persistent (%d blocks) %.2f "
+                     "us per iteration -> %s\n",
+                     form_.us_per_iteration(0), persist_grid_, form_.us_per_iteration(1),
+                     form_.chosen() ? "persistent" : "graphs");
+    }
+  }
+
+  // A timing cycle runs from the first plain run after a termination check to the next check:
+  // all its plain runs use one form, and its events bracket everything the GPU does in between
+  // (major steps, fixed-point errors and every launch boundary), so the forms are compared on
+  // what they cost the loop.
+  void run_plain(long R, long k)
+  {
+    if (!cycle_open_) {
+      cycle_form_     = form_.next();
+      cycle_k0_       = k;
+      cycle_one_time_ = false;
+      cycle_open_     = true;
+      form_.begin(s_);
+    }
+    cycle_one_time_ |= cycle_form_ == 1 ? launch_persistent((int)R) : run_graphs(R);
+  }
+  void close_cycle(long k)
+  {
+    if (!cycle_open_) return;
+    cycle_open_ = false;
+    form_.end(s_, cycle_form_, k - cycle_k0_, cycle_one_time_);
+  }
+
+  // Returns true when a graph had to be captured and instantiated first.
+  bool run_graphs(long R)
+  {
+    bool built = false;
     for (int L = 128; L >= 1; L >>= 1) {
       while (R >= L) {
         auto it = graphs_.find(L);
@@ -731,12 +857,14 @@ class engine {
           B200_CUDA_CHECK(cudaGraphInstantiate(&e, g, 0));
           cudaGraphDestroy(g);
           it = graphs_.emplace(L, e).first;
+          built = true;
         }
         B200_CUDA_CHECK(cudaGraphLaunch(it->second, s_));
         launches_ += 2.0 * L + 1.0;
         R -= L;
       }
     }
+    return built;
   }
 
   void set_scalars(long long t0)
@@ -761,6 +889,17 @@ class engine {
 
   // Residuals and objectives of (xu_, yu_, su_) on the unscaled problem (c64_, lc64_, uc64_).
   conv_info evaluate_unscaled()
+  {
+    enqueue_conv(hres_);
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    collect_form_timing();
+    return read_conv(hres_);
+  }
+
+  // The kernels of a termination check on (xu_, yu_, su_) and the copy of their results to the
+  // pinned host buffer h: h[0..6] the sums, h[8] two error flags (the persistent kernel's barrier
+  // status and the tiled sweeps' bounded-wait flag).
+  void enqueue_conv(double* h)
   {
     const auto A = view64(L_.A), AT = view64(L_.AT);
     sell_map_kernel<double, double, term_primal_epi><<<sell_grid(A), kBlock, 0, s_>>>(
@@ -788,18 +927,37 @@ class engine {
     }
     B200_LAUNCH_CHECK();
     B200_CUDA_CHECK(
-      cudaMemcpyAsync(hres_, dres_.data(), nres * sizeof(double), cudaMemcpyDeviceToHost, s_));
-    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
-    if constexpr (std::is_same_v<TX, float>) check_tile_error();
+      cudaMemcpyAsync(h, dres_.data(), nres * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    int* flags = reinterpret_cast<int*>(h + 8);
+    flags[0] = flags[1] = 0;
+    if (persist_launches_ > 0)
+      B200_CUDA_CHECK(cudaMemcpyAsync(flags, &pctl_.data()->status, sizeof(int),
+                                      cudaMemcpyDeviceToHost, s_));
+    if ((tile_primal_ || tile_dual_) && terr_.size() > 0)
+      B200_CUDA_CHECK(
+        cudaMemcpyAsync(flags + 1, terr_.data(), sizeof(int), cudaMemcpyDeviceToHost, s_));
+  }
+
+  // The check's results from h once the copies have completed.  Throws when a persistent launch's
+  // barrier or a tiled sweep's panel copy gave up its wait since the solve began.
+  conv_info read_conv(const double* h)
+  {
+    const int* flags = reinterpret_cast<const int*>(h + 8);
+    if (flags[0] != 0)
+      throw cuda_error(flags[0] == kBarrierTimedOut
+                         ? "persistent iterations: a grid barrier passed its deadline"
+                         : "persistent iterations: a grid barrier passed its poll limit");
+    if (flags[1] != 0)
+      throw cuda_error("tiled sweep: a panel copy did not complete within its wait limit");
     conv_info cv;
     if (p_.per_constraint_residual) {
-      cv.linf_primal = hres_[5];
-      cv.linf_dual   = hres_[6];
+      cv.linf_primal = h[5];
+      cv.linf_dual   = h[6];
     }
-    cv.l2_primal  = std::sqrt(hres_[0]);
-    cv.l2_dual    = std::sqrt(hres_[2]);
-    cv.primal_obj = hres_[3];
-    cv.dual_obj   = hres_[4] + hres_[1];
+    cv.l2_primal  = std::sqrt(h[0]);
+    cv.l2_dual    = std::sqrt(h[2]);
+    cv.primal_obj = h[3];
+    cv.dual_obj   = h[4] + h[1];
     if (obj_scale_ != 1.0 || obj_offset_ != 0.0) {
       cv.primal_obj = obj_scale_ * (cv.primal_obj + obj_offset_);
       cv.dual_obj   = obj_scale_ * (cv.dual_obj + obj_offset_);
@@ -827,6 +985,11 @@ class engine {
     r.primal_weight = omega_;
     r.restarts   = restarts_;
     r.kernel_launches = launches_;
+    // -1: the solve ended while both forms were still being timed.
+    r.plain_form          = form_.decided() ? form_.chosen() : -1;
+    r.persistent_blocks   = persist_grid_;
+    r.us_plain_graphs     = form_.decided() ? form_us_[0] : form_.us_per_iteration(0);
+    r.us_plain_persistent = form_.decided() ? form_us_[1] : form_.us_per_iteration(1);
   }
 
   bool meets(const conv_info& cv, double tol) const
@@ -937,48 +1100,10 @@ class engine {
       const bool cond  = (k % conditional_major(k)) == 0;
       bool restarted   = false;
       if (major || cond) {
+        close_cycle(k);
         const conv_info cv = evaluate();
-        // check_termination_criteria_kernel (reference termination_strategy.cu:311-352)
-        const bool pcr       = p_.per_constraint_residual;
-        const bool primal_ok = pcr ? cv.linf_primal <= p_.abs_primal
-                                   : cv.l2_primal <= p_.abs_primal + p_.rel_primal * b_norm_;
-        const bool dual_ok   = pcr ? cv.linf_dual <= p_.abs_dual
-                                   : cv.l2_dual <= p_.abs_dual + p_.rel_dual * c_norm_;
-        int status           = kNoTermination;
-        if (dual_ok && primal_ok && cv.gap <= p_.abs_gap + p_.rel_gap * cv.abs_obj)
-          status = kOptimal;
-        else if (primal_ok)
-          status = kPrimalFeasible;
-        if (p_.log_to_console && (k % 1000 == 0))
-          std::printf("%7ld %+.8e %+.8e  %8.2e   %8.2e     %8.2e   %.3fs\n", k, cv.primal_obj,
-                      cv.dual_obj, cv.gap, cv.l2_primal, cv.l2_dual, now_s() - t_start_);
-        if (k > 1 && status == kOptimal) return finish(r, kOptimal, cv, k);
-        // check_termination_criteria_kernel (reference termination_strategy.cu:354-376); Stable3
-        // returns any current infeasibility (never_restart_to_average, pdlp.cu:1089-1109).
-        if (p_.detect_infeasibility && status == kNoTermination) {
-          if (sched_.dual_ray_obj > 0.0 &&
-              sched_.max_dual_ray_inf / sched_.dual_ray_obj <= p_.primal_infeasible_tol)
-            return finish(r, kPrimalInfeasible, cv, k);
-          if (sched_.primal_ray_obj < 0.0 &&
-              sched_.max_primal_ray_inf / -sched_.primal_ray_obj <= p_.dual_infeasible_tol)
-            return finish(r, kDualInfeasible, cv, k);
-        }
-        if (now_s() - t_start_ >= p_.time_limit) return finish(r, kTimeLimit, cv, k);
-        if (k >= p_.iteration_limit) return finish(r, kIterationLimit, cv, k);
-        if (!std::isfinite(cv.l2_primal) || !std::isfinite(cv.l2_dual))
-          return finish(r, kNumericalError, cv, k);
-        if constexpr (std::is_same_v<TX, float>) {
-          const double q = termination_distance(
-            pcr ? cv.linf_primal : cv.l2_primal,
-            pcr ? p_.abs_primal : p_.abs_primal + p_.rel_primal * b_norm_,
-            pcr ? cv.linf_dual : cv.l2_dual, pcr ? p_.abs_dual : p_.abs_dual + p_.rel_dual * c_norm_,
-            cv.gap, p_.abs_gap + p_.rel_gap * cv.abs_obj);
-          if (q <= 0.5 * sched_.stall_ref) {
-            sched_.stall_ref = q;
-            sched_.stall_k   = k;
-          } else if (k - sched_.stall_k >= kStallWindow)
-            return finish(r, kStalled, cv, k);
-        }
+        const int st       = decide(cv, k);
+        if (st != kKeepGoing) return finish(r, st, cv, k);
 
         if (major) {
           // should_cupdlpx_restart (reference pdlp_restart_strategy.cu:689-754)
@@ -1045,7 +1170,7 @@ class engine {
           if (is_check(kk) || is_major_step(kk) || ((kk + 1) % kMajor == 0)) break;
           ++R;
         }
-        run_plain(R);
+        run_plain(R, k);
         k += R;
         since += R;
         continue;
@@ -1096,6 +1221,53 @@ class engine {
     }
   }
 
+  // Termination decision of the check at iteration k on its results cv (reference
+  // check_termination_criteria_kernel, termination_strategy.cu:311-376): the status that ends the
+  // loop (kStalled included), or kKeepGoing.
+  static constexpr int kKeepGoing = -1000;
+  int decide(const conv_info& cv, long k)
+  {
+    const bool pcr       = p_.per_constraint_residual;
+    const bool primal_ok = pcr ? cv.linf_primal <= p_.abs_primal
+                               : cv.l2_primal <= p_.abs_primal + p_.rel_primal * b_norm_;
+    const bool dual_ok   = pcr ? cv.linf_dual <= p_.abs_dual
+                               : cv.l2_dual <= p_.abs_dual + p_.rel_dual * c_norm_;
+    int status           = kNoTermination;
+    if (dual_ok && primal_ok && cv.gap <= p_.abs_gap + p_.rel_gap * cv.abs_obj)
+      status = kOptimal;
+    else if (primal_ok)
+      status = kPrimalFeasible;
+    if (p_.log_to_console && (k % 1000 == 0))
+      std::printf("%7ld %+.8e %+.8e  %8.2e   %8.2e     %8.2e   %.3fs\n", k, cv.primal_obj,
+                  cv.dual_obj, cv.gap, cv.l2_primal, cv.l2_dual, now_s() - t_start_);
+    if (k > 1 && status == kOptimal) return kOptimal;
+    // Stable3 returns any current infeasibility (never_restart_to_average, pdlp.cu:1089-1109).
+    if (p_.detect_infeasibility && status == kNoTermination) {
+      if (sched_.dual_ray_obj > 0.0 &&
+          sched_.max_dual_ray_inf / sched_.dual_ray_obj <= p_.primal_infeasible_tol)
+        return kPrimalInfeasible;
+      if (sched_.primal_ray_obj < 0.0 &&
+          sched_.max_primal_ray_inf / -sched_.primal_ray_obj <= p_.dual_infeasible_tol)
+        return kDualInfeasible;
+    }
+    if (now_s() - t_start_ >= p_.time_limit) return kTimeLimit;
+    if (k >= p_.iteration_limit) return kIterationLimit;
+    if (!std::isfinite(cv.l2_primal) || !std::isfinite(cv.l2_dual)) return kNumericalError;
+    if constexpr (std::is_same_v<TX, float>) {
+      const double q = termination_distance(
+        pcr ? cv.linf_primal : cv.l2_primal,
+        pcr ? p_.abs_primal : p_.abs_primal + p_.rel_primal * b_norm_,
+        pcr ? cv.linf_dual : cv.l2_dual, pcr ? p_.abs_dual : p_.abs_dual + p_.rel_dual * c_norm_,
+        cv.gap, p_.abs_gap + p_.rel_gap * cv.abs_obj);
+      if (q <= 0.5 * sched_.stall_ref) {
+        sched_.stall_ref = q;
+        sched_.stall_k   = k;
+      } else if (k - sched_.stall_k >= kStallWindow)
+        return kStalled;
+    }
+    return kKeepGoing;
+  }
+
   // ------------------------------------------------------------------ state
   const lp_device_input& in_;
   const pdlp_params& p_;
@@ -1121,6 +1293,17 @@ class engine {
   dbuf<float> tpart_;
   dbuf<int> terr_;
   double tune_ms_[4] = {0, 0, 0, 0};
+  // Persistent plain iterations: the launch's control block (barrier count, status), its grid,
+  // the choice of form and its cache key.
+  dbuf<persist_ctl> pctl_;
+  bool cycle_open_ = false, cycle_one_time_ = false;
+  int cycle_form_  = 0;
+  long cycle_k0_   = 0;
+  int persist_grid_      = 0;
+  long persist_launches_ = 0;
+  plain_form_tuner form_;
+  form_key form_key_{};
+  double form_us_[2] = {0, 0};  // the timings behind the choice (this solve's or the cached ones)
 
   double obj_scale_ = 1.0, obj_offset_ = 0.0;
   double c_norm_ = 0, b_norm_ = 0, beta_ = 1, gamma_ = 1;

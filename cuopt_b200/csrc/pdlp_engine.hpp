@@ -60,6 +60,7 @@ struct pdlp_params {
   int precision           = 0;  // 0 FP64, 1 mixed FP32/FP64
   int refinement_passes   = 0;
   int tiled_sweeps        = -1;  // mixed precision: -1 autotuned, 0 sliced ELL only, 1 tiled
+  int persistent          = -1;  // plain iterations: -1 timed choice, 0 CUDA graphs, 1 persistent
   double refinement_tol   = 1e-8;
   bool log_to_console     = false;
   // Infeasibility detection (CUOPT_INFEASIBILITY_DETECTION and its two tolerances).
@@ -106,6 +107,11 @@ struct pdlp_result {
   int restarts = 0, power_iterations = 0, refinement_passes = 0;
   bool crossover = false;  // the solution was replaced by the vertex of its active set
   double kernel_launches = 0;
+  // Form of the plain iterations: 0 CUDA graphs, 1 persistent kernel (its grid in blocks), and
+  // the median microseconds per iteration of the check-to-check cycles each form ran while the
+  // choice was made (0 where it was not timed).
+  int plain_form = 0, persistent_blocks = 0;
+  double us_plain_graphs = 0, us_plain_persistent = 0;
 };
 
 struct sweep_profile {

@@ -40,6 +40,7 @@ CUOPT_PDLP_PRECISION = "pdlp_precision"
 CUOPT_PDLP_REFINEMENT_PASSES = "pdlp_refinement_passes"
 CUOPT_PDLP_REFINEMENT_TOLERANCE = "pdlp_refinement_tolerance"
 CUOPT_PDLP_TILED_SWEEPS = "pdlp_tiled_sweeps"
+CUOPT_PDLP_PERSISTENT_ITERATIONS = "pdlp_persistent_iterations"
 
 _TOLERANCE_NAMES = (CUOPT_ABSOLUTE_DUAL_TOLERANCE, CUOPT_RELATIVE_DUAL_TOLERANCE,
                     CUOPT_ABSOLUTE_PRIMAL_TOLERANCE, CUOPT_RELATIVE_PRIMAL_TOLERANCE,

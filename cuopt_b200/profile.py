@@ -56,7 +56,8 @@ def main() -> None:
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c1_small")
-    ap.add_argument("--mode", choices=["solve", "sweeps", "batch", "adjoint", "climbers", "gather"],
+    ap.add_argument("--mode", choices=["solve", "sweeps", "batch", "adjoint", "climbers", "gather",
+                                       "barrier"],
                     default="sweeps")
     ap.add_argument("--fd-solver", type=int, default=2,
                     help="adjoint mode: instances also differenced through the full solver")
@@ -79,6 +80,10 @@ def main() -> None:
     ap.add_argument("--refine", type=int, default=0, help="> 0: continue a mixed-precision solve in FP64 to 1e-8")
     ap.add_argument("--tiled", type=int, default=-1, choices=[-1, 0, 1],
                     help="pdlp_tiled_sweeps: -1 autotuned, 0 sliced ELL only, 1 tiled where possible")
+    ap.add_argument("--persistent", type=int, default=-1, choices=[-1, 0, 1],
+                    help="pdlp_persistent_iterations: -1 timed choice, 0 CUDA graphs, 1 persistent")
+    ap.add_argument("--solves", type=int, default=1,
+                    help="solve mode: solves of the same LP (the statistics are the last one's)")
     a = ap.parse_args()
 
     if a.mode == "batch":
@@ -92,6 +97,9 @@ def main() -> None:
         return
     if a.mode == "gather":
         print(json.dumps(run_gather(a)))
+        return
+    if a.mode == "barrier":
+        print(json.dumps(run_barrier()))
         return
     m, n, k, seed = CONFIGS[a.config]
     lp = (gen.constructed_lp(m, n, k, seed=seed) if k
@@ -111,6 +119,7 @@ def main() -> None:
         L.cuOptSetFloatParameter(s, name.encode(), a.tol)
     L.cuOptSetIntegerParameter(s, b"pdlp_precision", 1 if a.precision == "mixed" else 0)
     L.cuOptSetIntegerParameter(s, b"pdlp_tiled_sweeps", a.tiled)
+    L.cuOptSetIntegerParameter(s, b"pdlp_persistent_iterations", a.persistent)
     L.cuOptSetParameter(s, b"log_to_console", b"false")
     if a.time_limit > 0:
         L.cuOptSetFloatParameter(s, b"time_limit", a.time_limit)
@@ -125,12 +134,17 @@ def main() -> None:
         y = torch.empty(m, device=dev, dtype=torch.float64)
         rc = torch.empty(n, device=dev, dtype=torch.float64)
         st, status = PDLPStatistics(), C.c_int32()
-        t0 = time.perf_counter()
-        code = L.cuOptSolveDevice(m, n, 1, 0.0, *ptr, s, stream, C.c_void_p(x.data_ptr()),
-                                  C.c_void_p(y.data_ptr()), C.c_void_p(rc.data_ptr()), C.byref(st),
-                                  C.byref(status))
-        torch.cuda.synchronize()
-        out.update({"rc": code, "status": status.value, "wall_s": time.perf_counter() - t0})
+        walls = []
+        for _ in range(max(1, a.solves)):
+            t0 = time.perf_counter()
+            code = L.cuOptSolveDevice(m, n, 1, 0.0, *ptr, s, stream, C.c_void_p(x.data_ptr()),
+                                      C.c_void_p(y.data_ptr()), C.c_void_p(rc.data_ptr()),
+                                      C.byref(st), C.byref(status))
+            torch.cuda.synchronize()
+            walls.append(time.perf_counter() - t0)
+            if code != 0:
+                break
+        out.update({"rc": code, "status": status.value, "wall_s": walls[-1], "walls_s": walls})
         out.update({f: getattr(st, f) for f, _ in PDLPStatistics._fields_})
         out["objective_rel_error"] = abs(st.primal_objective - lp.optimal_objective) / max(
             1.0, abs(lp.optimal_objective))
@@ -166,6 +180,21 @@ def gather_rates(m: int, n: int, nnz: int, stream) -> dict:
             if code != 0:
                 raise RuntimeError(f"cuOptProfileGatherRate returned {code}")
             out[f"{name}_fp{8 * eb}"] = {"gathers_per_s": rate.value, "chunks_in_flight": chunks.value}
+    return out
+
+
+def run_barrier() -> dict:
+    """Cost of the persistent kernel's grid barrier (cuOptProbeGridBarrier): microseconds per
+    barrier for grids of 8 to 1184 blocks, 5000 barriers each."""
+    from cuopt_b200._lib import lib
+
+    L = lib()
+    out = {}
+    for blocks in (8, 21, 57, 148, 296, 592, 740, 1184):
+        st, ms = C.c_int32(), C.c_double()
+        code = L.cuOptProbeGridBarrier(blocks, 5000, 0, 5000.0, None, C.byref(st), C.byref(ms))
+        out[str(blocks)] = ({"us_per_barrier": 1e3 * ms.value / 5000, "status": st.value}
+                            if code == 0 else {"rc": code})
     return out
 
 
@@ -227,6 +256,7 @@ def run_batch(a, models=None) -> dict:
     st.set_parameter(lpm.CUOPT_LOG_TO_CONSOLE, False)
     precision = getattr(a, "batch_precision", "fp64")
     st.set_parameter(lpm.CUOPT_PDLP_PRECISION, 1 if precision == "mixed" else 0)
+    st.set_parameter(lpm.CUOPT_PDLP_PERSISTENT_ITERATIONS, getattr(a, "persistent", -1))
     if getattr(a, "refine", 0):
         st.set_parameter(lpm.CUOPT_PDLP_REFINEMENT_PASSES, a.refine)
     if a.time_limit > 0:
@@ -257,6 +287,12 @@ def run_batch(a, models=None) -> dict:
            "fp64_resolved": sum(int(s.stats.get("refinement_passes", 0) > 0) for s in sols),
            "max_relative_kkt": max(kkt),
            "objective_rel_error_over_1e-6": sum(int(e > 1e-6) for e in obj_err),
+           "plain_iterations": {
+               "form": {0: "graphs", 1: "persistent"}.get(
+                   sols[0].stats.get("plain_iteration_form"), "undecided"),
+               "persistent_blocks": sols[0].stats.get("persistent_blocks"),
+               "us_per_iteration_graphs": sols[0].stats.get("plain_iteration_us_graphs"),
+               "us_per_iteration_persistent": sols[0].stats.get("plain_iteration_us_persistent")},
            "worst_instances": [{"i": i, "m": lps[i].m, "status": status[i], "iterations": iters[i],
                                 "objective_rel_error": obj_err[i], "relative_kkt": kkt[i],
                                 "optimal_objective": lps[i].optimal_objective,

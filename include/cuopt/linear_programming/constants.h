@@ -96,6 +96,14 @@
 #define CUOPT_PDLP_TILED_SWEEPS_AUTO -1
 #define CUOPT_PDLP_TILED_SWEEPS_OFF  0
 #define CUOPT_PDLP_TILED_SWEEPS_ON   1
+/* pdlp_persistent_iterations: the runs of plain iterations between termination checks are
+ * replayed from CUDA graphs (0) or run by one persistent cooperative kernel launch with a grid
+ * barrier after every sweep (1); -1 times both forms on the first runs of a solve (the iterates
+ * are the same either way) and keeps the faster one, remembered per problem shape. */
+#define CUOPT_PDLP_PERSISTENT_ITERATIONS      "pdlp_persistent_iterations"
+#define CUOPT_PDLP_PERSISTENT_ITERATIONS_AUTO -1
+#define CUOPT_PDLP_PERSISTENT_ITERATIONS_OFF  0
+#define CUOPT_PDLP_PERSISTENT_ITERATIONS_ON   1
 
 #define CUOPT_MODE_OPPORTUNISTIC 0
 #define CUOPT_MODE_DETERMINISTIC 1

@@ -40,6 +40,15 @@ typedef struct {
   cuopt_float_t loop_time;      /* seconds spent in the iteration loop */
   cuopt_float_t kernel_launches; /* kernels this library launched for the solve */
   cuopt_int_t crossover;         /* 1: the solution is the vertex of its active set ("crossover") */
+  /* Form of the plain iterations between termination checks: 0 CUDA-graph replays, 1 one
+   * persistent cooperative launch per run (pdlp_persistent_iterations), -1 still undecided when the
+   * solve ended; the persistent grid in blocks; and the median microseconds per iteration of the
+   * check-to-check cycles (major steps and launch boundaries included) that each form ran while the
+   * choice was made (0 where it was not timed). */
+  cuopt_int_t plain_iteration_form;
+  cuopt_int_t persistent_blocks;
+  cuopt_float_t plain_iteration_us_graphs;
+  cuopt_float_t plain_iteration_us_persistent;
 } cuOptPDLPStatistics;
 
 cuopt_int_t cuOptGetPDLPStatistics(cuOptSolution solution, cuOptPDLPStatistics* stats);
@@ -83,6 +92,22 @@ cuopt_int_t cuOptProfileScatterRate(cuopt_int_t vector_length,
                                     void* stream,
                                     cuopt_float_t* scatters_per_second,
                                     cuopt_int_t* chunks_in_flight);
+
+/* Measurement and test hook (no counterpart in the reference): the grid barrier that the
+ * persistent plain-iteration kernel (pdlp_persistent_iterations) places after every sweep, run
+ * alone.  A cooperative launch of `blocks` blocks of 256 threads (at most the co-resident count)
+ * passes `rounds` barriers.  With `unreachable` != 0 every barrier waits for one arrival more than
+ * the grid has, so no barrier can complete: each wait ends at the launch's deadline (`budget_ms`
+ * after its start, at most 10 s) and records status 1 (2 if its poll limit came first) instead of
+ * hanging.  Returns the recorded status (0: every barrier completed) and the device time from the
+ * first block's start to its end, in milliseconds. */
+cuopt_int_t cuOptProbeGridBarrier(cuopt_int_t blocks,
+                                  cuopt_int_t rounds,
+                                  cuopt_int_t unreachable,
+                                  cuopt_float_t budget_ms,
+                                  void* stream,
+                                  cuopt_int_t* status,
+                                  cuopt_float_t* elapsed_ms);
 
 /* Measurement hook (no counterpart in the reference): the random-gather ceiling of the device.
  * Streams `gathers` random int32 indices into a vector of `vector_length` elements of

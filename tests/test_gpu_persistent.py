@@ -1,0 +1,132 @@
+"""GPU tests of the persistent form of the plain PDHG iterations (pdlp_persistent_iterations).
+
+The persistent kernel runs the same sweeps with the same arithmetic as the CUDA-graph replays, so
+the expectation is exact: solves with the persistent form forced on, forced off and chosen by
+timing return bit-identical iterates, iteration counts and statuses, for single LPs (FP64 and
+mixed precision) and for block-diagonal batches.  The grid barrier between the sweeps is the only
+wait in the kernel; its bounded wait is checked on its own (cuOptProbeGridBarrier): a barrier that
+nothing can complete must end at its deadline with status 1, and the context must stay usable.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from cuopt_b200 import _lib
+from cuopt_b200 import generators as gen
+from cuopt_b200 import linear_programming as lpm
+from tests.helpers import datamodel_from_lp, settings
+
+pytestmark = pytest.mark.gpu
+
+GRAPHS, PERSISTENT, AUTO = 0, 1, -1
+
+
+def _settings(form, **kw):
+    s = settings(**kw)
+    s.set_parameter(lpm.CUOPT_PDLP_PERSISTENT_ITERATIONS, form)
+    return s
+
+
+def _same(a, b):
+    assert a.get_termination_status() == b.get_termination_status()
+    assert a.stats["number_of_steps_taken"] == b.stats["number_of_steps_taken"]
+    assert np.array_equal(a.get_primal_solution(), b.get_primal_solution())
+    assert np.array_equal(a.get_dual_solution(), b.get_dual_solution())
+    assert np.array_equal(a.get_reduced_cost(), b.get_reduced_cost())
+
+
+@pytest.fixture(scope="module")
+def lp_c0():
+    """The 2,000 x 5,000 constructed LP (8 non-zeros per column)."""
+    return gen.constructed_lp(2000, 5000, 8, seed=0)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_persistent_matches_graphs(lp_c0, precision):
+    dm = datamodel_from_lp(lp_c0)
+    g = lpm.Solve(dm, _settings(GRAPHS, tol=1e-6, precision=precision))
+    p = lpm.Solve(dm, _settings(PERSISTENT, tol=1e-6, precision=precision))
+    a = lpm.Solve(dm, _settings(AUTO, tol=1e-6, precision=precision))
+    assert g.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    _same(g, p)
+    _same(g, a)
+    assert g.stats["plain_iteration_form"] == GRAPHS
+    assert p.stats["plain_iteration_form"] == PERSISTENT
+    assert p.stats["persistent_blocks"] > 0
+    # The timed choice: both forms timed, the faster one kept.
+    assert a.stats["plain_iteration_form"] in (GRAPHS, PERSISTENT)
+    us_g, us_p = a.stats["plain_iteration_us_graphs"], a.stats["plain_iteration_us_persistent"]
+    assert us_g > 0 and us_p > 0
+    assert a.stats["plain_iteration_form"] == (PERSISTENT if us_p < us_g else GRAPHS)
+
+
+def test_persistent_matches_graphs_at_iteration_limits(lp_c0):
+    """Runs cut by an iteration limit inside a persistent launch's range end on the same iterate."""
+    dm = datamodel_from_lp(lp_c0)
+    for k in (7, 33, 250):
+        g = lpm.Solve(dm, _settings(GRAPHS, tol=1e-12, iteration_limit=k))
+        p = lpm.Solve(dm, _settings(PERSISTENT, tol=1e-12, iteration_limit=k))
+        assert g.get_termination_status() == lpm.LPTerminationStatus.IterationLimit
+        _same(g, p)
+
+
+def test_persistent_long_rows():
+    """Long rows (warp per row) and sliced rows in the same persistent sweeps."""
+    lp = gen.skewed_lp(400, 3000, seed=7, cap=3000)
+    dm = datamodel_from_lp(lp)
+    g = lpm.Solve(dm, _settings(GRAPHS, tol=1e-6))
+    p = lpm.Solve(dm, _settings(PERSISTENT, tol=1e-6))
+    _same(g, p)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_persistent_matches_graphs(precision):
+    lps = [gen.constructed_lp(m, int(2.5 * m), k, seed=70 + i)
+           for i, (m, k) in enumerate([(200, 6), (1300, 12), (450, 8), (3000, 9), (800, 7)])]
+    dms = [datamodel_from_lp(lp) for lp in lps]
+    g = lpm.BatchSolve(dms, _settings(GRAPHS, tol=1e-6, precision=precision))[0]
+    p = lpm.BatchSolve(dms, _settings(PERSISTENT, tol=1e-6, precision=precision))[0]
+    a = lpm.BatchSolve(dms, _settings(AUTO, tol=1e-6, precision=precision))[0]
+    for sg, sp, sa in zip(g, p, a):
+        assert sg.get_termination_status() == lpm.LPTerminationStatus.Optimal
+        _same(sg, sp)
+        _same(sg, sa)
+    assert all(s.stats["plain_iteration_form"] == PERSISTENT for s in p)
+    assert all(s.stats["plain_iteration_form"] == GRAPHS for s in g)
+
+
+def _probe(blocks, rounds, unreachable, budget_ms):
+    lib = _lib.lib()
+    st, ms = _lib.cuopt_int_t(), C.c_double()
+    rc = lib.cuOptProbeGridBarrier(blocks, rounds, unreachable, budget_ms, None, C.byref(st),
+                                   C.byref(ms))
+    return rc, st.value, ms.value
+
+
+def test_grid_barrier_completes_and_costs():
+    for blocks in (20, 148, 296):
+        rc, st, ms = _probe(blocks, 2000, 0, 5000.0)
+        assert rc == 0 and st == 0
+        assert ms / 2000 < 0.05  # well under 50 us per barrier
+
+
+def test_grid_barrier_deadline_ends_the_wait():
+    """A barrier that cannot complete ends at its 50 ms deadline with status 1; the context stays
+    usable (a solve afterwards succeeds)."""
+    rc, st, ms = _probe(148, 1, 1, 50.0)
+    assert rc == 0
+    assert st == 1
+    assert 45.0 <= ms < 2000.0
+    rc, st, ms = _probe(148, 10, 0, 1000.0)
+    assert rc == 0 and st == 0
+    lp = gen.constructed_lp(200, 500, 8, seed=11)
+    sol = lpm.Solve(datamodel_from_lp(lp), _settings(PERSISTENT, tol=1e-6))
+    assert sol.get_termination_status() == lpm.LPTerminationStatus.Optimal
+
+
+def test_grid_barrier_rejects_oversized_grids():
+    rc, _, _ = _probe(1_000_000, 1, 0, 10.0)
+    assert rc == 1  # CUOPT_INVALID_ARGUMENT: more blocks than can be co-resident, nothing launched
