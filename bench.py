@@ -195,7 +195,7 @@ class DeviceLP:
 
 
 def solve_device(L, dlp, settings, stream_ptr):
-    from cuopt_b200._lib import PDLPStatistics
+    from cuopt_b200._lib import PDLPStatistics, stats_dict
     st = PDLPStatistics()
     status = C.c_int32()
     rc = L.cuOptSolveDevice(dlp.m, dlp.n, 1, 0.0, *dlp.ptrs(), settings, C.c_void_p(stream_ptr),
@@ -203,16 +203,23 @@ def solve_device(L, dlp, settings, stream_ptr):
                             C.c_void_p(dlp.rc.data_ptr()), C.byref(st), C.byref(status))
     if rc != 0:
         raise RuntimeError(f"cuOptSolveDevice returned {rc}")
-    return status.value, {f: getattr(st, f) for f, _ in PDLPStatistics._fields_}
+    return status.value, stats_dict(st)
 
 
 def form_info(st):
-    """The form of the plain iterations a solve used and the cycle timings the choice was made on
-    (pdlp_persistent_iterations = -1: CUDA graphs against the persistent cooperative kernel)."""
+    """The tuned choices of a solve: the form of the plain iterations and the cycle timings it was
+    chosen on (pdlp_persistent_iterations = -1: CUDA graphs against the persistent cooperative
+    kernel), and the plain sweeps' warps per block with the ms per launch of 4, 8 and 16
+    (pdlp_sweep_warps_per_block = 0)."""
+    ms = list(st["sweep_block_shape_ms"])
     return {"form": {0: "graphs", 1: "persistent"}.get(st["plain_iteration_form"], "undecided"),
             "persistent_blocks": st["persistent_blocks"],
             "us_per_iteration_graphs": st["plain_iteration_us_graphs"],
-            "us_per_iteration_persistent": st["plain_iteration_us_persistent"]}
+            "us_per_iteration_persistent": st["plain_iteration_us_persistent"],
+            "sweep_warps_per_block": {"primal": st["sweep_warps_per_block_primal"],
+                                      "dual": st["sweep_warps_per_block_dual"]},
+            "sweep_ms_by_warps_per_block": {"primal": dict(zip(("4", "8", "16"), ms[:3])),
+                                            "dual": dict(zip(("4", "8", "16"), ms[3:]))}}
 
 
 def grid_barrier_costs(L):
@@ -425,6 +432,44 @@ def run_c0(L, torch, device, sptr, args, O=None):
     return out
 
 
+def run_c2(L, torch, device, sptr, args):
+    """The skewed-sparsity LP (500k x 1.5M, Zipf(1.3) row lengths capped at 5000, slacks added):
+    the plain sweeps' time and rates per row-length class (FP64 and mixed), and a solve sample of
+    a fixed iteration count (iterations per second and the relative KKT it reaches).  The full
+    solve to 1e-6 takes far longer than a bench run (its evidence is a separate measurement)."""
+    from cuopt_b200 import generators as gen
+    from cuopt_b200.profile import sweep_classes
+    from cuopt_b200.profile import CONFIGS as PCONF
+
+    m0, n0, _, seed = PCONF["c2"]
+    lp = gen.skewed_lp(m0, n0, seed=seed, explicit_slacks=True)
+    dlp = DeviceLP(lp, torch, device)
+    out = {"config": "c2", "m": lp.m, "n": lp.n, "nnz": lp.nnz}
+    for prec, name, elem in ((0, "fp64", 8), (1, "mixed", 4)):
+        sh = settings_handle(L, 1e-6, prec)
+        vals = [C.c_double() for _ in range(4)]
+        code = L.cuOptProfilePDHGSweeps(lp.m, lp.n, *dlp.ptrs(), sh, C.c_void_p(sptr), 10,
+                                        *[C.byref(v) for v in vals])
+        if code != 0:
+            raise RuntimeError(f"cuOptProfilePDHGSweeps returned {code}")
+        leg = {"primal_sweep_ms": vals[0].value, "dual_sweep_ms": vals[1].value,
+               "primal_gbs": vals[2].value / vals[0].value / 1e6,
+               "dual_gbs": vals[3].value / vals[1].value / 1e6,
+               "classes": sweep_classes(L, lp.m, lp.n, dlp.ptrs(), sh, C.c_void_p(sptr), 10, elem)}
+        L.cuOptDestroySolverSettings(C.byref(sh))
+        sh = settings_handle(L, 1e-6, prec, iteration_limit=args.c2_iterations)
+        status, st = solve_device(L, dlp, sh, sptr)
+        L.cuOptDestroySolverSettings(C.byref(sh))
+        it = st["number_of_steps_taken"]
+        leg["solve_sample"] = {"iterations": it, "status": status,
+                               "pdhg_iter_per_s": it / (st["loop_time"] or 1e-9),
+                               "setup_s": st["setup_time"], "relative_kkt": max(
+                                   st["l2_relative_primal_residual"],
+                                   st["l2_relative_dual_residual"], st["relative_gap"])}
+        out[name] = leg
+    return out
+
+
 def run_b200(args):
     import torch
 
@@ -572,6 +617,7 @@ def run_b200(args):
                                                               res["primal_obj"])
 
     c0 = run_c0(L, torch, device, sptr, args, O) if lone and not args.no_c0 else None
+    c2 = run_c2(L, torch, device, sptr, args) if lone and not args.no_c2 else None
 
     # 512 uneven LPs in one batched call vs all of them one by one (rank 0, N = 1): FP64 at 1e-6
     # and 1e-8, mixed precision at 1e-6 and refined in FP64 to 1e-8.
@@ -620,7 +666,8 @@ def run_b200(args):
                            "oracle itself is 6.8e-6 off on batch instance 284 at 1e-6); the legs "
                            "refined to 1e-8 are the ones held to 1e-6",
         "iteration_loop": {**form_info(last_mixed), "grid_barrier_us": grid_barrier_costs(L)},
-        "c0": c0, "batch_c3": batch, "batch_c3_mixed": batch_mixed, "adjoint_c4": adjoint,
+        "c0": c0, "c2": c2, "batch_c3": batch, "batch_c3_mixed": batch_mixed,
+        "adjoint_c4": adjoint,
         "roofline": roofline, "cpu_baseline": cpu,
         "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
@@ -656,6 +703,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-refine", action="store_true")
     ap.add_argument("--no-c0", action="store_true")
+    ap.add_argument("--no-c2", action="store_true")
+    ap.add_argument("--c2-iterations", type=int, default=4000,
+                    help="iteration count of the config-2 solve sample")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adjoint-fd-coords", type=int, default=32,

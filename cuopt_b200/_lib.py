@@ -47,7 +47,19 @@ class PDLPStatistics(C.Structure):
         ("persistent_blocks", cuopt_int_t),
         ("plain_iteration_us_graphs", cuopt_float_t),
         ("plain_iteration_us_persistent", cuopt_float_t),
+        ("sweep_warps_per_block_primal", cuopt_int_t),
+        ("sweep_warps_per_block_dual", cuopt_int_t),
+        ("sweep_block_shape_ms", cuopt_float_t * 6),
     ]
+
+
+def stats_dict(st) -> dict:
+    """A PDLPStatistics as a dict of Python numbers (array fields as lists)."""
+    out = {}
+    for f, _ in PDLPStatistics._fields_:
+        v = getattr(st, f)
+        out[f] = list(v) if isinstance(v, C.Array) else v
+    return out
 
 
 # name -> (restype, argtypes)
@@ -121,6 +133,8 @@ SIGNATURES = {
     "cuOptProfilePDHGSweeps": (cuopt_int_t, [cuopt_int_t, cuopt_int_t] + [C.c_void_p] * 8 +
                                [handle_t, C.c_void_p, cuopt_int_t] +
                                [C.POINTER(C.c_double)] * 4),
+    "cuOptProfileSweepClasses": (cuopt_int_t, [cuopt_int_t, cuopt_int_t] + [C.c_void_p] * 8 +
+                                 [handle_t, C.c_void_p, cuopt_int_t, C.POINTER(C.c_double)]),
     "cuOptProfileGatherRate": (cuopt_int_t, [cuopt_int_t, C.c_int64, cuopt_int_t, C.c_void_p,
                                              C.POINTER(C.c_double), C.POINTER(cuopt_int_t)]),
     "cuOptProfileScatterRate": (cuopt_int_t, [cuopt_int_t, C.c_int64, cuopt_int_t, C.c_void_p,

@@ -24,6 +24,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <limits>
 #include <map>
 #include <random>
@@ -648,6 +649,7 @@ class batch_engine {
     t_start_ = now_s();
     results_.assign(B_, pdlp_result{});
     setup();
+    tune_sweep_shape();
     init_plain_form(B_);
     t_loop_ = now_s();
     loop();
@@ -663,6 +665,9 @@ class batch_engine {
       results_[b].persistent_blocks   = first_blocks_;
       results_[b].us_plain_graphs     = first_us_[0];
       results_[b].us_plain_persistent = first_us_[1];
+      results_[b].wpb_primal          = wpb_primal_;
+      results_[b].wpb_dual            = wpb_dual_;
+      std::memcpy(results_[b].wpb_ms, wpb_ms_, sizeof(wpb_ms_));
     }
     (void)t;
     return results_;
@@ -1257,28 +1262,92 @@ class batch_engine {
   inst_ctx ctx_rows() const { return inst_ctx{rinst_.data(), active_d_.data(), sc_d_.data()}; }
   inst_ctx ctx_cols() const { return inst_ctx{cinst_.data(), active_d_.data(), sc_d_.data()}; }
 
+  // The plain sweeps run with the tuned number of warps per block (tune_sweep_shape).
   template <bool MAJOR, bool HALPERN, bool SAVE_ATY>
-  void launch_primal(int it_off)
+  void launch_primal(int it_off, int wpb = 0)
   {
     const auto A = wview<TX>(false, ATs_.data());
     b_primal_epi<TX, MAJOR, HALPERN, SAVE_ATY> e{x_.data(),    cs_.data(),   ls_.data(),
                                                  us_.data(),   xa_.data(),   xbar_.data(),
                                                  x_.data(),    xhat_.data(), slack_.data(),
                                                  aty_.data(),  ctx_cols(),   it_off};
-    sell_map_kernel<TX, TX, decltype(e)><<<sell_grid(A), kBlock, 0, s_>>>(A, y_.data(), e,
-                                                                         partials_.data());
+    if constexpr (!MAJOR && HALPERN && !SAVE_ATY)
+      launch_sell_wpb(wpb ? wpb : wpb_primal_, A, y_.data(), e, partials_.data(), s_);
+    else
+      sell_map_kernel<TX, TX, decltype(e)><<<sell_grid(A), kBlock, 0, s_>>>(A, y_.data(), e,
+                                                                           partials_.data());
     ++launches_;
   }
   template <bool MAJOR, bool HALPERN, bool FPE>
-  void launch_dual(int it_off)
+  void launch_dual(int it_off, int wpb = 0)
   {
     const auto A = wview<TX>(true, As_.data());
     b_dual_epi<TX, MAJOR, HALPERN, FPE> e{y_.data(),     lcs_.data(),  ucs_.data(),
                                           ya_.data(),    ybar_.data(), y_.data(),
                                           yhat_.data(),  rowbuf_.data(), ctx_rows(), it_off};
-    sell_map_kernel<TX, TX, decltype(e)><<<sell_grid(A), kBlock, 0, s_>>>(A, xbar_.data(), e,
-                                                                         partials_.data());
+    if constexpr (!MAJOR && HALPERN && !FPE)
+      launch_sell_wpb(wpb ? wpb : wpb_dual_, A, xbar_.data(), e, partials_.data(), s_);
+    else
+      sell_map_kernel<TX, TX, decltype(e)><<<sell_grid(A), kBlock, 0, s_>>>(A, xbar_.data(), e,
+                                                                           partials_.data());
     ++launches_;
+  }
+
+  // Block shape of the plain sweeps over all instances (pdlp_sweep_warps_per_block = 0): 4, 8 and 16 warps
+  // per block, one warm-up and three timed launches each; the fastest is kept.  The iterates the
+  // timed sweeps move are restored (x, y) or cleared (x_bar, y_bar) afterwards.
+  void tune_sweep_shape()
+  {
+    wpb_primal_ = wpb_dual_ = p_.sweep_wpb ? p_.sweep_wpb : kWarpsPerBlock;
+    if (p_.sweep_wpb) return;
+    const int m = in_.m, n = in_.n;
+    upload_scalars(std::vector<long>(B_, 0));
+    dbuf<TX> x0(n), y0(m);
+    B200_CUDA_CHECK(cudaMemcpyAsync(x0.data(), x_.data(), n * sizeof(TX),
+                                    cudaMemcpyDeviceToDevice, s_));
+    B200_CUDA_CHECK(cudaMemcpyAsync(y0.data(), y_.data(), m * sizeof(TX),
+                                    cudaMemcpyDeviceToDevice, s_));
+    cudaEvent_t e0, e1;
+    B200_CUDA_CHECK(cudaEventCreate(&e0));
+    B200_CUDA_CHECK(cudaEventCreate(&e1));
+    auto time_of = [&](auto&& launch) {
+      launch();
+      B200_CUDA_CHECK(cudaEventRecord(e0, s_));
+      for (int i = 0; i < 3; ++i) launch();
+      B200_CUDA_CHECK(cudaEventRecord(e1, s_));
+      B200_CUDA_CHECK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      B200_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+      return (double)ms / 3.0;
+    };
+    static constexpr int kShapes[3] = {4, 8, 16};
+    for (int q = 0; q < 3; ++q) {
+      wpb_ms_[0][q] = time_of([&] { launch_primal<false, true, false>(0, kShapes[q]); });
+      wpb_ms_[1][q] = time_of([&] { launch_dual<false, true, false>(0, kShapes[q]); });
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    auto best = [&](const double* t) {
+      int b = 1;
+      for (int q = 0; q < 3; ++q)
+        if (t[q] < t[b]) b = q;
+      return kShapes[b];
+    };
+    wpb_primal_ = best(wpb_ms_[0]);
+    wpb_dual_   = best(wpb_ms_[1]);
+    B200_CUDA_CHECK(cudaMemcpyAsync(x_.data(), x0.data(), n * sizeof(TX),
+                                    cudaMemcpyDeviceToDevice, s_));
+    B200_CUDA_CHECK(cudaMemcpyAsync(y_.data(), y0.data(), m * sizeof(TX),
+                                    cudaMemcpyDeviceToDevice, s_));
+    xbar_.zero(s_);
+    ybar_.zero(s_);
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    if (std::getenv("CUOPT_B200_TRACE"))
+      std::fprintf(stderr,
+                   "[cuopt_b200] batch sweep block shape: primal %.4f/%.4f/%.4f ms -> %d warps; "
+                   "dual %.4f/%.4f/%.4f ms -> %d warps (4/8/16 warps per block)\n",
+                   wpb_ms_[0][0], wpb_ms_[0][1], wpb_ms_[0][2], wpb_primal_, wpb_ms_[1][0],
+                   wpb_ms_[1][1], wpb_ms_[1][2], wpb_dual_);
   }
   void advance(int steps)
   {
@@ -1747,6 +1816,9 @@ class batch_engine {
   int form_active_ = 0, form_epochs_ = 0;
   int first_form_ = -1, first_blocks_ = 0;
   double first_us_[2] = {0, 0};
+  // Warps per block of the plain sweeps and the timings they were chosen by.
+  int wpb_primal_ = kWarpsPerBlock, wpb_dual_ = kWarpsPerBlock;
+  double wpb_ms_[2][3] = {{0, 0, 0}, {0, 0, 0}};
 };
 
 

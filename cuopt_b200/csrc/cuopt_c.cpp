@@ -720,6 +720,9 @@ cuopt_int_t cuOptGetPDLPStatistics(cuOptSolution solution, cuOptPDLPStatistics* 
   st->persistent_blocks               = r.persistent_blocks;
   st->plain_iteration_us_graphs       = r.us_plain_graphs;
   st->plain_iteration_us_persistent   = r.us_plain_persistent;
+  st->sweep_warps_per_block_primal    = r.wpb_primal;
+  st->sweep_warps_per_block_dual      = r.wpb_dual;
+  for (int q = 0; q < 6; ++q) st->sweep_block_shape_ms[q] = r.wpb_ms[q / 3][q % 3];
   return CUOPT_SUCCESS;
 }
 
@@ -807,6 +810,45 @@ cuopt_int_t cuOptProfilePDHGSweeps(cuopt_int_t m, cuopt_int_t n, const cuopt_flo
     return CUOPT_VALIDATION_ERROR;
   } catch (const std::exception& e) {
     std::fprintf(stderr, "cuOptProfilePDHGSweeps: %s\n", e.what());
+    return CUOPT_RUNTIME_ERROR;
+  }
+  return CUOPT_SUCCESS;
+}
+
+cuopt_int_t cuOptProfileSweepClasses(cuopt_int_t m, cuopt_int_t n, const cuopt_float_t* d_c,
+                                     const cuopt_int_t* d_off, const cuopt_int_t* d_idx,
+                                     const cuopt_float_t* d_val, const cuopt_float_t* d_lo,
+                                     const cuopt_float_t* d_up, const cuopt_float_t* d_vlo,
+                                     const cuopt_float_t* d_vup, cuOptSolverSettings settings,
+                                     void* stream, cuopt_int_t iterations, double* out)
+{
+  if (!settings || !d_c || !d_off || !d_lo || !d_up || !d_vlo || !d_vup || m <= 0 || n <= 0 ||
+      iterations <= 0 || !out)
+    return CUOPT_INVALID_ARGUMENT;
+  try {
+    cuopt_b200::lp_device_input in;
+    in.m       = m;
+    in.n       = n;
+    in.row_off = d_off;
+    in.col_idx = d_idx;
+    in.val     = d_val;
+    in.c       = d_c;
+    in.con_lo  = d_lo;
+    in.con_up  = d_up;
+    in.var_lo  = d_vlo;
+    in.var_up  = d_vup;
+    auto prm   = cuopt_b200::params_from_settings(*S(settings));
+    auto prof  = cuopt_b200::pdlp_profile_sweeps(in, prm, static_cast<cudaStream_t>(stream),
+                                                 iterations);
+    for (int s = 0; s < 2; ++s)
+      for (int q = 0; q < 7; ++q) out[7 * s + q] = prof.classes[s][q];
+  } catch (const std::bad_alloc&) {
+    return CUOPT_OUT_OF_MEMORY;
+  } catch (const std::invalid_argument& e) {
+    std::fprintf(stderr, "cuOptProfileSweepClasses: %s\n", e.what());
+    return CUOPT_VALIDATION_ERROR;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "cuOptProfileSweepClasses: %s\n", e.what());
     return CUOPT_RUNTIME_ERROR;
   }
   return CUOPT_SUCCESS;

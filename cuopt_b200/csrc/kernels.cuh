@@ -37,12 +37,12 @@ struct dev_sell {
   B200_HD int slice_count() const { return slice_list ? work_slices : n_slices; }
 };
 
-B200_HD inline int long_blocks(int n_long) { return ceil_div(n_long, kWarpsPerBlock); }
+B200_HD inline int long_blocks(int n_long, int wpb = kWarpsPerBlock) { return ceil_div(n_long, wpb); }
 // Grid of sell_map_kernel (and of the setup kernels, which always see full views).
 template <typename T>
-inline int sell_grid(const dev_sell<T>& a)
+inline int sell_grid(const dev_sell<T>& a, int wpb = kWarpsPerBlock)
 {
-  const int g = long_blocks(a.long_count()) + ceil_div(a.slice_count(), kWarpsPerBlock);
+  const int g = long_blocks(a.long_count(), wpb) + ceil_div(a.slice_count(), wpb);
   return g > 0 ? g : 1;  // an empty work list still launches one (idle) block
 }
 
@@ -209,11 +209,14 @@ __device__ __forceinline__ T gather_load(const T* __restrict__ g, int i)
     return g[i];
 }
 
-template <typename TM, typename TG, class Epi, bool COH = false>
+// WPB: warps (rows or slices) per block.  Only the grouping of warps into blocks depends on it,
+// not any row's arithmetic; sweeps with block reductions (kRed > 0) use kWarpsPerBlock.
+template <typename TM, typename TG, class Epi, bool COH = false, int WPB = kWarpsPerBlock>
 __device__ __forceinline__ void sell_map_block(const dev_sell<TM>& A, const TG* __restrict__ g,
                                                const Epi& epi, double* partials, int vb)
 {
   constexpr int K = Epi::kRed;
+  static_assert(K == 0 || WPB == kWarpsPerBlock, "block reductions assume kWarpsPerBlock warps");
   red_t<K> red;
 #pragma unroll
   for (int q = 0; q < (K > 0 ? K : 1); ++q) red.v[q] = 0.0;
@@ -223,9 +226,9 @@ __device__ __forceinline__ void sell_map_block(const dev_sell<TM>& A, const TG* 
     return;
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int lb   = long_blocks(A.long_count());
+  const int lb   = long_blocks(A.long_count(), WPB);
   if (vb < lb) {
-    const int q   = vb * kWarpsPerBlock + warp;
+    const int q   = vb * WPB + warp;
     const int row = q < A.long_count() ? (A.long_list ? A.long_list[q] : q) : 0;
     if (q < A.long_count() && !skip_rows(epi, row, row)) {
       const auto pre  = epi.load(row);
@@ -237,7 +240,7 @@ __device__ __forceinline__ void sell_map_block(const dev_sell<TM>& A, const TG* 
       if (lane == 0) epi(row, acc, pre, red);
     }
   } else {
-    const int q = (vb - lb) * kWarpsPerBlock + warp;
+    const int q = (vb - lb) * WPB + warp;
     const int s = q < A.slice_count() ? (A.slice_list ? A.slice_list[q] : q) : 0;
     if (q < A.slice_count() &&
         !skip_rows(epi, A.n_long + s * kWarp, min(A.n_long + s * kWarp + kWarp, A.rows) - 1)) {
@@ -293,6 +296,43 @@ __global__ void __launch_bounds__(kBlock) sell_map_kernel(const dev_sell<TM> A,
                                                           double* partials)
 {
   sell_map_block(A, g, epi, partials, (int)blockIdx.x);
+}
+
+// Blocks vb0, vb0 + 1, ... of a sweep's grid only (measurement of one row-length class: the
+// long rows are blocks [0, long_blocks), the slices the rest).
+template <typename TM, typename TG, class Epi>
+__global__ void __launch_bounds__(kBlock) sell_map_range_kernel(const dev_sell<TM> A,
+                                                                const TG* __restrict__ g, Epi epi,
+                                                                double* partials, int vb0)
+{
+  sell_map_block(A, g, epi, partials, vb0 + (int)blockIdx.x);
+}
+
+// The same sweep with WPB warps per block (the plain sweeps' block shape is autotuned).
+template <typename TM, typename TG, class Epi, int WPB>
+__global__ void __launch_bounds__(WPB * kWarp) sell_map_wpb_kernel(const dev_sell<TM> A,
+                                                                  const TG* __restrict__ g,
+                                                                  Epi epi, double* partials)
+{
+  sell_map_block<TM, TG, Epi, false, WPB>(A, g, epi, partials, (int)blockIdx.x);
+}
+
+// Launches sell_map_wpb_kernel with wpb (4, 8 or 16) warps per block.
+template <typename TM, typename TG, class Epi>
+void launch_sell_wpb(int wpb, const dev_sell<TM>& A, const TG* g, const Epi& epi,
+                     double* partials, cudaStream_t s)
+{
+  const int grid = sell_grid(A, wpb);
+  switch (wpb) {
+    case 4:
+      sell_map_wpb_kernel<TM, TG, Epi, 4><<<grid, 4 * kWarp, 0, s>>>(A, g, epi, partials);
+      break;
+    case 16:
+      sell_map_wpb_kernel<TM, TG, Epi, 16><<<grid, 16 * kWarp, 0, s>>>(A, g, epi, partials);
+      break;
+    default:
+      sell_map_kernel<TM, TG, Epi><<<sell_grid(A), kBlock, 0, s>>>(A, g, epi, partials);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -117,6 +117,7 @@ lp_settings::lp_settings()
      CUOPT_PDLP_TILED_SWEEPS_AUTO},
     {CUOPT_PDLP_PERSISTENT_ITERATIONS, CUOPT_PDLP_PERSISTENT_ITERATIONS_AUTO,
      CUOPT_PDLP_PERSISTENT_ITERATIONS_ON, CUOPT_PDLP_PERSISTENT_ITERATIONS_AUTO},
+    {CUOPT_PDLP_SWEEP_WARPS_PER_BLOCK, 0, 16, 0},
   };
   bparams = {
     {CUOPT_INFEASIBILITY_DETECTION, false}, {CUOPT_STRICT_INFEASIBILITY, false},
@@ -392,6 +393,9 @@ std::string solver_mode_error(const lp_settings& st)
   // Only Stable3, the reference's default mode (solve.cu:167-209), is built; the others need the
   // adaptive step size (adaptive_step_size_strategy.cu:168-270) and the KKT / trust-region
   // restarts, which are not.  Asking for them is an error rather than a silent substitution.
+  const int wpb = st.i(CUOPT_PDLP_SWEEP_WARPS_PER_BLOCK);
+  if (wpb != 0 && wpb != 4 && wpb != 8 && wpb != 16)
+    return "pdlp_sweep_warps_per_block must be 0 (chosen by timing), 4, 8 or 16";
   const int mode = st.i(CUOPT_PDLP_SOLVER_MODE);
   if (mode == CUOPT_PDLP_SOLVER_MODE_STABLE3) return {};
   static const char* names[] = {"Stable1", "Stable2", "Methodical1", "Fast1"};
@@ -415,6 +419,7 @@ pdlp_params params_from_settings(const lp_settings& st)
   prm.refinement_tol    = st.f(CUOPT_PDLP_REFINEMENT_TOLERANCE);
   prm.tiled_sweeps      = st.i(CUOPT_PDLP_TILED_SWEEPS);
   prm.persistent        = st.i(CUOPT_PDLP_PERSISTENT_ITERATIONS);
+  prm.sweep_wpb         = st.i(CUOPT_PDLP_SWEEP_WARPS_PER_BLOCK);
   prm.log_to_console    = st.b(CUOPT_LOG_TO_CONSOLE);
   prm.detect_infeasibility  = st.b(CUOPT_INFEASIBILITY_DETECTION);
   prm.per_constraint_residual = st.b(CUOPT_PER_CONSTRAINT_RESIDUAL);

@@ -93,6 +93,17 @@ std::map<form_key, form_choice>& form_cache()
   static std::map<form_key, form_choice> c;
   return c;
 }
+// Warps per block of the plain sweeps chosen by timing, with the timings (ms per launch with 4, 8
+// and 16 warps per block; primal sweep, then dual sweep), per shape, device and precision.
+struct shape_choice {
+  int wpb_primal, wpb_dual;
+  double ms[2][3];
+};
+std::map<form_key, shape_choice>& shape_cache()
+{
+  static std::map<form_key, shape_choice> c;
+  return c;
+}
 
 template <typename TX>
 class engine {
@@ -250,6 +261,7 @@ class engine {
       if (tune_tiles()) reset_iterates(true);  // the timed sweeps moved the iterates
       trace("engine: sweep autotuning");
     }
+    if (tune_sweep_shape()) reset_iterates(true);
     init_plain_form();
   }
 
@@ -549,28 +561,104 @@ class engine {
   dev_sell<TX> As_view() const { return view_of<TX>(L_.A, As_.data()); }
   dev_sell<TX> ATs_view() const { return view_of<TX>(L_.AT, ATs_.data()); }
 
+  // The plain sweeps (not major, Halpern step fused, no fixed-point error) run with the tuned
+  // number of warps per block; the others with kWarpsPerBlock.
   template <bool MAJOR, bool HALPERN, bool SAVE_ATY>
-  void launch_primal(int it_off)
+  void launch_primal(int it_off, int wpb = 0)
   {
     const auto A = ATs_view();
     primal_epi<TX, MAJOR, HALPERN, SAVE_ATY> e{x_.data(),    cs_.data(),    ls_.data(),
                                                us_.data(),   xa_.data(),    xbar_.data(),
                                                x_.data(),    xhat_.data(),  slack_.data(),
                                                aty_.data(),  scalars_.data(), it_off};
-    sell_map_kernel<TX, TX, decltype(e)><<<sell_grid(A), kBlock, 0, s_>>>(A, y_.data(), e,
-                                                                         partials_.data());
+    if constexpr (!MAJOR && HALPERN && !SAVE_ATY)
+      launch_sell_wpb(wpb ? wpb : wpb_primal_, A, y_.data(), e, partials_.data(), s_);
+    else
+      sell_map_kernel<TX, TX, decltype(e)><<<sell_grid(A), kBlock, 0, s_>>>(A, y_.data(), e,
+                                                                           partials_.data());
     ++launches_;
   }
   template <bool MAJOR, bool HALPERN, bool FPE>
-  void launch_dual(int it_off)
+  void launch_dual(int it_off, int wpb = 0)
   {
     const auto A = As_view();
     dual_epi<TX, MAJOR, HALPERN, FPE> e{y_.data(),    lcs_.data(), ucs_.data(),     ya_.data(),
                                         ybar_.data(), y_.data(),   yhat_.data(),    scalars_.data(),
                                         it_off};
-    sell_map_kernel<TX, TX, decltype(e)><<<sell_grid(A), kBlock, 0, s_>>>(A, xbar_.data(), e,
-                                                                         partials_.data());
+    if constexpr (!MAJOR && HALPERN && !FPE)
+      launch_sell_wpb(wpb ? wpb : wpb_dual_, A, xbar_.data(), e, partials_.data(), s_);
+    else
+      sell_map_kernel<TX, TX, decltype(e)><<<sell_grid(A), kBlock, 0, s_>>>(A, xbar_.data(), e,
+                                                                           partials_.data());
     ++launches_;
+  }
+
+  // Block shape of the plain sliced-ELL sweeps (pdlp_sweep_warps_per_block = 0): each sweep is timed with
+  // 4, 8 and 16 warps per block (one warm-up and three timed launches, CUDA events on the solve's
+  // stream) and keeps the fastest.  The shape only groups the same warps differently, so the
+  // iterates do not depend on it.  Decisions are remembered per problem shape, device and
+  // precision.  Returns true when sweeps were launched (the caller then resets the iterates).
+  bool tune_sweep_shape()
+  {
+    for (auto& t : wpb_ms_) t[0] = t[1] = t[2] = 0.0;
+    wpb_primal_ = wpb_dual_ = p_.sweep_wpb ? p_.sweep_wpb : kWarpsPerBlock;
+    if (p_.sweep_wpb) return false;
+    int dev = 0;
+    B200_CUDA_CHECK(cudaGetDevice(&dev));
+    const form_key key{in_.m, in_.n, L_.nnz, dev, (int)sizeof(TX)};
+    {
+      std::lock_guard<std::mutex> lock(tune_mutex());
+      auto it = shape_cache().find(key);
+      if (it != shape_cache().end()) {
+        wpb_primal_ = it->second.wpb_primal;
+        wpb_dual_   = it->second.wpb_dual;
+        std::memcpy(wpb_ms_, it->second.ms, sizeof(wpb_ms_));
+        return false;
+      }
+    }
+    set_scalars(0);
+    cudaEvent_t e0, e1;
+    B200_CUDA_CHECK(cudaEventCreate(&e0));
+    B200_CUDA_CHECK(cudaEventCreate(&e1));
+    auto time_of = [&](auto&& launch) {
+      launch();
+      B200_CUDA_CHECK(cudaEventRecord(e0, s_));
+      for (int i = 0; i < 3; ++i) launch();
+      B200_CUDA_CHECK(cudaEventRecord(e1, s_));
+      B200_CUDA_CHECK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      B200_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+      return (double)ms / 3.0;
+    };
+    static constexpr int kShapes[3] = {4, 8, 16};
+    for (int q = 0; q < 3; ++q) {
+      const int w = kShapes[q];
+      if (!(tile_primal_)) wpb_ms_[0][q] = time_of([&] { launch_primal<false, true, false>(0, w); });
+      if (!(tile_dual_)) wpb_ms_[1][q] = time_of([&] { launch_dual<false, true, false>(0, w); });
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    auto best = [&](const double* t) {
+      int b = 1;
+      for (int q = 0; q < 3; ++q)
+        if (t[q] > 0 && t[q] < t[b]) b = q;
+      return kShapes[b];
+    };
+    wpb_primal_ = best(wpb_ms_[0]);
+    wpb_dual_   = best(wpb_ms_[1]);
+    {
+      std::lock_guard<std::mutex> lock(tune_mutex());
+      shape_choice c{wpb_primal_, wpb_dual_, {}};
+      std::memcpy(c.ms, wpb_ms_, sizeof(wpb_ms_));
+      shape_cache()[key] = c;
+    }
+    if (std::getenv("CUOPT_B200_TRACE"))
+      std::fprintf(stderr,
+                   "[cuopt_b200] sweep block shape: primal %.4f/%.4f/%.4f ms -> %d warps; dual "
+                   "%.4f/%.4f/%.4f ms -> %d warps (4/8/16 warps per block)\n",
+                   wpb_ms_[0][0], wpb_ms_[0][1], wpb_ms_[0][2], wpb_primal_, wpb_ms_[1][0],
+                   wpb_ms_[1][1], wpb_ms_[1][2], wpb_dual_);
+    return true;
   }
 
   // Tiled forms of the plain (non-major, Halpern) sweeps: the tile kernel's partial sums, then the
@@ -990,6 +1078,9 @@ class engine {
     r.persistent_blocks   = persist_grid_;
     r.us_plain_graphs     = form_.decided() ? form_us_[0] : form_.us_per_iteration(0);
     r.us_plain_persistent = form_.decided() ? form_us_[1] : form_.us_per_iteration(1);
+    r.wpb_primal          = wpb_primal_;
+    r.wpb_dual            = wpb_dual_;
+    std::memcpy(r.wpb_ms, wpb_ms_, sizeof(wpb_ms_));
   }
 
   bool meets(const conv_info& cv, double tol) const
@@ -1304,6 +1395,9 @@ class engine {
   plain_form_tuner form_;
   form_key form_key_{};
   double form_us_[2] = {0, 0};  // the timings behind the choice (this solve's or the cached ones)
+  // Warps per block of the plain sweeps and the timings they were chosen by.
+  int wpb_primal_ = kWarpsPerBlock, wpb_dual_ = kWarpsPerBlock;
+  double wpb_ms_[2][3] = {{0, 0, 0}, {0, 0, 0}};
 
   double obj_scale_ = 1.0, obj_offset_ = 0.0;
   double c_norm_ = 0, b_norm_ = 0, beta_ = 1, gamma_ = 1;
@@ -1313,6 +1407,56 @@ class engine {
   double launches_ = 0;
 
  public:
+  // The plain sweeps split by row-length class: the long-row blocks and the slice blocks of each
+  // sweep launched alone (8 warps per block), `iterations` times each after one warm-up.
+  void profile_classes(sweep_profile& p, int iterations)
+  {
+    const auto A = As_view(), AT = ATs_view();
+    persist_pe pe{x_.data(),   cs_.data(),   ls_.data(),    us_.data(),  xa_.data(),
+                  xbar_.data(), x_.data(),   xhat_.data(),  slack_.data(), aty_.data(),
+                  scalars_.data(), 0};
+    persist_de de{y_.data(),    lcs_.data(), ucs_.data(),  ya_.data(),      ybar_.data(),
+                  y_.data(),    yhat_.data(), scalars_.data(), 0};
+    cudaEvent_t e0, e1;
+    B200_CUDA_CHECK(cudaEventCreate(&e0));
+    B200_CUDA_CHECK(cudaEventCreate(&e1));
+    auto time_of = [&](auto&& launch) {
+      launch();
+      B200_CUDA_CHECK(cudaEventRecord(e0, s_));
+      for (int i = 0; i < iterations; ++i) launch();
+      B200_CUDA_CHECK(cudaEventRecord(e1, s_));
+      B200_CUDA_CHECK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      B200_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+      return (double)ms / iterations;
+    };
+    auto classes = [&](const dev_matrix& M, const dev_sell<TX>& V, auto&& launch, double* out) {
+      int64_t long_nnz = 0;
+      B200_CUDA_CHECK(cudaMemcpyAsync(&long_nnz, M.long_off.data() + M.n_long, sizeof(int64_t),
+                                      cudaMemcpyDeviceToHost, s_));
+      B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+      const int lb = long_blocks(V.long_count()), g = sell_grid(V);
+      out[0] = M.n_long;
+      out[1] = (double)long_nnz;
+      out[2] = lb > 0 ? time_of([&] { launch(lb, 0); }) : 0.0;
+      out[3] = M.rows - M.n_long;
+      out[4] = (double)(L_.nnz - long_nnz);
+      out[5] = (double)(M.stored() - (long_nnz + kChunk - 1) / kChunk * kChunk);
+      out[6] = g > lb ? time_of([&] { launch(g - lb, lb); }) : 0.0;
+    };
+    classes(L_.AT, AT, [&](int grid, int vb0) {
+      sell_map_range_kernel<TX, TX, persist_pe><<<grid, kBlock, 0, s_>>>(AT, y_.data(), pe,
+                                                                         partials_.data(), vb0);
+    }, p.classes[0]);
+    classes(L_.A, A, [&](int grid, int vb0) {
+      sell_map_range_kernel<TX, TX, persist_de><<<grid, kBlock, 0, s_>>>(A, xbar_.data(), de,
+                                                                         partials_.data(), vb0);
+    }, p.classes[1]);
+    B200_LAUNCH_CHECK();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+
   // Times plain iterations sweep by sweep (measurement hook).
   sweep_profile profile(int iterations)
   {
@@ -1345,6 +1489,7 @@ class engine {
     for (auto& e : ev) cudaEventDestroy(e);
     p.ms_primal /= iterations;
     p.ms_dual /= iterations;
+    profile_classes(p, iterations);
     // Algorithmic bytes (CSR accounting): matrix values + indices, row offsets, one gather pass,
     // epilogue vectors (primal: read x c l u x_anchor, write x_bar x; dual: read y lc uc y_anchor,
     // write y).

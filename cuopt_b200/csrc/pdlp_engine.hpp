@@ -61,6 +61,7 @@ struct pdlp_params {
   int refinement_passes   = 0;
   int tiled_sweeps        = -1;  // mixed precision: -1 autotuned, 0 sliced ELL only, 1 tiled
   int persistent          = -1;  // plain iterations: -1 timed choice, 0 CUDA graphs, 1 persistent
+  int sweep_wpb           = 0;  // plain sweeps: warps per block (0: chosen by timing 4, 8, 16)
   double refinement_tol   = 1e-8;
   bool log_to_console     = false;
   // Infeasibility detection (CUOPT_INFEASIBILITY_DETECTION and its two tolerances).
@@ -112,10 +113,19 @@ struct pdlp_result {
   // choice was made (0 where it was not timed).
   int plain_form = 0, persistent_blocks = 0;
   double us_plain_graphs = 0, us_plain_persistent = 0;
+  // Warps per block of the plain primal / dual sweeps and the ms per launch measured with 4, 8
+  // and 16 warps per block (0 where not timed).
+  int wpb_primal = 8, wpb_dual = 8;
+  double wpb_ms[2][3] = {{0, 0, 0}, {0, 0, 0}};
 };
 
 struct sweep_profile {
   double ms_primal = 0, ms_dual = 0, bytes_primal = 0, bytes_dual = 0;
+  // Per row-length class, for the primal sweep (classes[0], rows of A^T) and the dual sweep
+  // (classes[1], rows of A): [0] rows in the long class (warp per row), [1] their non-zeros,
+  // [2] ms of the long-row blocks launched alone, [3] rows in slices, [4] their non-zeros, [5]
+  // stored slice elements (padding included), [6] ms of the slice blocks launched alone.
+  double classes[2][7] = {};
 };
 
 // The same LP with every array in device memory (user order).

@@ -17,7 +17,7 @@ from enum import IntEnum
 
 import numpy as np
 
-from ._lib import PDLPStatistics, handle_t, lib
+from ._lib import PDLPStatistics, handle_t, lib, stats_dict
 
 # Parameter names (reference constants.h:23-76)
 CUOPT_ABSOLUTE_DUAL_TOLERANCE = "absolute_dual_tolerance"
@@ -41,6 +41,7 @@ CUOPT_PDLP_REFINEMENT_PASSES = "pdlp_refinement_passes"
 CUOPT_PDLP_REFINEMENT_TOLERANCE = "pdlp_refinement_tolerance"
 CUOPT_PDLP_TILED_SWEEPS = "pdlp_tiled_sweeps"
 CUOPT_PDLP_PERSISTENT_ITERATIONS = "pdlp_persistent_iterations"
+CUOPT_PDLP_SWEEP_WARPS_PER_BLOCK = "pdlp_sweep_warps_per_block"
 
 _TOLERANCE_NAMES = (CUOPT_ABSOLUTE_DUAL_TOLERANCE, CUOPT_RELATIVE_DUAL_TOLERANCE,
                     CUOPT_ABSOLUTE_PRIMAL_TOLERANCE, CUOPT_RELATIVE_PRIMAL_TOLERANCE,
@@ -393,7 +394,7 @@ def _read_solution(sol: handle_t, m: int, n: int) -> Solution:
     L.cuOptGetErrorString(sol, buf, 1024)
     st = PDLPStatistics()
     L.cuOptGetPDLPStatistics(sol, C.byref(st))
-    stats = {f: getattr(st, f) for f, _ in PDLPStatistics._fields_}
+    stats = stats_dict(st)
     x, y, rc = np.zeros(n), np.zeros(m), np.zeros(n)
     if err.value == 0:
         L.cuOptGetPrimalSolution(sol, _ptr(x))

@@ -52,7 +52,7 @@ def main() -> None:
     import torch
 
     from cuopt_b200 import generators as gen
-    from cuopt_b200._lib import PDLPStatistics, lib
+    from cuopt_b200._lib import PDLPStatistics, lib, stats_dict
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c1_small")
@@ -145,7 +145,7 @@ def main() -> None:
             if code != 0:
                 break
         out.update({"rc": code, "status": status.value, "wall_s": walls[-1], "walls_s": walls})
-        out.update({f: getattr(st, f) for f, _ in PDLPStatistics._fields_})
+        out.update(stats_dict(st))
         out["objective_rel_error"] = abs(st.primal_objective - lp.optimal_objective) / max(
             1.0, abs(lp.optimal_objective))
         if code != 0:
@@ -159,11 +159,38 @@ def main() -> None:
         if code == 0:
             out["gbs_primal"] = vals[2].value / vals[0].value / 1e6
             out["gbs_dual"] = vals[3].value / vals[1].value / 1e6
+            out["classes"] = sweep_classes(L, m, n, ptr, s, stream, a.iterations,
+                                           4 if a.precision == "mixed" else 8)
         else:
             print(json.dumps(out))
             sys.exit(1)
     L.cuOptDestroySolverSettings(C.byref(s))
     print(json.dumps(out))
+
+
+def sweep_classes(L, m, n, ptr, settings, stream, iterations, elem) -> dict:
+    """The plain sweeps split by row-length class (cuOptProfileSweepClasses): per sweep and class,
+    rows, non-zeros, padding, ms per launch, gathers/s and algorithmic GB/s (values + indices of
+    the non-zeros, the row's offset and its epilogue vectors: primal 7, dual 5 elements)."""
+    out_v = (C.c_double * 14)()
+    code = L.cuOptProfileSweepClasses(m, n, *ptr, settings, stream, iterations, out_v)
+    if code != 0:
+        raise RuntimeError(f"cuOptProfileSweepClasses returned {code}")
+    res = {}
+    for s, (name, epi) in enumerate((("primal", 7), ("dual", 5))):
+        v = list(out_v[7 * s:7 * s + 7])
+        long_rows, long_nnz, long_ms, sl_rows, sl_nnz, sl_stored, sl_ms = v
+
+        def cls(rows, nnz, ms, stored, offset_bytes):
+            if rows == 0 or ms == 0:
+                return {"rows": int(rows), "nnz": int(nnz)}
+            byts = nnz * (elem + 4) + rows * (epi * elem + offset_bytes)
+            return {"rows": int(rows), "nnz": int(nnz), "stored": int(stored),
+                    "ms": ms, "gathers_per_s": nnz / (ms * 1e-3),
+                    "algorithmic_gbs": byts / (ms * 1e-3) / 1e9}
+        res[name] = {"long_rows": cls(long_rows, long_nnz, long_ms, long_nnz, 8),
+                     "sliced_rows": cls(sl_rows, sl_nnz, sl_ms, sl_stored, 8 / 32)}
+    return res
 
 
 def gather_rates(m: int, n: int, nnz: int, stream) -> dict:
@@ -292,7 +319,10 @@ def run_batch(a, models=None) -> dict:
                    sols[0].stats.get("plain_iteration_form"), "undecided"),
                "persistent_blocks": sols[0].stats.get("persistent_blocks"),
                "us_per_iteration_graphs": sols[0].stats.get("plain_iteration_us_graphs"),
-               "us_per_iteration_persistent": sols[0].stats.get("plain_iteration_us_persistent")},
+               "us_per_iteration_persistent": sols[0].stats.get("plain_iteration_us_persistent"),
+               "sweep_warps_per_block": [sols[0].stats.get("sweep_warps_per_block_primal"),
+                                         sols[0].stats.get("sweep_warps_per_block_dual")],
+               "sweep_block_shape_ms": sols[0].stats.get("sweep_block_shape_ms")},
            "worst_instances": [{"i": i, "m": lps[i].m, "status": status[i], "iterations": iters[i],
                                 "objective_rel_error": obj_err[i], "relative_kkt": kkt[i],
                                 "optimal_objective": lps[i].optimal_objective,

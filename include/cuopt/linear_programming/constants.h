@@ -104,6 +104,11 @@
 #define CUOPT_PDLP_PERSISTENT_ITERATIONS_AUTO -1
 #define CUOPT_PDLP_PERSISTENT_ITERATIONS_OFF  0
 #define CUOPT_PDLP_PERSISTENT_ITERATIONS_ON   1
+/* pdlp_sweep_warps_per_block: block shape of the plain sliced-ELL sweeps.  0 (default) chooses
+ * 4, 8 or 16 warps per block by timing each sweep at the first solve of a problem shape; 4, 8 or
+ * 16 fixes it (other values are a validation error).  The shape does not change any row's
+ * arithmetic, so the iterates are the same for every choice. */
+#define CUOPT_PDLP_SWEEP_WARPS_PER_BLOCK "pdlp_sweep_warps_per_block"
 
 #define CUOPT_MODE_OPPORTUNISTIC 0
 #define CUOPT_MODE_DETERMINISTIC 1

@@ -49,6 +49,12 @@ typedef struct {
   cuopt_int_t persistent_blocks;
   cuopt_float_t plain_iteration_us_graphs;
   cuopt_float_t plain_iteration_us_persistent;
+  /* Warps per block of the plain primal and dual sweeps (pdlp_sweep_warps_per_block), and the
+   * milliseconds per launch each shape took when they were chosen: primal with 4, 8, 16 warps,
+   * then dual with 4, 8, 16 (0 where not timed). */
+  cuopt_int_t sweep_warps_per_block_primal;
+  cuopt_int_t sweep_warps_per_block_dual;
+  cuopt_float_t sweep_block_shape_ms[6];
 } cuOptPDLPStatistics;
 
 cuopt_int_t cuOptGetPDLPStatistics(cuOptSolution solution, cuOptPDLPStatistics* stats);
@@ -121,6 +127,28 @@ cuopt_int_t cuOptProfileGatherRate(cuopt_int_t vector_length,
                                    void* stream,
                                    cuopt_float_t* gathers_per_second,
                                    cuopt_int_t* chunks_in_flight);
+
+/* Measurement hook (no counterpart in the reference): the plain sweeps of cuOptProfilePDHGSweeps
+ * split by row-length class.  After the same preparation, the long-row blocks (one warp per row)
+ * and the slice blocks (32-row slices) of each sweep are launched alone, `iterations` times each
+ * after a warm-up, with 8 warps per block.  out (14 values): for the primal sweep (rows of A^T),
+ * then the dual sweep (rows of A): rows in the long class, their non-zeros, ms per launch of the
+ * long-row blocks, rows in slices, their non-zeros, stored slice elements (padding included), ms
+ * per launch of the slice blocks. */
+cuopt_int_t cuOptProfileSweepClasses(cuopt_int_t num_constraints,
+                                     cuopt_int_t num_variables,
+                                     const cuopt_float_t* d_objective_coefficients,
+                                     const cuopt_int_t* d_row_offsets,
+                                     const cuopt_int_t* d_column_indices,
+                                     const cuopt_float_t* d_values,
+                                     const cuopt_float_t* d_constraint_lower_bounds,
+                                     const cuopt_float_t* d_constraint_upper_bounds,
+                                     const cuopt_float_t* d_variable_lower_bounds,
+                                     const cuopt_float_t* d_variable_upper_bounds,
+                                     cuOptSolverSettings settings,
+                                     void* stream,
+                                     cuopt_int_t iterations,
+                                     double* out);
 
 /* Measurement hook (no counterpart in the reference): prepares the device-resident LP exactly as
  * cuOptSolveDevice does, then runs `iterations` plain PDHG iterations launching the two fused

@@ -73,6 +73,46 @@ def test_persistent_matches_graphs_at_iteration_limits(lp_c0):
         _same(g, p)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_sweep_block_shapes_give_the_same_iterates(lp_c0, precision):
+    """4, 8 and 16 warps per block and the timed choice (pdlp_sweep_warps_per_block) only group
+    the same warps differently: bit-identical solves."""
+    dm = datamodel_from_lp(lp_c0)
+    sols = {}
+    for w in (0, 4, 8, 16):
+        s = _settings(GRAPHS, tol=1e-6, precision=precision)
+        s.set_parameter(lpm.CUOPT_PDLP_SWEEP_WARPS_PER_BLOCK, w)
+        sols[w] = lpm.Solve(dm, s)
+    for w in (4, 8, 16):
+        assert sols[w].stats["sweep_warps_per_block_primal"] == w
+        assert sols[w].stats["sweep_warps_per_block_dual"] == w
+        _same(sols[8], sols[w])
+    _same(sols[8], sols[0])
+    assert sols[0].stats["sweep_warps_per_block_primal"] in (4, 8, 16)
+    assert all(t > 0 for t in sols[0].stats["sweep_block_shape_ms"])
+    lp = gen.skewed_lp(400, 3000, seed=7, cap=3000)  # long rows (warp per row) as well
+    a, b = (lpm.Solve(datamodel_from_lp(lp), _settings(GRAPHS, tol=1e-6)) for _ in range(2))
+    s = _settings(GRAPHS, tol=1e-6)
+    s.set_parameter(lpm.CUOPT_PDLP_SWEEP_WARPS_PER_BLOCK, 16)
+    _same(a, lpm.Solve(datamodel_from_lp(lp), s))
+
+
+def test_batch_sweep_block_shapes_give_the_same_iterates():
+    lps = [gen.constructed_lp(m, int(2.5 * m), k, seed=90 + i)
+           for i, (m, k) in enumerate([(300, 6), (1100, 10), (2500, 8)])]
+    dms = [datamodel_from_lp(lp) for lp in lps]
+    ref = None
+    for w in (0, 4, 16):
+        s = _settings(GRAPHS, tol=1e-6, precision=1)
+        s.set_parameter(lpm.CUOPT_PDLP_SWEEP_WARPS_PER_BLOCK, w)
+        sols = lpm.BatchSolve(dms, s)[0]
+        if ref is None:
+            ref = sols
+        else:
+            for a, b in zip(ref, sols):
+                _same(a, b)
+
+
 def test_persistent_long_rows():
     """Long rows (warp per row) and sliced rows in the same persistent sweeps."""
     lp = gen.skewed_lp(400, 3000, seed=7, cap=3000)

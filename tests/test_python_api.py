@@ -62,3 +62,15 @@ def test_unbuilt_solver_modes_are_rejected(mode, name):
     assert name in sol.get_error_message()
     sols, _ = lpm.BatchSolve([chess_set_lp(), chess_set_lp()], s)
     assert all(x.get_error_status() == lpm.ErrorStatus.ValidationError for x in sols)
+
+
+@pytest.mark.parametrize("w", [1, 5, 12])
+def test_sweep_block_shape_must_be_a_built_one(w):
+    """pdlp_sweep_warps_per_block accepts 0 (timed choice), 4, 8 and 16; other values end with a
+    validation error before any device work."""
+    s = lpm.SolverSettings()
+    s.set_parameter(lpm.CUOPT_PDLP_SWEEP_WARPS_PER_BLOCK, w)
+    s.set_parameter(lpm.CUOPT_LOG_TO_CONSOLE, False)
+    sol = lpm.Solve(chess_set_lp(), s)
+    assert sol.get_error_status() == lpm.ErrorStatus.ValidationError
+    assert "pdlp_sweep_warps_per_block" in sol.get_error_message()
