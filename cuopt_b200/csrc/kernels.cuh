@@ -199,14 +199,15 @@ __device__ __forceinline__ bool skip_rows(const Epi& epi, int r0, int r1)
 // kernel that walks the grid).
 // Gathered-vector loads.  A kernel that writes the gathered vector itself (the persistent
 // iterations below) reads it through L2 (ld.global.cg), which its grid barrier keeps coherent;
-// every other sweep may use the read-only path.
+// every other sweep reads it through the read-only path (ld.global.nc): no sweep writes the
+// vector it gathers.
 template <bool COH, typename T>
 __device__ __forceinline__ T gather_load(const T* __restrict__ g, int i)
 {
   if constexpr (COH)
     return __ldcg(g + i);
   else
-    return g[i];
+    return __ldg(g + i);
 }
 
 // WPB: warps (rows or slices) per block.  Only the grouping of warps into blocks depends on it,
