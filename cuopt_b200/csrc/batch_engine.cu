@@ -1293,9 +1293,10 @@ class batch_engine {
     ++launches_;
   }
 
-  // Block shape of the plain sweeps over all instances (pdlp_sweep_warps_per_block = 0): 4, 8 and 16 warps
-  // per block, one warm-up and three timed launches each; the fastest is kept.  The iterates the
-  // timed sweeps move are restored (x, y) or cleared (x_bar, y_bar) afterwards.
+  // Block shape of the plain sweeps over all instances (pdlp_sweep_warps_per_block = 0): 4, 8 and
+  // 16 warps per block, a warm-up launch and about 1 ms of launches each; another shape replaces 8
+  // warps when it is at least 3 % faster.  The iterates the timed sweeps move are restored (x, y) or
+  // cleared (x_bar, y_bar) afterwards.
   void tune_sweep_shape()
   {
     wpb_primal_ = wpb_dual_ = p_.sweep_wpb ? p_.sweep_wpb : kWarpsPerBlock;
@@ -1310,15 +1311,21 @@ class batch_engine {
     cudaEvent_t e0, e1;
     B200_CUDA_CHECK(cudaEventCreate(&e0));
     B200_CUDA_CHECK(cudaEventCreate(&e1));
+    // One warm-up launch, then enough launches for about a millisecond of timed work (at least 3).
     auto time_of = [&](auto&& launch) {
-      launch();
       B200_CUDA_CHECK(cudaEventRecord(e0, s_));
-      for (int i = 0; i < 3; ++i) launch();
+      launch();
       B200_CUDA_CHECK(cudaEventRecord(e1, s_));
       B200_CUDA_CHECK(cudaEventSynchronize(e1));
       float ms = 0.f;
       B200_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-      return (double)ms / 3.0;
+      const int reps = std::max(3, std::min(200, (int)std::ceil(1.0 / std::max(ms, 1e-3f))));
+      B200_CUDA_CHECK(cudaEventRecord(e0, s_));
+      for (int i = 0; i < reps; ++i) launch();
+      B200_CUDA_CHECK(cudaEventRecord(e1, s_));
+      B200_CUDA_CHECK(cudaEventSynchronize(e1));
+      B200_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+      return (double)ms / reps;
     };
     static constexpr int kShapes[3] = {4, 8, 16};
     for (int q = 0; q < 3; ++q) {
@@ -1327,10 +1334,11 @@ class batch_engine {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    // Another shape replaces the default 8 warps only when it is at least 3 % faster.
     auto best = [&](const double* t) {
       int b = 1;
       for (int q = 0; q < 3; ++q)
-        if (t[q] < t[b]) b = q;
+        if (t[q] > 0 && t[q] < 0.97 * t[1] && t[q] < t[b]) b = q;
       return kShapes[b];
     };
     wpb_primal_ = best(wpb_ms_[0]);
