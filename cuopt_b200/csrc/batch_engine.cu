@@ -299,6 +299,40 @@ __global__ void bound_terms_kernel(const double* lo, const double* up, int n, do
   }
 }
 
+// Instance ranges in the internal order, where each instance's items are contiguous inside
+// [0, n_long) and inside [n_long, count): r[b] = {long_lo, long_hi, short_lo, short_hi}.  Segment
+// starts and ends are found where the instance id changes; an id out of [0, B) or a decrease
+// inside a part (instances not contiguous) is counted in bad[0].  r must be zeroed first.
+__global__ void instance_ranges_kernel(const int* inst, int count, int n_long, int B, int4* r,
+                                       int* bad)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const int b = inst[i];
+    if (b < 0 || b >= B) {
+      atomicAdd(bad, 1);
+      continue;
+    }
+    const bool is_long = i < n_long;
+    const bool first   = i == 0 || i == n_long;
+    const bool last    = i == count - 1 || i == n_long - 1;
+    const int prev     = first ? -1 : inst[i - 1];
+    const int next     = last ? -1 : inst[i + 1];
+    if (!first && prev > b) atomicAdd(bad, 1);
+    if (first || prev != b) {
+      if (is_long)
+        r[b].x = i;
+      else
+        r[b].z = i;
+    }
+    if (last || next != b) {
+      if (is_long)
+        r[b].y = i + 1;
+      else
+        r[b].w = i + 1;
+    }
+  }
+}
+
 __global__ void gather_int_kernel(const int* src, const int* perm, int count, int* dst)
 {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
@@ -703,6 +737,7 @@ class batch_engine {
     B200_LAUNCH_CHECK();
     rranges_ = ranges_of(rinst_, m, L_.A.n_long);
     cranges_ = ranges_of(cinst_, n, L_.AT.n_long);
+    trace("batch: instance ranges");
     rr_d_.resize(B_);
     cr_d_.resize(B_);
     rr_d_.upload(rranges_.data(), B_, s_);
@@ -836,31 +871,21 @@ class batch_engine {
   // instance ids are sorted inside [0, n_long) and inside [n_long, count).
   std::vector<int4> ranges_of(const dbuf<int>& inst, int count, int n_long)
   {
-    std::vector<int> h(count);
-    inst.download(h.data(), count, s_);
+    dbuf<int4> r(B_);
+    dbuf<int> bad(1);
+    r.zero(s_);
+    bad.zero(s_);
+    if (count > 0)
+      instance_ranges_kernel<<<vgrid_, kBlock, 0, s_>>>(inst.data(), count, n_long, B_, r.data(),
+                                                        bad.data());
+    B200_LAUNCH_CHECK();
+    std::vector<int4> h(B_);
+    int hbad = 0;
+    r.download(h.data(), B_, s_);
+    bad.download(&hbad, 1, s_);
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
-    std::vector<int4> r(B_, int4{0, 0, 0, 0});
-    std::vector<char> seen_long(B_, 0), seen_short(B_, 0);
-    for (int i = 0; i < count; ++i) {
-      const int b      = h[i];
-      const bool is_lo = i < n_long;
-      if (b < 0 || b >= B_) throw std::runtime_error("batch layout: instance id out of range");
-      if (i > 0 && i != n_long && h[i - 1] > b)
-        throw std::runtime_error("batch layout: instances not contiguous");
-      auto& seen = is_lo ? seen_long : seen_short;
-      if (!seen[b]) {
-        seen[b] = 1;
-        if (is_lo)
-          r[b].x = i;
-        else
-          r[b].z = i;
-      }
-      if (is_lo)
-        r[b].y = i + 1;
-      else
-        r[b].w = i + 1;
-    }
-    return r;
+    if (hbad) throw std::runtime_error("batch layout: instance ids out of range or not contiguous");
+    return h;
   }
 
   void fill(double* p, int n, double v)
