@@ -199,15 +199,16 @@ __device__ __forceinline__ bool skip_rows(const Epi& epi, int r0, int r1)
 // kernel that walks the grid).
 // Gathered-vector loads.  A kernel that writes the gathered vector itself (the persistent
 // iterations below) reads it through L2 (ld.global.cg), which its grid barrier keeps coherent;
-// every other sweep reads it through the read-only path (ld.global.nc): no sweep writes the
-// vector it gathers.
+// every other sweep uses plain loads of the restrict-qualified vector, which no sweep writes
+// (an explicit __ldg measured slower on the mixed-precision primal sweep: 73.1 against 69.9 us on
+// the 1M x 2M LP).
 template <bool COH, typename T>
 __device__ __forceinline__ T gather_load(const T* __restrict__ g, int i)
 {
   if constexpr (COH)
     return __ldcg(g + i);
   else
-    return __ldg(g + i);
+    return g[i];
 }
 
 // WPB: warps (rows or slices) per block.  Only the grouping of warps into blocks depends on it,
