@@ -822,42 +822,57 @@ struct power_state {
   int iters;
 };
 
-static __global__ void power_normalize_kernel(const double* z, double* q, int m, const double* sumsq,
-                                       power_state* ps)
+// The power iteration's vector steps.  Each scalar a step needs is summed by the consuming block
+// itself from the producer's block partials (ordered_block_sum, as finalize_sum_kernel does, so
+// every block gets the value finalize_sum_kernel would store): no separate finalize launches.
+//   q = z / |z|, |z|^2 from the vec_reduce partials (nz blocks).
+static __global__ void __launch_bounds__(kBlock)
+  power_normalize_sum_kernel(const double* z, double* q, int m, const double* part_z, int nz,
+                             power_state* ps)
 {
   if (ps->done) return;
-  const double nq = sqrt(*sumsq);
+  __shared__ double total;
+  ordered_block_sum<1>(part_z, nz, &total);
+  const double nq = sqrt(total);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
     q[i] = z[i] / nq;
   if (blockIdx.x == 0 && threadIdx.x == 0) ps->norm_z = nq;
 }
-
-// q <- q * (-s2) + z ; partial sum of squares of the result.
-static __global__ void __launch_bounds__(kBlock) power_residual_kernel(double* q, const double* z, int m,
-                                                                const double* s2,
-                                                                const power_state* ps,
-                                                                double* partials)
+//   s2 = q . z from the power_z sweep's partials (ns blocks); q <- q (-s2) + z; partial sums of
+//   squares of the result in part_r.
+static __global__ void __launch_bounds__(kBlock)
+  power_residual_sum_kernel(double* q, const double* z, int m, const double* part_s, int ns,
+                            const power_state* ps, double* part_r)
 {
   red_t<1> r;
   r.v[0] = 0.0;
   if (!ps->done) {
-    const double s = *s2;
+    __shared__ double s2;
+    ordered_block_sum<1>(part_s, ns, &s2);
+    const double s = s2;
     for (int i = blockIdx.x * kBlock + threadIdx.x; i < m; i += gridDim.x * kBlock) {
       const double v = q[i] * -s + z[i];
       q[i]           = v;
       r.v[0] += v * v;
     }
   }
-  block_reduce_store<1>(r, partials);
+  block_reduce_store<1>(r, part_r);
 }
-
-static __global__ void power_check_kernel(power_state* ps, const double* s2, const double* rsq, double tol)
+//   Record s2 and the residual (one block); done once the residual is below tol.
+static __global__ void __launch_bounds__(kBlock)
+  power_check_sum_kernel(power_state* ps, const double* part_s, int ns, const double* part_r,
+                         int nr, double tol)
 {
   if (ps->done) return;
-  ps->s2    = *s2;
-  ps->resid = sqrt(*rsq);
-  ps->iters += 1;
-  if (ps->resid < tol) ps->done = 1;
+  __shared__ double s2, rsq;
+  ordered_block_sum<1>(part_s, ns, &s2);
+  ordered_block_sum<1>(part_r, nr, &rsq);
+  if (threadIdx.x == 0) {
+    ps->s2    = s2;
+    ps->resid = sqrt(rsq);
+    ps->iters += 1;
+    if (ps->resid < tol) ps->done = 1;
+  }
 }
 
 // Golub-Kahan-Lanczos bidiagonalisation of the scaled A (the mixed-precision step size).  The

@@ -442,21 +442,22 @@ class engine {
     const auto As  = view_of<TX>(L_.A, As_.data());
     const auto ATs = view_of<TX>(L_.AT, ATs_.data());
     const int ga = sell_grid(As), gt = sell_grid(ATs);
-    double* res = dres_.data();
+    // Block partials: |z|^2 and q . z in the first half of partials_ (the second overwrites the
+    // first once it is consumed), the residual's in the second half.
+    double* part   = partials_.data();
+    double* part_r = partials_.data() + partials_.size() / 2;
     auto one_iteration = [&]() {
-      vec_reduce_kernel<0, double><<<vgrid_, kBlock, 0, s_>>>(dz.data(), nullptr, m,
-                                                              partials_.data(), &ps.data()->done);
-      finalize_sum_kernel<1><<<1, kBlock, 0, s_>>>(partials_.data(), vgrid_, res + 0);
-      power_normalize_kernel<<<vgrid_, kBlock, 0, s_>>>(dz.data(), dq.data(), m, res + 0, ps.data());
+      vec_reduce_kernel<0, double><<<vgrid_, kBlock, 0, s_>>>(dz.data(), nullptr, m, part,
+                                                              &ps.data()->done);
+      power_normalize_sum_kernel<<<vgrid_, kBlock, 0, s_>>>(dz.data(), dq.data(), m, part, vgrid_,
+                                                            ps.data());
       sell_map_kernel<TX, double, store_epi<double>><<<gt, kBlock, 0, s_>>>(
-        ATs, dq.data(), store_epi<double>{datq.data(), &ps.data()->done}, partials_.data());
+        ATs, dq.data(), store_epi<double>{datq.data(), &ps.data()->done}, part);
       sell_map_kernel<TX, double, power_z_epi><<<ga, kBlock, 0, s_>>>(
-        As, datq.data(), power_z_epi{dz.data(), dq.data(), &ps.data()->done}, partials_.data());
-      finalize_sum_kernel<1><<<1, kBlock, 0, s_>>>(partials_.data(), ga, res + 1);
-      power_residual_kernel<<<vgrid_, kBlock, 0, s_>>>(dq.data(), dz.data(), m, res + 1,
-                                                       ps.data(), partials_.data());
-      finalize_sum_kernel<1><<<1, kBlock, 0, s_>>>(partials_.data(), vgrid_, res + 2);
-      power_check_kernel<<<1, 1, 0, s_>>>(ps.data(), res + 1, res + 2, kPowerTol);
+        As, datq.data(), power_z_epi{dz.data(), dq.data(), &ps.data()->done}, part);
+      power_residual_sum_kernel<<<vgrid_, kBlock, 0, s_>>>(dq.data(), dz.data(), m, part, ga,
+                                                           ps.data(), part_r);
+      power_check_sum_kernel<<<1, kBlock, 0, s_>>>(ps.data(), part, ga, part_r, vgrid_, kPowerTol);
     };
     // Chunks of 32 iterations are captured once into a graph and replayed until convergence.
     cudaGraph_t graph;
@@ -473,7 +474,7 @@ class engine {
       } else {
         B200_CUDA_CHECK(cudaGraphLaunch(exec, s_));
       }
-      launches_ += 9.0 * std::min(32, kPowerMaxIters - done_iters);
+      launches_ += 6.0 * std::min(32, kPowerMaxIters - done_iters);
       B200_CUDA_CHECK(cudaMemcpyAsync(&h, ps.data(), sizeof(h), cudaMemcpyDeviceToHost, s_));
       B200_CUDA_CHECK(cudaStreamSynchronize(s_));
       if (h.done) break;
