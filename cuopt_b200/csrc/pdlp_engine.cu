@@ -446,18 +446,21 @@ class engine {
     // first once it is consumed), the residual's in the second half.
     double* part   = partials_.data();
     double* part_r = partials_.data() + partials_.size() / 2;
+    // The vector steps run on a grid sized to the m entries (at most vgrid_ blocks): small LPs
+    // launch a few blocks instead of vgrid_ mostly idle ones.
+    const int pg = std::max(1, std::min(vgrid_, ceil_div(m, kBlock)));
     auto one_iteration = [&]() {
-      vec_reduce_kernel<0, double><<<vgrid_, kBlock, 0, s_>>>(dz.data(), nullptr, m, part,
-                                                              &ps.data()->done);
-      power_normalize_sum_kernel<<<vgrid_, kBlock, 0, s_>>>(dz.data(), dq.data(), m, part, vgrid_,
-                                                            ps.data());
+      vec_reduce_kernel<0, double><<<pg, kBlock, 0, s_>>>(dz.data(), nullptr, m, part,
+                                                          &ps.data()->done);
+      power_normalize_sum_kernel<<<pg, kBlock, 0, s_>>>(dz.data(), dq.data(), m, part, pg,
+                                                        ps.data());
       sell_map_kernel<TX, double, store_epi<double>><<<gt, kBlock, 0, s_>>>(
         ATs, dq.data(), store_epi<double>{datq.data(), &ps.data()->done}, part);
       sell_map_kernel<TX, double, power_z_epi><<<ga, kBlock, 0, s_>>>(
         As, datq.data(), power_z_epi{dz.data(), dq.data(), &ps.data()->done}, part);
-      power_residual_sum_kernel<<<vgrid_, kBlock, 0, s_>>>(dq.data(), dz.data(), m, part, ga,
-                                                           ps.data(), part_r);
-      power_check_sum_kernel<<<1, kBlock, 0, s_>>>(ps.data(), part, ga, part_r, vgrid_, kPowerTol);
+      power_residual_sum_kernel<<<pg, kBlock, 0, s_>>>(dq.data(), dz.data(), m, part, ga,
+                                                       ps.data(), part_r);
+      power_check_sum_kernel<<<1, kBlock, 0, s_>>>(ps.data(), part, ga, part_r, pg, kPowerTol);
     };
     // Chunks of 32 iterations are captured once into a graph and replayed until convergence.
     cudaGraph_t graph;
