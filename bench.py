@@ -462,6 +462,7 @@ def run_c2(L, torch, device, sptr, args):
         L.cuOptDestroySolverSettings(C.byref(sh))
         it = st["number_of_steps_taken"]
         leg["solve_sample"] = {"iterations": it, "status": status,
+                               "continued_in_fp64": int(st["refinement_passes"] > 0),
                                "pdhg_iter_per_s": it / (st["loop_time"] or 1e-9),
                                "setup_s": st["setup_time"], "relative_kkt": max(
                                    st["l2_relative_primal_residual"],
