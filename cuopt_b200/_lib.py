@@ -47,6 +47,7 @@ class PDLPStatistics(C.Structure):
         ("persistent_blocks", cuopt_int_t),
         ("plain_iteration_us_graphs", cuopt_float_t),
         ("plain_iteration_us_persistent", cuopt_float_t),
+        ("plain_iteration_us_cluster", cuopt_float_t),
         ("sweep_warps_per_block_primal", cuopt_int_t),
         ("sweep_warps_per_block_dual", cuopt_int_t),
         ("sweep_block_shape_ms", cuopt_float_t * 6),

@@ -1422,7 +1422,8 @@ class batch_engine {
     form_active_ = n_active;
     cycle_open_  = false;
     ++form_epochs_;
-    form_.reset(p_.persistent, -1, coop && persist_grid_ > 0);
+    const bool avail[plain_form_tuner::kForms] = {true, coop && persist_grid_ > 0, false};
+    form_.reset(p_.persistent, -1, avail);
     if (n_active == B_ && form_.decided()) {  // forced (or the only form available)
       first_form_   = form_.chosen();
       first_blocks_ = persist_grid_;

@@ -720,6 +720,7 @@ cuopt_int_t cuOptGetPDLPStatistics(cuOptSolution solution, cuOptPDLPStatistics* 
   st->persistent_blocks               = r.persistent_blocks;
   st->plain_iteration_us_graphs       = r.us_plain_graphs;
   st->plain_iteration_us_persistent   = r.us_plain_persistent;
+  st->plain_iteration_us_cluster      = r.us_plain_cluster;
   st->sweep_warps_per_block_primal    = r.wpb_primal;
   st->sweep_warps_per_block_dual      = r.wpb_dual;
   for (int q = 0; q < 6; ++q) st->sweep_block_shape_ms[q] = r.wpb_ms[q / 3][q % 3];

@@ -458,6 +458,110 @@ __global__ void __launch_bounds__(kBlock)
   if (blockIdx.x == 0) adv(L);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Cluster-resident plain iterations for small LPs: one thread-block cluster of C blocks runs a run
+// of L plain iterations.  Every block keeps a full copy of both gathered vectors (y for the primal
+// sweep, x_bar for the dual sweep) in its shared memory, so the sweeps gather from shared memory;
+// a row's new value is written to global memory by its epilogue, as in the other forms, and
+// stored into every block's copy through distributed shared memory (mapa + st.shared::cluster).
+// A cluster barrier (arrive.release / wait.acquire: hardware, no spin loop) follows every sweep.
+// The block's virtual blocks of the sweep are rank, rank + C, ... with 32 warps each; every row is
+// computed by one warp exactly as in sell_map_kernel.
+constexpr int kClusterThreads = 1024;
+constexpr int kClusterWarps   = kClusterThreads / kWarp;
+
+__device__ __forceinline__ unsigned cluster_rank()
+{
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned cluster_size()
+{
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_barrier()
+{
+  asm volatile(
+    "barrier.cluster.arrive.release.aligned;\n"
+    "barrier.cluster.wait.acquire.aligned;\n" ::
+      : "memory");
+}
+// Stores v at shared-memory address saddr (a byte offset in this block's window) of block `rank`
+// of the cluster.
+__device__ __forceinline__ void dsmem_store(unsigned saddr, unsigned rank, double v)
+{
+  unsigned remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(saddr), "r"(rank));
+  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(remote), "d"(v) : "memory");
+}
+__device__ __forceinline__ void dsmem_store(unsigned saddr, unsigned rank, float v)
+{
+  unsigned remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(saddr), "r"(rank));
+  asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(remote), "f"(v) : "memory");
+}
+
+// Wraps a plain epilogue: after the row's step, the value the step stored into the gathered
+// vector (read back by the same thread) goes to every block's copy of that vector.
+template <class Base, typename TX>
+struct cluster_bcast_epi {
+  static constexpr int kRed = 0;
+  using pre_t               = typename Base::pre_t;
+  Base base;
+  const TX* written;  // the global vector the step stores into (x_bar or y)
+  unsigned copy;      // shared-memory address of this block's copy of that vector
+  unsigned blocks;    // cluster size
+  __device__ bool skip() const { return base.skip(); }
+  __device__ __forceinline__ pre_t load(int r) const { return base.load(r); }
+  __device__ __forceinline__ void operator()(int r, double acc, const pre_t& p, red_t<0>& red) const
+  {
+    base(r, acc, p, red);
+    const TX v            = written[r];
+    const unsigned target = copy + (unsigned)(r * (int)sizeof(TX));
+    for (unsigned c = 0; c < blocks; ++c) dsmem_store(target, c, v);
+  }
+};
+
+// Dynamic shared memory: the copy of y (m elements), then the copy of x_bar (n elements), the first
+// padded to 16 elements.  pe / de: the plain primal / dual epilogues (it_off set per iteration),
+// whose gathered vectors are y (de.y = de.yout) and x_bar (pe.xbar); gp / gd: the sweeps' virtual
+// block counts with kClusterWarps warps per block.
+template <typename TX, class PE, class DE>
+__global__ void __launch_bounds__(kClusterThreads)
+  cluster_plain_kernel(const dev_sell<TX> AT, const dev_sell<TX> A, PE pe, DE de, int L, int m,
+                       int gp, int gd, pdlp_scalars* st)
+{
+  extern __shared__ __align__(16) unsigned char cl_smem[];
+  TX* ys          = reinterpret_cast<TX*>(cl_smem);
+  const int m_pad = (m + 15) & ~15;
+  TX* xbs         = ys + m_pad;
+  const unsigned rank = cluster_rank(), blocks = cluster_size();
+  for (int i = threadIdx.x; i < m; i += blockDim.x) ys[i] = de.y[i];
+  // Every block of the cluster is running (and has its copy of y) before any block stores into
+  // another's shared memory.
+  cluster_barrier();
+  const unsigned ys_addr  = (unsigned)__cvta_generic_to_shared(ys);
+  const unsigned xbs_addr = (unsigned)__cvta_generic_to_shared(xbs);
+  for (int it = 0; it < L; ++it) {
+    pe.it_off = it;
+    de.it_off = it;
+    const cluster_bcast_epi<PE, TX> bp{pe, pe.xbar, xbs_addr, blocks};
+    for (int vb = (int)rank; vb < gp; vb += (int)blocks)
+      sell_map_block<TX, TX, cluster_bcast_epi<PE, TX>, false, kClusterWarps>(AT, ys, bp, nullptr,
+                                                                             vb);
+    cluster_barrier();
+    const cluster_bcast_epi<DE, TX> bd{de, de.yout, ys_addr, blocks};
+    for (int vb = (int)rank; vb < gd; vb += (int)blocks)
+      sell_map_block<TX, TX, cluster_bcast_epi<DE, TX>, false, kClusterWarps>(A, xbs, bd, nullptr,
+                                                                             vb);
+    cluster_barrier();
+  }
+  if (rank == 0 && threadIdx.x == 0) st->t0 += L;
+}
+
 // The barrier alone, for measuring its cost and for checking that a wait which cannot complete
 // (`unreachable` > 0 asks for more arrivals than the grid has blocks) ends with a status instead
 // of hanging: `rounds` barriers, then block 0 records the elapsed nanoseconds.

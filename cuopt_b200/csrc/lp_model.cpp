@@ -116,7 +116,7 @@ lp_settings::lp_settings()
     {CUOPT_PDLP_TILED_SWEEPS, CUOPT_PDLP_TILED_SWEEPS_AUTO, CUOPT_PDLP_TILED_SWEEPS_ON,
      CUOPT_PDLP_TILED_SWEEPS_AUTO},
     {CUOPT_PDLP_PERSISTENT_ITERATIONS, CUOPT_PDLP_PERSISTENT_ITERATIONS_AUTO,
-     CUOPT_PDLP_PERSISTENT_ITERATIONS_ON, CUOPT_PDLP_PERSISTENT_ITERATIONS_AUTO},
+     CUOPT_PDLP_PERSISTENT_ITERATIONS_CLUSTER, CUOPT_PDLP_PERSISTENT_ITERATIONS_AUTO},
     {CUOPT_PDLP_SWEEP_WARPS_PER_BLOCK, 0, 16, 0},
   };
   bparams = {

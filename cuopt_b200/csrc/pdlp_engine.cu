@@ -86,7 +86,7 @@ std::mutex& tune_mutex()
 using form_key = std::tuple<int, int, int64_t, int, int>;
 struct form_choice {
   int form;
-  double us_graphs, us_persistent;
+  double us[3];  // graphs, persistent kernel, cluster
 };
 std::map<form_key, form_choice>& form_cache()
 {
@@ -852,24 +852,81 @@ class engine {
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_fn(), kBlock, 0));
     const int need = std::max(sell_grid(ATs_view()), sell_grid(As_view()));
     persist_grid_  = std::min(need, per_sm * sms_);
-    // The persistent kernel runs the sliced-ELL sweeps only.
-    const bool ok = coop && persist_grid_ > 0 && !tile_primal_ && !tile_dual_;
+    // The persistent and cluster kernels run the sliced-ELL sweeps only.
+    const bool sell = !tile_primal_ && !tile_dual_;
+    const bool ok   = coop && persist_grid_ > 0 && sell;
     pctl_.resize(1);
     pctl_.zero(s_);
-    form_key_     = form_key{in_.m, in_.n, L_.nnz, dev, (int)sizeof(TX)};
-    int known     = -1;
-    form_us_[0] = form_us_[1] = 0.0;
+    // The cluster form where both gathered vectors fit in one block's shared memory.
+    int optin = 0;
+    B200_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cluster_smem_ = ((size_t)((in_.m + 15) & ~15) + (size_t)in_.n) * sizeof(TX);
+    bool cl_ok    = sell && cluster_smem_ + 1024 <= (size_t)optin;
+    if (cl_ok) {
+      B200_CUDA_CHECK(cudaFuncSetAttribute(cluster_fn(),
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)cluster_smem_));
+      cudaLaunchConfig_t cfg{};
+      cudaLaunchAttribute attr[1];
+      cluster_config(cfg, attr);
+      int clusters = 0;
+      cl_ok = cudaOccupancyMaxActiveClusters(&clusters, cluster_fn(), &cfg) == cudaSuccess &&
+              clusters > 0;
+      (void)cudaGetLastError();
+    }
+    form_key_ = form_key{in_.m, in_.n, L_.nnz, dev, (int)sizeof(TX)};
+    int known = -1;
+    for (double& u : form_us_) u = 0.0;
     if (p_.persistent == -1) {
       std::lock_guard<std::mutex> lock(tune_mutex());
       auto it = form_cache().find(form_key_);
       if (it != form_cache().end()) {
-        known       = it->second.form;
-        form_us_[0] = it->second.us_graphs;
-        form_us_[1] = it->second.us_persistent;
+        known = it->second.form;
+        std::memcpy(form_us_, it->second.us, sizeof(form_us_));
       }
     }
     cycle_open_ = false;
-    form_.reset(p_.persistent, known, ok);
+    const bool avail[plain_form_tuner::kForms] = {true, ok, cl_ok};
+    form_.reset(p_.persistent, known, avail);
+  }
+
+  // ------------------------------------------------------------------ cluster plain iterations
+  static constexpr int kClusterBlocks = 8;  // blocks per cluster (the portable maximum)
+  static const void* cluster_fn()
+  {
+    return (const void*)cluster_plain_kernel<TX, persist_pe, persist_de>;
+  }
+  void cluster_config(cudaLaunchConfig_t& cfg, cudaLaunchAttribute (&attr)[1]) const
+  {
+    cfg                              = cudaLaunchConfig_t{};
+    cfg.gridDim                      = dim3(kClusterBlocks);
+    cfg.blockDim                     = dim3(kClusterThreads);
+    cfg.dynamicSmemBytes             = cluster_smem_;
+    cfg.stream                       = s_;
+    attr[0].id                       = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x         = kClusterBlocks;
+    attr[0].val.clusterDim.y         = 1;
+    attr[0].val.clusterDim.z         = 1;
+    cfg.attrs                        = attr;
+    cfg.numAttrs                     = 1;
+  }
+  // Returns true for the first launch of the engine (which may include loading the kernel).
+  bool launch_cluster(int L)
+  {
+    const auto AT = ATs_view(), A = As_view();
+    persist_pe pe{x_.data(),   cs_.data(),   ls_.data(),    us_.data(),  xa_.data(),
+                  xbar_.data(), x_.data(),   xhat_.data(),  slack_.data(), aty_.data(),
+                  scalars_.data(), 0};
+    persist_de de{y_.data(),    lcs_.data(), ucs_.data(),  ya_.data(),      ybar_.data(),
+                  y_.data(),    yhat_.data(), scalars_.data(), 0};
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    cluster_config(cfg, attr);
+    B200_CUDA_CHECK(cudaLaunchKernelEx(&cfg, cluster_plain_kernel<TX, persist_pe, persist_de>, AT,
+                                       A, pe, de, L, in_.m, sell_grid(AT, kClusterWarps),
+                                       sell_grid(A, kClusterWarps), scalars_.data()));
+    ++launches_;
+    return cluster_launches_++ == 0;
   }
 
   // Returns true for the first launch of the engine (which may include loading the kernel).
@@ -902,18 +959,20 @@ class engine {
     const bool before = form_.decided();
     form_.collect();
     if (!before && form_.decided()) {
-      form_us_[0] = form_.us_per_iteration(0);
-      form_us_[1] = form_.us_per_iteration(1);
+      for (int f = 0; f < plain_form_tuner::kForms; ++f) form_us_[f] = form_.us_per_iteration(f);
       {
         std::lock_guard<std::mutex> lock(tune_mutex());
-        form_cache()[form_key_] = form_choice{form_.chosen(), form_us_[0], form_us_[1]};
+        form_choice c{form_.chosen(), {}};
+        std::memcpy(c.us, form_us_, sizeof(form_us_));
+        form_cache()[form_key_] = c;
       }
       if (std::getenv("CUOPT_B200_TRACE"))
         std::fprintf(stderr,
                      "[cuopt_b200] plain iterations: graphs %.2f us, persistent (%d blocks) %.2f "
-                     "us per iteration -> %s\n",
+                     "us, cluster %.2f us per iteration -> %s\n",
                      form_.us_per_iteration(0), persist_grid_, form_.us_per_iteration(1),
-                     form_.chosen() ? "persistent" : "graphs");
+                     form_.us_per_iteration(2),
+                     form_.chosen() == 2 ? "cluster" : form_.chosen() ? "persistent" : "graphs");
     }
   }
 
@@ -930,7 +989,9 @@ class engine {
       cycle_open_     = true;
       form_.begin(s_);
     }
-    cycle_one_time_ |= cycle_form_ == 1 ? launch_persistent((int)R) : run_graphs(R);
+    cycle_one_time_ |= cycle_form_ == 2   ? launch_cluster((int)R)
+                       : cycle_form_ == 1 ? launch_persistent((int)R)
+                                          : run_graphs(R);
   }
   void close_cycle(long k)
   {
@@ -1090,6 +1151,7 @@ class engine {
     r.persistent_blocks   = persist_grid_;
     r.us_plain_graphs     = form_.decided() ? form_us_[0] : form_.us_per_iteration(0);
     r.us_plain_persistent = form_.decided() ? form_us_[1] : form_.us_per_iteration(1);
+    r.us_plain_cluster    = form_.decided() ? form_us_[2] : form_.us_per_iteration(2);
     r.wpb_primal          = wpb_primal_;
     r.wpb_dual            = wpb_dual_;
     std::memcpy(r.wpb_ms, wpb_ms_, sizeof(wpb_ms_));
@@ -1406,7 +1468,9 @@ class engine {
   long persist_launches_ = 0;
   plain_form_tuner form_;
   form_key form_key_{};
-  double form_us_[2] = {0, 0};  // the timings behind the choice (this solve's or the cached ones)
+  double form_us_[3] = {0, 0, 0};  // the timings behind the choice (this solve's or cached)
+  size_t cluster_smem_ = 0;         // dynamic shared memory of the cluster form
+  long cluster_launches_ = 0;
   // Warps per block of the plain sweeps and the timings they were chosen by.
   int wpb_primal_ = kWarpsPerBlock, wpb_dual_ = kWarpsPerBlock;
   double wpb_ms_[2][3] = {{0, 0, 0}, {0, 0, 0}};

@@ -60,7 +60,7 @@ struct pdlp_params {
   int precision           = 0;  // 0 FP64, 1 mixed FP32/FP64
   int refinement_passes   = 0;
   int tiled_sweeps        = -1;  // mixed precision: -1 autotuned, 0 sliced ELL only, 1 tiled
-  int persistent          = -1;  // plain iterations: -1 timed choice, 0 CUDA graphs, 1 persistent
+  int persistent          = -1;  // plain iterations: -1 timed, 0 graphs, 1 persistent, 2 cluster
   int sweep_wpb           = 0;  // plain sweeps: warps per block (0: chosen by timing 4, 8, 16)
   double refinement_tol   = 1e-8;
   bool log_to_console     = false;
@@ -108,11 +108,12 @@ struct pdlp_result {
   int restarts = 0, power_iterations = 0, refinement_passes = 0;
   bool crossover = false;  // the solution was replaced by the vertex of its active set
   double kernel_launches = 0;
-  // Form of the plain iterations: 0 CUDA graphs, 1 persistent kernel (its grid in blocks), and
+  // Form of the plain iterations: 0 CUDA graphs, 1 persistent kernel (its grid in blocks), 2
+  // cluster-resident kernel, and
   // the median microseconds per iteration of the check-to-check cycles each form ran while the
   // choice was made (0 where it was not timed).
   int plain_form = 0, persistent_blocks = 0;
-  double us_plain_graphs = 0, us_plain_persistent = 0;
+  double us_plain_graphs = 0, us_plain_persistent = 0, us_plain_cluster = 0;
   // Warps per block of the plain primal / dual sweeps and the ms per launch measured with 4, 8
   // and 16 warps per block (0 where not timed).
   int wpb_primal = 8, wpb_dual = 8;

@@ -1,15 +1,18 @@
-// Choice between the two forms of a run of plain PDHG iterations (iterations that need neither a
+// Choice between the forms of a run of plain PDHG iterations (iterations that need neither a
 // termination test, a major step nor a fixed-point error):
 //   form 0: replays of cached CUDA graphs of 2^k iterations (two sweep kernels per iteration);
 //   form 1: one cooperative launch of the persistent kernel (persistent_plain_kernel), with a grid
+//           barrier after every sweep;
+//   form 2: one launch of a thread-block cluster that keeps the gathered vectors in the shared
+//           memory of each of its blocks (cluster_plain_kernel, small LPs only), with a cluster
 //           barrier after every sweep.
-// Both forms run the same sweeps with the same arithmetic, so the iterates do not depend on the
-// choice, and the choice can be made online: with pdlp_persistent_iterations = -1 the first
-// cycles of a solve (a cycle: the iterations from one termination check to the next, with their
-// major steps and every launch boundary) alternate between the forms, each timed with CUDA events
-// on the solve's stream, and once each form has kSamples timed cycles the one with the lower median
-// time per iteration is kept.  A cycle that included one-time work (a graph captured and
-// instantiated, the first launch of the persistent kernel) is not counted.
+// All forms run the same per-row arithmetic, so the iterates do not depend on the choice, and the
+// choice can be made online: with pdlp_persistent_iterations = -1 the first cycles of a solve (a
+// cycle: the iterations from one termination check to the next, with their major steps and every
+// launch boundary) rotate through the available forms, each timed with CUDA events on the solve's
+// stream, and once each has kSamples timed cycles the one with the lowest median time per iteration
+// is kept.  A cycle that included one-time work (a graph captured and instantiated, the first
+// launch of a kernel) is not counted.
 #pragma once
 
 #include "common.cuh"
@@ -23,6 +26,7 @@ namespace cuopt_b200 {
 
 class plain_form_tuner {
  public:
+  static constexpr int kForms   = 3;
   static constexpr int kSamples = 4;
 
   plain_form_tuner() = default;
@@ -40,29 +44,32 @@ class plain_form_tuner {
     }
   }
 
-  // mode: -1 tune, 0 graphs only, 1 persistent only.  `known` >= 0 is a form chosen before for the
-  // same work (kept without timing).  `persistent_ok` is false where the persistent kernel cannot
-  // run (no cooperative launch on the device).
-  void reset(int mode, int known, bool persistent_ok)
+  // mode: -1 tune among the available forms, or the form to use (0, 1, 2; an unavailable one
+  // falls back to 0).  `known` >= 0 is a form chosen before for the same work (kept without
+  // timing).  `available[f]` tells whether form f can run on this problem and device.
+  void reset(int mode, int known, const bool (&available)[kForms])
   {
     collect_all_dropped();
-    us_[0].clear();
-    us_[1].clear();
+    for (auto& u : us_) u.clear();
+    for (int f = 0; f < kForms; ++f) avail_[f] = f == 0 || available[f];
     turn_ = 0;
-    if (!persistent_ok || mode == 0)
+    if (mode >= 0)
+      chosen_ = mode < kForms && avail_[mode] ? mode : 0;
+    else if (known >= 0 && known < kForms && avail_[known])
+      chosen_ = known;
+    else if (count_available() == 1)
       chosen_ = 0;
-    else if (mode == 1)
-      chosen_ = 1;
     else
-      chosen_ = known;  // -1 while tuning
+      chosen_ = -1;  // tuning
   }
 
   bool decided() const { return chosen_ >= 0; }
   int chosen() const { return chosen_; }
-  // The form of the next run.
+  bool available(int f) const { return f >= 0 && f < kForms && avail_[f]; }
+  // The form of the next cycle.
   int next() const { return decided() ? chosen_ : turn_; }
 
-  // Brackets one cycle of `iters` iterations in `form` with events (only while tuning).
+  // Brackets one cycle (only while tuning).
   void begin(cudaStream_t s)
   {
     if (decided()) return;
@@ -79,11 +86,11 @@ class plain_form_tuner {
     cur_.one_time = one_time;
     B200_CUDA_CHECK(cudaEventRecord(cur_.e1, s));
     pending_.push_back(cur_);
-    if (!one_time) turn_ ^= 1;
+    if (!one_time) advance_turn();
   }
 
-  // Folds the runs whose closing event has completed into the samples (in launch order; the
-  // others stay pending) and decides once both forms have enough samples.
+  // Folds the cycles whose closing event has completed into the samples (in launch order; the
+  // others stay pending) and decides once every available form has enough samples.
   void collect()
   {
     size_t done = 0;
@@ -100,11 +107,16 @@ class plain_form_tuner {
       spare_.push_back(p);
     }
     pending_.erase(pending_.begin(), pending_.begin() + done);
-    if (!decided() && (int)us_[0].size() >= kSamples && (int)us_[1].size() >= kSamples)
-      chosen_ = us_per_iteration(1) < us_per_iteration(0) ? 1 : 0;
+    if (decided()) return;
+    for (int f = 0; f < kForms; ++f)
+      if (avail_[f] && (int)us_[f].size() < kSamples) return;
+    int best = 0;
+    for (int f = 1; f < kForms; ++f)
+      if (avail_[f] && us_per_iteration(f) < us_per_iteration(best)) best = f;
+    chosen_ = best;
   }
 
-  // Median time per iteration of a form over its counted runs (0 when it was not timed).
+  // Median time per iteration of a form over its counted cycles (0 when it was not timed).
   double us_per_iteration(int form) const
   {
     std::vector<double> v = us_[form];
@@ -121,6 +133,22 @@ class plain_form_tuner {
     long iters    = 0;
     bool one_time = false;
   };
+  int count_available() const
+  {
+    int c = 0;
+    for (bool a : avail_) c += a;
+    return c;
+  }
+  void advance_turn()
+  {
+    for (int k = 1; k <= kForms; ++k) {
+      const int f = (turn_ + k) % kForms;
+      if (avail_[f]) {
+        turn_ = f;
+        return;
+      }
+    }
+  }
   run take()
   {
     if (!spare_.empty()) {
@@ -141,9 +169,10 @@ class plain_form_tuner {
 
   std::vector<run> pending_, spare_;
   run cur_;
-  std::vector<double> us_[2];  // microseconds per iteration of each counted run, per form
-  int turn_ = 0;
-  int chosen_     = 0;  // graphs until reset() is called
+  std::vector<double> us_[kForms];  // microseconds per iteration of each counted cycle, per form
+  bool avail_[kForms] = {true, false, false};
+  int turn_           = 0;
+  int chosen_         = 0;  // graphs until reset() is called
 };
 
 }  // namespace cuopt_b200

@@ -97,13 +97,17 @@
 #define CUOPT_PDLP_TILED_SWEEPS_OFF  0
 #define CUOPT_PDLP_TILED_SWEEPS_ON   1
 /* pdlp_persistent_iterations: the runs of plain iterations between termination checks are
- * replayed from CUDA graphs (0) or run by one persistent cooperative kernel launch with a grid
- * barrier after every sweep (1); -1 times both forms on the first runs of a solve (the iterates
- * are the same either way) and keeps the faster one, remembered per problem shape. */
-#define CUOPT_PDLP_PERSISTENT_ITERATIONS      "pdlp_persistent_iterations"
-#define CUOPT_PDLP_PERSISTENT_ITERATIONS_AUTO -1
-#define CUOPT_PDLP_PERSISTENT_ITERATIONS_OFF  0
-#define CUOPT_PDLP_PERSISTENT_ITERATIONS_ON   1
+ * replayed from CUDA graphs (0), run by one persistent cooperative kernel launch with a grid
+ * barrier after every sweep (1), or, for LPs whose two gathered vectors fit in one block's shared
+ * memory, by one thread-block cluster that keeps them there (2; single LPs, not batches); -1
+ * times the available forms on the first check-to-check cycles of a solve (the iterates are the
+ * same either way) and keeps the fastest, remembered per problem shape.  A form that cannot run
+ * on the problem falls back to 0. */
+#define CUOPT_PDLP_PERSISTENT_ITERATIONS         "pdlp_persistent_iterations"
+#define CUOPT_PDLP_PERSISTENT_ITERATIONS_AUTO    -1
+#define CUOPT_PDLP_PERSISTENT_ITERATIONS_OFF     0
+#define CUOPT_PDLP_PERSISTENT_ITERATIONS_ON      1
+#define CUOPT_PDLP_PERSISTENT_ITERATIONS_CLUSTER 2
 /* pdlp_sweep_warps_per_block: block shape of the plain sliced-ELL sweeps.  0 (default) chooses
  * 4, 8 or 16 warps per block by timing each sweep at the first solve of a problem shape; 4, 8 or
  * 16 fixes it (other values are a validation error).  The shape does not change any row's

@@ -40,15 +40,17 @@ typedef struct {
   cuopt_float_t loop_time;      /* seconds spent in the iteration loop */
   cuopt_float_t kernel_launches; /* kernels this library launched for the solve */
   cuopt_int_t crossover;         /* 1: the solution is the vertex of its active set ("crossover") */
-  /* Form of the plain iterations between termination checks: 0 CUDA-graph replays, 1 one
-   * persistent cooperative launch per run (pdlp_persistent_iterations), -1 still undecided when the
+  /* Form of the plain iterations between termination checks (pdlp_persistent_iterations): 0
+   * CUDA-graph replays, 1 one persistent cooperative launch per run, 2 one thread-block cluster
+   * per run with the gathered vectors in shared memory (small LPs), -1 still undecided when the
    * solve ended; the persistent grid in blocks; and the median microseconds per iteration of the
-   * check-to-check cycles (major steps and launch boundaries included) that each form ran while the
-   * choice was made (0 where it was not timed). */
+   * check-to-check cycles (major steps and launch boundaries included) that each form ran while
+   * the choice was made (0 where it was not timed). */
   cuopt_int_t plain_iteration_form;
   cuopt_int_t persistent_blocks;
   cuopt_float_t plain_iteration_us_graphs;
   cuopt_float_t plain_iteration_us_persistent;
+  cuopt_float_t plain_iteration_us_cluster;
   /* Warps per block of the plain primal and dual sweeps (pdlp_sweep_warps_per_block), and the
    * milliseconds per launch each shape took when they were chosen: primal with 4, 8, 16 warps,
    * then dual with 4, 8, 16 (0 where not timed). */

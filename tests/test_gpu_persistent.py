@@ -1,9 +1,9 @@
-"""GPU tests of the persistent form of the plain PDHG iterations (pdlp_persistent_iterations).
+"""GPU tests of the forms of the plain PDHG iterations (pdlp_persistent_iterations): CUDA-graph
+replays, the persistent cooperative kernel and the cluster-resident kernel (small LPs).
 
-The persistent kernel runs the same sweeps with the same arithmetic as the CUDA-graph replays, so
-the expectation is exact: solves with the persistent form forced on, forced off and chosen by
-timing return bit-identical iterates, iteration counts and statuses, for single LPs (FP64 and
-mixed precision) and for block-diagonal batches.  The grid barrier between the sweeps is the only
+Every form computes each row exactly as the graph-replayed sweeps do, so the expectation is exact:
+solves with each form forced and chosen by timing return bit-identical iterates, iteration counts
+and statuses, for single LPs (FP64 and mixed precision) and for block-diagonal batches.  The grid barrier between the sweeps is the only
 wait in the kernel; its bounded wait is checked on its own (cuOptProbeGridBarrier): a barrier that
 nothing can complete must end at its deadline with status 1, and the context must stay usable.
 """
@@ -21,7 +21,7 @@ from tests.helpers import datamodel_from_lp, settings
 
 pytestmark = pytest.mark.gpu
 
-GRAPHS, PERSISTENT, AUTO = 0, 1, -1
+GRAPHS, PERSISTENT, CLUSTER, AUTO = 0, 1, 2, -1
 
 
 def _settings(form, **kw):
@@ -49,18 +49,21 @@ def test_persistent_matches_graphs(lp_c0, precision):
     dm = datamodel_from_lp(lp_c0)
     g = lpm.Solve(dm, _settings(GRAPHS, tol=1e-6, precision=precision))
     p = lpm.Solve(dm, _settings(PERSISTENT, tol=1e-6, precision=precision))
+    c = lpm.Solve(dm, _settings(CLUSTER, tol=1e-6, precision=precision))
     a = lpm.Solve(dm, _settings(AUTO, tol=1e-6, precision=precision))
     assert g.get_termination_status() == lpm.LPTerminationStatus.Optimal
     _same(g, p)
+    _same(g, c)
     _same(g, a)
     assert g.stats["plain_iteration_form"] == GRAPHS
     assert p.stats["plain_iteration_form"] == PERSISTENT
+    assert c.stats["plain_iteration_form"] == CLUSTER
     assert p.stats["persistent_blocks"] > 0
-    # The timed choice: both forms timed, the faster one kept.
-    assert a.stats["plain_iteration_form"] in (GRAPHS, PERSISTENT)
-    us_g, us_p = a.stats["plain_iteration_us_graphs"], a.stats["plain_iteration_us_persistent"]
-    assert us_g > 0 and us_p > 0
-    assert a.stats["plain_iteration_form"] == (PERSISTENT if us_p < us_g else GRAPHS)
+    # The timed choice: every form timed, the fastest kept.
+    us = [a.stats["plain_iteration_us_graphs"], a.stats["plain_iteration_us_persistent"],
+          a.stats["plain_iteration_us_cluster"]]
+    assert all(u > 0 for u in us)
+    assert a.stats["plain_iteration_form"] == int(np.argmin(us))
 
 
 def test_persistent_matches_graphs_at_iteration_limits(lp_c0):
@@ -69,8 +72,10 @@ def test_persistent_matches_graphs_at_iteration_limits(lp_c0):
     for k in (7, 33, 250):
         g = lpm.Solve(dm, _settings(GRAPHS, tol=1e-12, iteration_limit=k))
         p = lpm.Solve(dm, _settings(PERSISTENT, tol=1e-12, iteration_limit=k))
+        c = lpm.Solve(dm, _settings(CLUSTER, tol=1e-12, iteration_limit=k))
         assert g.get_termination_status() == lpm.LPTerminationStatus.IterationLimit
         _same(g, p)
+        _same(g, c)
 
 
 @pytest.mark.parametrize("precision", [0, 1])
@@ -119,7 +124,18 @@ def test_persistent_long_rows():
     dm = datamodel_from_lp(lp)
     g = lpm.Solve(dm, _settings(GRAPHS, tol=1e-6))
     p = lpm.Solve(dm, _settings(PERSISTENT, tol=1e-6))
+    c = lpm.Solve(dm, _settings(CLUSTER, tol=1e-6))
     _same(g, p)
+    _same(g, c)
+    assert c.stats["plain_iteration_form"] == CLUSTER
+
+
+def test_cluster_form_falls_back_on_large_lps():
+    """The cluster form needs both gathered vectors in one block's shared memory: for
+    20 000 + 50 000 FP64 entries (560 KB) a solve that asks for it runs the graphs."""
+    lp = gen.constructed_lp(20000, 50000, 8, seed=5)
+    s = lpm.Solve(datamodel_from_lp(lp), _settings(CLUSTER, tol=1e-4, iteration_limit=50))
+    assert s.stats["plain_iteration_form"] == GRAPHS
 
 
 @pytest.mark.parametrize("precision", [0, 1])
