@@ -208,14 +208,16 @@ def solve_device(L, dlp, settings, stream_ptr):
 
 def form_info(st):
     """The tuned choices of a solve: the form of the plain iterations and the cycle timings it was
-    chosen on (pdlp_persistent_iterations = -1: CUDA graphs against the persistent cooperative
-    kernel), and the plain sweeps' warps per block with the ms per launch of 4, 8 and 16
-    (pdlp_sweep_warps_per_block = 0)."""
+    chosen on (pdlp_persistent_iterations = -1: CUDA graphs, the persistent cooperative kernel and,
+    for small LPs, the cluster-resident kernel), and the plain sweeps' warps per block with the ms
+    per launch of 4, 8 and 16 (pdlp_sweep_warps_per_block = 0)."""
     ms = list(st["sweep_block_shape_ms"])
-    return {"form": {0: "graphs", 1: "persistent"}.get(st["plain_iteration_form"], "undecided"),
+    return {"form": {0: "graphs", 1: "persistent", 2: "cluster"}.get(st["plain_iteration_form"],
+                                                                       "undecided"),
             "persistent_blocks": st["persistent_blocks"],
             "us_per_iteration_graphs": st["plain_iteration_us_graphs"],
             "us_per_iteration_persistent": st["plain_iteration_us_persistent"],
+            "us_per_iteration_cluster": st["plain_iteration_us_cluster"],
             "sweep_warps_per_block": {"primal": st["sweep_warps_per_block_primal"],
                                       "dual": st["sweep_warps_per_block_dual"]},
             "sweep_ms_by_warps_per_block": {"primal": dict(zip(("4", "8", "16"), ms[:3])),

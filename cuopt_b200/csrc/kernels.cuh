@@ -227,7 +227,7 @@ __device__ __forceinline__ void sell_map_block(const dev_sell<TM>& A, const TG* 
     block_reduce_store<K, has_max_red<Epi>::value>(red, partials, vb);
     return;
   }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, warp = (threadIdx.x >> 5) & (WPB - 1);
   const int lb   = long_blocks(A.long_count(), WPB);
   if (vb < lb) {
     const int q   = vb * WPB + warp;
@@ -458,110 +458,6 @@ __global__ void __launch_bounds__(kBlock)
   if (blockIdx.x == 0) adv(L);
 }
 
-// ---------------------------------------------------------------------------------------------
-// Cluster-resident plain iterations for small LPs: one thread-block cluster of C blocks runs a run
-// of L plain iterations.  Every block keeps a full copy of both gathered vectors (y for the primal
-// sweep, x_bar for the dual sweep) in its shared memory, so the sweeps gather from shared memory;
-// a row's new value is written to global memory by its epilogue, as in the other forms, and
-// stored into every block's copy through distributed shared memory (mapa + st.shared::cluster).
-// A cluster barrier (arrive.release / wait.acquire: hardware, no spin loop) follows every sweep.
-// The block's virtual blocks of the sweep are rank, rank + C, ... with 32 warps each; every row is
-// computed by one warp exactly as in sell_map_kernel.
-constexpr int kClusterThreads = 1024;
-constexpr int kClusterWarps   = kClusterThreads / kWarp;
-
-__device__ __forceinline__ unsigned cluster_rank()
-{
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ unsigned cluster_size()
-{
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ void cluster_barrier()
-{
-  asm volatile(
-    "barrier.cluster.arrive.release.aligned;\n"
-    "barrier.cluster.wait.acquire.aligned;\n" ::
-      : "memory");
-}
-// Stores v at shared-memory address saddr (a byte offset in this block's window) of block `rank`
-// of the cluster.
-__device__ __forceinline__ void dsmem_store(unsigned saddr, unsigned rank, double v)
-{
-  unsigned remote;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(saddr), "r"(rank));
-  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(remote), "d"(v) : "memory");
-}
-__device__ __forceinline__ void dsmem_store(unsigned saddr, unsigned rank, float v)
-{
-  unsigned remote;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(saddr), "r"(rank));
-  asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(remote), "f"(v) : "memory");
-}
-
-// Wraps a plain epilogue: after the row's step, the value the step stored into the gathered
-// vector (read back by the same thread) goes to every block's copy of that vector.
-template <class Base, typename TX>
-struct cluster_bcast_epi {
-  static constexpr int kRed = 0;
-  using pre_t               = typename Base::pre_t;
-  Base base;
-  const TX* written;  // the global vector the step stores into (x_bar or y)
-  unsigned copy;      // shared-memory address of this block's copy of that vector
-  unsigned blocks;    // cluster size
-  __device__ bool skip() const { return base.skip(); }
-  __device__ __forceinline__ pre_t load(int r) const { return base.load(r); }
-  __device__ __forceinline__ void operator()(int r, double acc, const pre_t& p, red_t<0>& red) const
-  {
-    base(r, acc, p, red);
-    const TX v            = written[r];
-    const unsigned target = copy + (unsigned)(r * (int)sizeof(TX));
-    for (unsigned c = 0; c < blocks; ++c) dsmem_store(target, c, v);
-  }
-};
-
-// Dynamic shared memory: the copy of y (m elements), then the copy of x_bar (n elements), the first
-// padded to 16 elements.  pe / de: the plain primal / dual epilogues (it_off set per iteration),
-// whose gathered vectors are y (de.y = de.yout) and x_bar (pe.xbar); gp / gd: the sweeps' virtual
-// block counts with kClusterWarps warps per block.
-template <typename TX, class PE, class DE>
-__global__ void __launch_bounds__(kClusterThreads)
-  cluster_plain_kernel(const dev_sell<TX> AT, const dev_sell<TX> A, PE pe, DE de, int L, int m,
-                       int gp, int gd, pdlp_scalars* st)
-{
-  extern __shared__ __align__(16) unsigned char cl_smem[];
-  TX* ys          = reinterpret_cast<TX*>(cl_smem);
-  const int m_pad = (m + 15) & ~15;
-  TX* xbs         = ys + m_pad;
-  const unsigned rank = cluster_rank(), blocks = cluster_size();
-  for (int i = threadIdx.x; i < m; i += blockDim.x) ys[i] = de.y[i];
-  // Every block of the cluster is running (and has its copy of y) before any block stores into
-  // another's shared memory.
-  cluster_barrier();
-  const unsigned ys_addr  = (unsigned)__cvta_generic_to_shared(ys);
-  const unsigned xbs_addr = (unsigned)__cvta_generic_to_shared(xbs);
-  for (int it = 0; it < L; ++it) {
-    pe.it_off = it;
-    de.it_off = it;
-    const cluster_bcast_epi<PE, TX> bp{pe, pe.xbar, xbs_addr, blocks};
-    for (int vb = (int)rank; vb < gp; vb += (int)blocks)
-      sell_map_block<TX, TX, cluster_bcast_epi<PE, TX>, false, kClusterWarps>(AT, ys, bp, nullptr,
-                                                                             vb);
-    cluster_barrier();
-    const cluster_bcast_epi<DE, TX> bd{de, de.yout, ys_addr, blocks};
-    for (int vb = (int)rank; vb < gd; vb += (int)blocks)
-      sell_map_block<TX, TX, cluster_bcast_epi<DE, TX>, false, kClusterWarps>(A, xbs, bd, nullptr,
-                                                                             vb);
-    cluster_barrier();
-  }
-  if (rank == 0 && threadIdx.x == 0) st->t0 += L;
-}
-
 // The barrier alone, for measuring its cost and for checking that a wait which cannot complete
 // (`unreachable` > 0 asks for more arrivals than the grid has blocks) ends with a status instead
 // of hanging: `rounds` barriers, then block 0 records the elapsed nanoseconds.
@@ -583,10 +479,18 @@ static __global__ void persist_barrier_probe_kernel(persist_ctl* ctl, int rounds
 
 // The primal update of one variable j (shared by the single-LP and batch epilogues); `p` holds
 // x_j, c_j, l_j, u_j and the anchor x_a,j, `st` the step scalars of j's LP.
-template <typename TX, bool MAJOR, bool HALPERN, bool SAVE_ATY, class P>
+// Receives the value a row step stores into the vector the next sweep gathers (x_bar for the
+// primal step, y for the fused-Halpern dual step); the cluster-resident form copies it into the
+// cluster's shared-memory copies.
+struct no_sink {
+  __device__ __forceinline__ void operator()(int, double) const {}
+};
+
+template <typename TX, bool MAJOR, bool HALPERN, bool SAVE_ATY, class P, class Sink = no_sink>
 __device__ __forceinline__ void primal_row_step(int j, double acc, const P& p,
                                                 const pdlp_scalars* st, int it_off, TX* xbar,
-                                                TX* xout, TX* xhat, TX* slack, TX* aty)
+                                                TX* xout, TX* xhat, TX* slack, TX* aty,
+                                                const Sink& sink = Sink{})
 {
   const double tau  = st->tau;
   const double xj   = (double)p.x;
@@ -605,13 +509,14 @@ __device__ __forceinline__ void primal_row_step(int j, double acc, const P& p,
   } else {
     xbar[j] = (TX)xb;
   }
+  sink(j, (double)(TX)xb);
 }
 
 // The dual update of one constraint i; returns (y_bar_i - y_i)^2 for the fixed-point error.
-template <typename TX, bool MAJOR, bool HALPERN, class P>
+template <typename TX, bool MAJOR, bool HALPERN, class P, class Sink = no_sink>
 __device__ __forceinline__ double dual_row_step(int i, double acc, const P& p,
                                                 const pdlp_scalars* st, int it_off, TX* ybar,
-                                                TX* yout, TX* yhat)
+                                                TX* yout, TX* yhat, const Sink& sink = Sink{})
 {
   const double sigma = st->sigma;
   const double yi    = (double)p.y;
@@ -621,8 +526,10 @@ __device__ __forceinline__ double dual_row_step(int i, double acc, const P& p,
   if constexpr (MAJOR) yhat[i] = (TX)ny;
   const double yb = 2.0 * ny - yi;
   if constexpr (HALPERN) {
-    const double w = halpern_weight(st, it_off);
-    yout[i]        = (TX)(w * yb + (1.0 - w) * (double)p.ya);
+    const double w  = halpern_weight(st, it_off);
+    const TX y_next = (TX)(w * yb + (1.0 - w) * (double)p.ya);
+    yout[i]         = y_next;
+    sink(i, (double)y_next);
   } else {
     ybar[i] = (TX)yb;
   }
@@ -692,6 +599,139 @@ struct dual_epi {
     if constexpr (FPE) r.v[0] += d2;
   }
 };
+
+// ---------------------------------------------------------------------------------------------
+// Cluster-resident plain iterations for small LPs: one thread-block cluster of C blocks runs a run
+// of L plain iterations.  Every block keeps a full copy of both gathered vectors (y for the primal
+// sweep, x_bar for the dual sweep) in its shared memory, so the sweeps gather from shared memory;
+// a row's new value is written to global memory by its epilogue, as in the other forms, and
+// stored into every block's copy through distributed shared memory (mapa + st.shared::cluster).
+// A cluster barrier (arrive.release / wait.acquire: hardware, no spin loop) follows every sweep.
+// Every row is computed by one warp exactly as in sell_map_kernel.
+constexpr int kClusterThreads = 1024;
+constexpr int kClusterGroups  = kClusterThreads / kBlock;  // 8-warp groups per block
+
+__device__ __forceinline__ unsigned cluster_rank()
+{
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned cluster_size()
+{
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_barrier()
+{
+  asm volatile(
+    "barrier.cluster.arrive.release.aligned;\n"
+    "barrier.cluster.wait.acquire.aligned;\n" ::
+      : "memory");
+}
+// Stores v at shared-memory address saddr (a byte offset in this block's window) of block `rank`
+// of the cluster.
+__device__ __forceinline__ void dsmem_store(unsigned saddr, unsigned rank, double v)
+{
+  unsigned remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(saddr), "r"(rank));
+  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(remote), "d"(v) : "memory");
+}
+__device__ __forceinline__ void dsmem_store(unsigned saddr, unsigned rank, float v)
+{
+  unsigned remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(saddr), "r"(rank));
+  asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(remote), "f"(v) : "memory");
+}
+
+// Copies a row's new value into every block's shared-memory copy of its vector (base: the
+// shared-memory address of the copy in this block's window).
+template <typename TX>
+struct dsmem_sink {
+  unsigned base;
+  unsigned blocks;
+  __device__ __forceinline__ void operator()(int r, double v) const
+  {
+    const unsigned target = base + (unsigned)r * (unsigned)sizeof(TX);
+    for (unsigned c = 0; c < blocks; ++c) dsmem_store(target, c, (TX)v);
+  }
+};
+
+// The plain epilogues (primal_epi / dual_epi with the Halpern step fused) with the new x_bar_j,
+// or y_i, also sent to the cluster's copies.
+template <typename TX>
+struct cluster_primal_epi {
+  static constexpr int kRed = 0;
+  using base_t              = primal_epi<TX, false, true, false>;
+  using pre_t               = typename base_t::pre_t;
+  base_t base;
+  dsmem_sink<TX> sink;
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ pre_t load(int j) const { return base.load(j); }
+  __device__ __forceinline__ void operator()(int j, double acc, const pre_t& p, red_t<0>&) const
+  {
+    primal_row_step<TX, false, true, false>(j, acc, p, base.st, base.it_off, base.xbar, base.xout,
+                                            base.xhat, base.slack, base.aty, sink);
+  }
+};
+template <typename TX>
+struct cluster_dual_epi {
+  static constexpr int kRed = 0;
+  using base_t              = dual_epi<TX, false, true, false>;
+  using pre_t               = typename base_t::pre_t;
+  base_t base;
+  dsmem_sink<TX> sink;
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ pre_t load(int i) const { return base.load(i); }
+  __device__ __forceinline__ void operator()(int i, double acc, const pre_t& p, red_t<0>&) const
+  {
+    dual_row_step<TX, false, true>(i, acc, p, base.st, base.it_off, base.ybar, base.yout,
+                                   base.yhat, sink);
+  }
+};
+
+// Dynamic shared memory: the copy of y (m elements, padded to 16), then the copy of x_bar (n
+// elements).  pe / de: the plain primal / dual epilogues (it_off set per iteration), whose gathered
+// vectors are y (de.y = de.yout) and x_bar (pe.xbar).  Each block runs kClusterGroups groups of
+// kWarpsPerBlock warps; group g of block `rank` takes the sweep's 8-warp virtual blocks
+// rank + C g, rank + C g + C kClusterGroups, ... (gp / gd of them), so small sweeps spread over
+// every block of the cluster.
+template <typename TX>
+__global__ void __launch_bounds__(kClusterThreads)
+  cluster_plain_kernel(const dev_sell<TX> AT, const dev_sell<TX> A,
+                       primal_epi<TX, false, true, false> pe, dual_epi<TX, false, true, false> de,
+                       int L, int m, int gp, int gd, pdlp_scalars* st)
+{
+  extern __shared__ __align__(16) unsigned char cl_smem[];
+  TX* ys          = reinterpret_cast<TX*>(cl_smem);
+  const int m_pad = (m + 15) & ~15;
+  TX* xbs         = ys + m_pad;
+  const unsigned rank = cluster_rank(), blocks = cluster_size();
+  for (int i = threadIdx.x; i < m; i += blockDim.x) ys[i] = de.y[i];
+  // Every block of the cluster is running (and has its copy of y) before any block stores into
+  // another's shared memory.
+  cluster_barrier();
+  const dsmem_sink<TX> to_xbs{(unsigned)__cvta_generic_to_shared(xbs), blocks};
+  const dsmem_sink<TX> to_ys{(unsigned)__cvta_generic_to_shared(ys), blocks};
+  const int group  = threadIdx.x / (kWarpsPerBlock * kWarp);
+  const int first  = (int)rank + (int)blocks * group;
+  const int stride = (int)blocks * kClusterGroups;
+  for (int it = 0; it < L; ++it) {
+    pe.it_off = it;
+    de.it_off = it;
+    const cluster_primal_epi<TX> bp{pe, to_xbs};
+    for (int vb = first; vb < gp; vb += stride)
+      sell_map_block<TX, TX, cluster_primal_epi<TX>>(AT, ys, bp, nullptr, vb);
+    cluster_barrier();
+    const cluster_dual_epi<TX> bd{de, to_ys};
+    for (int vb = first; vb < gd; vb += stride)
+      sell_map_block<TX, TX, cluster_dual_epi<TX>>(A, xbs, bd, nullptr, vb);
+    cluster_barrier();
+  }
+  if (rank == 0 && threadIdx.x == 0) st->t0 += L;
+}
+
 
 // Row j of A^T applied to y_bar: interaction (A^T y_bar - A^T y) . (x_bar - x) and |x_bar - x|^2
 // (reference adaptive_step_size_strategy.cu:352-518).

@@ -894,7 +894,7 @@ class engine {
   static constexpr int kClusterBlocks = 8;  // blocks per cluster (the portable maximum)
   static const void* cluster_fn()
   {
-    return (const void*)cluster_plain_kernel<TX, persist_pe, persist_de>;
+    return (const void*)cluster_plain_kernel<TX>;
   }
   void cluster_config(cudaLaunchConfig_t& cfg, cudaLaunchAttribute (&attr)[1]) const
   {
@@ -922,9 +922,8 @@ class engine {
     cudaLaunchConfig_t cfg{};
     cudaLaunchAttribute attr[1];
     cluster_config(cfg, attr);
-    B200_CUDA_CHECK(cudaLaunchKernelEx(&cfg, cluster_plain_kernel<TX, persist_pe, persist_de>, AT,
-                                       A, pe, de, L, in_.m, sell_grid(AT, kClusterWarps),
-                                       sell_grid(A, kClusterWarps), scalars_.data()));
+    B200_CUDA_CHECK(cudaLaunchKernelEx(&cfg, cluster_plain_kernel<TX>, AT, A, pe, de, L, in_.m,
+                                       sell_grid(AT), sell_grid(A), scalars_.data()));
     ++launches_;
     return cluster_launches_++ == 0;
   }

@@ -80,8 +80,9 @@ def main() -> None:
     ap.add_argument("--refine", type=int, default=0, help="> 0: continue a mixed-precision solve in FP64 to 1e-8")
     ap.add_argument("--tiled", type=int, default=-1, choices=[-1, 0, 1],
                     help="pdlp_tiled_sweeps: -1 autotuned, 0 sliced ELL only, 1 tiled where possible")
-    ap.add_argument("--persistent", type=int, default=-1, choices=[-1, 0, 1],
-                    help="pdlp_persistent_iterations: -1 timed choice, 0 CUDA graphs, 1 persistent")
+    ap.add_argument("--persistent", type=int, default=-1, choices=[-1, 0, 1, 2],
+                    help="pdlp_persistent_iterations: -1 timed choice, 0 CUDA graphs, 1 persistent "
+                         "kernel, 2 cluster-resident kernel")
     ap.add_argument("--solves", type=int, default=1,
                     help="solve mode: solves of the same LP (the statistics are the last one's)")
     a = ap.parse_args()
