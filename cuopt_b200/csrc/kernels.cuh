@@ -1019,6 +1019,149 @@ static __global__ void __launch_bounds__(kBlock)
   }
 }
 
+// The power iteration of a small LP in one thread-block cluster of C blocks of kBlock threads, all
+// steps up to convergence (or max_iters) in one launch.  Every block keeps full copies of z, q and
+// A^T q in its shared memory: the vector steps (normalisation, residual, and their sums) run on
+// the local copies in every block at once, the two sweeps are split over the blocks (virtual
+// blocks rank, rank + C, ...) and send each new entry of A^T q and z, and each q . z block
+// partial, to every block's copy through distributed shared memory, so a step needs two cluster
+// barriers.  Every sum is formed exactly as in the multi-kernel form: the vector steps emulate
+// its pg blocks of kBlock threads (grid stride pg * kBlock, one block reduction each), the sweeps
+// are its virtual blocks, and every scalar is ordered_block_sum of the same block partials, so
+// both forms give the same step size bit for bit.
+template <typename TX>
+struct cluster_atq_epi {  // (A^T q)_j to every block's copy
+  static constexpr int kRed = 0;
+  dsmem_sink<double> sink;
+  struct pre_t {};
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ pre_t load(int) const { return pre_t{}; }
+  __device__ __forceinline__ void operator()(int j, double acc, const pre_t&, red_t<0>&) const
+  {
+    sink(j, acc);
+  }
+};
+struct cluster_z_epi {  // z_i = (A atq)_i to every block's copy; q . z block partial
+  static constexpr int kRed = 1;
+  dsmem_sink<double> sink;
+  const double* q;  // this block's copy of q
+  struct pre_t {
+    double q;
+  };
+  __device__ bool skip() const { return false; }
+  __device__ __forceinline__ pre_t load(int i) const { return pre_t{q[i]}; }
+  __device__ __forceinline__ void operator()(int i, double acc, const pre_t& p, red_t<1>& r) const
+  {
+    sink(i, acc);
+    r.v[0] += p.q * acc;
+  }
+};
+
+// Largest m (constraints) the cluster power iteration takes: its vector steps run pg = m / kBlock
+// emulated block reductions in every block.
+constexpr int kClusterPowerMaxRows = 8192;
+
+// Dynamic shared memory (doubles): z (m_pad), q (m_pad), A^T q (n_pad), the q . z partials of the
+// sweep's ga virtual blocks (ga_pad, a copy in every block), their local staging (ga_pad), and
+// the |z|^2 and residual partials of the pg emulated blocks (pg_pad each, local).
+inline size_t cluster_power_smem(int m, int n, int pg, int ga)
+{
+  auto pad = [](int v) { return (size_t)((v + 15) & ~15); };
+  return (2 * pad(m) + pad(n) + 2 * pad(ga) + 2 * pad(pg)) * sizeof(double);
+}
+
+template <typename TX>
+__global__ void __launch_bounds__(kBlock)
+  cluster_power_kernel(const dev_sell<TX> AT, const dev_sell<TX> A, const double* z0, int m, int n,
+                       int pg, int gt, int ga, power_state* ps, double tol, int max_iters)
+{
+  extern __shared__ __align__(16) unsigned char cp_smem[];
+  auto pad     = [](int v) { return (v + 15) & ~15; };
+  double* zc   = reinterpret_cast<double*>(cp_smem);
+  double* qc   = zc + pad(m);
+  double* atqc = qc + pad(m);
+  double* sc   = atqc + pad(n);  // q . z partials (every block's copy)
+  double* st   = sc + pad(ga);   // this block's partials before they are sent
+  double* pz   = st + pad(ga);   // |z|^2 partials
+  double* pr   = pz + pad(pg);   // residual partials
+  __shared__ double scalar;
+  const unsigned rank = cluster_rank(), C = cluster_size();
+  const dsmem_sink<double> to_z{(unsigned)__cvta_generic_to_shared(zc), C};
+  const dsmem_sink<double> to_atq{(unsigned)__cvta_generic_to_shared(atqc), C};
+  const unsigned sc_addr = (unsigned)__cvta_generic_to_shared(sc);
+
+  for (int i = threadIdx.x; i < m; i += kBlock) zc[i] = z0[i];
+  __syncthreads();
+  // |z|^2 partials of the pg emulated blocks (vec_reduce_kernel<0>).
+  auto sumsq = [&]() {
+    for (int b = 0; b < pg; ++b) {
+      red_t<1> r;
+      r.v[0] = 0.0;
+      for (int i = b * kBlock + threadIdx.x; i < m; i += pg * kBlock) {
+        const double v = zc[i];
+        r.v[0] += v * v;
+      }
+      block_reduce_store<1>(r, pz, b);
+    }
+    __syncthreads();
+  };
+  sumsq();
+  // Every block of the cluster is running before any block stores into another's memory.
+  cluster_barrier();
+  int it = 0, done = 0;
+  double nq = 0.0, s2 = 0.0, resid = 0.0;
+  while (it < max_iters && !done) {
+    // q = z / |z|  (power_normalize_sum_kernel), on the local copies.
+    ordered_block_sum<1>(pz, pg, &scalar);
+    nq = sqrt(scalar);
+    for (int i = threadIdx.x; i < m; i += kBlock) qc[i] = zc[i] / nq;
+    __syncthreads();
+    // A^T q over this block's virtual blocks, entries sent to every copy.
+    for (int vb = (int)rank; vb < gt; vb += (int)C)
+      sell_map_block<TX, double, cluster_atq_epi<TX>>(AT, qc, cluster_atq_epi<TX>{to_atq},
+                                                      nullptr, vb);
+    cluster_barrier();
+    // z = A (A^T q) with the q . z partial of each virtual block, both sent to every copy.
+    for (int vb = (int)rank; vb < ga; vb += (int)C) {
+      sell_map_block<TX, double, cluster_z_epi>(A, atqc, cluster_z_epi{to_z, qc}, st, vb);
+      if (threadIdx.x == 0)
+        for (unsigned c = 0; c < C; ++c)
+          dsmem_store(sc_addr + (unsigned)vb * (unsigned)sizeof(double), c, st[vb]);
+    }
+    cluster_barrier();
+    // q <- q (-s2) + z with its squares' partials (power_residual_sum_kernel), the next |z|^2
+    // partials, and the test of power_check_sum_kernel, all on the local copies.
+    ordered_block_sum<1>(sc, ga, &scalar);
+    s2 = scalar;
+    for (int b = 0; b < pg; ++b) {
+      red_t<1> r;
+      r.v[0] = 0.0;
+      for (int i = b * kBlock + threadIdx.x; i < m; i += pg * kBlock) {
+        const double v = qc[i] * -s2 + zc[i];
+        qc[i]          = v;
+        r.v[0] += v * v;
+      }
+      block_reduce_store<1>(r, pr, b);
+    }
+    __syncthreads();
+    sumsq();
+    ordered_block_sum<1>(pr, pg, &scalar);
+    resid = sqrt(scalar);
+    ++it;
+    done = resid < tol;
+  }
+  if (rank == 0 && threadIdx.x == 0) {
+    ps->norm_z = nq;
+    ps->s2     = s2;
+    ps->resid  = resid;
+    ps->iters  = it;
+    ps->done   = done;
+  }
+  // No block leaves while another may still store into its shared memory.
+  cluster_barrier();
+}
+
+
 // Golub-Kahan-Lanczos bidiagonalisation of the scaled A (the mixed-precision step size).  The
 // vectors are stored unnormalised; gk_state holds their norms: u has norm beta (beta_k), v has
 // norm alpha (alpha_{k-1}, or 0 before the first step).

@@ -449,6 +449,7 @@ class engine {
     // The vector steps run on a grid sized to the m entries (at most vgrid_ blocks): small LPs
     // launch a few blocks instead of vgrid_ mostly idle ones.
     const int pg = std::max(1, std::min(vgrid_, ceil_div(m, kBlock)));
+    if (cluster_power(As, ATs, dz.data(), ps.data(), pg, ga, gt)) return;
     auto one_iteration = [&]() {
       vec_reduce_kernel<0, double><<<pg, kBlock, 0, s_>>>(dz.data(), nullptr, m, part,
                                                           &ps.data()->done);
@@ -485,6 +486,68 @@ class engine {
     cudaGraphExecDestroy(exec);
     power_iters_ = h.iters;
     eta_         = kStepScaling / std::sqrt(h.s2);
+  }
+
+  // Small LPs (at most kClusterPowerNnz non-zeros and kClusterPowerMaxRows rows, z, q and A^T q
+  // within one block's shared memory, and unless CUDA graphs are asked for with
+  // pdlp_persistent_iterations = 0): the whole power iteration in one launch of
+  // cluster_power_kernel, which forms every sum as the multi-kernel form does (same step size bit
+  // for bit) with two cluster barriers per step in place of six kernel boundaries.  Returns false
+  // where it does not apply.
+  static constexpr int64_t kClusterPowerNnz = 262144;
+  bool cluster_power(const dev_sell<TX>& As, const dev_sell<TX>& ATs, const double* z0,
+                     power_state* ps, int pg, int ga, int gt)
+  {
+    if (p_.persistent == 0 || L_.nnz > kClusterPowerNnz || in_.m > kClusterPowerMaxRows)
+      return false;
+    int dev = 0, optin = 0;
+    B200_CUDA_CHECK(cudaGetDevice(&dev));
+    B200_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t smem = cluster_power_smem(in_.m, in_.n, pg, ga);
+    if (smem + 1024 > (size_t)optin) return false;
+    const void* fn = (const void*)cluster_power_kernel<TX>;
+    B200_CUDA_CHECK(
+      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int blocks = 0;
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    // 16 blocks where the device allows clusters of that size, else the portable 8.
+    for (int c : {16, 8}) {
+      if (c > 8)
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess) {
+          (void)cudaGetLastError();
+          continue;
+        }
+      cfg                      = cudaLaunchConfig_t{};
+      cfg.gridDim              = dim3(c);
+      cfg.blockDim             = dim3(kBlock);
+      cfg.dynamicSmemBytes     = smem;
+      cfg.stream               = s_;
+      attr[0].id               = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = c;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs                = attr;
+      cfg.numAttrs             = 1;
+      int clusters             = 0;
+      if (cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg) == cudaSuccess && clusters > 0) {
+        blocks = c;
+        break;
+      }
+      (void)cudaGetLastError();
+    }
+    if (blocks == 0) return false;
+    B200_CUDA_CHECK(cudaLaunchKernelEx(&cfg, cluster_power_kernel<TX>, ATs, As, z0, in_.m, in_.n,
+                                       pg, gt, ga, ps, kPowerTol, kPowerMaxIters));
+    ++launches_;
+    power_state h{};
+    B200_CUDA_CHECK(cudaMemcpyAsync(&h, ps, sizeof(h), cudaMemcpyDeviceToHost, s_));
+    B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+    power_iters_    = h.iters;
+    eta_            = kStepScaling / std::sqrt(h.s2);
+    cluster_blocks_ = blocks;
+    return true;
   }
 
   // Largest singular value of the scaled A by Golub-Kahan-Lanczos bidiagonalisation, used in
@@ -1469,6 +1532,7 @@ class engine {
   form_key form_key_{};
   double form_us_[3] = {0, 0, 0};  // the timings behind the choice (this solve's or cached)
   size_t cluster_smem_ = 0;         // dynamic shared memory of the cluster form
+  int cluster_blocks_  = 0;         // blocks of the cluster power iteration (0: not used)
   long cluster_launches_ = 0;
   // Warps per block of the plain sweeps and the timings they were chosen by.
   int wpb_primal_ = kWarpsPerBlock, wpb_dual_ = kWarpsPerBlock;
