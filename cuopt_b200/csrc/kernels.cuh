@@ -1070,6 +1070,23 @@ inline size_t cluster_power_smem(int m, int n, int pg, int ga)
   return (2 * pad(m) + pad(n) + 2 * pad(ga) + 2 * pad(pg)) * sizeof(double);
 }
 
+// ordered_block_sum<1> of nb <= 32 partials, formed by warp 0: each thread's compensated sum of a
+// single partial is that partial, and the block tree's levels above 16 only add zeros, so the
+// warp's shuffle tree of the same pairs gives the same value.  Result in *out for the block.
+__device__ __forceinline__ void small_ordered_sum(const double* p, int nb, double* out)
+{
+  if (threadIdx.x < kWarp) {
+    double v = (int)threadIdx.x < nb ? p[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int h = 16; h > 0; h >>= 1) v += __shfl_down_sync(0xffffffffu, v, h);
+    if (threadIdx.x == 0) *out = v;
+  }
+  __syncthreads();
+}
+
+// Largest emulated block count of the cluster power iteration's vector steps and sums.
+constexpr int kClusterPowerMaxBlocks = 32;
+
 template <typename TX>
 __global__ void __launch_bounds__(kBlock)
   cluster_power_kernel(const dev_sell<TX> AT, const dev_sell<TX> A, const double* z0, int m, int n,
@@ -1085,25 +1102,41 @@ __global__ void __launch_bounds__(kBlock)
   double* pz   = st + pad(ga);   // |z|^2 partials
   double* pr   = pz + pad(pg);   // residual partials
   __shared__ double scalar;
+  // Per-warp sums of the emulated blocks (block_reduce_store's first stage, all blocks at once).
+  __shared__ double wz[kClusterPowerMaxBlocks][kWarpsPerBlock];
+  __shared__ double wr[kClusterPowerMaxBlocks][kWarpsPerBlock];
   const unsigned rank = cluster_rank(), C = cluster_size();
+  const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
   const dsmem_sink<double> to_z{(unsigned)__cvta_generic_to_shared(zc), C};
   const dsmem_sink<double> to_atq{(unsigned)__cvta_generic_to_shared(atqc), C};
   const unsigned sc_addr = (unsigned)__cvta_generic_to_shared(sc);
 
   for (int i = threadIdx.x; i < m; i += kBlock) zc[i] = z0[i];
   __syncthreads();
+  // The pg block partials from the per-warp sums, summed over the warps in order
+  // (block_reduce_store's second stage).
+  auto finish_partials = [&](double (*w)[kWarpsPerBlock], double* out) {
+    __syncthreads();
+    if ((int)threadIdx.x < pg) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < kWarpsPerBlock; ++k) s += w[threadIdx.x][k];
+      out[threadIdx.x] = s;
+    }
+    __syncthreads();
+  };
   // |z|^2 partials of the pg emulated blocks (vec_reduce_kernel<0>).
   auto sumsq = [&]() {
     for (int b = 0; b < pg; ++b) {
-      red_t<1> r;
-      r.v[0] = 0.0;
+      double r = 0.0;
       for (int i = b * kBlock + threadIdx.x; i < m; i += pg * kBlock) {
         const double v = zc[i];
-        r.v[0] += v * v;
+        r += v * v;
       }
-      block_reduce_store<1>(r, pz, b);
+      r = warp_sum(r);
+      if (lane == 0) wz[b][warp] = r;
     }
-    __syncthreads();
+    finish_partials(wz, pz);
   };
   sumsq();
   // Every block of the cluster is running before any block stores into another's memory.
@@ -1112,7 +1145,7 @@ __global__ void __launch_bounds__(kBlock)
   double nq = 0.0, s2 = 0.0, resid = 0.0;
   while (it < max_iters && !done) {
     // q = z / |z|  (power_normalize_sum_kernel), on the local copies.
-    ordered_block_sum<1>(pz, pg, &scalar);
+    small_ordered_sum(pz, pg, &scalar);
     nq = sqrt(scalar);
     for (int i = threadIdx.x; i < m; i += kBlock) qc[i] = zc[i] / nq;
     __syncthreads();
@@ -1129,23 +1162,29 @@ __global__ void __launch_bounds__(kBlock)
           dsmem_store(sc_addr + (unsigned)vb * (unsigned)sizeof(double), c, st[vb]);
     }
     cluster_barrier();
-    // q <- q (-s2) + z with its squares' partials (power_residual_sum_kernel), the next |z|^2
-    // partials, and the test of power_check_sum_kernel, all on the local copies.
-    ordered_block_sum<1>(sc, ga, &scalar);
+    // q <- q (-s2) + z with its squares' partials (power_residual_sum_kernel) and the next |z|^2
+    // partials, then the test of power_check_sum_kernel, all on the local copies.
+    small_ordered_sum(sc, ga, &scalar);
     s2 = scalar;
     for (int b = 0; b < pg; ++b) {
-      red_t<1> r;
-      r.v[0] = 0.0;
+      double rr = 0.0, rz = 0.0;
       for (int i = b * kBlock + threadIdx.x; i < m; i += pg * kBlock) {
-        const double v = qc[i] * -s2 + zc[i];
-        qc[i]          = v;
-        r.v[0] += v * v;
+        const double zi = zc[i];
+        const double v  = qc[i] * -s2 + zi;
+        qc[i]           = v;
+        rr += v * v;
+        rz += zi * zi;
       }
-      block_reduce_store<1>(r, pr, b);
+      rr = warp_sum(rr);
+      rz = warp_sum(rz);
+      if (lane == 0) {
+        wr[b][warp] = rr;
+        wz[b][warp] = rz;
+      }
     }
-    __syncthreads();
-    sumsq();
-    ordered_block_sum<1>(pr, pg, &scalar);
+    finish_partials(wr, pr);
+    finish_partials(wz, pz);
+    small_ordered_sum(pr, pg, &scalar);
     resid = sqrt(scalar);
     ++it;
     done = resid < tol;

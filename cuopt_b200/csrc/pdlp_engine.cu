@@ -498,7 +498,8 @@ class engine {
   bool cluster_power(const dev_sell<TX>& As, const dev_sell<TX>& ATs, const double* z0,
                      power_state* ps, int pg, int ga, int gt)
   {
-    if (p_.persistent == 0 || L_.nnz > kClusterPowerNnz || in_.m > kClusterPowerMaxRows)
+    if (p_.persistent == 0 || L_.nnz > kClusterPowerNnz || in_.m > kClusterPowerMaxRows ||
+        pg > kClusterPowerMaxBlocks || ga > kClusterPowerMaxBlocks)
       return false;
     int dev = 0, optin = 0;
     B200_CUDA_CHECK(cudaGetDevice(&dev));
