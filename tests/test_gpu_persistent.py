@@ -46,12 +46,18 @@ def lp_c0():
 
 @pytest.mark.parametrize("precision", [0, 1])
 def test_persistent_matches_graphs(lp_c0, precision):
+    """Every form of the plain iterations gives the same solve.  In FP64 the graphs-only setting
+    (0) also runs the multi-kernel power iteration, the others the cluster power iteration of
+    small LPs, so the comparison covers that the two give the same step size bit for bit."""
     dm = datamodel_from_lp(lp_c0)
     g = lpm.Solve(dm, _settings(GRAPHS, tol=1e-6, precision=precision))
     p = lpm.Solve(dm, _settings(PERSISTENT, tol=1e-6, precision=precision))
     c = lpm.Solve(dm, _settings(CLUSTER, tol=1e-6, precision=precision))
     a = lpm.Solve(dm, _settings(AUTO, tol=1e-6, precision=precision))
     assert g.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert g.stats["step_size"] == c.stats["step_size"]
+    if precision == 0:
+        assert g.stats["power_iterations"] == c.stats["power_iterations"] > 0
     _same(g, p)
     _same(g, c)
     _same(g, a)
