@@ -1102,9 +1102,6 @@ __global__ void __launch_bounds__(kBlock)
   double* pz   = st + pad(ga);   // |z|^2 partials
   double* pr   = pz + pad(pg);   // residual partials
   __shared__ double scalar;
-  // Per-warp sums of the emulated blocks (block_reduce_store's first stage, all blocks at once).
-  __shared__ double wz[kClusterPowerMaxBlocks][kWarpsPerBlock];
-  __shared__ double wr[kClusterPowerMaxBlocks][kWarpsPerBlock];
   const unsigned rank = cluster_rank(), C = cluster_size();
   const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
   const dsmem_sink<double> to_z{(unsigned)__cvta_generic_to_shared(zc), C};
@@ -1113,30 +1110,25 @@ __global__ void __launch_bounds__(kBlock)
 
   for (int i = threadIdx.x; i < m; i += kBlock) zc[i] = z0[i];
   __syncthreads();
-  // The pg block partials from the per-warp sums, summed over the warps in order
-  // (block_reduce_store's second stage).
-  auto finish_partials = [&](double (*w)[kWarpsPerBlock], double* out) {
-    __syncthreads();
-    if ((int)threadIdx.x < pg) {
-      double s = 0.0;
-#pragma unroll
-      for (int k = 0; k < kWarpsPerBlock; ++k) s += w[threadIdx.x][k];
-      out[threadIdx.x] = s;
-    }
-    __syncthreads();
-  };
+  // An emulated block's partial is formed by one warp: for each of the block's 8 warps w, the
+  // warp's lanes take the sums of threads 32 w + lane, warp_sum pairs them as warp w's own
+  // warp_sum would, and the 8 results are added in order from 0.0 (block_reduce_store's two
+  // stages).  Warp k of this block forms the partials of emulated blocks k, k + 8, ...
   // |z|^2 partials of the pg emulated blocks (vec_reduce_kernel<0>).
   auto sumsq = [&]() {
-    for (int b = 0; b < pg; ++b) {
-      double r = 0.0;
-      for (int i = b * kBlock + threadIdx.x; i < m; i += pg * kBlock) {
-        const double v = zc[i];
-        r += v * v;
+    for (int b = warp; b < pg; b += kWarpsPerBlock) {
+      double s = 0.0;
+      for (int w = 0; w < kWarpsPerBlock; ++w) {
+        double r = 0.0;
+        for (int i = b * kBlock + w * kWarp + lane; i < m; i += pg * kBlock) {
+          const double v = zc[i];
+          r += v * v;
+        }
+        s += warp_sum(r);
       }
-      r = warp_sum(r);
-      if (lane == 0) wz[b][warp] = r;
+      if (lane == 0) pz[b] = s;
     }
-    finish_partials(wz, pz);
+    __syncthreads();
   };
   sumsq();
   // Every block of the cluster is running before any block stores into another's memory.
@@ -1166,24 +1158,26 @@ __global__ void __launch_bounds__(kBlock)
     // partials, then the test of power_check_sum_kernel, all on the local copies.
     small_ordered_sum(sc, ga, &scalar);
     s2 = scalar;
-    for (int b = 0; b < pg; ++b) {
-      double rr = 0.0, rz = 0.0;
-      for (int i = b * kBlock + threadIdx.x; i < m; i += pg * kBlock) {
-        const double zi = zc[i];
-        const double v  = qc[i] * -s2 + zi;
-        qc[i]           = v;
-        rr += v * v;
-        rz += zi * zi;
+    for (int b = warp; b < pg; b += kWarpsPerBlock) {
+      double sr = 0.0, sz = 0.0;
+      for (int w = 0; w < kWarpsPerBlock; ++w) {
+        double rr = 0.0, rz = 0.0;
+        for (int i = b * kBlock + w * kWarp + lane; i < m; i += pg * kBlock) {
+          const double zi = zc[i];
+          const double v  = qc[i] * -s2 + zi;
+          qc[i]           = v;
+          rr += v * v;
+          rz += zi * zi;
+        }
+        sr += warp_sum(rr);
+        sz += warp_sum(rz);
       }
-      rr = warp_sum(rr);
-      rz = warp_sum(rz);
       if (lane == 0) {
-        wr[b][warp] = rr;
-        wz[b][warp] = rz;
+        pr[b] = sr;
+        pz[b] = sz;
       }
     }
-    finish_partials(wr, pr);
-    finish_partials(wz, pz);
+    __syncthreads();
     small_ordered_sum(pr, pg, &scalar);
     resid = sqrt(scalar);
     ++it;
