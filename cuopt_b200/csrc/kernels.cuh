@@ -211,11 +211,60 @@ __device__ __forceinline__ T gather_load(const T* __restrict__ g, int i)
     return g[i];
 }
 
+// Where a sweep reads the matrix's values and indices from: global memory with evict-first loads
+// (every sweep but one), or a copy of the block's own virtual blocks in shared memory (the
+// cluster power iteration), whose element k of the view's arrays sits at k - shift.
+struct global_matrix {
+  static constexpr int64_t shift = 0;
+  template <typename T>
+  __device__ __forceinline__ T ld(const T* p) const
+  {
+    return ld_stream(p);
+  }
+  template <typename T>
+  __device__ __forceinline__ void chunk(const T* p, double (&v)[4]) const
+  {
+    load_chunk(p, v);
+  }
+  __device__ __forceinline__ int4 idx_chunk(const int* p) const { return load_idx_chunk(p); }
+};
+struct shared_matrix {
+  int64_t shift;
+  template <typename T>
+  __device__ __forceinline__ T ld(const T* p) const
+  {
+    return *p;
+  }
+  __device__ __forceinline__ void chunk(const float* p, double (&v)[4]) const
+  {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0]           = t.x;
+    v[1]           = t.y;
+    v[2]           = t.z;
+    v[3]           = t.w;
+  }
+  __device__ __forceinline__ void chunk(const double* p, double (&v)[4]) const
+  {
+    const double2 a = reinterpret_cast<const double2*>(p)[0];
+    const double2 b = reinterpret_cast<const double2*>(p)[1];
+    v[0]            = a.x;
+    v[1]            = a.y;
+    v[2]            = b.x;
+    v[3]            = b.y;
+  }
+  __device__ __forceinline__ int4 idx_chunk(const int* p) const
+  {
+    return *reinterpret_cast<const int4*>(p);
+  }
+};
+
 // WPB: warps (rows or slices) per block.  Only the grouping of warps into blocks depends on it,
 // not any row's arithmetic; sweeps with block reductions (kRed > 0) use kWarpsPerBlock.
-template <typename TM, typename TG, class Epi, bool COH = false, int WPB = kWarpsPerBlock>
+template <typename TM, typename TG, class Epi, bool COH = false, int WPB = kWarpsPerBlock,
+          class MS = global_matrix>
 __device__ __forceinline__ void sell_map_block(const dev_sell<TM>& A, const TG* __restrict__ g,
-                                               const Epi& epi, double* partials, int vb)
+                                               const Epi& epi, double* partials, int vb,
+                                               const MS& ms = MS{})
 {
   constexpr int K = Epi::kRed;
   static_assert(K == 0 || WPB == kWarpsPerBlock, "block reductions assume kWarpsPerBlock warps");
@@ -234,10 +283,10 @@ __device__ __forceinline__ void sell_map_block(const dev_sell<TM>& A, const TG* 
     const int row = q < A.long_count() ? (A.long_list ? A.long_list[q] : q) : 0;
     if (q < A.long_count() && !skip_rows(epi, row, row)) {
       const auto pre  = epi.load(row);
-      const int64_t b = A.long_off[row], e = A.long_off[row + 1];
+      const int64_t b = A.long_off[row] - ms.shift, e = A.long_off[row + 1] - ms.shift;
       double acc      = 0.0;
       for (int64_t k = b + lane; k < e; k += kWarp)
-        acc += (double)ld_stream(A.val + k) * (double)gather_load<COH>(g, ld_stream(A.idx + k));
+        acc += (double)ms.ld(A.val + k) * (double)gather_load<COH>(g, ms.ld(A.idx + k));
       acc = warp_sum(acc);
       if (lane == 0) epi(row, acc, pre, red);
     }
@@ -251,15 +300,15 @@ __device__ __forceinline__ void sell_map_block(const dev_sell<TM>& A, const TG* 
       const auto pre     = epi.load(valid ? row : A.rows - 1);
       const int64_t base = A.slice_off[s];
       const int nchunk   = (int)((A.slice_off[s + 1] - base) >> 7);  // 32 lanes x 4 elements
-      const TM* v        = A.val + base + lane * kChunk;
-      const int* ix      = A.idx + base + lane * kChunk;
+      const TM* v        = A.val + (base - ms.shift) + lane * kChunk;
+      const int* ix      = A.idx + (base - ms.shift) + lane * kChunk;
       double acc         = 0.0;
       int q              = 0;
       for (; q + 2 <= nchunk; q += 2) {
-        const int4 i0 = load_idx_chunk(ix), i1 = load_idx_chunk(ix + 32 * kChunk);
+        const int4 i0 = ms.idx_chunk(ix), i1 = ms.idx_chunk(ix + 32 * kChunk);
         double v0[4], v1[4];
-        load_chunk(v, v0);
-        load_chunk(v + 32 * kChunk, v1);
+        ms.chunk(v, v0);
+        ms.chunk(v + 32 * kChunk, v1);
         const TG g0 = gather_load<COH>(g, i0.x), g1 = gather_load<COH>(g, i0.y);
         const TG g2 = gather_load<COH>(g, i0.z), g3 = gather_load<COH>(g, i0.w);
         const TG g4 = gather_load<COH>(g, i1.x), g5 = gather_load<COH>(g, i1.y);
@@ -276,9 +325,9 @@ __device__ __forceinline__ void sell_map_block(const dev_sell<TM>& A, const TG* 
         ix += 64 * kChunk;
       }
       if (q < nchunk) {
-        const int4 i0 = load_idx_chunk(ix);
+        const int4 i0 = ms.idx_chunk(ix);
         double v0[4];
-        load_chunk(v, v0);
+        ms.chunk(v, v0);
         const TG g0 = gather_load<COH>(g, i0.x), g1 = gather_load<COH>(g, i0.y);
         const TG g2 = gather_load<COH>(g, i0.z), g3 = gather_load<COH>(g, i0.w);
         acc += v0[0] * (double)g0;
@@ -1084,13 +1133,35 @@ __device__ __forceinline__ void small_ordered_sum(const double* p, int nb, doubl
   __syncthreads();
 }
 
-// Largest emulated block count of the cluster power iteration's vector steps and sums.
+// Largest emulated block count of the cluster power iteration's vector steps and sums, and the
+// largest number of virtual blocks of one sweep that one block of the cluster takes.
 constexpr int kClusterPowerMaxBlocks = 32;
+constexpr int kClusterPowerMaxOwn    = 16;
 
+// Element range [lo, hi) of virtual block vb (8 warps) of a sweep's matrix: its long rows, or its
+// slices, are contiguous in the matrix's arrays.
+template <typename TX>
+__device__ __forceinline__ void vb_range(const dev_sell<TX>& M, int vb, int64_t& lo, int64_t& hi)
+{
+  const int lb = long_blocks(M.long_count());
+  if (vb < lb) {
+    const int q0 = vb * kWarpsPerBlock, q1 = min(q0 + kWarpsPerBlock, M.long_count());
+    lo           = M.long_off[q0];
+    hi           = M.long_off[q1];
+  } else {
+    const int s0 = (vb - lb) * kWarpsPerBlock, s1 = min(s0 + kWarpsPerBlock, M.slice_count());
+    lo           = M.slice_off[s0];
+    hi           = M.slice_off[s1];
+  }
+}
+
+// With `cache`, each block first copies the values and indices of its own virtual blocks of both
+// sweeps into shared memory after the vectors (each range 16-byte aligned) and reads them there.
 template <typename TX>
 __global__ void __launch_bounds__(kBlock)
   cluster_power_kernel(const dev_sell<TX> AT, const dev_sell<TX> A, const double* z0, int m, int n,
-                       int pg, int gt, int ga, power_state* ps, double tol, int max_iters)
+                       int pg, int gt, int ga, power_state* ps, double tol, int max_iters,
+                       int cache)
 {
   extern __shared__ __align__(16) unsigned char cp_smem[];
   auto pad     = [](int v) { return (v + 15) & ~15; };
@@ -1109,7 +1180,51 @@ __global__ void __launch_bounds__(kBlock)
   const unsigned sc_addr = (unsigned)__cvta_generic_to_shared(sc);
 
   for (int i = threadIdx.x; i < m; i += kBlock) zc[i] = z0[i];
+  // The matrix copy: per sweep (0: A^T, 1: A) and own virtual block k, the range's start and the
+  // byte offsets of its values and indices in the copy.
+  __shared__ long long own_lo[2][kClusterPowerMaxOwn];
+  __shared__ unsigned own_val[2][kClusterPowerMaxOwn], own_idx[2][kClusterPowerMaxOwn];
+  unsigned char* mat = reinterpret_cast<unsigned char*>(pr + pad(pg));
+  if (cache) {
+    unsigned used = 0;
+    for (int w = 0; w < 2; ++w) {
+      const dev_sell<TX>& M = w == 0 ? AT : A;
+      const int g           = w == 0 ? gt : ga;
+      int k                 = 0;
+      for (int vb = (int)rank; vb < g; vb += (int)C, ++k) {
+        int64_t lo, hi;
+        vb_range(M, vb, lo, hi);
+        const unsigned vbytes = (unsigned)(((hi - lo) * (int64_t)sizeof(TX) + 15) & ~15);
+        const unsigned ibytes = (unsigned)(((hi - lo) * (int64_t)sizeof(int) + 15) & ~15);
+        TX* dv                = reinterpret_cast<TX*>(mat + used);
+        int* di               = reinterpret_cast<int*>(mat + used + vbytes);
+        for (int64_t e = lo + threadIdx.x; e < hi; e += kBlock) {
+          dv[e - lo] = M.val[e];
+          di[e - lo] = M.idx[e];
+        }
+        if (threadIdx.x == 0) {
+          own_lo[w][k]  = lo;
+          own_val[w][k] = used;
+          own_idx[w][k] = used + vbytes;
+        }
+        used += vbytes + ibytes;
+      }
+    }
+  }
   __syncthreads();
+  // Sweep w's virtual block vb (the k-th of this block) from the copy or from global memory.
+  auto sweep = [&](int w, int vb, int k, const double* gv, auto epi, double* partials) {
+    const dev_sell<TX>& M = w == 0 ? AT : A;
+    if (cache) {
+      dev_sell<TX> V = M;
+      V.val          = reinterpret_cast<const TX*>(mat + own_val[w][k]);
+      V.idx          = reinterpret_cast<const int*>(mat + own_idx[w][k]);
+      sell_map_block<TX, double, decltype(epi), false, kWarpsPerBlock, shared_matrix>(
+        V, gv, epi, partials, vb, shared_matrix{own_lo[w][k]});
+    } else {
+      sell_map_block<TX, double, decltype(epi)>(M, gv, epi, partials, vb);
+    }
+  };
   // An emulated block's partial is formed by one warp: for each of the block's 8 warps w, the
   // warp's lanes take the sums of threads 32 w + lane, warp_sum pairs them as warp w's own
   // warp_sum would, and the 8 results are added in order from 0.0 (block_reduce_store's two
@@ -1142,13 +1257,12 @@ __global__ void __launch_bounds__(kBlock)
     for (int i = threadIdx.x; i < m; i += kBlock) qc[i] = zc[i] / nq;
     __syncthreads();
     // A^T q over this block's virtual blocks, entries sent to every copy.
-    for (int vb = (int)rank; vb < gt; vb += (int)C)
-      sell_map_block<TX, double, cluster_atq_epi<TX>>(AT, qc, cluster_atq_epi<TX>{to_atq},
-                                                      nullptr, vb);
+    for (int vb = (int)rank, k = 0; vb < gt; vb += (int)C, ++k)
+      sweep(0, vb, k, qc, cluster_atq_epi<TX>{to_atq}, nullptr);
     cluster_barrier();
     // z = A (A^T q) with the q . z partial of each virtual block, both sent to every copy.
-    for (int vb = (int)rank; vb < ga; vb += (int)C) {
-      sell_map_block<TX, double, cluster_z_epi>(A, atqc, cluster_z_epi{to_z, qc}, st, vb);
+    for (int vb = (int)rank, k = 0; vb < ga; vb += (int)C, ++k) {
+      sweep(1, vb, k, atqc, cluster_z_epi{to_z, qc}, st);
       if (threadIdx.x == 0)
         for (unsigned c = 0; c < C; ++c)
           dsmem_store(sc_addr + (unsigned)vb * (unsigned)sizeof(double), c, st[vb]);

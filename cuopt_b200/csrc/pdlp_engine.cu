@@ -504,15 +504,49 @@ class engine {
     int dev = 0, optin = 0;
     B200_CUDA_CHECK(cudaGetDevice(&dev));
     B200_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    const size_t smem = cluster_power_smem(in_.m, in_.n, pg, ga);
-    if (smem + 1024 > (size_t)optin) return false;
+    const size_t vec_smem = cluster_power_smem(in_.m, in_.n, pg, ga);
+    if (vec_smem + 1024 > (size_t)optin) return false;
+    // Shared memory a block needs to hold its own virtual blocks of both sweeps (cluster size c).
+    auto ranges = [&](const dev_matrix& M) {
+      std::vector<int64_t> lo(M.n_long + 1), so(M.n_slices + 1);
+      B200_CUDA_CHECK(cudaMemcpyAsync(lo.data(), M.long_off.data(), lo.size() * sizeof(int64_t),
+                                      cudaMemcpyDeviceToHost, s_));
+      B200_CUDA_CHECK(cudaMemcpyAsync(so.data(), M.slice_off.data(),
+                                      so.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+      B200_CUDA_CHECK(cudaStreamSynchronize(s_));
+      std::vector<int64_t> count;  // elements of each virtual block
+      const int lb = long_blocks(M.n_long);
+      for (int vb = 0; vb < lb; ++vb)
+        count.push_back(lo[std::min((vb + 1) * kWarpsPerBlock, M.n_long)] - lo[vb * kWarpsPerBlock]);
+      for (int s0 = 0; s0 < M.n_slices; s0 += kWarpsPerBlock)
+        count.push_back(so[std::min(s0 + kWarpsPerBlock, M.n_slices)] - so[s0]);
+      return count;
+    };
+    const std::vector<int64_t> cnt_t = ranges(L_.AT), cnt_a = ranges(L_.A);
+    auto copy_smem = [&](int c) -> size_t {
+      size_t worst = 0;
+      for (int r = 0; r < c; ++r) {
+        size_t bytes = 0;
+        int own      = 0;
+        for (const auto* cnt : {&cnt_t, &cnt_a}) {
+          int k = 0;
+          for (size_t vb = r; vb < cnt->size(); vb += c, ++k)
+            bytes += (((*cnt)[vb] * sizeof(TX) + 15) & ~size_t(15)) +
+                     (((*cnt)[vb] * sizeof(int) + 15) & ~size_t(15));
+          own = std::max(own, k);
+        }
+        if (own > kClusterPowerMaxOwn) return SIZE_MAX;
+        worst = std::max(worst, bytes);
+      }
+      return worst;
+    };
     const void* fn = (const void*)cluster_power_kernel<TX>;
-    B200_CUDA_CHECK(
-      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int blocks = 0;
+    int blocks = 0, cache = 0;
+    size_t smem = vec_smem;
     cudaLaunchConfig_t cfg{};
     cudaLaunchAttribute attr[1];
-    // 16 blocks where the device allows clusters of that size, else the portable 8.
+    // 16 blocks where the device allows clusters of that size, else the portable 8; the matrix
+    // copy where it fits beside the vectors.
     for (int c : {16, 8}) {
       if (c > 8)
         if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
@@ -520,6 +554,11 @@ class engine {
           (void)cudaGetLastError();
           continue;
         }
+      const size_t mat = copy_smem(c);
+      cache            = mat != SIZE_MAX && vec_smem + mat + 1024 <= (size_t)optin;
+      smem             = vec_smem + (cache ? mat : 0);
+      B200_CUDA_CHECK(
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       cfg                      = cudaLaunchConfig_t{};
       cfg.gridDim              = dim3(c);
       cfg.blockDim             = dim3(kBlock);
@@ -540,7 +579,7 @@ class engine {
     }
     if (blocks == 0) return false;
     B200_CUDA_CHECK(cudaLaunchKernelEx(&cfg, cluster_power_kernel<TX>, ATs, As, z0, in_.m, in_.n,
-                                       pg, gt, ga, ps, kPowerTol, kPowerMaxIters));
+                                       pg, gt, ga, ps, kPowerTol, kPowerMaxIters, cache));
     ++launches_;
     power_state h{};
     B200_CUDA_CHECK(cudaMemcpyAsync(&h, ps, sizeof(h), cudaMemcpyDeviceToHost, s_));
@@ -548,6 +587,10 @@ class engine {
     power_iters_    = h.iters;
     eta_            = kStepScaling / std::sqrt(h.s2);
     cluster_blocks_ = blocks;
+    if (std::getenv("CUOPT_B200_TRACE"))
+      std::fprintf(stderr, "[cuopt_b200] cluster power iteration: %d blocks, %zu bytes of shared "
+                           "memory each, matrix copy %s\n",
+                   blocks, smem, cache ? "on" : "off");
     return true;
   }
 
