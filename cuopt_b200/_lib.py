@@ -140,6 +140,8 @@ SIGNATURES = {
                                              C.POINTER(C.c_double), C.POINTER(cuopt_int_t)]),
     "cuOptProfileScatterRate": (cuopt_int_t, [cuopt_int_t, C.c_int64, cuopt_int_t, C.c_void_p,
                                               C.POINTER(C.c_double), C.POINTER(cuopt_int_t)]),
+    "cuOptProbeClusterBarrier": (cuopt_int_t, [cuopt_int_t, cuopt_int_t, cuopt_int_t, C.c_void_p,
+                                               C.POINTER(C.c_double)]),
     "cuOptProbeGridBarrier": (cuopt_int_t, [cuopt_int_t, cuopt_int_t, cuopt_int_t, C.c_double,
                                             C.c_void_p, C.POINTER(cuopt_int_t),
                                             C.POINTER(C.c_double)]),

@@ -218,6 +218,11 @@ def run_barrier() -> dict:
 
     L = lib()
     out = {}
+    for blocks, threads in ((8, 256), (16, 256), (8, 1024), (16, 1024), (2, 256)):
+        ms = C.c_double()
+        code = L.cuOptProbeClusterBarrier(blocks, threads, 5000, None, C.byref(ms))
+        out[f"cluster_{blocks}x{threads}"] = ({"us_per_barrier": 1e3 * ms.value / 5000}
+                                              if code == 0 else {"rc": code})
     for blocks in (8, 21, 57, 148, 296, 592, 740, 1184):
         st, ms = C.c_int32(), C.c_double()
         code = L.cuOptProbeGridBarrier(blocks, 5000, 0, 5000.0, None, C.byref(st), C.byref(ms))

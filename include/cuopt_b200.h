@@ -117,6 +117,17 @@ cuopt_int_t cuOptProbeGridBarrier(cuopt_int_t blocks,
                                   cuopt_int_t* status,
                                   cuopt_float_t* elapsed_ms);
 
+/* Measurement hook (no counterpart in the reference): the cluster barrier that the cluster-resident
+ * kernels (small LPs) place between their steps, run alone: one cluster of `blocks` (1 to 16)
+ * blocks of `threads` threads passes `rounds` barriers.  Returns the device time from the first
+ * block's start to its end, in milliseconds (CUOPT_INVALID_ARGUMENT where the device cannot run
+ * such a cluster). */
+cuopt_int_t cuOptProbeClusterBarrier(cuopt_int_t blocks,
+                                     cuopt_int_t threads,
+                                     cuopt_int_t rounds,
+                                     void* stream,
+                                     cuopt_float_t* elapsed_ms);
+
 /* Measurement hook (no counterpart in the reference): the random-gather ceiling of the device.
  * Streams `gathers` random int32 indices into a vector of `vector_length` elements of
  * `element_bytes` (4 or 8) bytes, in the sliced-ELL sweeps' chunk shape (a warp reads 32 lanes x 4
