@@ -8,6 +8,8 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
+#include <set>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -58,6 +60,22 @@ inline void configure_pool_once()
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
   }
   configured_device = dev;
+}
+
+// A kernel's dynamic shared memory limit is a property of the function, shared by every host
+// thread: set per launch, two solves on different threads could lower it under each other's
+// launch.  It is therefore raised once per function and device to the device's opt-in maximum;
+// launches that ask for less are unaffected.
+inline void allow_max_dynamic_smem(const void* fn)
+{
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0, optin = 0;
+  B200_CUDA_CHECK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (!done.insert({fn, dev}).second) return;
+  B200_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  B200_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
 }
 
 // Small pinned host scratch for scalar read-backs (per thread, allocated once).

@@ -467,9 +467,7 @@ std::vector<lsqr_result> lsqr_solve_batch(const std::vector<const lsqr_problem*>
   d_desc.upload(h_desc.data(), h_desc.size(), s);
   const int n_smem = (int)smem_ids.size(), n_glob = (int)glob_ids.size();
   if (n_smem > 0) {
-    B200_CUDA_CHECK(cudaFuncSetAttribute(lsqr_kernel<true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem_bytes));
+    allow_max_dynamic_smem((const void*)lsqr_kernel<true>);
     lsqr_kernel<true><<<n_smem, kLsqrThreads, smem_bytes, s>>>(d_desc.data(), d_out.data());
     B200_LAUNCH_CHECK();
   }

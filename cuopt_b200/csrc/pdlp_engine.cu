@@ -557,8 +557,7 @@ class engine {
       const size_t mat = copy_smem(c);
       cache            = mat != SIZE_MAX && vec_smem + mat + 1024 <= (size_t)optin;
       smem             = vec_smem + (cache ? mat : 0);
-      B200_CUDA_CHECK(
-        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      allow_max_dynamic_smem(fn);
       cfg                      = cudaLaunchConfig_t{};
       cfg.gridDim              = dim3(c);
       cfg.blockDim             = dim3(kBlock);
@@ -848,8 +847,8 @@ class engine {
     if (!have_t) tAT_ = tile_matrix{};
     if (!have_a && !have_t) return false;
     const size_t smem = std::max(have_a ? tA_.smem_bytes() : 0, have_t ? tAT_.smem_bytes() : 0);
-    B200_CUDA_CHECK(cudaFuncSetAttribute(tile_sweep_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    allow_max_dynamic_smem((const void*)tile_sweep_kernel);
+    (void)smem;
     tpart_.resize(std::max(have_a ? (size_t)tA_.groups * in_.m : 1,
                            have_t ? (size_t)tAT_.groups * in_.n : 1));
     terr_.resize(1);
@@ -970,9 +969,7 @@ class engine {
     cluster_smem_ = ((size_t)((in_.m + 15) & ~15) + (size_t)in_.n) * sizeof(TX);
     bool cl_ok    = sell && cluster_smem_ + 1024 <= (size_t)optin;
     if (cl_ok) {
-      B200_CUDA_CHECK(cudaFuncSetAttribute(cluster_fn(),
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)cluster_smem_));
+      allow_max_dynamic_smem(cluster_fn());
       cudaLaunchConfig_t cfg{};
       cudaLaunchAttribute attr[1];
       cluster_config(cfg, attr);
