@@ -64,8 +64,8 @@ inline void configure_pool_once()
 
 // A kernel's dynamic shared memory limit is a property of the function, shared by every host
 // thread: set per launch, two solves on different threads could lower it under each other's
-// launch.  It is therefore raised once per function and device to the device's opt-in maximum;
-// launches that ask for less are unaffected.
+// launch.  It is therefore raised once per function and device to the device's opt-in maximum
+// less the function's static shared memory; launches that ask for less are unaffected.
 inline void allow_max_dynamic_smem(const void* fn)
 {
   static std::mutex mu;
@@ -73,9 +73,24 @@ inline void allow_max_dynamic_smem(const void* fn)
   int dev = 0, optin = 0;
   B200_CUDA_CHECK(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lock(mu);
-  if (!done.insert({fn, dev}).second) return;
+  if (done.count({fn, dev})) return;
   B200_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  B200_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  cudaFuncAttributes fa{};
+  B200_CUDA_CHECK(cudaFuncGetAttributes(&fa, fn));
+  B200_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       optin - (int)fa.sharedSizeBytes));
+  done.insert({fn, dev});
+}
+
+// Dynamic shared memory a launch of fn may ask for on the current device.
+inline size_t max_dynamic_smem(const void* fn)
+{
+  int dev = 0, optin = 0;
+  B200_CUDA_CHECK(cudaGetDevice(&dev));
+  B200_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa{};
+  B200_CUDA_CHECK(cudaFuncGetAttributes(&fa, fn));
+  return (size_t)optin - fa.sharedSizeBytes;
 }
 
 // Small pinned host scratch for scalar read-backs (per thread, allocated once).

@@ -505,7 +505,8 @@ class engine {
     B200_CUDA_CHECK(cudaGetDevice(&dev));
     B200_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     const size_t vec_smem = cluster_power_smem(in_.m, in_.n, pg, ga);
-    if (vec_smem + 1024 > (size_t)optin) return false;
+    const size_t limit = max_dynamic_smem((const void*)cluster_power_kernel<TX>);
+    if (vec_smem > limit) return false;
     // Shared memory a block needs to hold its own virtual blocks of both sweeps (cluster size c).
     auto ranges = [&](const dev_matrix& M) {
       std::vector<int64_t> lo(M.n_long + 1), so(M.n_slices + 1);
@@ -555,7 +556,7 @@ class engine {
           continue;
         }
       const size_t mat = copy_smem(c);
-      cache            = mat != SIZE_MAX && vec_smem + mat + 1024 <= (size_t)optin;
+      cache            = mat != SIZE_MAX && vec_smem + mat <= limit;
       smem             = vec_smem + (cache ? mat : 0);
       allow_max_dynamic_smem(fn);
       cfg                      = cudaLaunchConfig_t{};
@@ -967,7 +968,7 @@ class engine {
     int optin = 0;
     B200_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     cluster_smem_ = ((size_t)((in_.m + 15) & ~15) + (size_t)in_.n) * sizeof(TX);
-    bool cl_ok    = sell && cluster_smem_ + 1024 <= (size_t)optin;
+    bool cl_ok    = sell && cluster_smem_ <= max_dynamic_smem(cluster_fn());
     if (cl_ok) {
       allow_max_dynamic_smem(cluster_fn());
       cudaLaunchConfig_t cfg{};
