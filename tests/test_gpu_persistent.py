@@ -136,6 +136,20 @@ def test_persistent_long_rows():
     assert c.stats["plain_iteration_form"] == CLUSTER
 
 
+def test_cluster_kernels_without_the_matrix_copy():
+    """4000 x 10000 in FP64: the power iteration's vectors fit in a cluster block's shared memory
+    but its share of the matrices does not (the kernel reads them from global memory), and the
+    plain iterations' vectors fit: both cluster kernels give the multi-kernel solve bit for bit."""
+    lp = gen.constructed_lp(4000, 10000, 8, seed=17)
+    dm = datamodel_from_lp(lp)
+    g = lpm.Solve(dm, _settings(GRAPHS, tol=1e-6))
+    c = lpm.Solve(dm, _settings(CLUSTER, tol=1e-6))
+    assert g.get_termination_status() == lpm.LPTerminationStatus.Optimal
+    assert c.stats["plain_iteration_form"] == CLUSTER
+    assert g.stats["step_size"] == c.stats["step_size"]
+    _same(g, c)
+
+
 def test_cluster_form_falls_back_on_large_lps():
     """The cluster form needs both gathered vectors in one block's shared memory: for
     20 000 + 50 000 FP64 entries (560 KB) a solve that asks for it runs the graphs."""
