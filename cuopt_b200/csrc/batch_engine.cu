@@ -27,6 +27,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <tuple>
 #include <random>
 #include <stdexcept>
 
@@ -658,6 +659,48 @@ struct inst_conv {
   double l2_primal = 0, l2_dual = 0, primal_obj = 0, dual_obj = 0, gap = 0, abs_obj = 0;
 };
 
+// Timing decisions of batch solves, remembered for the life of the process as those of single
+// solves are: per batch shape (rows, columns, non-zeros, instances), device, iterate precision and
+// the parameter that restricts the decision, and for the form of the plain iterations per set of
+// active instances (a hash of their indices; 0 when all are active).  A later solve of the same
+// batch reuses them instead of timing again.
+using batch_key = std::tuple<int, int, int64_t, int, int, int, int, uint64_t>;
+struct batch_form_choice {
+  int form;
+  double us[2];  // graphs, persistent kernel: microseconds per iteration when it was chosen
+};
+struct batch_shape_choice {
+  int wpb_primal, wpb_dual;
+  double ms[2][3];
+};
+std::mutex& batch_tune_mutex()
+{
+  static std::mutex mu;
+  return mu;
+}
+std::map<batch_key, batch_form_choice>& batch_form_cache()
+{
+  static std::map<batch_key, batch_form_choice> c;
+  return c;
+}
+std::map<batch_key, batch_shape_choice>& batch_shape_cache()
+{
+  static std::map<batch_key, batch_shape_choice> c;
+  return c;
+}
+// FNV-1a hash of the indices of the active instances (0 when every instance is active).
+uint64_t active_set_hash(const std::vector<int>& act)
+{
+  if (std::all_of(act.begin(), act.end(), [](int a) { return a != 0; })) return 0;
+  uint64_t h = 1469598103934665603ull;
+  for (size_t b = 0; b < act.size(); ++b)
+    if (act[b]) {
+      h ^= (uint64_t)b + 1;
+      h *= 1099511628211ull;
+    }
+  return h == 0 ? 1 : h;
+}
+
 template <typename TX>
 class batch_engine {
  public:
@@ -1269,7 +1312,7 @@ class batch_engine {
     B200_CUDA_CHECK(cudaStreamSynchronize(s_));
     lists_on_ = true;
     drop_graphs();
-    init_plain_form((int)std::count(act.begin(), act.end(), 1));
+    init_plain_form((int)std::count(act.begin(), act.end(), 1), active_set_hash(act));
   }
   void clear_work()
   {
@@ -1326,6 +1369,17 @@ class batch_engine {
   {
     wpb_primal_ = wpb_dual_ = p_.sweep_wpb ? p_.sweep_wpb : kWarpsPerBlock;
     if (p_.sweep_wpb) return;
+    const batch_key key = tune_key(0, 0);
+    {
+      std::lock_guard<std::mutex> lock(batch_tune_mutex());
+      auto it = batch_shape_cache().find(key);
+      if (it != batch_shape_cache().end()) {
+        wpb_primal_ = it->second.wpb_primal;
+        wpb_dual_   = it->second.wpb_dual;
+        std::memcpy(wpb_ms_, it->second.ms, sizeof(wpb_ms_));
+        return;
+      }
+    }
     const int m = in_.m, n = in_.n;
     upload_scalars(std::vector<long>(B_, 0));
     dbuf<TX> x0(n), y0(m);
@@ -1368,6 +1422,12 @@ class batch_engine {
     };
     wpb_primal_ = best(wpb_ms_[0]);
     wpb_dual_   = best(wpb_ms_[1]);
+    {
+      std::lock_guard<std::mutex> lock(batch_tune_mutex());
+      batch_shape_choice c{wpb_primal_, wpb_dual_, {}};
+      std::memcpy(c.ms, wpb_ms_, sizeof(wpb_ms_));
+      batch_shape_cache()[key] = c;
+    }
     B200_CUDA_CHECK(cudaMemcpyAsync(x_.data(), x0.data(), n * sizeof(TX),
                                     cudaMemcpyDeviceToDevice, s_));
     B200_CUDA_CHECK(cudaMemcpyAsync(y_.data(), y0.data(), m * sizeof(TX),
@@ -1405,7 +1465,13 @@ class batch_engine {
   {
     return (const void*)persistent_plain_kernel<TX, persist_pe, persist_de, advance_active>;
   }
-  void init_plain_form(int n_active)
+  batch_key tune_key(int param, uint64_t set_hash) const
+  {
+    int dev = 0;
+    B200_CUDA_CHECK(cudaGetDevice(&dev));
+    return batch_key{in_.m, in_.n, L_.nnz, B_, dev, (int)sizeof(TX), param, set_hash};
+  }
+  void init_plain_form(int n_active, uint64_t set_hash = 0)
   {
     int dev = 0, coop = 0, per_sm = 0;
     B200_CUDA_CHECK(cudaGetDevice(&dev));
@@ -1423,10 +1489,24 @@ class batch_engine {
     cycle_open_  = false;
     ++form_epochs_;
     const bool avail[plain_form_tuner::kForms] = {true, coop && persist_grid_ > 0, false};
-    form_.reset(p_.persistent, -1, avail);
-    if (n_active == B_ && form_.decided()) {  // forced (or the only form available)
+    form_key_   = tune_key(p_.persistent, set_hash);
+    int known   = -1;
+    known_us_[0] = known_us_[1] = 0.0;
+    if (p_.persistent < 0) {
+      std::lock_guard<std::mutex> lock(batch_tune_mutex());
+      auto it = batch_form_cache().find(form_key_);
+      if (it != batch_form_cache().end()) {
+        known        = it->second.form;
+        known_us_[0] = it->second.us[0];
+        known_us_[1] = it->second.us[1];
+      }
+    }
+    form_.reset(p_.persistent, known, avail);
+    if (n_active == B_ && form_.decided()) {  // forced, remembered, or the only form available
       first_form_   = form_.chosen();
       first_blocks_ = persist_grid_;
+      first_us_[0]  = known_us_[0];
+      first_us_[1]  = known_us_[1];
     }
   }
   void trace_form()
@@ -1448,7 +1528,12 @@ class batch_engine {
   {
     const bool before = form_.decided();
     form_.collect();
-    if (!before && form_.decided()) trace_form();
+    if (!before && form_.decided()) {
+      trace_form();
+      std::lock_guard<std::mutex> lock(batch_tune_mutex());
+      batch_form_cache()[form_key_] =
+        batch_form_choice{form_.chosen(), {form_.us_per_iteration(0), form_.us_per_iteration(1)}};
+    }
   }
   // Returns true for the first launch of the engine (which may include loading the kernel).
   bool launch_persistent(int L)
@@ -1850,6 +1935,8 @@ class batch_engine {
   int form_active_ = 0, form_epochs_ = 0;
   int first_form_ = -1, first_blocks_ = 0;
   double first_us_[2] = {0, 0};
+  batch_key form_key_{};           // the current work list's form decision in batch_form_cache
+  double known_us_[2] = {0, 0};    // its timings, when it was remembered from an earlier solve
   // Warps per block of the plain sweeps and the timings they were chosen by.
   int wpb_primal_ = kWarpsPerBlock, wpb_dual_ = kWarpsPerBlock;
   double wpb_ms_[2][3] = {{0, 0, 0}, {0, 0, 0}};

@@ -174,6 +174,27 @@ def test_batch_persistent_matches_graphs(precision):
     assert all(s.stats["plain_iteration_form"] == GRAPHS for s in g)
 
 
+def test_batch_timing_decisions_are_remembered():
+    """A second solve of the same batch reuses the first one's timed decisions (sweep block shapes,
+    form of the plain iterations per set of active instances) and reports the same timings; the
+    iterates do not depend on them."""
+    lps = [gen.constructed_lp(m, int(2.5 * m), k, seed=110 + i)
+           for i, (m, k) in enumerate([(300, 6), (1700, 9), (900, 11)])]
+    dms = [datamodel_from_lp(lp) for lp in lps]
+    s = _settings(AUTO, tol=1e-6, precision=1)
+    first = lpm.BatchSolve(dms, s)[0]
+    again = lpm.BatchSolve(dms, s)[0]
+    for a, b in zip(first, again):
+        assert a.get_termination_status() == lpm.LPTerminationStatus.Optimal
+        _same(a, b)
+    for key in ("plain_iteration_form", "plain_iteration_us_graphs",
+                "plain_iteration_us_persistent", "sweep_warps_per_block_primal",
+                "sweep_warps_per_block_dual", "sweep_block_shape_ms"):
+        assert first[0].stats[key] == again[0].stats[key], key
+    assert first[0].stats["plain_iteration_us_graphs"] > 0
+    assert all(t > 0 for t in first[0].stats["sweep_block_shape_ms"])
+
+
 def _probe(blocks, rounds, unreachable, budget_ms):
     lib = _lib.lib()
     st, ms = _lib.cuopt_int_t(), C.c_double()
