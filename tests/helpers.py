@@ -170,6 +170,18 @@ def chess_set_lp() -> lpm.DataModel:
     return dm
 
 
+def trivial_two_row_lp() -> lpm.DataModel:
+    """min x  s.t.  x <= 1 (twice),  x >= 0: the LP of the reference's Python solver test
+    (python/cuopt/cuopt/tests/linear_programming/test_lp_solver.py:46-79), which expects Optimal with
+    x = 0, zero residuals, zero objectives and zero gap at tolerance 1e-2."""
+    dm = lpm.DataModel()
+    dm.set_csr_constraint_matrix([1.0, 1.0], [0, 0], [0, 1, 2])
+    dm.set_constraint_bounds([1.0, 1.0])
+    dm.set_objective_coefficients([1.0])
+    dm.set_row_types(["L", "L"])
+    return dm
+
+
 def with_variable_bounds(view, j, lo, up):
     """A copy of an oracle view whose variable j has the bounds [lo, up] (a climber's LP)."""
     import copy

@@ -1,6 +1,7 @@
 """GPU tests on the small LPs written out in the reference's own tests: the ranged C API problem
 (c_api_tests.cpp:105-112), the maximisation whose objective must equal its dual objective
-(c_api_tests.cpp:149-165) and the chess-set LP (dual_simplex/unit_tests/solve.cpp:23-94).
+(c_api_tests.cpp:149-165), the chess-set LP (dual_simplex/unit_tests/solve.cpp:23-94) and the
+trivial two-row LP of the Python solver test (test_lp_solver.py:46-79).
 
 Each is solved through the C-ABI and checked against the golden values of those tests (with their
 tolerances) and against the oracle: same status and iteration count, objective within 1e-9
@@ -13,7 +14,7 @@ import pytest
 from cuopt_b200 import linear_programming as lpm
 from oracle import oracle as O
 from tests.helpers import (MAXIMIZE_DUAL_RHS, chess_set_lp, oracle_view, reference_maximize_dual_lp,
-                           reference_ranged_lp, rel, settings)
+                           reference_ranged_lp, rel, settings, trivial_two_row_lp)
 
 pytestmark = pytest.mark.gpu
 
@@ -49,6 +50,22 @@ def test_chess_set(golden):
     x = sol.get_primal_solution()
     assert abs(sol.get_primal_objective() - g["objective"]) <= 1e-2
     assert abs(x[0] - g["x"][0]) <= 1e-6 and abs(x[1] - g["x"][1]) <= 1e-3
+
+
+def test_trivial_two_row_lp():
+    """The reference runs this LP in Stable2 with a note that its Stable3 does not terminate on it;
+    Stable3 here (and in the oracle) ends Optimal, with the values that test asserts: x = 0, zero
+    residuals, objectives and gap, solved by PDLP."""
+    sol = _solve_both(trivial_two_row_lp(), 1e-2)
+    st = sol.get_lp_stats()
+    assert sol.get_termination_reason() == "Optimal"
+    assert sol.get_primal_solution()[0] == pytest.approx(0.0)
+    assert st["primal_residual"] == pytest.approx(0.0)
+    assert st["dual_residual"] == pytest.approx(0.0)
+    assert sol.get_primal_objective() == pytest.approx(0.0)
+    assert sol.get_dual_objective() == pytest.approx(0.0)
+    assert st["gap"] == pytest.approx(0.0)
+    assert sol.get_solved_by_pdlp()
 
 
 def test_afiro_climbers_with_different_bounds_like_the_reference(golden, golden_dir):

@@ -12,7 +12,7 @@ from cuopt_b200 import generators as gen
 from cuopt_b200 import linear_programming as lpm
 from oracle import oracle as O
 from tests.helpers import (MAXIMIZE_DUAL_RHS, chess_set_lp, oracle_view, reference_maximize_dual_lp,
-                           reference_ranged_lp, rel)
+                           reference_ranged_lp, rel, trivial_two_row_lp)
 
 
 def test_methodical1_initial_step_and_weight_match_reference_golden(golden, golden_dir):
@@ -279,6 +279,16 @@ def test_chess_set(golden, tol):
     assert res["status"] == 1
     assert abs(res["primal_obj"] - g["objective"]) <= 1e-2
     assert abs(x[0] - g["x"][0]) <= 1e-6 and abs(x[1] - g["x"][1]) <= 1e-3
+
+
+def test_trivial_two_row_lp():
+    """python/cuopt/cuopt/tests/linear_programming/test_lp_solver.py:46-79 (run there in Stable2):
+    Optimal at 1e-2 with x = 0, objectives 0 and gap 0."""
+    res, x, y, _ = O.solve(oracle_view(trivial_two_row_lp()), tol=1e-2)
+    assert res["status"] == 1
+    assert x[0] == pytest.approx(0.0)
+    assert res["primal_obj"] == pytest.approx(0.0) and res["dual_obj"] == pytest.approx(0.0)
+    assert res["gap"] == pytest.approx(0.0)
 
 
 @pytest.mark.parametrize("j,lo,up", [(5, 4.0, 5.0), (1, -7.0, 13.0)])
