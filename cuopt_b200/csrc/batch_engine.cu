@@ -15,6 +15,7 @@
 // a fixed order (the layout keeps every instance's rows contiguous inside the long-row and the
 // sliced parts, see make_keys_kernel).
 #include "device_layout.cuh"
+#include "host_io.hpp"
 #include "kernels.cuh"
 #include "pdlp_engine.hpp"
 #include "pdlp_schedule.hpp"
@@ -1204,7 +1205,8 @@ class batch_engine {
         rows_.offsets.data(), B_, part_r.data(), pact.data(), st.data(), betas.data(), k);
     };
     std::vector<double> ha((size_t)B_ * ld), hb((size_t)B_ * ld), prev(B_, -1.0), sigma2(B_, 0.0);
-    std::vector<double> a(ld), bb(ld);
+    std::vector<char> done(B_, 0);
+    std::vector<int> used_steps(B_, 0);
     eta_.assign(B_, 0.0);
     power_iters_.assign(B_, 0);
     int left = B_, listed = B_, k = 0;
@@ -1217,30 +1219,38 @@ class batch_engine {
       alphas.download(ha.data(), (size_t)k * B_, s_);
       betas.download(hb.data(), (size_t)(k + 1) * B_, s_);
       B200_CUDA_CHECK(cudaStreamSynchronize(s_));
-      for (int b = 0; b < B_; ++b) {
-        if (!pact_h[b]) continue;
-        // betas[0] holds |z0|; the recurrence coefficients are betas[1..].
-        for (int j = 0; j < k; ++j) a[j] = ha[(size_t)j * B_ + b];
-        for (int j = 0; j <= k; ++j) bb[j] = hb[(size_t)j * B_ + b];
-        bool breakdown = false;
-        int used         = k;
-        for (int j = 0; j < k; ++j)
-          if (!(a[j] > 0.0) || !(bb[j + 1] > 0.0) || !std::isfinite(a[j]) ||
-              !std::isfinite(bb[j + 1])) {
-            used      = j + 1;
-            breakdown = true;
-            break;
-          }
-        sigma2[b] = largest_bidiagonal_sigma2(a.data(), bb.data() + 1, used);
-        const bool done = breakdown || k >= kLanczosMaxSteps ||
-                          (prev[b] > 0.0 && std::fabs(sigma2[b] - prev[b]) <= kLanczosTol * sigma2[b]);
-        prev[b] = sigma2[b];
-        if (done) {
-          pact_h[b]        = 0;
-          power_iters_[b]  = used;
+      // Each instance's estimate (a Sturm bisection per instance, the host's share of the step)
+      // is independent of the others: instances are split over host threads, each writing only
+      // its own entries, so the results do not depend on the split.
+      parallel_ranges(B_, [&](int b0, int b1) {
+        std::vector<double> a(ld), bb(ld);
+        for (int b = b0; b < b1; ++b) {
+          if (!pact_h[b]) continue;
+          // betas[0] holds |z0|; the recurrence coefficients are betas[1..].
+          for (int j = 0; j < k; ++j) a[j] = ha[(size_t)j * B_ + b];
+          for (int j = 0; j <= k; ++j) bb[j] = hb[(size_t)j * B_ + b];
+          bool breakdown = false;
+          int used       = k;
+          for (int j = 0; j < k; ++j)
+            if (!(a[j] > 0.0) || !(bb[j + 1] > 0.0) || !std::isfinite(a[j]) ||
+                !std::isfinite(bb[j + 1])) {
+              used      = j + 1;
+              breakdown = true;
+              break;
+            }
+          sigma2[b]     = largest_bidiagonal_sigma2(a.data(), bb.data() + 1, used);
+          done[b]       = breakdown || k >= kLanczosMaxSteps ||
+                    (prev[b] > 0.0 && std::fabs(sigma2[b] - prev[b]) <= kLanczosTol * sigma2[b]);
+          used_steps[b] = used;
+          prev[b]       = sigma2[b];
+        }
+      });
+      for (int b = 0; b < B_; ++b)
+        if (pact_h[b] && done[b]) {
+          pact_h[b]       = 0;
+          power_iters_[b] = used_steps[b];
           --left;
         }
-      }
       if (left == 0) break;
       pact.upload(pact_h.data(), B_, s_);
       if (2 * left <= listed) {

@@ -16,11 +16,11 @@
 
 namespace cuopt_b200 {
 
-// memcpy split over up to 8 host threads for large copies.
+// memcpy split over up to 16 host threads for large copies.
 inline void parallel_memcpy(void* dst, const void* src, size_t bytes)
 {
   constexpr size_t kChunk = size_t(2) << 20;  // at least this much per thread
-  const unsigned hw       = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  const unsigned hw       = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
   const unsigned parts    = (unsigned)std::min<size_t>(hw, bytes / kChunk);
   if (parts <= 1) {
     std::memcpy(dst, src, bytes);
@@ -40,7 +40,42 @@ inline void parallel_memcpy(void* dst, const void* src, size_t bytes)
   for (auto& th : pool) th.join();
 }
 
-// Copies the pieces one after another into dst, split over up to 8 host threads by bytes (a
+// fn(lo, hi) over [0, count) split into contiguous ranges on up to 16 host threads (the calling
+// thread takes the last range; at least `grain` items per range, so small counts run on the
+// calling thread alone).
+template <class F>
+void parallel_ranges(int count, F&& fn, int grain = 16)
+{
+  const int hw    = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  const int parts = std::max(1, std::min(hw, count / std::max(1, grain)));
+  if (parts <= 1) {
+    fn(0, count);
+    return;
+  }
+  auto range = [count, parts](int t, int& lo, int& hi) {
+    lo = (int)((int64_t)count * t / parts);
+    hi = (int)((int64_t)count * (t + 1) / parts);
+  };
+  std::vector<std::thread> pool;
+  int started = 0;
+  try {
+    for (; started < parts - 1; ++started)
+      pool.emplace_back([&fn, &range, t = started] {
+        int lo, hi;
+        range(t, lo, hi);
+        fn(lo, hi);
+      });
+  } catch (...) {  // no thread to spare: the rest runs here
+  }
+  for (int t = started; t < parts; ++t) {
+    int lo, hi;
+    range(t, lo, hi);
+    fn(lo, hi);
+  }
+  for (auto& th : pool) th.join();
+}
+
+// Copies the pieces one after another into dst, split over up to 16 host threads by bytes (a
 // thread's range may cover many small pieces or part of a large one).
 struct host_piece {
   const void* src;
@@ -49,7 +84,7 @@ struct host_piece {
 inline void parallel_gather(char* dst, const host_piece* pieces, size_t count, size_t total)
 {
   constexpr size_t kPerThread = size_t(2) << 20;
-  const unsigned hw    = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  const unsigned hw    = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
   const unsigned parts = (unsigned)std::max<size_t>(1, std::min<size_t>(hw, total / kPerThread));
   auto copy_range = [&](size_t lo, size_t hi) {  // bytes [lo, hi) of the concatenation
     size_t at = 0;

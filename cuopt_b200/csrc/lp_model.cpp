@@ -687,13 +687,16 @@ static void solve_batch_chunk(const std::vector<const lp_problem*>& ps,
   staged_download(hx.data(), x.data(), n * sizeof(double), s);
   staged_download(hy.data(), y.data(), m * sizeof(double), s);
   staged_download(hrc.data(), rc.data(), n * sizeof(double), s);
-  for (int b = 0; b < bi.count; ++b) {
-    lp_solution& o = out[ids[b]];
-    o.r            = rs[b];
-    o.r.x.assign(hx.begin() + bi.col_start[b], hx.begin() + bi.col_start[b + 1]);
-    o.r.rc.assign(hrc.begin() + bi.col_start[b], hrc.begin() + bi.col_start[b + 1]);
-    o.r.y.assign(hy.begin() + bi.row_start[b], hy.begin() + bi.row_start[b + 1]);
-  }
+  // Every instance's slices of the batch solution (independent copies, split over host threads).
+  parallel_ranges(bi.count, [&](int b0, int b1) {
+    for (int b = b0; b < b1; ++b) {
+      lp_solution& o = out[ids[b]];
+      o.r            = rs[b];
+      o.r.x.assign(hx.begin() + bi.col_start[b], hx.begin() + bi.col_start[b + 1]);
+      o.r.rc.assign(hrc.begin() + bi.col_start[b], hrc.begin() + bi.col_start[b + 1]);
+      o.r.y.assign(hy.begin() + bi.row_start[b], hy.begin() + bi.row_start[b + 1]);
+    }
+  });
   // Instances whose FP32 iterates stalled continue, together, in FP64 from where they stopped:
   // their solutions, step sizes and primal weights start an FP64 batch.  With refinement asked
   // for (pdlp_refinement_passes > 0), the Optimal instances of a mixed batch continue with them,
