@@ -762,14 +762,20 @@ std::vector<lp_solution> solve_batch(const std::vector<const lp_problem*>& ps, c
     return out;
   }
   std::vector<row_bounds> rb(ps.size());
-  std::vector<size_t> eligible;
-  for (size_t i = 0; i < ps.size(); ++i) {
-    try {
-      if (prepare_for_pdlp(*ps[i], st, rb[i], out[i])) eligible.push_back(i);
-    } catch (const std::exception& e) {
-      set_error(out[i], CUOPT_RUNTIME_ERROR, e.what());
+  std::vector<char> goes(ps.size(), 0);
+  // Every problem is checked and prepared on its own (split over host threads).
+  parallel_ranges((int)ps.size(), [&](int i0, int i1) {
+    for (int i = i0; i < i1; ++i) {
+      try {
+        goes[i] = prepare_for_pdlp(*ps[i], st, rb[i], out[i]);
+      } catch (const std::exception& e) {
+        set_error(out[i], CUOPT_RUNTIME_ERROR, e.what());
+      }
     }
-  }
+  });
+  std::vector<size_t> eligible;
+  for (size_t i = 0; i < ps.size(); ++i)
+    if (goes[i]) eligible.push_back(i);
   const pdlp_params prm = params_from_settings(st);
   // Chunks that fit the batch layout: at most 65535 instances and int32 totals.
   size_t pos = 0;
