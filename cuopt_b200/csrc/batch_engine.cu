@@ -534,21 +534,47 @@ __global__ void __launch_bounds__(kBlock) b_chunk_sum_kernel(const int4* chunks,
   if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
-// s2 = q . z of the instance;  q <- q (-s2) + z over chunk c;  part_r[c] = sum of the new q^2.
+// The power iteration's step folds the next step's norm and normalisation into this step's
+// chunk kernels (same values as the separate kernels above, two launches fewer per step):
+// part[c] = sum of rowbuf (q_i z_i) over chunk c and part_z[c] = sum of z_i^2 over chunk c.
 __global__ void __launch_bounds__(kBlock)
-  b_chunk_residual_kernel(const int4* chunks, const int* chunk_off, const int* pactive,
-                          const double* part_s2, const double* z, double* q, double* part_r)
+  b_chunk_sum_sumsq_kernel(const int4* chunks, const int* pactive, const double* v,
+                           const double* z, double* part, double* part_z)
 {
   const int4 ch = chunks[blockIdx.x];
   if (!pactive[ch.x]) return;
-  __shared__ double slot;
+  __shared__ double sm[kBlock];
+  ksum acc, acc_z;
+  for (int i = ch.y + threadIdx.x; i < ch.z; i += kBlock) {
+    acc.add(v[i]);
+    acc_z.add(z[i] * z[i]);
+  }
+  const double t   = block_sum(acc, sm);
+  const double t_z = block_sum(acc_z, sm);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x]   = t;
+    part_z[blockIdx.x] = t_z;
+  }
+}
+
+// s2 = q . z of the instance;  part_r[c] = sum over chunk c of (z - s2 q)^2;  then q <- z / |z|,
+// the next step's normalised vector.
+__global__ void __launch_bounds__(kBlock)
+  b_chunk_residual_next_kernel(const int4* chunks, const int* chunk_off, const int* pactive,
+                               const double* part_s2, const double* part_z, const double* z,
+                               double* q, double* part_r)
+{
+  const int4 ch = chunks[blockIdx.x];
+  if (!pactive[ch.x]) return;
+  __shared__ double slot, slot_z;
   __shared__ double sm[kBlock];
   const double s2 = instance_total(part_s2, chunk_off, ch.x, &slot);
+  const double nq = sqrt(instance_total(part_z, chunk_off, ch.x, &slot_z));
   ksum acc;
   for (int i = ch.y + threadIdx.x; i < ch.z; i += kBlock) {
     const double v = q[i] * -s2 + z[i];
-    q[i]           = v;
     acc.add(v * v);
+    q[i] = z[i] / nq;
   }
   const double t = block_sum(acc, sm);
   if (threadIdx.x == 0) part_r[blockIdx.x] = t;
@@ -1079,24 +1105,27 @@ class batch_engine {
       part_r(std::max(nchunks, 1));
     const int4* dchunks_p   = rows_.chunks.data();
     const int* dchunk_off_p = rows_.offsets.data();
+    // q = z0 / |z0| once; every step then ends with the next step's q (z / |z|).
+    b_chunk_sumsq_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks_p, pact.data(), dz.data(),
+                                                     part_z.data());
+    b_chunk_normalize_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks_p, dchunk_off_p, pact.data(),
+                                                         part_z.data(), dz.data(), dq.data());
+    launches_ += 2;
+    B200_LAUNCH_CHECK();
     auto one_iteration = [&]() {
       const auto As  = wview<TX>(true, As_.data());
       const auto ATs = wview<TX>(false, ATs_.data());
-      b_chunk_sumsq_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks_p, pact.data(), dz.data(),
-                                                       part_z.data());
-      b_chunk_normalize_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks_p, dchunk_off_p,
-                                                           pact.data(), part_z.data(), dz.data(),
-                                                           dq.data());
       sell_map_kernel<TX, double, b_store_epi<double>><<<sell_grid(ATs), kBlock, 0, s_>>>(
         ATs, dq.data(), b_store_epi<double>{datq.data(), cctx}, partials_.data());
       sell_map_kernel<TX, double, b_power_z_epi><<<sell_grid(As), kBlock, 0, s_>>>(
         As, datq.data(), b_power_z_epi{dz.data(), dq.data(), rowbuf_.data(), rctx},
         partials_.data());
-      b_chunk_sum_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks_p, pact.data(), rowbuf_.data(),
-                                                     part_s2.data());
-      b_chunk_residual_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks_p, dchunk_off_p,
-                                                          pact.data(), part_s2.data(), dz.data(),
-                                                          dq.data(), part_r.data());
+      b_chunk_sum_sumsq_kernel<<<nchunks, kBlock, 0, s_>>>(dchunks_p, pact.data(),
+                                                           rowbuf_.data(), dz.data(),
+                                                           part_s2.data(), part_z.data());
+      b_chunk_residual_next_kernel<<<nchunks, kBlock, 0, s_>>>(
+        dchunks_p, dchunk_off_p, pact.data(), part_s2.data(), part_z.data(), dz.data(),
+        dq.data(), part_r.data());
       b_power_check_kernel<<<ceil_div(B_, kBlock), kBlock, 0, s_>>>(
         dchunk_off_p, B_, part_s2.data(), part_r.data(), pact.data(), ps.data(), kPowerTol,
         remaining.data());
@@ -1122,7 +1151,7 @@ class batch_engine {
       } else {
         B200_CUDA_CHECK(cudaGraphLaunch(exec, s_));
       }
-      launches_ += 7.0 * std::min(32, kPowerMaxIters - done_iters);
+      launches_ += 5.0 * std::min(32, kPowerMaxIters - done_iters);
       remaining.download(&left, 1, s_);
       B200_CUDA_CHECK(cudaStreamSynchronize(s_));
       if (left == 0) break;
