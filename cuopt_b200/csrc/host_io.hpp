@@ -9,6 +9,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <exception>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -42,7 +44,8 @@ inline void parallel_memcpy(void* dst, const void* src, size_t bytes)
 
 // fn(lo, hi) over [0, count) split into contiguous ranges on up to 16 host threads (the calling
 // thread takes the last range; at least `grain` items per range, so small counts run on the
-// calling thread alone).
+// calling thread alone).  An exception thrown by fn on any thread is rethrown to the caller once
+// every range has ended (the first one, if several threw).
 template <class F>
 void parallel_ranges(int count, F&& fn, int grain = 16)
 {
@@ -52,27 +55,25 @@ void parallel_ranges(int count, F&& fn, int grain = 16)
     fn(0, count);
     return;
   }
-  auto range = [count, parts](int t, int& lo, int& hi) {
-    lo = (int)((int64_t)count * t / parts);
-    hi = (int)((int64_t)count * (t + 1) / parts);
+  std::mutex mu;
+  std::exception_ptr failure;
+  auto run = [&](int t) {
+    try {
+      fn((int)((int64_t)count * t / parts), (int)((int64_t)count * (t + 1) / parts));
+    } catch (...) {
+      std::lock_guard<std::mutex> lock(mu);
+      if (!failure) failure = std::current_exception();
+    }
   };
   std::vector<std::thread> pool;
   int started = 0;
   try {
-    for (; started < parts - 1; ++started)
-      pool.emplace_back([&fn, &range, t = started] {
-        int lo, hi;
-        range(t, lo, hi);
-        fn(lo, hi);
-      });
+    for (; started < parts - 1; ++started) pool.emplace_back(run, started);
   } catch (...) {  // no thread to spare: the rest runs here
   }
-  for (int t = started; t < parts; ++t) {
-    int lo, hi;
-    range(t, lo, hi);
-    fn(lo, hi);
-  }
+  for (int t = started; t < parts; ++t) run(t);
   for (auto& th : pool) th.join();
+  if (failure) std::rethrow_exception(failure);
 }
 
 // Copies the pieces one after another into dst, split over up to 16 host threads by bytes (a
